@@ -1,0 +1,257 @@
+"""ctypes wrapper of the CPU FP64 restatement (``libfeicar_oracle.so``).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by bench.py's CPU-baseline leg, always as the checker, never as the
+product path.  Parity status: pinned by known answers only; the Fortran
+reference cannot be compiled in this image, so parity against reference
+outputs is unpinned.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libfeicar_oracle.so")
+
+OR_PBC_DIRICHLET, OR_PBC_NEUMANN = 1, 2
+OR_SOLVER_LSOR, OR_SOLVER_MG = 1, 3
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("it_solver_type", C.c_int),
+        ("itermax_pson", C.c_int),
+        ("restol_pson", C.c_double),
+        ("restol_gcp", C.c_double),
+        ("itermax_gc", C.c_int),
+        ("omega_pson", C.c_double),
+        ("iterInter", C.c_int),
+        ("pbc", C.c_int * 6),
+        ("ppp", C.c_double * 6),
+        ("vel_zero_gradient", C.c_int * 6),
+        ("mix_GC_form", C.c_int),
+        ("is_PBC_homogeneous", C.c_int),
+        ("freeze_solid", C.c_int),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("outer_iterations", C.c_int),
+        ("vcycles", C.c_int),
+        ("maxres", C.c_double),
+        ("maxres2", C.c_double),
+        ("relres", C.c_double),
+        ("seconds", C.c_double),
+    ]
+
+
+def build() -> str:
+    """Compile the restatement with its Makefile (gcc, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(
+            os.path.join(_HERE, "feicar_oracle.c")
+        ):
+            build()
+        L = C.CDLL(_LIB)
+        P = C.c_void_p
+        dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        L.or_case_create.restype = P
+        L.or_case_create.argtypes = [C.c_int] * 3 + [dp] * 3 + [C.c_int] * 3
+        L.or_case_destroy.argtypes = [P]
+        L.or_case_dims.argtypes = [P, C.POINTER(C.c_int)]
+        L.or_case_level_dims.argtypes = [P, C.c_int, C.POINTER(C.c_int)]
+        L.or_case_add_body.argtypes = [P, C.c_int, C.c_int, dp,
+                                       np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS"),
+                                       C.c_int, C.c_double, C.c_int]
+        L.or_case_update_body.argtypes = [P, C.c_int, dp]
+        L.or_set_iblank_body_fast.argtypes = [P, C.c_int, C.c_int]
+        L.or_gcm_set_internal_boundary.argtypes = [P, C.c_double, C.c_double]
+        L.or_mg_prepare.argtypes = [P]
+        L.or_get_field_i8.argtypes = [P, C.c_int, C.c_void_p]
+        L.or_get_counts.argtypes = [P, C.POINTER(C.c_int)]
+        L.or_get_ghosts.argtypes = [P] + [C.c_void_p] * 9
+        L.or_get_deads.argtypes = [P] + [C.c_void_p] * 8
+        L.or_get_mg_mask.argtypes = [P, C.c_int, C.c_int, C.c_void_p]
+        L.or_solve_poisson.argtypes = [P] + [C.c_void_p] * 5 + [C.POINTER(Params), C.POINTER(Stats)]
+        L.or_ghostcell_pressure.argtypes = [P] + [C.c_void_p] * 5 + [C.POINTER(Params), C.POINTER(C.c_int)]
+        L.or_calc_residual.restype = C.c_double
+        L.or_calc_residual.argtypes = [P, C.c_void_p, C.c_void_p]
+        L.or_relres.restype = C.c_double
+        L.or_relres.argtypes = [P, C.c_void_p, C.c_void_p]
+        L.or_tdma.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_int]
+        L.or_invert8.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+        L.or_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def default_params(**kw) -> Params:
+    """Reference-mode parameters (input.dat keys of MAIN.F90:214-254)."""
+    p = Params()
+    p.it_solver_type = OR_SOLVER_MG
+    p.itermax_pson = kw.get("itermax_pson", 200)
+    p.restol_pson = kw.get("restol_pson", 1e-10)
+    p.restol_gcp = kw.get("restol_gcp", 1e-10)
+    p.itermax_gc = kw.get("itermax_gc", 50)
+    p.omega_pson = kw.get("omega_pson", 1.2)
+    p.iterInter = kw.get("iterInter", 4)
+    for f in range(6):
+        p.pbc[f] = kw.get("pbc", [OR_PBC_NEUMANN] * 6)[f]
+        p.ppp[f] = kw.get("ppp", [0.0] * 6)[f]
+        p.vel_zero_gradient[f] = kw.get("vzg", [0] * 6)[f]
+    p.mix_GC_form = kw.get("mix_GC_form", 0)
+    p.is_PBC_homogeneous = kw.get("is_PBC_homogeneous", 1)
+    p.freeze_solid = kw.get("freeze_solid", 1)
+    if kw.get("lsor"):
+        p.it_solver_type = OR_SOLVER_LSOR
+    return p
+
+
+class OracleCase:
+    """One grid + bodies + GCM state + MG hierarchy of the restatement."""
+
+    def __init__(self, grid, mgrids=(0, 0, 0)):
+        self.grid = grid
+        L = lib()
+        self.h = L.or_case_create(
+            grid.nx, grid.ny, grid.nz,
+            np.ascontiguousarray(grid.xn, dtype=np.float64),
+            np.ascontiguousarray(grid.yn, dtype=np.float64),
+            np.ascontiguousarray(grid.zn, dtype=np.float64), *mgrids)
+        if not self.h:
+            raise ValueError("or_case_create failed")
+        d = (C.c_int * 4)()
+        L.or_case_dims(self.h, d)
+        self.mLevel = d[3]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_case_destroy(self.h)
+            self.h = None
+
+    @property
+    def shape(self):
+        return self.grid.shape
+
+    def level_dims(self, lev):
+        d = (C.c_int * 3)()
+        lib().or_case_level_dims(self.h, lev, d)
+        return tuple(d)
+
+    def add_body(self, body):
+        xyz = np.ascontiguousarray(body.verts, dtype=np.float64).ravel()
+        tri = np.ascontiguousarray(body.tri, dtype=np.int32).ravel()
+        rc = lib().or_case_add_body(self.h, body.nvert, body.ntri, xyz, tri, body.surface,
+                                    body.membrane_tkns, body.body_dim)
+        if rc:
+            raise ValueError(f"or_case_add_body -> {rc}")
+
+    def update_body(self, ibody, verts):
+        rc = lib().or_case_update_body(self.h, ibody, np.ascontiguousarray(verts, np.float64).ravel())
+        if rc:
+            raise ValueError(f"or_case_update_body -> {rc}")
+
+    def set_iblank(self, ntime=1, ntime_start=0):
+        return lib().or_set_iblank_body_fast(self.h, ntime, ntime_start)
+
+    def gcm(self, pln=2.0, plnD=2.0):
+        return lib().or_gcm_set_internal_boundary(self.h, pln, plnD)
+
+    def mg_prepare(self):
+        return lib().or_mg_prepare(self.h)
+
+    def field(self, which):
+        out = np.zeros(self.shape, dtype=np.int8, order="F")
+        lib().or_get_field_i8(self.h, which, _ptr(out))
+        return out
+
+    def mg_mask(self, lev, which):
+        I, J, K = self.level_dims(lev)
+        out = np.zeros((I + 2, J + 2, K + 2), dtype=np.int8, order="F")
+        lib().or_get_mg_mask(self.h, lev, which, _ptr(out))
+        return out
+
+    def counts(self):
+        d = (C.c_int * 6)()
+        lib().or_get_counts(self.h, d)
+        keys = ["nGhost", "nDead", "nWarnSide", "nHostFail", "nStencilSolid", "nFallbackDead"]
+        return dict(zip(keys, list(d)))
+
+    def ghosts(self):
+        n = self.counts()["nGhost"]
+        r = dict(ijk=np.zeros((n, 3), np.int32), cell=np.zeros((n, 3), np.int32),
+                 coefN=np.zeros((n, 8)), coefD=np.zeros((n, 8)), bi=np.zeros((n, 3)),
+                 ip=np.zeros((n, 3)), probe=np.zeros(n), closest=np.zeros(n, np.int32),
+                 alpha=np.zeros(n))
+        lib().or_get_ghosts(self.h, *[_ptr(r[k]) for k in
+                                      ["ijk", "cell", "coefN", "coefD", "bi", "ip", "probe", "closest", "alpha"]])
+        return r
+
+    def deads(self):
+        n = self.counts()["nDead"]
+        r = dict(ijk=np.zeros((n, 3), np.int32), cell=np.zeros((n, 3), np.int32),
+                 coefN=np.zeros((n, 8)), coefD=np.zeros((n, 8)), bi=np.zeros((n, 3)),
+                 ip=np.zeros((n, 3)), probe=np.zeros(n), closest=np.zeros(n, np.int32))
+        lib().or_get_deads(self.h, *[_ptr(r[k]) for k in
+                                     ["ijk", "cell", "coefN", "coefD", "bi", "ip", "probe", "closest"]])
+        return r
+
+    def solve_poisson(self, p, div, p_old=None, params=None, dpdn_g=None, dpdn_d=None):
+        """CORE_POISSON.F90:83-200 on Fortran-ordered float64 arrays (p is
+        updated in place).  Returns (status, stats dict)."""
+        assert p.flags.f_contiguous and div.flags.f_contiguous
+        prm = params or default_params()
+        st = Stats()
+        rc = lib().or_solve_poisson(self.h, _ptr(p), _ptr(div), _ptr(p_old), _ptr(dpdn_g),
+                                    _ptr(dpdn_d), C.byref(prm), C.byref(st))
+        return rc, {k: getattr(st, k) for k, _ in Stats._fields_}
+
+    def ghostcell_pressure(self, p, div, p_old=None, params=None):
+        prm = params or default_params()
+        it = C.c_int()
+        rc = lib().or_ghostcell_pressure(self.h, _ptr(p), _ptr(div), _ptr(p_old), None, None,
+                                         C.byref(prm), C.byref(it))
+        return rc, it.value
+
+    def relres(self, p, div):
+        return lib().or_relres(self.h, _ptr(p), _ptr(div))
+
+    def calc_residual(self, p, div):
+        return lib().or_calc_residual(self.h, _ptr(p), _ptr(div))
+
+
+def tdma(a, b, c, r, n1, n2):
+    u = np.zeros_like(r)
+    lib().or_tdma(_ptr(a), _ptr(b), _ptr(c), _ptr(r), _ptr(u), n1, n2)
+    return u
+
+
+def invert8(a):
+    """8x8 inverse with LAPACK getrf/getri semantics (column-major in/out)."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    out = np.zeros((8, 8), order="F")
+    info = C.c_int()
+    lib().or_invert8(_ptr(a), _ptr(out), C.byref(info))
+    return out, info.value
+
+
+def set_threads(n):
+    lib().or_set_threads(n)
