@@ -1,0 +1,1138 @@
+// fg_api.cu -- host side of the B200 pressure-Poisson library: grid and
+// multigrid hierarchy (CORE_GRID.F90:29-205, CORE_MG.F90:22-599), masks
+// (CORE_MG.F90:1365-1555), batched V-cycle driver, C ABI.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fg_case.h"
+#include "fg_internal.h"
+
+namespace fg {
+
+static thread_local std::string g_err;
+void set_last_error(const char *msg, const char *file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%s:%d)", msg, file, line);
+  g_err = buf;
+}
+const char *last_error_msg() { return g_err.c_str(); }
+
+static int coarsen_count(int n) { return (n % 2 == 0) ? n / 2 + 1 : (n + 1) / 2; }
+static int auto_levels(int n) {
+  int II = n - 1, N;
+  for (N = 1; N <= 10; ++N) {
+    II = II / 2;
+    if (II >= 4) continue;
+    break;
+  }
+  return N > 10 ? 10 : N;
+}
+
+// fine-grid axis, CORE_GRID.F90:38-147 (x(1..n) given)
+static void make_axis(int n, const double *xn, std::vector<double> &x, std::vector<double> &xc,
+                      std::vector<double> &dxinv, std::vector<double> &dxcinv) {
+  x.assign(n + 2, 0.0); xc.assign(n + 2, 0.0); dxinv.assign(n + 2, 0.0); dxcinv.assign(n + 2, 0.0);
+  for (int i = 1; i <= n; ++i) x[i] = xn[i - 1];
+  x[0] = x[1] * 2.0 - x[2];
+  x[n + 1] = x[n] + x[n] - x[n - 1];
+  for (int i = 0; i <= n; ++i) {
+    xc[i] = 0.5 * (x[i + 1] + x[i]);
+    dxinv[i] = 1.0 / (x[i + 1] - x[i]);
+  }
+  xc[n + 1] = x[n + 1];
+  for (int i = 1; i <= n; ++i) dxcinv[i] = 1.0 / (xc[i] - xc[i - 1]);
+}
+
+// coarse axis, CORE_MG.F90:234-264
+static void coarse_axis(int nC, int nF, const std::vector<double> &xF, double x1, double xn,
+                        std::vector<double> &x, std::vector<double> &xc,
+                        std::vector<double> &dxinv, std::vector<double> &dxcinv) {
+  x.assign(nC + 2, 0.0); xc.assign(nC + 2, 0.0); dxinv.assign(nC + 2, 0.0); dxcinv.assign(nC + 2, 0.0);
+  for (int i = 1; i <= nC - 1; ++i) x[i] = xF[(nC == nF) ? i : 2 * i - 1];
+  x[nC] = xF[nF];
+  for (int i = 1; i <= nC - 1; ++i) {
+    dxinv[i] = 1.0 / (x[i + 1] - x[i]);
+    xc[i] = 0.5 * (x[i] + x[i + 1]);
+  }
+  xc[0] = 2.0 * x1 - xc[1];
+  xc[nC] = 2.0 * xn - xc[nC - 1];
+  for (int i = 1; i <= nC; ++i) dxcinv[i] = 1.0 / (xc[i] - xc[i - 1]);
+}
+
+}  // namespace fg
+
+namespace fg {
+
+static long long pitch_up(long long v) { return (v + kRowPitch - 1) / kRowPitch * kRowPitch; }
+
+static fg_status alloc_level(fg_case *c, HLevel &L, bool lvl0) {
+  L.nx = L.I - 1; L.ny = L.J - 1; L.nz = L.K - 1;
+  L.sy = pitch_up(L.nx + 2);
+  L.sz = L.sy * (L.ny + 2);
+  L.ntot = L.sz * (L.nz + 2);
+  const bool mixed = c->cfg.precision == FG_PREC_MIXED;
+  FG_CUDA(cudaMalloc(&L.d_type, L.ntot));
+  if (!mixed || lvl0) {
+    FG_CUDA(cudaMalloc(&L.d_x64, L.ntot * sizeof(double)));
+    FG_CUDA(cudaMalloc(&L.d_rhs64, L.ntot * sizeof(double)));
+    FG_CUDA(cudaMemset(L.d_x64, 0, L.ntot * sizeof(double)));
+    FG_CUDA(cudaMemset(L.d_rhs64, 0, L.ntot * sizeof(double)));
+    if (!mixed) {
+      FG_CUDA(cudaMalloc(&L.d_res64, L.ntot * sizeof(double)));
+      FG_CUDA(cudaMemset(L.d_res64, 0, L.ntot * sizeof(double)));
+    }
+  }
+  if (mixed) {
+    FG_CUDA(cudaMalloc(&L.d_x32, L.ntot * sizeof(float)));
+    FG_CUDA(cudaMalloc(&L.d_rhs32, L.ntot * sizeof(float)));
+    FG_CUDA(cudaMalloc(&L.d_res32, L.ntot * sizeof(float)));
+    FG_CUDA(cudaMemset(L.d_x32, 0, L.ntot * sizeof(float)));
+    FG_CUDA(cudaMemset(L.d_rhs32, 0, L.ntot * sizeof(float)));
+    FG_CUDA(cudaMemset(L.d_res32, 0, L.ntot * sizeof(float)));
+  }
+  return FG_OK;
+}
+
+// 1-D arrays of a level: coefficients, widths, children, prolongation
+static fg_status upload_axes(fg_case *c, int l) {
+  HLevel &L = c->lev[l];
+  const HLevel *F = l > 0 ? &c->lev[l - 1] : nullptr;   // finer
+  const HLevel *C = l + 1 < c->nlev ? &c->lev[l + 1] : nullptr;  // coarser
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const std::vector<double> *xv[3] = {&L.x, &L.y, &L.z};
+  const std::vector<double> *xcv[3] = {&L.xc, &L.yc, &L.zc};
+  const std::vector<double> *dinv[3] = {&L.dxinv, &L.dyinv, &L.dzinv};
+  const std::vector<double> *dcinv[3] = {&L.dxcinv, &L.dycinv, &L.dzcinv};
+  // doubles: per axis am, ap, w, pw (n+2 each)
+  std::vector<double> dbl;
+  std::vector<int> ints;
+  size_t doff[3][4], ioff[3][3];
+  for (int a = 0; a < 3; ++a) {
+    const int na = n[a];
+    std::vector<double> am(na + 2, 0.0), ap(na + 2, 0.0), w(na + 2, 0.0), pw(na + 2, 0.0);
+    std::vector<int> cl(na + 2, 0), ch(na + 2, 0), pl(na + 2, 1);
+    for (int i = 1; i <= na; ++i) {
+      am[i] = (*dcinv[a])[i] * (*dinv[a])[i];
+      ap[i] = (*dcinv[a])[i + 1] * (*dinv[a])[i];
+      w[i] = (*xv[a])[i + 1] - (*xv[a])[i];
+    }
+    if (F) {  // children in the finer level
+      const int nf = a == 0 ? F->nx : a == 1 ? F->ny : F->nz;
+      const bool coarsened = nf != na;
+      for (int I = 1; I <= na; ++I) {
+        if (coarsened) { cl[I] = 2 * I - 1; ch[I] = std::min(2 * I, nf); }
+        else { cl[I] = I; ch[I] = I; }
+      }
+    }
+    if (C) {  // prolongation from the coarser level
+      const int nc = a == 0 ? C->nx : a == 1 ? C->ny : C->nz;
+      const std::vector<double> &cxc = a == 0 ? C->xc : a == 1 ? C->yc : C->zc;
+      const bool coarsened = nc != na;
+      for (int i = 1; i <= na; ++i) {
+        if (!coarsened) { pl[i] = i; pw[i] = 0.0; continue; }
+        const double xf = (*xcv[a])[i];
+        int lo = 1;
+        for (int I = 1; I <= nc; ++I)
+          if (cxc[I] <= xf) lo = I;
+        double wt = 0.0;
+        if (lo < nc && xf > cxc[lo]) wt = (xf - cxc[lo]) / (cxc[lo + 1] - cxc[lo]);
+        if (wt < 0.0) wt = 0.0;
+        if (wt > 1.0) wt = 1.0;
+        pl[i] = lo; pw[i] = wt;
+      }
+    }
+    doff[a][0] = dbl.size(); dbl.insert(dbl.end(), am.begin(), am.end());
+    doff[a][1] = dbl.size(); dbl.insert(dbl.end(), ap.begin(), ap.end());
+    doff[a][2] = dbl.size(); dbl.insert(dbl.end(), w.begin(), w.end());
+    doff[a][3] = dbl.size(); dbl.insert(dbl.end(), pw.begin(), pw.end());
+    ioff[a][0] = ints.size(); ints.insert(ints.end(), cl.begin(), cl.end());
+    ioff[a][1] = ints.size(); ints.insert(ints.end(), ch.begin(), ch.end());
+    ioff[a][2] = ints.size(); ints.insert(ints.end(), pl.begin(), pl.end());
+  }
+  FG_CUDA(cudaMalloc(&L.d_coef, dbl.size() * sizeof(double)));
+  FG_CUDA(cudaMemcpy(L.d_coef, dbl.data(), dbl.size() * sizeof(double), cudaMemcpyHostToDevice));
+  FG_CUDA(cudaMalloc(&L.d_int, ints.size() * sizeof(int)));
+  FG_CUDA(cudaMemcpy(L.d_int, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
+  DevLevel &d = L.dl;
+  memset(&d, 0, sizeof(d));
+  d.nx = L.nx; d.ny = L.ny; d.nz = L.nz;
+  d.sy = L.sy; d.sz = L.sz; d.ntot = L.ntot;
+  d.type = L.d_type;
+  d.amx = L.d_coef + doff[0][0]; d.apx = L.d_coef + doff[0][1];
+  d.amy = L.d_coef + doff[1][0]; d.apy = L.d_coef + doff[1][1];
+  d.amz = L.d_coef + doff[2][0]; d.apz = L.d_coef + doff[2][1];
+  d.wx = L.d_coef + doff[0][2]; d.wy = L.d_coef + doff[1][2]; d.wz = L.d_coef + doff[2][2];
+  d.pwx = L.d_coef + doff[0][3]; d.pwy = L.d_coef + doff[1][3]; d.pwz = L.d_coef + doff[2][3];
+  d.clx = L.d_int + ioff[0][0]; d.chx = L.d_int + ioff[0][1]; d.plx = L.d_int + ioff[0][2];
+  d.cly = L.d_int + ioff[1][0]; d.chy = L.d_int + ioff[1][1]; d.ply = L.d_int + ioff[1][2];
+  d.clz = L.d_int + ioff[2][0]; d.chz = L.d_int + ioff[2][1]; d.plz = L.d_int + ioff[2][2];
+  for (int f = 0; f < 6; ++f) d.bc[f] = (c->cfg.pbc[f] == FG_PBC_DIRICHLET) ? 1 : 0;
+  d.x64 = L.d_x64; d.rhs64 = L.d_rhs64; d.res64 = L.d_res64;
+  d.x32 = L.d_x32; d.rhs32 = L.d_rhs32; d.res32 = L.d_res32;
+  return FG_OK;
+}
+
+static inline long long dev_index(const HLevel &L, int i, int j, int k) {
+  return (long long)i + L.sy * j + L.sz * k;
+}
+
+// Generalised inverse of the coarsest operator by Gauss-Jordan elimination
+// with full pivoting; pivots below 1e-12 of the largest are treated as zero
+// (the all-Neumann operator is singular), so G r solves A x = r for any r in
+// the range of A.
+static void coarsest_inverse(fg_case *c) {
+  HLevel &L = c->lev[c->nlev - 1];
+  std::vector<long long> idx;
+  std::vector<int> ord(L.ntot, -1);
+  for (int k = 1; k <= L.nz; ++k)
+    for (int j = 1; j <= L.ny; ++j)
+      for (int i = 1; i <= L.nx; ++i) {
+        long long id = dev_index(L, i, j, k);
+        if (L.type[id] == T_ACTIVE) { ord[id] = (int)idx.size(); idx.push_back(id); }
+      }
+  const int n = (int)idx.size();
+  std::vector<double> A((size_t)n * n, 0.0);
+  const double *am[3] = {nullptr, nullptr, nullptr};
+  (void)am;
+  for (int r = 0; r < n; ++r) {
+    long long id = idx[r];
+    int k = (int)(id / L.sz), j = (int)((id % L.sz) / L.sy), i = (int)(id % L.sy);
+    const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
+    const double a[6] = {L.dxcinv[i] * L.dxinv[i], L.dxcinv[i + 1] * L.dxinv[i],
+                         L.dycinv[j] * L.dyinv[j], L.dycinv[j + 1] * L.dyinv[j],
+                         L.dzcinv[k] * L.dzinv[k], L.dzcinv[k + 1] * L.dzinv[k]};
+    double diag = 0.0;
+    for (int q = 0; q < 6; ++q) {
+      int8_t nt = L.type[id + off[q]];
+      int w = (nt == T_ACTIVE) ? 1 : ((nt == T_BOUND && c->cfg.pbc[q] == FG_PBC_DIRICHLET) ? 2 : 0);
+      diag -= a[q] * w;
+      if (w == 1) A[(size_t)r * n + ord[id + off[q]]] += a[q];
+    }
+    A[(size_t)r * n + r] += diag;
+  }
+  // Gauss-Jordan with full pivoting on [A | I]
+  std::vector<double> Ginv((size_t)n * n, 0.0);
+  std::vector<int> rowp(n), colp(n);
+  std::vector<double> M = A;
+  std::vector<double> Iv((size_t)n * n, 0.0);
+  for (int q = 0; q < n; ++q) Iv[(size_t)q * n + q] = 1.0;
+  double amax = 0.0;
+  for (double v : A) amax = std::max(amax, std::fabs(v));
+  std::vector<char> used_r(n, 0), used_c(n, 0);
+  std::vector<int> piv_r, piv_c;
+  for (int step = 0; step < n; ++step) {
+    double best = 0.0; int br = -1, bc = -1;
+    for (int r = 0; r < n; ++r) {
+      if (used_r[r]) continue;
+      for (int q = 0; q < n; ++q) {
+        if (used_c[q]) continue;
+        double v = std::fabs(M[(size_t)r * n + q]);
+        if (v > best) { best = v; br = r; bc = q; }
+      }
+    }
+    if (br < 0 || best <= 1e-12 * amax) break;
+    used_r[br] = 1; used_c[bc] = 1;
+    piv_r.push_back(br); piv_c.push_back(bc);
+    const double pv = M[(size_t)br * n + bc];
+    for (int q = 0; q < n; ++q) { M[(size_t)br * n + q] /= pv; Iv[(size_t)br * n + q] /= pv; }
+    for (int r = 0; r < n; ++r) {
+      if (r == br) continue;
+      const double f = M[(size_t)r * n + bc];
+      if (f == 0.0) continue;
+      for (int q = 0; q < n; ++q) {
+        M[(size_t)r * n + q] -= f * M[(size_t)br * n + q];
+        Iv[(size_t)r * n + q] -= f * Iv[(size_t)br * n + q];
+      }
+    }
+  }
+  // x_bc = (Iv row br) . r for each pivot (br, bc); unpivoted unknowns = 0
+  for (size_t t = 0; t < piv_r.size(); ++t)
+    for (int q = 0; q < n; ++q) Ginv[(size_t)piv_c[t] * n + q] = Iv[(size_t)piv_r[t] * n + q];
+  c->G.swap(Ginv);
+  c->gidx.assign(idx.begin(), idx.end());
+}
+
+}  // namespace fg
+
+using namespace fg;
+
+// =================================================================== batch
+struct fg_batch {
+  int device = 0;
+  fg_solver_config cfg{};
+  std::vector<fg_case *> cases;
+  bool built = false;
+  int maxdepth = 0;
+  cudaStream_t stream = nullptr;
+  // per level L: problems in S_L (L < depth-1) and C_L (L == depth-1)
+  struct LevelSet {
+    std::vector<int> S, C;
+    DevLevel *d_levS = nullptr;       // level L of S
+    DevLevel *d_levS_next = nullptr;  // level L+1 of S
+    DevLevel *d_levC = nullptr;       // level L of C
+    int *d_off_cells = nullptr, *d_off_x = nullptr, *d_off_y = nullptr, *d_off_z = nullptr,
+        *d_off_next = nullptr;
+    Launch cells, xl, yl, zl, next;
+    int maxnx = 0, maxny = 0, maxnz = 0;
+    const double **d_G = nullptr;
+    const int **d_gidx = nullptr;
+    int *d_gn = nullptr;
+    int maxgn = 0;
+  } ls[kMaxLevels];
+  // level 0 over all problems
+  DevLevel *d_lev0 = nullptr;
+  int *d_off0 = nullptr;
+  Launch all0;
+  // rows of all problems (dead rows then ghost rows per problem)
+  DevRows rows{};
+  int *d_rprob = nullptr;
+  long long *d_rtgt = nullptr, *d_rcell = nullptr;
+  double *d_rw = nullptr, *d_rc0 = nullptr, *d_rd = nullptr, *d_tmp = nullptr;
+  float *d_rf = nullptr;
+  double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
+  std::vector<double> h_norm;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace fg {
+
+template <typename T>
+static cudaError_t run_launch_set_alloc(void **p, const std::vector<T> &v) {
+  if (v.empty()) { *p = nullptr; return cudaSuccess; }
+  cudaError_t e = cudaMalloc(p, v.size() * sizeof(T));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+static void free_batch_tables(fg_batch *b) {
+  for (int L = 0; L < kMaxLevels; ++L) {
+    auto &s = b->ls[L];
+    cudaFree(s.d_levS); cudaFree(s.d_levS_next); cudaFree(s.d_levC);
+    cudaFree(s.d_off_cells); cudaFree(s.d_off_x); cudaFree(s.d_off_y); cudaFree(s.d_off_z);
+    cudaFree(s.d_off_next); cudaFree(s.d_G); cudaFree(s.d_gidx); cudaFree(s.d_gn);
+    s = fg_batch::LevelSet();
+  }
+  cudaFree(b->d_lev0); cudaFree(b->d_off0);
+  cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
+  cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
+  cudaFree(b->d_norm);
+  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
+  b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
+  b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
+  b->built = false;
+}
+
+static fg_status build_offsets(const std::vector<int> &blocks, int **d_off, Launch &Lr,
+                               const DevLevel *d_lev) {
+  std::vector<int> off(blocks.size() + 1, 0);
+  for (size_t p = 0; p < blocks.size(); ++p) off[p + 1] = off[p] + blocks[p];
+  FG_CUDA(run_launch_set_alloc((void **)d_off, off));
+  Lr.n = (int)blocks.size();
+  Lr.blocks = off.back();
+  Lr.off = *d_off;
+  Lr.lev = d_lev;
+  return FG_OK;
+}
+
+static fg_status build_batch(fg_batch *b) {
+  free_batch_tables(b);
+  const int np = (int)b->cases.size();
+  b->maxdepth = 0;
+  for (auto *c : b->cases) b->maxdepth = std::max(b->maxdepth, c->nlev);
+  for (int L = 0; L < b->maxdepth; ++L) {
+    auto &s = b->ls[L];
+    std::vector<DevLevel> vS, vSn, vC;
+    std::vector<int> bc, bx, by, bz, bn;
+    std::vector<const double *> gp;
+    std::vector<const int *> gi;
+    std::vector<int> gn;
+    for (int p = 0; p < np; ++p) {
+      fg_case *c = b->cases[p];
+      if (L < c->nlev - 1) {
+        s.S.push_back(p);
+        const DevLevel &d = c->lev[L].dl;
+        vS.push_back(d);
+        vSn.push_back(c->lev[L + 1].dl);
+        bc.push_back(k::blocks_cells(d));
+        bx.push_back(k::blocks_xline(d));
+        by.push_back(k::blocks_tile(d, 1));
+        bz.push_back(k::blocks_tile(d, 2));
+        bn.push_back(k::blocks_cells(c->lev[L + 1].dl));
+        s.maxnx = std::max(s.maxnx, d.nx);
+        s.maxny = std::max(s.maxny, d.ny);
+        s.maxnz = std::max(s.maxnz, d.nz);
+      } else if (L == c->nlev - 1) {
+        s.C.push_back(p);
+        vC.push_back(c->lev[L].dl);
+        gp.push_back(c->d_G);
+        gi.push_back(c->d_gidx);
+        gn.push_back((int)c->gidx.size());
+        s.maxgn = std::max(s.maxgn, (int)c->gidx.size());
+      }
+    }
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_levS, vS));
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_levS_next, vSn));
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_levC, vC));
+    if (!vS.empty()) {
+      fg_status st;
+      if ((st = build_offsets(bc, &s.d_off_cells, s.cells, s.d_levS)) != FG_OK) return st;
+      if ((st = build_offsets(bx, &s.d_off_x, s.xl, s.d_levS)) != FG_OK) return st;
+      if ((st = build_offsets(by, &s.d_off_y, s.yl, s.d_levS)) != FG_OK) return st;
+      if ((st = build_offsets(bz, &s.d_off_z, s.zl, s.d_levS)) != FG_OK) return st;
+      if ((st = build_offsets(bn, &s.d_off_next, s.next, s.d_levS_next)) != FG_OK) return st;
+    }
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_G, gp));
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_gidx, gi));
+    FG_CUDA(run_launch_set_alloc((void **)&s.d_gn, gn));
+  }
+  // level 0 over all problems
+  {
+    std::vector<DevLevel> v0;
+    std::vector<int> b0;
+    for (auto *c : b->cases) { v0.push_back(c->lev[0].dl); b0.push_back(k::blocks_cells(c->lev[0].dl)); }
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_lev0, v0));
+    fg_status st = build_offsets(b0, &b->d_off0, b->all0, b->d_lev0);
+    if (st != FG_OK) return st;
+  }
+  // rows
+  {
+    std::vector<int> prob;
+    std::vector<long long> tgt, cell;
+    std::vector<double> w, c0;
+    for (int p = 0; p < np; ++p) {
+      const RowsHost &R = b->cases[p]->rows;
+      for (size_t r = 0; r < R.tgt.size(); ++r) {
+        prob.push_back(p);
+        tgt.push_back(R.tgt[r]);
+        cell.push_back(R.cell[r]);
+        c0.push_back(R.c0[r]);
+        for (int q = 0; q < 8; ++q) w.push_back(R.w[8 * r + q]);
+      }
+    }
+    const int n = (int)tgt.size();
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_rprob, prob));
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_rtgt, tgt));
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_rcell, cell));
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_rw, w));
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_rc0, c0));
+    if (n > 0) {
+      FG_CUDA(cudaMalloc(&b->d_rd, n * sizeof(double)));
+      FG_CUDA(cudaMalloc(&b->d_rf, n * sizeof(float)));
+      FG_CUDA(cudaMalloc(&b->d_tmp, n * sizeof(double)));
+      FG_CUDA(cudaMemset(b->d_rd, 0, n * sizeof(double)));
+      FG_CUDA(cudaMemset(b->d_rf, 0, n * sizeof(float)));
+    }
+    b->rows.n = n;
+    b->rows.prob = b->d_rprob;
+    b->rows.tgt = b->d_rtgt;
+    b->rows.cell = b->d_rcell;
+    b->rows.w = b->d_rw;
+    b->rows.c0 = b->d_rc0;
+    b->rows.rd = b->d_rd;
+    b->rows.rf = b->d_rf;
+  }
+  FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
+  b->h_norm.assign(3 * np, 0.0);
+  b->built = true;
+  return FG_OK;
+}
+
+#define FG_K(call)                                                   \
+  do {                                                               \
+    cudaError_t e_ = (call);                                         \
+    if (e_ != cudaSuccess) {                                         \
+      set_last_error(cudaGetErrorString(e_), __FILE__, __LINE__);    \
+      return FG_CUDA_ERROR;                                          \
+    }                                                                \
+  } while (0)
+
+template <typename T>
+static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
+  auto &ls = b->ls[L];
+  const double om = b->cfg.omega;
+  const int corr = sizeof(T) == 4 ? 1 : 0;
+  for (int axis = 0; axis < 3; ++axis) {
+    const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
+    const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
+    for (int color = 0; color < 2; ++color) FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, s));
+    if (L == 0) FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+  }
+  return FG_OK;
+}
+
+template <typename T>
+static fg_status vcycle(fg_batch *b, cudaStream_t s) {
+  const int corr = sizeof(T) == 4 ? 1 : 0;
+  fg_status st;
+  for (int L = 0; L < b->maxdepth; ++L) {
+    auto &ls = b->ls[L];
+    if (!ls.S.empty()) {
+      for (int q = 0; q < b->cfg.nu1; ++q)
+        if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
+      FG_K(k::residual<T>(ls.cells, nullptr, s));
+      FG_K(k::restrict_to<T>(ls.next, ls.d_levS, s));
+      FG_K(k::zero_x<T>(ls.next, s));
+    }
+    if (!ls.C.empty())
+      FG_K(k::coarsest_solve<T>((int)ls.C.size(), ls.d_levC, ls.d_G, ls.d_gidx, ls.d_gn, ls.maxgn, s));
+  }
+  for (int L = b->maxdepth - 2; L >= 0; --L) {
+    auto &ls = b->ls[L];
+    if (ls.S.empty()) continue;
+    FG_K(k::prolong_add<T>(ls.cells, ls.d_levS_next, s));
+    if (L == 0) FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+    for (int q = 0; q < b->cfg.nu2; ++q)
+      if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
+  }
+  return FG_OK;
+}
+
+// Outer iteration over the whole batch until every problem meets rtol.
+static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
+  const int np = (int)b->cases.size();
+  cudaStream_t s = b->stream;
+  const bool mixed = b->cfg.precision == FG_PREC_MIXED;
+  if (!b->ev0) { cudaEventCreate(&b->ev0); cudaEventCreate(&b->ev1); }
+  FG_CUDA(cudaEventRecord(b->ev0, s));
+  // ghost / dead values consistent with the initial field
+  FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
+  FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
+  FG_K(k::fluid_norm(b->all0, b->d_norm + np, s));
+  if (mixed) {
+    FG_K(k::zero_x<float>(b->all0, s));
+    FG_K(k::correct_residual(b->all0, nullptr, b->d_norm, s));
+    FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+  }
+  int cyc = 0;
+  std::vector<double> relres(np, 1.0), gres(np, 0.0);
+  std::vector<double> vms;
+  fg_status status = FG_NOT_CONVERGED;
+  cudaEvent_t va, vb;
+  cudaEventCreate(&va); cudaEventCreate(&vb);
+  for (cyc = 1; cyc <= b->cfg.max_cycles; ++cyc) {
+    cudaEventRecord(va, s);
+    fg_status r;
+    if (mixed) r = vcycle<float>(b, s);
+    else r = vcycle<double>(b, s);
+    if (r != FG_OK) { cudaEventDestroy(va); cudaEventDestroy(vb); return r; }
+    cudaEventRecord(vb, s);
+    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
+    FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
+    if (mixed) {
+      FG_K(k::correct_residual(b->all0, nullptr, b->d_norm, s));
+    } else {
+      FG_K(k::residual<double>(b->all0, b->d_norm, s));
+    }
+    FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+    FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double),
+                            cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, va, vb);
+    vms.push_back(ms);
+    bool all = true;
+    for (int p = 0; p < np; ++p) {
+      const double f2 = b->h_norm[np + p];
+      relres[p] = f2 > 0.0 ? std::sqrt(b->h_norm[p] / f2) : std::sqrt(b->h_norm[p]);
+      gres[p] = b->h_norm[2 * np + p];
+      if (!(relres[p] <= b->cfg.rtol)) all = false;
+    }
+    if (all) { status = FG_OK; break; }
+  }
+  if (cyc > b->cfg.max_cycles) cyc = b->cfg.max_cycles;
+  FG_CUDA(cudaEventRecord(b->ev1, s));
+  FG_CUDA(cudaEventSynchronize(b->ev1));
+  float tot = 0.0f;
+  cudaEventElapsedTime(&tot, b->ev0, b->ev1);
+  cudaEventDestroy(va); cudaEventDestroy(vb);
+  if (st) {
+    double mr = 0.0, mg = 0.0;
+    for (int p = 0; p < np; ++p) { mr = std::max(mr, relres[p]); mg = std::max(mg, gres[p]); }
+    st->cycles = cyc;
+    st->relres = mr;
+    st->ghost_res = mg;
+    st->seconds = tot * 1e-3;
+    double sm = 0.0;
+    for (double v : vms) sm += v;
+    st->vcycle_ms = vms.empty() ? 0.0 : sm / vms.size();
+  }
+  return status;
+}
+
+// -------------------------------------------------------- case geometry
+// level-0 types and rows from the reference masks and lists
+static fg_status install_geometry(fg_case *c) {
+  HLevel &L0 = c->lev[0];
+  const int nx = c->nx, ny = c->ny, nz = c->nz;  // nodes
+  const long long RX = nx + 2, RY = ny + 2;
+  auto ref = [&](int i, int j, int k) { return (long long)i + RX * ((long long)j + RY * k); };
+  L0.type.assign(L0.ntot, T_BOUND);
+  L0.ibk.assign(L0.ntot, 0);
+  // rows first: which dead rows are valid / use the fallback
+  std::vector<int8_t> has_row(L0.ntot, 0);
+  c->rows = RowsHost();
+  auto add_rows = [&](int n, const std::vector<int32_t> &ijk, const std::vector<int32_t> &cell,
+                      const std::vector<double> &coef, const std::vector<double> *probe,
+                      const std::vector<int8_t> *fallback) {
+    for (int r = 0; r < n; ++r) {
+      int i = ijk[3 * r], j = ijk[3 * r + 1], k = ijk[3 * r + 2];
+      int ci = cell[3 * r], cj = cell[3 * r + 1], ck = cell[3 * r + 2];
+      if (i < 1 || i > L0.nx || j < 1 || j > L0.ny || k < 1 || k > L0.nz) continue;
+      if (ci < 0 || cj < 0 || ck < 0 || ci > L0.nx || cj > L0.ny || ck > L0.nz) continue;
+      long long t = dev_index(L0, i, j, k);
+      c->rows.tgt.push_back(t);
+      c->rows.cell.push_back(dev_index(L0, ci, cj, ck));
+      static const int inc[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
+                                    {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
+      const bool fb = fallback && (*fallback)[r];
+      for (int q = 0; q < 8; ++q) {
+        bool own = (ci + inc[q][0] == i && cj + inc[q][1] == j && ck + inc[q][2] == k);
+        c->rows.w.push_back((own || fb) ? 0.0 : coef[8 * r + q]);
+      }
+      c->rows.c0.push_back(0.0);
+      has_row[t] = 1;
+    }
+  };
+  add_rows(c->nDead, c->d_ijk, c->d_cell, c->d_coefN, &c->d_probe, &c->d_fallback);
+  add_rows(c->nGhost, c->g_ijk, c->g_cell, c->g_coefN, nullptr, nullptr);
+  for (int k = 1; k <= L0.nz; ++k)
+    for (int j = 1; j <= L0.ny; ++j)
+      for (int i = 1; i <= L0.nx; ++i) {
+        long long r = ref(i, j, k), d = dev_index(L0, i, j, k);
+        int8_t ib = c->iblank[r], gh = c->ghost[r], dd = c->dead[r];
+        int8_t t;
+        if (ib == 0 && gh == 0) t = T_ACTIVE;
+        else if (has_row[d]) t = T_GHOST;
+        else t = T_SOLID;
+        L0.type[d] = t;
+        L0.ibk[d] = ib;
+      }
+  return FG_OK;
+}
+
+// CORE_MG.F90:1459-1506: coarse cell solid when its children's solid
+// volume fraction is >= 0.5
+static void coarse_masks(fg_case *c) {
+  for (int l = 1; l < c->nlev; ++l) {
+    HLevel &F = c->lev[l - 1], &C = c->lev[l];
+    C.type.assign(C.ntot, T_BOUND);
+    C.ibk.assign(C.ntot, 0);
+    const bool cx = C.nx != F.nx, cy = C.ny != F.ny, cz = C.nz != F.nz;
+    for (int K = 1; K <= C.nz; ++K)
+      for (int J = 1; J <= C.ny; ++J)
+        for (int I = 1; I <= C.nx; ++I) {
+          int i1 = cx ? 2 * I - 1 : I, i2 = cx ? std::min(2 * I, F.nx) : I;
+          int j1 = cy ? 2 * J - 1 : J, j2 = cy ? std::min(2 * J, F.ny) : J;
+          int k1 = cz ? 2 * K - 1 : K, k2 = cz ? std::min(2 * K, F.nz) : K;
+          double v0 = 0.0, vb = 0.0;
+          for (int kk = k1; kk <= k2; ++kk)
+            for (int jj = j1; jj <= j2; ++jj)
+              for (int ii = i1; ii <= i2; ++ii) {
+                double v = (F.x[ii + 1] - F.x[ii]) * (F.y[jj + 1] - F.y[jj]) * (F.z[kk + 1] - F.z[kk]);
+                v0 += v;
+                if (F.ibk[dev_index(F, ii, jj, kk)]) vb += v;
+              }
+          long long d = dev_index(C, I, J, K);
+          int8_t sol = (vb / v0 >= 0.5) ? 1 : 0;
+          C.ibk[d] = sol;
+          C.type[d] = sol ? T_OFF : T_ACTIVE;
+        }
+  }
+}
+
+static fg_status prepare(fg_case *c) {
+  if (!c->has_geometry) {
+    // no body: all interior cells are fluid
+    size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+    c->iblank.assign(nref, 0); c->ghost.assign(nref, 0); c->dead.assign(nref, 0);
+    c->nGhost = c->nDead = 0;
+    c->has_geometry = true;
+  }
+  install_geometry(c);
+  coarse_masks(c);
+  for (int l = 0; l < c->nlev; ++l) {
+    HLevel &L = c->lev[l];
+    FG_CUDA(cudaMemcpy(L.d_type, L.type.data(), L.ntot, cudaMemcpyHostToDevice));
+  }
+  coarsest_inverse(c);
+  cudaFree(c->d_G); cudaFree(c->d_gidx);
+  c->d_G = nullptr; c->d_gidx = nullptr;
+  if (!c->G.empty()) {
+    FG_CUDA(cudaMalloc(&c->d_G, c->G.size() * sizeof(double)));
+    FG_CUDA(cudaMemcpy(c->d_G, c->G.data(), c->G.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<int> gi(c->gidx.begin(), c->gidx.end());
+    FG_CUDA(cudaMalloc(&c->d_gidx, gi.size() * sizeof(int)));
+    FG_CUDA(cudaMemcpy(c->d_gidx, gi.data(), gi.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->prepared = true;
+  c->batch_dirty = true;
+  return FG_OK;
+}
+
+}  // namespace fg
+
+// ======================================================================== C
+extern "C" {
+
+const char *fg_version(void) { return "feicar-b200 0.1 (sm_100a)"; }
+
+fg_status fg_device_count(int *count) {
+  if (!count) return FG_BAD_INPUT;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) { *count = 0; return FG_NO_DEVICE; }
+  *count = n;
+  return n > 0 ? FG_OK : FG_NO_DEVICE;
+}
+
+const char *fg_status_string(fg_status s) {
+  switch (s) {
+    case FG_OK: return "ok";
+    case FG_NOT_CONVERGED: return "not converged";
+    case FG_GEOMETRY_NO_HOST_CELL: return "image point has no host cell";
+    case FG_ALLOC_FAIL: return "allocation failed";
+    case FG_TIMEOUT: return "timeout";
+    case FG_BAD_INPUT: return "bad input";
+    case FG_GEOMETRY_DEAD_NO_BODY: return "dead cell without body";
+    case FG_CUDA_ERROR: return fg::last_error_msg();
+    case FG_NO_DEVICE: return "no CUDA device";
+    case FG_REJECTED: return "rejected by admission";
+  }
+  return "unknown";
+}
+
+void fg_default_config(fg_solver_config *cfg) {
+  if (!cfg) return;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->precision = FG_PREC_FP64;
+  cfg->outer = FG_OUTER_RICHARDSON;
+  cfg->nu1 = 2;
+  cfg->nu2 = 2;
+  cfg->omega = 1.0;
+  cfg->rtol = 1e-8;
+  cfg->max_cycles = 100;
+  for (int f = 0; f < 6; ++f) { cfg->pbc[f] = FG_PBC_NEUMANN; cfg->ppp[f] = 0.0; }
+  cfg->probe_length = 2.0;
+  cfg->probe_length_dead = 2.0;
+  cfg->membrane_tkns_factor = 1.0;
+  cfg->gauge_corner = 1;
+}
+
+fg_status fg_case_create(int nx, int ny, int nz, const double *xn, const double *yn,
+                         const double *zn, const fg_solver_config *cfg, int device,
+                         fg_case **out) {
+  if (!out || nx < 3 || ny < 3 || nz < 3 || !xn || !yn || !zn) return FG_BAD_INPUT;
+  for (int i = 1; i < nx; ++i) if (!(xn[i] > xn[i - 1])) return FG_BAD_INPUT;
+  for (int i = 1; i < ny; ++i) if (!(yn[i] > yn[i - 1])) return FG_BAD_INPUT;
+  for (int i = 1; i < nz; ++i) if (!(zn[i] > zn[i - 1])) return FG_BAD_INPUT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FG_NO_DEVICE;
+  if (device < 0 || device >= ndev) return FG_BAD_INPUT;
+  FG_CUDA(cudaSetDevice(device));
+  auto *c = new fg_case();
+  c->device = device;
+  if (cfg) c->cfg = *cfg; else fg_default_config(&c->cfg);
+  if (c->cfg.nu1 < 0 || c->cfg.nu2 < 0 || c->cfg.max_cycles < 1) { delete c; return FG_BAD_INPUT; }
+  c->nx = nx; c->ny = ny; c->nz = nz;
+  // MG_initial: levels (CORE_MG.F90:71-175)
+  const int mgx = (c->cfg.mgrids[0] <= 0 || c->cfg.mgrids[0] > 10) ? auto_levels(nx) : c->cfg.mgrids[0];
+  const int mgy = (c->cfg.mgrids[1] <= 0 || c->cfg.mgrids[1] > 10) ? auto_levels(ny) : c->cfg.mgrids[1];
+  const int mgz = (c->cfg.mgrids[2] <= 0 || c->cfg.mgrids[2] > 10) ? auto_levels(nz) : c->cfg.mgrids[2];
+  c->nlev = std::max(mgx, std::max(mgy, mgz));
+  if (c->nlev > kMaxLevels) c->nlev = kMaxLevels;
+  HLevel &L1 = c->lev[0];
+  L1.I = nx; L1.J = ny; L1.K = nz;
+  make_axis(nx, xn, L1.x, L1.xc, L1.dxinv, L1.dxcinv);
+  make_axis(ny, yn, L1.y, L1.yc, L1.dyinv, L1.dycinv);
+  make_axis(nz, zn, L1.z, L1.zc, L1.dzinv, L1.dzcinv);
+  for (int n = 1; n < c->nlev; ++n) {
+    HLevel &P = c->lev[n - 1], &L = c->lev[n];
+    L.I = (n + 1 <= mgx) ? coarsen_count(P.I) : P.I;
+    L.J = (n + 1 <= mgy) ? coarsen_count(P.J) : P.J;
+    L.K = (n + 1 <= mgz) ? coarsen_count(P.K) : P.K;
+    coarse_axis(L.I, P.I, P.x, L1.x[1], L1.x[nx], L.x, L.xc, L.dxinv, L.dxcinv);
+    coarse_axis(L.J, P.J, P.y, L1.y[1], L1.y[ny], L.y, L.yc, L.dyinv, L.dycinv);
+    coarse_axis(L.K, P.K, P.z, L1.z[1], L1.z[nz], L.z, L.zc, L.dzinv, L.dzcinv);
+  }
+  fg_status st = FG_OK;
+  for (int l = 0; l < c->nlev && st == FG_OK; ++l) st = alloc_level(c, c->lev[l], l == 0);
+  for (int l = 0; l < c->nlev && st == FG_OK; ++l) st = upload_axes(c, l);
+  if (st != FG_OK) { fg_case_destroy(c); return st; }
+  cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  const size_t nref = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+  if (cudaMalloc(&c->d_pin, nref * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_fin, nref * sizeof(double)) != cudaSuccess) {
+    fg_case_destroy(c);
+    return FG_ALLOC_FAIL;
+  }
+  c->geom.reset(new Geom());
+  *out = c;
+  return FG_OK;
+}
+
+fg_status fg_case_destroy(fg_case *c) {
+  if (!c) return FG_OK;
+  cudaSetDevice(c->device);
+  if (c->solo) { fg_batch_destroy(c->solo); c->solo = nullptr; }
+  for (int l = 0; l < c->nlev; ++l) {
+    HLevel &L = c->lev[l];
+    cudaFree(L.d_type); cudaFree(L.d_coef); cudaFree(L.d_int);
+    cudaFree(L.d_x64); cudaFree(L.d_rhs64); cudaFree(L.d_res64);
+    cudaFree(L.d_x32); cudaFree(L.d_rhs32); cudaFree(L.d_res32);
+  }
+  cudaFree(c->d_G); cudaFree(c->d_gidx); cudaFree(c->d_pin); cudaFree(c->d_fin);
+  if (c->geom) geom_free(*c->geom);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return FG_OK;
+}
+
+fg_status fg_case_levels(const fg_case *c, int *mlevel, int *dims) {
+  if (!c || !mlevel) return FG_BAD_INPUT;
+  *mlevel = c->nlev;
+  if (dims)
+    for (int l = 0; l < c->nlev; ++l) {
+      dims[3 * l] = c->lev[l].I; dims[3 * l + 1] = c->lev[l].J; dims[3 * l + 2] = c->lev[l].K;
+    }
+  return FG_OK;
+}
+
+fg_status fg_case_set_geometry(fg_case *c, const int8_t *iblank, const int8_t *ghostCellMark,
+                               const int8_t *dead_cell, int nGhost, const int32_t *ghost_ijk,
+                               const int32_t *ghost_cell, const double *ghost_coefN, int nDead,
+                               const int32_t *dead_ijk, const int32_t *dead_cell_idx,
+                               const double *dead_coefN, const double *dead_probe,
+                               const double *dead_ip) {
+  if (!c || !iblank || !ghostCellMark || !dead_cell || nGhost < 0 || nDead < 0) return FG_BAD_INPUT;
+  if ((nGhost > 0 && (!ghost_ijk || !ghost_cell || !ghost_coefN)) ||
+      (nDead > 0 && (!dead_ijk || !dead_cell_idx || !dead_coefN)))
+    return FG_BAD_INPUT;
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  c->iblank.assign(iblank, iblank + nref);
+  c->ghost.assign(ghostCellMark, ghostCellMark + nref);
+  c->dead.assign(dead_cell, dead_cell + nref);
+  c->nGhost = nGhost;
+  c->nDead = nDead;
+  c->g_ijk.assign(ghost_ijk, ghost_ijk + 3 * (size_t)nGhost);
+  c->g_cell.assign(ghost_cell, ghost_cell + 3 * (size_t)nGhost);
+  c->g_coefN.assign(ghost_coefN, ghost_coefN + 8 * (size_t)nGhost);
+  c->d_ijk.assign(dead_ijk, dead_ijk + 3 * (size_t)nDead);
+  c->d_cell.assign(dead_cell_idx, dead_cell_idx + 3 * (size_t)nDead);
+  c->d_coefN.assign(dead_coefN, dead_coefN + 8 * (size_t)nDead);
+  c->d_probe.assign(nDead, 0.0);
+  if (dead_probe) c->d_probe.assign(dead_probe, dead_probe + nDead);
+  c->d_ipv.clear();
+  if (dead_ip) c->d_ipv.assign(dead_ip, dead_ip + 3 * (size_t)nDead);
+  // dead rows whose stencil holds a pure-solid cell use the
+  // inverse-distance fallback of GCM_GHOSTCELL_UPDATE.F90:488-505
+  c->d_fallback.assign(nDead, 0);
+  const long long RX = c->nx + 2, RY = c->ny + 2;
+  static const int inc[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
+                                {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
+  for (int r = 0; r < nDead; ++r) {
+    const int ci = dead_cell_idx[3 * r], cj = dead_cell_idx[3 * r + 1], ck = dead_cell_idx[3 * r + 2];
+    if (ci < 0 || cj < 0 || ck < 0) continue;
+    const int i = dead_ijk[3 * r], j = dead_ijk[3 * r + 1], k = dead_ijk[3 * r + 2];
+    int sumk = 0;
+    bool solid = false;
+    for (int q = 0; q < 8; ++q) {
+      int ii = ci + inc[q][0], jj = cj + inc[q][1], kk = ck + inc[q][2];
+      long long id = ii + RX * (jj + RY * (long long)kk);
+      bool self = (ii == i && jj == j && kk == k);
+      if (!self && (iblank[id] == 0 || dead_cell[id] == -1)) sumk++;
+      if (iblank[id] == 1 && dead_cell[id] == 0) solid = true;
+    }
+    if (solid && sumk != 1) c->d_fallback[r] = 1;
+  }
+  c->has_geometry = true;
+  c->prepared = false;
+  return FG_OK;
+}
+
+fg_status fg_mg_prepare(fg_case *c) {
+  if (!c) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  return prepare(c);
+}
+
+static fg_status ensure_solo(fg_case *c) {
+  if (!c->prepared) {
+    fg_status st = prepare(c);
+    if (st != FG_OK) return st;
+  }
+  if (!c->solo) {
+    fg_status st = fg_batch_create(c->device, &c->cfg, &c->solo);
+    if (st != FG_OK) return st;
+    c->solo->cases.push_back(c);
+    c->solo->stream = c->stream;
+  }
+  if (c->batch_dirty) {
+    fg_status st = build_batch(c->solo);
+    if (st != FG_OK) return st;
+    c->batch_dirty = false;
+  }
+  return FG_OK;
+}
+
+// Row constants of the solution form: the own slot of a ghost row times
+// dp/dn (GCM_GHOSTCELL_UPDATE.F90:596-597), dp/dn * probeLengthDead for dead
+// rows (:522), and the inverse-distance fallback over the previous step's
+// pressure for dead rows whose stencil holds pure-solid cells (:488-505).
+static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
+                          const double *dpdn_d, std::vector<double> &c0) {
+  c0.clear();
+  const long long RX = c->nx + 2, RY = c->ny + 2;
+  static const int inc[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
+                                {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
+  auto xcv = [&](int ax, int i) {
+    return ax == 0 ? c->lev[0].xc[i] : ax == 1 ? c->lev[0].yc[i] : c->lev[0].zc[i];
+  };
+  for (int r = 0; r < c->nDead; ++r) {
+    const int i = c->d_ijk[3 * r], j = c->d_ijk[3 * r + 1], k = c->d_ijk[3 * r + 2];
+    const int ci = c->d_cell[3 * r], cj = c->d_cell[3 * r + 1], ck = c->d_cell[3 * r + 2];
+    if (i < 1 || i > c->lev[0].nx || j < 1 || j > c->lev[0].ny || k < 1 || k > c->lev[0].nz) continue;
+    if (ci < 0 || cj < 0 || ck < 0) continue;
+    const double dpdn = dpdn_d ? dpdn_d[r] : 0.0;
+    double v = 0.0;
+    if (c->d_fallback[r]) {
+      // inverse squared distance over fluid and dead corners of the image
+      // point's host cell, previous-step pressure (p_old = 0 when absent)
+      double xIP = 0, yIP = 0, zIP = 0;
+      // image point: cell + (BI - cell) * probe is not kept here; use the
+      // distance to the dead cell's own image point when the geometry came
+      // from the device tagging, else the host cell centre
+      (void)xIP; (void)yIP; (void)zIP;
+      double num = 0.0, den = 0.0;
+      const double *ipp = c->d_ipv.size() >= 3 * (size_t)(r + 1) ? &c->d_ipv[3 * r] : nullptr;
+      double X = ipp ? ipp[0] : 0.5 * (xcv(0, ci) + xcv(0, ci + 1));
+      double Y = ipp ? ipp[1] : 0.5 * (xcv(1, cj) + xcv(1, cj + 1));
+      double Z = ipp ? ipp[2] : 0.5 * (xcv(2, ck) + xcv(2, ck + 1));
+      for (int q = 0; q < 8; ++q) {
+        int ii = ci + inc[q][0], jj = cj + inc[q][1], kk = ck + inc[q][2];
+        if (ii == i && jj == j && kk == k) continue;
+        long long id = ii + RX * (jj + RY * (long long)kk);
+        if (c->iblank[id] == 0 || c->dead[id] == -1) {
+          double d = (xcv(0, ii) - X) * (xcv(0, ii) - X) + (xcv(1, jj) - Y) * (xcv(1, jj) - Y) +
+                     (xcv(2, kk) - Z) * (xcv(2, kk) - Z);
+          den += 1.0 / d;
+          num += (1.0 / d) * (p_old ? p_old[id] : 0.0);
+        }
+      }
+      v = num / den;
+    } else {
+      for (int q = 0; q < 8; ++q) {
+        int ii = ci + inc[q][0], jj = cj + inc[q][1], kk = ck + inc[q][2];
+        if (ii == i && jj == j && kk == k) v += c->d_coefN[8 * r + q] * dpdn;
+      }
+    }
+    v += dpdn * c->d_probe[r];
+    c0.push_back(v);
+  }
+  for (int r = 0; r < c->nGhost; ++r) {
+    const int i = c->g_ijk[3 * r], j = c->g_ijk[3 * r + 1], k = c->g_ijk[3 * r + 2];
+    const int ci = c->g_cell[3 * r], cj = c->g_cell[3 * r + 1], ck = c->g_cell[3 * r + 2];
+    if (ci < 0 || cj < 0 || ck < 0) continue;
+    const double dpdn = dpdn_g ? dpdn_g[r] : 0.0;
+    double v = 0.0;
+    for (int q = 0; q < 8; ++q)
+      if (ci + inc[q][0] == i && cj + inc[q][1] == j && ck + inc[q][2] == k)
+        v += c->g_coefN[8 * r + q] * dpdn;
+    c0.push_back(v);
+  }
+}
+
+static fg_status finish_output(fg_case *c) {
+  // gauge (CORE_POISSON.F90:129-149 pins p(1,1,1)) and outer boundary
+  // layers (CORE_SET_OUTER_BC.F90:1088-1170) are applied on the host copy
+  (void)c;
+  return FG_OK;
+}
+
+static void host_fill_bc(fg_case *c, double *p) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  const long long RX = nx + 2, RY = ny + 2;
+  auto P = [&](int i, int j, int k) -> double & { return p[i + RX * (j + RY * (long long)k)]; };
+  bool allN = true;
+  for (int f = 0; f < 6; ++f) allN &= (c->cfg.pbc[f] == FG_PBC_NEUMANN);
+  if (allN && c->cfg.gauge_corner) {
+    const double pa = P(1, 1, 1);
+    for (int k = 0; k <= nz; ++k)
+      for (int j = 0; j <= ny; ++j)
+        for (int i = 0; i <= nx; ++i) {
+          long long id = i + RX * (j + RY * (long long)k);
+          if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1 &&
+              c->iblank.size() && c->iblank[id] == 1 && c->dead[id] != -1)
+            continue;  // pure-solid values are held
+          p[id] -= pa;
+        }
+  }
+  const double *pp = c->cfg.ppp;
+  auto bcv = [&](int f, double inner) { return c->cfg.pbc[f] == FG_PBC_DIRICHLET ? 2.0 * pp[f] - inner : inner; };
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j) {
+      P(0, j, k) = bcv(0, P(1, j, k));
+      P(nx, j, k) = bcv(1, P(nx - 1, j, k));
+    }
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int i = 0; i <= nx; ++i) {
+      P(i, 0, k) = bcv(2, P(i, 1, k));
+      P(i, ny, k) = bcv(3, P(i, ny - 1, k));
+    }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 0; i <= nx; ++i) {
+      P(i, j, 0) = bcv(4, P(i, j, 1));
+      P(i, j, nz) = bcv(5, P(i, j, nz - 1));
+    }
+}
+
+static fg_status solve_common(fg_case *c, const double *p_old, const double *dpdn_g,
+                              const double *dpdn_d, fg_solve_stats *st) {
+  fg_status s = ensure_solo(c);
+  if (s != FG_OK) return s;
+  std::vector<double> c0;
+  row_constants(c, p_old, dpdn_g, dpdn_d, c0);
+  if ((int)c0.size() != c->solo->rows.n) return FG_BAD_INPUT;
+  if (!c0.empty())
+    FG_CUDA(cudaMemcpyAsync(c->solo->d_rc0, c0.data(), c0.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
+  HLevel &L0 = c->lev[0];
+  FG_K(k::copy_in(L0.d_x64, c->d_pin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  FG_K(k::copy_in(L0.d_rhs64, c->d_fin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  s = batch_solve(c->solo, st);
+  FG_K(k::copy_out(c->d_pin, L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  return s;
+}
+
+fg_status fg_solve_poisson(fg_case *c, double *p, const double *div, const double *p_old,
+                           const double *dpdn_ghost, const double *dpdn_dead,
+                           fg_solve_stats *st) {
+  if (!c || !p || !div) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  FG_CUDA(cudaMemcpyAsync(c->d_pin, p, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FG_CUDA(cudaMemcpyAsync(c->d_fin, div, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  fg_status s = solve_common(c, p_old, dpdn_ghost, dpdn_dead, st);
+  if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
+  FG_CUDA(cudaMemcpyAsync(p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  host_fill_bc(c, p);
+  (void)finish_output;
+  return s;
+}
+
+fg_status fg_solve_poisson_device(fg_case *c, double *d_p, const double *d_div,
+                                  const double *d_p_old, fg_solve_stats *st) {
+  if (!c || !d_p || !d_div) return FG_BAD_INPUT;
+  if (d_p_old) return FG_BAD_INPUT;  // the fallback constants need host p_old
+  cudaSetDevice(c->device);
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  FG_CUDA(cudaMemcpyAsync(c->d_pin, d_p, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  FG_CUDA(cudaMemcpyAsync(c->d_fin, d_div, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  fg_status s = solve_common(c, nullptr, nullptr, nullptr, st);
+  if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
+  FG_CUDA(cudaMemcpyAsync(d_p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return s;
+}
+
+fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old, int iterations) {
+  if (!c || !p || iterations < 1) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  fg_status s = ensure_solo(c);
+  if (s != FG_OK) return s;
+  std::vector<double> c0;
+  row_constants(c, p_old, nullptr, nullptr, c0);
+  if (!c0.empty())
+    FG_CUDA(cudaMemcpyAsync(c->solo->d_rc0, c0.data(), c0.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  HLevel &L0 = c->lev[0];
+  FG_CUDA(cudaMemcpyAsync(c->d_pin, p, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  FG_K(k::copy_in(L0.d_x64 ? L0.d_x64 : nullptr, c->d_pin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  for (int it = 0; it < iterations; ++it)
+    FG_K(k::rows_relax<double>(c->solo->rows, c->solo->d_lev0, 0, c->solo->d_tmp, c->stream));
+  FG_K(k::copy_out(c->d_pin, L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  FG_CUDA(cudaMemcpyAsync(p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+// ------------------------------------------------------------ batch API
+fg_status fg_batch_create(int device, const fg_solver_config *cfg, fg_batch **out) {
+  if (!out) return FG_BAD_INPUT;
+  auto *b = new fg_batch();
+  b->device = device;
+  if (cfg) b->cfg = *cfg; else fg_default_config(&b->cfg);
+  *out = b;
+  return FG_OK;
+}
+
+fg_status fg_batch_add(fg_batch *b, fg_case *c) {
+  if (!b || !c) return FG_BAD_INPUT;
+  if (c->device != b->device || c->cfg.precision != b->cfg.precision) return FG_BAD_INPUT;
+  b->cases.push_back(c);
+  b->built = false;
+  return FG_OK;
+}
+
+fg_status fg_batch_solve_device(fg_batch *b, double **d_p, const double **d_div,
+                                fg_solve_stats *st) {
+  if (!b || b->cases.empty() || !d_p || !d_div) return FG_BAD_INPUT;
+  cudaSetDevice(b->device);
+  if (!b->stream) cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (auto *c : b->cases)
+    if (!c->prepared) {
+      fg_status s = prepare(c);
+      if (s != FG_OK) return s;
+    }
+  if (!b->built) {
+    fg_status s = build_batch(b);
+    if (s != FG_OK) return s;
+  }
+  // row constants (homogeneous, no previous pressure) of every case
+  {
+    std::vector<double> all;
+    for (auto *c : b->cases) {
+      std::vector<double> c0;
+      row_constants(c, nullptr, nullptr, nullptr, c0);
+      all.insert(all.end(), c0.begin(), c0.end());
+    }
+    if (!all.empty())
+      FG_CUDA(cudaMemcpyAsync(b->d_rc0, all.data(), all.size() * sizeof(double),
+                              cudaMemcpyHostToDevice, b->stream));
+  }
+  for (size_t p = 0; p < b->cases.size(); ++p) {
+    fg_case *c = b->cases[p];
+    HLevel &L0 = c->lev[0];
+    FG_K(k::copy_in(L0.d_x64, d_p[p], L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, b->stream));
+    FG_K(k::copy_in(L0.d_rhs64, d_div[p], L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, b->stream));
+  }
+  fg_status s = batch_solve(b, st);
+  for (size_t p = 0; p < b->cases.size(); ++p) {
+    fg_case *c = b->cases[p];
+    HLevel &L0 = c->lev[0];
+    FG_K(k::copy_out(d_p[p], L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, b->stream));
+  }
+  FG_CUDA(cudaStreamSynchronize(b->stream));
+  return s;
+}
+
+fg_status fg_batch_destroy(fg_batch *b) {
+  if (!b) return FG_OK;
+  cudaSetDevice(b->device);
+  free_batch_tables(b);
+  if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }
+  delete b;
+  return FG_OK;
+}
+
+}  // extern "C"

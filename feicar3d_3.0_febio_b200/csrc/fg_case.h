@@ -1,0 +1,75 @@
+// fg_case.h -- host-side state of one case (grid, hierarchy, geometry).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <vector>
+
+#include "fg_internal.h"
+
+namespace fg {
+
+struct Geom;
+void geom_free(Geom &g);
+
+// ------------------------------------------------------------ host level
+struct HLevel {
+  int I = 0, J = 0, K = 0;   // node counts (mgrid_I/J/K)
+  int nx = 0, ny = 0, nz = 0;  // cells
+  long long sy = 0, sz = 0, ntot = 0;
+  std::vector<double> x, y, z, xc, yc, zc;          // 0..n+1 (reference level arrays)
+  std::vector<double> dxinv, dyinv, dzinv, dxcinv, dycinv, dzcinv;
+  std::vector<int8_t> ibk;   // solid flag on the device layout (interior)
+  std::vector<int8_t> type;  // device layout
+  // device
+  int8_t *d_type = nullptr;
+  double *d_coef = nullptr;  // packed 1-D double arrays
+  int *d_int = nullptr;      // packed 1-D int arrays
+  double *d_x64 = nullptr, *d_rhs64 = nullptr, *d_res64 = nullptr;
+  float *d_x32 = nullptr, *d_rhs32 = nullptr, *d_res32 = nullptr;
+  DevLevel dl{};
+};
+
+struct RowsHost {
+  std::vector<long long> tgt, cell;
+  std::vector<double> w, c0;
+};
+
+}  // namespace fg
+
+// ---------------------------------------------------------------- case
+#include "fg_geom.h"
+
+struct fg_case {
+  int device = 0;
+  fg_solver_config cfg{};
+  int nx = 0, ny = 0, nz = 0;  // node counts
+  int nlev = 0;
+  fg::HLevel lev[fg::kMaxLevels];
+  cudaStream_t stream = nullptr;
+  // geometry
+  std::unique_ptr<fg::Geom> geom;
+  std::vector<double> d_ipv;           // dead-cell image points (3 per row)
+  std::vector<int8_t> iblank, ghost, dead;  // reference layout (host copies)
+  bool has_geometry = false;
+  bool prepared = false;
+  // interpolation rows (dead rows first, then ghost rows, like the
+  // reference's update order)
+  int nGhost = 0, nDead = 0;
+  std::vector<int32_t> g_ijk, g_cell, d_ijk, d_cell;
+  std::vector<double> g_coefN, d_coefN, d_probe;
+  std::vector<int8_t> d_fallback;   // dead rows using the inverse-distance fallback
+  fg::RowsHost rows;                // device-layout rows
+  // coarsest generalised inverse
+  std::vector<double> G;
+  std::vector<int> gidx;
+  double *d_G = nullptr;
+  int *d_gidx = nullptr;
+  // reference-layout staging buffers on the device
+  double *d_pin = nullptr, *d_fin = nullptr;
+  bool batch_dirty = true;
+  struct fg_batch *solo = nullptr;
+};
+

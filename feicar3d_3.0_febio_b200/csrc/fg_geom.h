@@ -1,0 +1,34 @@
+// fg_geom.h -- device state of the immersed-boundary tagging of one case.
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+namespace fg {
+
+struct DevBody {
+  int nvert = 0, ntri = 0, type = 1, body_dim = 3;
+  double membrane_tkns = 0.0;
+  std::vector<double> xyz;     // host copy, 3 per vertex
+  std::vector<int32_t> tri;    // host copy, 3 per triangle (0-based)
+  double *d_xyz = nullptr;     // SoA: x[nvert], y[nvert], z[nvert]
+  double *d_en = nullptr;      // element normals (3*ntri, SoA)
+  double *d_vn = nullptr;      // vertex normals (3*nvert, SoA)
+  int32_t *d_tri = nullptr;    // 3*ntri
+  int32_t *d_v2t_off = nullptr, *d_v2t = nullptr;  // vertex -> triangles
+};
+
+struct Geom {
+  std::vector<DevBody> bodies;
+  int8_t *d_iblank = nullptr, *d_ghost = nullptr, *d_dead = nullptr, *d_body = nullptr;
+  int8_t *d_band = nullptr, *d_tmp = nullptr;
+  double *d_xc = nullptr;      // xc[0..nx+1], yc, zc concatenated
+  int nWarnSide = 0, nHostFail = 0;
+  // lists (host copies after fg_gcm_set_internal_boundary)
+  std::vector<double> g_coefD, g_bi, g_ip, g_probe, g_alpha, d_coefD, d_bi, d_probe;
+  std::vector<int32_t> g_closest, d_closest;
+  bool tagged = false;
+};
+
+}  // namespace fg

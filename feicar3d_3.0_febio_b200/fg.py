@@ -1,0 +1,313 @@
+"""Python binding of the C ABI in include/feicar_b200.h (libfeicar_b200.so).
+
+The class :class:`Case` mirrors the Fortran subroutines of the reference's
+pressure path that a time step calls, with the same names and argument
+meaning (host arrays are Fortran-ordered ``(0:nx+1, 0:ny+1, 0:nz+1)``
+fields, nx/ny/nz node counts):
+
+* ``set_iblank_body_fast``        BOUNDARY_IBLANK_FAST.F90:2
+* ``gcm_set_internal_boundary``   GCM_SET_BOUNDARY.F90:2
+* ``mg_prepare``                  CORE_MG.F90:1365
+* ``solve_poisson``               CORE_POISSON.F90:83
+* ``ghostcell_pressure``          GCM_GHOSTCELL_UPDATE.F90:361
+
+There is no fallback: without the compiled library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfeicar_b200.so")
+
+FG_OK, FG_NOT_CONVERGED = 0, 1
+FG_PBC_DIRICHLET, FG_PBC_NEUMANN = 1, 2
+FG_PREC_FP64, FG_PREC_MIXED = 0, 1
+STATUS = {0: "ok", 1: "not converged", 2: "image point has no host cell", 3: "allocation failed",
+          4: "timeout", 5: "bad input", 6: "dead cell without body", 7: "CUDA error",
+          8: "no CUDA device", 9: "rejected by admission"}
+
+
+class FGError(RuntimeError):
+    def __init__(self, status, what):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+class SolverConfig(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int),
+        ("outer", C.c_int),
+        ("nu1", C.c_int),
+        ("nu2", C.c_int),
+        ("omega", C.c_double),
+        ("rtol", C.c_double),
+        ("max_cycles", C.c_int),
+        ("pbc", C.c_int * 6),
+        ("ppp", C.c_double * 6),
+        ("mgrids", C.c_int * 3),
+        ("probe_length", C.c_double),
+        ("probe_length_dead", C.c_double),
+        ("membrane_tkns_factor", C.c_double),
+        ("gauge_corner", C.c_int),
+    ]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [
+        ("cycles", C.c_int),
+        ("relres", C.c_double),
+        ("ghost_res", C.c_double),
+        ("seconds", C.c_double),
+        ("vcycle_ms", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library; raises when it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is not built; run __graft_entry__.build() or make -C csrc")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+        L.fg_version.restype = C.c_char_p
+        L.fg_status_string.restype = C.c_char_p
+        L.fg_status_string.argtypes = [ip]
+        L.fg_device_count.argtypes = [C.POINTER(C.c_int)]
+        L.fg_default_config.argtypes = [C.POINTER(SolverConfig)]
+        L.fg_case_create.argtypes = [ip, ip, ip, vp, vp, vp, C.POINTER(SolverConfig), ip, C.POINTER(vp)]
+        L.fg_case_destroy.argtypes = [vp]
+        L.fg_case_levels.argtypes = [vp, C.POINTER(C.c_int), vp]
+        L.fg_case_add_body.argtypes = [vp, ip, ip, vp, vp, ip, dp, ip]
+        L.fg_case_update_body.argtypes = [vp, ip, vp]
+        L.fg_set_iblank_body_fast.argtypes = [vp, vp]
+        L.fg_gcm_set_internal_boundary.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.fg_get_ghost_rows.argtypes = [vp] + [vp] * 9
+        L.fg_get_dead_rows.argtypes = [vp] + [vp] * 8
+        L.fg_get_band.argtypes = [vp, vp]
+        L.fg_case_set_geometry.argtypes = [vp, vp, vp, vp, ip, vp, vp, vp, ip, vp, vp, vp, vp, vp]
+        L.fg_mg_prepare.argtypes = [vp]
+        L.fg_solve_poisson.argtypes = [vp, vp, vp, vp, vp, vp, C.POINTER(SolveStats)]
+        L.fg_solve_poisson_device.argtypes = [vp, vp, vp, vp, C.POINTER(SolveStats)]
+        L.fg_ghostcell_pressure.argtypes = [vp, vp, vp, ip]
+        L.fg_batch_create.argtypes = [ip, C.POINTER(SolverConfig), C.POINTER(vp)]
+        L.fg_batch_add.argtypes = [vp, vp]
+        L.fg_batch_solve_device.argtypes = [vp, vp, vp, C.POINTER(SolveStats)]
+        L.fg_batch_destroy.argtypes = [vp]
+        for name in ["fg_device_count", "fg_case_create", "fg_case_destroy", "fg_case_levels",
+                     "fg_case_add_body", "fg_case_update_body", "fg_set_iblank_body_fast",
+                     "fg_gcm_set_internal_boundary", "fg_get_ghost_rows", "fg_get_dead_rows",
+                     "fg_get_band", "fg_case_set_geometry", "fg_mg_prepare", "fg_solve_poisson",
+                     "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
+                     "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy"]:
+            getattr(L, name).restype = ip
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc, what, ok=(FG_OK,)):
+    if rc not in ok:
+        msg = lib().fg_status_string(rc).decode()
+        raise FGError(rc, f"{what} [{msg}]")
+    return rc
+
+
+def default_config(**kw) -> SolverConfig:
+    cfg = SolverConfig()
+    lib().fg_default_config(C.byref(cfg))
+    for k, v in kw.items():
+        if k in ("pbc", "ppp", "mgrids"):
+            arr = getattr(cfg, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().fg_device_count(C.byref(n))
+    return n.value
+
+
+class Case:
+    """One grid + bodies + device-resident GCM state and MG hierarchy."""
+
+    def __init__(self, grid, config: SolverConfig | None = None, device: int = 0):
+        self.grid = grid
+        self.cfg = config or default_config()
+        h = C.c_void_p()
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (grid.xn, grid.yn, grid.zn)]
+        self._keep = xs
+        _check(lib().fg_case_create(grid.nx, grid.ny, grid.nz, _p(xs[0]), _p(xs[1]), _p(xs[2]),
+                                    C.byref(self.cfg), device, C.byref(h)), "fg_case_create")
+        self.h = h
+        self.nGhost = 0
+        self.nDead = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fg_case_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def shape(self):
+        return self.grid.shape
+
+    def levels(self):
+        n = C.c_int()
+        dims = np.zeros(3 * 16, np.int32)
+        _check(lib().fg_case_levels(self.h, C.byref(n), _p(dims)), "fg_case_levels")
+        return [tuple(dims[3 * i:3 * i + 3]) for i in range(n.value)]
+
+    # -------------------------------------------------------- geometry
+    def add_body(self, body):
+        xyz = np.ascontiguousarray(body.verts, dtype=np.float64).ravel()
+        tri = np.ascontiguousarray(body.tri, dtype=np.int32).ravel()
+        _check(lib().fg_case_add_body(self.h, body.nvert, body.ntri, _p(xyz), _p(tri), body.surface,
+                                      body.membrane_tkns, body.body_dim), "fg_case_add_body")
+
+    def update_body(self, ibody, verts):
+        xyz = np.ascontiguousarray(verts, dtype=np.float64).ravel()
+        _check(lib().fg_case_update_body(self.h, ibody, _p(xyz)), "fg_case_update_body")
+
+    def set_iblank_body_fast(self):
+        ib = np.zeros(self.shape, np.int8, order="F")
+        _check(lib().fg_set_iblank_body_fast(self.h, _p(ib)), "fg_set_iblank_body_fast")
+        return ib
+
+    def gcm_set_internal_boundary(self):
+        ib = np.zeros(self.shape, np.int8, order="F")
+        gh = np.zeros(self.shape, np.int8, order="F")
+        dd = np.zeros(self.shape, np.int8, order="F")
+        ng, nd = C.c_int(), C.c_int()
+        rc = lib().fg_gcm_set_internal_boundary(self.h, _p(ib), _p(gh), _p(dd), C.byref(ng), C.byref(nd))
+        _check(rc, "fg_gcm_set_internal_boundary")
+        self.nGhost, self.nDead = ng.value, nd.value
+        return ib, gh, dd
+
+    def band(self):
+        b = np.zeros(self.shape, np.int8, order="F")
+        _check(lib().fg_get_band(self.h, _p(b)), "fg_get_band")
+        return b
+
+    def ghost_rows(self):
+        n = self.nGhost
+        r = dict(ijk=np.zeros((n, 3), np.int32), cell=np.zeros((n, 3), np.int32),
+                 coefN=np.zeros((n, 8)), coefD=np.zeros((n, 8)), bi=np.zeros((n, 3)),
+                 ip=np.zeros((n, 3)), probe=np.zeros(n), closest=np.zeros(n, np.int32),
+                 alpha=np.zeros(n))
+        _check(lib().fg_get_ghost_rows(self.h, *[_p(r[k]) for k in
+                                                 ["ijk", "cell", "coefN", "coefD", "bi", "ip", "probe",
+                                                  "closest", "alpha"]]), "fg_get_ghost_rows")
+        return r
+
+    def dead_rows(self):
+        n = self.nDead
+        r = dict(ijk=np.zeros((n, 3), np.int32), cell=np.zeros((n, 3), np.int32),
+                 coefN=np.zeros((n, 8)), coefD=np.zeros((n, 8)), bi=np.zeros((n, 3)),
+                 ip=np.zeros((n, 3)), probe=np.zeros(n), closest=np.zeros(n, np.int32))
+        _check(lib().fg_get_dead_rows(self.h, *[_p(r[k]) for k in
+                                                ["ijk", "cell", "coefN", "coefD", "bi", "ip", "probe",
+                                                 "closest"]]), "fg_get_dead_rows")
+        return r
+
+    def set_geometry(self, iblank, ghost, dead, ghosts: dict, deads: dict):
+        """Masks and interpolation rows computed elsewhere (e.g. a host that
+        keeps its own GCM setup)."""
+        arrs = [np.asfortranarray(a, dtype=np.int8) for a in (iblank, ghost, dead)]
+        g = {k: np.ascontiguousarray(ghosts[k]) for k in ("ijk", "cell", "coefN")}
+        d = {k: np.ascontiguousarray(deads[k]) for k in ("ijk", "cell", "coefN", "probe", "ip")}
+        g["ijk"] = g["ijk"].astype(np.int32); g["cell"] = g["cell"].astype(np.int32)
+        d["ijk"] = d["ijk"].astype(np.int32); d["cell"] = d["cell"].astype(np.int32)
+        self._geo_keep = (arrs, g, d)
+        _check(lib().fg_case_set_geometry(
+            self.h, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]), len(g["ijk"]), _p(g["ijk"]), _p(g["cell"]),
+            _p(g["coefN"]), len(d["ijk"]), _p(d["ijk"]), _p(d["cell"]), _p(d["coefN"]), _p(d["probe"]),
+            _p(d["ip"])), "fg_case_set_geometry")
+        self.nGhost, self.nDead = len(g["ijk"]), len(d["ijk"])
+
+    def mg_prepare(self):
+        _check(lib().fg_mg_prepare(self.h), "fg_mg_prepare")
+
+    # ----------------------------------------------------------- solve
+    def solve_poisson(self, p, div, p_old=None, dpdn_ghost=None, dpdn_dead=None,
+                      allow_not_converged=False):
+        """p is updated in place (Fortran-ordered float64 field)."""
+        assert p.dtype == np.float64 and p.flags.f_contiguous and p.shape == self.shape
+        div = np.asfortranarray(div, dtype=np.float64)
+        st = SolveStats()
+        rc = lib().fg_solve_poisson(self.h, _p(p), _p(div), _p(p_old), _p(dpdn_ghost), _p(dpdn_dead),
+                                    C.byref(st))
+        ok = (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,)
+        _check(rc, "fg_solve_poisson", ok)
+        return st.as_dict()
+
+    def solve_poisson_device(self, d_p: int, d_div: int, allow_not_converged=False):
+        """Device pointers (ints) of Fortran-layout float64 fields."""
+        st = SolveStats()
+        rc = lib().fg_solve_poisson_device(self.h, C.c_void_p(d_p), C.c_void_p(d_div), None, C.byref(st))
+        ok = (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,)
+        _check(rc, "fg_solve_poisson_device", ok)
+        return st.as_dict()
+
+    def ghostcell_pressure(self, p, p_old=None, iterations=1):
+        _check(lib().fg_ghostcell_pressure(self.h, _p(p), _p(p_old), iterations), "fg_ghostcell_pressure")
+
+
+class Batch:
+    """Many cases solved together: one launch per multigrid stage."""
+
+    def __init__(self, config: SolverConfig | None = None, device: int = 0):
+        self.cfg = config or default_config()
+        h = C.c_void_p()
+        _check(lib().fg_batch_create(device, C.byref(self.cfg), C.byref(h)), "fg_batch_create")
+        self.h = h
+        self.cases = []
+
+    def add(self, case: Case):
+        _check(lib().fg_batch_add(self.h, case.h), "fg_batch_add")
+        self.cases.append(case)
+
+    def solve_device(self, d_ps, d_divs, allow_not_converged=False):
+        n = len(self.cases)
+        P = (C.c_void_p * n)(*[C.c_void_p(x) for x in d_ps])
+        D = (C.c_void_p * n)(*[C.c_void_p(x) for x in d_divs])
+        st = SolveStats()
+        rc = lib().fg_batch_solve_device(self.h, P, D, C.byref(st))
+        ok = (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,)
+        _check(rc, "fg_batch_solve_device", ok)
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

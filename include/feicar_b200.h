@@ -1,0 +1,172 @@
+/*
+ * feicar_b200.h -- C ABI of the B200 (sm_100a) pressure-Poisson path of
+ * FEICAR3D: immersed-boundary tagging, ghost-cell pressure boundary
+ * condition and the multigrid Poisson solve.
+ *
+ * Every entry point takes plain pointers and sizes, returns an fg_status
+ * and never aborts; host arrays are the reference's Fortran module arrays
+ * passed by c_loc (column-major, i fastest, lower bound 0):
+ *     field(0:nx+1, 0:ny+1, 0:nz+1)   nx, ny, nz = NODE counts
+ * which is how one MPI rank with nProcs = 1 lays them out
+ * (CORE_MEMORY_ALLOCATE.F90:23-96, CORE_PARALLEL.F90:170-185).
+ * The library keeps device-resident copies of the grid hierarchy, masks,
+ * ghost/dead lists and solver state per handle across time steps.
+ *
+ * One handle is used from one host thread; every call is ordered on the
+ * handle's CUDA stream.
+ */
+#ifndef FEICAR_B200_H
+#define FEICAR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fg_status {
+  FG_OK = 0,
+  FG_NOT_CONVERGED = 1,          /* CORE_POISSON.F90:195-198 prints      */
+  FG_GEOMETRY_NO_HOST_CELL = 2,  /* GCM_SET_BOUNDARY.F90:476-492         */
+  FG_ALLOC_FAIL = 3,
+  FG_TIMEOUT = 4,
+  FG_BAD_INPUT = 5,
+  FG_GEOMETRY_DEAD_NO_BODY = 6,  /* GCM_SET_BOUNDARY.F90:1061-1066       */
+  FG_CUDA_ERROR = 7,
+  FG_NO_DEVICE = 8,
+  FG_REJECTED = 9                /* serving admission refused            */
+} fg_status;
+
+enum { FG_PBC_DIRICHLET = 1, FG_PBC_NEUMANN = 2 };
+enum { FG_SOLID = 1, FG_MEMBRANE = 2 };
+enum { FG_PREC_FP64 = 0, FG_PREC_MIXED = 1 };
+enum { FG_OUTER_RICHARDSON = 0, FG_OUTER_BICGSTAB = 1 };
+
+/* Solver settings: the input.dat keys of MAIN.F90:214-254 that the pressure
+ * path reads, plus the knobs of the multigrid run on the GPU. */
+typedef struct fg_solver_config {
+  int    precision;          /* FG_PREC_FP64 or FG_PREC_MIXED              */
+  int    outer;              /* FG_OUTER_RICHARDSON / FG_OUTER_BICGSTAB     */
+  int    nu1, nu2;           /* pre/post smoothing steps (x, y, z lines)   */
+  double omega;              /* line relaxation factor (omega_pson)        */
+  double rtol;               /* ||f - A p||_2 / ||f||_2 on fluid rows       */
+  int    max_cycles;         /* outer iterations (itermax_pson)            */
+  int    pbc[6];             /* pbcx1..pbcz2                               */
+  double ppp[6];             /* pppx1..pppz2 (Dirichlet values)            */
+  int    mgrids[3];          /* mgrids_x/y/z, 0 = automatic (CORE_MG:69-102)*/
+  double probe_length;       /* probeLengthNormalized                      */
+  double probe_length_dead;  /* probeLengthNormalizedD                     */
+  double membrane_tkns_factor;
+  int    gauge_corner;       /* 1: subtract p(1,1,1) when all-Neumann      */
+} fg_solver_config;
+
+typedef struct fg_solve_stats {
+  int    cycles;             /* outer iterations used                       */
+  double relres;             /* final relative residual (fluid rows)        */
+  double ghost_res;          /* final max |ghost/dead row residual|         */
+  double seconds;            /* device time of the solve                    */
+  double vcycle_ms;          /* mean device time of one V-cycle             */
+} fg_solve_stats;
+
+typedef struct fg_case fg_case;
+
+/* Library. */
+const char *fg_version(void);
+fg_status fg_device_count(int *count);
+void fg_default_config(fg_solver_config *cfg);
+const char *fg_status_string(fg_status s);
+
+/* Replaces make_grid/metrics (CORE_GRID.F90:29-205) and MG_initial
+ * (CORE_MG.F90:22-599): xn/yn/zn are the node coordinates x(1..nx),
+ * y(1..ny), z(1..nz).  Allocates the device hierarchy on `device`. */
+fg_status fg_case_create(int nx, int ny, int nz, const double *xn,
+                         const double *yn, const double *zn,
+                         const fg_solver_config *cfg, int device,
+                         fg_case **out);
+fg_status fg_case_destroy(fg_case *c);
+/* node counts of level lev (mgrid_I/J/K) and the number of levels */
+fg_status fg_case_levels(const fg_case *c, int *mlevel, int *dims /*3*MAX*/);
+
+/* Body surfaces (BOUNDARY_MARKER_INIT / BOUNDARY_SET_ARCLENGTH_NORM input):
+ * xyz[3*nvert], tri[3*ntri] 0-based, normals (v2-v1)x(v3-v2) into body. */
+fg_status fg_case_add_body(fg_case *c, int nvert, int ntri, const double *xyz,
+                           const int32_t *tri, int surface_type,
+                           double membrane_tkns, int body_dim);
+/* Moves body `ibody` (BOUNDARY_MOVE.F90:151-186 output). */
+fg_status fg_case_update_body(fg_case *c, int ibody, const double *xyz);
+
+/* Replaces set_iblank_body_fast (BOUNDARY_IBLANK_FAST.F90:2-854) on the
+ * device.  iblank (host, int8, the field above) may be NULL. */
+fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank);
+/* Replaces GCM_set_internal_boundary (GCM_SET_BOUNDARY.F90:2-604,
+ * :880-1491): smoothing, ghost and dead lists, image points, weights.
+ * Any output pointer may be NULL. */
+fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank,
+                                       int8_t *ghostCellMark,
+                                       int8_t *dead_cell, int *nGhost,
+                                       int *nDead);
+/* Copies of the ghost / dead lists (1 row each, k-j-i list order):
+ * ijk[3n], cell[3n] (host cell lower corner), coefN[8n], coefD[8n],
+ * bi[3n] body intercept, ip[3n] image point, probe[n], closest[n]. */
+fg_status fg_get_ghost_rows(const fg_case *c, int32_t *ijk, int32_t *cell,
+                            double *coefN, double *coefD, double *bi,
+                            double *ip, double *probe, int32_t *closest,
+                            double *alpha);
+fg_status fg_get_dead_rows(const fg_case *c, int32_t *ijk, int32_t *cell,
+                           double *coefN, double *coefD, double *bi,
+                           double *ip, double *probe, int32_t *closest);
+/* band flag of the last tagging (1 = cell of the triangle-box band) */
+fg_status fg_get_band(const fg_case *c, int8_t *band);
+
+/* Supplies masks and interpolation rows computed by the caller instead of
+ * the two calls above (a host that keeps its own GCM setup). */
+fg_status fg_case_set_geometry(fg_case *c, const int8_t *iblank,
+                               const int8_t *ghostCellMark,
+                               const int8_t *dead_cell, int nGhost,
+                               const int32_t *ghost_ijk,
+                               const int32_t *ghost_cell,
+                               const double *ghost_coefN, int nDead,
+                               const int32_t *dead_ijk,
+                               const int32_t *dead_cell_idx,
+                               const double *dead_coefN,
+                               const double *dead_probe,
+                               const double *dead_ip);
+
+/* Replaces mg_prepare (CORE_MG.F90:1365-1555): coarse masks. */
+fg_status fg_mg_prepare(fg_case *c);
+
+/* Replaces solve_poisson (CORE_POISSON.F90:83-200) with its ghost-cell
+ * update (GCM_GHOSTCELL_UPDATE.F90:361-739) and mg_solve: p (in: initial
+ * guess, out: converged pressure) and div are host fields; p_old is the
+ * previous time step's pressure read by the dead-cell fallback (NULL = 0);
+ * dpdn_ghost[nGhost], dpdn_dead[nDead] may be NULL (homogeneous).
+ * Host<->device copies happen inside the call. */
+fg_status fg_solve_poisson(fg_case *c, double *p, const double *div,
+                           const double *p_old, const double *dpdn_ghost,
+                           const double *dpdn_dead, fg_solve_stats *st);
+/* Same with device pointers on the handle's layout-compatible arrays
+ * (Fortran field layout, double, on the handle's device). */
+fg_status fg_solve_poisson_device(fg_case *c, double *d_p,
+                                  const double *d_div, const double *d_p_old,
+                                  fg_solve_stats *st);
+/* One ghost/dead-cell update pass on a host field (GCM_ghostcell_pressure
+ * with itermax_gc iterations). */
+fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old,
+                                int iterations);
+
+/* ----- batched uneven solves: many cases per launch per MG stage ----- */
+typedef struct fg_batch fg_batch;
+fg_status fg_batch_create(int device, const fg_solver_config *cfg,
+                          fg_batch **out);
+fg_status fg_batch_add(fg_batch *b, fg_case *c);
+/* Solves every case of the batch; p[i] and div[i] are device fields of
+ * case i (as for fg_solve_poisson_device). */
+fg_status fg_batch_solve_device(fg_batch *b, double **d_p,
+                                const double **d_div, fg_solve_stats *st);
+fg_status fg_batch_destroy(fg_batch *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
