@@ -81,6 +81,8 @@ static fg_status alloc_level(fg_case *c, HLevel &L, bool lvl0) {
   L.ntot = L.sz * (L.nz + 2);
   const bool mixed = c->cfg.precision == FG_PREC_MIXED;
   FG_CUDA(cudaMalloc(&L.d_type, L.ntot));
+  FG_CUDA(cudaMalloc(&L.d_mask, L.ntot));
+  FG_CUDA(cudaMemset(L.d_mask, 0, L.ntot));
   if (!mixed || lvl0) {
     FG_CUDA(cudaMalloc(&L.d_x64, L.ntot * sizeof(double)));
     FG_CUDA(cudaMalloc(&L.d_rhs64, L.ntot * sizeof(double)));
@@ -167,6 +169,7 @@ static fg_status upload_axes(fg_case *c, int l) {
   d.nx = L.nx; d.ny = L.ny; d.nz = L.nz;
   d.sy = L.sy; d.sz = L.sz; d.ntot = L.ntot;
   d.type = L.d_type;
+  d.mask = L.d_mask;
   d.amx = L.d_coef + doff[0][0]; d.apx = L.d_coef + doff[0][1];
   d.amy = L.d_coef + doff[1][0]; d.apy = L.d_coef + doff[1][1];
   d.amz = L.d_coef + doff[2][0]; d.apz = L.d_coef + doff[2][1];
@@ -298,6 +301,7 @@ struct fg_batch {
   long long *d_rtgt = nullptr, *d_rcell = nullptr;
   double *d_rw = nullptr, *d_rc0 = nullptr, *d_rd = nullptr, *d_tmp = nullptr;
   float *d_rf = nullptr;
+  double *d_part = nullptr;   // per-block partial sums of level-0 reductions
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
   std::vector<double> h_norm;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -324,7 +328,8 @@ static void free_batch_tables(fg_batch *b) {
   cudaFree(b->d_lev0); cudaFree(b->d_off0);
   cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
   cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
-  cudaFree(b->d_norm);
+  cudaFree(b->d_norm); cudaFree(b->d_part);
+  b->d_part = nullptr;
   b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
   b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
@@ -441,6 +446,7 @@ static fg_status build_batch(fg_batch *b) {
     b->rows.rf = b->d_rf;
   }
   FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
+  FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, b->all0.blocks) * sizeof(double)));
   b->h_norm.assign(3 * np, 0.0);
   b->built = true;
   return FG_OK;
@@ -478,7 +484,7 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
     if (!ls.S.empty()) {
       for (int q = 0; q < b->cfg.nu1; ++q)
         if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
-      FG_K(k::residual<T>(ls.cells, nullptr, s));
+      FG_K(k::residual<T>(ls.cells, nullptr, nullptr, s));
       FG_K(k::restrict_to<T>(ls.next, ls.d_levS, s));
       FG_K(k::zero_x<T>(ls.next, s));
     }
@@ -506,10 +512,10 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
   // ghost / dead values consistent with the initial field
   FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
   FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
-  FG_K(k::fluid_norm(b->all0, b->d_norm + np, s));
+  FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
   if (mixed) {
     FG_K(k::zero_x<float>(b->all0, s));
-    FG_K(k::correct_residual(b->all0, nullptr, b->d_norm, s));
+    FG_K(k::correct_residual(b->all0, b->d_norm, b->d_part, s));
     FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
   }
   int cyc = 0;
@@ -528,9 +534,9 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
     FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
     if (mixed) {
-      FG_K(k::correct_residual(b->all0, nullptr, b->d_norm, s));
+      FG_K(k::correct_residual(b->all0, b->d_norm, b->d_part, s));
     } else {
-      FG_K(k::residual<double>(b->all0, b->d_norm, s));
+      FG_K(k::residual<double>(b->all0, b->d_norm, b->d_part, s));
     }
     FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
     FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double),
@@ -649,6 +655,26 @@ static void coarse_masks(fg_case *c) {
   }
 }
 
+// operator mask of every interior cell (see DevLevel::mask)
+static void build_mask(HLevel &L) {
+  L.mask.assign(L.ntot, 0);
+  const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
+  for (int k = 1; k <= L.nz; ++k)
+    for (int j = 1; j <= L.ny; ++j)
+      for (int i = 1; i <= L.nx; ++i) {
+        const long long id = dev_index(L, i, j, k);
+        const int8_t t = L.type[id];
+        uint8_t m = 0;
+        for (int q = 0; q < 6; ++q) {
+          const int8_t nt = L.type[id + off[q]];
+          if (nt == T_ACTIVE || nt == T_GHOST || nt == T_SOLID) m |= (uint8_t)(1u << q);
+        }
+        if (t == T_ACTIVE) m |= 64;
+        if (t == T_ACTIVE || t == T_GHOST) m |= 128;
+        L.mask[id] = m;
+      }
+}
+
 static fg_status prepare(fg_case *c) {
   if (!c->has_geometry) {
     // no body: all interior cells are fluid
@@ -661,7 +687,9 @@ static fg_status prepare(fg_case *c) {
   coarse_masks(c);
   for (int l = 0; l < c->nlev; ++l) {
     HLevel &L = c->lev[l];
+    build_mask(L);
     FG_CUDA(cudaMemcpy(L.d_type, L.type.data(), L.ntot, cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(L.d_mask, L.mask.data(), L.ntot, cudaMemcpyHostToDevice));
   }
   coarsest_inverse(c);
   cudaFree(c->d_G); cudaFree(c->d_gidx);
@@ -785,7 +813,7 @@ fg_status fg_case_destroy(fg_case *c) {
   if (c->solo) { fg_batch_destroy(c->solo); c->solo = nullptr; }
   for (int l = 0; l < c->nlev; ++l) {
     HLevel &L = c->lev[l];
-    cudaFree(L.d_type); cudaFree(L.d_coef); cudaFree(L.d_int);
+    cudaFree(L.d_type); cudaFree(L.d_mask); cudaFree(L.d_coef); cudaFree(L.d_int);
     cudaFree(L.d_x64); cudaFree(L.d_rhs64); cudaFree(L.d_res64);
     cudaFree(L.d_x32); cudaFree(L.d_rhs32); cudaFree(L.d_res32);
   }

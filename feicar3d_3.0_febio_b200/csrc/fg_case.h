@@ -25,6 +25,8 @@ struct HLevel {
   std::vector<int8_t> type;  // device layout
   // device
   int8_t *d_type = nullptr;
+  uint8_t *d_mask = nullptr;
+  std::vector<uint8_t> mask;
   double *d_coef = nullptr;  // packed 1-D double arrays
   int *d_int = nullptr;      // packed 1-D int arrays
   double *d_x64 = nullptr, *d_rhs64 = nullptr, *d_res64 = nullptr;

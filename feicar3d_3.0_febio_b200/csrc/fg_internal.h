@@ -33,6 +33,10 @@ struct DevLevel {
   long long sy, sz;      // strides in elements
   long long ntot;        // elements of one field
   const int8_t *type;
+  // per-cell operator mask: bit q (0..5) = face q coupled (neighbour
+  // active, ghost or solid; faces -x,+x,-y,+y,-z,+z), bit 6 = active row,
+  // bit 7 = receives the coarse correction (active or ghost)
+  const uint8_t *mask;
   // per-axis operator coefficients indexed by cell 1..n (arrays of n+2):
   // am(i) couples cell i to i-1, ap(i) to i+1 (CORE_MG.F90:674-676)
   const double *amx, *apx, *amy, *apy, *amz, *apz;
@@ -95,8 +99,9 @@ size_t smem_line(int n, int tsize, int lines_per_block);
 template <typename T>
 cudaError_t line_sweep(const Launch &L, int axis, int color, double omega, int maxn,
                        cudaStream_t s);
+// norm2[p] += ||r||^2 of entry p when norm2 != null (part: one double per block)
 template <typename T>
-cudaError_t residual(const Launch &L, double *norm2, cudaStream_t s);
+cudaError_t residual(const Launch &L, double *norm2, double *part, cudaStream_t s);
 template <typename T>
 cudaError_t restrict_to(const Launch &fine_cells_of_coarse, const DevLevel *fine,
                         cudaStream_t s);
@@ -112,9 +117,8 @@ cudaError_t rows_residual(const DevRows &R, const DevLevel *lev0, double *maxabs
 template <typename T>
 cudaError_t coarsest_solve(int nprob, const DevLevel *lev, const double *const *ginv,
                            const int *const *gidx, const int *gn, int maxn, cudaStream_t s);
-cudaError_t correct_residual(const Launch &L0_64, const DevLevel *lev32, double *norm2,
-                             cudaStream_t s);
-cudaError_t fluid_norm(const Launch &L, double *norm2, cudaStream_t s);
+cudaError_t correct_residual(const Launch &L0, double *norm2, double *part, cudaStream_t s);
+cudaError_t fluid_norm(const Launch &L, double *norm2, double *part, cudaStream_t s);
 cudaError_t copy_in(double *dst, const double *src, int nx, int ny, int nz, long long sy,
                     long long sz, cudaStream_t s);
 cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, long long sy,

@@ -17,10 +17,29 @@
 namespace fg {
 namespace k {
 
-constexpr int XL_WARPS = 4;    // x-lines per block
-constexpr int TILE_I = 32;     // i-extent of a y/z tile
-constexpr int YZ_WARPS = 16;   // lines of one colour per y/z tile
-constexpr int CELL_BLOCK = 256;
+constexpr int XL_WARPS = 8;    // x-lines per block
+constexpr int TILE_I = 16;     // i-extent of a y/z tile
+constexpr int YZ_WARPS = 8;    // lines of one colour per y/z tile
+constexpr int CELL_BLOCK = 128;
+
+// Cell kernels tile each level by rows: block lb covers cells
+// i = 1 + 128 t + threadIdx.x of row (j,k), so no thread divides by a
+// runtime extent (only one 32-bit division per block).
+constexpr int CELL_ROWS = 8;  // rows (j,k) per block
+struct CellIdx { int i, j, k; bool ok; };
+// cell of row r (0..CELL_ROWS-1) of block lb
+__device__ __forceinline__ CellIdx cell_of(const DevLevel &L, int lb, int r) {
+  const int tpr = (L.nx + CELL_BLOCK - 1) / CELL_BLOCK;
+  const int rb = lb / tpr;
+  const int t = lb - rb * tpr;
+  const int row = rb * CELL_ROWS + r;
+  CellIdx c;
+  c.j = 1 + row % L.ny;
+  c.k = 1 + row / L.ny;
+  c.i = 1 + t * CELL_BLOCK + (int)threadIdx.x;
+  c.ok = c.i <= L.nx && c.k <= L.nz;
+  return c;
+}
 
 __device__ __forceinline__ int find_entry(const int *off, int n, int b) {
   int lo = 0, hi = n - 1;
@@ -38,12 +57,48 @@ __device__ __forceinline__ int face_w(int8_t nt, int bc) {
   return (nt == T_ACTIVE || nt == T_GHOST || nt == T_SOLID) ? 1 : ((nt == T_BOUND && bc) ? 2 : 0);
 }
 
-// padded position of row r of a line split into P chunks (base, rem): one
-// unused slot after every chunk keeps the per-lane chunk reads of the
-// solver off a single shared-memory bank
-__device__ __forceinline__ int padpos(int r, int base, int rem) {
-  int big = rem * (base + 1);
-  int c = r < big ? r / (base + 1) : rem + (r - big) / base;
+// Reciprocal by Newton-Raphson refinement of the hardware estimate
+// (rcp.approx): each step y <- y + y (1 - x y) doubles the number of correct
+// bits, two steps take the FP64 estimate to full double precision and one
+// the FP32 estimate to full single precision.  Used for the pivots of the
+// line solves (diagonally dominant, no denormals).
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ float rcp_nr(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  const float e = fmaf(-x, y, 1.0f);
+  return fmaf(y, e, y);
+}
+
+// Row -> padded position for a line split into P chunks of base or base+1
+// rows: one unused slot after every chunk keeps the per-lane chunk reads
+// of the solver on distinct shared-memory banks.  The chunk of a row is
+// found with multiply-high by ceil(2^32/d), exact for r, d < 2^16.
+struct PadMap {
+  int big, rem;
+  unsigned m0, m1;  // magic numbers for base and base+1
+};
+__host__ __device__ __forceinline__ unsigned magic_u32(int d) {
+  return (unsigned)((0xffffffffull + (unsigned long long)d) / (unsigned long long)d);
+}
+__device__ __forceinline__ PadMap padmap(int base, int rem) {
+  PadMap pm;
+  pm.big = rem * (base + 1);
+  pm.rem = rem;
+  pm.m0 = magic_u32(base);
+  pm.m1 = magic_u32(base + 1);
+  return pm;
+}
+__device__ __forceinline__ int padpos(int r, const PadMap &pm) {
+  const int c = r < pm.big ? (int)__umulhi((unsigned)r, pm.m1)
+                           : pm.rem + (int)__umulhi((unsigned)(r - pm.big), pm.m0);
   return r + c;
 }
 
@@ -55,39 +110,78 @@ __host__ __device__ __forceinline__ void chunking(int n, int &P, int &base, int 
 }
 
 // ------------------------------------------------------- row staging
-// Coefficients of row (cell id) of a line along AXIS: b = diagonal,
-// d = rhs minus the transverse couplings, flags bit0 active, bit1 coupled to
-// the previous cell of the line, bit2 coupled to the next one.  Non-active
-// cells become identity rows holding their current value.
-template <typename T, int AXIS>
-__device__ __forceinline__ void stage_row(const DevLevel &L, long long id, int i, int j, int k,
-                                          const T *__restrict__ x, const T *__restrict__ rhs,
-                                          T &b, T &d, uint8_t &f) {
-  const int8_t t = L.type[id];
-  if (t != T_ACTIVE) {
-    b = T(1); d = x[id]; f = 0;
-    return;
-  }
-  double diag = 0.0;
-  T acc = rhs[id];
-  uint8_t fl = 1;
-  const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
-  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+// A line along axis A has two faces on its own axis (qm = 2A, qp = 2A+1)
+// and four transverse faces whose coefficients are constant along it.
+struct LineCoef {
+  double tq[4];   // transverse face coefficients
+  long long to[4];  // element offsets of the transverse neighbours
+  int qt[4];      // transverse face ids
+  double tdir;    // 2a over transverse Dirichlet boundary faces of the line
+  int qm, qp;     // own-axis face ids
+  int dirm, dirp; // Dirichlet boundary at the first / last row
+};
+
+__device__ __forceinline__ LineCoef line_coef(const DevLevel &L, int axis, int i, int j, int k) {
+  LineCoef c;
+  const double am[3] = {L.amx[i], L.amy[j], L.amz[k]};
+  const double ap[3] = {L.apx[i], L.apy[j], L.apz[k]};
+  const long long st[3] = {1, L.sy, L.sz};
+  const int idx[3] = {i, j, k};
+  const int nn[3] = {L.nx, L.ny, L.nz};
+  int t = 0;
+  c.tdir = 0.0;
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const int w = face_w(L.type[id + off[q]], L.bc[q]);
-    diag -= a[q] * (double)w;
-    if (q / 2 == AXIS) {
-      if (w == 1) fl |= (q & 1) ? 4 : 2;
-    } else if (w == 1) {
-      acc -= (T)a[q] * x[id + off[q]];
-    }
+  for (int ax = 0; ax < 3; ++ax) {
+    if (ax == axis) continue;
+    c.qt[t] = 2 * ax; c.tq[t] = am[ax]; c.to[t] = -st[ax];
+    if (idx[ax] == 1 && L.bc[2 * ax]) c.tdir += 2.0 * am[ax];
+    ++t;
+    c.qt[t] = 2 * ax + 1; c.tq[t] = ap[ax]; c.to[t] = st[ax];
+    if (idx[ax] == nn[ax] && L.bc[2 * ax + 1]) c.tdir += 2.0 * ap[ax];
+    ++t;
   }
-  if (diag == 0.0) {  // no face left: keep the value (CORE_MG.F90:690-695)
-    b = T(1); d = x[id]; f = 0;
-    return;
-  }
-  b = (T)diag; d = acc; f = fl;
+  c.qm = 2 * axis; c.qp = 2 * axis + 1;
+  c.dirm = L.bc[2 * axis]; c.dirp = L.bc[2 * axis + 1];
+  return c;
+}
+
+// Row coefficients from the staged mask: a couples to the previous row, c
+// to the next, b the diagonal (sum over the kept faces, doubled on
+// Dirichlet boundary faces).  Non-active rows are identities.
+template <typename T>
+__device__ __forceinline__ void row_coef(uint8_t mk, int r, int n, double am, double ap,
+                                         const LineCoef &lc, T &a, T &b, T &c) {
+  if (!(mk & 64)) { a = T(0); c = T(0); b = T(1); return; }
+  double diag = -lc.tdir;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    if ((mk >> lc.qt[q]) & 1) diag -= lc.tq[q];
+  const bool cm = (mk >> lc.qm) & 1, cp = (mk >> lc.qp) & 1;
+  if (cm) diag -= am; else if (r == 0 && lc.dirm) diag -= 2.0 * am;
+  if (cp) diag -= ap; else if (r == n - 1 && lc.dirp) diag -= 2.0 * ap;
+  a = cm ? (T)am : T(0);
+  c = cp ? (T)ap : T(0);
+  b = (T)diag;
+}
+
+// Right-hand side of a row: rhs minus the transverse couplings; rows that
+// are not active (or have no face left, CORE_MG.F90:690-695) hold their
+// value.  All loads are issued unconditionally.
+template <typename T>
+__device__ __forceinline__ void stage(const DevLevel &L, long long id, const LineCoef &lc,
+                                      const T *__restrict__ x, const T *__restrict__ rhs,
+                                      T &d, uint8_t &mk) {
+  mk = L.mask[id];
+  const T r = rhs[id], xo = x[id];
+  const T x0 = x[id + lc.to[0]], x1 = x[id + lc.to[1]], x2 = x[id + lc.to[2]], x3 = x[id + lc.to[3]];
+  T acc = r;
+  if ((mk >> lc.qt[0]) & 1) acc -= (T)lc.tq[0] * x0;
+  if ((mk >> lc.qt[1]) & 1) acc -= (T)lc.tq[1] * x1;
+  if ((mk >> lc.qt[2]) & 1) acc -= (T)lc.tq[2] * x2;
+  if ((mk >> lc.qt[3]) & 1) acc -= (T)lc.tq[3] * x3;
+  const bool isolated = ((mk & 63) == 0) && lc.tdir == 0.0 && !lc.dirm && !lc.dirp;
+  if (!(mk & 64) || isolated) { d = xo; mk = (uint8_t)(mk & ~64); }
+  else d = acc;
 }
 
 // ------------------------------------------------------ warp line solve
@@ -133,10 +227,15 @@ __device__ __forceinline__ Eq<T> shfl_eq_down(const Eq<T> &e, int t, int lane) {
 // reduction across lanes, and each lane back-substitutes its chunk.  The
 // solution overwrites d.
 template <typename T, int MAXM>
-__device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am, const double *__restrict__ ap,
-                           const T *sb, T *sd, const uint8_t *sf, int lane) {
+__device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am,
+                                           const double *__restrict__ ap, const LineCoef &lc,
+                                           T *sd, const uint8_t *sf, int lane) {
   if (n == 1) {
-    if (lane == 0) sd[0] = sd[0] / sb[0];
+    if (lane == 0) {
+      T a, b, c;
+      row_coef<T>(sf[0], 0, 1, am[1], ap[1], lc, a, b, c);
+      sd[0] = sd[0] / b;
+    }
     __syncwarp();
     return;
   }
@@ -147,34 +246,42 @@ __device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am,
   const int s = lane * base + (lane < rem ? lane : rem);
   const int ps = s + lane;
   T al[MAXM], ga[MAXM], de[MAXM];
-  Eq<T> F{T(0), T(1), T(0), T(0)}, L{T(0), T(1), T(0), T(0)};
-  T a0 = T(0), b0 = T(1), c0 = T(0), d0 = T(0);
+  // chunk-end equations: F (first row)   aF L_{l-1} + bF F_l + cF L_l = dF
+  //                      L (last row)    aL F_l + L_l + cL F_{l+1} = dL
+  T aF = T(0), bF = T(1), cF = T(0), dF = T(0), aL = T(0), cL = T(0), dL = T(0);
   if (own) {
-    {
-      const uint8_t f0 = sf[ps];
-      a0 = (f0 & 2) ? (T)am[s + 1] : T(0);
-      c0 = (f0 & 4) ? (T)ap[s + 1] : T(0);
-      b0 = sb[ps];
-      d0 = sd[ps];
+    T a0, b0, c0;
+    row_coef<T>(sf[ps], s, n, am[s + 1], ap[s + 1], lc, a0, b0, c0);
+    const T d0 = sd[ps];
+    // operands of every row of the chunk are loaded up front (clamped to the
+    // chunk so the loads are unconditional and leave the elimination chain)
+    uint8_t fq_[MAXM];
+    double amq_[MAXM], apq_[MAXM];
+    T dq_[MAXM];
+#pragma unroll
+    for (int q = 1; q < MAXM; ++q) {
+      const int qq = q < m ? q : m - 1;
+      fq_[q] = sf[ps + qq];
+      amq_[q] = am[s + qq + 1];
+      apq_[q] = ap[s + qq + 1];
+      dq_[q] = sd[ps + qq];
     }
 #pragma unroll
     for (int q = 1; q < MAXM; ++q) {
       if (q < m) {
-        const uint8_t fq = sf[ps + q];
-        const T aq = (fq & 2) ? (T)am[s + q + 1] : T(0);
-        const T cq = (fq & 4) ? (T)ap[s + q + 1] : T(0);
-        const T bq = sb[ps + q], dq = sd[ps + q];
+        T aq, bq, cq;
+        row_coef<T>(fq_[q], s + q, n, amq_[q], apq_[q], lc, aq, bq, cq);
+        const T dq = dq_[q];
         if (q == 1) {
-          const T r = T(1) / bq;
+          const T r = rcp_nr(bq);
           al[1] = aq * r; ga[1] = cq * r; de[1] = dq * r;
         } else {
-          const T r = T(1) / (bq - aq * ga[q - 1]);
+          const T r = rcp_nr(bq - aq * ga[q - 1]);
           al[q] = -aq * al[q - 1] * r;
           ga[q] = cq * r;
           de[q] = (dq - aq * de[q - 1]) * r;
         }
-        // the last row of the chunk (q = m-1) gives the L equation
-        L.a = al[q]; L.b = T(1); L.c = ga[q]; L.d = de[q];
+        aL = al[q]; cL = ga[q]; dL = de[q];  // last row of the chunk
       }
     }
     T pa = T(0), pb = T(-1), pd = T(0);
@@ -188,26 +295,39 @@ __device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am,
         pa = na; pb = nb; pd = nd;
       }
     }
-    F.a = a0; F.b = b0 - c0 * pa; F.c = -c0 * pb; F.d = d0 - c0 * pd;
+    aF = a0; bF = b0 - c0 * pa; cF = -c0 * pb; dF = d0 - c0 * pd;
   }
-  // parallel cyclic reduction over the 2*32 chunk-end equations
-  {
-    const Eq<T> Lm = shfl_eq_up(L, 1, lane);
-    const Eq<T> Fp = shfl_eq_down(F, 1, lane);
-    const Eq<T> nF = pcr_combine(F, Lm, L);
-    const Eq<T> nL = pcr_combine(L, F, Fp);
-    F = nF; L = nL;
-  }
+  // eliminate the L unknowns: L_l = dL - aL F_l - cL F_{l+1}, so each lane
+  // holds one equation of a tridiagonal system in F_0 .. F_31
+  T aLp = __shfl_up_sync(0xffffffffu, aL, 1);
+  T cLp = __shfl_up_sync(0xffffffffu, cL, 1);
+  T dLp = __shfl_up_sync(0xffffffffu, dL, 1);
+  if (lane == 0) { aLp = T(0); cLp = T(0); dLp = T(0); }
+  T A = -aF * aLp;
+  T B = bF - aF * cLp - cF * aL;
+  T Cc = -cF * cL;
+  T D = dF - aF * dLp - cF * dL;
+  if (!own) { A = T(0); B = T(1); Cc = T(0); D = T(0); }
+  // parallel cyclic reduction over 32 equations, one reciprocal per step
 #pragma unroll
   for (int t = 1; t < 32; t <<= 1) {
-    const Eq<T> Fm = shfl_eq_up(F, t, lane), Fp = shfl_eq_down(F, t, lane);
-    const Eq<T> Lm = shfl_eq_up(L, t, lane), Lp = shfl_eq_down(L, t, lane);
-    const Eq<T> nF = pcr_combine(F, Fm, Fp);
-    const Eq<T> nL = pcr_combine(L, Lm, Lp);
-    F = nF; L = nL;
+    const T ib = rcp_nr(B);
+    T la = __shfl_up_sync(0xffffffffu, A, t), lc2 = __shfl_up_sync(0xffffffffu, Cc, t);
+    T ld = __shfl_up_sync(0xffffffffu, D, t), lib = __shfl_up_sync(0xffffffffu, ib, t);
+    T ra = __shfl_down_sync(0xffffffffu, A, t), rc = __shfl_down_sync(0xffffffffu, Cc, t);
+    T rd = __shfl_down_sync(0xffffffffu, D, t), rib = __shfl_down_sync(0xffffffffu, ib, t);
+    if (lane < t) { la = T(0); lc2 = T(0); ld = T(0); lib = T(0); }
+    if (lane + t >= 32) { ra = T(0); rc = T(0); rd = T(0); rib = T(0); }
+    const T k1 = A * lib, k2 = Cc * rib;
+    const T nA = -la * k1, nC = -rc * k2;
+    const T nB = B - lc2 * k1 - ra * k2;
+    const T nD = D - ld * k1 - rd * k2;
+    A = nA; Cc = nC; B = nB; D = nD;
   }
+  const T xF = D / B;
+  const T xFn = __shfl_down_sync(0xffffffffu, xF, 1);
   if (own) {
-    const T xF = F.d / F.b, xL = L.d / L.b;
+    const T xL = dL - aL * xF - cL * (lane + 1 < 32 ? xFn : T(0));
 #pragma unroll
     for (int q = 1; q < MAXM; ++q)
       if (q <= m - 2) sd[ps + q] = de[q] - al[q] * xF - ga[q] * xL;
@@ -235,7 +355,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) &
 // ------------------------------------------------------- x-line kernel
 // Lines (j,k) with (j+k)%2 == color; one warp per line.
 template <typename T, int MAXM>
-__global__ void __launch_bounds__(XL_WARPS * 32)
+__global__ void __launch_bounds__(XL_WARPS * 32, 2)
 k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = find_entry(off, nent, blockIdx.x);
@@ -248,10 +368,9 @@ k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   const int jj = q % nyh;
   const int n = L.nx;
   const int np = line_pad(n);
-  const size_t per = align16(np * sizeof(T)) * 2 + align16(np);
-  T *sb = reinterpret_cast<T *>(smem + per * warp);
-  T *sd = reinterpret_cast<T *>(smem + per * warp + align16(np * sizeof(T)));
-  uint8_t *sf = smem + per * warp + 2 * align16(np * sizeof(T));
+  const size_t per = align16(np * sizeof(T)) + align16(np);
+  T *sd = reinterpret_cast<T *>(smem + per * warp);
+  uint8_t *sf = smem + per * warp + align16(np * sizeof(T));
   if (k > L.nz) return;
   const int j0 = (((1 + k) & 1) == color) ? 1 : 2;
   const int j = j0 + 2 * jj;
@@ -260,29 +379,40 @@ k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   const T *rhs = PrecOf<T>::rhs(L);
   int P, base, rem;
   chunking(n, P, base, rem);
-  const long long row = L.sy * j + L.sz * k;
-  for (int r = lane; r < n; r += 32) {
-    T b, d; uint8_t f;
-    stage_row<T, 0>(L, row + r + 1, r + 1, j, k, x, rhs, b, d, f);
-    const int pp = padpos(r, base, rem);
-    sb[pp] = b; sd[pp] = d; sf[pp] = f;
+  const PadMap pm = padmap(base, rem);
+  const LineCoef lc = line_coef(L, 0, 1, j, k);
+  const long long row = L.sy * j + L.sz * k + 1;
+  for (int r0 = lane; r0 < n; r0 += 128) {
+    T d[4]; uint8_t f[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + 32 * u;
+      if (r < n) stage<T>(L, row + r, lc, x, rhs, d[u], f[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = r0 + 32 * u;
+      if (r < n) { const int pp = padpos(r, pm); sd[pp] = d[u]; sf[pp] = f[u]; }
+    }
   }
   __syncwarp();
-  warp_solve<T, MAXM>(n, L.amx, L.apx, sb, sd, sf, lane);
+  warp_solve<T, MAXM>(n, L.amx, L.apx, lc, sd, sf, lane);
   for (int r = lane; r < n; r += 32) {
-    const int pp = padpos(r, base, rem);
-    if (sf[pp] & 1) {
-      const long long id = row + r + 1;
+    const int pp = padpos(r, pm);
+    if (sf[pp] & 64) {
+      const long long id = row + r;
       x[id] = (omega == T(1)) ? sd[pp] : x[id] + omega * (sd[pp] - x[id]);
     }
   }
 }
 
 // ----------------------------------------------------- y/z-line kernel
-// AXIS 1: lines (i,k) along j, colour (i+k)%2, tiles of 32 i at fixed k.
-// AXIS 2: lines (i,j) along k, colour (i+j)%2, tiles of 32 i at fixed j.
+// AXIS 1: lines (i,k) along j, colour (i+k)%2, tiles of 16 i at fixed k.
+// AXIS 2: lines (i,j) along k, colour (i+j)%2, tiles of 16 i at fixed j.
+// The 8 lines of the colour in a tile are staged together (cell e of the
+// tile: line slot e%8, row e/8), then one warp solves each line.
 template <typename T, int MAXM, int AXIS>
-__global__ void __launch_bounds__(YZ_WARPS * 32)
+__global__ void __launch_bounds__(YZ_WARPS * 32, 2)
 k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = find_entry(off, nent, blockIdx.x);
@@ -297,29 +427,40 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   const long long os = AXIS == 1 ? L.sz : L.sy;
   const int np = line_pad(n);
   const int lstride = np + 1;  // per-line stride (elements), odd in words
-  T *sb = reinterpret_cast<T *>(smem);
-  T *sd = reinterpret_cast<T *>(smem + align16((size_t)YZ_WARPS * lstride * sizeof(T)));
-  uint8_t *sf = smem + 2 * align16((size_t)YZ_WARPS * lstride * sizeof(T));
+  T *sd = reinterpret_cast<T *>(smem);
+  uint8_t *sf = smem + align16((size_t)YZ_WARPS * lstride * sizeof(T));
   const int il0 = (color + i0 + o) & 1;  // tile-local i of the first line of this colour
   T *x = PrecOf<T>::x(L);
   const T *rhs = PrecOf<T>::rhs(L);
   int P, base, rem;
   chunking(n, P, base, rem);
+  const PadMap pm = padmap(base, rem);
   const int tid = threadIdx.x;
-  const int total = TILE_I * n;
-  for (int e = tid; e < total; e += YZ_WARPS * 32) {
-    const int il = e & (TILE_I - 1), r = e / TILE_I;
-    if ((il & 1) != il0) continue;
-    const int i = i0 + il;
-    if (i > L.nx) continue;
-    const int slot = il >> 1;
-    const int jj = AXIS == 1 ? r + 1 : o;
-    const int kk = AXIS == 1 ? o : r + 1;
-    const long long id = i + L.sy * jj + L.sz * kk;
-    T b, d; uint8_t f;
-    stage_row<T, AXIS>(L, id, i, jj, kk, x, rhs, b, d, f);
-    const int pp = slot * lstride + padpos(r, base, rem);
-    sb[pp] = b; sd[pp] = d; sf[pp] = f;
+  const int total = YZ_WARPS * n;
+  constexpr int NT = YZ_WARPS * 32;
+  {
+    // each thread stages one line (slot fixed per thread) for rows r0, r0+2, ...
+    const int slot = tid % YZ_WARPS;
+    const int i = i0 + il0 + 2 * slot;
+    const bool valid = i <= L.nx;
+    const LineCoef lc = line_coef(L, AXIS, i, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
+    const long long base_id = i + os * o;
+    for (int e0 = tid; e0 < total; e0 += 4 * NT) {
+      T d[4]; uint8_t f[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * NT;
+        if (valid && e < total) stage<T>(L, base_id + ls * (e / YZ_WARPS + 1), lc, x, rhs, d[u], f[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int e = e0 + u * NT;
+        if (valid && e < total) {
+          const int pp = slot * lstride + padpos(e / YZ_WARPS, pm);
+          sd[pp] = d[u]; sf[pp] = f[u];
+        }
+      }
+    }
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
@@ -328,27 +469,30 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
     if (i <= L.nx) {
       const double *am = AXIS == 1 ? L.amy : L.amz;
       const double *ap = AXIS == 1 ? L.apy : L.apz;
-      warp_solve<T, MAXM>(n, am, ap, sb + warp * lstride, sd + warp * lstride,
-                          sf + warp * lstride, lane);
+      const LineCoef lc = line_coef(L, AXIS, i, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
+      warp_solve<T, MAXM>(n, am, ap, lc, sd + warp * lstride, sf + warp * lstride, lane);
     }
   }
   __syncthreads();
-  for (int e = tid; e < total; e += YZ_WARPS * 32) {
-    const int il = e & (TILE_I - 1), r = e / TILE_I;
-    if ((il & 1) != il0) continue;
-    const int i = i0 + il;
-    if (i > L.nx) continue;
-    const int pp = (il >> 1) * lstride + padpos(r, base, rem);
-    if (sf[pp] & 1) {
-      const long long id = i + ls * (r + 1) + os * o;
-      x[id] = (omega == T(1)) ? sd[pp] : x[id] + omega * (sd[pp] - x[id]);
+  {
+    const int slot = tid % YZ_WARPS;
+    const int i = i0 + il0 + 2 * slot;
+    if (i <= L.nx) {
+      const long long base_id = i + os * o;
+      for (int e = tid; e < total; e += NT) {
+        const int r = e / YZ_WARPS;
+        const int pp = slot * lstride + padpos(r, pm);
+        if (sf[pp] & 64) {
+          const long long id = base_id + ls * (r + 1);
+          x[id] = (omega == T(1)) ? sd[pp] : x[id] + omega * (sd[pp] - x[id]);
+        }
+      }
     }
   }
 }
 
 int blocks_cells(const DevLevel &L) {
-  long long c = (long long)L.nx * L.ny * L.nz;
-  return (int)((c + CELL_BLOCK - 1) / CELL_BLOCK);
+  return ((L.nx + CELL_BLOCK - 1) / CELL_BLOCK) * ((L.ny * L.nz + CELL_ROWS - 1) / CELL_ROWS);
 }
 int blocks_xline(const DevLevel &L) {
   long long lines = (long long)((L.ny + 1) / 2) * L.nz;
@@ -361,11 +505,11 @@ int blocks_tile(const DevLevel &L, int axis) {
 size_t smem_line(int n, int tsize, int lines) {
   const int np = line_pad(n);
   if (lines == XL_WARPS) {
-    const size_t per = align16((size_t)np * tsize) * 2 + align16(np);
+    const size_t per = align16((size_t)np * tsize) + align16(np);
     return per * XL_WARPS;
   }
   const int lstride = np + 1;
-  return 2 * align16((size_t)YZ_WARPS * lstride * tsize) + align16((size_t)YZ_WARPS * lstride);
+  return align16((size_t)YZ_WARPS * lstride * tsize) + align16((size_t)YZ_WARPS * lstride);
 }
 
 template <typename T, int MAXM>
@@ -408,7 +552,6 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
 }
 
 // ---------------------------------------------------------- residual
-template <typename T>
 __device__ __forceinline__ double block_sum(double v) {
   __shared__ double red[CELL_BLOCK / 32];
 #pragma unroll
@@ -425,126 +568,157 @@ __device__ __forceinline__ double block_sum(double v) {
   return t;
 }
 
+// (A x) at an active cell from its mask: sum over the kept faces of
+// a (x_n - x_c), Dirichlet boundary faces contributing -2 a x_c
 template <typename T>
 __device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, int j, int k,
-                                       const T *__restrict__ x) {
-  double diag = 0.0;
-  T acc = T(0);
-  const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
+                                       uint8_t mk, const T *__restrict__ x) {
+  const T xc = x[id];
+  const T x0 = x[id - 1], x1 = x[id + 1], x2 = x[id - L.sy], x3 = x[id + L.sy];
+  const T x4 = x[id - L.sz], x5 = x[id + L.sz];
   const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+  const T xn[6] = {x0, x1, x2, x3, x4, x5};
+  const bool atb[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
+  T acc = T(0);
+  double diag = 0.0;
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
-    const int w = face_w(L.type[id + off[q]], L.bc[q]);
-    diag -= a[q] * (double)w;
-    if (w == 1) acc += (T)a[q] * x[id + off[q]];
+    if ((mk >> q) & 1) { acc += (T)a[q] * xn[q]; diag -= a[q]; }
+    else if (atb[q] && L.bc[q]) diag -= 2.0 * a[q];
   }
-  return acc + (T)diag * x[id];
+  return acc + (T)diag * xc;
+}
+
+// per-entry sum of the block partials of a launch (1024 threads, eight
+// independent loads in flight per thread)
+__global__ void __launch_bounds__(1024) k_reduce_parts(const int *off, const double *part, double *out) {
+  const int p = blockIdx.x;
+  const int b0 = off[p], b1 = off[p + 1];
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = b0 + threadIdx.x; b < b1; b += 8 * 1024) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int q = b + u * 1024;
+      if (q < b1) v[u] += part[q];
+    }
+  }
+  double t = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double w = red[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) w += __shfl_down_sync(0xffffffffu, w, o);
+    if (threadIdx.x == 0) out[p] += w;
+  }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_residual(const int *off, int nent, const DevLevel *levs, double *norm2) {
+k_residual(const int *off, int nent, const DevLevel *levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)L.nx * L.ny * L.nz;
+  const int lb = blockIdx.x - off[p];
+  const T *x = PrecOf<T>::x(L);
+  const T *rhs = PrecOf<T>::rhs(L);
+  T *res = PrecOf<T>::res(L);
   double r2 = 0.0;
-  if (e < nc) {
-    const int i = 1 + (int)(e % L.nx);
-    const int j = 1 + (int)((e / L.nx) % L.ny);
-    const int k = 1 + (int)(e / ((long long)L.nx * L.ny));
-    const long long id = i + L.sy * j + L.sz * k;
+#pragma unroll 2
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    const uint8_t mk = L.mask[id];
     T r = T(0);
-    if (L.type[id] == T_ACTIVE) {
-      const T *x = PrecOf<T>::x(L);
-      r = PrecOf<T>::rhs(L)[id] - apply_row<T>(L, id, i, j, k, x);
-    }
-    PrecOf<T>::res(L)[id] = r;
-    r2 = (double)r * (double)r;
+    if (mk & 64) r = rhs[id] - apply_row<T>(L, id, c.i, c.j, c.k, mk, x);
+    res[id] = r;
+    r2 += (double)r * (double)r;
   }
-  if (norm2) {
-    const double t = block_sum<T>(r2);
-    if (threadIdx.x == 0) atomicAdd(norm2 + p, t);
+  if (part) {
+    const double t = block_sum(r2);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
   }
 }
 
 template <typename T>
-cudaError_t residual(const Launch &Lr, double *norm2, cudaStream_t s) {
+cudaError_t residual(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
-  k_residual<T><<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, norm2);
+  k_residual<T><<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, norm2 ? part : nullptr);
+  if (norm2) k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
   return cudaGetLastError();
 }
 
 // ||f||^2 over active cells of level 0 (FP64 rhs)
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_fluid_norm(const int *off, int nent, const DevLevel *levs, double *norm2) {
+k_fluid_norm(const int *off, int nent, const DevLevel *levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)L.nx * L.ny * L.nz;
+  const int lb = blockIdx.x - off[p];
   double r2 = 0.0;
-  if (e < nc) {
-    const int i = 1 + (int)(e % L.nx);
-    const int j = 1 + (int)((e / L.nx) % L.ny);
-    const int k = 1 + (int)(e / ((long long)L.nx * L.ny));
-    const long long id = i + L.sy * j + L.sz * k;
-    if (L.type[id] == T_ACTIVE) r2 = L.rhs64[id] * L.rhs64[id];
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    if (L.mask[id] & 64) r2 += L.rhs64[id] * L.rhs64[id];
   }
-  const double t = block_sum<double>(r2);
-  if (threadIdx.x == 0) atomicAdd(norm2 + p, t);
+  const double t = block_sum(r2);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-cudaError_t fluid_norm(const Launch &Lr, double *norm2, cudaStream_t s) {
+cudaError_t fluid_norm(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
-  k_fluid_norm<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, norm2);
+  k_fluid_norm<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, part);
+  k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
   return cudaGetLastError();
 }
 
 // Mixed precision outer step, part 1: p += e (FP64 += FP32) and e = 0.
-// Part 2 is k_residual<double>-like but writes the FP32 residual.
 __global__ void __launch_bounds__(CELL_BLOCK)
 k_correct(const int *off, int nent, const DevLevel *levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)L.nx * L.ny * L.nz;
-  if (e >= nc) return;
-  const int i = 1 + (int)(e % L.nx);
-  const int j = 1 + (int)((e / L.nx) % L.ny);
-  const int k = 1 + (int)(e / ((long long)L.nx * L.ny));
-  const long long id = i + L.sy * j + L.sz * k;
-  const float ev = L.x32[id];
-  L.x64[id] = L.x64[id] + (double)ev;
-  L.x32[id] = 0.0f;
+  const int lb = blockIdx.x - off[p];
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    const float ev = L.x32[id];
+    L.x64[id] = L.x64[id] + (double)ev;
+    L.x32[id] = 0.0f;
+  }
 }
 
+// part 2: FP64 residual of the corrected field, stored as the FP32 rhs of
+// the next correction V-cycle
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_residual_mixed(const int *off, int nent, const DevLevel *levs, double *norm2) {
+k_residual_mixed(const int *off, int nent, const DevLevel *levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)L.nx * L.ny * L.nz;
+  const int lb = blockIdx.x - off[p];
   double r2 = 0.0;
-  if (e < nc) {
-    const int i = 1 + (int)(e % L.nx);
-    const int j = 1 + (int)((e / L.nx) % L.ny);
-    const int k = 1 + (int)(e / ((long long)L.nx * L.ny));
-    const long long id = i + L.sy * j + L.sz * k;
+#pragma unroll 2
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
     double r = 0.0;
-    if (L.type[id] == T_ACTIVE) r = L.rhs64[id] - apply_row<double>(L, id, i, j, k, L.x64);
+    const uint8_t mk = L.mask[id];
+    if (mk & 64) r = L.rhs64[id] - apply_row<double>(L, id, c.i, c.j, c.k, mk, L.x64);
     L.rhs32[id] = (float)r;
-    r2 = r * r;
+    r2 += r * r;
   }
-  const double t = block_sum<double>(r2);
-  if (threadIdx.x == 0) atomicAdd(norm2 + p, t);
+  const double t = block_sum(r2);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-cudaError_t correct_residual(const Launch &Lr, const DevLevel *unused, double *norm2,
-                             cudaStream_t s) {
-  (void)unused;
+cudaError_t correct_residual(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
   k_correct<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev);
-  k_residual_mixed<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, norm2);
+  k_residual_mixed<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, part);
+  k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
   return cudaGetLastError();
 }
 
@@ -557,28 +731,28 @@ k_restrict(const int *off, int nent, const DevLevel *coarse, const DevLevel *fin
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &C = coarse[p];
   const DevLevel &F = fine[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)C.nx * C.ny * C.nz;
-  if (e >= nc) return;
-  const int I = 1 + (int)(e % C.nx);
-  const int J = 1 + (int)((e / C.nx) % C.ny);
-  const int K = 1 + (int)(e / ((long long)C.nx * C.ny));
-  const long long id = I + C.sy * J + C.sz * K;
+  const int lb = blockIdx.x - off[p];
   T *rc = PrecOf<T>::rhs(C);
-  if (C.type[id] != T_ACTIVE) { rc[id] = T(0); return; }
   const T *rf = PrecOf<T>::res(F);
-  double s = 0.0, v = 0.0;
-  for (int k = C.clz[K]; k <= C.chz[K]; ++k)
-    for (int j = C.cly[J]; j <= C.chy[J]; ++j) {
-      const double wyz = F.wy[j] * F.wz[k];
-      const long long rb = F.sy * j + F.sz * k;
-      for (int i = C.clx[I]; i <= C.chx[I]; ++i) {
-        const double w = F.wx[i] * wyz;
-        s += w * (double)rf[rb + i];
-        v += w;
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(C, lb, rr);
+    if (!c.ok) continue;
+    const int I = c.i, J = c.j, K = c.k;
+    const long long id = I + C.sy * J + C.sz * K;
+    if (!(C.mask[id] & 64)) { rc[id] = T(0); continue; }
+    double s = 0.0, v = 0.0;
+    for (int k = C.clz[K]; k <= C.chz[K]; ++k)
+      for (int j = C.cly[J]; j <= C.chy[J]; ++j) {
+        const double wyz = F.wy[j] * F.wz[k];
+        const long long rb = F.sy * j + F.sz * k;
+        for (int i = C.clx[I]; i <= C.chx[I]; ++i) {
+          const double w = F.wx[i] * wyz;
+          s += w * (double)rf[rb + i];
+          v += w;
+        }
       }
-    }
-  rc[id] = (T)(s / v);
+    rc[id] = (T)(s / v);
+  }
 }
 
 template <typename T>
@@ -597,34 +771,30 @@ k_prolong(const int *off, int nent, const DevLevel *fine, const DevLevel *coarse
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &F = fine[p];
   const DevLevel &C = coarse[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)F.nx * F.ny * F.nz;
-  if (e >= nc) return;
-  const int i = 1 + (int)(e % F.nx);
-  const int j = 1 + (int)((e / F.nx) % F.ny);
-  const int k = 1 + (int)(e / ((long long)F.nx * F.ny));
-  const long long id = i + F.sy * j + F.sz * k;
-  const int8_t t = F.type[id];
-  if (t != T_ACTIVE && t != T_GHOST) return;
-  const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
-  const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
-  const double wx1 = F.pwx[i], wy1 = F.pwy[j], wz1 = F.pwz[k];
+  const int lb = blockIdx.x - off[p];
   const T *xc = PrecOf<T>::x(C);
-  double s = 0.0, ws = 0.0;
+  T *x = PrecOf<T>::x(F);
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(F, lb, rr);
+    if (!c.ok) continue;
+    const int i = c.i, j = c.j, k = c.k;
+    const long long id = i + F.sy * j + F.sz * k;
+    if (!(F.mask[id] & 128)) continue;
+    const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
+    const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
+    const double wx1 = F.pwx[i], wy1 = F.pwy[j], wz1 = F.pwz[k];
+    double s = 0.0, ws = 0.0;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
-    const int ci = (c & 1) ? i1 : i0, cj = (c & 2) ? j1 : j0, ck = (c & 4) ? k1 : k0;
-    const double w = ((c & 1) ? wx1 : 1.0 - wx1) * ((c & 2) ? wy1 : 1.0 - wy1) *
-                     ((c & 4) ? wz1 : 1.0 - wz1);
-    const long long cid = ci + C.sy * cj + C.sz * ck;
-    if (w > 0.0 && C.type[cid] == T_ACTIVE) {
-      s += w * (double)xc[cid];
-      ws += w;
+    for (int q = 0; q < 8; ++q) {
+      const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
+      const double w = ((q & 1) ? wx1 : 1.0 - wx1) * ((q & 2) ? wy1 : 1.0 - wy1) *
+                       ((q & 4) ? wz1 : 1.0 - wz1);
+      const long long cid = ci + C.sy * cj + C.sz * ck;
+      const double act = (C.mask[cid] & 64) ? w : 0.0;
+      s += act * (double)xc[cid];
+      ws += act;
     }
-  }
-  if (ws > 1e-12) {
-    T *x = PrecOf<T>::x(F);
-    x[id] = x[id] + (T)(s / ws);
+    if (ws > 1e-12) x[id] = x[id] + (T)(s / ws);
   }
 }
 
@@ -640,13 +810,12 @@ __global__ void __launch_bounds__(CELL_BLOCK)
 k_zero(const int *off, int nent, const DevLevel *levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
-  const long long e = (long long)(blockIdx.x - off[p]) * CELL_BLOCK + threadIdx.x;
-  const long long nc = (long long)L.nx * L.ny * L.nz;
-  if (e >= nc) return;
-  const int i = 1 + (int)(e % L.nx);
-  const int j = 1 + (int)((e / L.nx) % L.ny);
-  const int k = 1 + (int)(e / ((long long)L.nx * L.ny));
-  PrecOf<T>::x(L)[i + L.sy * j + L.sz * k] = T(0);
+  const int lb = blockIdx.x - off[p];
+  T *x = PrecOf<T>::x(L);
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (c.ok) x[c.i + L.sy * c.j + L.sz * c.k] = T(0);
+  }
 }
 
 template <typename T>
@@ -704,21 +873,37 @@ cudaError_t rows_relax(const DevRows &R, const DevLevel *lev0, int corr, double 
 __global__ void __launch_bounds__(CELL_BLOCK)
 k_rows_residual(DevRows R, const DevLevel *lev0, double *maxabs) {
   const int r = blockIdx.x * CELL_BLOCK + threadIdx.x;
-  if (r >= R.n) return;
-  const int p = R.prob[r];
-  const DevLevel &L = lev0[p];
-  const double *x = L.x64;
-  const long long b = R.cell[r], sy = L.sy, sz = L.sz;
-  const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
-  double acc = 0.0;
+  const bool valid = r < R.n;
+  const int p = valid ? R.prob[r] : -1;
+  unsigned long long v = 0ull;
+  if (valid) {
+    const DevLevel &L = lev0[p];
+    const double *x = L.x64;
+    const long long b = R.cell[r], sy = L.sy, sz = L.sz;
+    const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
+    double acc = 0.0;
 #pragma unroll
-  for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * x[b + o[q]];
-  const double rt = acc + R.c0[r] - x[R.tgt[r]];
-  R.rd[r] = rt;
-  R.rf[r] = (float)rt;
-  if (maxabs)
-    atomicMax(reinterpret_cast<unsigned long long *>(maxabs + p),
-              (unsigned long long)__double_as_longlong(fabs(rt)));
+    for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * x[b + o[q]];
+    const double rt = acc + R.c0[r] - x[R.tgt[r]];
+    R.rd[r] = rt;
+    R.rf[r] = (float)rt;
+    v = (unsigned long long)__double_as_longlong(fabs(rt));  // order-preserving for >= 0
+  }
+  if (!maxabs) return;
+  // rows of one problem are contiguous: one atomic per warp when the warp's
+  // valid rows share a problem
+  const int p0 = __shfl_sync(0xffffffffu, p, 0);
+  const bool same = __all_sync(0xffffffffu, !valid || p == p0);
+  if (same) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long w = __shfl_down_sync(0xffffffffu, v, o);
+      v = v > w ? v : w;
+    }
+    if ((threadIdx.x & 31) == 0 && p0 >= 0)
+      atomicMax(reinterpret_cast<unsigned long long *>(maxabs + p0), v);
+  } else if (valid) {
+    atomicMax(reinterpret_cast<unsigned long long *>(maxabs + p), v);
+  }
 }
 
 cudaError_t rows_residual(const DevRows &R, const DevLevel *lev0, double *maxabs,
@@ -796,8 +981,8 @@ cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, lon
 
 template cudaError_t line_sweep<double>(const Launch &, int, int, double, int, cudaStream_t);
 template cudaError_t line_sweep<float>(const Launch &, int, int, double, int, cudaStream_t);
-template cudaError_t residual<double>(const Launch &, double *, cudaStream_t);
-template cudaError_t residual<float>(const Launch &, double *, cudaStream_t);
+template cudaError_t residual<double>(const Launch &, double *, double *, cudaStream_t);
+template cudaError_t residual<float>(const Launch &, double *, double *, cudaStream_t);
 template cudaError_t restrict_to<double>(const Launch &, const DevLevel *, cudaStream_t);
 template cudaError_t restrict_to<float>(const Launch &, const DevLevel *, cudaStream_t);
 template cudaError_t prolong_add<double>(const Launch &, const DevLevel *, cudaStream_t);
