@@ -1,0 +1,481 @@
+#!/usr/bin/env python
+"""Throughput of the FEICAR3D pressure-Poisson path on B200.
+
+One step = one pressure solve of the workload from a zero initial guess to
+relative residual 1e-8 (||f - A p|| / ||f|| over fluid rows) through the
+library's C ABI.  Workload (default): 512x256x256 cells on [0,16]x[0,8]x[0,8],
+tanh-stretched (beta = 2) in y and z, a sphere of diameter 1 at (4,4,4)
+given as an 81920-triangle icosphere, tagged on the device (iblank, ghost
+and dead lists), seeded smoothed-noise RHS (sigma = 0.01 face velocity) with
+a known discrete solution.  The headline path is the mixed-precision one
+(FP32 V-cycle inside FP64 defect correction); the plain FP64 GPU path is
+measured beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank solves its own copy
+of the workload (replicas: the reference's solve has no cross-problem
+exchange), timing is the maximum over ranks and ``value`` counts the solves
+of all ranks.  ``--impl reference`` times the CPU restatement of the
+reference's own solver (CORE_POISSON.F90 / CORE_MG.F90 / CORE_TDMA.F90) on
+the host cores instead, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib.util
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "feicar3d_3.0_febio_b200")
+
+METRIC = "Poisson solves/s & HBM GB/s, mixed vs FP64 MG at 1e-8 resid; p50/p99 latency"
+UNIT = "solves/s"
+RTOL = 1e-8
+
+# DRAM bytes per finest-level cell of one launch of the dominant kernel
+# class, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
+# 128x64x64 sphere case, mixed path (profiles/line_smoother_config0_mixed.md).
+# None until that capture exists.
+DRAM_BYTES_PER_CELL = {}
+
+
+def _load_pkg():
+    if "feicar_b200" in sys.modules:
+        return sys.modules["feicar_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "feicar_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["feicar_b200"] = mod
+    spec.loader.exec_module(mod)
+    importlib.import_module("feicar_b200.fg")
+    importlib.import_module("feicar_b200.synth")
+    return mod
+
+
+def workload(name):
+    synth = _load_pkg().synth
+    if name == "config1":
+        return (synth.config1_grid(), synth.config1_body(),
+                "512x256x256 cells on [0,16]x[0,8]x[0,8], tanh-stretched (beta=2) in y,z; "
+                "sphere d=1 at (4,4,4), 81920-triangle icosphere")
+    if name == "config0":
+        return (synth.config0_grid(), synth.config0_body(),
+                "128x64x64 uniform cells on [0,8]x[0,4]x[0,4]; sphere d=1 at (2,2,2), "
+                "20480-triangle icosphere")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of this GPU's clocks during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.proc = None
+        self.path = None
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(dev).uuid)
+            sel = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            sel = str(dev)
+        self.sel = sel
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.sel, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 8:
+                    continue
+                try:
+                    sm.append(float(parts[0]))
+                    smax.append(float(parts[1]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[4:8]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if sm:
+            out.update(sm_mhz=float(np.median(sm)), sm_max_mhz=float(max(smax)),
+                       reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+# ------------------------------------------------------------ our path
+def build_case(fg, synth, grid, body, precision, dev, geometry_from=None):
+    cfg = fg.default_config(precision=precision, rtol=RTOL, max_cycles=200)
+    c = fg.Case(grid, cfg, device=dev)
+    if geometry_from is None:
+        c.add_body(body)
+        c.set_iblank_body_fast()
+        ib, gh, dd = c.gcm_set_internal_boundary()
+        geo = (ib, gh, dd, c.ghost_rows(), c.dead_rows())
+    else:
+        geo = geometry_from
+        c.set_geometry(*geo)
+    c.mg_prepare()
+    return c, geo
+
+
+def fluid_mask(grid, ib):
+    m = np.zeros(grid.shape, bool)
+    m[1:grid.nx, 1:grid.ny, 1:grid.nz] = ib[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0
+    return m
+
+
+def relerr(p, ref, m):
+    a = p[m] - p[m].mean()
+    b = ref[m] - ref[m].mean()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def timed_device_solves(torch, fg, c, d_p, d_f, steps, stream):
+    """K solves, CUDA events on the case's stream; per-step events too."""
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    stats = []
+    with torch.cuda.stream(stream):
+        evs[0].record(stream)
+        for k in range(steps):
+            d_p.zero_()
+            stats.append(c.solve_poisson_device(d_p.data_ptr(), d_f.data_ptr()))
+            evs[k + 1].record(stream)
+    stream.synchronize()
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    return evs[0].elapsed_time(evs[-1]), per, stats
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    pkg = _load_pkg()
+    fg, synth = pkg.fg, pkg.synth
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    grid, body, desc = workload(args.workload)
+    t0 = time.time()
+    prec_main = fg.FG_PREC_MIXED if args.precision == "mixed" else fg.FG_PREC_FP64
+    c_main, geo = build_case(fg, synth, grid, body, prec_main, dev)
+    t_tag = time.time() - t0
+    ib, gh, dd, G, D = geo
+    rows = [synth.Interp(D["ijk"], D["cell"], D["coefN"]), synth.Interp(G["ijk"], G["cell"], G["coefN"])]
+    rhs, phi = synth.manufactured_rhs(grid, ib, gh, dd, rows, seed=rank)
+    mask = fluid_mask(grid, ib)
+    nref = int(np.prod(grid.shape))
+    rev = grid.shape[::-1]
+    d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).to(f"cuda:{dev}")
+    d_p = torch.zeros(rev, dtype=torch.float64, device=f"cuda:{dev}")
+    c_main.set_stream(stream.cuda_stream)
+
+    # FP64 GPU path on the same geometry
+    other = fg.FG_PREC_FP64 if prec_main == fg.FG_PREC_MIXED else fg.FG_PREC_MIXED
+    c_other, _ = build_case(fg, synth, grid, body, other, dev, geometry_from=geo)
+    c_other.set_stream(stream.cuda_stream)
+
+    # warm-up (both paths)
+    for _ in range(args.warmup):
+        timed_device_solves(torch, fg, c_main, d_p, d_f, 1, stream)
+    for _ in range(max(1, args.warmup // 2)):
+        timed_device_solves(torch, fg, c_other, d_p, d_f, 1, stream)
+
+    # timed region: headline path, with per-class event timing
+    c_main.profile(True)
+    clocks = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    n0 = fg.launch_count()
+    tot_ms, per_ms, stats = timed_device_solves(torch, fg, c_main, d_p, d_f, args.steps, stream)
+    n1 = fg.launch_count()
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier()
+    prof = c_main.profile_read()
+    c_main.profile(False)
+    tot_ms = max_over_ranks(tot_ms)
+    p_main = d_p.cpu().numpy().transpose(2, 1, 0)
+    err_main = relerr(p_main, phi, mask)
+
+    # plain FP64 (or the other) GPU path, same steps
+    barrier()
+    tot_o, per_o, stats_o = timed_device_solves(torch, fg, c_other, d_p, d_f, args.steps, stream)
+    barrier()
+    tot_o = max_over_ranks(tot_o)
+    p_o = d_p.cpu().numpy().transpose(2, 1, 0)
+    err_o = relerr(p_o, phi, mask)
+
+    # end to end through the host-buffer entry point (pinned host memory)
+    p_h_t = torch.zeros(rev, dtype=torch.float64).pin_memory()
+    f_h_t = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).pin_memory()
+    p_h = p_h_t.numpy().transpose(2, 1, 0)  # Fortran view of the pinned buffer
+    f_h = f_h_t.numpy().transpose(2, 1, 0)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        p_h[...] = 0.0
+        c_main.solve_poisson(p_h, f_h)
+    e1.record(stream)
+    stream.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    err_e2e = relerr(np.array(p_h), phi, mask)
+
+    # roofline of the dominant launch class
+    hbm, peak_kind = peaks()
+    line = {k: v for k, v in prof.items() if k.startswith("line_") and k != "line_coarse"}
+    dom = max(line, key=lambda k: line[k]["ms"])
+    dm = prof[dom]
+    achieved = (dm["bytes"] / 1e9) / (dm["ms"] / 1e3) if dm["ms"] > 0 else 0.0
+    total_prof_ms = sum(v["ms"] for v in prof.values())
+    cells = (grid.nx - 1) * (grid.ny - 1) * (grid.nz - 1)
+    traffic = None
+    key = (args.workload, args.precision, dom)
+    if key in DRAM_BYTES_PER_CELL:
+        traffic = DRAM_BYTES_PER_CELL[key] * cells / 2.0
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(grid, body, rhs, args.cpu_iters)
+
+    if rank == 0:
+        nsteps = args.steps * world
+        ms_step = tot_ms / args.steps
+        lat = np.array(per_ms)
+        out = {
+            "metric": METRIC,
+            "value": nsteps / (tot_ms / 1e3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+            "data": "synthetic (seeded smoothed-noise RHS with known discrete solution; body tagged on device)",
+            "config": {
+                "workload": args.workload, "desc": desc, "cells": cells,
+                "precision": args.precision, "rtol": RTOL, "cycle": "V(2,2) x/y/z zebra line relaxation",
+                "parallelism": f"replicas x{world}",
+                "l2": "inputs larger than L2 (working set > 1 GB per solve)",
+            },
+            "cycles": [s["cycles"] for s in stats][-1],
+            "relres": max(s["relres"] for s in stats),
+            "err_vs_exact": err_main,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "cell_updates_per_s": cells * nsteps / (tot_ms / 1e3),
+            "fp64" if args.precision == "mixed" else "mixed": {
+                "value": nsteps / (tot_o / 1e3), "ms_per_step": tot_o / args.steps,
+                "cycles": stats_o[-1]["cycles"], "relres": max(s["relres"] for s in stats_o),
+                "err_vs_exact": err_o,
+            },
+            "speedup_mixed_over_fp64": (tot_o / tot_ms) if args.precision == "mixed" else (tot_ms / tot_o),
+            "roofline": {
+                "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                "launches": dm["launches"], "avg_launch_us": 1e3 * dm["ms"] / max(1, dm["launches"]),
+                "share_of_timed_launch_groups": dm["ms"] / total_prof_ms if total_prof_ms else None,
+            },
+            "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+            "e2e": {"value": nsteps / (e2e_ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": 2 * nref * 8, "d2h_bytes_per_step": nref * 8,
+                    "err_vs_exact": err_e2e},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": n1 - n0,
+            "setup_s": {"tag_and_prepare": t_tag},
+        }
+        print(json.dumps(out), flush=True)
+    c_other.close()
+    c_main.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------- CPU reference
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
+def cpu_baseline_sample(grid, body, rhs, iters):
+    """The CPU restatement of the reference solver on the same grid, body
+    and RHS: `iters` outer iterations of solve_poisson (each one MG cycle,
+    ghost-cell update, residual), continued from the previous iterate.
+    solves/s = 1 / (seconds per iteration x iterations to reach 1e-8), the
+    iteration count extrapolated from the measured per-iteration residual
+    reduction."""
+    O = _oracle()
+    t0 = time.time()
+    oc = O.OracleCase(grid)
+    oc.add_body(body)
+    oc.set_iblank()
+    oc.gcm(2.0, 2.0)
+    oc.mg_prepare()
+    t_setup = time.time() - t0
+    p = np.zeros(grid.shape, order="F")
+    f = np.asfortranarray(rhs)
+    res, secs = [], []
+    for _ in range(iters):
+        t = time.time()
+        rc, st = oc.solve_poisson(p, f, params=O.default_params(itermax_pson=1, iterInter=0,
+                                                                restol_pson=RTOL))
+        secs.append(time.time() - t)
+        res.append(oc.relres(p, f))
+    s_it = float(np.mean(secs))
+    rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if len(res) > 1 and res[0] > 0 else float("nan")
+    if 0.0 < rho < 1.0:
+        n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho))
+    else:
+        n_need = float("nan")
+    val = 1.0 / (s_it * n_need) if n_need == n_need else None
+    return {"value": val, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{iters} outer iterations (one V-cycle each, iterInter=0) of the reference "
+                      f"solve_poisson restatement (MG V-cycle, line SOR, ghost-cell update) on the full grid; "
+                      f"{s_it:.2f} s/iteration, residual factor {rho:.3f}/iteration, "
+                      f"{n_need:.1f} iterations to 1e-8 (extrapolated); setup {t_setup:.1f} s untimed",
+            "s_per_iteration": s_it, "relres": res}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    grid, body, desc = workload(args.workload)
+    synth = _load_pkg().synth
+    O = _oracle()
+    oc = O.OracleCase(grid)
+    oc.add_body(body)
+    oc.set_iblank()
+    oc.gcm(2.0, 2.0)
+    oc.mg_prepare()
+    G, D = oc.ghosts(), oc.deads()
+    rows = [synth.Interp(D["ijk"], D["cell"], D["coefN"]), synth.Interp(G["ijk"], G["cell"], G["coefN"])]
+    rhs, phi = synth.manufactured_rhs(grid, oc.field(0), oc.field(1), oc.field(2), rows, seed=0)
+    f = np.asfortranarray(rhs)
+    p = np.zeros(grid.shape, order="F")
+    prm = O.default_params(itermax_pson=1, iterInter=0, restol_pson=RTOL)
+    for _ in range(args.warmup):
+        oc.solve_poisson(p, f, params=prm)
+    p[...] = 0.0
+    res, secs = [], []
+    for _ in range(args.steps):
+        t = time.time()
+        oc.solve_poisson(p, f, params=prm)
+        secs.append(time.time() - t)
+        res.append(oc.relres(p, f))
+    s_it = float(np.mean(secs))
+    rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if len(res) > 1 and res[0] > 0 else float("nan")
+    n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
+    val = 1.0 / (s_it * n_need) if n_need == n_need else 0.0
+    sample = (f"each step one outer iteration (one V-cycle, iterInter=0) of the reference solve_poisson "
+              f"restatement on the full "
+              f"grid (continued iterate); solves/s = 1/(s per iteration x {n_need:.1f} iterations to 1e-8, "
+              f"extrapolated from residual factor {rho:.3f})")
+    cells = (grid.nx - 1) * (grid.ny - 1) * (grid.nz - 1)
+    out = {
+        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * s_it, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "desc": desc, "cells": cells, "precision": "fp64",
+                   "rtol": RTOL},
+        "impl": "reference",
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "relres": res,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="config1")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

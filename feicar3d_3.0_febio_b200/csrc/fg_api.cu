@@ -165,22 +165,32 @@ static fg_status upload_axes(fg_case *c, int l) {
   FG_CUDA(cudaMalloc(&L.d_int, ints.size() * sizeof(int)));
   FG_CUDA(cudaMemcpy(L.d_int, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
   DevLevel &d = L.dl;
-  memset(&d, 0, sizeof(d));
+  d = DevLevel{};
   d.nx = L.nx; d.ny = L.ny; d.nz = L.nz;
   d.sy = L.sy; d.sz = L.sz; d.ntot = L.ntot;
-  d.type = L.d_type;
-  d.mask = L.d_mask;
-  d.amx = L.d_coef + doff[0][0]; d.apx = L.d_coef + doff[0][1];
-  d.amy = L.d_coef + doff[1][0]; d.apy = L.d_coef + doff[1][1];
-  d.amz = L.d_coef + doff[2][0]; d.apz = L.d_coef + doff[2][1];
-  d.wx = L.d_coef + doff[0][2]; d.wy = L.d_coef + doff[1][2]; d.wz = L.d_coef + doff[2][2];
-  d.pwx = L.d_coef + doff[0][3]; d.pwy = L.d_coef + doff[1][3]; d.pwz = L.d_coef + doff[2][3];
-  d.clx = L.d_int + ioff[0][0]; d.chx = L.d_int + ioff[0][1]; d.plx = L.d_int + ioff[0][2];
-  d.cly = L.d_int + ioff[1][0]; d.chy = L.d_int + ioff[1][1]; d.ply = L.d_int + ioff[1][2];
-  d.clz = L.d_int + ioff[2][0]; d.chz = L.d_int + ioff[2][1]; d.plz = L.d_int + ioff[2][2];
+  const long long nt = L.ntot, ax[3] = {L.nx + 2, L.ny + 2, L.nz + 2};
+  d.type = mkptr<const int8_t>(L.d_type, nt, K_TYPE);
+  d.mask = mkptr<const uint8_t>(L.d_mask, nt, K_MASK);
+  const double *cf = L.d_coef;
+  const int *ci = L.d_int;
+  d.amx = mkptr(cf + doff[0][0], ax[0], K_AXIS); d.apx = mkptr(cf + doff[0][1], ax[0], K_AXIS);
+  d.amy = mkptr(cf + doff[1][0], ax[1], K_AXIS); d.apy = mkptr(cf + doff[1][1], ax[1], K_AXIS);
+  d.amz = mkptr(cf + doff[2][0], ax[2], K_AXIS); d.apz = mkptr(cf + doff[2][1], ax[2], K_AXIS);
+  d.wx = mkptr(cf + doff[0][2], ax[0], K_WIDTH); d.wy = mkptr(cf + doff[1][2], ax[1], K_WIDTH);
+  d.wz = mkptr(cf + doff[2][2], ax[2], K_WIDTH);
+  d.pwx = mkptr(cf + doff[0][3], ax[0], K_PROL); d.pwy = mkptr(cf + doff[1][3], ax[1], K_PROL);
+  d.pwz = mkptr(cf + doff[2][3], ax[2], K_PROL);
+  d.clx = mkptr(ci + ioff[0][0], ax[0], K_CHILD); d.chx = mkptr(ci + ioff[0][1], ax[0], K_CHILD);
+  d.plx = mkptr(ci + ioff[0][2], ax[0], K_PROL);
+  d.cly = mkptr(ci + ioff[1][0], ax[1], K_CHILD); d.chy = mkptr(ci + ioff[1][1], ax[1], K_CHILD);
+  d.ply = mkptr(ci + ioff[1][2], ax[1], K_PROL);
+  d.clz = mkptr(ci + ioff[2][0], ax[2], K_CHILD); d.chz = mkptr(ci + ioff[2][1], ax[2], K_CHILD);
+  d.plz = mkptr(ci + ioff[2][2], ax[2], K_PROL);
   for (int f = 0; f < 6; ++f) d.bc[f] = (c->cfg.pbc[f] == FG_PBC_DIRICHLET) ? 1 : 0;
-  d.x64 = L.d_x64; d.rhs64 = L.d_rhs64; d.res64 = L.d_res64;
-  d.x32 = L.d_x32; d.rhs32 = L.d_rhs32; d.res32 = L.d_res32;
+  d.x64 = mkptr(L.d_x64, nt, K_X); d.rhs64 = mkptr(L.d_rhs64, nt, K_RHS);
+  d.res64 = mkptr(L.d_res64, nt, K_RES);
+  d.x32 = mkptr(L.d_x32, nt, K_X); d.rhs32 = mkptr(L.d_rhs32, nt, K_RHS);
+  d.res32 = mkptr(L.d_res32, nt, K_RES);
   return FG_OK;
 }
 
@@ -204,8 +214,6 @@ static void coarsest_inverse(fg_case *c) {
       }
   const int n = (int)idx.size();
   std::vector<double> A((size_t)n * n, 0.0);
-  const double *am[3] = {nullptr, nullptr, nullptr};
-  (void)am;
   for (int r = 0; r < n; ++r) {
     long long id = idx[r];
     int k = (int)(id / L.sz), j = (int)((id % L.sz) / L.sy), i = (int)(id % L.sy);
@@ -286,6 +294,7 @@ struct fg_batch {
         *d_off_next = nullptr;
     Launch cells, xl, yl, zl, next;
     int maxnx = 0, maxny = 0, maxnz = 0;
+    double ncells = 0.0;  // cells of level L summed over S
     const double **d_G = nullptr;
     const int **d_gidx = nullptr;
     int *d_gn = nullptr;
@@ -305,6 +314,19 @@ struct fg_batch {
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
   std::vector<double> h_norm;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // optional CUDA-event timing of launch classes (fg_profile)
+  struct Prof {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    struct Rec {
+      int cls;
+      size_t e0;
+      double bytes;
+    };
+    std::vector<Rec> recs;
+    fg_profile acc{};
+  } prof;
 };
 
 namespace fg {
@@ -375,6 +397,7 @@ static fg_status build_batch(fg_batch *b) {
         s.maxnx = std::max(s.maxnx, d.nx);
         s.maxny = std::max(s.maxny, d.ny);
         s.maxnz = std::max(s.maxnz, d.nz);
+        s.ncells += (double)d.nx * d.ny * d.nz;
       } else if (L == c->nlev - 1) {
         s.C.push_back(p);
         vC.push_back(c->lev[L].dl);
@@ -437,13 +460,13 @@ static fg_status build_batch(fg_batch *b) {
       FG_CUDA(cudaMemset(b->d_rf, 0, n * sizeof(float)));
     }
     b->rows.n = n;
-    b->rows.prob = b->d_rprob;
-    b->rows.tgt = b->d_rtgt;
-    b->rows.cell = b->d_rcell;
-    b->rows.w = b->d_rw;
-    b->rows.c0 = b->d_rc0;
-    b->rows.rd = b->d_rd;
-    b->rows.rf = b->d_rf;
+    b->rows.prob = mkptr<const int>(b->d_rprob, n, K_ROWS);
+    b->rows.tgt = mkptr<const long long>(b->d_rtgt, n, K_ROWS);
+    b->rows.cell = mkptr<const long long>(b->d_rcell, n, K_ROWS);
+    b->rows.w = mkptr<const double>(b->d_rw, 8LL * n, K_ROWS);
+    b->rows.c0 = mkptr<const double>(b->d_rc0, n, K_ROWS);
+    b->rows.rd = mkptr(b->d_rd, n, K_ROWS);
+    b->rows.rf = mkptr(b->d_rf, n, K_ROWS);
   }
   FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
   FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, b->all0.blocks) * sizeof(double)));
@@ -461,6 +484,50 @@ static fg_status build_batch(fg_batch *b) {
     }                                                                \
   } while (0)
 
+// Event pair around a group of launches of class cls when timing is on.
+static size_t prof_begin(fg_batch *b, cudaStream_t s) {
+  auto &P = b->prof;
+  if (!P.on) return (size_t)-1;
+  while (P.pool.size() < P.used + 2) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return (size_t)-1;
+    P.pool.push_back(e);
+  }
+  const size_t e0 = P.used;
+  P.used += 2;
+  cudaEventRecord(P.pool[e0], s);
+  return e0;
+}
+static void prof_end(fg_batch *b, size_t e0, int cls, double bytes, cudaStream_t s) {
+  auto &P = b->prof;
+  if (!P.on || e0 == (size_t)-1) return;
+  cudaEventRecord(P.pool[e0 + 1], s);
+  P.recs.push_back({cls, e0, bytes});
+}
+// after the stream has drained: fold the recorded pairs into the totals
+static void prof_collect(fg_batch *b) {
+  auto &P = b->prof;
+  for (const auto &r : P.recs) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, P.pool[r.e0], P.pool[r.e0 + 1]) == cudaSuccess) {
+      P.acc.class_launches[r.cls] += 1;
+      P.acc.class_ms[r.cls] += ms;
+      P.acc.class_bytes[r.cls] += r.bytes;
+    }
+  }
+  P.recs.clear();
+  P.used = 0;
+}
+
+// algorithmic bytes of one colour of a directional line sweep over `cells`
+// cells: right-hand side read, unknown written, unknown read once as a
+// neighbour, the mask byte, and the old value of the line when omega != 1
+template <typename T>
+static double sweep_bytes(double cells, double omega) {
+  const double s = (double)sizeof(T);
+  return 0.5 * cells * (3.0 * s + 1.0 + (omega != 1.0 ? s : 0.0));
+}
+
 template <typename T>
 static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
   auto &ls = b->ls[L];
@@ -469,8 +536,17 @@ static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
   for (int axis = 0; axis < 3; ++axis) {
     const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
     const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
-    for (int color = 0; color < 2; ++color) FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, s));
-    if (L == 0) FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+    const int cls = L == 0 ? FG_PROF_LINE_X0 + axis : FG_PROF_LINE_COARSE;
+    for (int color = 0; color < 2; ++color) {
+      const size_t e0 = prof_begin(b, s);
+      FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, s));
+      prof_end(b, e0, cls, sweep_bytes<T>(ls.ncells, om), s);
+    }
+    if (L == 0) {
+      const size_t e0 = prof_begin(b, s);
+      FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+      prof_end(b, e0, FG_PROF_ROWS, 0.0, s);
+    }
   }
   return FG_OK;
 }
@@ -484,18 +560,29 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
     if (!ls.S.empty()) {
       for (int q = 0; q < b->cfg.nu1; ++q)
         if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
+      const size_t e0 = prof_begin(b, s);
       FG_K(k::residual<T>(ls.cells, nullptr, nullptr, s));
       FG_K(k::restrict_to<T>(ls.next, ls.d_levS, s));
       FG_K(k::zero_x<T>(ls.next, s));
+      prof_end(b, e0, FG_PROF_TRANSFER, 0.0, s);
     }
-    if (!ls.C.empty())
+    if (!ls.C.empty()) {
+      const size_t e0 = prof_begin(b, s);
       FG_K(k::coarsest_solve<T>((int)ls.C.size(), ls.d_levC, ls.d_G, ls.d_gidx, ls.d_gn, ls.maxgn, s));
+      prof_end(b, e0, FG_PROF_COARSEST, 0.0, s);
+    }
   }
   for (int L = b->maxdepth - 2; L >= 0; --L) {
     auto &ls = b->ls[L];
     if (ls.S.empty()) continue;
+    size_t e0 = prof_begin(b, s);
     FG_K(k::prolong_add<T>(ls.cells, ls.d_levS_next, s));
-    if (L == 0) FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+    prof_end(b, e0, FG_PROF_TRANSFER, 0.0, s);
+    if (L == 0) {
+      e0 = prof_begin(b, s);
+      FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
+      prof_end(b, e0, FG_PROF_ROWS, 0.0, s);
+    }
     for (int q = 0; q < b->cfg.nu2; ++q)
       if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
   }
@@ -533,12 +620,14 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     cudaEventRecord(vb, s);
     FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
     FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
+    const size_t e0 = prof_begin(b, s);
     if (mixed) {
       FG_K(k::correct_residual(b->all0, b->d_norm, b->d_part, s));
     } else {
       FG_K(k::residual<double>(b->all0, b->d_norm, b->d_part, s));
     }
     FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
     FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double),
                             cudaMemcpyDeviceToHost, s));
     FG_CUDA(cudaStreamSynchronize(s));
@@ -560,6 +649,7 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
   float tot = 0.0f;
   cudaEventElapsedTime(&tot, b->ev0, b->ev1);
   cudaEventDestroy(va); cudaEventDestroy(vb);
+  if (b->prof.on) prof_collect(b);
   if (st) {
     double mr = 0.0, mg = 0.0;
     for (int p = 0; p < np; ++p) { mr = std::max(mr, relres[p]); mg = std::max(mg, gres[p]); }
@@ -578,7 +668,7 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
 // level-0 types and rows from the reference masks and lists
 static fg_status install_geometry(fg_case *c) {
   HLevel &L0 = c->lev[0];
-  const int nx = c->nx, ny = c->ny, nz = c->nz;  // nodes
+  const int nx = c->nx, ny = c->ny;  // nodes
   const long long RX = nx + 2, RY = ny + 2;
   auto ref = [&](int i, int j, int k) { return (long long)i + RX * ((long long)j + RY * k); };
   L0.type.assign(L0.ntot, T_BOUND);
@@ -731,7 +821,10 @@ const char *fg_status_string(fg_status s) {
     case FG_TIMEOUT: return "timeout";
     case FG_BAD_INPUT: return "bad input";
     case FG_GEOMETRY_DEAD_NO_BODY: return "dead cell without body";
-    case FG_CUDA_ERROR: return fg::last_error_msg();
+    case FG_CUDA_ERROR: {
+      const char *m = fg::last_error_msg();
+      return (m && *m) ? m : "CUDA error";
+    }
     case FG_NO_DEVICE: return "no CUDA device";
     case FG_REJECTED: return "rejected by admission";
   }
@@ -798,7 +891,8 @@ fg_status fg_case_create(int nx, int ny, int nz, const double *xn, const double 
   cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   const size_t nref = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
   if (cudaMalloc(&c->d_pin, nref * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->d_fin, nref * sizeof(double)) != cudaSuccess) {
+      cudaMalloc(&c->d_fin, nref * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_gauge, sizeof(double)) != cudaSuccess) {
     fg_case_destroy(c);
     return FG_ALLOC_FAIL;
   }
@@ -818,8 +912,9 @@ fg_status fg_case_destroy(fg_case *c) {
     cudaFree(L.d_x32); cudaFree(L.d_rhs32); cudaFree(L.d_res32);
   }
   cudaFree(c->d_G); cudaFree(c->d_gidx); cudaFree(c->d_pin); cudaFree(c->d_fin);
+  cudaFree(c->d_gauge);
   if (c->geom) geom_free(*c->geom);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
   return FG_OK;
 }
@@ -932,13 +1027,10 @@ static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
     const double dpdn = dpdn_d ? dpdn_d[r] : 0.0;
     double v = 0.0;
     if (c->d_fallback[r]) {
-      // inverse squared distance over fluid and dead corners of the image
-      // point's host cell, previous-step pressure (p_old = 0 when absent)
-      double xIP = 0, yIP = 0, zIP = 0;
-      // image point: cell + (BI - cell) * probe is not kept here; use the
-      // distance to the dead cell's own image point when the geometry came
-      // from the device tagging, else the host cell centre
-      (void)xIP; (void)yIP; (void)zIP;
+      // inverse squared distance from the dead cell's image point (the
+      // host cell's centre when the caller supplied no image points) over
+      // the fluid and dead corners of the host cell, previous-step pressure
+      // (p_old = 0 when absent)
       double num = 0.0, den = 0.0;
       const double *ipp = c->d_ipv.size() >= 3 * (size_t)(r + 1) ? &c->d_ipv[3 * r] : nullptr;
       double X = ipp ? ipp[0] : 0.5 * (xcv(0, ci) + xcv(0, ci + 1));
@@ -978,48 +1070,13 @@ static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
   }
 }
 
+// gauge and outer boundary layers on the device copy of the output
 static fg_status finish_output(fg_case *c) {
-  // gauge (CORE_POISSON.F90:129-149 pins p(1,1,1)) and outer boundary
-  // layers (CORE_SET_OUTER_BC.F90:1088-1170) are applied on the host copy
-  (void)c;
-  return FG_OK;
-}
-
-static void host_fill_bc(fg_case *c, double *p) {
-  const int nx = c->nx, ny = c->ny, nz = c->nz;
-  const long long RX = nx + 2, RY = ny + 2;
-  auto P = [&](int i, int j, int k) -> double & { return p[i + RX * (j + RY * (long long)k)]; };
   bool allN = true;
   for (int f = 0; f < 6; ++f) allN &= (c->cfg.pbc[f] == FG_PBC_NEUMANN);
-  if (allN && c->cfg.gauge_corner) {
-    const double pa = P(1, 1, 1);
-    for (int k = 0; k <= nz; ++k)
-      for (int j = 0; j <= ny; ++j)
-        for (int i = 0; i <= nx; ++i) {
-          long long id = i + RX * (j + RY * (long long)k);
-          if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1 &&
-              c->iblank.size() && c->iblank[id] == 1 && c->dead[id] != -1)
-            continue;  // pure-solid values are held
-          p[id] -= pa;
-        }
-  }
-  const double *pp = c->cfg.ppp;
-  auto bcv = [&](int f, double inner) { return c->cfg.pbc[f] == FG_PBC_DIRICHLET ? 2.0 * pp[f] - inner : inner; };
-  for (int k = 1; k <= nz - 1; ++k)
-    for (int j = 1; j <= ny - 1; ++j) {
-      P(0, j, k) = bcv(0, P(1, j, k));
-      P(nx, j, k) = bcv(1, P(nx - 1, j, k));
-    }
-  for (int k = 1; k <= nz - 1; ++k)
-    for (int i = 0; i <= nx; ++i) {
-      P(i, 0, k) = bcv(2, P(i, 1, k));
-      P(i, ny, k) = bcv(3, P(i, ny - 1, k));
-    }
-  for (int j = 1; j <= ny - 1; ++j)
-    for (int i = 0; i <= nx; ++i) {
-      P(i, j, 0) = bcv(4, P(i, j, 1));
-      P(i, j, nz) = bcv(5, P(i, j, nz - 1));
-    }
+  FG_K(k::finish_field(c->d_pin, &c->lev[0].dl, c->nx, c->ny, c->nz, c->cfg.pbc, c->cfg.ppp,
+                       (allN && c->cfg.gauge_corner) ? 1 : 0, c->d_gauge, c->stream));
+  return FG_OK;
 }
 
 static fg_status solve_common(fg_case *c, const double *p_old, const double *dpdn_g,
@@ -1050,10 +1107,10 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div, const doubl
   FG_CUDA(cudaMemcpyAsync(c->d_fin, div, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   fg_status s = solve_common(c, p_old, dpdn_ghost, dpdn_dead, st);
   if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
+  fg_status f = finish_output(c);
+  if (f != FG_OK) return f;
   FG_CUDA(cudaMemcpyAsync(p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   FG_CUDA(cudaStreamSynchronize(c->stream));
-  host_fill_bc(c, p);
-  (void)finish_output;
   return s;
 }
 
@@ -1067,6 +1124,8 @@ fg_status fg_solve_poisson_device(fg_case *c, double *d_p, const double *d_div,
   FG_CUDA(cudaMemcpyAsync(c->d_fin, d_div, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   fg_status s = solve_common(c, nullptr, nullptr, nullptr, st);
   if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
+  fg_status f = finish_output(c);
+  if (f != FG_OK) return f;
   FG_CUDA(cudaMemcpyAsync(d_p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   FG_CUDA(cudaStreamSynchronize(c->stream));
   return s;
@@ -1154,8 +1213,49 @@ fg_status fg_batch_solve_device(fg_batch *b, double **d_p, const double **d_div,
   return s;
 }
 
+fg_status fg_case_set_stream(fg_case *c, void *stream) {
+  if (!c) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  if (stream) {
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+  } else {
+    FG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+  }
+  if (c->solo) c->solo->stream = c->stream;
+  return FG_OK;
+}
+
+fg_status fg_launch_count(long long *count) {
+  if (!count) return FG_BAD_INPUT;
+  *count = launches_so_far();
+  return FG_OK;
+}
+
+fg_status fg_case_profile(fg_case *c, int enable) {
+  if (!c) return FG_BAD_INPUT;
+  fg_status st = ensure_solo(c);
+  if (st != FG_OK) return st;
+  auto &P = c->solo->prof;
+  P.on = enable != 0;
+  P.recs.clear();
+  P.used = 0;
+  P.acc = fg_profile{};
+  return FG_OK;
+}
+
+fg_status fg_case_profile_read(const fg_case *c, fg_profile *out) {
+  if (!c || !out || !c->solo) return FG_BAD_INPUT;
+  *out = c->solo->prof.acc;
+  return FG_OK;
+}
+
 fg_status fg_batch_destroy(fg_batch *b) {
   if (!b) return FG_OK;
+  for (cudaEvent_t e : b->prof.pool) cudaEventDestroy(e);
   cudaSetDevice(b->device);
   free_batch_tables(b);
   if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }

@@ -51,6 +51,7 @@ struct fg_case {
   int nlev = 0;
   fg::HLevel lev[fg::kMaxLevels];
   cudaStream_t stream = nullptr;
+  bool own_stream = true;  // false after fg_case_set_stream(c, caller's stream)
   // geometry
   std::unique_ptr<fg::Geom> geom;
   std::vector<double> d_ipv;           // dead-cell image points (3 per row)
@@ -71,6 +72,7 @@ struct fg_case {
   int *d_gidx = nullptr;
   // reference-layout staging buffers on the device
   double *d_pin = nullptr, *d_fin = nullptr;
+  double *d_gauge = nullptr;  // p(1,1,1) of the output gauge
   bool batch_dirty = true;
   struct fg_batch *solo = nullptr;
 };

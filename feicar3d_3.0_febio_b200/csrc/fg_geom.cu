@@ -1,10 +1,25 @@
-// fg_geom.cu -- immersed-boundary tagging on the device (placeholder entry
-// points; the kernels follow).
+// fg_geom.cu -- immersed-boundary tagging and ghost/dead-cell geometry on the
+// device (sm_100a).  Compiled with --fmad=false: every FP64 expression is
+// evaluated one IEEE operation at a time in the written order, so iblank,
+// the ghost and dead lists and their host cells are bit-identical to the
+// CPU restatement of BOUNDARY_IBLANK_FAST.F90 and GCM_SET_BOUNDARY.F90.
+//
+// Fields here use the reference layout (0:nx+1, 0:ny+1, 0:nz+1), nx, ny, nz
+// node counts, index i + (nx+2)*(j + (ny+2)*k).
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "fg_case.h"
 
 namespace fg {
+
 void geom_free(Geom &g) {
   for (auto &b : g.bodies) {
     cudaFree(b.d_xyz); cudaFree(b.d_en); cudaFree(b.d_vn); cudaFree(b.d_tri);
@@ -13,15 +28,1223 @@ void geom_free(Geom &g) {
   g.bodies.clear();
   cudaFree(g.d_iblank); cudaFree(g.d_ghost); cudaFree(g.d_dead); cudaFree(g.d_body);
   cudaFree(g.d_band); cudaFree(g.d_tmp); cudaFree(g.d_xc);
+  g.d_iblank = g.d_ghost = g.d_dead = g.d_body = g.d_band = g.d_tmp = nullptr;
+  g.d_xc = nullptr;
 }
+
+namespace geo {
+
+// grid arrays in reference indexing, all length n+2
+struct Grid {
+  int nx, ny, nz;
+  long long NX, NY;
+  const double *x, *y, *z, *xc, *yc, *zc, *dx, *dy, *dz, *dxc, *dyc, *dzc;
+};
+
+struct Body {
+  int nvert, ntri, type, dim;
+  double mt;  // membrane thickness
+  const double *vx, *vy, *vz;  // vertices
+  const double *enx, *eny, *enz;  // element unit normals
+  const double *vnx, *vny, *vnz;  // vertex unit normals
+  const int *tri;
+  const int *v2t_off, *v2t;
+};
+
+__device__ __forceinline__ long long ridx(const Grid &g, int i, int j, int k) {
+  return (long long)i + g.NX * ((long long)j + g.NY * (long long)k);
+}
+
+// ------------------------------------------------- body intercept query
+__device__ void cross3(const double *r, const double *s, double *o) {
+  o[0] = r[1] * s[2] - s[1] * r[2];
+  o[1] = r[2] * s[0] - s[2] * r[0];
+  o[2] = r[0] * s[1] - s[0] * r[1];
+}
+
+// BOUNDARY_IBLANK_FAST.F90:1220-1313
+__device__ void bi_inside(const double *xv, const double *yv, const double *zv, double xb,
+                          double yb, double zb, double *a123o, double *adiffo) {
+  double s12 = sqrt((xv[1] - xv[0]) * (xv[1] - xv[0]) + (yv[1] - yv[0]) * (yv[1] - yv[0]) + (zv[1] - zv[0]) * (zv[1] - zv[0]));
+  double s23 = sqrt((xv[2] - xv[1]) * (xv[2] - xv[1]) + (yv[2] - yv[1]) * (yv[2] - yv[1]) + (zv[2] - zv[1]) * (zv[2] - zv[1]));
+  double s31 = sqrt((xv[0] - xv[2]) * (xv[0] - xv[2]) + (yv[0] - yv[2]) * (yv[0] - yv[2]) + (zv[0] - zv[2]) * (zv[0] - zv[2]));
+  double s14 = sqrt((xb - xv[0]) * (xb - xv[0]) + (yb - yv[0]) * (yb - yv[0]) + (zb - zv[0]) * (zb - zv[0]));
+  double s24 = sqrt((xb - xv[1]) * (xb - xv[1]) + (yb - yv[1]) * (yb - yv[1]) + (zb - zv[1]) * (zb - zv[1]));
+  double s34 = sqrt((xb - xv[2]) * (xb - xv[2]) + (yb - yv[2]) * (yb - yv[2]) + (zb - zv[2]) * (zb - zv[2]));
+  double p123 = 0.5 * (s12 + s23 + s31);
+  double p124 = 0.5 * (s12 + s24 + s14);
+  double p234 = 0.5 * (s23 + s24 + s34);
+  double p314 = 0.5 * (s31 + s34 + s14);
+  double a123 = sqrt(p123 * fabs(p123 - s12) * fabs(p123 - s23) * fabs(p123 - s31));
+  double a124 = sqrt(p124 * fabs(p124 - s12) * fabs(p124 - s24) * fabs(p124 - s14));
+  double a234 = sqrt(p234 * fabs(p234 - s23) * fabs(p234 - s24) * fabs(p234 - s34));
+  double a314 = sqrt(p314 * fabs(p314 - s31) * fabs(p314 - s34) * fabs(p314 - s14));
+  *a123o = a123;
+  *adiffo = a124 + a234 + a314 - a123;
+}
+
+// BOUNDARY_IBLANK_FAST.F90:1316-1536 (side fallback as in the restatement)
+__device__ void bi_outside(const double *xv, const double *yv, const double *zv, double xcg,
+                           double ycg, double zcg, const double *xvn, const double *yvn,
+                           const double *zvn, double *xb, double *yb, double *zb, double *dist,
+                           double *nx_, double *ny_, double *nz_, int *warn) {
+  double v4[3] = {*xb, *yb, *zb};
+  int sel = -1;
+  double best = 0.0;
+  int bestside = 1;
+  for (int iside = 1; iside <= 3; ++iside) {
+    int mside = iside + 1;
+    if (iside == 3) mside = 1;
+    int kside = iside == 1 ? 3 : (iside == 2 ? 1 : 2);
+    double v1[3] = {xv[iside - 1], yv[iside - 1], zv[iside - 1]};
+    double v2[3] = {xv[mside - 1], yv[mside - 1], zv[mside - 1]};
+    double v3[3] = {xv[kside - 1], yv[kside - 1], zv[kside - 1]};
+    double a[3] = {v3[0] - v1[0], v3[1] - v1[1], v3[2] - v1[2]};
+    double b[3] = {v2[0] - v1[0], v2[1] - v1[1], v2[2] - v1[2]};
+    double cc[3] = {v4[0] - v1[0], v4[1] - v1[1], v4[2] - v1[2]};
+    double axb[3], cxb[3];
+    cross3(a, b, axb);
+    cross3(cc, b, cxb);
+    double dotVal = cxb[0] * axb[0] + cxb[1] * axb[1] + cxb[2] * axb[2];
+    if (iside == 1 || dotVal < best) { best = dotVal; bestside = iside; }
+    if (dotVal <= 0.0) { sel = iside; break; }
+  }
+  if (sel < 0) { sel = bestside; (*warn)++; }
+  int s1 = sel == 1 ? 0 : (sel == 2 ? 1 : 2);
+  int s2 = sel == 1 ? 1 : (sel == 2 ? 2 : 0);
+  double n12x = xv[s2] - xv[s1], n12y = yv[s2] - yv[s1], n12z = zv[s2] - zv[s1];
+  double mag = sqrt(n12x * n12x + n12y * n12y + n12z * n12z);
+  n12x = n12x / mag; n12y = n12y / mag; n12z = n12z / mag;
+  double plen = (*xb - xv[s1]) * n12x + (*yb - yv[s1]) * n12y + (*zb - zv[s1]) * n12z;
+  double xB = xv[s1] + plen * n12x, yB = yv[s1] + plen * n12y, zB = zv[s1] + plen * n12z;
+  double d1 = sqrt((xv[s1] - xB) * (xv[s1] - xB) + (yv[s1] - yB) * (yv[s1] - yB) + (zv[s1] - zB) * (zv[s1] - zB)) / mag;
+  double d2 = sqrt((xv[s2] - xB) * (xv[s2] - xB) + (yv[s2] - yB) * (yv[s2] - yB) + (zv[s2] - zB) * (zv[s2] - zB)) / mag;
+  if (d1 <= 1.0 && d2 <= 1.0) {
+    *xb = xB; *yb = yB; *zb = zB;
+    *nx_ = 0.5 * (xvn[s1] + xvn[s2]);
+    *ny_ = 0.5 * (yvn[s1] + yvn[s2]);
+    *nz_ = 0.5 * (zvn[s1] + zvn[s2]);
+  } else if (d2 > 1.0) {
+    *xb = xv[s1]; *yb = yv[s1]; *zb = zv[s1];
+    *nx_ = xvn[s1]; *ny_ = yvn[s1]; *nz_ = zvn[s1];
+  } else {
+    *xb = xv[s2]; *yb = yv[s2]; *zb = zv[s2];
+    *nx_ = xvn[s2]; *ny_ = yvn[s2]; *nz_ = zvn[s2];
+  }
+  *dist = sqrt((xcg - *xb) * (xcg - *xb) + (ycg - *yb) * (ycg - *yb) + (zcg - *zb) * (zcg - *zb));
+}
+
+struct BIResult {
+  double x, y, z, dist, dot;
+  int elem;
+};
+
+// BOUNDARY_IBLANK_FAST.F90:857-1216 for one point, by one warp: the
+// nearest vertex (first index of the minimum) by a lane-parallel scan, then
+// the incident triangles of that vertex one per lane, the kept element being
+// the last one (in triangle order) at the minimum distance -- the element
+// the sequential "dist <= distMin" loop keeps.
+__device__ BIResult body_intercept_warp(const Body &B, double xC, double yC, double zC,
+                                        int lane, int *warn) {
+  double dmin = 0.0;
+  int vmin = 0x7fffffff;
+  for (int m = lane; m < B.nvert; m += 32) {
+    const double dd = (B.vx[m] - xC) * (B.vx[m] - xC) + (B.vy[m] - yC) * (B.vy[m] - yC) +
+                      (B.vz[m] - zC) * (B.vz[m] - zC);
+    if (vmin == 0x7fffffff || dd < dmin) { dmin = dd; vmin = m; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double od = __shfl_down_sync(0xffffffffu, dmin, o);
+    const int ov = __shfl_down_sync(0xffffffffu, vmin, o);
+    const bool take = (ov != 0x7fffffff) &&
+                      (vmin == 0x7fffffff || od < dmin || (od == dmin && ov < vmin));
+    if (take) { dmin = od; vmin = ov; }
+  }
+  vmin = __shfl_sync(0xffffffffu, vmin, 0);
+  const int t0 = B.v2t_off[vmin], t1 = B.v2t_off[vmin + 1];
+  double bestd = 1.0e16, bx = 0, by = 0, bz = 0, bnx = 0, bny = 0, bnz = 0;
+  int bel = -1;
+  int lw = 0;
+  for (int q0 = t0; q0 < t1; q0 += 32) {
+    const int q = q0 + lane;
+    double dist = 1.0e300, xt = 0, yt = 0, zt = 0, tnx = 0, tny = 0, tnz = 0;
+    int e = -1;
+    if (q < t1) {
+      e = B.v2t[q];
+      const int n1 = B.tri[3 * e], n2 = B.tri[3 * e + 1], n3 = B.tri[3 * e + 2];
+      double xv[3] = {B.vx[n1], B.vx[n2], B.vx[n3]};
+      double yv[3] = {B.vy[n1], B.vy[n2], B.vy[n3]};
+      double zv[3] = {B.vz[n1], B.vz[n2], B.vz[n3]};
+      const double xn = B.enx[e], yn = B.eny[e], zn = B.enz[e];
+      double xvn[3] = {B.vnx[n1], B.vnx[n2], B.vnx[n3]};
+      double yvn[3] = {B.vny[n1], B.vny[n2], B.vny[n3]};
+      double zvn[3] = {B.vnz[n1], B.vnz[n2], B.vnz[n3]};
+      const double planeConst = -xn * xv[0] - yn * yv[0] - zn * zv[0];
+      const double dtp = -(xn * xC + yn * yC + zn * zC + planeConst);
+      xt = xC + xn * dtp; yt = yC + yn * dtp; zt = zC + zn * dtp;
+      double a123, adiff;
+      bi_inside(xv, yv, zv, xt, yt, zt, &a123, &adiff);
+      dist = sqrt((xC - xt) * (xC - xt) + (yC - yt) * (yC - yt) + (zC - zt) * (zC - zt));
+      if (fabs(adiff) < 1.0e-6 * a123) {
+        tnx = xn; tny = yn; tnz = zn;
+      } else {
+        bi_outside(xv, yv, zv, xC, yC, zC, xvn, yvn, zvn, &xt, &yt, &zt, &dist, &tnx, &tny, &tnz, &lw);
+      }
+    }
+    // minimum distance over the batch, then the last position holding it
+    double md = dist;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) md = fmin(md, __shfl_xor_sync(0xffffffffu, md, o));
+    const unsigned hit = __ballot_sync(0xffffffffu, q < t1 && dist == md);
+    if (hit && md <= bestd) {
+      const int src = 31 - __clz(hit);
+      bestd = md;
+      bel = __shfl_sync(0xffffffffu, e, src);
+      bx = __shfl_sync(0xffffffffu, xt, src); by = __shfl_sync(0xffffffffu, yt, src);
+      bz = __shfl_sync(0xffffffffu, zt, src);
+      bnx = __shfl_sync(0xffffffffu, tnx, src); bny = __shfl_sync(0xffffffffu, tny, src);
+      bnz = __shfl_sync(0xffffffffu, tnz, src);
+    }
+  }
+  // the side-selection fallback count of the lanes
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lw += __shfl_down_sync(0xffffffffu, lw, o);
+  if (lane == 0 && warn) *warn += lw;
+  BIResult r;
+  r.x = bx; r.y = by; r.z = bz; r.elem = bel;
+  r.dist = sqrt((bx - xC) * (bx - xC) + (by - yC) * (by - yC) + (bz - zC) * (bz - zC));
+  r.dot = (xC - bx) * bnx + (yC - by) * bny + (zC - bz) * bnz;
+  return r;
+}
+
+// ------------------------------------------------------------- band
+// :153-396.  One thread per triangle: index box of the vertices (last
+// bracketing index on each side, as the sequential scans), then marks it.
+__global__ void k_band(Grid g, Body B, int8_t *band) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= B.ntri) return;
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int v1 = B.tri[3 * m], v2 = B.tri[3 * m + 1], v3 = B.tri[3 * m + 2];
+  const double xv[3] = {B.vx[v1], B.vx[v2], B.vx[v3]};
+  const double yv[3] = {B.vy[v1], B.vy[v2], B.vy[v3]};
+  const double zv[3] = {B.vz[v1], B.vz[v2], B.vz[v3]};
+  const int Nm = (B.type == 2) ? 3 : 0;
+  const double mtN = B.mt * (double)Nm;
+  if ((xv[0] <= g.x[1] && xv[1] <= g.x[1] && xv[2] <= g.x[1]) ||
+      (xv[0] >= g.x[nx] && xv[1] >= g.x[nx] && xv[2] >= g.x[nx]) ||
+      (yv[0] + mtN <= g.y[1] && yv[1] + mtN <= g.y[1] && yv[2] + mtN <= g.y[1]) ||
+      (yv[0] - mtN >= g.y[ny] && yv[1] - mtN >= g.y[ny] && yv[2] - mtN >= g.y[ny]) ||
+      (zv[0] + mtN <= g.z[1] && zv[1] + mtN <= g.z[1] && zv[2] + mtN <= g.z[1]) ||
+      (zv[0] - mtN >= g.z[nz] && zv[1] - mtN >= g.z[nz] && zv[2] - mtN >= g.z[nz]))
+    return;
+  double xmn = xv[0], xmx = xv[0], ymn = yv[0], ymx = yv[0], zmn = zv[0], zmx = zv[0];
+  for (int q = 1; q < 3; ++q) {
+    if (xv[q] < xmn) xmn = xv[q];
+    if (xv[q] > xmx) xmx = xv[q];
+    if (yv[q] < ymn) ymn = yv[q];
+    if (yv[q] > ymx) ymx = yv[q];
+    if (zv[q] < zmn) zmn = zv[q];
+    if (zv[q] > zmx) zmx = zv[q];
+  }
+  if (B.type == 2) {
+    xmn = xmn - mtN; xmx = xmx + mtN; ymn = ymn - mtN; ymx = ymx + mtN;
+    zmn = zmn - mtN; zmx = zmx + mtN;
+  }
+  int iMin = 0, iMax = 0, jMin = 0, jMax = 0, kMin = 0, kMax = 0;
+  for (int i = 0; i <= nx - 1; ++i) {
+    if ((g.xc[i] - xmn) * (g.xc[i + 1] - xmn) <= 0.0) iMin = i;
+    if ((g.xc[i] - xmx) * (g.xc[i + 1] - xmx) <= 0.0) iMax = i + 1;
+  }
+  if (iMin == 0) iMin = 1;
+  if (iMax == 0 || iMax == nx) iMax = nx - 1;
+  for (int j = 0; j <= ny - 1; ++j) {
+    if ((g.yc[j] - ymn) * (g.yc[j + 1] - ymn) <= 0.0) jMin = j;
+    if ((g.yc[j] - ymx) * (g.yc[j + 1] - ymx) <= 0.0) jMax = j + 1;
+  }
+  if (jMin == 0) jMin = 1;
+  if (jMax == 0 || jMax == ny) jMax = ny - 1;
+  for (int k = 0; k <= nz - 1; ++k) {
+    if ((g.zc[k] - zmn) * (g.zc[k + 1] - zmn) <= 0.0) kMin = k;
+    if ((g.zc[k] - zmx) * (g.zc[k + 1] - zmx) <= 0.0) kMax = k + 1;
+  }
+  if (kMin == 0) kMin = 1;
+  if (kMax == 0 || kMax == nz) kMax = nz - 1;
+  for (int k = kMin; k <= kMax; ++k)
+    for (int j = jMin; j <= jMax; ++j)
+      for (int i = iMin; i <= iMax; ++i) band[ridx(g, i, j, k)] = 1;
+}
+
+// :417-474 dot-normal (or membrane distance) classification of band cells,
+// one warp per band cell; bodies are tested from the last to the first
+struct Bodies {
+  int n;
+  Body b[8];
+};
+
+__global__ void k_classify(Grid g, Bodies BB, const int *cells, int ncells, int8_t *ibt,
+                           int8_t *body, int *warn) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= ncells) return;
+  const long long id = cells[w];
+  const int i = (int)(id % g.NX), j = (int)((id / g.NX) % g.NY), k = (int)(id / (g.NX * g.NY));
+  const double xP = g.xc[i], yP = g.yc[j], zP = g.zc[k];
+  int hit = 0;
+  int lw = 0;
+  for (int ib = BB.n - 1; ib >= 0; --ib) {
+    const BIResult r = body_intercept_warp(BB.b[ib], xP, yP, zP, lane, &lw);
+    if (BB.b[ib].type == 2) {
+      const double de = sqrt((xP - r.x) * (xP - r.x) + (yP - r.y) * (yP - r.y) + (zP - r.z) * (zP - r.z));
+      if (de < BB.b[ib].mt / 2.0) { hit = ib + 1; break; }
+    } else {
+      if (r.dot >= 0.0) { hit = ib + 1; break; }
+    }
+  }
+  if (lane == 0) {
+    ibt[id] = hit ? 1 : 0;
+    if (hit) body[id] = (int8_t)hit;
+    if (lw) atomicAdd(warn, lw);
+  }
+}
+
+// :509-536 i-direction fill, one thread per (j,k) line; :725-730 outflow copy
+__global__ void k_fill(Grid g, const int8_t *band, int8_t *ibt, int8_t *body) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nyl = g.ny - 1;
+  if (t >= nyl * (g.nz - 1)) return;
+  const int j = 1 + t % nyl, k = 1 + t / nyl;
+  const long long r0 = ridx(g, 0, j, k);
+  for (int ii = 1; ii <= g.nx - 1; ++ii)
+    if (band[r0 + ii]) { ibt[r0] = ibt[r0 + ii]; body[r0] = body[r0 + ii]; break; }
+  for (int i = 1; i <= g.nx - 1; ++i) {
+    if (band[r0 + i]) continue;
+    ibt[r0 + i] = ibt[r0 + i - 1];
+    if (ibt[r0 + i] == 1) body[r0 + i] = body[r0 + i - 1];
+  }
+  ibt[r0 + g.nx] = ibt[r0 + g.nx - 1];
+  body[r0 + g.nx] = body[r0 + g.nx - 1];
+}
+
+// :763-787 commit over i = 0..nx of the interior (j,k)
+__global__ void k_commit(Grid g, const int8_t *ibt, int8_t *ib) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)(g.nx + 1) * (g.ny - 1) * (g.nz - 1);
+  if (e >= n) return;
+  const int i = (int)(e % (g.nx + 1));
+  const int j = 1 + (int)((e / (g.nx + 1)) % (g.ny - 1));
+  const int k = 1 + (int)(e / ((long long)(g.nx + 1) * (g.ny - 1)));
+  const long long id = ridx(g, i, j, k);
+  ib[id] = ibt[id];
+}
+
+// ------------------------------------------------------- smoothing
+// In-place passes of GCM_SET_BOUNDARY.F90:132-223 and :1639-1692 give every
+// cell the count over its "backward" neighbours (already visited in the
+// loop order) in their UPDATED state and over the forward ones in their
+// state at the start of the pass.  Flags only go 0 -> 1, so iterating
+//   X(c) = old(c) OR [count(X over backward) + count(old over forward) >= thr]
+// from X = old reaches the sequential result in at most (longest chain)
+// steps; each step is a Jacobi update from cur to nxt.
+// mode 0: 3-D pass (k,j,i order, 6 faces, >= 5); mode 1: x planes (j,k
+// order within an i plane, >= 3); mode 2: y planes (i,k order, >= 3).
+__global__ void k_smooth_step(Grid g, int mode, const int8_t *old, const int8_t *cur, int8_t *nxt,
+                              const int8_t *bold, const int8_t *bcur, int8_t *bnxt, int *changed) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)(g.nx - 1) * (g.ny - 1) * (g.nz - 1);
+  if (e >= n) return;
+  const int i = 1 + (int)(e % (g.nx - 1));
+  const int j = 1 + (int)((e / (g.nx - 1)) % (g.ny - 1));
+  const int k = 1 + (int)(e / ((long long)(g.nx - 1) * (g.ny - 1)));
+  const long long id = ridx(g, i, j, k);
+  if (old[id] == 1) { nxt[id] = 1; bnxt[id] = bcur[id]; return; }
+  const long long sx = 1, sy = g.NX, sz = g.NX * g.NY;
+  // neighbour offsets in the reference enumeration order, and which are
+  // backward in the loop order
+  long long off[6];
+  bool back[6];
+  int nn, thr;
+  if (mode == 0) {
+    off[0] = -sz; off[1] = -sy; off[2] = -sx; off[3] = sx; off[4] = sy; off[5] = sz;
+    back[0] = back[1] = back[2] = true; back[3] = back[4] = back[5] = false;
+    nn = 6; thr = 5;
+  } else if (mode == 1) {
+    off[0] = -sz; off[1] = -sy; off[2] = sy; off[3] = sz;
+    back[0] = true; back[1] = true; back[2] = false; back[3] = false;
+    nn = 4; thr = 3;
+  } else {
+    off[0] = -sz; off[1] = -sx; off[2] = sx; off[3] = sz;
+    back[0] = true; back[1] = true; back[2] = false; back[3] = false;
+    nn = 4; thr = 3;
+  }
+  int s = 0, ibody = 0;
+  for (int q = 0; q < nn; ++q) {
+    const long long nb = id + off[q];
+    const int8_t v = back[q] ? cur[nb] : old[nb];
+    const int8_t bv = back[q] ? bcur[nb] : bold[nb];
+    if (v == 1) {
+      s++;
+      if (bv > 0) ibody = bv;
+    }
+  }
+  int8_t nv = 0, nb = bcur[id];
+  if (s >= thr) { nv = 1; nb = (int8_t)(ibody > 0 ? ibody : 1); }
+  nxt[id] = nv;
+  bnxt[id] = nb;
+  if (nv != cur[id]) atomicOr(changed, 1);
+}
+
+// ---------------------------------------------------------- ghosts
+// GCM_SET_BOUNDARY.F90:800-876: fluid interior cells face-adjacent to an
+// iblank cell; their body is that of the first such iblank cell in (k,j,i)
+// order among the cells the reference loop visits (i in [1,nx-1]).
+__global__ void k_ghost_mark(Grid g, const int8_t *ib, int8_t *ghost, int8_t *body) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)(g.nx - 1) * (g.ny - 1) * (g.nz - 1);
+  if (e >= n) return;
+  const int i = 1 + (int)(e % (g.nx - 1));
+  const int j = 1 + (int)((e / (g.nx - 1)) % (g.ny - 1));
+  const int k = 1 + (int)(e / ((long long)(g.nx - 1) * (g.ny - 1)));
+  const long long id = ridx(g, i, j, k);
+  if (ib[id] != 0) { ghost[id] = 0; return; }
+  const long long sy = g.NX, sz = g.NX * g.NY;
+  // ascending linear index: -z, -y, -x, +x, +y, +z
+  const long long off[6] = {-sz, -sy, -1, 1, sy, sz};
+  const int ii[6] = {i, i, i - 1, i + 1, i, i};
+  int8_t gb = 0, is_g = 0;
+  for (int q = 0; q < 6; ++q) {
+    if (ii[q] < 1 || ii[q] > g.nx - 1) continue;
+    const long long nb = id + off[q];
+    if (ib[nb] == 1) { is_g = 1; gb = body[nb]; break; }
+  }
+  ghost[id] = is_g;
+  if (is_g) body[id] = gb;  // each ghost reads only iblank cells' bodies
+}
+
+// GCM_SET_BOUNDARY.F90:946-964: iblank face neighbours of ghost cells
+__global__ void k_dead_mark(Grid g, const int8_t *ib, const int8_t *ghost, int8_t *dead) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)(g.nx + 2) * (g.ny + 2) * (g.nz + 2);
+  if (e >= n) return;
+  const int i = (int)(e % g.NX);
+  const int j = (int)((e / g.NX) % g.NY);
+  const int k = (int)(e / (g.NX * g.NY));
+  if (ib[e] != 1) { dead[e] = 0; return; }
+  const long long sy = g.NX, sz = g.NX * g.NY;
+  const int ci[6] = {i - 1, i + 1, i, i, i, i};
+  const int cj[6] = {j, j, j - 1, j + 1, j, j};
+  const int ck[6] = {k, k, k, k, k - 1, k + 1};
+  const long long off[6] = {-1, 1, -sy, sy, -sz, sz};
+  int8_t d = 0;
+  for (int q = 0; q < 6; ++q) {
+    if (ci[q] < 1 || ci[q] > g.nx - 1 || cj[q] < 1 || cj[q] > g.ny - 1 || ck[q] < 1 || ck[q] > g.nz - 1)
+      continue;
+    if (ghost[e + off[q]] == 1) { d = -1; break; }
+  }
+  dead[e] = d;
+}
+
+// -------------------------------------------------- image points
+__device__ __forceinline__ int nint_d(double v) {
+  return (int)(v >= 0.0 ? floor(v + 0.5) : -floor(-v + 0.5));
+}
+
+// GCM_SET_BOUNDARY.F90:607-797 (inverse: LAPACK getrf/getri semantics as in
+// the restatement)
+__device__ int invert8(double *a, double *inv) {
+  int ipiv[8];
+  int info = 0;
+#define A(i, j) a[(i) + 8 * (j)]
+  for (int j = 0; j < 8; ++j) {
+    int p = j;
+    double mx = fabs(A(j, j));
+    for (int i = j + 1; i < 8; ++i)
+      if (fabs(A(i, j)) > mx) { mx = fabs(A(i, j)); p = i; }
+    ipiv[j] = p;
+    if (A(p, j) == 0.0) { if (info == 0) info = j + 1; continue; }
+    if (p != j)
+      for (int q = 0; q < 8; ++q) { double t = A(j, q); A(j, q) = A(p, q); A(p, q) = t; }
+    double r = 1.0 / A(j, j);
+    for (int i = j + 1; i < 8; ++i) A(i, j) = A(i, j) * r;
+    for (int q = j + 1; q < 8; ++q)
+      for (int i = j + 1; i < 8; ++i) A(i, q) = A(i, q) - A(i, j) * A(j, q);
+  }
+  if (info) return info;
+  for (int j = 0; j < 8; ++j) {
+    A(j, j) = 1.0 / A(j, j);
+    double ajj = -A(j, j);
+    for (int i = 0; i < j; ++i) {
+      double s = 0.0;
+      for (int q = i; q < j; ++q) s = s + A(i, q) * A(q, j);
+      inv[i] = s;
+    }
+    for (int i = 0; i < j; ++i) A(i, j) = inv[i] * ajj;
+  }
+  double work[8];
+  for (int j = 7; j >= 0; --j) {
+    for (int i = j + 1; i < 8; ++i) { work[i] = A(i, j); A(i, j) = 0.0; }
+    for (int q = j + 1; q < 8; ++q)
+      for (int i = 0; i < 8; ++i) A(i, j) = A(i, j) - A(i, q) * work[q];
+  }
+  for (int j = 6; j >= 0; --j) {
+    int jp = ipiv[j];
+    if (jp != j)
+      for (int i = 0; i < 8; ++i) { double t = A(i, j); A(i, j) = A(i, jp); A(i, jp) = t; }
+  }
+#undef A
+  for (int q = 0; q < 64; ++q) inv[q] = a[q];
+  return 0;
+}
+
+__constant__ int c_incI[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+__constant__ int c_incJ[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+__constant__ int c_incK[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+
+__device__ void van_matrix(const Grid &g, int iG, int jG, int kG, int ic, int jc, int kc, double xIP,
+                           double yIP, double zIP, double xBI, double yBI, double zBI, double xN,
+                           double yN, double zN, double *cD, double *cN) {
+  double vD[64], vN[64], iD[64], iN[64];
+  for (int r = 0; r < 8; ++r) {
+    int i = ic + c_incI[r], j = jc + c_incJ[r], k = kc + c_incK[r];
+    double x1 = g.xc[i], x2 = g.yc[j], x3 = g.zc[k];
+    double rowD[8] = {x1 * x2 * x3, x1 * x2, x1 * x3, x2 * x3, x1, x2, x3, 1.0};
+    double rowN[8];
+    for (int q = 0; q < 8; ++q) rowN[q] = rowD[q];
+    if (i == iG && j == jG && k == kG) {
+      x1 = xBI; x2 = yBI; x3 = zBI;
+      rowD[0] = x1 * x2 * x3; rowD[1] = x1 * x2; rowD[2] = x1 * x3; rowD[3] = x2 * x3;
+      rowD[4] = x1; rowD[5] = x2; rowD[6] = x3; rowD[7] = 1.0;
+      rowN[0] = xN * x2 * x3 + yN * x1 * x3 + zN * x1 * x2;
+      rowN[1] = xN * x2 + yN * x1;
+      rowN[2] = xN * x3 + zN * x1;
+      rowN[3] = yN * x3 + zN * x2;
+      rowN[4] = xN; rowN[5] = yN; rowN[6] = zN; rowN[7] = 0.0;
+    }
+    for (int q = 0; q < 8; ++q) { vD[r + 8 * q] = rowD[q]; vN[r + 8 * q] = rowN[q]; }
+  }
+  invert8(vD, iD);
+  invert8(vN, iN);
+  for (int r = 0; r < 8; ++r) {
+    cD[r] = iD[0 + 8 * r] * xIP * yIP * zIP + iD[1 + 8 * r] * xIP * yIP + iD[2 + 8 * r] * xIP * zIP +
+            iD[3 + 8 * r] * yIP * zIP + iD[4 + 8 * r] * xIP + iD[5 + 8 * r] * yIP +
+            iD[6 + 8 * r] * zIP + iD[7 + 8 * r];
+    cN[r] = iN[0 + 8 * r] * xIP * yIP * zIP + iN[1 + 8 * r] * xIP * yIP + iN[2 + 8 * r] * xIP * zIP +
+            iN[3 + 8 * r] * yIP * zIP + iN[4 + 8 * r] * xIP + iN[5 + 8 * r] * yIP +
+            iN[6 + 8 * r] * zIP + iN[7 + 8 * r];
+  }
+}
+
+// Per ghost cell (warp): body intercept, image point, host cell
+// (GCM_SET_BOUNDARY.F90:321-475).  Writes bi, ip, probe, cell, closest, the
+// intercept normal and ds.
+struct RowOut {
+  double *bi;  // body intercept (before the membrane shift)
+  double *bw;  // intercept the interpolation weights use
+  double *ip, *probe, *nrm, *ds;
+  int *cell, *closest;
+};
+
+__global__ void k_ghost_geom(Grid g, Bodies BB, const int *list, int n, const int8_t *body,
+                             double pln, RowOut out, int *warn) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const long long id = list[w];
+  const int iG = (int)(id % g.NX), jG = (int)((id / g.NX) % g.NY), kG = (int)(id / (g.NX * g.NY));
+  int ib = body[id] - 1;
+  if (ib < 0) ib = 0;
+  if (ib >= BB.n) ib = BB.n - 1;
+  const double xGC = g.xc[iG], yGC = g.yc[jG], zGC = g.zc[kG];
+  int lw = 0;
+  BIResult r = body_intercept_warp(BB.b[ib], xGC, yGC, zGC, lane, &lw);
+  if (lane != 0) return;
+  if (lw) atomicAdd(warn, lw);
+  double xBI = r.x, yBI = r.y, zBI = r.z;
+  if (BB.b[ib].dim == 2) zBI = zGC;
+  out.closest[w] = r.elem;
+  out.bi[3 * w] = xBI; out.bi[3 * w + 1] = yBI; out.bi[3 * w + 2] = zBI;
+  double ds = sqrt((xGC - xBI) * (xGC - xBI) + (yGC - yBI) * (yGC - yBI) + (zGC - zBI) * (zGC - zBI));
+  const double sx = (xGC - xBI) / ds, sy = (yGC - yBI) / ds, sz = (zGC - zBI) / ds;
+  if (BB.b[ib].type == 2) {
+    const double mt = BB.b[ib].mt;
+    xBI = xBI + mt / 2.0 * sx; yBI = yBI + mt / 2.0 * sy; zBI = zBI + mt / 2.0 * sz;
+    ds = sqrt((xGC - xBI) * (xGC - xBI) + (yGC - yBI) * (yGC - yBI) + (zGC - zBI) * (zGC - zBI));
+  }
+  out.nrm[3 * w] = -sx; out.nrm[3 * w + 1] = -sy; out.nrm[3 * w + 2] = -sz;
+  out.ds[w] = ds;
+  out.probe[w] = ds * pln;
+  const double xIP = xBI - (xBI - xGC) * pln;
+  const double yIP = yBI - (yBI - yGC) * pln;
+  const double zIP = zBI - (zBI - zGC) * pln;
+  out.ip[3 * w] = xIP; out.ip[3 * w + 1] = yIP; out.ip[3 * w + 2] = zIP;
+  out.bw[3 * w] = xBI; out.bw[3 * w + 1] = yBI; out.bw[3 * w + 2] = zBI;
+  double maxDelta = g.dx[iG];
+  if (g.dy[jG] > maxDelta) maxDelta = g.dy[jG];
+  if (g.dz[kG] > maxDelta) maxDelta = g.dz[kG];
+  const int iR = 2 * nint_d(maxDelta / g.dx[iG] + 0.5);
+  const int jR = 2 * nint_d(maxDelta / g.dy[jG] + 0.5);
+  const int kR = 2 * nint_d(maxDelta / g.dz[kG] + 0.5);
+  int ic = -1, jc = -1, kc = -1;
+  int lo = iG - iR, hi = iG + iR;
+  if (lo < 0) lo = 0;
+  if (hi > g.nx) hi = g.nx;
+  for (int i = lo; i <= hi; ++i)
+    if (g.xc[i] <= xIP && g.xc[i + 1] > xIP) ic = i;
+  lo = jG - jR; hi = jG + jR;
+  if (lo < 0) lo = 0;
+  if (hi > g.ny) hi = g.ny;
+  for (int j = lo; j <= hi; ++j)
+    if (g.yc[j] <= yIP && g.yc[j + 1] > yIP) jc = j;
+  lo = kG - kR; hi = kG + kR;
+  if (lo < 0) lo = 0;
+  if (hi > g.nz) hi = g.nz;
+  for (int k = lo; k <= hi; ++k)
+    if (g.zc[k] <= zIP && g.zc[k + 1] > zIP) kc = k;
+  out.cell[3 * w] = ic; out.cell[3 * w + 1] = jc; out.cell[3 * w + 2] = kc;
+}
+
+// Per dead cell (warp): GCM_SET_BOUNDARY.F90:1053-1409 up to the host cell
+__global__ void k_dead_geom(Grid g, Bodies BB, const int *list, int n, const int8_t *body,
+                            double plnD, RowOut out, int *warn, int *nobody) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const long long id = list[w];
+  const int iG = (int)(id % g.NX), jG = (int)((id / g.NX) % g.NY), kG = (int)(id / (g.NX * g.NY));
+  const int ib = body[id] - 1;
+  if (ib < 0 || ib >= BB.n) {
+    if (lane == 0) {
+      atomicAdd(nobody, 1);
+      out.cell[3 * w] = -1; out.cell[3 * w + 1] = -1; out.cell[3 * w + 2] = -1;
+      out.ds[w] = -1.0;  // contributes nothing to alphaGhost
+    }
+    return;
+  }
+  const double xDC = g.xc[iG], yDC = g.yc[jG], zDC = g.zc[kG];
+  int lw = 0;
+  BIResult r = body_intercept_warp(BB.b[ib], xDC, yDC, zDC, lane, &lw);
+  if (lane != 0) return;
+  if (lw) atomicAdd(warn, lw);
+  double xBI = r.x, yBI = r.y, zBI = r.z;
+  if (BB.b[ib].dim == 2) zBI = zDC;
+  out.closest[w] = r.elem;
+  out.bi[3 * w] = xBI; out.bi[3 * w + 1] = yBI; out.bi[3 * w + 2] = zBI;
+  double ds = sqrt((xDC - xBI) * (xDC - xBI) + (yDC - yBI) * (yDC - yBI) + (zDC - zBI) * (zDC - zBI));
+  double sx = (xBI - xDC) / ds, sy = (yBI - yDC) / ds, sz = (zBI - zDC) / ds;
+  const double bnx = -sx, bny = -sy, bnz = -sz;
+  if (BB.b[ib].type == 2) {
+    const double mt = BB.b[ib].mt;
+    sx = -sx; sy = -sy; sz = -sz;
+    if (ds >= mt / 2.0) {
+      const double s = ds + (double)0.1f * (ds - mt / 2.0);
+      xBI = xBI + s * sx; yBI = yBI + s * sy; zBI = zBI + s * sz;
+    } else {
+      xBI = xBI + mt / 2.0 * sx; yBI = yBI + mt / 2.0 * sy; zBI = zBI + mt / 2.0 * sz;
+    }
+    double zIP = zDC + (zBI - zDC) * plnD;
+    double yIP = yDC + (yBI - yDC) * plnD;
+    int guard = 0;
+    while ((yIP < g.yc[0] || yIP > g.yc[g.ny + 1]) && guard++ < 200) {
+      const double d1 = sqrt((xDC - xBI) * (xDC - xBI) + (yDC - yBI) * (yDC - yBI) + (zDC - zBI) * (zDC - zBI));
+      const double t = -0.5 * d1;
+      xBI = xBI + t * sx; yBI = yBI + t * sy; zBI = zBI + t * sz;
+      yIP = yDC + (yBI - yDC) * plnD;
+    }
+    guard = 0;
+    while ((zIP < g.zc[0] || zIP > g.zc[g.nz + 1]) && guard++ < 200) {
+      const double d1 = sqrt((xDC - xBI) * (xDC - xBI) + (yDC - yBI) * (yDC - yBI) + (zDC - zBI) * (zDC - zBI));
+      const double t = -0.5 * d1;
+      xBI = xBI + t * sx; yBI = yBI + t * sy; zBI = zBI + t * sz;
+      zIP = zDC + (zBI - zDC) * plnD;
+    }
+    ds = sqrt((xDC - xBI) * (xDC - xBI) + (yDC - yBI) * (yDC - yBI) + (zDC - zBI) * (zDC - zBI));
+  }
+  out.ds[w] = ds;
+  out.nrm[3 * w] = bnx; out.nrm[3 * w + 1] = bny; out.nrm[3 * w + 2] = bnz;
+  double xIP = xDC + (xBI - xDC) * plnD;
+  double yIP = yDC + (yBI - yDC) * plnD;
+  double zIP = zDC + (zBI - zDC) * plnD;
+  double probe = ds * plnD;
+  if (yIP < g.yc[0] || yIP > g.yc[g.ny + 1]) {
+    yIP = (fabs(yIP - g.yc[0]) < fabs(yIP - g.yc[g.ny + 1])) ? g.yc[0] : g.yc[g.ny + 1];
+    probe = sqrt((xDC - xIP) * (xDC - xIP) + (yDC - yIP) * (yDC - yIP) + (zDC - zIP) * (zDC - zIP));
+  }
+  if (zIP < g.zc[0] || zIP > g.zc[g.nz + 1]) {
+    zIP = (fabs(zIP - g.zc[0]) < fabs(zIP - g.zc[g.nz + 1])) ? g.zc[0] : g.zc[g.nz + 1];
+    probe = sqrt((xDC - xIP) * (xDC - xIP) + (yDC - yIP) * (yDC - yIP) + (zDC - zIP) * (zDC - zIP));
+  }
+  out.probe[w] = probe;
+  out.ip[3 * w] = xIP; out.ip[3 * w + 1] = yIP; out.ip[3 * w + 2] = zIP;
+  out.bw[3 * w] = xBI; out.bw[3 * w + 1] = yBI; out.bw[3 * w + 2] = zBI;
+  double maxDelta = g.dx[iG];
+  if (g.dy[jG] > maxDelta) maxDelta = g.dy[jG];
+  if (g.dz[kG] > maxDelta) maxDelta = g.dz[kG];
+  const int iR = 2 * nint_d(maxDelta / g.dx[iG] + 0.5);
+  const int jR = 2 * nint_d(maxDelta / g.dy[jG] + 0.5);
+  const int kR = 2 * nint_d(maxDelta / g.dz[kG] + 0.5);
+  int ic = -1, jc = -1, kc = -1;
+  int lo = iG - iR, hi = iG + iR;
+  if (lo < 0) lo = 0;
+  if (hi > g.nx) hi = g.nx;
+  for (int i = lo; i <= hi; ++i)
+    if (g.xc[i] <= xIP && g.xc[i + 1] >= xIP) ic = i;
+  lo = jG - jR; hi = jG + jR;
+  if (lo < 0) lo = 0;
+  if (hi > g.ny) hi = g.ny;
+  for (int j = lo; j <= hi; ++j)
+    if (g.yc[j] <= yIP && g.yc[j + 1] >= yIP) jc = j;
+  lo = kG - kR; hi = kG + kR;
+  if (lo < 0) lo = 0;
+  if (hi > g.nz) hi = g.nz;
+  for (int k = lo; k <= hi; ++k)
+    if (g.zc[k] <= zIP && g.zc[k + 1] >= zIP) kc = k;
+  out.cell[3 * w] = ic; out.cell[3 * w + 1] = jc; out.cell[3 * w + 2] = kc;
+}
+
+// weights of one row (thread per row): ghost rows evaluate the interpolant
+// at the ghost cell centre (GCM_SET_BOUNDARY.F90:521-523), dead rows at the
+// image point (:1451-1453)
+__global__ void k_weights(Grid g, const int *list, int n, RowOut out, int at_image, double *cD,
+                          double *cN, int *hostfail) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n) return;
+  const int ic = out.cell[3 * w], jc = out.cell[3 * w + 1], kc = out.cell[3 * w + 2];
+  if (ic < 0 || jc < 0 || kc < 0) {
+    atomicAdd(hostfail, 1);
+    for (int q = 0; q < 8; ++q) { cD[8 * w + q] = 0.0; cN[8 * w + q] = 0.0; }
+    return;
+  }
+  const long long id = list[w];
+  const int iG = (int)(id % g.NX), jG = (int)((id / g.NX) % g.NY), kG = (int)(id / (g.NX * g.NY));
+  double X, Y, Z;
+  if (at_image) { X = out.ip[3 * w]; Y = out.ip[3 * w + 1]; Z = out.ip[3 * w + 2]; }
+  else { X = g.xc[iG]; Y = g.yc[jG]; Z = g.zc[kG]; }
+  van_matrix(g, iG, jG, kG, ic, jc, kc, X, Y, Z, out.bw[3 * w], out.bw[3 * w + 1], out.bw[3 * w + 2],
+             out.nrm[3 * w], out.nrm[3 * w + 1], out.nrm[3 * w + 2], cD + 8 * w, cN + 8 * w);
+}
+
+// alphaGhost (GCM_SET_BOUNDARY.F90:1218-1277, 1477-1489): per ghost, the sum
+// over its face-adjacent dead cells, in dead-list (k,j,i) order, of
+// (ds / dxc)^2, then 1 - sqrt(sum)
+__global__ void k_alpha(Grid g, const int *glist, int ng, const int8_t *dead, const int *dead_rank,
+                        const double *dead_ds, double *alpha) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= ng) return;
+  const long long id = glist[w];
+  const int i = (int)(id % g.NX), j = (int)((id / g.NX) % g.NY), k = (int)(id / (g.NX * g.NY));
+  const long long sy = g.NX, sz = g.NX * g.NY;
+  // dead neighbours in ascending linear index: -z, -y, -x, +x, +y, +z; the
+  // ghost is the dead cell's (+z, +y, +x, -x, -y, -z) neighbour and the
+  // reference divides by dzc(k_dead+1)=dzc(k), dyc(j), dxc(i), dxc(i+1)...
+  const long long off[6] = {-sz, -sy, -1, 1, sy, sz};
+  const double h[6] = {g.dzc[k], g.dyc[j], g.dxc[i], g.dxc[i + 1], g.dyc[j + 1], g.dzc[k + 1]};
+  const int ci[6] = {i, i, i - 1, i + 1, i, i};
+  double s = 0.0;
+  for (int q = 0; q < 6; ++q) {
+    if (ci[q] < 1 || ci[q] > g.nx - 1) continue;
+    const long long nb = id + off[q];
+    if (dead[nb] != -1) continue;
+    const int rk = dead_rank[nb];
+    if (rk < 0 || dead_ds[rk] < 0.0) continue;
+    const double t = dead_ds[rk] / h[q];
+    s = s + t * t;
+  }
+  alpha[w] = 1.0 - sqrt(s);
+}
+
+__global__ void k_rank(const int *list, int n, int *rank) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < n) rank[list[w]] = w;
+}
+
+struct IsFlag {
+  const int8_t *f;
+  int8_t want;
+  __host__ __device__ bool operator()(const int &i) const { return f[i] == want; }
+};
+
+// dead cells that get a row: i in [1, nx-1], j in [0, ny], k in [0, nz]
+// (GCM_SET_BOUNDARY.F90:1036-1047)
+struct IsDeadRow {
+  const int8_t *f;
+  int NX, NY, nx, ny, nz;
+  __host__ __device__ bool operator()(const int &e) const {
+    if (f[e] != -1) return false;
+    const int i = e % NX, j = (e / NX) % NY, k = e / (NX * NY);
+    return i >= 1 && i <= nx - 1 && j <= ny && k <= nz;
+  }
+};
+
+}  // namespace geo
+
+// ---------------------------------------------------------------- host
+static fg_status geom_grid(fg_case *c, geo::Grid &g) {
+  Geom &G = *c->geom;
+  const int n3[3] = {c->nx, c->ny, c->nz};
+  if (!G.d_xc) {
+    std::vector<double> all;
+    const HLevel &L = c->lev[0];
+    const std::vector<double> *xs[3] = {&L.x, &L.y, &L.z};
+    const std::vector<double> *xcs[3] = {&L.xc, &L.yc, &L.zc};
+    for (int a = 0; a < 3; ++a) {
+      const int n = n3[a];
+      std::vector<double> dx(n + 2, 0.0), dxc(n + 2, 0.0);
+      for (int i = 0; i <= n; ++i) dx[i] = (*xs[a])[i + 1] - (*xs[a])[i];
+      for (int i = 1; i <= n; ++i) dxc[i] = (*xcs[a])[i] - (*xcs[a])[i - 1];
+      all.insert(all.end(), xs[a]->begin(), xs[a]->end());
+      all.insert(all.end(), xcs[a]->begin(), xcs[a]->end());
+      all.insert(all.end(), dx.begin(), dx.end());
+      all.insert(all.end(), dxc.begin(), dxc.end());
+    }
+    FG_CUDA(cudaMalloc(&G.d_xc, all.size() * sizeof(double)));
+    FG_CUDA(cudaMemcpy(G.d_xc, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const double *p = G.d_xc;
+  const double *ax[3][4];
+  for (int a = 0; a < 3; ++a)
+    for (int w = 0; w < 4; ++w) { ax[a][w] = p; p += n3[a] + 2; }
+  g.nx = c->nx; g.ny = c->ny; g.nz = c->nz;
+  g.NX = c->nx + 2; g.NY = c->ny + 2;
+  g.x = ax[0][0]; g.xc = ax[0][1]; g.dx = ax[0][2]; g.dxc = ax[0][3];
+  g.y = ax[1][0]; g.yc = ax[1][1]; g.dy = ax[1][2]; g.dyc = ax[1][3];
+  g.z = ax[2][0]; g.zc = ax[2][1]; g.dz = ax[2][2]; g.dzc = ax[2][3];
+  return FG_OK;
+}
+
+// BOUNDARY_SET_ARCLENGTH_NORM.F90:46-175 on the host (same operation order
+// as the restatement; host code is compiled without FMA contraction)
+static void host_normals(const DevBody &B, std::vector<double> &en, std::vector<double> &vn) {
+  const int nt = B.ntri, nv = B.nvert;
+  en.assign(3 * (size_t)nt, 0.0);
+  vn.assign(3 * (size_t)nv, 0.0);
+  const double *X = B.xyz.data();
+  double *vnx = vn.data(), *vny = vn.data() + nv, *vnz = vn.data() + 2 * nv;
+  double *enx = en.data(), *eny = en.data() + nt, *enz = en.data() + 2 * nt;
+  for (int m = 0; m < nt; ++m) {
+    const int n1 = B.tri[3 * m], n2 = B.tri[3 * m + 1], n3 = B.tri[3 * m + 2];
+    const double ax = X[3 * n2] - X[3 * n1], ay = X[3 * n2 + 1] - X[3 * n1 + 1], az = X[3 * n2 + 2] - X[3 * n1 + 2];
+    const double bx = X[3 * n3] - X[3 * n2], by = X[3 * n3 + 1] - X[3 * n2 + 1], bz = X[3 * n3 + 2] - X[3 * n2 + 2];
+    const double nxv = (ay * bz - az * by);
+    const double nyv = (az * bx - ax * bz);
+    const double nzv = (ax * by - ay * bx);
+    const double mag = sqrt(nxv * nxv + nyv * nyv + nzv * nzv);
+    enx[m] = nxv / mag; eny[m] = nyv / mag; enz[m] = nzv / mag;
+    vnx[n1] = vnx[n1] + enx[m]; vnx[n2] = vnx[n2] + enx[m]; vnx[n3] = vnx[n3] + enx[m];
+    vny[n1] = vny[n1] + eny[m]; vny[n2] = vny[n2] + eny[m]; vny[n3] = vny[n3] + eny[m];
+    vnz[n1] = vnz[n1] + enz[m]; vnz[n2] = vnz[n2] + enz[m]; vnz[n3] = vnz[n3] + enz[m];
+  }
+  for (int v = 0; v < nv; ++v) {
+    const double mag = sqrt(vnx[v] * vnx[v] + vny[v] * vny[v] + vnz[v] * vnz[v]);
+    vnx[v] = vnx[v] / mag; vny[v] = vny[v] / mag; vnz[v] = vnz[v] / mag;
+  }
+}
+
+static fg_status upload_body(DevBody &B) {
+  std::vector<double> en, vn;
+  host_normals(B, en, vn);
+  std::vector<double> soa(3 * (size_t)B.nvert);
+  for (int v = 0; v < B.nvert; ++v) {
+    soa[v] = B.xyz[3 * v]; soa[B.nvert + v] = B.xyz[3 * v + 1]; soa[2 * B.nvert + v] = B.xyz[3 * v + 2];
+  }
+  if (!B.d_xyz) {
+    FG_CUDA(cudaMalloc(&B.d_xyz, soa.size() * sizeof(double)));
+    FG_CUDA(cudaMalloc(&B.d_en, en.size() * sizeof(double)));
+    FG_CUDA(cudaMalloc(&B.d_vn, vn.size() * sizeof(double)));
+  }
+  FG_CUDA(cudaMemcpy(B.d_xyz, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice));
+  FG_CUDA(cudaMemcpy(B.d_en, en.data(), en.size() * sizeof(double), cudaMemcpyHostToDevice));
+  FG_CUDA(cudaMemcpy(B.d_vn, vn.data(), vn.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return FG_OK;
+}
+
+static geo::Body dev_body(const DevBody &B) {
+  geo::Body b;
+  b.nvert = B.nvert; b.ntri = B.ntri; b.type = B.type; b.dim = B.body_dim; b.mt = B.membrane_tkns;
+  b.vx = B.d_xyz; b.vy = B.d_xyz + B.nvert; b.vz = B.d_xyz + 2 * B.nvert;
+  b.enx = B.d_en; b.eny = B.d_en + B.ntri; b.enz = B.d_en + 2 * B.ntri;
+  b.vnx = B.d_vn; b.vny = B.d_vn + B.nvert; b.vnz = B.d_vn + 2 * B.nvert;
+  b.tri = B.d_tri; b.v2t_off = B.d_v2t_off; b.v2t = B.d_v2t;
+  return b;
+}
+
+static fg_status ensure_fields(fg_case *c) {
+  Geom &G = *c->geom;
+  const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  if (!G.d_iblank) {
+    FG_CUDA(cudaMalloc(&G.d_iblank, n));
+    FG_CUDA(cudaMalloc(&G.d_ghost, n));
+    FG_CUDA(cudaMalloc(&G.d_dead, n));
+    FG_CUDA(cudaMalloc(&G.d_body, n));
+    FG_CUDA(cudaMalloc(&G.d_band, n));
+    FG_CUDA(cudaMalloc(&G.d_tmp, 4 * n));  // iblankTemp, smoothing buffers
+    FG_CUDA(cudaMemset(G.d_iblank, 0, n));
+  }
+  return FG_OK;
+}
+
+// stream compaction of the cell indices satisfying pred, in linear (k,j,i)
+// order; *d_out is (re)allocated to the count
+template <typename Pred>
+static fg_status compact(Pred pred, size_t n, int **d_out, int *count, cudaStream_t s) {
+  int *d_n = nullptr, *tmpout = nullptr;
+  void *d_tmp = nullptr;
+  size_t tmp = 0;
+  thrust::counting_iterator<int> it(0);
+  FG_CUDA(cub::DeviceSelect::If(nullptr, tmp, it, tmpout, d_n, (int)n, pred, s));
+  FG_CUDA(cudaMalloc(&d_n, sizeof(int)));
+  FG_CUDA(cudaMalloc(&d_tmp, tmp));
+  FG_CUDA(cudaMalloc(&tmpout, n * sizeof(int)));
+  FG_CUDA(cub::DeviceSelect::If(d_tmp, tmp, it, tmpout, d_n, (int)n, pred, s));
+  FG_CUDA(cudaMemcpyAsync(count, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  cudaFree(*d_out);
+  *d_out = nullptr;
+  FG_CUDA(cudaMalloc(d_out, (size_t)std::max(1, *count) * sizeof(int)));
+  FG_CUDA(cudaMemcpyAsync(*d_out, tmpout, (size_t)(*count) * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  cudaFree(tmpout); cudaFree(d_tmp); cudaFree(d_n);
+  return FG_OK;
+}
+
 }  // namespace fg
 
+using namespace fg;
+
 extern "C" {
-fg_status fg_case_add_body(fg_case *, int, int, const double *, const int32_t *, int, double, int) { return FG_BAD_INPUT; }
-fg_status fg_case_update_body(fg_case *, int, const double *) { return FG_BAD_INPUT; }
-fg_status fg_set_iblank_body_fast(fg_case *, int8_t *) { return FG_BAD_INPUT; }
-fg_status fg_gcm_set_internal_boundary(fg_case *, int8_t *, int8_t *, int8_t *, int *, int *) { return FG_BAD_INPUT; }
-fg_status fg_get_ghost_rows(const fg_case *, int32_t *, int32_t *, double *, double *, double *, double *, double *, int32_t *, double *) { return FG_BAD_INPUT; }
-fg_status fg_get_dead_rows(const fg_case *, int32_t *, int32_t *, double *, double *, double *, double *, double *, int32_t *) { return FG_BAD_INPUT; }
-fg_status fg_get_band(const fg_case *, int8_t *) { return FG_BAD_INPUT; }
+
+fg_status fg_case_add_body(fg_case *c, int nvert, int ntri, const double *xyz, const int32_t *tri,
+                           int surface_type, double membrane_tkns, int body_dim) {
+  if (!c || nvert < 3 || ntri < 1 || !xyz || !tri) return FG_BAD_INPUT;
+  if (c->geom->bodies.size() >= 8) return FG_BAD_INPUT;
+  for (long long m = 0; m < 3LL * ntri; ++m)
+    if (tri[m] < 0 || tri[m] >= nvert) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  DevBody B;
+  B.nvert = nvert; B.ntri = ntri; B.type = surface_type; B.body_dim = body_dim;
+  B.membrane_tkns = membrane_tkns;
+  B.xyz.assign(xyz, xyz + 3 * (size_t)nvert);
+  B.tri.assign(tri, tri + 3 * (size_t)ntri);
+  // vertex -> triangles in ascending triangle order (the full scan of
+  // BOUNDARY_IBLANK_FAST.F90:992-999 visits them in that order)
+  std::vector<int32_t> cnt(nvert, 0), off(nvert + 1, 0), v2t;
+  for (int m = 0; m < ntri; ++m) {
+    int a = tri[3 * m], b = tri[3 * m + 1], d = tri[3 * m + 2];
+    cnt[a]++;
+    if (b != a) cnt[b]++;
+    if (d != a && d != b) cnt[d]++;
+  }
+  for (int v = 0; v < nvert; ++v) off[v + 1] = off[v] + cnt[v];
+  v2t.assign(off[nvert], 0);
+  std::fill(cnt.begin(), cnt.end(), 0);
+  for (int m = 0; m < ntri; ++m) {
+    int a = tri[3 * m], b = tri[3 * m + 1], d = tri[3 * m + 2];
+    v2t[off[a] + cnt[a]++] = m;
+    if (b != a) v2t[off[b] + cnt[b]++] = m;
+    if (d != a && d != b) v2t[off[d] + cnt[d]++] = m;
+  }
+  FG_CUDA(cudaMalloc(&B.d_tri, 3 * (size_t)ntri * sizeof(int32_t)));
+  FG_CUDA(cudaMemcpy(B.d_tri, tri, 3 * (size_t)ntri * sizeof(int32_t), cudaMemcpyHostToDevice));
+  FG_CUDA(cudaMalloc(&B.d_v2t_off, (nvert + 1) * sizeof(int32_t)));
+  FG_CUDA(cudaMemcpy(B.d_v2t_off, off.data(), (nvert + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+  FG_CUDA(cudaMalloc(&B.d_v2t, std::max<size_t>(1, v2t.size()) * sizeof(int32_t)));
+  FG_CUDA(cudaMemcpy(B.d_v2t, v2t.data(), v2t.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  fg_status st = upload_body(B);
+  if (st != FG_OK) return st;
+  c->geom->bodies.push_back(B);
+  return FG_OK;
 }
+
+fg_status fg_case_update_body(fg_case *c, int ibody, const double *xyz) {
+  if (!c || !xyz || ibody < 0 || ibody >= (int)c->geom->bodies.size()) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  DevBody &B = c->geom->bodies[ibody];
+  B.xyz.assign(xyz, xyz + 3 * (size_t)B.nvert);
+  return upload_body(B);
+}
+
+static geo::Bodies make_bodies(fg_case *c) {
+  geo::Bodies BB;
+  memset(&BB, 0, sizeof(BB));
+  BB.n = (int)c->geom->bodies.size();
+  for (int b = 0; b < BB.n; ++b) BB.b[b] = dev_body(c->geom->bodies[b]);
+  return BB;
+}
+
+fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank) {
+  if (!c || c->geom->bodies.empty()) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  Geom &G = *c->geom;
+  fg_status st = ensure_fields(c);
+  if (st != FG_OK) return st;
+  geo::Grid g;
+  if ((st = geom_grid(c, g)) != FG_OK) return st;
+  const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  int8_t *ibt = G.d_tmp;
+  FG_CUDA(cudaMemsetAsync(G.d_band, 0, n, s));
+  FG_CUDA(cudaMemsetAsync(ibt, 0, n, s));
+  FG_CUDA(cudaMemsetAsync(G.d_body, 0, n, s));
+  geo::Bodies BB = make_bodies(c);
+  for (int b = BB.n - 1; b >= 0; --b)
+    geo::k_band<<<(BB.b[b].ntri + 127) / 128, 128, 0, s>>>(g, BB.b[b], G.d_band);
+  FG_CUDA(cudaGetLastError());
+  // band cells of the interior classification range (j, k in [1, n-1])
+  int *d_cells = nullptr, ncell = 0;
+  if ((st = compact(geo::IsFlag{G.d_band, 1}, n, &d_cells, &ncell, s)) != FG_OK) return st;
+  int *d_warn = nullptr;
+  FG_CUDA(cudaMalloc(&d_warn, sizeof(int)));
+  FG_CUDA(cudaMemsetAsync(d_warn, 0, sizeof(int), s));
+  if (ncell > 0) {
+    const int wpb = 4;
+    geo::k_classify<<<(ncell + wpb - 1) / wpb, 32 * wpb, 0, s>>>(g, BB, d_cells, ncell, ibt, G.d_body, d_warn);
+    FG_CUDA(cudaGetLastError());
+  }
+  const int nl = (c->ny - 1) * (c->nz - 1);
+  geo::k_fill<<<(nl + 127) / 128, 128, 0, s>>>(g, G.d_band, ibt, G.d_body);
+  const long long nc = (long long)(c->nx + 1) * (c->ny - 1) * (c->nz - 1);
+  geo::k_commit<<<(unsigned)((nc + 255) / 256), 256, 0, s>>>(g, ibt, G.d_iblank);
+  FG_CUDA(cudaGetLastError());
+  int hw = 0;
+  FG_CUDA(cudaMemcpyAsync(&hw, d_warn, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  G.nWarnSide = hw;
+  cudaFree(d_cells); cudaFree(d_warn);
+  if (iblank) FG_CUDA(cudaMemcpy(iblank, G.d_iblank, n, cudaMemcpyDeviceToHost));
+  G.tagged = true;
+  return FG_OK;
+}
+
+fg_status fg_get_band(const fg_case *c, int8_t *band) {
+  if (!c || !band || !c->geom->d_band) return FG_BAD_INPUT;
+  const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  FG_CUDA(cudaMemcpy(band, c->geom->d_band, n, cudaMemcpyDeviceToHost));
+  return FG_OK;
+}
+
+// One in-place smoothing pass (mode 0: 3-D, 1: x planes, 2: y planes) as a
+// Jacobi fixed-point iteration.  Every dependency chain of the sequential
+// pass steps backward along x, y or z, so the iteration is exact after at
+// most nx + ny + nz steps.
+static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_changed) {
+  Geom &G = *c->geom;
+  cudaStream_t s = c->stream;
+  const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  int8_t *old = G.d_tmp, *cur = G.d_tmp + n, *nxt = G.d_tmp + 2 * n, *bold = G.d_tmp + 3 * n;
+  int8_t *bcur = G.d_dead, *bnxt = G.d_ghost;  // free until the lists are built
+  FG_CUDA(cudaMemcpyAsync(old, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(cur, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(nxt, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(bold, G.d_body, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(bcur, G.d_body, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(bnxt, G.d_body, n, cudaMemcpyDeviceToDevice, s));
+  const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
+  const int cap = c->nx + c->ny + c->nz + 2;
+  bool done = false;
+  for (int it = 0; it < cap && !done; ++it) {
+    int h = 0;
+    FG_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
+    geo::k_smooth_step<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, mode, old, cur, nxt, bold,
+                                                                     bcur, bnxt, d_changed);
+    FG_CUDA(cudaGetLastError());
+    FG_CUDA(cudaMemcpyAsync(&h, d_changed, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    std::swap(cur, nxt);
+    std::swap(bcur, bnxt);
+    done = (h == 0);
+  }
+  if (!done) {
+    set_last_error("iblank smoothing did not reach its fixed point", __FILE__, __LINE__);
+    return FG_TIMEOUT;
+  }
+  FG_CUDA(cudaMemcpyAsync(G.d_iblank, cur, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(G.d_body, bcur, n, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  return FG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// device buffers of one row list (ghost or dead)
+struct RowBufs {
+  geo::RowOut o{};
+  double *cD = nullptr, *cN = nullptr;
+  fg_status alloc(int m) {
+    const size_t mm = (size_t)std::max(1, m);
+    FG_CUDA(cudaMalloc(&o.bi, 3 * mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.bw, 3 * mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.ip, 3 * mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.nrm, 3 * mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.probe, mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.ds, mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&o.cell, 3 * mm * sizeof(int)));
+    FG_CUDA(cudaMalloc(&o.closest, mm * sizeof(int)));
+    FG_CUDA(cudaMalloc(&cD, 8 * mm * sizeof(double)));
+    FG_CUDA(cudaMalloc(&cN, 8 * mm * sizeof(double)));
+    return FG_OK;
+  }
+  ~RowBufs() {
+    cudaFree(o.bi); cudaFree(o.bw); cudaFree(o.ip); cudaFree(o.nrm); cudaFree(o.probe);
+    cudaFree(o.ds); cudaFree(o.cell); cudaFree(o.closest); cudaFree(cD); cudaFree(cN);
+  }
+};
+
+template <typename T>
+fg_status d2h(const T *d, size_t m, std::vector<T> &h) {
+  h.resize(m);
+  if (m) FG_CUDA(cudaMemcpy(h.data(), d, m * sizeof(T), cudaMemcpyDeviceToHost));
+  return FG_OK;
+}
+
+void list_ijk(const std::vector<int> &l, long long NX, long long NY, std::vector<int32_t> &ijk) {
+  ijk.resize(3 * l.size());
+  for (size_t r = 0; r < l.size(); ++r) {
+    ijk[3 * r] = (int32_t)(l[r] % NX);
+    ijk[3 * r + 1] = (int32_t)((l[r] / NX) % NY);
+    ijk[3 * r + 2] = (int32_t)(l[r] / (NX * NY));
+  }
+}
+
+struct DevList {
+  int *p = nullptr;
+  ~DevList() { cudaFree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghostCellMark,
+                                       int8_t *dead_cell, int *nGhost, int *nDead) {
+  if (!c || !c->geom->tagged) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  Geom &G = *c->geom;
+  geo::Grid g;
+  fg_status st = geom_grid(c, g);
+  if (st != FG_OK) return st;
+  const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  DevList flag, gl, dl, rank;
+  FG_CUDA(cudaMalloc(&flag.p, 4 * sizeof(int)));
+  // smoothing: 5 x 3-D, 5 x x-planes, 5 x y-planes (GCM_SET_BOUNDARY.F90:115-223, :1618-1697)
+  for (int mode = 0; mode < 3; ++mode)
+    for (int it = 0; it < 5; ++it)
+      if ((st = smooth_pass(c, g, mode, flag.p)) != FG_OK) return st;
+  const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
+  FG_CUDA(cudaMemsetAsync(G.d_ghost, 0, n, s));  // held smoothing scratch
+  geo::k_ghost_mark<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_body);
+  FG_CUDA(cudaGetLastError());
+  geo::k_dead_mark<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_dead);
+  FG_CUDA(cudaGetLastError());
+  int ng = 0, nd = 0;
+  if ((st = compact(geo::IsFlag{G.d_ghost, 1}, n, &gl.p, &ng, s)) != FG_OK) return st;
+  geo::IsDeadRow dpred{G.d_dead, c->nx + 2, c->ny + 2, c->nx, c->ny, c->nz};
+  if ((st = compact(dpred, n, &dl.p, &nd, s)) != FG_OK) return st;
+  geo::Bodies BB = make_bodies(c);
+  RowBufs gb, db;
+  if ((st = gb.alloc(ng)) != FG_OK) return st;
+  if ((st = db.alloc(nd)) != FG_OK) return st;
+  DevList alpha_buf;
+  double *alpha = nullptr;
+  FG_CUDA(cudaMalloc(&alpha, (size_t)std::max(1, ng) * sizeof(double)));
+  alpha_buf.p = reinterpret_cast<int *>(alpha);
+  FG_CUDA(cudaMemsetAsync(flag.p, 0, 4 * sizeof(int), s));
+  const double pln = c->cfg.probe_length, plnD = c->cfg.probe_length_dead;
+  if (ng > 0) {
+    geo::k_ghost_geom<<<(ng + 3) / 4, 128, 0, s>>>(g, BB, gl.p, ng, G.d_body, pln, gb.o, flag.p);
+    geo::k_weights<<<(ng + 63) / 64, 64, 0, s>>>(g, gl.p, ng, gb.o, 0, gb.cD, gb.cN, flag.p + 1);
+  }
+  if (nd > 0) {
+    geo::k_dead_geom<<<(nd + 3) / 4, 128, 0, s>>>(g, BB, dl.p, nd, G.d_body, plnD, db.o, flag.p,
+                                                  flag.p + 2);
+    geo::k_weights<<<(nd + 63) / 64, 64, 0, s>>>(g, dl.p, nd, db.o, 1, db.cD, db.cN, flag.p + 1);
+  }
+  FG_CUDA(cudaGetLastError());
+  FG_CUDA(cudaMalloc(&rank.p, n * sizeof(int)));
+  FG_CUDA(cudaMemsetAsync(rank.p, 0xff, n * sizeof(int), s));
+  if (nd > 0) geo::k_rank<<<(nd + 255) / 256, 256, 0, s>>>(dl.p, nd, rank.p);
+  if (ng > 0) geo::k_alpha<<<(ng + 255) / 256, 256, 0, s>>>(g, gl.p, ng, G.d_dead, rank.p, db.o.ds, alpha);
+  FG_CUDA(cudaGetLastError());
+  int flags[4] = {0, 0, 0, 0};
+  FG_CUDA(cudaMemcpyAsync(flags, flag.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  G.nWarnSide += flags[0];
+  G.nHostFail = flags[1];
+  // host copies of masks and rows
+  std::vector<int8_t> hib, hgh, hde;
+  if ((st = d2h(G.d_iblank, n, hib)) != FG_OK) return st;
+  if ((st = d2h(G.d_ghost, n, hgh)) != FG_OK) return st;
+  if ((st = d2h(G.d_dead, n, hde)) != FG_OK) return st;
+  std::vector<int> hgl, hdl;
+  if ((st = d2h((const int *)gl.p, (size_t)ng, hgl)) != FG_OK) return st;
+  if ((st = d2h((const int *)dl.p, (size_t)nd, hdl)) != FG_OK) return st;
+  std::vector<int32_t> g_ijk, d_ijk, g_cell, d_cell;
+  std::vector<double> g_coefN, d_coefN, d_probe, d_ip;
+  list_ijk(hgl, c->nx + 2, c->ny + 2, g_ijk);
+  list_ijk(hdl, c->nx + 2, c->ny + 2, d_ijk);
+  if ((st = d2h((const int32_t *)gb.o.cell, 3 * (size_t)ng, g_cell)) != FG_OK) return st;
+  if ((st = d2h((const int32_t *)db.o.cell, 3 * (size_t)nd, d_cell)) != FG_OK) return st;
+  if ((st = d2h((const double *)gb.cN, 8 * (size_t)ng, g_coefN)) != FG_OK) return st;
+  if ((st = d2h((const double *)db.cN, 8 * (size_t)nd, d_coefN)) != FG_OK) return st;
+  if ((st = d2h((const double *)db.o.probe, (size_t)nd, d_probe)) != FG_OK) return st;
+  if ((st = d2h((const double *)db.o.ip, 3 * (size_t)nd, d_ip)) != FG_OK) return st;
+  if ((st = d2h((const double *)gb.cD, 8 * (size_t)ng, G.g_coefD)) != FG_OK) return st;
+  if ((st = d2h((const double *)gb.o.bi, 3 * (size_t)ng, G.g_bi)) != FG_OK) return st;
+  if ((st = d2h((const double *)gb.o.ip, 3 * (size_t)ng, G.g_ip)) != FG_OK) return st;
+  if ((st = d2h((const double *)gb.o.probe, (size_t)ng, G.g_probe)) != FG_OK) return st;
+  if ((st = d2h((const double *)alpha, (size_t)ng, G.g_alpha)) != FG_OK) return st;
+  if ((st = d2h((const int32_t *)gb.o.closest, (size_t)ng, G.g_closest)) != FG_OK) return st;
+  if ((st = d2h((const double *)db.cD, 8 * (size_t)nd, G.d_coefD)) != FG_OK) return st;
+  if ((st = d2h((const double *)db.o.bi, 3 * (size_t)nd, G.d_bi)) != FG_OK) return st;
+  if ((st = d2h((const int32_t *)db.o.closest, (size_t)nd, G.d_closest)) != FG_OK) return st;
+  // hand the masks and rows to the solver (same path as caller-supplied
+  // geometry, which also marks the dead rows using the fallback)
+  st = fg_case_set_geometry(c, hib.data(), hgh.data(), hde.data(), ng, g_ijk.data(), g_cell.data(),
+                            g_coefN.data(), nd, d_ijk.data(), d_cell.data(), d_coefN.data(),
+                            d_probe.data(), d_ip.data());
+  if (st != FG_OK) return st;
+  if (iblank) memcpy(iblank, hib.data(), n);
+  if (ghostCellMark) memcpy(ghostCellMark, hgh.data(), n);
+  if (dead_cell) memcpy(dead_cell, hde.data(), n);
+  if (nGhost) *nGhost = ng;
+  if (nDead) *nDead = nd;
+  if (flags[2]) return FG_GEOMETRY_DEAD_NO_BODY;
+  if (G.nHostFail) return FG_GEOMETRY_NO_HOST_CELL;
+  return FG_OK;
+}
+
+fg_status fg_get_ghost_rows(const fg_case *c, int32_t *ijk, int32_t *cell, double *coefN,
+                            double *coefD, double *bi, double *ip, double *probe,
+                            int32_t *closest, double *alpha) {
+  if (!c) return FG_BAD_INPUT;
+  const Geom &G = *c->geom;
+  const size_t n = (size_t)c->nGhost;
+  if (ijk) memcpy(ijk, c->g_ijk.data(), 3 * n * sizeof(int32_t));
+  if (cell) memcpy(cell, c->g_cell.data(), 3 * n * sizeof(int32_t));
+  if (coefN) memcpy(coefN, c->g_coefN.data(), 8 * n * sizeof(double));
+  if (coefD && G.g_coefD.size() >= 8 * n) memcpy(coefD, G.g_coefD.data(), 8 * n * sizeof(double));
+  if (bi && G.g_bi.size() >= 3 * n) memcpy(bi, G.g_bi.data(), 3 * n * sizeof(double));
+  if (ip && G.g_ip.size() >= 3 * n) memcpy(ip, G.g_ip.data(), 3 * n * sizeof(double));
+  if (probe && G.g_probe.size() >= n) memcpy(probe, G.g_probe.data(), n * sizeof(double));
+  if (closest && G.g_closest.size() >= n) memcpy(closest, G.g_closest.data(), n * sizeof(int32_t));
+  if (alpha && G.g_alpha.size() >= n) memcpy(alpha, G.g_alpha.data(), n * sizeof(double));
+  return FG_OK;
+}
+
+fg_status fg_get_dead_rows(const fg_case *c, int32_t *ijk, int32_t *cell, double *coefN,
+                           double *coefD, double *bi, double *ip, double *probe,
+                           int32_t *closest) {
+  if (!c) return FG_BAD_INPUT;
+  const Geom &G = *c->geom;
+  const size_t n = (size_t)c->nDead;
+  if (ijk) memcpy(ijk, c->d_ijk.data(), 3 * n * sizeof(int32_t));
+  if (cell) memcpy(cell, c->d_cell.data(), 3 * n * sizeof(int32_t));
+  if (coefN) memcpy(coefN, c->d_coefN.data(), 8 * n * sizeof(double));
+  if (coefD && G.d_coefD.size() >= 8 * n) memcpy(coefD, G.d_coefD.data(), 8 * n * sizeof(double));
+  if (bi && G.d_bi.size() >= 3 * n) memcpy(bi, G.d_bi.data(), 3 * n * sizeof(double));
+  if (ip && c->d_ipv.size() >= 3 * n) memcpy(ip, c->d_ipv.data(), 3 * n * sizeof(double));
+  if (probe && c->d_probe.size() >= n) memcpy(probe, c->d_probe.data(), n * sizeof(double));
+  if (closest && G.d_closest.size() >= n) memcpy(closest, G.d_closest.data(), n * sizeof(int32_t));
+  return FG_OK;
+}
+
+}  // extern "C"

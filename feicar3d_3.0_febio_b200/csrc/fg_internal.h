@@ -27,43 +27,99 @@ enum : int8_t {
 constexpr int kMaxLevels = 12;
 constexpr int kRowPitch = 32;  // elements
 
+// Device arrays of the level and row descriptors.  In a checked build
+// (-DFG_CHECKED, for diagnosing a memory fault) each one carries its length:
+// an index outside it is recorded (first offender, hit count, kinds hit) and
+// the access goes to a scratch slot, so the faulting access never happens.
+// Normal builds use plain pointers and generate the same code as without.
+#ifdef FG_CHECKED
+struct CheckRec {
+  unsigned long long hits;
+  long long idx, lim;
+  int kid;
+  unsigned kinds;
+};
+static __device__ CheckRec g_check;
+static __device__ double g_check_sink[8];
+__device__ __forceinline__ void check_record(long long i, long long n, int kid) {
+  if (atomicAdd(&g_check.hits, 1ull) == 0ull) {
+    g_check.idx = i;
+    g_check.lim = n;
+    g_check.kid = kid;
+  }
+  atomicOr(&g_check.kinds, 1u << (kid & 31));
+}
+template <class T>
+struct DPtr {
+  T *p;
+  long long n;
+  int kid;
+  __host__ __device__ DPtr() : p(nullptr), n(0), kid(0) {}
+  __host__ __device__ DPtr(T *q, long long m, int k) : p(q), n(m), kid(k) {}
+  template <class U>
+  __host__ __device__ DPtr(const DPtr<U> &o) : p(o.p), n(o.n), kid(o.kid) {}
+  __device__ T &operator[](long long i) const {
+    if (p != nullptr && i >= 0 && i < n) return p[i];
+    check_record(i, p ? n : -1, kid);
+    return *reinterpret_cast<T *>(g_check_sink);
+  }
+  __host__ __device__ DPtr operator+(long long o) const { return DPtr(p + o, n - o, kid); }
+  __host__ __device__ explicit operator bool() const { return p != nullptr; }
+};
+template <class T> using dptr = DPtr<T>;
+template <class T>
+__host__ __device__ inline DPtr<T> mkptr(T *p, long long n, int kid) { return DPtr<T>(p, n, kid); }
+#define FG_RESTRICT
+#else
+template <class T> using dptr = T *;
+template <class T>
+__host__ __device__ inline T *mkptr(T *p, long long, int) { return p; }
+#define FG_RESTRICT __restrict__
+#endif
+
+// array kinds reported by a checked build
+enum : int {
+  K_TYPE = 1, K_MASK = 2, K_AXIS = 3, K_WIDTH = 4, K_CHILD = 5, K_PROL = 6, K_X = 7, K_RHS = 8,
+  K_RES = 9, K_ROWS = 10, K_SMEM_D = 11, K_SMEM_F = 12
+};
+
 struct DevLevel {
   int nx, ny, nz;        // interior cells per axis
   int pad_;
   long long sy, sz;      // strides in elements
   long long ntot;        // elements of one field
-  const int8_t *type;
+  dptr<const int8_t> type;
   // per-cell operator mask: bit q (0..5) = face q coupled (neighbour
   // active, ghost or solid; faces -x,+x,-y,+y,-z,+z), bit 6 = active row,
   // bit 7 = receives the coarse correction (active or ghost)
-  const uint8_t *mask;
+  dptr<const uint8_t> mask;
   // per-axis operator coefficients indexed by cell 1..n (arrays of n+2):
   // am(i) couples cell i to i-1, ap(i) to i+1 (CORE_MG.F90:674-676)
-  const double *amx, *apx, *amy, *apy, *amz, *apz;
+  dptr<const double> amx, apx, amy, apy, amz, apz;
   // cell widths indexed by cell 1..n
-  const double *wx, *wy, *wz;
+  dptr<const double> wx, wy, wz;
   // children (in the next finer level) of each cell of THIS level: [lo, hi]
-  const int *clx, *chx, *cly, *chy, *clz, *chz;
+  dptr<const int> clx, chx, cly, chy, clz, chz;
   // prolongation into THIS level from the next coarser one: lower coarse
   // cell and the weight of the upper one, per fine cell (1..n)
-  const int *plx, *ply, *plz;
-  const double *pwx, *pwy, *pwz;
+  dptr<const int> plx, ply, plz;
+  dptr<const double> pwx, pwy, pwz;
   int bc[6];             // 0 Neumann (face dropped), 1 Dirichlet
   // value arrays (only those of the level's precision are set)
-  double *x64, *rhs64, *res64;
-  float *x32, *rhs32, *res32;
+  dptr<double> x64, rhs64, res64;
+  dptr<float> x32, rhs32, res32;
 };
 
 // interpolation rows of the fine level (ghost or dead cells) of a batch
 struct DevRows {
   int n;
-  const int *prob;        // problem of each row
-  const long long *tgt;   // target element index
-  const long long *cell;  // host-cell lower-corner element index
-  const double *w;        // 8 weights per row (own slot zeroed)
-  const double *c0;       // constant term per row (solution form)
-  double *rd;             // row residual, FP64 (correction form constant)
-  float *rf;              // row residual, FP32
+  dptr<const int> prob;        // problem of each row
+  dptr<const long long> tgt;   // target element index
+  dptr<const long long> cell;  // host-cell lower-corner element index
+  dptr<const double> w;        // 8 weights per row (own slot zeroed)
+  dptr<const double> c0;       // constant term per row (solution form)
+  dptr<double> rd;             // row residual, FP64 (correction form constant)
+  dptr<float> rf;              // row residual, FP32
 };
 
 // one launch over a set of problems: block b belongs to entry p with
@@ -78,6 +134,10 @@ struct Launch {
 
 void set_last_error(const char *msg, const char *file, int line);
 const char *last_error_msg();
+
+// kernels launched by this process (every launch site adds its count)
+void note_launches(long long n);
+long long launches_so_far();
 
 #define FG_CUDA(call)                                                  \
   do {                                                                 \
@@ -94,7 +154,7 @@ namespace k {
 int blocks_cells(const DevLevel &L);
 int blocks_xline(const DevLevel &L);
 int blocks_tile(const DevLevel &L, int axis);
-size_t smem_line(int n, int tsize, int lines_per_block);
+size_t smem_line(int n, int tsize, int axis);
 
 template <typename T>
 cudaError_t line_sweep(const Launch &L, int axis, int color, double omega, int maxn,
@@ -123,6 +183,16 @@ cudaError_t copy_in(double *dst, const double *src, int nx, int ny, int nz, long
                     long long sz, cudaStream_t s);
 cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, long long sy,
                      long long sz, cudaStream_t s);
+// gauge shift and outer boundary layers of a reference-layout field
+// (CORE_POISSON.F90:129-149, CORE_SET_OUTER_BC.F90:1088-1170): with all
+// faces Neumann and gauge set, p -= p(1,1,1) on every cell of 0..n except
+// pure-solid interior cells; then the faces x, y, z in that order copy
+// (Neumann) or reflect about ppp (Dirichlet) the first interior layer.
+// nx, ny, nz are node counts; lev0 is the host copy of the level-0
+// descriptor (its type array marks the pure-solid cells).
+cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz,
+                         const int *pbc, const double *ppp, int gauge, double *scratch,
+                         cudaStream_t s);
 }  // namespace k
 
 }  // namespace fg

@@ -10,11 +10,18 @@
 // (CORE_MG.F90:615-938 relaxes lines lexicographically; here lines of one
 // colour are solved in parallel, one warp per line).
 #include <cuda_runtime.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #include "fg_internal.h"
 
 namespace fg {
+
+static std::atomic<long long> g_launches{0};
+void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+
 namespace k {
 
 constexpr int XL_WARPS = 8;    // x-lines per block
@@ -169,8 +176,8 @@ __device__ __forceinline__ void row_coef(uint8_t mk, int r, int n, double am, do
 // value.  All loads are issued unconditionally.
 template <typename T>
 __device__ __forceinline__ void stage(const DevLevel &L, long long id, const LineCoef &lc,
-                                      const T *__restrict__ x, const T *__restrict__ rhs,
-                                      T &d, uint8_t &mk) {
+                                      dptr<const T> FG_RESTRICT x,
+                                      dptr<const T> FG_RESTRICT rhs, T &d, uint8_t &mk) {
   mk = L.mask[id];
   const T r = rhs[id], xo = x[id];
   const T x0 = x[id + lc.to[0]], x1 = x[id + lc.to[1]], x2 = x[id + lc.to[2]], x3 = x[id + lc.to[3]];
@@ -227,9 +234,9 @@ __device__ __forceinline__ Eq<T> shfl_eq_down(const Eq<T> &e, int t, int lane) {
 // reduction across lanes, and each lane back-substitutes its chunk.  The
 // solution overwrites d.
 template <typename T, int MAXM>
-__device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am,
-                                           const double *__restrict__ ap, const LineCoef &lc,
-                                           T *sd, const uint8_t *sf, int lane) {
+__device__ __forceinline__ void warp_solve(int n, dptr<const double> FG_RESTRICT am,
+                                           dptr<const double> FG_RESTRICT ap, const LineCoef &lc,
+                                           dptr<T> sd, dptr<const uint8_t> sf, int lane) {
   if (n == 1) {
     if (lane == 0) {
       T a, b, c;
@@ -339,15 +346,27 @@ __device__ __forceinline__ void warp_solve(int n, const double *__restrict__ am,
 
 template <typename T> struct PrecOf;
 template <> struct PrecOf<double> {
-  static __device__ __forceinline__ double *x(const DevLevel &L) { return L.x64; }
-  static __device__ __forceinline__ double *rhs(const DevLevel &L) { return L.rhs64; }
-  static __device__ __forceinline__ double *res(const DevLevel &L) { return L.res64; }
+  static __device__ __forceinline__ dptr<double> x(const DevLevel &L) { return L.x64; }
+  static __device__ __forceinline__ dptr<double> rhs(const DevLevel &L) { return L.rhs64; }
+  static __device__ __forceinline__ dptr<double> res(const DevLevel &L) { return L.res64; }
 };
 template <> struct PrecOf<float> {
-  static __device__ __forceinline__ float *x(const DevLevel &L) { return L.x32; }
-  static __device__ __forceinline__ float *rhs(const DevLevel &L) { return L.rhs32; }
-  static __device__ __forceinline__ float *res(const DevLevel &L) { return L.res32; }
+  static __device__ __forceinline__ dptr<float> x(const DevLevel &L) { return L.x32; }
+  static __device__ __forceinline__ dptr<float> rhs(const DevLevel &L) { return L.rhs32; }
+  static __device__ __forceinline__ dptr<float> res(const DevLevel &L) { return L.res32; }
 };
+
+// bytes of dynamic shared memory of the launch (checked builds bound the
+// staging arrays by it)
+__device__ __forceinline__ long long dyn_smem_bytes() {
+#ifdef FG_CHECKED
+  unsigned v;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+  return (long long)v;
+#else
+  return 0;
+#endif
+}
 
 __host__ __device__ __forceinline__ int line_pad(int n) { return n + 33; }
 __host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
@@ -369,14 +388,17 @@ k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   const int n = L.nx;
   const int np = line_pad(n);
   const size_t per = align16(np * sizeof(T)) + align16(np);
-  T *sd = reinterpret_cast<T *>(smem + per * warp);
-  uint8_t *sf = smem + per * warp + align16(np * sizeof(T));
+  const long long dyn = dyn_smem_bytes();
+  dptr<T> sd = mkptr(reinterpret_cast<T *>(smem + per * warp),
+                     (dyn - (long long)(per * warp)) / (long long)sizeof(T), K_SMEM_D);
+  dptr<uint8_t> sf = mkptr(smem + per * warp + align16(np * sizeof(T)),
+                           dyn - (long long)(per * warp + align16(np * sizeof(T))), K_SMEM_F);
   if (k > L.nz) return;
   const int j0 = (((1 + k) & 1) == color) ? 1 : 2;
   const int j = j0 + 2 * jj;
   if (j > L.ny) return;
-  T *x = PrecOf<T>::x(L);
-  const T *rhs = PrecOf<T>::rhs(L);
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
   int P, base, rem;
   chunking(n, P, base, rem);
   const PadMap pm = padmap(base, rem);
@@ -427,11 +449,13 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   const long long os = AXIS == 1 ? L.sz : L.sy;
   const int np = line_pad(n);
   const int lstride = np + 1;  // per-line stride (elements), odd in words
-  T *sd = reinterpret_cast<T *>(smem);
-  uint8_t *sf = smem + align16((size_t)YZ_WARPS * lstride * sizeof(T));
+  const long long dyn = dyn_smem_bytes();
+  const size_t fo = align16((size_t)YZ_WARPS * lstride * sizeof(T));
+  dptr<T> sd = mkptr(reinterpret_cast<T *>(smem), (long long)fo / (long long)sizeof(T), K_SMEM_D);
+  dptr<uint8_t> sf = mkptr(smem + fo, dyn - (long long)fo, K_SMEM_F);
   const int il0 = (color + i0 + o) & 1;  // tile-local i of the first line of this colour
-  T *x = PrecOf<T>::x(L);
-  const T *rhs = PrecOf<T>::rhs(L);
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
   int P, base, rem;
   chunking(n, P, base, rem);
   const PadMap pm = padmap(base, rem);
@@ -443,7 +467,7 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
     const int slot = tid % YZ_WARPS;
     const int i = i0 + il0 + 2 * slot;
     const bool valid = i <= L.nx;
-    const LineCoef lc = line_coef(L, AXIS, i, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
+    const LineCoef lc = line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
     const long long base_id = i + os * o;
     for (int e0 = tid; e0 < total; e0 += 4 * NT) {
       T d[4]; uint8_t f[4];
@@ -467,8 +491,8 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   {
     const int i = i0 + il0 + 2 * warp;
     if (i <= L.nx) {
-      const double *am = AXIS == 1 ? L.amy : L.amz;
-      const double *ap = AXIS == 1 ? L.apy : L.apz;
+      const auto am = AXIS == 1 ? L.amy : L.amz;
+      const auto ap = AXIS == 1 ? L.apy : L.apz;
       const LineCoef lc = line_coef(L, AXIS, i, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
       warp_solve<T, MAXM>(n, am, ap, lc, sd + warp * lstride, sf + warp * lstride, lane);
     }
@@ -502,9 +526,11 @@ int blocks_tile(const DevLevel &L, int axis) {
   int ntx = (L.nx + TILE_I - 1) / TILE_I;
   return ntx * (axis == 1 ? L.nz : L.ny);
 }
-size_t smem_line(int n, int tsize, int lines) {
+// dynamic shared memory of a line launch: axis 0 uses the per-warp layout
+// of k_xline, axes 1 and 2 the interleaved tile layout of k_yzline
+size_t smem_line(int n, int tsize, int axis) {
   const int np = line_pad(n);
-  if (lines == XL_WARPS) {
+  if (axis == 0) {
     const size_t per = align16((size_t)np * tsize) + align16(np);
     return per * XL_WARPS;
   }
@@ -517,20 +543,23 @@ static cudaError_t launch_line(const Launch &Lr, int axis, int color, double ome
                                cudaStream_t s) {
   const T om = (T)omega;
   if (axis == 0) {
-    const size_t sm = smem_line(maxn, sizeof(T), XL_WARPS);
+    const size_t sm = smem_line(maxn, sizeof(T), 0);
     auto kern = k_xline<T, MAXM>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     kern<<<Lr.blocks, XL_WARPS * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, om);
+    note_launches(1);
   } else {
-    const size_t sm = smem_line(maxn, sizeof(T), YZ_WARPS);
+    const size_t sm = smem_line(maxn, sizeof(T), axis);
     if (axis == 1) {
       auto kern = k_yzline<T, MAXM, 1>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<Lr.blocks, YZ_WARPS * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, om);
+      note_launches(1);
     } else {
       auto kern = k_yzline<T, MAXM, 2>;
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       kern<<<Lr.blocks, YZ_WARPS * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, om);
+      note_launches(1);
     }
   }
   return cudaGetLastError();
@@ -572,7 +601,7 @@ __device__ __forceinline__ double block_sum(double v) {
 // a (x_n - x_c), Dirichlet boundary faces contributing -2 a x_c
 template <typename T>
 __device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, int j, int k,
-                                       uint8_t mk, const T *__restrict__ x) {
+                                       uint8_t mk, dptr<const T> FG_RESTRICT x) {
   const T xc = x[id];
   const T x0 = x[id - 1], x1 = x[id + 1], x2 = x[id - L.sy], x3 = x[id + L.sy];
   const T x4 = x[id - L.sz], x5 = x[id + L.sz];
@@ -622,9 +651,9 @@ k_residual(const int *off, int nent, const DevLevel *levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  const T *x = PrecOf<T>::x(L);
-  const T *rhs = PrecOf<T>::rhs(L);
-  T *res = PrecOf<T>::res(L);
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  auto res = PrecOf<T>::res(L);
   double r2 = 0.0;
 #pragma unroll 2
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
@@ -647,7 +676,11 @@ template <typename T>
 cudaError_t residual(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
   k_residual<T><<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, norm2 ? part : nullptr);
-  if (norm2) k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
+  note_launches(1);
+  if (norm2) {
+    k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
+    note_launches(1);
+  }
   return cudaGetLastError();
 }
 
@@ -671,7 +704,9 @@ k_fluid_norm(const int *off, int nent, const DevLevel *levs, double *part) {
 cudaError_t fluid_norm(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
   k_fluid_norm<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, part);
+  note_launches(1);
   k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -717,8 +752,11 @@ k_residual_mixed(const int *off, int nent, const DevLevel *levs, double *part) {
 cudaError_t correct_residual(const Launch &Lr, double *norm2, double *part, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
   k_correct<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev);
+  note_launches(1);
   k_residual_mixed<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, part);
+  note_launches(1);
   k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -732,8 +770,8 @@ k_restrict(const int *off, int nent, const DevLevel *coarse, const DevLevel *fin
   const DevLevel &C = coarse[p];
   const DevLevel &F = fine[p];
   const int lb = blockIdx.x - off[p];
-  T *rc = PrecOf<T>::rhs(C);
-  const T *rf = PrecOf<T>::res(F);
+  auto rc = PrecOf<T>::rhs(C);
+  auto rf = PrecOf<T>::res(F);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(C, lb, rr);
     if (!c.ok) continue;
@@ -759,6 +797,7 @@ template <typename T>
 cudaError_t restrict_to(const Launch &Lc, const DevLevel *fine, cudaStream_t s) {
   if (Lc.empty()) return cudaSuccess;
   k_restrict<T><<<Lc.blocks, CELL_BLOCK, 0, s>>>(Lc.off, Lc.n, Lc.lev, fine);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -772,8 +811,8 @@ k_prolong(const int *off, int nent, const DevLevel *fine, const DevLevel *coarse
   const DevLevel &F = fine[p];
   const DevLevel &C = coarse[p];
   const int lb = blockIdx.x - off[p];
-  const T *xc = PrecOf<T>::x(C);
-  T *x = PrecOf<T>::x(F);
+  auto xc = PrecOf<T>::x(C);
+  auto x = PrecOf<T>::x(F);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(F, lb, rr);
     if (!c.ok) continue;
@@ -802,6 +841,7 @@ template <typename T>
 cudaError_t prolong_add(const Launch &Lf, const DevLevel *coarse, cudaStream_t s) {
   if (Lf.empty()) return cudaSuccess;
   k_prolong<T><<<Lf.blocks, CELL_BLOCK, 0, s>>>(Lf.off, Lf.n, Lf.lev, coarse);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -811,7 +851,7 @@ k_zero(const int *off, int nent, const DevLevel *levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  T *x = PrecOf<T>::x(L);
+  auto x = PrecOf<T>::x(L);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(L, lb, rr);
     if (c.ok) x[c.i + L.sy * c.j + L.sz * c.k] = T(0);
@@ -822,6 +862,7 @@ template <typename T>
 cudaError_t zero_x(const Launch &Lr, cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
   k_zero<T><<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -837,7 +878,7 @@ k_rows(DevRows R, const DevLevel *lev0, int corr, double *tmp) {
   const int r = blockIdx.x * CELL_BLOCK + threadIdx.x;
   if (r >= R.n) return;
   const DevLevel &L = lev0[R.prob[r]];
-  const T *x = PrecOf<T>::x(L);
+  auto x = PrecOf<T>::x(L);
   const long long b = R.cell[r], sy = L.sy, sz = L.sz;
   const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
   double acc = 0.0;
@@ -864,7 +905,9 @@ cudaError_t rows_relax(const DevRows &R, const DevLevel *lev0, int corr, double 
   if (R.n <= 0) return cudaSuccess;
   const int nb = (R.n + CELL_BLOCK - 1) / CELL_BLOCK;
   k_rows<T><<<nb, CELL_BLOCK, 0, s>>>(R, lev0, corr, tmp);
+  note_launches(1);
   k_rows_scatter<T><<<nb, CELL_BLOCK, 0, s>>>(R, lev0, tmp);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -878,7 +921,7 @@ k_rows_residual(DevRows R, const DevLevel *lev0, double *maxabs) {
   unsigned long long v = 0ull;
   if (valid) {
     const DevLevel &L = lev0[p];
-    const double *x = L.x64;
+    const auto x = L.x64;
     const long long b = R.cell[r], sy = L.sy, sz = L.sz;
     const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
     double acc = 0.0;
@@ -910,6 +953,7 @@ cudaError_t rows_residual(const DevRows &R, const DevLevel *lev0, double *maxabs
                           cudaStream_t s) {
   if (R.n <= 0) return cudaSuccess;
   k_rows_residual<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, maxabs);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -925,8 +969,8 @@ k_coarsest(const DevLevel *levs, const double *const *G, const int *const *gidx,
   const int n = gn[p];
   const int *idx = gidx[p];
   const double *g = G[p];
-  const T *rhs = PrecOf<T>::rhs(L);
-  T *x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  auto x = PrecOf<T>::x(L);
   for (int c = threadIdx.x; c < n; c += blockDim.x) sr[c] = (double)rhs[idx[c]];
   __syncthreads();
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
@@ -945,6 +989,7 @@ cudaError_t coarsest_solve(int nprob, const DevLevel *lev, const double *const *
   if (sm > 48 * 1024)
     cudaFuncSetAttribute(k_coarsest<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   k_coarsest<T><<<nprob, 256, sm, s>>>(lev, G, gidx, gn);
+  note_launches(1);
   return cudaGetLastError();
 }
 
@@ -970,14 +1015,99 @@ cudaError_t copy_in(double *dst, const double *src, int nx, int ny, int nz, long
                     long long sz, cudaStream_t s) {
   const long long n = (long long)(nx + 2) * (ny + 2) * (nz + 2);
   k_copy_in<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dst, src, nx, ny, nz, sy, sz);
+  note_launches(1);
   return cudaGetLastError();
 }
 cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, long long sy,
                      long long sz, cudaStream_t s) {
   const long long n = (long long)(nx + 2) * (ny + 2) * (nz + 2);
   k_copy_out<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dst, src, nx, ny, nz, sy, sz);
+  note_launches(1);
   return cudaGetLastError();
 }
+
+// ------------------------------------------------ output finishing
+__global__ void k_gauge_save(const double *ref, long long id111, double *pa) { *pa = ref[id111]; }
+
+__global__ void k_gauge(double *ref, const DevLevel L, int nx, int ny, int nz, const double *pa) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long X = nx + 1, Y = ny + 1, Z = nz + 1;  // indices 0..n
+  if (e >= X * Y * Z) return;
+  const int i = (int)(e % X), j = (int)((e / X) % Y), k = (int)(e / (X * Y));
+  if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1 &&
+      L.type[i + L.sy * j + L.sz * k] == T_SOLID)
+    return;  // pure-solid values are held
+  ref[i + (long long)(nx + 2) * (j + (long long)(ny + 2) * k)] -= *pa;
+}
+
+struct FaceBC {
+  int pbc[6];
+  double ppp[6];
+};
+
+// face pair of one axis; a = 0: x faces over j,k in 1..n-1; a = 1: y faces
+// over i in 0..nx, k in 1..nz-1; a = 2: z faces over i in 0..nx, j in 1..ny-1
+__global__ void k_faces(double *ref, int nx, int ny, int nz, int a, FaceBC bc) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long RX = nx + 2, RY = ny + 2;
+  long long lo, hi, in0, in1;
+  if (a == 0) {
+    const long long nj = ny - 1;
+    if (e >= nj * (nz - 1)) return;
+    const long long j = 1 + e % nj, k = 1 + e / nj;
+    const long long b = RX * (j + RY * k);
+    lo = b; in0 = b + 1; hi = b + nx; in1 = b + nx - 1;
+  } else if (a == 1) {
+    const long long ni = nx + 1;
+    if (e >= ni * (nz - 1)) return;
+    const long long i = e % ni, k = 1 + e / ni;
+    lo = i + RX * (RY * k); in0 = lo + RX;
+    hi = i + RX * (ny + RY * k); in1 = hi - RX;
+  } else {
+    const long long ni = nx + 1;
+    if (e >= ni * (ny - 1)) return;
+    const long long i = e % ni, j = 1 + e / ni;
+    lo = i + RX * j; in0 = lo + RX * RY;
+    hi = i + RX * (j + RY * (long long)nz); in1 = hi - RX * RY;
+  }
+  const double v0 = ref[in0], v1 = ref[in1];
+  ref[lo] = bc.pbc[2 * a] == 1 ? 2.0 * bc.ppp[2 * a] - v0 : v0;
+  ref[hi] = bc.pbc[2 * a + 1] == 1 ? 2.0 * bc.ppp[2 * a + 1] - v1 : v1;
+}
+
+cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz, const int *pbc,
+                         const double *ppp, int gauge, double *scratch, cudaStream_t s) {
+  if (gauge) {
+    const long long id111 = 1 + (long long)(nx + 2) * (1 + (long long)(ny + 2));
+    k_gauge_save<<<1, 1, 0, s>>>(ref, id111, scratch);
+    note_launches(1);
+    const long long n = (long long)(nx + 1) * (ny + 1) * (nz + 1);
+    k_gauge<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ref, *lev0, nx, ny, nz, scratch);
+    note_launches(1);
+  }
+  FaceBC bc;
+  for (int f = 0; f < 6; ++f) { bc.pbc[f] = pbc[f]; bc.ppp[f] = ppp[f]; }
+  const long long nf[3] = {(long long)(ny - 1) * (nz - 1), (long long)(nx + 1) * (nz - 1),
+                           (long long)(nx + 1) * (ny - 1)};
+  for (int a = 0; a < 3; ++a) {
+    k_faces<<<(unsigned)((nf[a] + 255) / 256), 256, 0, s>>>(ref, nx, ny, nz, a, bc);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+#ifdef FG_CHECKED
+// first recorded out-of-range access of a checked build: {hits, index,
+// limit, kind, kinds bitmask}; resets the record
+extern "C" fg_status fg_debug_check(long long *out) {
+  CheckRec h{};
+  if (cudaMemcpyFromSymbol(&h, g_check, sizeof(h)) != cudaSuccess) return FG_CUDA_ERROR;
+  out[0] = (long long)h.hits; out[1] = h.idx; out[2] = h.lim; out[3] = h.kid; out[4] = h.kinds;
+  const CheckRec z{};
+  if (cudaMemcpyToSymbol(g_check, &z, sizeof(z)) != cudaSuccess) return FG_CUDA_ERROR;
+  return FG_OK;
+}
+#endif
 
 template cudaError_t line_sweep<double>(const Launch &, int, int, double, int, cudaStream_t);
 template cudaError_t line_sweep<float>(const Launch &, int, int, double, int, cudaStream_t);

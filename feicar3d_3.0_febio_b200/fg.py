@@ -21,7 +21,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfeicar_b200.so")
+# FEICAR_B200_LIB selects another build of the library (e.g. the bounds-checked
+# diagnostic build of csrc/Makefile's "checked" target)
+LIB_PATH = os.environ.get("FEICAR_B200_LIB") or os.path.join(_HERE, "libfeicar_b200.so")
 
 FG_OK, FG_NOT_CONVERGED = 0, 1
 FG_PBC_DIRICHLET, FG_PBC_NEUMANN = 1, 2
@@ -69,6 +71,22 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+PROF_CLASSES = ["line_x0", "line_y0", "line_z0", "line_coarse", "residual0", "transfer", "rows",
+                "coarsest"]
+
+
+class Profile(C.Structure):
+    _fields_ = [
+        ("class_launches", C.c_longlong * 8),
+        ("class_ms", C.c_double * 8),
+        ("class_bytes", C.c_double * 8),
+    ]
+
+    def as_dict(self):
+        return {name: {"launches": self.class_launches[i], "ms": self.class_ms[i],
+                       "bytes": self.class_bytes[i]} for i, name in enumerate(PROF_CLASSES)}
+
+
 _lib = None
 
 
@@ -105,12 +123,17 @@ def lib():
         L.fg_batch_add.argtypes = [vp, vp]
         L.fg_batch_solve_device.argtypes = [vp, vp, vp, C.POINTER(SolveStats)]
         L.fg_batch_destroy.argtypes = [vp]
+        L.fg_case_set_stream.argtypes = [vp, vp]
+        L.fg_launch_count.argtypes = [C.POINTER(C.c_longlong)]
+        L.fg_case_profile.argtypes = [vp, ip]
+        L.fg_case_profile_read.argtypes = [vp, C.POINTER(Profile)]
         for name in ["fg_device_count", "fg_case_create", "fg_case_destroy", "fg_case_levels",
                      "fg_case_add_body", "fg_case_update_body", "fg_set_iblank_body_fast",
                      "fg_gcm_set_internal_boundary", "fg_get_ghost_rows", "fg_get_dead_rows",
                      "fg_get_band", "fg_case_set_geometry", "fg_mg_prepare", "fg_solve_poisson",
                      "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
-                     "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy"]:
+                     "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy", "fg_case_set_stream",
+                     "fg_launch_count", "fg_case_profile", "fg_case_profile_read"]:
             getattr(L, name).restype = ip
         _lib = L
     return _lib
@@ -138,6 +161,13 @@ def default_config(**kw) -> SolverConfig:
         else:
             setattr(cfg, k, v)
     return cfg
+
+
+def launch_count() -> int:
+    """Kernels the library has launched in this process."""
+    n = C.c_longlong(0)
+    _check(lib().fg_launch_count(C.byref(n)), "fg_launch_count")
+    return n.value
 
 
 def device_count() -> int:
@@ -272,6 +302,20 @@ class Case:
         ok = (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,)
         _check(rc, "fg_solve_poisson_device", ok)
         return st.as_dict()
+
+    def set_stream(self, stream_handle: int | None):
+        """Order the case's work on a caller's cudaStream_t (an int handle,
+        e.g. ``torch.cuda.current_stream().cuda_stream``); None: own stream."""
+        _check(lib().fg_case_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
+               "fg_case_set_stream")
+
+    def profile(self, enable=True):
+        _check(lib().fg_case_profile(self.h, 1 if enable else 0), "fg_case_profile")
+
+    def profile_read(self) -> dict:
+        pr = Profile()
+        _check(lib().fg_case_profile_read(self.h, C.byref(pr)), "fg_case_profile_read")
+        return pr.as_dict()
 
     def ghostcell_pressure(self, p, p_old=None, iterations=1):
         _check(lib().fg_ghostcell_pressure(self.h, _p(p), _p(p_old), iterations), "fg_ghostcell_pressure")

@@ -155,6 +155,38 @@ fg_status fg_solve_poisson_device(fg_case *c, double *d_p,
 fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old,
                                 int iterations);
 
+/* ----- stream, launch count and timing (no reference counterpart: the
+ * reference prints wall time per solve_poisson call only,
+ * CORE_TIME_STEP.F90:180-185) ----- */
+/* Orders the handle's work on the caller's cudaStream_t (NULL: back to a
+ * stream of the handle's own). */
+fg_status fg_case_set_stream(fg_case *c, void *stream);
+/* Kernels this process has launched through the library so far. */
+fg_status fg_launch_count(long long *count);
+
+enum {
+  FG_PROF_LINE_X0 = 0,     /* finest-level x line sweeps (one colour each) */
+  FG_PROF_LINE_Y0 = 1,     /* finest-level y line sweeps                   */
+  FG_PROF_LINE_Z0 = 2,     /* finest-level z line sweeps                   */
+  FG_PROF_LINE_COARSE = 3, /* line sweeps of the coarse levels             */
+  FG_PROF_RESIDUAL = 4,    /* finest residual / correction / norms         */
+  FG_PROF_TRANSFER = 5,    /* residual, restriction, prolongation (coarse) */
+  FG_PROF_ROWS = 6,        /* ghost / dead row relaxation                  */
+  FG_PROF_COARSEST = 7,    /* coarsest dense solve                         */
+  FG_PROF_NCLASS = 8
+};
+typedef struct fg_profile {
+  long long class_launches[FG_PROF_NCLASS]; /* timed launch groups       */
+  double class_ms[FG_PROF_NCLASS];          /* CUDA-event device time    */
+  double class_bytes[FG_PROF_NCLASS];       /* algorithmic bytes (line
+                                               sweeps: 3s+1 per cell per
+                                               direction, +s if omega!=1) */
+} fg_profile;
+/* enable != 0: later solves on c bracket each launch group with CUDA
+ * events on the handle's stream; resets the totals. */
+fg_status fg_case_profile(fg_case *c, int enable);
+fg_status fg_case_profile_read(const fg_case *c, fg_profile *out);
+
 /* ----- batched uneven solves: many cases per launch per MG stage ----- */
 typedef struct fg_batch fg_batch;
 fg_status fg_batch_create(int device, const fg_solver_config *cfg,
