@@ -313,6 +313,7 @@ struct fg_batch {
   double *d_part = nullptr;   // per-block partial sums of level-0 reductions
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
   std::vector<double> h_norm;
+  std::vector<double> history;  // max relative residual over the batch after each cycle
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // optional CUDA-event timing of launch classes (fg_profile)
   struct Prof {
@@ -606,6 +607,7 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
   }
   int cyc = 0;
+  b->history.clear();
   std::vector<double> relres(np, 1.0), gres(np, 0.0);
   std::vector<double> vms;
   fg_status status = FG_NOT_CONVERGED;
@@ -635,12 +637,15 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     cudaEventElapsedTime(&ms, va, vb);
     vms.push_back(ms);
     bool all = true;
+    double worst = 0.0;
     for (int p = 0; p < np; ++p) {
       const double f2 = b->h_norm[np + p];
       relres[p] = f2 > 0.0 ? std::sqrt(b->h_norm[p] / f2) : std::sqrt(b->h_norm[p]);
       gres[p] = b->h_norm[2 * np + p];
+      worst = std::max(worst, relres[p]);
       if (!(relres[p] <= b->cfg.rtol)) all = false;
     }
+    b->history.push_back(worst);
     if (all) { status = FG_OK; break; }
   }
   if (cyc > b->cfg.max_cycles) cyc = b->cfg.max_cycles;
@@ -1232,6 +1237,16 @@ fg_status fg_case_set_stream(fg_case *c, void *stream) {
 fg_status fg_launch_count(long long *count) {
   if (!count) return FG_BAD_INPUT;
   *count = launches_so_far();
+  return FG_OK;
+}
+
+fg_status fg_case_history(const fg_case *c, double *relres, int capacity, int *count) {
+  if (!c || !count) return FG_BAD_INPUT;
+  const std::vector<double> empty;
+  const std::vector<double> &h = c->solo ? c->solo->history : empty;
+  *count = (int)h.size();
+  if (relres)
+    for (int q = 0; q < capacity && q < (int)h.size(); ++q) relres[q] = h[q];
   return FG_OK;
 }
 

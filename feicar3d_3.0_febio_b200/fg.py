@@ -126,6 +126,7 @@ def lib():
         L.fg_case_set_stream.argtypes = [vp, vp]
         L.fg_launch_count.argtypes = [C.POINTER(C.c_longlong)]
         L.fg_case_profile.argtypes = [vp, ip]
+        L.fg_case_history.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         L.fg_case_profile_read.argtypes = [vp, C.POINTER(Profile)]
         for name in ["fg_device_count", "fg_case_create", "fg_case_destroy", "fg_case_levels",
                      "fg_case_add_body", "fg_case_update_body", "fg_set_iblank_body_fast",
@@ -133,7 +134,8 @@ def lib():
                      "fg_get_band", "fg_case_set_geometry", "fg_mg_prepare", "fg_solve_poisson",
                      "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
                      "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy", "fg_case_set_stream",
-                     "fg_launch_count", "fg_case_profile", "fg_case_profile_read"]:
+                     "fg_launch_count", "fg_case_profile", "fg_case_profile_read",
+                     "fg_case_history"]:
             getattr(L, name).restype = ip
         _lib = L
     return _lib
@@ -308,6 +310,14 @@ class Case:
         e.g. ``torch.cuda.current_stream().cuda_stream``); None: own stream."""
         _check(lib().fg_case_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
                "fg_case_set_stream")
+
+    def history(self) -> np.ndarray:
+        """Relative residual after each cycle of the last solve."""
+        n = C.c_int(0)
+        _check(lib().fg_case_history(self.h, None, 0, C.byref(n)), "fg_case_history")
+        out = np.zeros(n.value)
+        _check(lib().fg_case_history(self.h, _p(out), n.value, C.byref(n)), "fg_case_history")
+        return out
 
     def profile(self, enable=True):
         _check(lib().fg_case_profile(self.h, 1 if enable else 0), "fg_case_profile")

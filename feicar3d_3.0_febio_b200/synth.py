@@ -460,6 +460,34 @@ def config1_body() -> Body:
     return sphere_body((4.0, 4.0, 4.0), 1.0, 6)
 
 
+def config2_grid() -> Grid:
+    """256x128x128 uniform cells on [0,8]x[0,4]x[0,4] (h = 1/32)."""
+    return Grid(uniform_nodes(256, 0, 8), uniform_nodes(128, 0, 4), uniform_nodes(128, 0, 4))
+
+
+def config2_plate() -> Body:
+    """Flat 1x1 plate of 2*64*64 triangles on the membrane path, thickness
+    factor * sqrt(dx^2+dy^2+dz^2) with factor 1 and h = 1/32, in its
+    reference position (leading edge on x = 0, the x-z plane)."""
+    return plate_body(n=64, size=1.0, tkns_factor=1.0, grid_h=1.0 / 32.0)
+
+
+CONFIG2_PIVOT = (2.0, 2.0, 2.0)
+
+
+def config2_verts(base: Body, step: int, period: int = 100, amp_deg: float = 30.0) -> np.ndarray:
+    """Plate vertices at time step ``step``: pitch amp*sin(2 pi step/period)
+    about the z-axis through the leading edge placed at (2, 2, 2)."""
+    ang = math.radians(amp_deg) * math.sin(2.0 * math.pi * step / period)
+    return pitch_plate(base, CONFIG2_PIVOT, ang)
+
+
+def config2_body(step: int) -> Body:
+    base = config2_plate()
+    return Body(verts=config2_verts(base, step), tri=base.tri, surface=2,
+                membrane_tkns=base.membrane_tkns)
+
+
 def small_grid(ncx=32, ncy=16, ncz=16, L=(4.0, 2.0, 2.0), stretch=None) -> Grid:
     ax = [uniform_nodes(ncx, 0, L[0])]
     if stretch:

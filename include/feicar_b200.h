@@ -182,6 +182,10 @@ typedef struct fg_profile {
                                                sweeps: 3s+1 per cell per
                                                direction, +s if omega!=1) */
 } fg_profile;
+/* Relative residual after each cycle of the last solve on c (the
+ * reference prints its per-cycle MG residuals with infoconv = 1,
+ * CORE_MG.F90:1811-1813): *count = cycles, relres[0..capacity-1] filled. */
+fg_status fg_case_history(const fg_case *c, double *relres, int capacity, int *count);
 /* enable != 0: later solves on c bracket each launch group with CUDA
  * events on the handle's stream; resets the totals. */
 fg_status fg_case_profile(fg_case *c, int enable);
