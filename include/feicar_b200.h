@@ -191,6 +191,38 @@ fg_status fg_case_history(const fg_case *c, double *relres, int capacity, int *c
 fg_status fg_case_profile(fg_case *c, int enable);
 fg_status fg_case_profile_read(const fg_case *c, fg_profile *out);
 
+/* ----- ghost/dead row relaxation without any allocation (no counterpart
+ * in the reference) -----
+ * For callers that cannot call cudaMalloc -- code that only gets device
+ * memory from a pool or framework it does not own, code where an
+ * allocation would stall the device or a latency budget, Fortran hosts
+ * passing arrays they manage themselves.  Runs `iterations` Jacobi passes
+ * of the interpolation rows (the update fg_ghostcell_pressure performs) on
+ * the caller's device field d_p, laid out like the reference arrays
+ * (0:nx+1, 0:ny+1, 0:nz+1), nx/ny/nz node counts.  Row r sets
+ *     p[tgt[r]] = sum_q w[8r+q] * p[cell[r] + corner_q] + c0[r]
+ * with corner_q the 8 corners of the host cell whose lower corner is the
+ * element cell[r], in the order of GCM_MEMORY_ALLOCATE.F90:593-623 (a
+ * target's own corner carries weight 0); all rows of a pass read the
+ * field before any row writes it.  tgt and cell are element indices of
+ * the field; rows whose indices leave the field are skipped.  d_c0 may be
+ * NULL (all zero).  Work is queued on `stream` (a cudaStream_t, NULL for
+ * the default stream) and the call returns without waiting.
+ * Scratch: a fixed device array of FG_NOALLOC_MAX_ROWS doubles (2 MiB),
+ * present on every GPU that loads the library until the process exits;
+ * nrows > FG_NOALLOC_MAX_ROWS returns FG_BAD_INPUT.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so
+ * make the first call on each device before any stream capture.  Every
+ * call on a device shares the one array: calls that overlap on the GPU
+ * (other streams, other host threads) race and must be ordered by the
+ * caller.  Nothing in it needs to start at zero -- each pass writes every
+ * value it reads. */
+#define FG_NOALLOC_MAX_ROWS 262144
+fg_status fg_rows_relax_noalloc(int nx, int ny, int nz, double *d_p, int nrows,
+                                const int64_t *d_tgt, const int64_t *d_cell,
+                                const double *d_w, const double *d_c0,
+                                int iterations, void *stream);
+
 /* ----- batched uneven solves: many cases per launch per MG stage ----- */
 typedef struct fg_batch fg_batch;
 fg_status fg_batch_create(int device, const fg_solver_config *cfg,
