@@ -68,6 +68,12 @@ def workload(name):
         return (synth.config1_grid(), synth.config1_body(),
                 "512x256x256 cells on [0,16]x[0,8]x[0,8], tanh-stretched (beta=2) in y,z; "
                 "sphere d=1 at (4,4,4), 81920-triangle icosphere")
+    if name == "slab512x256x128":
+        return (synth.Grid(synth.uniform_nodes(512, 0, 16), synth.tanh_nodes(256, 0, 8, 2.0),
+                           synth.tanh_nodes(128, 0, 4, 2.0)),
+                synth.sphere_body((4.0, 4.0, 2.0), 1.0, 5),
+                "512x256x128 cells on [0,16]x[0,8]x[0,4], tanh-stretched (beta=2) in y,z; "
+                "sphere d=1 at (4,4,2): x, y, z lines of 512, 256, 128 cells (kernel profiling case)")
     if name == "config0":
         return (synth.config0_grid(), synth.config0_body(),
                 "128x64x64 uniform cells on [0,8]x[0,4]x[0,4]; sphere d=1 at (2,2,2), "
@@ -190,6 +196,30 @@ def timed_device_solves(torch, fg, c, d_p, d_f, steps, stream):
     return evs[0].elapsed_time(evs[-1]), per, stats
 
 
+def run_kernels_only(torch, fg, synth, grid, c, geo, args, dev):
+    """One case, W warm-up and K timed solves, nothing else on the device
+    (the case a kernel profiler captures)."""
+    ib, gh, dd, G, D = geo
+    rows = [synth.Interp(D["ijk"], D["cell"], D["coefN"]), synth.Interp(G["ijk"], G["cell"], G["coefN"])]
+    rhs, _ = synth.manufactured_rhs(grid, ib, gh, dd, rows, seed=0)
+    stream = torch.cuda.Stream(device=dev)
+    c.set_stream(stream.cuda_stream)
+    d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).to(f"cuda:{dev}")
+    d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device=f"cuda:{dev}")
+    for _ in range(args.warmup):
+        timed_device_solves(torch, fg, c, d_p, d_f, 1, stream)
+    c.profile(True)
+    tot, per, stats = timed_device_solves(torch, fg, c, d_p, d_f, args.steps, stream)
+    prof = c.profile_read()
+    print(json.dumps({"workload": args.workload, "ms_per_solve": tot / args.steps,
+                      "cycles": stats[-1]["cycles"], "relres": stats[-1]["relres"],
+                      "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
+                      "classes_gbs": {k: round(v["bytes"] / 1e6 / v["ms"], 1)
+                                      for k, v in prof.items() if v["ms"] > 0 and v["bytes"] > 0}}),
+          flush=True)
+    c.close()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -222,6 +252,9 @@ def run_ours(args):
     t0 = time.time()
     prec_main = fg.FG_PREC_MIXED if args.precision == "mixed" else fg.FG_PREC_FP64
     c_main, geo = build_case(fg, synth, grid, body, prec_main, dev)
+    if args.kernels_only:
+        run_kernels_only(torch, fg, synth, grid, c_main, geo, args, dev)
+        return
     t_tag = time.time() - t0
     ib, gh, dd, G, D = geo
     rows = [synth.Interp(D["ijk"], D["cell"], D["coefN"]), synth.Interp(G["ijk"], G["cell"], G["coefN"])]
@@ -324,7 +357,7 @@ def run_ours(args):
             "data": "synthetic (seeded smoothed-noise RHS with known discrete solution; body tagged on device)",
             "config": {
                 "workload": args.workload, "desc": desc, "cells": cells,
-                "precision": args.precision, "rtol": RTOL, "cycle": "V(2,2) x/y/z zebra line relaxation",
+                "precision": args.precision, "rtol": RTOL, "cycle": "FGMRES(8) right-preconditioned by one V(2,2) cycle, x/y/z zebra line relaxation",
                 "parallelism": f"replicas x{world}",
                 "l2": "inputs larger than L2 (working set > 1 GB per solve)",
             },
@@ -468,6 +501,8 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="one case, timed solves only (for kernel profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -74,32 +74,39 @@ namespace fg {
 
 static long long pitch_up(long long v) { return (v + kRowPitch - 1) / kRowPitch * kRowPitch; }
 
+// Field arrays get kFieldPad elements in front of element 0, so element
+// (1, j, k) -- the first interior cell of every row -- starts on a
+// 16-element boundary for every element type (rows are 32-element
+// pitched): 16-byte vector loads of a line's cells from cell 1 on.
+constexpr long long kFieldPad = 15;
+template <typename T>
+static fg_status alloc_field(HLevel &L, T **p) {
+  void *raw = nullptr;
+  FG_CUDA(cudaMalloc(&raw, (size_t)(L.ntot + kFieldPad + 1) * sizeof(T)));
+  L.raw.push_back(raw);
+  FG_CUDA(cudaMemset(raw, 0, (size_t)(L.ntot + kFieldPad + 1) * sizeof(T)));
+  *p = reinterpret_cast<T *>(raw) + kFieldPad;
+  return FG_OK;
+}
+
 static fg_status alloc_level(fg_case *c, HLevel &L, bool lvl0) {
   L.nx = L.I - 1; L.ny = L.J - 1; L.nz = L.K - 1;
   L.sy = pitch_up(L.nx + 2);
   L.sz = L.sy * (L.ny + 2);
   L.ntot = L.sz * (L.nz + 2);
   const bool mixed = c->cfg.precision == FG_PREC_MIXED;
-  FG_CUDA(cudaMalloc(&L.d_type, L.ntot));
-  FG_CUDA(cudaMalloc(&L.d_mask, L.ntot));
-  FG_CUDA(cudaMemset(L.d_mask, 0, L.ntot));
+  fg_status st;
+  if ((st = alloc_field(L, &L.d_type)) != FG_OK) return st;
+  if ((st = alloc_field(L, &L.d_mask)) != FG_OK) return st;
   if (!mixed || lvl0) {
-    FG_CUDA(cudaMalloc(&L.d_x64, L.ntot * sizeof(double)));
-    FG_CUDA(cudaMalloc(&L.d_rhs64, L.ntot * sizeof(double)));
-    FG_CUDA(cudaMemset(L.d_x64, 0, L.ntot * sizeof(double)));
-    FG_CUDA(cudaMemset(L.d_rhs64, 0, L.ntot * sizeof(double)));
-    if (!mixed) {
-      FG_CUDA(cudaMalloc(&L.d_res64, L.ntot * sizeof(double)));
-      FG_CUDA(cudaMemset(L.d_res64, 0, L.ntot * sizeof(double)));
-    }
+    if ((st = alloc_field(L, &L.d_x64)) != FG_OK) return st;
+    if ((st = alloc_field(L, &L.d_rhs64)) != FG_OK) return st;
+    if (!mixed && (st = alloc_field(L, &L.d_res64)) != FG_OK) return st;
   }
   if (mixed) {
-    FG_CUDA(cudaMalloc(&L.d_x32, L.ntot * sizeof(float)));
-    FG_CUDA(cudaMalloc(&L.d_rhs32, L.ntot * sizeof(float)));
-    FG_CUDA(cudaMalloc(&L.d_res32, L.ntot * sizeof(float)));
-    FG_CUDA(cudaMemset(L.d_x32, 0, L.ntot * sizeof(float)));
-    FG_CUDA(cudaMemset(L.d_rhs32, 0, L.ntot * sizeof(float)));
-    FG_CUDA(cudaMemset(L.d_res32, 0, L.ntot * sizeof(float)));
+    if ((st = alloc_field(L, &L.d_x32)) != FG_OK) return st;
+    if ((st = alloc_field(L, &L.d_rhs32)) != FG_OK) return st;
+    if ((st = alloc_field(L, &L.d_res32)) != FG_OK) return st;
   }
   return FG_OK;
 }
@@ -314,6 +321,14 @@ struct fg_batch {
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
   std::vector<double> h_norm;
   std::vector<double> history;  // max relative residual over the batch after each cycle
+  // FGMRES state (outer == FG_OUTER_FGMRES): per problem 2m+3 FP64 vectors
+  // P, F, V_0..V_m, Z_0..Z_{m-1} of the finest level's layout
+  bool krylov = false;  // during an FGMRES solve: V-cycles in correction form
+  int km = 0;
+  std::vector<void *> kraw;
+  KDesc *d_kd = nullptr;
+  double *d_kpart = nullptr, *d_kout = nullptr, *d_kcoef = nullptr;
+  std::vector<double> h_kout, h_kcoef;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // optional CUDA-event timing of launch classes (fg_profile)
   struct Prof {
@@ -353,6 +368,11 @@ static void free_batch_tables(fg_batch *b) {
   cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
   cudaFree(b->d_norm); cudaFree(b->d_part);
   b->d_part = nullptr;
+  for (void *r : b->kraw) cudaFree(r);
+  b->kraw.clear();
+  cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
+  b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
+  b->km = 0;
   b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
   b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
@@ -384,6 +404,14 @@ static fg_status build_batch(fg_batch *b) {
     std::vector<const int *> gi;
     std::vector<int> gn;
     for (int p = 0; p < np; ++p) {
+      const fg_case *c = b->cases[p];
+      if (L < c->nlev - 1) {
+        s.maxnx = std::max(s.maxnx, c->lev[L].nx);
+        s.maxny = std::max(s.maxny, c->lev[L].ny);
+        s.maxnz = std::max(s.maxnz, c->lev[L].nz);
+      }
+    }
+    for (int p = 0; p < np; ++p) {
       fg_case *c = b->cases[p];
       if (L < c->nlev - 1) {
         s.S.push_back(p);
@@ -391,13 +419,10 @@ static fg_status build_batch(fg_batch *b) {
         vS.push_back(d);
         vSn.push_back(c->lev[L + 1].dl);
         bc.push_back(k::blocks_cells(d));
-        bx.push_back(k::blocks_xline(d));
-        by.push_back(k::blocks_tile(d, 1));
-        bz.push_back(k::blocks_tile(d, 2));
+        bx.push_back(k::blocks_xline(d, s.maxnx));
+        by.push_back(k::blocks_tile(d, 1, s.maxny));
+        bz.push_back(k::blocks_tile(d, 2, s.maxnz));
         bn.push_back(k::blocks_cells(c->lev[L + 1].dl));
-        s.maxnx = std::max(s.maxnx, d.nx);
-        s.maxny = std::max(s.maxny, d.ny);
-        s.maxnz = std::max(s.maxnz, d.nz);
         s.ncells += (double)d.nx * d.ny * d.nz;
       } else if (L == c->nlev - 1) {
         s.C.push_back(p);
@@ -533,7 +558,7 @@ template <typename T>
 static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
   auto &ls = b->ls[L];
   const double om = b->cfg.omega;
-  const int corr = sizeof(T) == 4 ? 1 : 0;
+  const int corr = (b->krylov || sizeof(T) == 4) ? 1 : 0;
   for (int axis = 0; axis < 3; ++axis) {
     const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
     const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
@@ -554,7 +579,7 @@ static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
 
 template <typename T>
 static fg_status vcycle(fg_batch *b, cudaStream_t s) {
-  const int corr = sizeof(T) == 4 ? 1 : 0;
+  const int corr = (b->krylov || sizeof(T) == 4) ? 1 : 0;
   fg_status st;
   for (int L = 0; L < b->maxdepth; ++L) {
     auto &ls = b->ls[L];
@@ -591,7 +616,10 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
 }
 
 // Outer iteration over the whole batch until every problem meets rtol.
+static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st);
+
 static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
+  if (b->cfg.outer == FG_OUTER_FGMRES) return batch_solve_fgmres(b, st);
   const int np = (int)b->cases.size();
   cudaStream_t s = b->stream;
   const bool mixed = b->cfg.precision == FG_PREC_MIXED;
@@ -659,6 +687,282 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     double mr = 0.0, mg = 0.0;
     for (int p = 0; p < np; ++p) { mr = std::max(mr, relres[p]); mg = std::max(mg, gres[p]); }
     st->cycles = cyc;
+    st->relres = mr;
+    st->ghost_res = mg;
+    st->seconds = tot * 1e-3;
+    double sm = 0.0;
+    for (double v : vms) sm += v;
+    st->vcycle_ms = vms.empty() ? 0.0 : sm / vms.size();
+  }
+  return status;
+}
+
+// ------------------------------------------------------------ FGMRES
+static int krylov_restart(const fg_solver_config &cfg) {
+  int m = cfg.restart > 0 ? cfg.restart : 10;
+  if (m < 2) m = 2;
+  if (m > KR_MAXV - 1) m = KR_MAXV - 1;
+  return m;
+}
+
+static fg_status ensure_krylov(fg_batch *b) {
+  const int m = krylov_restart(b->cfg);
+  if (b->km == m && b->d_kd) return FG_OK;
+  for (void *r : b->kraw) cudaFree(r);
+  b->kraw.clear();
+  cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
+  const int np = (int)b->cases.size();
+  const int nvec = 2 * m + 3;
+  std::vector<KDesc> kd(np);
+  for (int p = 0; p < np; ++p) {
+    const HLevel &L0 = b->cases[p]->lev[0];
+    void *raw = nullptr;
+    FG_CUDA(cudaMalloc(&raw, (size_t)nvec * L0.ntot * sizeof(double)));
+    b->kraw.push_back(raw);
+    FG_CUDA(cudaMemset(raw, 0, (size_t)nvec * L0.ntot * sizeof(double)));
+    kd[p].base = reinterpret_cast<double *>(raw);
+    kd[p].n = L0.ntot;
+  }
+  FG_CUDA(run_launch_set_alloc((void **)&b->d_kd, kd));
+  FG_CUDA(cudaMalloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * std::max(1, b->all0.blocks) * sizeof(double)));
+  FG_CUDA(cudaMalloc(&b->d_kout, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
+  FG_CUDA(cudaMalloc(&b->d_kcoef, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
+  b->h_kout.assign((size_t)np * (KR_MAXV + 2), 0.0);
+  b->h_kcoef.assign((size_t)np * (KR_MAXV + 2), 0.0);
+  b->km = m;
+  return FG_OK;
+}
+
+// Flexible GMRES(m) on the finest-level system (fluid rows of the 7-point
+// operator and the ghost/dead interpolation rows), right-preconditioned by
+// one V-cycle in correction form (FP32 in the mixed path, which is why the
+// flexible variant is used).  All problems of the batch iterate in
+// lockstep; each has its own Arnoldi basis, Hessenberg matrix and Givens
+// rotations (host).  Convergence: true fluid-row relative residual <= rtol
+// at a restart.
+static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
+  const int np = (int)b->cases.size();
+  cudaStream_t s = b->stream;
+  const bool mixed = b->cfg.precision == FG_PREC_MIXED;
+  fg_status r = ensure_krylov(b);
+  if (r != FG_OK) return r;
+  const int m = b->km;
+  const int VP = 0, VF = 1, V0 = 2, Z0 = 3 + m;
+  const int CS = KR_MAXV + 2;  // coefficient / output stride per problem
+  if (!b->ev0) { cudaEventCreate(&b->ev0); cudaEventCreate(&b->ev1); }
+  FG_CUDA(cudaEventRecord(b->ev0, s));
+  FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
+  FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
+  FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
+  std::vector<KDesc> kd(np);
+  for (int p = 0; p < np; ++p) {
+    const HLevel &L0 = b->cases[p]->lev[0];
+    kd[p] = KDesc{reinterpret_cast<double *>(b->kraw[p]), L0.ntot};
+    FG_CUDA(cudaMemcpyAsync(kd[p].base + VP * kd[p].n, L0.d_x64, L0.ntot * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(kd[p].base + VF * kd[p].n, L0.d_rhs64, L0.ntot * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+  }
+  b->krylov = true;
+  b->history.clear();
+  auto upload_coef = [&]() -> fg_status {
+    FG_CUDA(cudaMemcpyAsync(b->d_kcoef, b->h_kcoef.data(), b->h_kcoef.size() * sizeof(double),
+                            cudaMemcpyHostToDevice, s));
+    return FG_OK;
+  };
+  auto read_out = [&]() -> fg_status {
+    FG_CUDA(cudaMemcpyAsync(b->h_kout.data(), b->d_kout, b->h_kout.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    return FG_OK;
+  };
+  std::vector<double> f2(np, 0.0), relres(np, 1.0), beta(np, 0.0);
+  std::vector<double> H((size_t)np * (m + 1) * m, 0.0), g((size_t)np * (m + 1), 0.0);
+  std::vector<double> cs_((size_t)np * m, 0.0), sn_((size_t)np * m, 0.0);
+  std::vector<int> ncol(np, 0);
+  std::vector<char> done(np, 0);
+  auto Hx = [&](int p, int i, int j) -> double & { return H[((size_t)p * (m + 1) + i) * m + j]; };
+  int cycles = 0;
+  std::vector<double> vms;
+  cudaEvent_t va, vb;
+  cudaEventCreate(&va); cudaEventCreate(&vb);
+  fg_status status = FG_NOT_CONVERGED;
+  bool first = true;
+  fg_status err = FG_OK;
+  while (err == FG_OK) {
+    // ---- true residual V0 = F - A P, fluid norm, full norm
+    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
+    const size_t e_r = prof_begin(b, s);
+    FG_K(k::kr_resid(b->all0, b->rows, b->d_lev0, b->d_kd, VP, VF, V0, b->d_part, b->d_norm, s));
+    FG_K(k::kr_dots(b->all0, b->d_kd, V0, V0, 0, b->d_kpart, b->d_kout, CS, s));
+    prof_end(b, e_r, FG_PROF_RESIDUAL, 0.0, s);
+    FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if ((err = read_out()) != FG_OK) break;
+    bool all = true;
+    double worst = 0.0;
+    for (int p = 0; p < np; ++p) {
+      if (first) f2[p] = b->h_norm[np + p];
+      relres[p] = f2[p] > 0.0 ? std::sqrt(b->h_norm[p] / f2[p]) : std::sqrt(b->h_norm[p]);
+      beta[p] = std::sqrt(std::max(0.0, b->h_kout[(size_t)p * CS + 0]));
+      worst = std::max(worst, relres[p]);
+      done[p] = (relres[p] <= b->cfg.rtol || beta[p] == 0.0) ? 1 : 0;
+      if (!done[p]) all = false;
+    }
+    first = false;
+    b->history.push_back(worst);
+    if (all) { status = FG_OK; break; }
+    if (cycles >= b->cfg.max_cycles) break;
+    // ---- V0 /= beta
+    for (int p = 0; p < np; ++p) {
+      b->h_kcoef[(size_t)p * CS] = done[p] ? 0.0 : 1.0 / beta[p];
+      ncol[p] = 0;
+      for (int i = 0; i <= m; ++i) g[(size_t)p * (m + 1) + i] = 0.0;
+      g[(size_t)p * (m + 1)] = beta[p];
+    }
+    if ((err = upload_coef()) != FG_OK) break;
+    FG_K(k::kr_axpy(b->all0, b->d_kd, V0, V0, 0, b->d_kcoef, CS, s));
+    int jlast = 0;
+    for (int j = 0; j < m && cycles < b->cfg.max_cycles; ++j) {
+      // ---- Z_j = M^-1 V_j (one V-cycle from zero, correction form)
+      size_t e0 = prof_begin(b, s);
+      if (mixed) FG_K(k::kr_stage<float>(b->all0, b->rows, b->d_lev0, b->d_kd, V0 + j, s));
+      else FG_K(k::kr_stage<double>(b->all0, b->rows, b->d_lev0, b->d_kd, V0 + j, s));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+      cudaEventRecord(va, s);
+      r = mixed ? vcycle<float>(b, s) : vcycle<double>(b, s);
+      if (r != FG_OK) { err = r; break; }
+      cudaEventRecord(vb, s);
+      ++cycles;
+      e0 = prof_begin(b, s);
+      if (mixed) FG_K(k::kr_unstage<float>(b->all0, b->d_kd, Z0 + j, s));
+      else FG_K(k::kr_unstage<double>(b->all0, b->d_kd, Z0 + j, s));
+      // ---- W = A Z_j into V_{j+1}; inner products with V_0..V_j and |W|^2
+      FG_K(k::kr_apply(b->all0, b->rows, b->d_lev0, b->d_kd, Z0 + j, V0 + j + 1, s));
+      FG_K(k::kr_dots(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kpart, b->d_kout, CS, s));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+      if ((err = read_out()) != FG_OK) break;
+      {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, va, vb);
+        vms.push_back(ms);
+      }
+      // classical Gram-Schmidt; a second pass where it cancelled badly
+      bool reorth = false;
+      std::vector<double> hcol((size_t)np * (j + 2), 0.0), ww(np, 0.0);
+      for (int p = 0; p < np; ++p) {
+        const double *o = &b->h_kout[(size_t)p * CS];
+        double sum = 0.0;
+        for (int i = 0; i <= j; ++i) { hcol[(size_t)p * (j + 2) + i] = o[i]; sum += o[i] * o[i]; }
+        ww[p] = o[j + 1];
+        if (!done[p] && ww[p] - sum < 0.5 * ww[p]) reorth = true;
+      }
+      if (reorth) {
+        for (int p = 0; p < np; ++p) {
+          double *cf = &b->h_kcoef[(size_t)p * CS];
+          cf[0] = 1.0;
+          for (int i = 0; i <= j; ++i) cf[1 + i] = done[p] ? 0.0 : -hcol[(size_t)p * (j + 2) + i];
+        }
+        if ((err = upload_coef()) != FG_OK) break;
+        e0 = prof_begin(b, s);
+        FG_K(k::kr_axpy(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kcoef, CS, s));
+        FG_K(k::kr_dots(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kpart, b->d_kout, CS, s));
+        prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+        if ((err = read_out()) != FG_OK) break;
+      }
+      // normalise: V_{j+1} = (W - sum h_i V_i) / h_{j+1}
+      for (int p = 0; p < np; ++p) {
+        double *cf = &b->h_kcoef[(size_t)p * CS];
+        const double *o = &b->h_kout[(size_t)p * CS];
+        double sum = 0.0;
+        for (int i = 0; i <= j; ++i) {
+          const double hi = o[i];  // second-pass corrections when reorthogonalised
+          if (reorth) hcol[(size_t)p * (j + 2) + i] += hi;
+          sum += hi * hi;
+        }
+        const double h2 = o[j + 1] - sum;
+        const double hn = h2 > 0.0 ? std::sqrt(h2) : 0.0;
+        hcol[(size_t)p * (j + 2) + j + 1] = hn;
+        const bool brk = done[p] || !(hn > 1e-14 * beta[p]);
+        cf[0] = brk ? 0.0 : 1.0 / hn;
+        for (int i = 0; i <= j; ++i) cf[1 + i] = brk ? 0.0 : -o[i] / hn;
+        if (done[p]) continue;
+        // Hessenberg column j, previous rotations, new rotation
+        for (int i = 0; i <= j + 1; ++i) Hx(p, i, j) = hcol[(size_t)p * (j + 2) + i];
+        for (int i = 0; i < j; ++i) {
+          const double c = cs_[(size_t)p * m + i], sv = sn_[(size_t)p * m + i];
+          const double h0 = Hx(p, i, j), h1 = Hx(p, i + 1, j);
+          Hx(p, i, j) = c * h0 + sv * h1;
+          Hx(p, i + 1, j) = -sv * h0 + c * h1;
+        }
+        const double a = Hx(p, j, j), bb = Hx(p, j + 1, j);
+        const double rr = std::hypot(a, bb);
+        const double c = rr > 0.0 ? a / rr : 1.0, sv = rr > 0.0 ? bb / rr : 0.0;
+        cs_[(size_t)p * m + j] = c; sn_[(size_t)p * m + j] = sv;
+        Hx(p, j, j) = rr; Hx(p, j + 1, j) = 0.0;
+        double *gp = &g[(size_t)p * (m + 1)];
+        gp[j + 1] = -sv * gp[j];
+        gp[j] = c * gp[j];
+        ncol[p] = j + 1;
+        if (brk) done[p] = 1;
+      }
+      if ((err = upload_coef()) != FG_OK) break;
+      e0 = prof_begin(b, s);
+      FG_K(k::kr_axpy(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kcoef, CS, s));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+      jlast = j + 1;
+      // residual estimate |g_{j+1}| (all rows) over the fluid-row |f|
+      bool inner_done = true;
+      double west = 0.0;
+      for (int p = 0; p < np; ++p) {
+        const double est = std::fabs(g[(size_t)p * (m + 1) + ncol[p]]);
+        const double rel = f2[p] > 0.0 ? est / std::sqrt(f2[p]) : est;
+        west = std::max(west, rel);
+        if (!(done[p] || rel <= 0.5 * b->cfg.rtol)) inner_done = false;
+      }
+      b->history.push_back(west);
+      if (inner_done) break;
+    }
+    if (err != FG_OK) break;
+    // ---- P += sum_i y_i Z_i, y from the rotated Hessenberg system
+    for (int p = 0; p < np; ++p) {
+      double *cf = &b->h_kcoef[(size_t)p * CS];
+      for (int i = 0; i < CS; ++i) cf[i] = 0.0;
+      cf[0] = 1.0;
+      const int nc = ncol[p];
+      std::vector<double> y(nc, 0.0);
+      for (int i = nc - 1; i >= 0; --i) {
+        double v = g[(size_t)p * (m + 1) + i];
+        for (int q = i + 1; q < nc; ++q) v -= Hx(p, i, q) * y[q];
+        y[i] = Hx(p, i, i) != 0.0 ? v / Hx(p, i, i) : 0.0;
+      }
+      for (int i = 0; i < nc; ++i) cf[1 + i] = y[i];
+    }
+    if ((err = upload_coef()) != FG_OK) break;
+    if (jlast > 0) FG_K(k::kr_axpy(b->all0, b->d_kd, VP, Z0, jlast, b->d_kcoef, CS, s));
+  }
+  cudaEventDestroy(va); cudaEventDestroy(vb);
+  b->krylov = false;
+  if (err != FG_OK) return err;
+  // solution back into the finest-level field; ghost-row residual for stats
+  for (int p = 0; p < np; ++p) {
+    const HLevel &L0 = b->cases[p]->lev[0];
+    FG_CUDA(cudaMemcpyAsync(L0.d_x64, kd[p].base + VP * kd[p].n, L0.ntot * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(L0.d_rhs64, kd[p].base + VF * kd[p].n, L0.ntot * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+  }
+  FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
+  FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+  FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaEventRecord(b->ev1, s));
+  FG_CUDA(cudaEventSynchronize(b->ev1));
+  float tot = 0.0f;
+  cudaEventElapsedTime(&tot, b->ev0, b->ev1);
+  if (b->prof.on) prof_collect(b);
+  if (st) {
+    double mr = 0.0, mg = 0.0;
+    for (int p = 0; p < np; ++p) { mr = std::max(mr, relres[p]); mg = std::max(mg, b->h_norm[2 * np + p]); }
+    st->cycles = cycles;
     st->relres = mr;
     st->ghost_res = mg;
     st->seconds = tot * 1e-3;
@@ -840,7 +1144,8 @@ void fg_default_config(fg_solver_config *cfg) {
   if (!cfg) return;
   memset(cfg, 0, sizeof(*cfg));
   cfg->precision = FG_PREC_FP64;
-  cfg->outer = FG_OUTER_RICHARDSON;
+  cfg->outer = FG_OUTER_FGMRES;
+  cfg->restart = 8;
   cfg->nu1 = 2;
   cfg->nu2 = 2;
   cfg->omega = 1.0;
@@ -912,9 +1217,9 @@ fg_status fg_case_destroy(fg_case *c) {
   if (c->solo) { fg_batch_destroy(c->solo); c->solo = nullptr; }
   for (int l = 0; l < c->nlev; ++l) {
     HLevel &L = c->lev[l];
-    cudaFree(L.d_type); cudaFree(L.d_mask); cudaFree(L.d_coef); cudaFree(L.d_int);
-    cudaFree(L.d_x64); cudaFree(L.d_rhs64); cudaFree(L.d_res64);
-    cudaFree(L.d_x32); cudaFree(L.d_rhs32); cudaFree(L.d_res32);
+    cudaFree(L.d_coef); cudaFree(L.d_int);
+    for (void *r : L.raw) cudaFree(r);
+    L.raw.clear();
   }
   cudaFree(c->d_G); cudaFree(c->d_gidx); cudaFree(c->d_pin); cudaFree(c->d_fin);
   cudaFree(c->d_gauge);

@@ -31,6 +31,7 @@ struct HLevel {
   int *d_int = nullptr;      // packed 1-D int arrays
   double *d_x64 = nullptr, *d_rhs64 = nullptr, *d_res64 = nullptr;
   float *d_x32 = nullptr, *d_rhs32 = nullptr, *d_res32 = nullptr;
+  std::vector<void *> raw;   // allocations behind the offset field pointers
   DevLevel dl{};
 };
 

@@ -148,12 +148,21 @@ long long launches_so_far();
     }                                                                  \
   } while (0)
 
+// Krylov vectors of one problem (FGMRES outer iteration): nvec FP64 fields
+// of the finest level's layout, n elements each, vector v at base + v*n
+struct KDesc {
+  double *base;
+  long long n;
+};
+constexpr int KR_MAXV = 16;  // most vectors one dot-product pass reads
+
 // kernel launchers (fg_mg.cu)
 namespace k {
 // blocks needed by one problem's level for each kernel family
 int blocks_cells(const DevLevel &L);
-int blocks_xline(const DevLevel &L);
-int blocks_tile(const DevLevel &L, int axis);
+int blocks_xline(const DevLevel &L, int maxn);
+// y/z tiles: blocks depend on the kernel the level set's longest line picks
+int blocks_tile(const DevLevel &L, int axis, int maxn);
 size_t smem_line(int n, int tsize, int axis);
 
 template <typename T>
@@ -193,6 +202,25 @@ cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, lon
 cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz,
                          const int *pbc, const double *ppp, int gauge, double *scratch,
                          cudaStream_t s);
+// FGMRES pieces over the finest level of a batch (Launch of all level-0
+// cells; rows of all problems).  kr_resid: vd = F - A P (and rows), norm2[p]
+// += fluid-row |r|^2; kr_apply: vd = A vs; kr_dots: out[p*ostride + i] =
+// (vw, v0+i) for i < nv, out[p*ostride + nv] = (vw, vw); kr_axpy: vd =
+// coef[p*cs]*vd + sum_i coef[p*cs+1+i] vec(s0+i); kr_stage/kr_unstage move
+// a vector into / out of the precision-T correction arrays of level 0.
+cudaError_t kr_resid(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vp,
+                     int vf, int vd, double *part, double *norm2, cudaStream_t s);
+cudaError_t kr_apply(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
+                     int vd, cudaStream_t s);
+cudaError_t kr_dots(const Launch &L0, const KDesc *kd, int vw, int v0, int nv, double *part, double *out,
+                    int ostride, cudaStream_t s);
+cudaError_t kr_axpy(const Launch &L0, const KDesc *kd, int vd, int s0, int ns, const double *coef, int cs,
+                    cudaStream_t s);
+template <typename T>
+cudaError_t kr_stage(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
+                     cudaStream_t s);
+template <typename T>
+cudaError_t kr_unstage(const Launch &L0, const KDesc *kd, int vd, cudaStream_t s);
 }  // namespace k
 
 }  // namespace fg

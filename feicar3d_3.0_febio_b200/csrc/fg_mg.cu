@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <string.h>
 #include <stdint.h>
 
 #include "fg_internal.h"
@@ -371,6 +372,339 @@ __device__ __forceinline__ long long dyn_smem_bytes() {
 __host__ __device__ __forceinline__ int line_pad(int n) { return n + 33; }
 __host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
 
+// ------------------------------------------- register-staged line kernels
+// M consecutive elements of a row (16-byte aligned start, see the field
+// padding of the allocator) into registers.
+template <typename T, int M, typename P>
+__device__ __forceinline__ void load_run(T (&v)[M], const P &base, long long off) {
+#ifdef FG_CHECKED
+#pragma unroll
+  for (int q = 0; q < M; ++q) v[q] = base[off + q];
+#else
+  static_assert((M * sizeof(T)) % 4 == 0, "run of at least 4 bytes");
+  const T *src = &base[off];
+  if constexpr ((M * sizeof(T)) % 16 == 0) {
+    const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+#pragma unroll
+    for (int u = 0; u < (int)(M * sizeof(T) / 16); ++u) {
+      const uint4 w = s4[u];
+      memcpy(&v[u * (16 / sizeof(T))], &w, 16);
+    }
+  } else if constexpr ((M * sizeof(T)) % 8 == 0) {
+    const uint2 *s2 = reinterpret_cast<const uint2 *>(src);
+#pragma unroll
+    for (int u = 0; u < (int)(M * sizeof(T) / 8); ++u) {
+      const uint2 w = s2[u];
+      memcpy(&v[u * (8 / sizeof(T))], &w, 8);
+    }
+  } else {
+    const unsigned w = *reinterpret_cast<const unsigned *>(src);
+    memcpy(&v[0], &w, 4);
+  }
+#endif
+}
+
+template <typename T, int M, typename P>
+__device__ __forceinline__ void store_run(const P &base, long long off, const T (&v)[M], int valid) {
+#ifndef FG_CHECKED
+  if (valid >= M) {
+    T *dst = &base[off];
+    if constexpr ((M * sizeof(T)) % 16 == 0) {
+      uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+#pragma unroll
+      for (int u = 0; u < (int)(M * sizeof(T) / 16); ++u) {
+        uint4 w;
+        memcpy(&w, &v[u * (16 / sizeof(T))], 16);
+        d4[u] = w;
+      }
+      return;
+    }
+  }
+#endif
+#pragma unroll
+  for (int q = 0; q < M; ++q)
+    if (q < valid) base[off + q] = v[q];
+}
+
+// Parallel cyclic reduction of W equations A x_{l-1} + B x_l + C x_{l+1}
+// = D held one per lane of a W-lane segment of the warp (sl = lane within
+// the segment; A of the first and C of the last are zero); returns x of
+// this lane.  One reciprocal per step (rcp_nr).
+template <typename T, int W>
+__device__ __forceinline__ T pcr_seg(T A, T B, T Cc, T D, int sl) {
+#pragma unroll
+  for (int t = 1; t < W; t <<= 1) {
+    const T ib = rcp_nr(B);
+    T la = __shfl_up_sync(0xffffffffu, A, t, W), lc2 = __shfl_up_sync(0xffffffffu, Cc, t, W);
+    T ld = __shfl_up_sync(0xffffffffu, D, t, W), lib = __shfl_up_sync(0xffffffffu, ib, t, W);
+    T ra = __shfl_down_sync(0xffffffffu, A, t, W), rc = __shfl_down_sync(0xffffffffu, Cc, t, W);
+    T rd = __shfl_down_sync(0xffffffffu, D, t, W), rib = __shfl_down_sync(0xffffffffu, ib, t, W);
+    if (sl < t) { la = T(0); lc2 = T(0); ld = T(0); lib = T(0); }
+    if (sl + t >= W) { ra = T(0); rc = T(0); rd = T(0); rib = T(0); }
+    const T k1 = A * lib, k2 = Cc * rib;
+    const T nA = -la * k1, nC = -rc * k2;
+    const T nB = B - lc2 * k1 - ra * k2;
+    const T nD = D - ld * k1 - rd * k2;
+    A = nA; Cc = nC; B = nB; D = nD;
+  }
+  return D / B;
+}
+
+// One chunk of M consecutive rows of a line, held by one thread: the rows'
+// right-hand sides d (held rows: their current value) and masks mk (0 for
+// held rows) are given; the row coefficients come from the mask and the
+// axis coefficients am/ap.  Eliminates the chunk down and up (partition
+// method): afterwards x_u = d_u - al_u F - ga_u L for 0 < u < M-1, with F
+// = x_0 and L = x_{M-1}, and the chunk's F/L equations are
+//     aF L_prev + bF F + cF L = dF,   L = dL - aL F - cL F_next.
+// Rows r >= n (past the line end) are identities.
+template <typename T, int M, typename PA>
+__device__ __forceinline__ void chunk_eliminate(int r0, int n, const uint8_t (&mk)[M], T (&d)[M],
+                                                T (&al)[M], T (&ga)[M], const PA &am_,
+                                                const PA &ap_, const LineCoef &lc, T &aF, T &bF,
+                                                T &cF, T &dF, T &aL, T &cL, T &dL) {
+  T a0 = T(0), b0 = T(1), c0 = T(0), d0 = T(0);
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    T a = T(0), b = T(1), c = T(0), dd = T(0);
+    if (r < n) {
+      const uint8_t m8 = mk[u];
+      dd = d[u];
+      if (m8 & 64) {
+        const double am = am_[1 + r], ap = ap_[1 + r];
+        double diag = -lc.tdir;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if ((m8 >> lc.qt[t]) & 1) diag -= lc.tq[t];
+        const bool cm = (m8 >> lc.qm) & 1, cp = (m8 >> lc.qp) & 1;
+        if (cm) diag -= am; else if (r == 0 && lc.dirm) diag -= 2.0 * am;
+        if (cp) diag -= ap; else if (r == n - 1 && lc.dirp) diag -= 2.0 * ap;
+        a = cm ? (T)am : T(0);
+        c = cp ? (T)ap : T(0);
+        b = (T)diag;
+      }
+    }
+    if (u == 0) {
+      a0 = a; b0 = b; c0 = c; d0 = dd;
+    } else if (u == 1) {
+      const T rr = rcp_nr(b);
+      al[1] = a * rr; ga[1] = c * rr; d[1] = dd * rr;
+    } else {
+      const T rr = rcp_nr(b - a * ga[u - 1]);
+      al[u] = -a * al[u - 1] * rr;
+      ga[u] = c * rr;
+      d[u] = (dd - a * d[u - 1]) * rr;
+    }
+  }
+  aL = al[M - 1]; cL = ga[M - 1]; dL = d[M - 1];
+  T pa = T(0), pb = T(-1), pd = T(0);
+#pragma unroll
+  for (int u = M - 2; u >= 1; --u) {
+    const T nd = d[u] - ga[u] * pd;
+    const T na = al[u] - ga[u] * pa;
+    const T nb = -ga[u] * pb;
+    al[u] = na; ga[u] = nb; d[u] = nd;
+    pa = na; pb = nb; pd = nd;
+  }
+  aF = a0; bF = b0 - c0 * pa; cF = -c0 * pb; dF = d0 - c0 * pd;
+}
+
+// Zebra x-line relaxation, lines (j,k) with (j+k)%2 == color, W lanes per
+// line (32/W lines per warp).  Lane l of a line owns rows [M l, M l + M),
+// loaded straight into registers with 16-byte loads (rows past the line
+// end are identity equations), eliminates them down and up, and the W
+// chunk-first unknowns are solved by PCR across the line's lanes.  One
+// pass over rhs, mask, the line's own values and its four neighbour
+// lines; no shared memory.
+template <typename T, int M, int W>
+__global__ void __launch_bounds__(XL_WARPS * 32, 1)
+k_xline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sl = lane % W;
+  const int nyh = (L.ny + 1) >> 1;
+  const int q = (lb * XL_WARPS + warp) * (32 / W) + lane / W;
+  int k = 1 + q / nyh;
+  const int jj = q % nyh;
+  int j = ((((1 + k) & 1) == color) ? 1 : 2) + 2 * jj;
+  const bool line_ok = k <= L.nz && j <= L.ny;
+  if (!line_ok) { k = 1; j = 1; }  // idle segment: identity rows, no loads or stores
+  const int n = L.nx;
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  const LineCoef lc = line_coef(L, 0, 1, j, k);
+  const long long row = L.sy * j + L.sz * k + 1;  // cell i = 1
+  const int r0 = sl * M;
+  const bool any = line_ok && r0 < n;
+  T d[M], al[M], ga[M];
+  uint8_t mk[M];
+#pragma unroll
+  for (int u = 0; u < M; ++u) { d[u] = T(0); mk[u] = 0; }
+  const bool iso_line = lc.tdir == 0.0 && !lc.dirm && !lc.dirp;
+  if (any) {
+    // every load of the chunk is issued before the first use
+    T nb[4][M], xv[M];
+    load_run<T, M>(d, rhs, row + r0);
+    load_run<uint8_t, M>(mk, L.mask, row + r0);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) load_run<T, M>(nb[t], x, row + r0 + lc.to[t]);
+    load_run<T, M>(xv, x, row + r0);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const T cq = (T)lc.tq[t];
+#pragma unroll
+      for (int u = 0; u < M; ++u)
+        if ((mk[u] >> lc.qt[t]) & 1) d[u] -= cq * nb[t][u];
+    }
+#pragma unroll
+    for (int u = 0; u < M; ++u) {
+      const bool held = !(mk[u] & 64) || (((mk[u] & 63) == 0) && iso_line);
+      if (held) { d[u] = xv[u]; mk[u] = 0; }
+    }
+  }
+  T aF, bF, cF, dF, aL, cL, dL;
+  chunk_eliminate<T, M>(r0, any ? n : r0, mk, d, al, ga, L.amx, L.apx, lc, aF, bF, cF, dF, aL, cL, dL);
+  // reduced system in the chunk-first unknowns F_l
+  T aLp = __shfl_up_sync(0xffffffffu, aL, 1, W);
+  T cLp = __shfl_up_sync(0xffffffffu, cL, 1, W);
+  T dLp = __shfl_up_sync(0xffffffffu, dL, 1, W);
+  if (sl == 0) { aLp = T(0); cLp = T(0); dLp = T(0); }
+  const T xF = pcr_seg<T, W>(-aF * aLp, bF - aF * cLp - cF * aL, -cF * cL, dF - aF * dLp - cF * dL, sl);
+  const T xFn = __shfl_down_sync(0xffffffffu, xF, 1, W);
+  if (!any) return;
+  const T xL = dL - aL * xF - cL * (sl + 1 < W ? xFn : T(0));
+  T out[M];
+  out[0] = xF;
+#pragma unroll
+  for (int u = 1; u < M - 1; ++u) out[u] = d[u] - al[u] * xF - ga[u] * xL;
+  out[M - 1] = xL;
+  if (omega != T(1)) {
+    T xo[M];
+    load_run<T, M>(xo, x, row + r0);
+#pragma unroll
+    for (int u = 0; u < M; ++u) out[u] = xo[u] + omega * (out[u] - xo[u]);
+  }
+  const int valid = n - r0 < M ? n - r0 : M;
+  store_run<T, M>(x, row + r0, out, valid);
+}
+
+// Zebra line relaxation along y (AXIS 1, lines (i,k), colour (i+k)%2) or z
+// (AXIS 2, lines (i,j), colour (i+j)%2).  A block takes the 32 lines of
+// one colour in a 64-cell i-tile (lane l: i = i0 + par + 2l, so every
+// load of a warp spans 64 consecutive cells) and CH warps, warp w holding
+// rows [M w, M w + M) of all 32 lines in registers.  Each thread
+// eliminates its chunk down and up; the CH chunk equations of a line go
+// through shared memory and one thread per line solves them (Thomas),
+// then every thread back-substitutes its rows.
+constexpr int YZ_MAXROWS = 256;  // longest line of k_yzline_reg (M 16 x CH 16)
+template <typename T>
+struct ChunkEq { T a, b, c, d; };
+
+template <typename T, int M, int CH, int AXIS>
+__global__ void __launch_bounds__(CH * 32)
+k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+  __shared__ T s_lc[CH][32][3];   // last-row equation of each chunk
+  __shared__ ChunkEq<T> s_eq[CH][32];
+  __shared__ T s_f[CH + 1][32];   // chunk-first unknowns
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const int ntx = (L.nx + 63) >> 6;
+  const int ti = lb % ntx;
+  const int o = 1 + lb / ntx;  // k for AXIS 1, j for AXIS 2
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i0 = 1 + 64 * ti;
+  const int par = (color + i0 + o) & 1;
+  const int i = i0 + par + 2 * lane;
+  const bool valid = i <= L.nx;
+  const int n = AXIS == 1 ? L.ny : L.nz;
+  const long long ls = AXIS == 1 ? L.sy : L.sz;  // row stride along the line
+  const long long os = AXIS == 1 ? L.sz : L.sy;  // stride of the fixed index
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  const LineCoef lc = line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
+  const long long base = (long long)(valid ? i : L.nx) + os * o;  // row index 0 of the line
+  const int r0 = w * M;
+  const bool any = valid && r0 < n;
+  T d[M], al[M], ga[M];
+  uint8_t mk[M];
+  const bool iso_line = lc.tdir == 0.0 && !lc.dirm && !lc.dirp;
+  // all loads of a row are issued unconditionally (none waits on the mask)
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    d[u] = T(0); mk[u] = 0;
+    if (any && r < n) {
+      const long long id = base + ls * (r + 1);
+      uint8_t m8 = L.mask[id];
+      const T rv = rhs[id];
+      const T xv = x[id];
+      T nb[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) nb[t] = x[id + lc.to[t]];
+      T acc = rv;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) acc -= ((m8 >> lc.qt[t]) & 1) ? (T)lc.tq[t] * nb[t] : T(0);
+      const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+      if (held) { acc = xv; m8 = 0; }
+      d[u] = acc;
+      mk[u] = m8;
+    }
+  }
+  T aF, bF, cF, dF, aL, cL, dL;
+  chunk_eliminate<T, M>(r0, any ? n : r0, mk, d, al, ga, AXIS == 1 ? L.amy : L.amz,
+                        AXIS == 1 ? L.apy : L.apz, lc, aF, bF, cF, dF, aL, cL, dL);
+  s_lc[w][lane][0] = aL; s_lc[w][lane][1] = cL; s_lc[w][lane][2] = dL;
+  __syncthreads();
+  {
+    T aLp = T(0), cLp = T(0), dLp = T(0);
+    if (w > 0) { aLp = s_lc[w - 1][lane][0]; cLp = s_lc[w - 1][lane][1]; dLp = s_lc[w - 1][lane][2]; }
+    ChunkEq<T> e;
+    e.a = -aF * aLp;
+    e.b = bF - aF * cLp - cF * aL;
+    e.c = -cF * cL;
+    e.d = dF - aF * dLp - cF * dL;
+    s_eq[w][lane] = e;
+  }
+  __syncthreads();
+  if (w == 0) {
+    // Thomas over the chunk equations of line `lane` (chunks past the line
+    // end are identities); the forward sweep is kept in place
+    T cprev = T(0), dprev = T(0);
+    for (int q = 0; q < CH; ++q) {
+      const ChunkEq<T> e = s_eq[q][lane];
+      const T rr = rcp_nr(e.b - e.a * cprev);
+      cprev = e.c * rr;
+      dprev = (e.d - e.a * dprev) * rr;
+      s_eq[q][lane].c = cprev;
+      s_eq[q][lane].d = dprev;
+    }
+    T xn = T(0);
+    for (int q = CH - 1; q >= 0; --q) {
+      xn = s_eq[q][lane].d - s_eq[q][lane].c * xn;
+      s_f[q][lane] = xn;
+    }
+    s_f[CH][lane] = T(0);
+  }
+  __syncthreads();
+  if (!any) return;
+  const T xF = s_f[w][lane];
+  const T xFn = s_f[w + 1][lane];
+  const T xL = dL - aL * xF - cL * xFn;
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    if (r >= n) break;
+    T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+    const long long id = base + ls * (r + 1);
+    if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+    x[id] = v;
+  }
+}
+
 // ------------------------------------------------------- x-line kernel
 // Lines (j,k) with (j+k)%2 == color; one warp per line.
 template <typename T, int MAXM>
@@ -518,12 +852,16 @@ k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
 int blocks_cells(const DevLevel &L) {
   return ((L.nx + CELL_BLOCK - 1) / CELL_BLOCK) * ((L.ny * L.nz + CELL_ROWS - 1) / CELL_ROWS);
 }
-int blocks_xline(const DevLevel &L) {
-  long long lines = (long long)((L.ny + 1) / 2) * L.nz;
-  return (int)((lines + XL_WARPS - 1) / XL_WARPS);
+// lanes per x line of k_xline_reg for a level set whose longest x line is maxn
+int xline_lanes(int maxn) { return maxn <= 16 ? 4 : maxn <= 32 ? 8 : maxn <= 64 ? 16 : 32; }
+int blocks_xline(const DevLevel &L, int maxn) {
+  const long long lines = (long long)((L.ny + 1) / 2) * L.nz;
+  const long long per_block = (long long)XL_WARPS * (32 / xline_lanes(maxn));
+  return (int)((lines + per_block - 1) / per_block);
 }
-int blocks_tile(const DevLevel &L, int axis) {
-  int ntx = (L.nx + TILE_I - 1) / TILE_I;
+int blocks_tile(const DevLevel &L, int axis, int maxn) {
+  const int w = maxn <= YZ_MAXROWS ? 64 : TILE_I;  // k_yzline_reg or k_yzline
+  const int ntx = (L.nx + w - 1) / w;
   return ntx * (axis == 1 ? L.nz : L.ny);
 }
 // dynamic shared memory of a line launch: axis 0 uses the per-warp layout
@@ -566,10 +904,48 @@ static cudaError_t launch_line(const Launch &Lr, int axis, int color, double ome
 }
 
 // maxn: the longest line of this launch along `axis`
+template <typename T, int M, int W>
+static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaStream_t s) {
+  k_xline_reg<T, M, W><<<Lr.blocks, XL_WARPS * 32, 0, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename T, int M, int CH>
+static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
+  if (axis == 1)
+    k_yzline_reg<T, M, CH, 1><<<Lr.blocks, CH * 32, 0, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  else
+    k_yzline_reg<T, M, CH, 2><<<Lr.blocks, CH * 32, 0, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+// x lines always take the register kernel (lines up to 1024 cells; lines
+// per warp as xline_lanes); y/z lines up to YZ_MAXROWS cells take
+// k_yzline_reg, longer ones the shared-memory tile kernel (blocks_tile and
+// blocks_xline count blocks the same way)
 template <typename T>
 cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int maxn,
                        cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
+  if (axis == 0) {
+    if (maxn <= 16) return launch_xreg<T, 4, 4>(Lr, color, omega, s);
+    if (maxn <= 32) return launch_xreg<T, 4, 8>(Lr, color, omega, s);
+    if (maxn <= 64) return launch_xreg<T, 4, 16>(Lr, color, omega, s);
+    if (maxn <= 128) return launch_xreg<T, 4, 32>(Lr, color, omega, s);
+    if (maxn <= 256) return launch_xreg<T, 8, 32>(Lr, color, omega, s);
+    if (maxn <= 512) return launch_xreg<T, 16, 32>(Lr, color, omega, s);
+    if (maxn <= 1024) return launch_xreg<T, 32, 32>(Lr, color, omega, s);
+    return cudaErrorInvalidValue;  // lines longer than 1024 cells
+  }
+  if (maxn <= YZ_MAXROWS) {
+    if (maxn <= 16) return launch_yzreg<T, 4, 4>(Lr, axis, color, omega, s);
+    if (maxn <= 32) return launch_yzreg<T, 4, 8>(Lr, axis, color, omega, s);
+    if (maxn <= 64) return launch_yzreg<T, 4, 16>(Lr, axis, color, omega, s);
+    if (maxn <= 128) return launch_yzreg<T, 8, 16>(Lr, axis, color, omega, s);
+    return launch_yzreg<T, 16, 16>(Lr, axis, color, omega, s);
+  }
   int P, base, rem;
   chunking(maxn, P, base, rem);
   const int m = base + (rem ? 1 : 0);
@@ -1095,6 +1471,266 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
   }
   return cudaGetLastError();
 }
+
+// ------------------------------------------------------------- FGMRES
+// Krylov vectors of one problem: `nvec` FP64 fields of the finest level's
+// layout (n elements each) starting at base; vector v is base + v*n.  All
+// vectors are zero outside the rows of the system (active and ghost/dead
+// cells), so sums over every interior cell are sums over the rows.
+__device__ __forceinline__ bool is_row(const DevLevel &L, long long id, uint8_t mk) {
+  return (mk & 64) || L.type[id] == T_GHOST;
+}
+
+// dst = F - A P on active rows, 0 on every other interior cell; part[b] =
+// block sum of the squared active-row residuals (fluid-row norm)
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vp, int vf, int vd,
+           double *part) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const double *P = kd[p].base + vp * kd[p].n, *F = kd[p].base + vf * kd[p].n;
+  double *D = kd[p].base + vd * kd[p].n;
+  double r2 = 0.0;
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    const uint8_t mk = L.mask[id];
+    double r = 0.0;
+    if (mk & 64) r = F[id] - apply_row<double>(L, id, c.i, c.j, c.k, mk, mkptr(P, kd[p].n, K_X));
+    D[id] = r;
+    r2 += r * r;
+  }
+  const double t = block_sum(r2);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// dst = A src on active rows, 0 on every other interior cell
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_apply(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vs, int vd) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const double *S = kd[p].base + vs * kd[p].n;
+  double *D = kd[p].base + vd * kd[p].n;
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    const uint8_t mk = L.mask[id];
+    D[id] = (mk & 64) ? apply_row<double>(L, id, c.i, c.j, c.k, mk, mkptr(S, kd[p].n, K_X)) : 0.0;
+  }
+}
+
+// interpolation rows: mode 0 -> dst[t] = c0 + sum w src[corner] - src[t]
+// (residual of x_t - sum w x = c0), mode 1 -> dst[t] = src[t] - sum w
+// src[corner] (the row of A), mode 2 -> correction constants of the
+// preconditioner: rd = rf = src[t]
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_rows(DevRows R, const DevLevel *lev0, const KDesc *kd, int mode, int vs, int vd) {
+  const int r = blockIdx.x * CELL_BLOCK + threadIdx.x;
+  if (r >= R.n) return;
+  const int p = R.prob[r];
+  const DevLevel &L = lev0[p];
+  const double *S = kd[p].base + vs * kd[p].n;
+  const long long t = R.tgt[r];
+  if (mode == 2) {
+    R.rd[r] = S[t];
+    R.rf[r] = (float)S[t];
+    return;
+  }
+  double *D = kd[p].base + vd * kd[p].n;
+  const long long b = R.cell[r], sy = L.sy, sz = L.sz;
+  const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
+  double acc = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * S[b + o[q]];
+  D[t] = mode == 0 ? R.c0[r] + acc - S[t] : S[t] - acc;
+}
+
+// block partials of (w, v_i) for i < nv and of (w, w): part[i * nblk + b]
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_dots(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vw, int v0, int nv,
+          int nblk, double *part) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const long long n = kd[p].n;
+  const double *Wv = kd[p].base + vw * n;
+  const double *V = kd[p].base + v0 * n;
+  double acc[KR_MAXV + 1];
+#pragma unroll
+  for (int i = 0; i <= KR_MAXV; ++i) acc[i] = 0.0;
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    const double w = Wv[id];
+#pragma unroll
+    for (int i = 0; i < KR_MAXV; ++i)
+      if (i < nv) acc[i] += w * V[id + i * n];
+    acc[KR_MAXV] += w * w;
+  }
+#pragma unroll
+  for (int i = 0; i < KR_MAXV; ++i) {
+    if (i < nv) {  // nv is the same for the whole block
+      const double t = block_sum(acc[i]);
+      if (threadIdx.x == 0) part[(size_t)i * nblk + blockIdx.x] = t;
+      __syncthreads();
+    }
+  }
+  const double t = block_sum(acc[KR_MAXV]);
+  if (threadIdx.x == 0) part[(size_t)nv * nblk + blockIdx.x] = t;
+}
+
+// out[p * ostride + i] = sum of part[i * nblk + off[p] .. off[p+1]) for
+// i < nsum (grid: problems x nsum)
+__global__ void __launch_bounds__(256)
+k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostride) {
+  const int p = blockIdx.x, i = blockIdx.y;
+  double v = 0.0;
+  for (int b = off[p] + threadIdx.x; b < off[p + 1]; b += 256) v += part[(size_t)i * nblk + b];
+  __shared__ double red[8];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    out[(size_t)p * ostride + i] = t;
+  }
+}
+
+// dst = coef[p*cs] * dst + sum_{i<ns} coef[p*cs + 1 + i] * vec(s0 + i)
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_axpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, int s0, int ns,
+          const double *coef, int cs) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const long long n = kd[p].n;
+  double *D = kd[p].base + vd * n;
+  const double *S = kd[p].base + s0 * n;
+  const double *cf = coef + (size_t)p * cs;
+  const double a0 = cf[0];
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    double v = a0 * D[id];
+    for (int i = 0; i < ns; ++i) v += cf[1 + i] * S[id + i * n];
+    D[id] = v;
+  }
+}
+
+// preconditioner input: rhs_T = v on active rows (0 elsewhere), x_T = 0
+template <typename T>
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_stage(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vs) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const double *S = kd[p].base + vs * kd[p].n;
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    rhs[id] = (L.mask[id] & 64) ? (T)S[id] : T(0);
+    x[id] = T(0);
+  }
+}
+
+// preconditioner output: z = x_T on rows, 0 elsewhere
+template <typename T>
+__global__ void __launch_bounds__(CELL_BLOCK)
+k_kr_unstage(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  double *D = kd[p].base + vd * kd[p].n;
+  auto x = PrecOf<T>::x(L);
+  for (int rr = 0; rr < CELL_ROWS; ++rr) {
+    const CellIdx c = cell_of(L, lb, rr);
+    if (!c.ok) continue;
+    const long long id = c.i + L.sy * c.j + L.sz * c.k;
+    D[id] = is_row(L, id, L.mask[id]) ? (double)x[id] : 0.0;
+  }
+}
+
+cudaError_t kr_resid(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vp,
+                     int vf, int vd, double *part, double *norm2, cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  k_kr_resid<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vp, vf, vd, part);
+  k_reduce_parts<<<L0.n, 1024, 0, s>>>(L0.off, part, norm2);
+  note_launches(2);
+  if (R.n > 0) {
+    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, vp, vd);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t kr_apply(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
+                     int vd, cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  k_kr_apply<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vs, vd);
+  note_launches(1);
+  if (R.n > 0) {
+    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vs, vd);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t kr_dots(const Launch &L0, const KDesc *kd, int vw, int v0, int nv, double *part, double *out,
+                    int ostride, cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  if (nv > KR_MAXV) return cudaErrorInvalidValue;
+  k_kr_dots<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vw, v0, nv, L0.blocks, part);
+  k_kr_reduce<<<dim3(L0.n, nv + 1), 256, 0, s>>>(L0.off, part, L0.blocks, out, ostride);
+  note_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t kr_axpy(const Launch &L0, const KDesc *kd, int vd, int s0, int ns, const double *coef, int cs,
+                    cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  k_kr_axpy<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vd, s0, ns, coef, cs);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t kr_stage(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
+                     cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  k_kr_stage<T><<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vs);
+  note_launches(1);
+  if (R.n > 0) {
+    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, vs, vs);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t kr_unstage(const Launch &L0, const KDesc *kd, int vd, cudaStream_t s) {
+  if (L0.empty()) return cudaSuccess;
+  k_kr_unstage<T><<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vd);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template cudaError_t kr_stage<double>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
+                                      cudaStream_t);
+template cudaError_t kr_stage<float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
+                                     cudaStream_t);
+template cudaError_t kr_unstage<double>(const Launch &, const KDesc *, int, cudaStream_t);
+template cudaError_t kr_unstage<float>(const Launch &, const KDesc *, int, cudaStream_t);
 
 #ifdef FG_CHECKED
 // first recorded out-of-range access of a checked build: {hits, index,

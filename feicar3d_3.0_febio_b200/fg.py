@@ -28,6 +28,7 @@ LIB_PATH = os.environ.get("FEICAR_B200_LIB") or os.path.join(_HERE, "libfeicar_b
 FG_OK, FG_NOT_CONVERGED = 0, 1
 FG_PBC_DIRICHLET, FG_PBC_NEUMANN = 1, 2
 FG_PREC_FP64, FG_PREC_MIXED = 0, 1
+FG_OUTER_RICHARDSON, FG_OUTER_FGMRES = 0, 1
 STATUS = {0: "ok", 1: "not converged", 2: "image point has no host cell", 3: "allocation failed",
           4: "timeout", 5: "bad input", 6: "dead cell without body", 7: "CUDA error",
           8: "no CUDA device", 9: "rejected by admission"}
@@ -55,6 +56,7 @@ class SolverConfig(C.Structure):
         ("probe_length_dead", C.c_double),
         ("membrane_tkns_factor", C.c_double),
         ("gauge_corner", C.c_int),
+        ("restart", C.c_int),
     ]
 
 

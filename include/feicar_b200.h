@@ -41,13 +41,15 @@ typedef enum fg_status {
 enum { FG_PBC_DIRICHLET = 1, FG_PBC_NEUMANN = 2 };
 enum { FG_SOLID = 1, FG_MEMBRANE = 2 };
 enum { FG_PREC_FP64 = 0, FG_PREC_MIXED = 1 };
-enum { FG_OUTER_RICHARDSON = 0, FG_OUTER_BICGSTAB = 1 };
+enum { FG_OUTER_RICHARDSON = 0, FG_OUTER_FGMRES = 1 };
 
 /* Solver settings: the input.dat keys of MAIN.F90:214-254 that the pressure
  * path reads, plus the knobs of the multigrid run on the GPU. */
 typedef struct fg_solver_config {
   int    precision;          /* FG_PREC_FP64 or FG_PREC_MIXED              */
-  int    outer;              /* FG_OUTER_RICHARDSON / FG_OUTER_BICGSTAB     */
+  int    outer;              /* FG_OUTER_RICHARDSON: V-cycles on p;
+                                FG_OUTER_FGMRES: flexible GMRES(restart)
+                                preconditioned by one V-cycle            */
   int    nu1, nu2;           /* pre/post smoothing steps (x, y, z lines)   */
   double omega;              /* line relaxation factor (omega_pson)        */
   double rtol;               /* ||f - A p||_2 / ||f||_2 on fluid rows       */
@@ -59,6 +61,7 @@ typedef struct fg_solver_config {
   double probe_length_dead;  /* probeLengthNormalizedD                     */
   double membrane_tkns_factor;
   int    gauge_corner;       /* 1: subtract p(1,1,1) when all-Neumann      */
+  int    restart;            /* FGMRES restart length (2..15)              */
 } fg_solver_config;
 
 typedef struct fg_solve_stats {

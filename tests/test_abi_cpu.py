@@ -44,6 +44,7 @@ def test_default_config_matches_reference_defaults():
     assert list(cfg.pbc) == [fg.FG_PBC_NEUMANN] * 6
     assert cfg.probe_length == 2.0 and cfg.probe_length_dead == 2.0
     assert cfg.gauge_corner == 1
+    assert cfg.outer == fg.FG_OUTER_FGMRES and cfg.restart == 8
 
 
 def test_null_and_bad_arguments_are_rejected():

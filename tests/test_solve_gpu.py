@@ -90,13 +90,15 @@ def _grids():
 GRIDS = _grids()
 
 
+@pytest.mark.parametrize("outer", ["fgmres", "richardson"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 @pytest.mark.parametrize("name", list(GRIDS))
-def test_converges_to_discrete_solution(name, prec):
+def test_converges_to_discrete_solution(name, prec, outer):
     grid, bodies = GRIDS[name]
     _, ib, rhs, phi = _problem(grid, bodies)
     p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
-    c = _case(grid, bodies, precision=p_, rtol=1e-12, max_cycles=120)
+    o_ = fg.FG_OUTER_FGMRES if outer == "fgmres" else fg.FG_OUTER_RICHARDSON
+    c = _case(grid, bodies, precision=p_, outer=o_, rtol=1e-12, max_cycles=120)
     p = np.zeros(grid.shape, order="F")
     st = c.solve_poisson(p, rhs)
     assert st["relres"] <= 1e-12
