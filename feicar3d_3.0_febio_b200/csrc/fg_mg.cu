@@ -153,6 +153,25 @@ __device__ __forceinline__ LineCoef line_coef(const DevLevel &L, int axis, int i
   return c;
 }
 
+// The coefficients of line_coef in the arithmetic type T of a sweep along
+// AXIS, with the face ids fixed at compile time: transverse faces t = 0..3
+// are the lower and upper faces of the first, then the second axis other
+// than AXIS, at element offsets -s0, +s0, -s1, +s1.
+template <typename T, int AXIS>
+struct LineCoefT {
+  static constexpr int A0 = AXIS == 0 ? 1 : 0;
+  static constexpr int A1 = AXIS == 2 ? 1 : 2;
+  __host__ __device__ static constexpr int qt(int t) { return t < 2 ? 2 * A0 + t : 2 * A1 + t - 2; }
+  static constexpr int qm = 2 * AXIS, qp = 2 * AXIS + 1;
+  T tq[4];
+  T tdir;
+  bool dirm, dirp;
+  __device__ __forceinline__ explicit LineCoefT(const LineCoef &c)
+      : tq{(T)c.tq[0], (T)c.tq[1], (T)c.tq[2], (T)c.tq[3]}, tdir((T)c.tdir), dirm(c.dirm != 0),
+        dirp(c.dirp != 0) {}
+  __device__ __forceinline__ bool iso() const { return tdir == T(0) && !dirm && !dirp; }
+};
+
 // Row coefficients from the staged mask: a couples to the previous row, c
 // to the next, b the diagonal (sum over the kept faces, doubled on
 // Dirichlet boundary faces).  Non-active rows are identities.
@@ -510,6 +529,117 @@ __device__ __forceinline__ void chunk_eliminate(int r0, int n, const uint8_t (&m
   aF = a0; bF = b0 - c0 * pa; cF = -c0 * pb; dF = d0 - c0 * pd;
 }
 
+// chunk_eliminate with coefficients in T (LineCoefT) and the couplings
+// along the line staged as am_[r], ap_[r] for line row r (0-based).
+template <typename T, int M, typename LC>
+__device__ __forceinline__ void chunk_eliminate_t(int r0, int n, const uint8_t (&mk)[M], T (&d)[M],
+                                                  T (&al)[M], T (&ga)[M], const T *am_, const T *ap_,
+                                                  const LC &lc, T &aF, T &bF, T &cF, T &dF, T &aL,
+                                                  T &cL, T &dL) {
+  T a0 = T(0), b0 = T(1), c0 = T(0), d0 = T(0);
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    T a = T(0), b = T(1), c = T(0), dd = T(0);
+    if (r < n) {
+      const uint8_t m8 = mk[u];
+      dd = d[u];
+      if (m8 & 64) {
+        const T am = am_[r], ap = ap_[r];
+        T diag = -lc.tdir;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if ((m8 >> LC::qt(t)) & 1) diag -= lc.tq[t];
+        const bool cm = (m8 >> LC::qm) & 1, cp = (m8 >> LC::qp) & 1;
+        if (cm) diag -= am; else if (r == 0 && lc.dirm) diag -= T(2) * am;
+        if (cp) diag -= ap; else if (r == n - 1 && lc.dirp) diag -= T(2) * ap;
+        a = cm ? am : T(0);
+        c = cp ? ap : T(0);
+        b = diag;
+      }
+    }
+    if (u == 0) {
+      a0 = a; b0 = b; c0 = c; d0 = dd;
+    } else if (u == 1) {
+      const T rr = rcp_nr(b);
+      al[1] = a * rr; ga[1] = c * rr; d[1] = dd * rr;
+    } else {
+      const T rr = rcp_nr(b - a * ga[u - 1]);
+      al[u] = -a * al[u - 1] * rr;
+      ga[u] = c * rr;
+      d[u] = (dd - a * d[u - 1]) * rr;
+    }
+  }
+  aL = al[M - 1]; cL = ga[M - 1]; dL = d[M - 1];
+  T pa = T(0), pb = T(-1), pd = T(0);
+#pragma unroll
+  for (int u = M - 2; u >= 1; --u) {
+    const T nd = d[u] - ga[u] * pd;
+    const T na = al[u] - ga[u] * pa;
+    const T nb = -ga[u] * pb;
+    al[u] = na; ga[u] = nb; d[u] = nd;
+    pa = na; pb = nb; pd = nd;
+  }
+  aF = a0; bF = b0 - c0 * pa; cF = -c0 * pb; dF = d0 - c0 * pd;
+}
+
+// chunk_eliminate with the per-row state in shared memory: row u of the
+// calling thread's chunk at sal[u*st], sga[u*st], sd[u*st] (sd holds the
+// right-hand sides on entry); am_[r], ap_[r] couple line row r (0-based) to
+// rows r-1 and r+1.
+template <typename T, int M, typename LC>
+__device__ __forceinline__ void chunk_eliminate_smem(int r0, int n, const uint8_t (&mk)[M], T *sd, T *sal,
+                                                     T *sga, int st, const T *am_, const T *ap_,
+                                                     const LC &lc, T &aF, T &bF, T &cF, T &dF,
+                                                     T &aL, T &cL, T &dL) {
+  T a0 = T(0), b0 = T(1), c0 = T(0), d0 = T(0);
+  T alp = T(0), gap = T(0), dp = T(0);
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    T a = T(0), b = T(1), c = T(0), dd = T(0);
+    if (r < n) {
+      const uint8_t m8 = mk[u];
+      dd = sd[u * st];
+      if (m8 & 64) {
+        const T am = am_[r], ap = ap_[r];
+        T diag = -lc.tdir;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if ((m8 >> LC::qt(t)) & 1) diag -= lc.tq[t];
+        const bool cm = (m8 >> LC::qm) & 1, cp = (m8 >> LC::qp) & 1;
+        if (cm) diag -= am; else if (r == 0 && lc.dirm) diag -= T(2) * am;
+        if (cp) diag -= ap; else if (r == n - 1 && lc.dirp) diag -= T(2) * ap;
+        a = cm ? am : T(0);
+        c = cp ? ap : T(0);
+        b = diag;
+      }
+    }
+    if (u == 0) {
+      a0 = a; b0 = b; c0 = c; d0 = dd;
+    } else {
+      const T rr = u == 1 ? rcp_nr(b) : rcp_nr(b - a * gap);
+      const T nal = u == 1 ? a * rr : -a * alp * rr;
+      const T nga = c * rr;
+      const T nd = u == 1 ? dd * rr : (dd - a * dp) * rr;
+      sal[u * st] = nal; sga[u * st] = nga; sd[u * st] = nd;
+      alp = nal; gap = nga; dp = nd;
+    }
+  }
+  aL = alp; cL = gap; dL = dp;
+  T pa = T(0), pb = T(-1), pd = T(0);
+#pragma unroll
+  for (int u = M - 2; u >= 1; --u) {
+    const T du = sd[u * st], au = sal[u * st], gu = sga[u * st];
+    const T nd = du - gu * pd;
+    const T na = au - gu * pa;
+    const T nb = -gu * pb;
+    sal[u * st] = na; sga[u * st] = nb; sd[u * st] = nd;
+    pa = na; pb = nb; pd = nd;
+  }
+  aF = a0; bF = b0 - c0 * pa; cF = -c0 * pb; dF = d0 - c0 * pd;
+}
+
 // Zebra x-line relaxation, lines (j,k) with (j+k)%2 == color, W lanes per
 // line (32/W lines per warp).  Lane l of a line owns rows [M l, M l + M),
 // loaded straight into registers with 16-byte loads (rows past the line
@@ -591,6 +721,167 @@ k_xline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) 
   store_run<T, M>(x, row + r0, out, valid);
 }
 
+// A lane's chunk of M values (or M mask bytes) moved between registers and
+// shared memory as 16-byte (8-byte) pieces: with the chunk stride a multiple
+// of 16 bytes, 8 lanes of a phase hit distinct bank groups.
+template <typename T, int M>
+__device__ __forceinline__ void lds_chunk(const unsigned char *p, T (&v)[M]) {
+  constexpr int W = 16 / sizeof(T);
+#pragma unroll
+  for (int c = 0; c < M / W; ++c) {
+    const uint4 q = reinterpret_cast<const uint4 *>(p)[c];
+    memcpy(&v[c * W], &q, 16);
+  }
+}
+template <typename T, int M>
+__device__ __forceinline__ void sts_chunk(unsigned char *p, const T (&v)[M]) {
+  constexpr int W = 16 / sizeof(T);
+#pragma unroll
+  for (int c = 0; c < M / W; ++c) {
+    uint4 q;
+    memcpy(&q, &v[c * W], 16);
+    reinterpret_cast<uint4 *>(p)[c] = q;
+  }
+}
+template <int M>
+__device__ __forceinline__ void lds_mask(const unsigned char *p, uint8_t (&m)[M]) {
+  if constexpr (M == 8) {
+    const uint2 q = *reinterpret_cast<const uint2 *>(p);
+    memcpy(m, &q, 8);
+  } else {
+#pragma unroll
+    for (int c = 0; c < M / 16; ++c) {
+      const uint4 q = reinterpret_cast<const uint4 *>(p)[c];
+      memcpy(&m[16 * c], &q, 16);
+    }
+  }
+}
+
+// Zebra x-line relaxation for lines of 129..1024 cells: one warp per line,
+// XS_WARPS lines per block.  Consecutive lanes load consecutive 4-cell
+// pieces of the line (rhs, mask, own values, four neighbour lines: every
+// load instruction reads whole 32-byte sectors) and form each row's
+// right-hand side; the rows go to shared memory in chunk order (lane l's M
+// rows at a padded stride), each lane eliminates its chunk in registers,
+// the 32 chunk-first unknowns are solved by PCR, and the results return
+// through shared memory to coalesced stores.
+constexpr int XS_WARPS = 4;
+constexpr int XS_PIECE = 4;  // cells per piece of the coalesced phases
+template <typename T, int M>
+struct XsLayout {
+  static constexpr int CT = M * (int)sizeof(T) + 16;  // padded chunk of T
+  static constexpr int LT = 32 * CT;                  // right-hand sides, then results
+  static constexpr int PER_WARP = LT + 32 * M;        // + mask bytes in line order
+};
+
+// Line (j,k) of warp `warp` in block `lb` of a level's x sweep; false when
+// the warp has no line.
+__device__ __forceinline__ bool xs_line(const DevLevel &L, int lb, int warp, int color, int &j, int &k) {
+  const int nyh = (L.ny + 1) >> 1;
+  const int q = lb * XS_WARPS + warp;
+  k = 1 + q / nyh;
+  const int jj = q % nyh;
+  if (k > L.nz) return false;
+  j = ((((1 + k) & 1) == color) ? 1 : 2) + 2 * jj;
+  return j <= L.ny;
+}
+
+template <typename T, int M>
+__global__ void __launch_bounds__(XS_WARPS * 32)
+k_xline_smem(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+  using LY = XsLayout<T, M>;
+  using LC = LineCoefT<T, 0>;
+  constexpr int P = XS_PIECE;
+  extern __shared__ __align__(16) unsigned char xs_smem[];
+  __shared__ T s_am[32 * M], s_ap[32 * M];  // couplings along x (one level per block)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  const int n = L.nx;
+  for (int r = threadIdx.x; r < n; r += XS_WARPS * 32) {
+    s_am[r] = (T)L.amx[1 + r];
+    s_ap[r] = (T)L.apx[1 + r];
+  }
+  __syncthreads();
+  int j, k;
+  if (!xs_line(L, lb, warp, color, j, k)) return;  // uniform over the warp
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  const LC lc(line_coef(L, 0, 1, j, k));
+  const bool iso_line = lc.iso();
+  const long long row = L.sy * j + L.sz * k + 1;  // cell i = 1
+  const long long to[4] = {-L.sy, L.sy, -L.sz, L.sz};
+  unsigned char *sw = xs_smem + (size_t)warp * LY::PER_WARP;
+  unsigned char *s_d = sw, *s_mk = sw + LY::LT;
+  // right-hand sides of the line's rows, piece by piece (pieces past the
+  // line end are not read by the elimination)
+#pragma unroll
+  for (int c = 0; c < M / P; ++c) {
+    const int e = (lane + 32 * c) * P;
+    if (e < n) {
+      T rv[P], xo[P], dv[P];
+      uint8_t m4[P];
+      load_run<T, P>(rv, rhs, row + e);
+      load_run<T, P>(xo, x, row + e);
+      load_run<uint8_t, P>(m4, L.mask, row + e);
+      T nb[4][P];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) load_run<T, P>(nb[t], x, row + e + to[t]);
+#pragma unroll
+      for (int v = 0; v < P; ++v) {
+        uint8_t m8 = m4[v];
+        T acc = rv[v];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t][v] : T(0);
+        const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+        if (held) { acc = xo[v]; m8 = 0; }
+        dv[v] = acc;
+        m4[v] = m8;
+      }
+      sts_chunk<T, P>(s_d + (e / M) * LY::CT + (e % M) * sizeof(T), dv);
+      unsigned w4;
+      memcpy(&w4, m4, 4);
+      *reinterpret_cast<unsigned *>(s_mk + e) = w4;
+    }
+  }
+  __syncwarp();
+  const int r0 = lane * M;
+  T d[M], al[M], ga[M];
+  uint8_t mk[M];
+  lds_chunk<T, M>(s_d + lane * LY::CT, d);
+  lds_mask<M>(s_mk + lane * M, mk);
+  T aF, bF, cF, dF, aL, cL, dL;
+  chunk_eliminate_t<T, M>(r0, r0 < n ? n : r0, mk, d, al, ga, s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
+  T aLp = __shfl_up_sync(0xffffffffu, aL, 1);
+  T cLp = __shfl_up_sync(0xffffffffu, cL, 1);
+  T dLp = __shfl_up_sync(0xffffffffu, dL, 1);
+  if (lane == 0) { aLp = T(0); cLp = T(0); dLp = T(0); }
+  const T xF = pcr_seg<T, 32>(-aF * aLp, bF - aF * cLp - cF * aL, -cF * cL, dF - aF * dLp - cF * dL, lane);
+  const T xFn = __shfl_down_sync(0xffffffffu, xF, 1);
+  const T xL = dL - aL * xF - cL * (lane + 1 < 32 ? xFn : T(0));
+#pragma unroll
+  for (int u = 0; u < M; ++u) d[u] = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+  __syncwarp();
+  sts_chunk<T, M>(s_d + lane * LY::CT, d);
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < M / P; ++c) {
+    const int e = (lane + 32 * c) * P;
+    if (e < n) {
+      T v[P];
+      lds_chunk<T, P>(s_d + (e / M) * LY::CT + (e % M) * sizeof(T), v);
+      if (omega != T(1)) {
+        T xo[P];
+        load_run<T, P>(xo, x, row + e);
+#pragma unroll
+        for (int q = 0; q < P; ++q) v[q] = xo[q] + omega * (v[q] - xo[q]);
+      }
+      store_run<T, P>(x, row + e, v, n - e);
+    }
+  }
+}
+
 // Zebra line relaxation along y (AXIS 1, lines (i,k), colour (i+k)%2) or z
 // (AXIS 2, lines (i,j), colour (i+j)%2).  A block takes the 32 lines of
 // one colour in a 64-cell i-tile (lane l: i = i0 + par + 2l, so every
@@ -604,11 +895,18 @@ template <typename T>
 struct ChunkEq { T a, b, c, d; };
 
 template <typename T, int M, int CH, int AXIS>
-__global__ void __launch_bounds__(CH * 32)
+__global__ void __launch_bounds__(CH * 32, (sizeof(T) == 4 && CH == 16) ? (M <= 8 ? 3 : 2) : 1)
 k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) {
-  __shared__ T s_lc[CH][32][3];   // last-row equation of each chunk
+  using LC = LineCoefT<T, AXIS>;
   __shared__ ChunkEq<T> s_eq[CH][32];
   __shared__ T s_f[CH + 1][32];   // chunk-first unknowns
+  __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
+  extern __shared__ __align__(16) unsigned char yz_smem[];
+  constexpr int NT = CH * 32;     // per-row stride of the state arrays
+  T *s_d = reinterpret_cast<T *>(yz_smem);
+  T *s_al = s_d + M * NT;
+  T *s_ga = s_al + M * NT;
+  const int tid = threadIdx.x;
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -625,43 +923,54 @@ k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega)
   const long long os = AXIS == 1 ? L.sz : L.sy;  // stride of the fixed index
   auto x = PrecOf<T>::x(L);
   auto rhs = PrecOf<T>::rhs(L);
-  const LineCoef lc = line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1);
+  const LC lc(line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1));
   const long long base = (long long)(valid ? i : L.nx) + os * o;  // row index 0 of the line
   const int r0 = w * M;
   const bool any = valid && r0 < n;
-  T d[M], al[M], ga[M];
   uint8_t mk[M];
-  const bool iso_line = lc.tdir == 0.0 && !lc.dirm && !lc.dirp;
+  const bool iso_line = lc.iso();
+  {
+    auto am = AXIS == 1 ? L.amy : L.amz;
+    auto ap = AXIS == 1 ? L.apy : L.apz;
+    for (int r = tid; r < n; r += NT) { s_am[r] = (T)am[1 + r]; s_ap[r] = (T)ap[1 + r]; }
+  }
+  __syncthreads();
   // all loads of a row are issued unconditionally (none waits on the mask)
 #pragma unroll
   for (int u = 0; u < M; ++u) {
     const int r = r0 + u;
-    d[u] = T(0); mk[u] = 0;
+    T dv = T(0);
+    mk[u] = 0;
     if (any && r < n) {
       const long long id = base + ls * (r + 1);
       uint8_t m8 = L.mask[id];
       const T rv = rhs[id];
       const T xv = x[id];
       T nb[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) nb[t] = x[id + lc.to[t]];
+      nb[0] = x[id - 1];
+      nb[1] = x[id + 1];
+      nb[2] = x[id - os];
+      nb[3] = x[id + os];
       T acc = rv;
 #pragma unroll
-      for (int t = 0; t < 4; ++t) acc -= ((m8 >> lc.qt[t]) & 1) ? (T)lc.tq[t] * nb[t] : T(0);
+      for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
       const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
       if (held) { acc = xv; m8 = 0; }
-      d[u] = acc;
+      dv = acc;
       mk[u] = m8;
     }
+    s_d[u * NT + tid] = dv;
   }
   T aF, bF, cF, dF, aL, cL, dL;
-  chunk_eliminate<T, M>(r0, any ? n : r0, mk, d, al, ga, AXIS == 1 ? L.amy : L.amz,
-                        AXIS == 1 ? L.apy : L.apz, lc, aF, bF, cF, dF, aL, cL, dL);
-  s_lc[w][lane][0] = aL; s_lc[w][lane][1] = cL; s_lc[w][lane][2] = dL;
+  chunk_eliminate_smem<T, M>(r0, any ? n : r0, mk, s_d + tid, s_al + tid, s_ga + tid, NT,
+                             s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
   __syncthreads();
   {
     T aLp = T(0), cLp = T(0), dLp = T(0);
-    if (w > 0) { aLp = s_lc[w - 1][lane][0]; cLp = s_lc[w - 1][lane][1]; dLp = s_lc[w - 1][lane][2]; }
+    if (w > 0) {  // last-row equation of the previous chunk (row M-1 is not touched upward)
+      const int tp = tid - 32;
+      aLp = s_al[(M - 1) * NT + tp]; cLp = s_ga[(M - 1) * NT + tp]; dLp = s_d[(M - 1) * NT + tp];
+    }
     ChunkEq<T> e;
     e.a = -aF * aLp;
     e.b = bF - aF * cLp - cF * aL;
@@ -698,7 +1007,7 @@ k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega)
   for (int u = 0; u < M; ++u) {
     const int r = r0 + u;
     if (r >= n) break;
-    T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+    T v = u == 0 ? xF : (u == M - 1 ? xL : s_d[u * NT + tid] - s_al[u * NT + tid] * xF - s_ga[u * NT + tid] * xL);
     const long long id = base + ls * (r + 1);
     if (omega != T(1)) v = x[id] + omega * (v - x[id]);
     x[id] = v;
@@ -856,7 +1165,9 @@ int blocks_cells(const DevLevel &L) {
 int xline_lanes(int maxn) { return maxn <= 16 ? 4 : maxn <= 32 ? 8 : maxn <= 64 ? 16 : 32; }
 int blocks_xline(const DevLevel &L, int maxn) {
   const long long lines = (long long)((L.ny + 1) / 2) * L.nz;
-  const long long per_block = (long long)XL_WARPS * (32 / xline_lanes(maxn));
+  // lines of more than 128 cells: k_xline_smem, one line per warp
+  const long long per_block = maxn > 128 ? (long long)XS_WARPS
+                                         : (long long)XL_WARPS * (32 / xline_lanes(maxn));
   return (int)((lines + per_block - 1) / per_block);
 }
 int blocks_tile(const DevLevel &L, int axis, int maxn) {
@@ -911,12 +1222,28 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
   return cudaGetLastError();
 }
 
+template <typename T, int M>
+static cudaError_t launch_xsmem(const Launch &Lr, int color, double omega, cudaStream_t s) {
+  const size_t sm = (size_t)XS_WARPS * XsLayout<T, M>::PER_WARP;
+  auto kern = k_xline_smem<T, M>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  kern<<<Lr.blocks, XS_WARPS * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
 template <typename T, int M, int CH>
 static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
-  if (axis == 1)
-    k_yzline_reg<T, M, CH, 1><<<Lr.blocks, CH * 32, 0, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
-  else
-    k_yzline_reg<T, M, CH, 2><<<Lr.blocks, CH * 32, 0, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  const size_t sm = (size_t)3 * M * CH * 32 * sizeof(T);  // row state: d, al, ga
+  if (axis == 1) {
+    auto kern = k_yzline_reg<T, M, CH, 1>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<Lr.blocks, CH * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  } else {
+    auto kern = k_yzline_reg<T, M, CH, 2>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<Lr.blocks, CH * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  }
   note_launches(1);
   return cudaGetLastError();
 }
@@ -934,9 +1261,9 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
     if (maxn <= 32) return launch_xreg<T, 4, 8>(Lr, color, omega, s);
     if (maxn <= 64) return launch_xreg<T, 4, 16>(Lr, color, omega, s);
     if (maxn <= 128) return launch_xreg<T, 4, 32>(Lr, color, omega, s);
-    if (maxn <= 256) return launch_xreg<T, 8, 32>(Lr, color, omega, s);
-    if (maxn <= 512) return launch_xreg<T, 16, 32>(Lr, color, omega, s);
-    if (maxn <= 1024) return launch_xreg<T, 32, 32>(Lr, color, omega, s);
+    if (maxn <= 256) return launch_xsmem<T, 8>(Lr, color, omega, s);
+    if (maxn <= 512) return launch_xsmem<T, 16>(Lr, color, omega, s);
+    if (maxn <= 1024) return launch_xsmem<T, 32>(Lr, color, omega, s);
     return cudaErrorInvalidValue;  // lines longer than 1024 cells
   }
   if (maxn <= YZ_MAXROWS) {
