@@ -309,8 +309,9 @@ struct fg_batch {
   } ls[kMaxLevels];
   // level 0 over all problems
   DevLevel *d_lev0 = nullptr;
-  int *d_off0 = nullptr;
-  Launch all0;
+  int *d_off0 = nullptr, *d_offf0 = nullptr;
+  Launch all0;   // level-0 cells of all problems
+  Launch flat0;  // level-0 vector elements of all problems (flat passes)
   // rows of all problems (dead rows then ghost rows per problem)
   DevRows rows{};
   int *d_rprob = nullptr;
@@ -321,12 +322,15 @@ struct fg_batch {
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
   std::vector<double> h_norm;
   std::vector<double> history;  // max relative residual over the batch after each cycle
-  // FGMRES state (outer == FG_OUTER_FGMRES): per problem 2m+3 FP64 vectors
-  // P, F, V_0..V_m, Z_0..Z_{m-1} of the finest level's layout
+  // FGMRES state (outer == FG_OUTER_FGMRES): per problem the FP64 vectors
+  // P, F and the basis V_0..V_m, Z_0..Z_{m-1} (FP32 in the mixed path) of
+  // the finest level's layout
   bool krylov = false;  // during an FGMRES solve: V-cycles in correction form
   int km = 0;
+  int kbytes = 0;  // bytes per basis element of the allocated vectors
   std::vector<void *> kraw;
   KDesc *d_kd = nullptr;
+  std::vector<KDesc> h_kd;
   double *d_kpart = nullptr, *d_kout = nullptr, *d_kcoef = nullptr;
   std::vector<double> h_kout, h_kcoef;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -363,7 +367,7 @@ static void free_batch_tables(fg_batch *b) {
     cudaFree(s.d_off_next); cudaFree(s.d_G); cudaFree(s.d_gidx); cudaFree(s.d_gn);
     s = fg_batch::LevelSet();
   }
-  cudaFree(b->d_lev0); cudaFree(b->d_off0);
+  cudaFree(b->d_lev0); cudaFree(b->d_off0); cudaFree(b->d_offf0);
   cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
   cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
   cudaFree(b->d_norm); cudaFree(b->d_part);
@@ -373,7 +377,8 @@ static void free_batch_tables(fg_batch *b) {
   cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
   b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
   b->km = 0;
-  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
+  b->kbytes = 0;
+  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
   b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
   b->built = false;
@@ -451,10 +456,16 @@ static fg_status build_batch(fg_batch *b) {
   // level 0 over all problems
   {
     std::vector<DevLevel> v0;
-    std::vector<int> b0;
-    for (auto *c : b->cases) { v0.push_back(c->lev[0].dl); b0.push_back(k::blocks_cells(c->lev[0].dl)); }
+    std::vector<int> b0, bf;
+    for (auto *c : b->cases) {
+      v0.push_back(c->lev[0].dl);
+      b0.push_back(k::blocks_cells(c->lev[0].dl));
+      bf.push_back(k::blocks_flat(c->lev[0].ntot));
+    }
     FG_CUDA(run_launch_set_alloc((void **)&b->d_lev0, v0));
     fg_status st = build_offsets(b0, &b->d_off0, b->all0, b->d_lev0);
+    if (st != FG_OK) return st;
+    st = build_offsets(bf, &b->d_offf0, b->flat0, b->d_lev0);
     if (st != FG_OK) return st;
   }
   // rows
@@ -705,63 +716,80 @@ static int krylov_restart(const fg_solver_config &cfg) {
   return m;
 }
 
-static fg_status ensure_krylov(fg_batch *b) {
+// Krylov vectors per problem in three allocations with the field padding:
+// P, F (FP64) and the m+1 basis and m preconditioned vectors (basis type,
+// `bytes` per element); one vector every `stride` elements.
+static fg_status ensure_krylov(fg_batch *b, int bytes) {
   const int m = krylov_restart(b->cfg);
-  if (b->km == m && b->d_kd) return FG_OK;
+  if (b->km == m && b->kbytes == bytes && b->d_kd) return FG_OK;
   for (void *r : b->kraw) cudaFree(r);
   b->kraw.clear();
   cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
+  b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
+  b->km = 0;
   const int np = (int)b->cases.size();
-  const int nvec = 2 * m + 3;
   std::vector<KDesc> kd(np);
   for (int p = 0; p < np; ++p) {
     const HLevel &L0 = b->cases[p]->lev[0];
-    void *raw = nullptr;
-    FG_CUDA(cudaMalloc(&raw, (size_t)nvec * L0.ntot * sizeof(double)));
-    b->kraw.push_back(raw);
-    FG_CUDA(cudaMemset(raw, 0, (size_t)nvec * L0.ntot * sizeof(double)));
-    kd[p].base = reinterpret_cast<double *>(raw);
+    const long long stride = L0.ntot + 32;  // multiple of 32 elements
+    const size_t nel[3] = {(size_t)(2 * stride + 32), (size_t)((m + 1) * stride + 32),
+                           (size_t)(m * stride + 32)};
+    const size_t esz[3] = {sizeof(double), (size_t)bytes, (size_t)bytes};
+    unsigned char *raw[3];
+    for (int q = 0; q < 3; ++q) {
+      void *r = nullptr;
+      FG_CUDA(cudaMalloc(&r, nel[q] * esz[q]));
+      b->kraw.push_back(r);
+      FG_CUDA(cudaMemset(r, 0, nel[q] * esz[q]));
+      raw[q] = reinterpret_cast<unsigned char *>(r) + kFieldPad * esz[q];
+    }
+    kd[p].P = reinterpret_cast<double *>(raw[0]);
+    kd[p].F = kd[p].P + stride;
+    kd[p].V = raw[1];
+    kd[p].Z = raw[2];
     kd[p].n = L0.ntot;
+    kd[p].stride = stride;
   }
   FG_CUDA(run_launch_set_alloc((void **)&b->d_kd, kd));
-  FG_CUDA(cudaMalloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * std::max(1, b->all0.blocks) * sizeof(double)));
+  b->h_kd = kd;
+  const int nblk = std::max(1, std::max(b->all0.blocks, b->flat0.blocks));
+  FG_CUDA(cudaMalloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * nblk * sizeof(double)));
   FG_CUDA(cudaMalloc(&b->d_kout, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
   FG_CUDA(cudaMalloc(&b->d_kcoef, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
   b->h_kout.assign((size_t)np * (KR_MAXV + 2), 0.0);
   b->h_kcoef.assign((size_t)np * (KR_MAXV + 2), 0.0);
   b->km = m;
+  b->kbytes = bytes;
   return FG_OK;
 }
 
 // Flexible GMRES(m) on the finest-level system (fluid rows of the 7-point
 // operator and the ghost/dead interpolation rows), right-preconditioned by
 // one V-cycle in correction form (FP32 in the mixed path, which is why the
-// flexible variant is used).  All problems of the batch iterate in
-// lockstep; each has its own Arnoldi basis, Hessenberg matrix and Givens
-// rotations (host).  Convergence: true fluid-row relative residual <= rtol
-// at a restart.
-static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
+// flexible variant is used).  B is the basis type (FP32 in the mixed path:
+// the solution, right-hand side and the true residual at every restart
+// stay FP64, so the basis precision only limits how far one restart cycle
+// reduces the residual), T the V-cycle's.  All problems of the batch
+// iterate in lockstep; each has its own Arnoldi basis, Hessenberg matrix
+// and Givens rotations (host).  Convergence: true fluid-row relative
+// residual <= rtol at a restart.
+template <typename B, typename T>
+static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
   const int np = (int)b->cases.size();
   cudaStream_t s = b->stream;
-  const bool mixed = b->cfg.precision == FG_PREC_MIXED;
-  fg_status r = ensure_krylov(b);
+  fg_status r = ensure_krylov(b, (int)sizeof(B));
   if (r != FG_OK) return r;
   const int m = b->km;
-  const int VP = 0, VF = 1, V0 = 2, Z0 = 3 + m;
   const int CS = KR_MAXV + 2;  // coefficient / output stride per problem
   if (!b->ev0) { cudaEventCreate(&b->ev0); cudaEventCreate(&b->ev1); }
   FG_CUDA(cudaEventRecord(b->ev0, s));
   FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
   FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
   FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
-  std::vector<KDesc> kd(np);
   for (int p = 0; p < np; ++p) {
     const HLevel &L0 = b->cases[p]->lev[0];
-    kd[p] = KDesc{reinterpret_cast<double *>(b->kraw[p]), L0.ntot};
-    FG_CUDA(cudaMemcpyAsync(kd[p].base + VP * kd[p].n, L0.d_x64, L0.ntot * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    FG_CUDA(cudaMemcpyAsync(kd[p].base + VF * kd[p].n, L0.d_rhs64, L0.ntot * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(b->h_kd[p].P, L0.d_x64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(b->h_kd[p].F, L0.d_rhs64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
   b->krylov = true;
   b->history.clear();
@@ -790,11 +818,11 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
   bool first = true;
   fg_status err = FG_OK;
   while (err == FG_OK) {
-    // ---- true residual V0 = F - A P, fluid norm, full norm
+    // ---- true residual V_0 = F - A P, fluid norm, full norm
     FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
     const size_t e_r = prof_begin(b, s);
-    FG_K(k::kr_resid(b->all0, b->rows, b->d_lev0, b->d_kd, VP, VF, V0, b->d_part, b->d_norm, s));
-    FG_K(k::kr_dots(b->all0, b->d_kd, V0, V0, 0, b->d_kpart, b->d_kout, CS, s));
+    FG_K(k::kr_resid<B>(b->all0, b->rows, b->d_lev0, b->d_kd, 0, b->d_part, b->d_norm, s));
+    FG_K(k::kr_dots<B>(b->flat0, b->d_kd, 0, 0, b->d_kpart, b->d_kout, CS, s));
     prof_end(b, e_r, FG_PROF_RESIDUAL, 0.0, s);
     FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
     if ((err = read_out()) != FG_OK) break;
@@ -812,7 +840,7 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
     b->history.push_back(worst);
     if (all) { status = FG_OK; break; }
     if (cycles >= b->cfg.max_cycles) break;
-    // ---- V0 /= beta
+    // ---- V_0 /= beta, staged as the first preconditioner input
     for (int p = 0; p < np; ++p) {
       b->h_kcoef[(size_t)p * CS] = done[p] ? 0.0 : 1.0 / beta[p];
       ncol[p] = 0;
@@ -820,25 +848,24 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
       g[(size_t)p * (m + 1)] = beta[p];
     }
     if ((err = upload_coef()) != FG_OK) break;
-    FG_K(k::kr_axpy(b->all0, b->d_kd, V0, V0, 0, b->d_kcoef, CS, s));
+    {
+      const size_t e0 = prof_begin(b, s);
+      FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, 0, 0, 0, b->d_kcoef, CS, true, s)));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    }
     int jlast = 0;
     for (int j = 0; j < m && cycles < b->cfg.max_cycles; ++j) {
       // ---- Z_j = M^-1 V_j (one V-cycle from zero, correction form)
-      size_t e0 = prof_begin(b, s);
-      if (mixed) FG_K(k::kr_stage<float>(b->all0, b->rows, b->d_lev0, b->d_kd, V0 + j, s));
-      else FG_K(k::kr_stage<double>(b->all0, b->rows, b->d_lev0, b->d_kd, V0 + j, s));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
       cudaEventRecord(va, s);
-      r = mixed ? vcycle<float>(b, s) : vcycle<double>(b, s);
+      r = vcycle<T>(b, s);
       if (r != FG_OK) { err = r; break; }
       cudaEventRecord(vb, s);
       ++cycles;
-      e0 = prof_begin(b, s);
-      if (mixed) FG_K(k::kr_unstage<float>(b->all0, b->d_kd, Z0 + j, s));
-      else FG_K(k::kr_unstage<double>(b->all0, b->d_kd, Z0 + j, s));
-      // ---- W = A Z_j into V_{j+1}; inner products with V_0..V_j and |W|^2
-      FG_K(k::kr_apply(b->all0, b->rows, b->d_lev0, b->d_kd, Z0 + j, V0 + j + 1, s));
-      FG_K(k::kr_dots(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kpart, b->d_kout, CS, s));
+      // ---- Z_j from the V-cycle, W = A Z_j into V_{j+1}; inner products
+      // with V_0..V_j and |W|^2
+      size_t e0 = prof_begin(b, s);
+      FG_K((k::kr_apply<B, T>(b->all0, b->rows, b->d_lev0, b->d_kd, j, j + 1, s)));
+      FG_K(k::kr_dots<B>(b->flat0, b->d_kd, j + 1, j + 1, b->d_kpart, b->d_kout, CS, s));
       prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
       if ((err = read_out()) != FG_OK) break;
       {
@@ -864,8 +891,9 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
         }
         if ((err = upload_coef()) != FG_OK) break;
         e0 = prof_begin(b, s);
-        FG_K(k::kr_axpy(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kcoef, CS, s));
-        FG_K(k::kr_dots(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kpart, b->d_kout, CS, s));
+        FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, j + 1, 0, j + 1, b->d_kcoef, CS,
+                                false, s)));
+        FG_K(k::kr_dots<B>(b->flat0, b->d_kd, j + 1, j + 1, b->d_kpart, b->d_kout, CS, s));
         prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
         if ((err = read_out()) != FG_OK) break;
       }
@@ -905,10 +933,6 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
         ncol[p] = j + 1;
         if (brk) done[p] = 1;
       }
-      if ((err = upload_coef()) != FG_OK) break;
-      e0 = prof_begin(b, s);
-      FG_K(k::kr_axpy(b->all0, b->d_kd, V0 + j + 1, V0, j + 1, b->d_kcoef, CS, s));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
       jlast = j + 1;
       // residual estimate |g_{j+1}| (all rows) over the fluid-row |f|
       bool inner_done = true;
@@ -920,7 +944,15 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
         if (!(done[p] || rel <= 0.5 * b->cfg.rtol)) inner_done = false;
       }
       b->history.push_back(west);
-      if (inner_done) break;
+      // the next basis vector, staged as the next preconditioner input
+      // unless the cycle ends here
+      const bool more = !inner_done && j + 1 < m && cycles < b->cfg.max_cycles;
+      if ((err = upload_coef()) != FG_OK) break;
+      e0 = prof_begin(b, s);
+      FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, j + 1, 0, j + 1, b->d_kcoef, CS, more,
+                              s)));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+      if (!more) break;
     }
     if (err != FG_OK) break;
     // ---- P += sum_i y_i Z_i, y from the rotated Hessenberg system
@@ -938,7 +970,11 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
       for (int i = 0; i < nc; ++i) cf[1 + i] = y[i];
     }
     if ((err = upload_coef()) != FG_OK) break;
-    if (jlast > 0) FG_K(k::kr_axpy(b->all0, b->d_kd, VP, Z0, jlast, b->d_kcoef, CS, s));
+    if (jlast > 0) {
+      const size_t e0 = prof_begin(b, s);
+      FG_K(k::kr_update<B>(b->flat0, b->d_kd, jlast, b->d_kcoef, CS, s));
+      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    }
   }
   cudaEventDestroy(va); cudaEventDestroy(vb);
   b->krylov = false;
@@ -946,10 +982,8 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
   // solution back into the finest-level field; ghost-row residual for stats
   for (int p = 0; p < np; ++p) {
     const HLevel &L0 = b->cases[p]->lev[0];
-    FG_CUDA(cudaMemcpyAsync(L0.d_x64, kd[p].base + VP * kd[p].n, L0.ntot * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    FG_CUDA(cudaMemcpyAsync(L0.d_rhs64, kd[p].base + VF * kd[p].n, L0.ntot * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(L0.d_x64, b->h_kd[p].P, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    FG_CUDA(cudaMemcpyAsync(L0.d_rhs64, b->h_kd[p].F, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
   }
   FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
   FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
@@ -971,6 +1005,11 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
     st->vcycle_ms = vms.empty() ? 0.0 : sm / vms.size();
   }
   return status;
+}
+
+static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
+  if (b->cfg.precision == FG_PREC_MIXED) return fgmres_run<float, float>(b, st);
+  return fgmres_run<double, double>(b, st);
 }
 
 // -------------------------------------------------------- case geometry

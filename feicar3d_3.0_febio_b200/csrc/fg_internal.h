@@ -148,11 +148,17 @@ long long launches_so_far();
     }                                                                  \
   } while (0)
 
-// Krylov vectors of one problem (FGMRES outer iteration): nvec FP64 fields
-// of the finest level's layout, n elements each, vector v at base + v*n
+// Krylov vectors of one problem (FGMRES outer iteration), all in the finest
+// level's layout with the field padding (element 1 on a 16-byte boundary):
+// the solution P and right-hand side F in FP64, the basis V_0..V_m and the
+// preconditioned vectors Z_0..Z_{m-1} in the basis type B (FP32 in the
+// mixed path, FP64 otherwise).  Vector v of a kind starts at its base +
+// v*stride.  Every vector is zero outside the rows of the system.
 struct KDesc {
-  double *base;
-  long long n;
+  double *P, *F;
+  void *V, *Z;
+  long long n;       // elements of one vector (the level's ntot)
+  long long stride;  // elements from one vector to the next
 };
 constexpr int KR_MAXV = 16;  // most vectors one dot-product pass reads
 
@@ -160,6 +166,8 @@ constexpr int KR_MAXV = 16;  // most vectors one dot-product pass reads
 namespace k {
 // blocks needed by one problem's level for each kernel family
 int blocks_cells(const DevLevel &L);
+// flat passes over the n elements of a level-0 field (Krylov vectors)
+int blocks_flat(long long n);
 int blocks_xline(const DevLevel &L, int maxn);
 // y/z tiles: blocks depend on the kernel the level set's longest line picks
 int blocks_tile(const DevLevel &L, int axis, int maxn);
@@ -202,25 +210,34 @@ cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, lon
 cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz,
                          const int *pbc, const double *ppp, int gauge, double *scratch,
                          cudaStream_t s);
-// FGMRES pieces over the finest level of a batch (Launch of all level-0
-// cells; rows of all problems).  kr_resid: vd = F - A P (and rows), norm2[p]
-// += fluid-row |r|^2; kr_apply: vd = A vs; kr_dots: out[p*ostride + i] =
-// (vw, v0+i) for i < nv, out[p*ostride + nv] = (vw, vw); kr_axpy: vd =
-// coef[p*cs]*vd + sum_i coef[p*cs+1+i] vec(s0+i); kr_stage/kr_unstage move
-// a vector into / out of the precision-T correction arrays of level 0.
-cudaError_t kr_resid(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vp,
-                     int vf, int vd, double *part, double *norm2, cudaStream_t s);
-cudaError_t kr_apply(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
-                     int vd, cudaStream_t s);
-cudaError_t kr_dots(const Launch &L0, const KDesc *kd, int vw, int v0, int nv, double *part, double *out,
+// FGMRES pieces over the finest level of a batch: `cells` launches over
+// the level-0 cells of all problems, `flat` over their vector elements
+// (blocks_flat); rows of all problems.  B is the basis type, T the type of
+// the preconditioner's level-0 arrays.
+//  kr_resid:  V_vd = F - A P (rows included), norm2[p] += fluid-row |r|^2
+//  kr_apply:  Z_vz = preconditioner output x_T on rows (0 elsewhere),
+//             V_vw = A Z_vz (rows included)
+//  kr_dots:   out[p*ostride + i] = (V_vw, V_i) for i < nv,
+//             out[p*ostride + nv] = (V_vw, V_vw)
+//  kr_vaxpy:  V_vd = c0 V_vd + sum_{i<ns} c_{1+i} V_{s0+i} (c = coef + p*cs);
+//             with stage, also the preconditioner input: rhs_T = V_vd on
+//             active rows (0 elsewhere), x_T = 0, row constants = V_vd
+//  kr_update: P += sum_{i<ns} c_{1+i} Z_i
+template <typename B>
+cudaError_t kr_resid(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
+                     double *part, double *norm2, cudaStream_t s);
+template <typename B, typename T>
+cudaError_t kr_apply(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vz,
+                     int vw, cudaStream_t s);
+template <typename B>
+cudaError_t kr_dots(const Launch &flat, const KDesc *kd, int vw, int nv, double *part, double *out,
                     int ostride, cudaStream_t s);
-cudaError_t kr_axpy(const Launch &L0, const KDesc *kd, int vd, int s0, int ns, const double *coef, int cs,
-                    cudaStream_t s);
-template <typename T>
-cudaError_t kr_stage(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
-                     cudaStream_t s);
-template <typename T>
-cudaError_t kr_unstage(const Launch &L0, const KDesc *kd, int vd, cudaStream_t s);
+template <typename B, typename T>
+cudaError_t kr_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
+                     int s0, int ns, const double *coef, int cs, bool stage, cudaStream_t s);
+template <typename B>
+cudaError_t kr_update(const Launch &flat, const KDesc *kd, int ns, const double *coef, int cs,
+                      cudaStream_t s);
 }  // namespace k
 
 }  // namespace fg

@@ -1800,24 +1800,47 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
 }
 
 // ------------------------------------------------------------- FGMRES
-// Krylov vectors of one problem: `nvec` FP64 fields of the finest level's
-// layout (n elements each) starting at base; vector v is base + v*n.  All
-// vectors are zero outside the rows of the system (active and ghost/dead
-// cells), so sums over every interior cell are sums over the rows.
+// Vector v of a Krylov set (basis V or preconditioned Z) of one problem.
+template <typename B>
+__device__ __forceinline__ dptr<B> kvec(const KDesc &d, void *base, int v) {
+  return mkptr(reinterpret_cast<B *>(base) + (long long)v * d.stride, d.n, K_X);
+}
+
 __device__ __forceinline__ bool is_row(const DevLevel &L, long long id, uint8_t mk) {
   return (mk & 64) || L.type[id] == T_GHOST;
 }
 
-// dst = F - A P on active rows, 0 on every other interior cell; part[b] =
+// (A x) at an active cell in FP64 from values of type T: the sum of
+// apply_row (kept faces a (x_n - x_c), Dirichlet boundary faces -2 a x_c)
+template <typename T, typename P>
+__device__ __forceinline__ double apply_row_d(const DevLevel &L, long long id, int i, int j, int k,
+                                              uint8_t mk, const P &x) {
+  const double xc = (double)x[id];
+  const double xn[6] = {(double)x[id - 1],    (double)x[id + 1],    (double)x[id - L.sy],
+                        (double)x[id + L.sy], (double)x[id - L.sz], (double)x[id + L.sz]};
+  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+  const bool atb[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
+  double acc = 0.0, diag = 0.0;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    if ((mk >> q) & 1) { acc += a[q] * xn[q]; diag -= a[q]; }
+    else if (atb[q] && L.bc[q]) diag -= 2.0 * a[q];
+  }
+  return acc + diag * xc;
+}
+
+// V_vd = F - A P on active rows, 0 on every other interior cell; part[b] =
 // block sum of the squared active-row residuals (fluid-row norm)
+template <typename B>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vp, int vf, int vd,
-           double *part) {
+k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  const double *P = kd[p].base + vp * kd[p].n, *F = kd[p].base + vf * kd[p].n;
-  double *D = kd[p].base + vd * kd[p].n;
+  const KDesc &d = kd[p];
+  auto P = mkptr<const double>(d.P, d.n, K_X);
+  auto F = mkptr<const double>(d.F, d.n, K_RHS);
+  auto D = kvec<B>(d, d.V, vd);
   double r2 = 0.0;
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(L, lb, rr);
@@ -1825,90 +1848,157 @@ k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
     const long long id = c.i + L.sy * c.j + L.sz * c.k;
     const uint8_t mk = L.mask[id];
     double r = 0.0;
-    if (mk & 64) r = F[id] - apply_row<double>(L, id, c.i, c.j, c.k, mk, mkptr(P, kd[p].n, K_X));
-    D[id] = r;
+    if (mk & 64) r = F[id] - apply_row_d<double>(L, id, c.i, c.j, c.k, mk, P);
+    D[id] = (B)r;
     r2 += r * r;
   }
   const double t = block_sum(r2);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// dst = A src on active rows, 0 on every other interior cell
+// Preconditioner output x_T into Z_vz (rows; 0 elsewhere) and W = A x_T
+// into V_vw on active rows (0 on every other interior cell).  x_T is zero on
+// the pure-solid cells an active row may couple to (they are held at the
+// staged zero), so A x_T equals A Z_vz there.
+template <typename B, typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_apply(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vs, int vd) {
+k_kr_apply(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  const double *S = kd[p].base + vs * kd[p].n;
-  double *D = kd[p].base + vd * kd[p].n;
+  const KDesc &d = kd[p];
+  auto x = PrecOf<T>::x(L);
+  auto Z = kvec<B>(d, d.Z, vz);
+  auto W = kvec<B>(d, d.V, vw);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(L, lb, rr);
     if (!c.ok) continue;
     const long long id = c.i + L.sy * c.j + L.sz * c.k;
     const uint8_t mk = L.mask[id];
-    D[id] = (mk & 64) ? apply_row<double>(L, id, c.i, c.j, c.k, mk, mkptr(S, kd[p].n, K_X)) : 0.0;
+    Z[id] = is_row(L, id, mk) ? (B)x[id] : B(0);
+    W[id] = (mk & 64) ? (B)apply_row_d<T>(L, id, c.i, c.j, c.k, mk, x) : B(0);
   }
 }
 
-// interpolation rows: mode 0 -> dst[t] = c0 + sum w src[corner] - src[t]
-// (residual of x_t - sum w x = c0), mode 1 -> dst[t] = src[t] - sum w
-// src[corner] (the row of A), mode 2 -> correction constants of the
-// preconditioner: rd = rf = src[t]
+// interpolation rows: mode 0 -> V_vd[t] = c0 + sum w P[corner] - P[t] (the
+// row's residual in solution form), mode 1 -> V_vd[t] = Z_vs[t] - sum w
+// Z_vs[corner] (the row of A), mode 2 -> correction constants of the
+// preconditioner: rd = rf = V_vs[t]
+template <typename B>
 __global__ void __launch_bounds__(CELL_BLOCK)
 k_kr_rows(DevRows R, const DevLevel *lev0, const KDesc *kd, int mode, int vs, int vd) {
   const int r = blockIdx.x * CELL_BLOCK + threadIdx.x;
   if (r >= R.n) return;
   const int p = R.prob[r];
   const DevLevel &L = lev0[p];
-  const double *S = kd[p].base + vs * kd[p].n;
+  const KDesc &d = kd[p];
   const long long t = R.tgt[r];
   if (mode == 2) {
-    R.rd[r] = S[t];
-    R.rf[r] = (float)S[t];
+    const B v = kvec<B>(d, d.V, vs)[t];
+    R.rd[r] = (double)v;
+    R.rf[r] = (float)v;
     return;
   }
-  double *D = kd[p].base + vd * kd[p].n;
+  auto D = kvec<B>(d, d.V, vd);
   const long long b = R.cell[r], sy = L.sy, sz = L.sz;
   const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
   double acc = 0.0;
+  if (mode == 0) {
+    auto S = mkptr<const double>(d.P, d.n, K_X);
 #pragma unroll
-  for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * S[b + o[q]];
-  D[t] = mode == 0 ? R.c0[r] + acc - S[t] : S[t] - acc;
+    for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * S[b + o[q]];
+    D[t] = (B)(R.c0[r] + acc - S[t]);
+  } else {
+    auto S = kvec<B>(d, d.Z, vs);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * (double)S[b + o[q]];
+    D[t] = (B)((double)S[t] - acc);
+  }
 }
 
-// block partials of (w, v_i) for i < nv and of (w, w): part[i * nblk + b]
-__global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_dots(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vw, int v0, int nv,
-          int nblk, double *part) {
+// Flat passes over Krylov vectors: 4-element pieces starting at element 1
+// (16-byte aligned by the padding), FLAT_PPT pieces per thread interleaved
+// across the block so every load instruction covers consecutive pieces.
+// Elements 0 and past the last piece are boundary cells, zero in every
+// vector and never written.
+constexpr int FLAT_THREADS = 256;
+constexpr int FLAT_PPT = 4;
+int blocks_flat(long long n) {
+  const long long nq = (n - 1) / 4;
+  return (int)((nq + FLAT_THREADS * FLAT_PPT - 1) / (FLAT_THREADS * FLAT_PPT));
+}
+__device__ __forceinline__ long long flat_elem(int lb, int u) {
+  return 1 + 4 * (((long long)lb * FLAT_PPT + u) * FLAT_THREADS + threadIdx.x);
+}
+__device__ __forceinline__ long long flat_end(long long n) { return 1 + 4 * ((n - 1) / 4); }
+
+// block partials of (V_vw, V_i) for i < nv and of (V_vw, V_vw):
+// part[i * nblk + b], part[nv * nblk + b]
+template <typename B>
+__global__ void __launch_bounds__(FLAT_THREADS)
+k_kr_dots(const int *off, int nent, const KDesc *kd, int vw, int nv, int nblk, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
-  const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  const long long n = kd[p].n;
-  const double *Wv = kd[p].base + vw * n;
-  const double *V = kd[p].base + v0 * n;
+  const KDesc &d = kd[p];
+  const long long lim = flat_end(d.n);
+  B w[FLAT_PPT][4];
+  bool ok[FLAT_PPT];
   double acc[KR_MAXV + 1];
 #pragma unroll
   for (int i = 0; i <= KR_MAXV; ++i) acc[i] = 0.0;
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    const double w = Wv[id];
+  {
+    auto W = kvec<B>(d, d.V, vw);
 #pragma unroll
-    for (int i = 0; i < KR_MAXV; ++i)
-      if (i < nv) acc[i] += w * V[id + i * n];
-    acc[KR_MAXV] += w * w;
-  }
+    for (int u = 0; u < FLAT_PPT; ++u) {
+      const long long e = flat_elem(lb, u);
+      ok[u] = e < lim;
+      if (ok[u]) load_run<B, 4>(w[u], W, e);
+      else
 #pragma unroll
-  for (int i = 0; i < KR_MAXV; ++i) {
-    if (i < nv) {  // nv is the same for the whole block
-      const double t = block_sum(acc[i]);
-      if (threadIdx.x == 0) part[(size_t)i * nblk + blockIdx.x] = t;
-      __syncthreads();
+        for (int q = 0; q < 4; ++q) w[u][q] = B(0);
     }
   }
-  const double t = block_sum(acc[KR_MAXV]);
-  if (threadIdx.x == 0) part[(size_t)nv * nblk + blockIdx.x] = t;
+#pragma unroll
+  for (int u = 0; u < FLAT_PPT; ++u)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[KR_MAXV] += (double)w[u][q] * (double)w[u][q];
+#pragma unroll
+  for (int i = 0; i < KR_MAXV; ++i) {
+    if (i < nv) {
+      auto V = kvec<B>(d, d.V, i);
+      B v[FLAT_PPT][4];
+#pragma unroll
+      for (int u = 0; u < FLAT_PPT; ++u) {
+        if (ok[u]) load_run<B, 4>(v[u], V, flat_elem(lb, u));
+        else
+#pragma unroll
+          for (int q = 0; q < 4; ++q) v[u][q] = B(0);
+      }
+#pragma unroll
+      for (int u = 0; u < FLAT_PPT; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[i] += (double)w[u][q] * (double)v[u][q];
+    }
+  }
+  __shared__ double red[FLAT_THREADS / 32][KR_MAXV + 1];
+  const int wi = threadIdx.x >> 5, ln = threadIdx.x & 31;
+#pragma unroll
+  for (int i = 0; i <= KR_MAXV; ++i) {
+    if (i < nv || i == KR_MAXV) {
+      double v = acc[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (ln == 0) red[wi][i] = v;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x <= nv) {
+    const int slot = (int)threadIdx.x < nv ? (int)threadIdx.x : KR_MAXV;
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < FLAT_THREADS / 32; ++q) t += red[q][slot];
+    part[(size_t)threadIdx.x * nblk + blockIdx.x] = t;
+  }
 }
 
 // out[p * ostride + i] = sum of part[i * nblk + off[p] .. off[p+1]) for
@@ -1930,134 +2020,188 @@ k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostri
   }
 }
 
-// dst = coef[p*cs] * dst + sum_{i<ns} coef[p*cs + 1 + i] * vec(s0 + i)
-__global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_axpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, int s0, int ns,
-          const double *coef, int cs) {
+// V_vd = c0 V_vd + sum_{i<ns} c_{1+i} V_{s0+i} (FP64 arithmetic); with
+// stage, rhs_T = V_vd on active rows (0 elsewhere) and x_T = 0
+template <typename B, typename T>
+__global__ void __launch_bounds__(FLAT_THREADS)
+k_kr_vaxpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, int s0, int ns,
+           const double *coef, int cs, int stage) {
   const int p = find_entry(off, nent, blockIdx.x);
-  const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  const long long n = kd[p].n;
-  double *D = kd[p].base + vd * n;
-  const double *S = kd[p].base + s0 * n;
+  const KDesc &d = kd[p];
+  const long long lim = flat_end(d.n);
   const double *cf = coef + (size_t)p * cs;
-  const double a0 = cf[0];
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    double v = a0 * D[id];
-    for (int i = 0; i < ns; ++i) v += cf[1 + i] * S[id + i * n];
-    D[id] = v;
+  auto D = kvec<B>(d, d.V, vd);
+  double acc[FLAT_PPT][4];
+  bool ok[FLAT_PPT];
+  {
+    const double c0 = cf[0];
+#pragma unroll
+    for (int u = 0; u < FLAT_PPT; ++u) {
+      const long long e = flat_elem(lb, u);
+      ok[u] = e < lim;
+      B v[4] = {B(0), B(0), B(0), B(0)};
+      if (ok[u]) load_run<B, 4>(v, D, e);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[u][q] = c0 * (double)v[q];
+    }
   }
-}
-
-// preconditioner input: rhs_T = v on active rows (0 elsewhere), x_T = 0
-template <typename T>
-__global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_stage(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vs) {
-  const int p = find_entry(off, nent, blockIdx.x);
+  for (int i = 0; i < ns; ++i) {
+    const double ci = cf[1 + i];
+    auto S = kvec<B>(d, d.V, s0 + i);
+    B v[FLAT_PPT][4];
+#pragma unroll
+    for (int u = 0; u < FLAT_PPT; ++u) {
+      if (ok[u]) load_run<B, 4>(v[u], S, flat_elem(lb, u));
+      else
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[u][q] = B(0);
+    }
+#pragma unroll
+    for (int u = 0; u < FLAT_PPT; ++u)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[u][q] += ci * (double)v[u][q];
+  }
   const DevLevel &L = levs[p];
-  const int lb = blockIdx.x - off[p];
-  const double *S = kd[p].base + vs * kd[p].n;
-  auto x = PrecOf<T>::x(L);
-  auto rhs = PrecOf<T>::rhs(L);
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    rhs[id] = (L.mask[id] & 64) ? (T)S[id] : T(0);
-    x[id] = T(0);
+#pragma unroll
+  for (int u = 0; u < FLAT_PPT; ++u) {
+    if (!ok[u]) continue;
+    const long long e = flat_elem(lb, u);
+    B o[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) o[q] = (B)acc[u][q];
+    store_run<B, 4>(D, e, o, 4);
+    if (stage) {
+      uint8_t m4[4];
+      load_run<uint8_t, 4>(m4, L.mask, e);
+      T r4[4], z4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) { r4[q] = (m4[q] & 64) ? (T)o[q] : T(0); z4[q] = T(0); }
+      store_run<T, 4>(PrecOf<T>::rhs(L), e, r4, 4);
+      store_run<T, 4>(PrecOf<T>::x(L), e, z4, 4);
+    }
   }
 }
 
-// preconditioner output: z = x_T on rows, 0 elsewhere
-template <typename T>
-__global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_unstage(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd) {
+// P += sum_{i<ns} c_{1+i} Z_i (c_0 is 1)
+template <typename B>
+__global__ void __launch_bounds__(FLAT_THREADS)
+k_kr_update(const int *off, int nent, const KDesc *kd, int ns, const double *coef, int cs) {
   const int p = find_entry(off, nent, blockIdx.x);
-  const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
-  double *D = kd[p].base + vd * kd[p].n;
-  auto x = PrecOf<T>::x(L);
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    D[id] = is_row(L, id, L.mask[id]) ? (double)x[id] : 0.0;
+  const KDesc &d = kd[p];
+  const long long lim = flat_end(d.n);
+  const double *cf = coef + (size_t)p * cs;
+  auto P = mkptr<double>(d.P, d.n, K_X);
+  double acc[FLAT_PPT][4];
+  bool ok[FLAT_PPT];
+#pragma unroll
+  for (int u = 0; u < FLAT_PPT; ++u) {
+    const long long e = flat_elem(lb, u);
+    ok[u] = e < lim;
+    if (ok[u]) load_run<double, 4>(acc[u], P, e);
   }
+  for (int i = 0; i < ns; ++i) {
+    const double ci = cf[1 + i];
+    auto S = kvec<B>(d, d.Z, i);
+#pragma unroll
+    for (int u = 0; u < FLAT_PPT; ++u) {
+      if (!ok[u]) continue;
+      B v[4];
+      load_run<B, 4>(v, S, flat_elem(lb, u));
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[u][q] += ci * (double)v[q];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < FLAT_PPT; ++u)
+    if (ok[u]) store_run<double, 4>(P, flat_elem(lb, u), acc[u], 4);
 }
 
-cudaError_t kr_resid(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vp,
-                     int vf, int vd, double *part, double *norm2, cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
-  k_kr_resid<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vp, vf, vd, part);
-  k_reduce_parts<<<L0.n, 1024, 0, s>>>(L0.off, part, norm2);
+static int rows_blocks(const DevRows &R) { return (R.n + CELL_BLOCK - 1) / CELL_BLOCK; }
+
+template <typename B>
+cudaError_t kr_resid(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
+                     double *part, double *norm2, cudaStream_t s) {
+  if (cells.empty()) return cudaSuccess;
+  k_kr_resid<B><<<cells.blocks, CELL_BLOCK, 0, s>>>(cells.off, cells.n, cells.lev, kd, vd, part);
+  k_reduce_parts<<<cells.n, 1024, 0, s>>>(cells.off, part, norm2);
   note_launches(2);
   if (R.n > 0) {
-    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, vp, vd);
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, 0, vd);
     note_launches(1);
   }
   return cudaGetLastError();
 }
 
-cudaError_t kr_apply(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
-                     int vd, cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
-  k_kr_apply<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vs, vd);
+template <typename B, typename T>
+cudaError_t kr_apply(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vz,
+                     int vw, cudaStream_t s) {
+  if (cells.empty()) return cudaSuccess;
+  k_kr_apply<B, T><<<cells.blocks, CELL_BLOCK, 0, s>>>(cells.off, cells.n, cells.lev, kd, vz, vw);
   note_launches(1);
   if (R.n > 0) {
-    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vs, vd);
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vz, vw);
     note_launches(1);
   }
   return cudaGetLastError();
 }
 
-cudaError_t kr_dots(const Launch &L0, const KDesc *kd, int vw, int v0, int nv, double *part, double *out,
+template <typename B>
+cudaError_t kr_dots(const Launch &flat, const KDesc *kd, int vw, int nv, double *part, double *out,
                     int ostride, cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
+  if (flat.empty()) return cudaSuccess;
   if (nv > KR_MAXV) return cudaErrorInvalidValue;
-  k_kr_dots<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vw, v0, nv, L0.blocks, part);
-  k_kr_reduce<<<dim3(L0.n, nv + 1), 256, 0, s>>>(L0.off, part, L0.blocks, out, ostride);
+  k_kr_dots<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, vw, nv, flat.blocks, part);
+  k_kr_reduce<<<dim3(flat.n, nv + 1), 256, 0, s>>>(flat.off, part, flat.blocks, out, ostride);
   note_launches(2);
   return cudaGetLastError();
 }
 
-cudaError_t kr_axpy(const Launch &L0, const KDesc *kd, int vd, int s0, int ns, const double *coef, int cs,
-                    cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
-  k_kr_axpy<<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vd, s0, ns, coef, cs);
+template <typename B, typename T>
+cudaError_t kr_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
+                     int s0, int ns, const double *coef, int cs, bool stage, cudaStream_t s) {
+  if (flat.empty()) return cudaSuccess;
+  if (ns > KR_MAXV) return cudaErrorInvalidValue;
+  k_kr_vaxpy<B, T><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, flat.lev, kd, vd, s0, ns, coef,
+                                                        cs, stage ? 1 : 0);
   note_launches(1);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t kr_stage(const Launch &L0, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vs,
-                     cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
-  k_kr_stage<T><<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vs);
-  note_launches(1);
-  if (R.n > 0) {
-    k_kr_rows<<<(R.n + CELL_BLOCK - 1) / CELL_BLOCK, CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, vs, vs);
+  if (stage && R.n > 0) {
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, vd, vd);
     note_launches(1);
   }
   return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t kr_unstage(const Launch &L0, const KDesc *kd, int vd, cudaStream_t s) {
-  if (L0.empty()) return cudaSuccess;
-  k_kr_unstage<T><<<L0.blocks, CELL_BLOCK, 0, s>>>(L0.off, L0.n, L0.lev, kd, vd);
+template <typename B>
+cudaError_t kr_update(const Launch &flat, const KDesc *kd, int ns, const double *coef, int cs,
+                      cudaStream_t s) {
+  if (flat.empty() || ns == 0) return cudaSuccess;
+  if (ns > KR_MAXV) return cudaErrorInvalidValue;
+  k_kr_update<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, ns, coef, cs);
   note_launches(1);
   return cudaGetLastError();
 }
 
-template cudaError_t kr_stage<double>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
-                                      cudaStream_t);
-template cudaError_t kr_stage<float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
+template cudaError_t kr_resid<float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
+                                     double *, double *, cudaStream_t);
+template cudaError_t kr_resid<double>(const Launch &, const DevRows &, const DevLevel *, const KDesc *, int,
+                                      double *, double *, cudaStream_t);
+template cudaError_t kr_apply<float, float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *,
+                                            int, int, cudaStream_t);
+template cudaError_t kr_apply<double, double>(const Launch &, const DevRows &, const DevLevel *,
+                                              const KDesc *, int, int, cudaStream_t);
+template cudaError_t kr_dots<float>(const Launch &, const KDesc *, int, int, double *, double *, int,
+                                    cudaStream_t);
+template cudaError_t kr_dots<double>(const Launch &, const KDesc *, int, int, double *, double *, int,
                                      cudaStream_t);
-template cudaError_t kr_unstage<double>(const Launch &, const KDesc *, int, cudaStream_t);
-template cudaError_t kr_unstage<float>(const Launch &, const KDesc *, int, cudaStream_t);
+template cudaError_t kr_vaxpy<float, float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *,
+                                            int, int, int, const double *, int, bool, cudaStream_t);
+template cudaError_t kr_vaxpy<double, double>(const Launch &, const DevRows &, const DevLevel *,
+                                              const KDesc *, int, int, int, const double *, int, bool,
+                                              cudaStream_t);
+template cudaError_t kr_update<float>(const Launch &, const KDesc *, int, const double *, int, cudaStream_t);
+template cudaError_t kr_update<double>(const Launch &, const KDesc *, int, const double *, int, cudaStream_t);
 
 #ifdef FG_CHECKED
 // first recorded out-of-range access of a checked build: {hits, index,
