@@ -793,15 +793,17 @@ k_xline_smem(const int *off, int nent, const DevLevel *levs, int color, T omega)
   using LC = LineCoefT<T, 0>;
   constexpr int P = XS_PIECE;
   extern __shared__ __align__(16) unsigned char xs_smem[];
-  __shared__ T s_am[32 * M], s_ap[32 * M];  // couplings along x (one level per block)
+  // couplings along x (one level per block), row r at r + r / M: lane l's
+  // chunk starts at l (M + 1), so the lanes' reads fall in distinct banks
+  __shared__ T s_am[32 * (M + 1)], s_ap[32 * (M + 1)];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
   const int n = L.nx;
   for (int r = threadIdx.x; r < n; r += XS_WARPS * 32) {
-    s_am[r] = (T)L.amx[1 + r];
-    s_ap[r] = (T)L.apx[1 + r];
+    s_am[r + r / M] = (T)L.amx[1 + r];
+    s_ap[r + r / M] = (T)L.apx[1 + r];
   }
   __syncthreads();
   int j, k;
@@ -852,7 +854,8 @@ k_xline_smem(const int *off, int nent, const DevLevel *levs, int color, T omega)
   lds_chunk<T, M>(s_d + lane * LY::CT, d);
   lds_mask<M>(s_mk + lane * M, mk);
   T aF, bF, cF, dF, aL, cL, dL;
-  chunk_eliminate_t<T, M>(r0, r0 < n ? n : r0, mk, d, al, ga, s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
+  chunk_eliminate_t<T, M>(r0, r0 < n ? n : r0, mk, d, al, ga, s_am + lane, s_ap + lane, lc, aF, bF, cF, dF,
+                          aL, cL, dL);
   T aLp = __shfl_up_sync(0xffffffffu, aL, 1);
   T cLp = __shfl_up_sync(0xffffffffu, cL, 1);
   T dLp = __shfl_up_sync(0xffffffffu, dL, 1);
@@ -891,8 +894,12 @@ k_xline_smem(const int *off, int nent, const DevLevel *levs, int color, T omega)
 // through shared memory and one thread per line solves them (Thomas),
 // then every thread back-substitutes its rows.
 constexpr int YZ_MAXROWS = 256;  // longest line of k_yzline_reg (M 16 x CH 16)
+constexpr int YP_LINES = 8;      // lines per block of k_yzline_pcr
+constexpr int YP_MINROWS = 65;   // shortest line of k_yzline_pcr
 template <typename T>
 struct ChunkEq { T a, b, c, d; };
+template <typename T>
+struct Eq3 { T a, c, d; };  // a x_prev + x + c x_next = d
 
 template <typename T, int M, int CH, int AXIS>
 __global__ void __launch_bounds__(CH * 32, (sizeof(T) == 4 && CH == 16) ? (M <= 8 ? 3 : 2) : 1)
@@ -1171,7 +1178,8 @@ int blocks_xline(const DevLevel &L, int maxn) {
   return (int)((lines + per_block - 1) / per_block);
 }
 int blocks_tile(const DevLevel &L, int axis, int maxn) {
-  const int w = maxn <= YZ_MAXROWS ? 64 : TILE_I;  // k_yzline_reg or k_yzline
+  // k_yzline_reg, k_yzline_pcr or k_yzline
+  const int w = maxn < YP_MINROWS ? 64 : maxn <= YZ_MAXROWS ? 2 * YP_LINES : TILE_I;
   const int ntx = (L.nx + w - 1) / w;
   return ntx * (axis == 1 ? L.nz : L.ny);
 }
@@ -1222,12 +1230,150 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
   return cudaGetLastError();
 }
 
+// Zebra y/z line relaxation in short chunks, for lines of YP_MINROWS..
+// YZ_MAXROWS cells.  A block takes YP_LINES lines of one colour in an i-tile
+// of 2 YP_LINES cells (thread t: line t % YP_LINES at i = i0 + par + 2 (t % YP_LINES),
+// chunk t / YP_LINES of CH chunks of M rows).  Every thread issues the
+// loads of all its rows at once, eliminates its chunk in registers, the CH
+// chunk equations of each line are solved by parallel cyclic reduction
+// across the block (log2 CH steps through shared memory), and every thread
+// back-substitutes its rows.
+template <typename T, int M, int CH, int AXIS>
+__global__ void __launch_bounds__(CH * YP_LINES, ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
+                                                   ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1)
+k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+  using LC = LineCoefT<T, AXIS>;
+  constexpr int NT = CH * YP_LINES;
+  __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
+  // two buffers of unit-diagonal chunk equations (a, c, d); the last-row
+  // equations of the chunks (aL, cL, dL) use the second before the reduction
+  extern __shared__ __align__(16) unsigned char yp_smem[];
+  auto s_eq = reinterpret_cast<Eq3<T>(*)[CH][YP_LINES]>(yp_smem);
+  auto s_last = reinterpret_cast<T(*)[CH][YP_LINES]>(&s_eq[1][0][0]);
+  const int tid = threadIdx.x;
+  const int l = tid % YP_LINES, c = tid / YP_LINES;
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  constexpr int TW = 2 * YP_LINES;  // cells of an i-tile
+  const int ntx = (L.nx + TW - 1) / TW;
+  const int ti = lb % ntx;
+  const int o = 1 + lb / ntx;  // k for AXIS 1, j for AXIS 2
+  const int i0 = 1 + TW * ti;
+  const int par = (color + i0 + o) & 1;
+  const int i = i0 + par + 2 * l;
+  const bool valid = i <= L.nx;
+  const int n = AXIS == 1 ? L.ny : L.nz;
+  const long long ls = AXIS == 1 ? L.sy : L.sz;  // row stride along the line
+  const long long os = AXIS == 1 ? L.sz : L.sy;  // stride of the fixed index
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  {
+    auto am = AXIS == 1 ? L.amy : L.amz;
+    auto ap = AXIS == 1 ? L.apy : L.apz;
+    for (int r = tid; r < n; r += NT) { s_am[r] = (T)am[1 + r]; s_ap[r] = (T)ap[1 + r]; }
+  }
+  const LC lc(line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1));
+  const bool iso_line = lc.iso();
+  const long long base = (long long)(valid ? i : L.nx) + os * o;  // row index 0 of the line
+  const int r0 = c * M;
+  const bool any = valid && r0 < n;
+  T d[M], al[M], ga[M];
+  uint8_t mk[M];
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    d[u] = T(0);
+    mk[u] = 0;
+    if (any && r < n) {
+      const long long id = base + ls * (r + 1);
+      uint8_t m8 = L.mask[id];
+      const T rv = rhs[id];
+      const T xv = x[id];
+      const T nb[4] = {x[id - 1], x[id + 1], x[id - os], x[id + os]};
+      T acc = rv;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
+      const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+      if (held) { acc = xv; m8 = 0; }
+      d[u] = acc;
+      mk[u] = m8;
+    }
+  }
+  __syncthreads();  // s_am, s_ap
+  T aF, bF, cF, dF, aL, cL, dL;
+  chunk_eliminate_t<T, M>(r0, any ? n : r0, mk, d, al, ga, s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
+  s_last[0][c][l] = aL;
+  s_last[1][c][l] = cL;
+  s_last[2][c][l] = dL;
+  __syncthreads();
+  {
+    // equation of the chunk-first unknowns (previous chunk's last row
+    // eliminated), normalised to a unit diagonal
+    T aLp = T(0), cLp = T(0), dLp = T(0);
+    if (c > 0) { aLp = s_last[0][c - 1][l]; cLp = s_last[1][c - 1][l]; dLp = s_last[2][c - 1][l]; }
+    const T rb = rcp_nr(bF - aF * cLp - cF * aL);
+    Eq3<T> e;
+    e.a = -aF * aLp * rb;
+    e.c = -cF * cL * rb;
+    e.d = (dF - aF * dLp - cF * dL) * rb;
+    __syncthreads();  // every s_last read before the buffers are written
+    s_eq[0][c][l] = e;
+  }
+  __syncthreads();
+  int buf = 0;
+#pragma unroll
+  for (int st = 1; st < CH; st <<= 1) {
+    const Eq3<T> cur = s_eq[buf][c][l];
+    Eq3<T> lo{T(0), T(0), T(0)}, hi{T(0), T(0), T(0)};
+    if (c >= st) lo = s_eq[buf][c - st][l];
+    if (c + st < CH) hi = s_eq[buf][c + st][l];
+    const T rn = rcp_nr(T(1) - cur.a * lo.c - cur.c * hi.a);
+    Eq3<T> ne;
+    ne.a = -cur.a * lo.a * rn;
+    ne.c = -cur.c * hi.c * rn;
+    ne.d = (cur.d - cur.a * lo.d - cur.c * hi.d) * rn;
+    s_eq[buf ^ 1][c][l] = ne;
+    buf ^= 1;
+    __syncthreads();
+  }
+  const T xF = s_eq[buf][c][l].d;
+  const T xFn = c + 1 < CH ? s_eq[buf][c + 1][l].d : T(0);
+  if (!any) return;
+  const T xL = dL - aL * xF - cL * xFn;
+#pragma unroll
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    if (r >= n) break;
+    T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+    const long long id = base + ls * (r + 1);
+    if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+    x[id] = v;
+  }
+}
+
 template <typename T, int M>
 static cudaError_t launch_xsmem(const Launch &Lr, int color, double omega, cudaStream_t s) {
   const size_t sm = (size_t)XS_WARPS * XsLayout<T, M>::PER_WARP;
   auto kern = k_xline_smem<T, M>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   kern<<<Lr.blocks, XS_WARPS * 32, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template <typename T, int M, int CH>
+static cudaError_t launch_yzpcr(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
+  const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
+  if (axis == 1) {
+    auto kern = k_yzline_pcr<T, M, CH, 1>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  } else {
+    auto kern = k_yzline_pcr<T, M, CH, 2>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+  }
   note_launches(1);
   return cudaGetLastError();
 }
@@ -1265,6 +1411,10 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
     if (maxn <= 512) return launch_xsmem<T, 16>(Lr, color, omega, s);
     if (maxn <= 1024) return launch_xsmem<T, 32>(Lr, color, omega, s);
     return cudaErrorInvalidValue;  // lines longer than 1024 cells
+  }
+  if (maxn >= YP_MINROWS && maxn <= YZ_MAXROWS) {
+    if (maxn <= 128) return launch_yzpcr<T, 8, 16>(Lr, axis, color, omega, s);
+    return launch_yzpcr<T, 8, 32>(Lr, axis, color, omega, s);
   }
   if (maxn <= YZ_MAXROWS) {
     if (maxn <= 16) return launch_yzreg<T, 4, 4>(Lr, axis, color, omega, s);
