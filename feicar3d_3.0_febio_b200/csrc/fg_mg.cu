@@ -33,7 +33,7 @@ constexpr int CELL_BLOCK = 128;
 // Cell kernels tile each level by rows: block lb covers cells
 // i = 1 + 128 t + threadIdx.x of row (j,k), so no thread divides by a
 // runtime extent (only one 32-bit division per block).
-constexpr int CELL_ROWS = 8;  // rows (j,k) per block
+constexpr int CELL_ROWS = 4;  // rows (j,k) per block
 struct CellIdx { int i, j, k; bool ok; };
 // cell of row r (0..CELL_ROWS-1) of block lb
 __device__ __forceinline__ CellIdx cell_of(const DevLevel &L, int lb, int r) {
