@@ -74,6 +74,12 @@ def workload(name):
                 synth.sphere_body((4.0, 4.0, 2.0), 1.0, 5),
                 "512x256x128 cells on [0,16]x[0,8]x[0,4], tanh-stretched (beta=2) in y,z; "
                 "sphere d=1 at (4,4,2): x, y, z lines of 512, 256, 128 cells (kernel profiling case)")
+    if name == "cube256":
+        return (synth.Grid(synth.uniform_nodes(256, 0, 8), synth.tanh_nodes(256, 0, 8, 2.0),
+                           synth.tanh_nodes(256, 0, 8, 2.0)),
+                synth.sphere_body((4.0, 4.0, 4.0), 1.0, 5),
+                "256x256x256 cells on [0,8]^3, tanh-stretched (beta=2) in y,z; sphere d=1 at (4,4,4): "
+                "the y and z line kernels of the 512x256x256 case on half its cells (kernel profiling case)")
     if name == "config0":
         return (synth.config0_grid(), synth.config0_body(),
                 "128x64x64 uniform cells on [0,8]x[0,4]x[0,4]; sphere d=1 at (2,2,2), "
