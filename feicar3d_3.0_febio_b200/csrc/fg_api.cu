@@ -334,6 +334,14 @@ struct fg_batch {
   double *d_kpart = nullptr, *d_kout = nullptr, *d_kcoef = nullptr;
   std::vector<double> h_kout, h_kcoef;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // the V-cycle captured as a CUDA graph (replayed while the batch's tables
+  // stay as built); key: precision and correction form
+  struct VGraph {
+    cudaGraphExec_t exec = nullptr;
+    int key = -1;
+    long long launches = 0;  // kernels per replay
+    bool off = false;        // capture failed once: launch directly
+  } vg;
   // optional CUDA-event timing of launch classes (fg_profile)
   struct Prof {
     bool on = false;
@@ -372,6 +380,8 @@ static void free_batch_tables(fg_batch *b) {
   cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
   cudaFree(b->d_norm); cudaFree(b->d_part);
   b->d_part = nullptr;
+  if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
+  b->vg = fg_batch::VGraph();
   for (void *r : b->kraw) cudaFree(r);
   b->kraw.clear();
   cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
@@ -626,6 +636,44 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
   return FG_OK;
 }
 
+// One V-cycle as a CUDA graph: captured on first use after the batch's
+// tables are built, then replayed (one launch instead of a few hundred on a
+// deep hierarchy).  Direct launches while launch classes are timed, while
+// the stream is already being captured by the caller, or after a capture
+// failed.
+template <typename T>
+static fg_status run_vcycle(fg_batch *b, cudaStream_t s) {
+  if (b->prof.on || b->vg.off) return vcycle<T>(b, s);
+  const int key = (sizeof(T) == 4 ? 1 : 0) | (b->krylov ? 2 : 0);
+  if (!b->vg.exec || b->vg.key != key) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FG_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return vcycle<T>(b, s);
+    if (b->vg.exec) { cudaGraphExecDestroy(b->vg.exec); b->vg.exec = nullptr; }
+    const long long n0 = thread_launches();
+    FG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const fg_status st = vcycle<T>(b, s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    const long long captured = thread_launches() - n0;
+    note_launches(-captured);  // counted when replayed
+    cudaError_t ei = cudaErrorUnknown;
+    if (st == FG_OK && e == cudaSuccess && g) ei = cudaGraphInstantiate(&b->vg.exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      b->vg.exec = nullptr;
+      b->vg.off = true;
+      (void)cudaGetLastError();
+      return vcycle<T>(b, s);
+    }
+    b->vg.key = key;
+    b->vg.launches = captured;
+  }
+  FG_CUDA(cudaGraphLaunch(b->vg.exec, s));
+  note_launches(b->vg.launches);
+  return FG_OK;
+}
+
 // Outer iteration over the whole batch until every problem meets rtol.
 static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st);
 
@@ -655,8 +703,8 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
   for (cyc = 1; cyc <= b->cfg.max_cycles; ++cyc) {
     cudaEventRecord(va, s);
     fg_status r;
-    if (mixed) r = vcycle<float>(b, s);
-    else r = vcycle<double>(b, s);
+    if (mixed) r = run_vcycle<float>(b, s);
+    else r = run_vcycle<double>(b, s);
     if (r != FG_OK) { cudaEventDestroy(va); cudaEventDestroy(vb); return r; }
     cudaEventRecord(vb, s);
     FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
@@ -857,7 +905,7 @@ static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
     for (int j = 0; j < m && cycles < b->cfg.max_cycles; ++j) {
       // ---- Z_j = M^-1 V_j (one V-cycle from zero, correction form)
       cudaEventRecord(va, s);
-      r = vcycle<T>(b, s);
+      r = run_vcycle<T>(b, s);
       if (r != FG_OK) { err = r; break; }
       cudaEventRecord(vb, s);
       ++cycles;

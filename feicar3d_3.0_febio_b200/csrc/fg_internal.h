@@ -138,6 +138,7 @@ const char *last_error_msg();
 // kernels launched by this process (every launch site adds its count)
 void note_launches(long long n);
 long long launches_so_far();
+long long thread_launches();  // launches noted by the calling thread
 
 #define FG_CUDA(call)                                                  \
   do {                                                                 \

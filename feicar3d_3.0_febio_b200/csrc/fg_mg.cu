@@ -20,8 +20,13 @@
 namespace fg {
 
 static std::atomic<long long> g_launches{0};
-void note_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local long long t_launches = 0;  // this thread's share
+void note_launches(long long n) {
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
 long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+long long thread_launches() { return t_launches; }
 
 namespace k {
 
