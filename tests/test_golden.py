@@ -89,3 +89,22 @@ def test_device_config0_pressure_sample(prec):
     ref = smp["p"]
     assert np.linalg.norm(v - ref) / np.linalg.norm(ref) <= 1e-9
     c.close()
+
+
+@pytest.mark.gpu
+def test_device_config2_plate_steps_match_oracle():
+    """The pitching plate moved step by step through one handle (as the
+    time loop re-tags it): iblank, ghostCellMark, dead_cell and the ghost /
+    dead lists equal the oracle's at further points of the period, on both
+    sides of the neutral position and on the way back."""
+    base = synth.config2_plate()
+    grid = synth.config2_grid()
+    c = fg.Case(grid, fg.default_config())
+    c.add_body(synth.config2_body(0))
+    for step in range(0, 80):
+        if step:
+            c.update_body(0, synth.config2_verts(base, step))
+        c.set_iblank_body_fast()
+        if step in (10, 40, 60, 79):
+            assert _device_digests(c) == _oracle_digests(grid, synth.config2_body(step)), step
+    c.close()
