@@ -42,11 +42,14 @@ METRIC = "Poisson solves/s & HBM GB/s, mixed vs FP64 MG at 1e-8 resid; p50/p99 l
 UNIT = "solves/s"
 RTOL = 1e-8
 
-# DRAM bytes per finest-level cell of one launch of the dominant kernel
+# DRAM bytes per finest-level cell of one colour launch of the dominant line
 # class, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
-# 128x64x64 sphere case, mixed path (profiles/line_smoother_config0_mixed.md).
-# None until that capture exists.
-DRAM_BYTES_PER_CELL = {}
+# 256^3 case, whose y and z lines run the same kernels as the 512x256x256
+# case's (256-row lines, k_yzline_pcr<float, 8, 32, axis>); a launch moves
+# the same bytes per cell, so the figure scales by the cell count
+# (profiles/yzline_pcr_cube256_mixed.md).
+DRAM_BYTES_PER_CELL = {("config1", "mixed", "line_y0"): (170.546 + 33.888) / 16.7772,
+                       ("config1", "mixed", "line_z0"): (170.532 + 34.614) / 16.7772}
 
 
 def _load_pkg():
@@ -536,7 +539,7 @@ def run_ours(args):
     traffic = None
     key = (args.workload, args.precision, dom)
     if key in DRAM_BYTES_PER_CELL:
-        traffic = DRAM_BYTES_PER_CELL[key] * cells / 2.0
+        traffic = DRAM_BYTES_PER_CELL[key] * cells
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
