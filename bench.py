@@ -609,6 +609,19 @@ def _oracle():
     return O
 
 
+def host_threads():
+    """Host threads this process may run on (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+PAR_NOTE = ("the line sweeps run as z-slabs, one per thread, as the reference runs them on nProcZ MPI "
+            "ranks (sequential inside a slab, the neighbour's plane from before the sweep across slab "
+            "faces, z lines in per-slab segments); residual and transfers in parallel loops")
+
+
 def cpu_baseline_sample(grid, body, rhs, iters):
     """The CPU restatement of the reference solver on the same grid, body
     and RHS: `iters` outer iterations of solve_poisson (each one MG cycle,
@@ -617,6 +630,8 @@ def cpu_baseline_sample(grid, body, rhs, iters):
     iteration count extrapolated from the measured per-iteration residual
     reduction."""
     O = _oracle()
+    nthr = host_threads()
+    O.set_threads(nthr)
     t0 = time.time()
     oc = O.OracleCase(grid)
     oc.add_body(body)
@@ -640,9 +655,11 @@ def cpu_baseline_sample(grid, body, rhs, iters):
     else:
         n_need = float("nan")
     val = 1.0 / (s_it * n_need) if n_need == n_need else None
-    return {"value": val, "unit": UNIT, "cores": 1, "kind": "port",
+    O.set_threads(1)
+    return {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
             "sample": f"{iters} outer iterations (one V-cycle each, iterInter=0) of the reference "
-                      f"solve_poisson restatement (MG V-cycle, line SOR, ghost-cell update) on the full grid; "
+                      f"solve_poisson restatement (MG V-cycle, line SOR, ghost-cell update) on the full grid, "
+                      f"{nthr} threads ({PAR_NOTE}); "
                       f"{s_it:.2f} s/iteration, residual factor {rho:.3f}/iteration, "
                       f"{n_need:.1f} iterations to 1e-8 (extrapolated); setup {t_setup:.1f} s untimed",
             "s_per_iteration": s_it, "relres": res}
@@ -656,6 +673,8 @@ def run_reference(args):
     grid, body, desc = workload(args.workload)
     synth = _load_pkg().synth
     O = _oracle()
+    nthr = host_threads()
+    O.set_threads(nthr)
     oc = O.OracleCase(grid)
     oc.add_body(body)
     oc.set_iblank()
@@ -681,7 +700,7 @@ def run_reference(args):
     n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
     val = 1.0 / (s_it * n_need) if n_need == n_need else 0.0
     sample = (f"each step one outer iteration (one V-cycle, iterInter=0) of the reference solve_poisson "
-              f"restatement on the full "
+              f"restatement on {nthr} threads ({PAR_NOTE}) on the full "
               f"grid (continued iterate); solves/s = 1/(s per iteration x {n_need:.1f} iterations to 1e-8, "
               f"extrapolated from residual factor {rho:.3f})")
     cells = (grid.nx - 1) * (grid.ny - 1) * (grid.nz - 1)
@@ -692,7 +711,7 @@ def run_reference(args):
         "config": {"workload": args.workload, "desc": desc, "cells": cells, "precision": "fp64",
                    "rtol": RTOL},
         "impl": "reference",
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthr, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "relres": res,
     }

@@ -1296,9 +1296,171 @@ static void outer_bc(or_case *c, double *pres, int lev, const or_params *prm) {
 #undef PL
 }
 
+/* itsolv_mg on `ns` z-slabs at once (ns = threads), as the reference runs
+ * it on nProcZ MPI ranks (CORE_PARALLEL pencils, one plane of halo): inside
+ * a slab the sweeps are the sequential ones above; across slab faces the
+ * neighbour's plane is its value before the sweep (a copy taken after each
+ * outer_bc, as the ranks exchange halos), and z lines are solved per slab
+ * segment with those halo values as fixed end rows.  ns = 1 is exactly the
+ * sequential sweep.  Used only for the timed CPU baseline. */
+static void itsolv_mg_slabs(or_case *c, int lev, double *var, const double *r,
+                            const int8_t *igk, const or_params *prm, int ns) {
+  const or_level *L = &c->lev[lev];
+  const int nxm = L->I, JL1 = 1, JL2 = L->J - 1, KL1 = 1, KL2 = L->K - 1;
+  const long NXl = L->I + 2, NYl = L->J + 2, PL = NXl * NYl;
+  const double om = prm->omega_pson;
+  const int nk = KL2 - KL1 + 1;
+  int nmax = L->I > L->J ? L->I : L->J;
+  if (L->K > nmax) nmax = L->K;
+  double *halo = dzalloc(2L * ns * PL);  /* slab s: [2s] plane lo-1, [2s+1] plane hi+1 */
+#define V(i, j, k) var[(long)(i) + NXl * ((long)(j) + NYl * (long)(k))]
+#define R(i, j, k) r[(long)(i) + NXl * ((long)(j) + NYl * (long)(k))]
+#define G(i, j, k) igk[(long)(i) + NXl * ((long)(j) + NYl * (long)(k))]
+#define SLO(s) (KL1 + (int)(((long)nk * (s)) / ns))
+#define SHI(s) (KL1 + (int)(((long)nk * ((s) + 1)) / ns) - 1)
+#define VH(i, j, k)                                                                              \
+  ((k) < lo ? halo[(2L * s) * PL + (i) + NXl * (long)(j)]                                       \
+            : (k) > hi ? halo[(2L * s + 1) * PL + (i) + NXl * (long)(j)] : V(i, j, k))
+#define TAKE_HALOS()                                                                             \
+  for (int s = 0; s < ns; ++s) {                                                                 \
+    memcpy(halo + (2L * s) * PL, var + (long)(SLO(s) - 1) * PL, sizeof(double) * (size_t)PL);    \
+    memcpy(halo + (2L * s + 1) * PL, var + (long)(SHI(s) + 1) * PL, sizeof(double) * (size_t)PL); \
+  }
+  /* x lines */
+  outer_bc(c, var, lev, prm);
+  TAKE_HALOS();
+#pragma omp parallel for num_threads(ns) schedule(static, 1)
+  for (int s = 0; s < ns; ++s) {
+    const int lo = SLO(s), hi = SHI(s);
+    double *w = dzalloc(6L * (nmax + 2));
+    double *am = w, *ac = w + (nmax + 2), *ap = w + 2 * (nmax + 2), *rh = w + 3 * (nmax + 2);
+    double *du = w + 4 * (nmax + 2), *g = w + 5 * (nmax + 2);
+    for (int k = lo; k <= hi; ++k) {
+      double amz = L->dzcinv[k] * L->dzinv[k];
+      double apz = L->dzcinv[k + 1] * L->dzinv[k];
+      double acz = -(amz + apz);
+      for (int j = JL1; j <= JL2; ++j) {
+        double amy = L->dycinv[j] * L->dyinv[j];
+        double apy = L->dycinv[j + 1] * L->dyinv[j];
+        double acy = -(amy + apy);
+        for (int i = 1; i <= nxm - 1; ++i) {
+          am[i] = L->dxcinv[i] * L->dxinv[i];
+          ap[i] = L->dxcinv[i + 1] * L->dxinv[i];
+          ac[i] = -(am[i] + ap[i]);
+          rh[i] = R(i, j, k) - V(i, j - 1, k) * amy - V(i, j + 1, k) * apy - VH(i, j, k - 1) * amz -
+                  VH(i, j, k + 1) * apz;
+          double flag = (double)(1 - G(i, j, k));
+          am[i] = am[i] * flag;
+          ap[i] = ap[i] * flag;
+          ac[i] = (ac[i] + acy + acz) * flag + (1.0 - flag);
+          rh[i] = rh[i] * flag + (1.0 - flag) * V(i, j, k);
+          if (fabs(ac[i]) < TINY_F32) { am[i] = 0.0; ap[i] = 0.0; ac[i] = 1.0; rh[i] = V(i, j, k); }
+        }
+        am[0] = 0.0; ap[0] = 0.0; ac[0] = 1.0; rh[0] = V(0, j, k);
+        am[nxm] = 0.0; ap[nxm] = 0.0; ac[nxm] = 1.0; rh[nxm] = V(nxm, j, k);
+        tdma_ws(am, ac, ap, rh, du, 0, nxm, g);
+        for (int i = 0; i <= nxm; ++i) V(i, j, k) = V(i, j, k) * (1.0 - om) + om * du[i];
+      }
+    }
+    free(w);
+  }
+  /* y lines, zebra in i */
+  const int j0 = JL1 - 1, j1 = JL2 + 1;
+  for (int col = 1; col <= 2; ++col) {
+    outer_bc(c, var, lev, prm);
+    TAKE_HALOS();
+#pragma omp parallel for num_threads(ns) schedule(static, 1)
+    for (int s = 0; s < ns; ++s) {
+      const int lo = SLO(s), hi = SHI(s);
+      double *w = dzalloc(6L * (nmax + 2));
+      double *am = w, *ac = w + (nmax + 2), *ap = w + 2 * (nmax + 2), *rh = w + 3 * (nmax + 2);
+      double *du = w + 4 * (nmax + 2), *g = w + 5 * (nmax + 2);
+      for (int k = lo; k <= hi; ++k) {
+        double amz = L->dzcinv[k] * L->dzinv[k];
+        double apz = L->dzcinv[k + 1] * L->dzinv[k];
+        double acz = -(amz + apz);
+        for (int i = col; i <= nxm - 1; i += 2) {
+          double amx = L->dxcinv[i] * L->dxinv[i];
+          double apx = L->dxcinv[i + 1] * L->dxinv[i];
+          double acx = -(amx + apx);
+          for (int j = JL1; j <= JL2; ++j) {
+            am[j] = L->dycinv[j] * L->dyinv[j];
+            ap[j] = L->dycinv[j + 1] * L->dyinv[j];
+            ac[j] = -(am[j] + ap[j]);
+            rh[j] = R(i, j, k) - V(i - 1, j, k) * amx - V(i + 1, j, k) * apx - VH(i, j, k - 1) * amz -
+                    VH(i, j, k + 1) * apz;
+            double flag = (double)(1 - G(i, j, k));
+            am[j] = am[j] * flag;
+            ap[j] = ap[j] * flag;
+            ac[j] = (acx + ac[j] + acz) * flag + (1.0 - flag);
+            rh[j] = rh[j] * flag + (1.0 - flag) * V(i, j, k);
+            if (fabs(ac[j]) < TINY_F32) { am[j] = 0.0; ap[j] = 0.0; ac[j] = 1.0; rh[j] = V(i, j, k); }
+          }
+          am[j0] = 0.0; ap[j0] = 0.0; ac[j0] = 1.0; rh[j0] = V(i, JL1 - 1, k);
+          am[j1] = 0.0; ap[j1] = 0.0; ac[j1] = 1.0; rh[j1] = V(i, JL2 + 1, k);
+          tdma_ws(am, ac, ap, rh, du, j0, j1, g);
+          for (int j = j0; j <= j1; ++j) V(i, j, k) = V(i, j, k) * (1.0 - om) + om * du[j];
+        }
+      }
+      free(w);
+    }
+  }
+  /* z lines, one segment per slab between the halo planes */
+  outer_bc(c, var, lev, prm);
+  TAKE_HALOS();
+#pragma omp parallel for num_threads(ns) schedule(static, 1)
+  for (int s = 0; s < ns; ++s) {
+    const int lo = SLO(s), hi = SHI(s);
+    double *w = dzalloc(6L * (nmax + 2));
+    double *am = w, *ac = w + (nmax + 2), *ap = w + 2 * (nmax + 2), *rh = w + 3 * (nmax + 2);
+    double *du = w + 4 * (nmax + 2), *g = w + 5 * (nmax + 2);
+    for (int j = JL1; j <= JL2; ++j) {
+      double amy = L->dycinv[j] * L->dyinv[j];
+      double apy = L->dycinv[j + 1] * L->dyinv[j];
+      double acy = -(amy + apy);
+      for (int i = 1; i <= nxm - 1; ++i) {
+        double amx = L->dxcinv[i] * L->dxinv[i];
+        double apx = L->dxcinv[i + 1] * L->dxinv[i];
+        double acx = -(amx + apx);
+        for (int k = lo; k <= hi; ++k) {
+          am[k] = L->dzcinv[k] * L->dzinv[k];
+          ap[k] = L->dzcinv[k + 1] * L->dzinv[k];
+          ac[k] = -(am[k] + ap[k]);
+          rh[k] = R(i, j, k) - V(i - 1, j, k) * amx - V(i + 1, j, k) * apx - V(i, j - 1, k) * amy -
+                  V(i, j + 1, k) * apy;
+          double flag = (double)(1 - G(i, j, k));
+          am[k] = am[k] * flag;
+          ap[k] = ap[k] * flag;
+          ac[k] = (acx + acy + ac[k]) * flag + (1.0 - flag);
+          rh[k] = rh[k] * flag + (1.0 - flag) * V(i, j, k);
+          if (fabs(ac[k]) < TINY_F32) { am[k] = 0.0; ap[k] = 0.0; ac[k] = 1.0; rh[k] = V(i, j, k); }
+        }
+        am[lo - 1] = 0.0; ap[lo - 1] = 0.0; ac[lo - 1] = 1.0; rh[lo - 1] = VH(i, j, lo - 1);
+        am[hi + 1] = 0.0; ap[hi + 1] = 0.0; ac[hi + 1] = 1.0; rh[hi + 1] = VH(i, j, hi + 1);
+        tdma_ws(am, ac, ap, rh, du, lo - 1, hi + 1, g);
+        for (int k = lo; k <= hi; ++k) V(i, j, k) = V(i, j, k) * (1.0 - om) + om * du[k];
+      }
+    }
+    free(w);
+  }
+#undef TAKE_HALOS
+#undef VH
+#undef SLO
+#undef SHI
+#undef V
+#undef R
+#undef G
+  free(halo);
+}
+
 /* CORE_MG.F90:615-938 itsolv_mg (one line-SOR sweep x, zebra y, z) */
 static void itsolv_mg(or_case *c, int lev, double *var, const double *r,
                       const int8_t *igk, const or_params *prm) {
+  {
+    const int nk = c->lev[lev].K - 1;
+    const int ns = g_threads < nk ? g_threads : nk;
+    if (ns > 1) { itsolv_mg_slabs(c, lev, var, r, igk, prm, ns); return; }
+  }
   const or_level *L = &c->lev[lev];
   const int nxm = L->I, JL1 = 1, JL2 = L->J - 1, KL1 = 1, KL2 = L->K - 1;
   const long NXl = L->I + 2, NYl = L->J + 2;
@@ -1415,6 +1577,7 @@ static void residual_mg(const or_case *c, int lev, const double *var,
                         double *rrr, const int8_t *igk) {
   const or_level *L = &c->lev[lev];
   const long NXl = L->I + 2, NYl = L->J + 2;
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1)
   for (int k = 1; k <= L->K - 1; ++k)
     for (int j = 1; j <= L->J - 1; ++j)
       for (int i = 1; i <= L->I - 1; ++i) {
@@ -1441,6 +1604,7 @@ static void mg_inject(const or_case *c, int N, const double *rr1, double *rr2) {
   long nC = (long)(C->I + 2) * (C->J + 2) * (C->K + 2);
   memset(rr2, 0, sizeof(double) * (size_t)nC);
   int ic = (F->I != C->I), jc = (F->J != C->J), kc = (F->K != C->K);
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1)
   for (int k = 1; k <= C->K - 1; ++k)
     for (int j = 1; j <= C->J - 1; ++j)
       for (int i = 1; i <= C->I - 1; ++i) {
@@ -1487,6 +1651,7 @@ static void mg_interp(const or_case *c, int N, const double *phi1,
   memset(dphi, 0, sizeof(double) * (size_t)nF);
   int ic = (F->I != C->I), jc = (F->J != C->J), kc = (F->K != C->K);
   const int nx2 = F->I, ny2 = F->J, nz2 = F->K, JL1 = 1, JL2 = F->J - 1, KL1 = 1, KL2 = F->K - 1;
+#pragma omp parallel for num_threads(g_threads) if (g_threads > 1)
   for (int k = KL1; k <= KL2; ++k)
     for (int j = JL1; j <= JL2; ++j)
       for (int i = 1; i <= nx2 - 1; ++i) {
