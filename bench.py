@@ -62,6 +62,7 @@ def _load_pkg():
     spec.loader.exec_module(mod)
     importlib.import_module("feicar_b200.fg")
     importlib.import_module("feicar_b200.synth")
+    importlib.import_module("feicar_b200.replicas")
     return mod
 
 
@@ -231,13 +232,18 @@ def run_kernels_only(torch, fg, synth, grid, c, geo, args, dev):
     c.close()
 
 
-def run_batch(torch, fg, synth, args, dev, stream):
+def run_batch(torch, fg, synth, args, dev, stream, R):
     """The batched workload: 64 cubic problems (edge log-uniform 32..192
     cells, seeded ellipsoids, tagged on the device) solved together by one
     fg_batch per precision, every stage of every problem in one launch and
     the V-cycle replayed as a CUDA graph.  Also times the same problems one
-    case after another (each case's own solve) for comparison."""
-    probs = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)
+    case after another (each case's own solve) for comparison.  With N
+    ranks the problems are split between them by cost (replicas, no
+    collective on the data path); the job time is the slowest rank's."""
+    allp = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)
+    shard = _load_pkg().replicas.shard_balanced(
+        [float((g.nx - 1) * (g.ny - 1) * (g.nz - 1)) for g, _, _ in allp], R.world)[R.rank]
+    probs = [allp[i] for i in shard]
     out = {}
     for prec_name, prec in (("mixed", fg.FG_PREC_MIXED), ("fp64", fg.FG_PREC_FP64)):
         cfg = fg.default_config(precision=prec, rtol=RTOL, max_cycles=200)
@@ -273,14 +279,16 @@ def run_batch(torch, fg, synth, args, dev, stream):
                 batch_once()
             stream.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            R.barrier()
             n0 = fg.launch_count()
             e0.record(stream)
             for _ in range(args.steps):
                 st = batch_once()
             e1.record(stream)
             stream.synchronize()
+            R.barrier()
             n1 = fg.launch_count()
-            ms = e0.elapsed_time(e1) / args.steps
+            ms = R.max(e0.elapsed_time(e1) / args.steps)
             # one case after another through each case's own solve
             for c, p_, f_ in zip(cases, d_p, d_f):
                 p_.zero_()
@@ -293,26 +301,29 @@ def run_batch(torch, fg, synth, args, dev, stream):
                 c.solve_poisson_device(p_.data_ptr(), f_.data_ptr())
             s1.record(stream)
             stream.synchronize()
-            ms_solo = s0.elapsed_time(s1)
-        out[prec_name] = {"ms_per_batch": ms, "solves_per_s": len(probs) / (ms / 1e3),
+            ms_solo = R.max(s0.elapsed_time(s1))
+        out[prec_name] = {"ms_per_batch": ms, "solves_per_s": len(allp) / (ms / 1e3),
                           "cycles": st["cycles"], "relres": st["relres"],
                           "launches_per_batch": (n1 - n0) / args.steps,
-                          "one_by_one_solves_per_s": len(probs) / (ms_solo / 1e3),
+                          "one_by_one_solves_per_s": len(allp) / (ms_solo / 1e3),
                           "setup_s": t_setup}
         bt.close()
         for c in cases:
             c.close()
         del d_p, d_f
         torch.cuda.empty_cache()
-    cells = sum((g.nx - 1) * (g.ny - 1) * (g.nz - 1) for g, _, _ in probs)
+    cells = sum((g.nx - 1) * (g.ny - 1) * (g.nz - 1) for g, _, _ in allp)
     m = out["mixed"]
+    if R.rank != 0:
+        return
     print(json.dumps({
-        "metric": METRIC, "value": m["solves_per_s"], "unit": UNIT, "n_gpus": 1,
+        "metric": METRIC, "value": m["solves_per_s"], "unit": UNIT, "n_gpus": R.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_batch"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (64 seeded ellipsoid problems, manufactured RHS; tagged on device)",
-        "config": {"workload": "batch64", "problems": len(probs), "cells": cells,
-                   "edges": [g.nx - 1 for g, _, _ in probs], "rtol": RTOL,
+        "config": {"workload": "batch64", "problems": len(allp), "cells": cells,
+                   "edges": [g.nx - 1 for g, _, _ in allp], "rtol": RTOL,
+                   "parallelism": f"replicas x{R.world} (problems split by cost)",
                    "cycle": "FGMRES(8) right-preconditioned by one V(2,2) cycle (CUDA graph), one launch per stage for all problems",
                    "l2": "inputs larger than L2"},
         "step": "one batched solve of all 64 problems from zero to 1e-8",
@@ -433,19 +444,13 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(device=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    R = pkg.replicas.Ranks(dist if world > 1 else None, device=f"cuda:{dev}")
+    barrier, max_over_ranks = R.barrier, R.max
 
     if args.workload == "batch64":
-        run_batch(torch, fg, synth, args, dev, stream)
+        run_batch(torch, fg, synth, args, dev, stream, R)
+        if world > 1:
+            dist.destroy_process_group()
         return
     if args.workload == "config2":
         run_config2(torch, fg, synth, args, dev, stream)
