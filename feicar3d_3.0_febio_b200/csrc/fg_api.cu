@@ -328,6 +328,7 @@ struct fg_batch {
   bool krylov = false;  // during an FGMRES solve: V-cycles in correction form
   int km = 0;
   int kbytes = 0;  // bytes per basis element of the allocated vectors
+  std::vector<long long> ksig;  // level-0 sizes and partial-sum blocks they were made for
   std::vector<void *> kraw;
   KDesc *d_kd = nullptr;
   std::vector<KDesc> h_kd;
@@ -382,16 +383,23 @@ static void free_batch_tables(fg_batch *b) {
   b->d_part = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
+  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
+  b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
+  b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
+  b->built = false;
+}
+
+// The FGMRES vectors outlive a rebuild of the tables (a new geometry of the
+// same problems keeps their sizes): every solve rewrites each vector's
+// interior before reading it, and nothing writes outside it.
+static void free_krylov(fg_batch *b) {
   for (void *r : b->kraw) cudaFree(r);
   b->kraw.clear();
   cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
   b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
   b->km = 0;
   b->kbytes = 0;
-  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
-  b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
-  b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
-  b->built = false;
+  b->ksig.clear();
 }
 
 static fg_status build_offsets(const std::vector<int> &blocks, int **d_off, Launch &Lr,
@@ -769,12 +777,11 @@ static int krylov_restart(const fg_solver_config &cfg) {
 // `bytes` per element); one vector every `stride` elements.
 static fg_status ensure_krylov(fg_batch *b, int bytes) {
   const int m = krylov_restart(b->cfg);
-  if (b->km == m && b->kbytes == bytes && b->d_kd) return FG_OK;
-  for (void *r : b->kraw) cudaFree(r);
-  b->kraw.clear();
-  cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
-  b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
-  b->km = 0;
+  std::vector<long long> sig;
+  for (auto *c : b->cases) sig.push_back(c->lev[0].ntot);
+  sig.push_back(std::max(b->all0.blocks, b->flat0.blocks));
+  if (b->km == m && b->kbytes == bytes && b->d_kd && b->ksig == sig) return FG_OK;
+  free_krylov(b);
   const int np = (int)b->cases.size();
   std::vector<KDesc> kd(np);
   for (int p = 0; p < np; ++p) {
@@ -808,6 +815,7 @@ static fg_status ensure_krylov(fg_batch *b, int bytes) {
   b->h_kcoef.assign((size_t)np * (KR_MAXV + 2), 0.0);
   b->km = m;
   b->kbytes = bytes;
+  b->ksig = sig;
   return FG_OK;
 }
 
@@ -1096,6 +1104,8 @@ static fg_status install_geometry(fg_case *c) {
   };
   add_rows(c->nDead, c->d_ijk, c->d_cell, c->d_coefN, &c->d_probe, &c->d_fallback);
   add_rows(c->nGhost, c->g_ijk, c->g_cell, c->g_coefN, nullptr, nullptr);
+  // every cell is written once: the planes go to the host threads
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= L0.nz; ++k)
     for (int j = 1; j <= L0.ny; ++j)
       for (int i = 1; i <= L0.nx; ++i) {
@@ -1119,6 +1129,7 @@ static void coarse_masks(fg_case *c) {
     C.type.assign(C.ntot, T_BOUND);
     C.ibk.assign(C.ntot, 0);
     const bool cx = C.nx != F.nx, cy = C.ny != F.ny, cz = C.nz != F.nz;
+#pragma omp parallel for schedule(static)
     for (int K = 1; K <= C.nz; ++K)
       for (int J = 1; J <= C.ny; ++J)
         for (int I = 1; I <= C.nx; ++I) {
@@ -1145,6 +1156,7 @@ static void coarse_masks(fg_case *c) {
 static void build_mask(HLevel &L) {
   L.mask.assign(L.ntot, 0);
   const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
+#pragma omp parallel for schedule(static)
   for (int k = 1; k <= L.nz; ++k)
     for (int j = 1; j <= L.ny; ++j)
       for (int i = 1; i <= L.nx; ++i) {
@@ -1665,6 +1677,7 @@ fg_status fg_batch_destroy(fg_batch *b) {
   for (cudaEvent_t e : b->prof.pool) cudaEventDestroy(e);
   cudaSetDevice(b->device);
   free_batch_tables(b);
+  free_krylov(b);
   if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }
   delete b;
   return FG_OK;

@@ -30,6 +30,11 @@ void geom_free(Geom &g) {
   cudaFree(g.d_band); cudaFree(g.d_tmp); cudaFree(g.d_xc);
   g.d_iblank = g.d_ghost = g.d_dead = g.d_body = g.d_band = g.d_tmp = nullptr;
   g.d_xc = nullptr;
+  for (DevScratch *b : {&g.cub_tmp, &g.sel_out, &g.sel_count, &g.cells, &g.glist, &g.dlist, &g.alpha,
+                        &g.rank, &g.flags})
+    b->release();
+  g.rg.release();
+  g.rd.release();
 }
 
 namespace geo {
@@ -883,26 +888,24 @@ static fg_status ensure_fields(fg_case *c) {
 }
 
 // stream compaction of the cell indices satisfying pred, in linear (k,j,i)
-// order; *d_out is (re)allocated to the count
+// order, into `out` (grown to the count); the case's grow-only scratch holds
+// the temporaries, so a call allocates nothing once the sizes are known.
+// One synchronisation (the count).
 template <typename Pred>
-static fg_status compact(Pred pred, size_t n, int **d_out, int *count, cudaStream_t s) {
-  int *d_n = nullptr, *tmpout = nullptr;
-  void *d_tmp = nullptr;
+static fg_status compact(Geom &G, Pred pred, size_t n, DevScratch &out, int *count, cudaStream_t s) {
   size_t tmp = 0;
   thrust::counting_iterator<int> it(0);
-  FG_CUDA(cub::DeviceSelect::If(nullptr, tmp, it, tmpout, d_n, (int)n, pred, s));
-  FG_CUDA(cudaMalloc(&d_n, sizeof(int)));
-  FG_CUDA(cudaMalloc(&d_tmp, tmp));
-  FG_CUDA(cudaMalloc(&tmpout, n * sizeof(int)));
-  FG_CUDA(cub::DeviceSelect::If(d_tmp, tmp, it, tmpout, d_n, (int)n, pred, s));
-  FG_CUDA(cudaMemcpyAsync(count, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cub::DeviceSelect::If(nullptr, tmp, it, (int *)nullptr, (int *)nullptr, (int)n, pred, s));
+  FG_CUDA(G.cub_tmp.ensure(tmp));
+  FG_CUDA(G.sel_out.ensure(n * sizeof(int)));
+  FG_CUDA(G.sel_count.ensure(sizeof(int)));
+  FG_CUDA(cub::DeviceSelect::If(G.cub_tmp.p, tmp, it, G.sel_out.as<int>(), G.sel_count.as<int>(), (int)n,
+                                pred, s));
+  FG_CUDA(cudaMemcpyAsync(count, G.sel_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaStreamSynchronize(s));
-  cudaFree(*d_out);
-  *d_out = nullptr;
-  FG_CUDA(cudaMalloc(d_out, (size_t)std::max(1, *count) * sizeof(int)));
-  FG_CUDA(cudaMemcpyAsync(*d_out, tmpout, (size_t)(*count) * sizeof(int), cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaStreamSynchronize(s));
-  cudaFree(tmpout); cudaFree(d_tmp); cudaFree(d_n);
+  FG_CUDA(out.ensure((size_t)std::max(1, *count) * sizeof(int)));
+  if (*count > 0)
+    FG_CUDA(cudaMemcpyAsync(out.p, G.sel_out.p, (size_t)(*count) * sizeof(int), cudaMemcpyDeviceToDevice, s));
   return FG_OK;
 }
 
@@ -989,10 +992,11 @@ fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank) {
     geo::k_band<<<(BB.b[b].ntri + 127) / 128, 128, 0, s>>>(g, BB.b[b], G.d_band);
   FG_CUDA(cudaGetLastError());
   // band cells of the interior classification range (j, k in [1, n-1])
-  int *d_cells = nullptr, ncell = 0;
-  if ((st = compact(geo::IsFlag{G.d_band, 1}, n, &d_cells, &ncell, s)) != FG_OK) return st;
-  int *d_warn = nullptr;
-  FG_CUDA(cudaMalloc(&d_warn, sizeof(int)));
+  int ncell = 0;
+  if ((st = compact(G, geo::IsFlag{G.d_band, 1}, n, G.cells, &ncell, s)) != FG_OK) return st;
+  int *d_cells = G.cells.as<int>();
+  FG_CUDA(G.flags.ensure(16 * sizeof(int)));
+  int *d_warn = G.flags.as<int>();
   FG_CUDA(cudaMemsetAsync(d_warn, 0, sizeof(int), s));
   if (ncell > 0) {
     const int wpb = 4;
@@ -1008,7 +1012,6 @@ fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank) {
   FG_CUDA(cudaMemcpyAsync(&hw, d_warn, sizeof(int), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaStreamSynchronize(s));
   G.nWarnSide = hw;
-  cudaFree(d_cells); cudaFree(d_warn);
   if (iblank) FG_CUDA(cudaMemcpy(iblank, G.d_iblank, n, cudaMemcpyDeviceToHost));
   G.tagged = true;
   return FG_OK;
@@ -1039,18 +1042,26 @@ static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_ch
   FG_CUDA(cudaMemcpyAsync(bnxt, G.d_body, n, cudaMemcpyDeviceToDevice, s));
   const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
   const int cap = c->nx + c->ny + c->nz + 2;
+  // SMOOTH_BATCH steps per host check, step q flagging into slot q: the
+  // fixed point is reached at the first step that changes nothing, and the
+  // steps after it change nothing either
+  constexpr int SMOOTH_BATCH = 8;
   bool done = false;
-  for (int it = 0; it < cap && !done; ++it) {
-    int h = 0;
-    FG_CUDA(cudaMemsetAsync(d_changed, 0, sizeof(int), s));
-    geo::k_smooth_step<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, mode, old, cur, nxt, bold,
-                                                                     bcur, bnxt, d_changed);
+  for (int it = 0; it < cap && !done;) {
+    int h[SMOOTH_BATCH];
+    const int nb = std::min(SMOOTH_BATCH, cap - it);
+    FG_CUDA(cudaMemsetAsync(d_changed, 0, nb * sizeof(int), s));
+    for (int q = 0; q < nb; ++q) {
+      geo::k_smooth_step<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, mode, old, cur, nxt, bold,
+                                                                       bcur, bnxt, d_changed + q);
+      std::swap(cur, nxt);
+      std::swap(bcur, bnxt);
+    }
     FG_CUDA(cudaGetLastError());
-    FG_CUDA(cudaMemcpyAsync(&h, d_changed, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaMemcpyAsync(h, d_changed, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
     FG_CUDA(cudaStreamSynchronize(s));
-    std::swap(cur, nxt);
-    std::swap(bcur, bnxt);
-    done = (h == 0);
+    it += nb;
+    done = (h[nb - 1] == 0);
   }
   if (!done) {
     set_last_error("iblank smoothing did not reach its fixed point", __FILE__, __LINE__);
@@ -1065,27 +1076,23 @@ static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_ch
 }  // extern "C"
 
 namespace {
-// device buffers of one row list (ghost or dead)
+// device outputs of one row list (ghost or dead): a view of the case's
+// grow-only row scratch, sized for m rows
 struct RowBufs {
   geo::RowOut o{};
   double *cD = nullptr, *cN = nullptr;
-  fg_status alloc(int m) {
-    const size_t mm = (size_t)std::max(1, m);
-    FG_CUDA(cudaMalloc(&o.bi, 3 * mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.bw, 3 * mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.ip, 3 * mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.nrm, 3 * mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.probe, mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.ds, mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&o.cell, 3 * mm * sizeof(int)));
-    FG_CUDA(cudaMalloc(&o.closest, mm * sizeof(int)));
-    FG_CUDA(cudaMalloc(&cD, 8 * mm * sizeof(double)));
-    FG_CUDA(cudaMalloc(&cN, 8 * mm * sizeof(double)));
+  fg_status bind(RowScratch &r, int m) {
+    const size_t mm = (size_t)std::max(1, m), d = sizeof(double);
+    FG_CUDA(r.bi.ensure(3 * mm * d)); FG_CUDA(r.bw.ensure(3 * mm * d));
+    FG_CUDA(r.ip.ensure(3 * mm * d)); FG_CUDA(r.nrm.ensure(3 * mm * d));
+    FG_CUDA(r.probe.ensure(mm * d)); FG_CUDA(r.ds.ensure(mm * d));
+    FG_CUDA(r.cell.ensure(3 * mm * sizeof(int))); FG_CUDA(r.closest.ensure(mm * sizeof(int)));
+    FG_CUDA(r.cD.ensure(8 * mm * d)); FG_CUDA(r.cN.ensure(8 * mm * d));
+    o.bi = r.bi.as<double>(); o.bw = r.bw.as<double>(); o.ip = r.ip.as<double>();
+    o.nrm = r.nrm.as<double>(); o.probe = r.probe.as<double>(); o.ds = r.ds.as<double>();
+    o.cell = r.cell.as<int>(); o.closest = r.closest.as<int>();
+    cD = r.cD.as<double>(); cN = r.cN.as<double>();
     return FG_OK;
-  }
-  ~RowBufs() {
-    cudaFree(o.bi); cudaFree(o.bw); cudaFree(o.ip); cudaFree(o.nrm); cudaFree(o.probe);
-    cudaFree(o.ds); cudaFree(o.cell); cudaFree(o.closest); cudaFree(cD); cudaFree(cN);
   }
 };
 
@@ -1105,10 +1112,6 @@ void list_ijk(const std::vector<int> &l, long long NX, long long NY, std::vector
   }
 }
 
-struct DevList {
-  int *p = nullptr;
-  ~DevList() { cudaFree(p); }
-};
 }  // namespace
 
 extern "C" {
@@ -1123,12 +1126,12 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   fg_status st = geom_grid(c, g);
   if (st != FG_OK) return st;
   const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
-  DevList flag, gl, dl, rank;
-  FG_CUDA(cudaMalloc(&flag.p, 4 * sizeof(int)));
+  FG_CUDA(G.flags.ensure(16 * sizeof(int)));
+  int *flagp = G.flags.as<int>();
   // smoothing: 5 x 3-D, 5 x x-planes, 5 x y-planes (GCM_SET_BOUNDARY.F90:115-223, :1618-1697)
   for (int mode = 0; mode < 3; ++mode)
     for (int it = 0; it < 5; ++it)
-      if ((st = smooth_pass(c, g, mode, flag.p)) != FG_OK) return st;
+      if ((st = smooth_pass(c, g, mode, flagp + 4)) != FG_OK) return st;
   const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
   FG_CUDA(cudaMemsetAsync(G.d_ghost, 0, n, s));  // held smoothing scratch
   geo::k_ghost_mark<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_body);
@@ -1136,36 +1139,36 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   geo::k_dead_mark<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_dead);
   FG_CUDA(cudaGetLastError());
   int ng = 0, nd = 0;
-  if ((st = compact(geo::IsFlag{G.d_ghost, 1}, n, &gl.p, &ng, s)) != FG_OK) return st;
+  if ((st = compact(G, geo::IsFlag{G.d_ghost, 1}, n, G.glist, &ng, s)) != FG_OK) return st;
   geo::IsDeadRow dpred{G.d_dead, c->nx + 2, c->ny + 2, c->nx, c->ny, c->nz};
-  if ((st = compact(dpred, n, &dl.p, &nd, s)) != FG_OK) return st;
+  if ((st = compact(G, dpred, n, G.dlist, &nd, s)) != FG_OK) return st;
+  const int *glp = G.glist.as<int>(), *dlp = G.dlist.as<int>();
   geo::Bodies BB = make_bodies(c);
   RowBufs gb, db;
-  if ((st = gb.alloc(ng)) != FG_OK) return st;
-  if ((st = db.alloc(nd)) != FG_OK) return st;
-  DevList alpha_buf;
-  double *alpha = nullptr;
-  FG_CUDA(cudaMalloc(&alpha, (size_t)std::max(1, ng) * sizeof(double)));
-  alpha_buf.p = reinterpret_cast<int *>(alpha);
-  FG_CUDA(cudaMemsetAsync(flag.p, 0, 4 * sizeof(int), s));
+  if ((st = gb.bind(G.rg, ng)) != FG_OK) return st;
+  if ((st = db.bind(G.rd, nd)) != FG_OK) return st;
+  FG_CUDA(G.alpha.ensure((size_t)std::max(1, ng) * sizeof(double)));
+  double *alpha = G.alpha.as<double>();
+  FG_CUDA(cudaMemsetAsync(flagp, 0, 4 * sizeof(int), s));
   const double pln = c->cfg.probe_length, plnD = c->cfg.probe_length_dead;
   if (ng > 0) {
-    geo::k_ghost_geom<<<(ng + 3) / 4, 128, 0, s>>>(g, BB, gl.p, ng, G.d_body, pln, gb.o, flag.p);
-    geo::k_weights<<<(ng + 63) / 64, 64, 0, s>>>(g, gl.p, ng, gb.o, 0, gb.cD, gb.cN, flag.p + 1);
+    geo::k_ghost_geom<<<(ng + 3) / 4, 128, 0, s>>>(g, BB, glp, ng, G.d_body, pln, gb.o, flagp);
+    geo::k_weights<<<(ng + 63) / 64, 64, 0, s>>>(g, glp, ng, gb.o, 0, gb.cD, gb.cN, flagp + 1);
   }
   if (nd > 0) {
-    geo::k_dead_geom<<<(nd + 3) / 4, 128, 0, s>>>(g, BB, dl.p, nd, G.d_body, plnD, db.o, flag.p,
-                                                  flag.p + 2);
-    geo::k_weights<<<(nd + 63) / 64, 64, 0, s>>>(g, dl.p, nd, db.o, 1, db.cD, db.cN, flag.p + 1);
+    geo::k_dead_geom<<<(nd + 3) / 4, 128, 0, s>>>(g, BB, dlp, nd, G.d_body, plnD, db.o, flagp,
+                                                  flagp + 2);
+    geo::k_weights<<<(nd + 63) / 64, 64, 0, s>>>(g, dlp, nd, db.o, 1, db.cD, db.cN, flagp + 1);
   }
   FG_CUDA(cudaGetLastError());
-  FG_CUDA(cudaMalloc(&rank.p, n * sizeof(int)));
-  FG_CUDA(cudaMemsetAsync(rank.p, 0xff, n * sizeof(int), s));
-  if (nd > 0) geo::k_rank<<<(nd + 255) / 256, 256, 0, s>>>(dl.p, nd, rank.p);
-  if (ng > 0) geo::k_alpha<<<(ng + 255) / 256, 256, 0, s>>>(g, gl.p, ng, G.d_dead, rank.p, db.o.ds, alpha);
+  FG_CUDA(G.rank.ensure(n * sizeof(int)));
+  int *rankp = G.rank.as<int>();
+  FG_CUDA(cudaMemsetAsync(rankp, 0xff, n * sizeof(int), s));
+  if (nd > 0) geo::k_rank<<<(nd + 255) / 256, 256, 0, s>>>(dlp, nd, rankp);
+  if (ng > 0) geo::k_alpha<<<(ng + 255) / 256, 256, 0, s>>>(g, glp, ng, G.d_dead, rankp, db.o.ds, alpha);
   FG_CUDA(cudaGetLastError());
   int flags[4] = {0, 0, 0, 0};
-  FG_CUDA(cudaMemcpyAsync(flags, flag.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaMemcpyAsync(flags, flagp, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaStreamSynchronize(s));
   G.nWarnSide += flags[0];
   G.nHostFail = flags[1];
@@ -1175,8 +1178,8 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   if ((st = d2h(G.d_ghost, n, hgh)) != FG_OK) return st;
   if ((st = d2h(G.d_dead, n, hde)) != FG_OK) return st;
   std::vector<int> hgl, hdl;
-  if ((st = d2h((const int *)gl.p, (size_t)ng, hgl)) != FG_OK) return st;
-  if ((st = d2h((const int *)dl.p, (size_t)nd, hdl)) != FG_OK) return st;
+  if ((st = d2h(glp, (size_t)ng, hgl)) != FG_OK) return st;
+  if ((st = d2h(dlp, (size_t)nd, hdl)) != FG_OK) return st;
   std::vector<int32_t> g_ijk, d_ijk, g_cell, d_cell;
   std::vector<double> g_coefN, d_coefN, d_probe, d_ip;
   list_ijk(hgl, c->nx + 2, c->ny + 2, g_ijk);

@@ -1,6 +1,7 @@
 // fg_geom.h -- device state of the immersed-boundary tagging of one case.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <vector>
@@ -19,8 +20,41 @@ struct DevBody {
   int32_t *d_v2t_off = nullptr, *d_v2t = nullptr;  // vertex -> triangles
 };
 
+// Device buffer that only grows: kept across calls, so re-tagging a moving
+// body on every time step allocates (and synchronises on a free) only while
+// the lists are still growing.
+struct DevScratch {
+  void *p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const cudaError_t e = cudaMalloc(&p, bytes > 0 ? bytes : 1);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+  void release() { cudaFree(p); p = nullptr; cap = 0; }
+};
+
+// device outputs of one row list (ghost or dead) of the tagging
+struct RowScratch {
+  DevScratch bi, bw, ip, nrm, probe, ds, cell, closest, cD, cN;
+  void release() {
+    bi.release(); bw.release(); ip.release(); nrm.release(); probe.release(); ds.release();
+    cell.release(); closest.release(); cD.release(); cN.release();
+  }
+};
+
 struct Geom {
   std::vector<DevBody> bodies;
+  // grow-only scratch of the tagging calls: compaction (CUB temporary
+  // storage, selection, count), the band cells, the ghost and dead lists and
+  // their row outputs, alpha, the dead-row rank map and the status flags
+  DevScratch cub_tmp, sel_out, sel_count, cells, glist, dlist, alpha, rank, flags;
+  RowScratch rg, rd;
   int8_t *d_iblank = nullptr, *d_ghost = nullptr, *d_dead = nullptr, *d_body = nullptr;
   int8_t *d_band = nullptr, *d_tmp = nullptr;
   double *d_xc = nullptr;      // xc[0..nx+1], yc, zc concatenated
