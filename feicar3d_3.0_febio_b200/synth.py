@@ -497,6 +497,37 @@ def small_grid(ncx=32, ncy=16, ncz=16, L=(4.0, 2.0, 2.0), stretch=None) -> Grid:
     return Grid(*ax)
 
 
+def serving_template(seed: int):
+    """One problem shape of the serving workload: edge n log-uniform in
+    [32, 256] cells, aspect 1:1:1 or 2:1:1 (x doubled) with p = 1/2, on
+    [0, a] x [0,1]^2; a sphere (diameter U(0.3, 0.6)) or a randomly rotated
+    ellipsoid (semi-axes U(0.15, 0.35)) with p = 1/2, 5120 triangles, at the
+    centre of the unit cube that starts at the inflow side.  Returns
+    (grid, body)."""
+    rng = np.random.default_rng(7000 + seed)
+    edge = int(round(math.exp(rng.uniform(math.log(32), math.log(256)))))
+    a = 2 if rng.random() < 0.5 else 1
+    g = Grid(uniform_nodes(a * edge, 0, float(a)), uniform_nodes(edge, 0, 1.0), uniform_nodes(edge, 0, 1.0))
+    centre = (0.5, 0.5, 0.5)
+    if rng.random() < 0.5:
+        b = sphere_body(centre, rng.uniform(0.3, 0.6), 4)
+    else:
+        b = ellipsoid_body(centre, rng.uniform(0.15, 0.35, size=3), random_rotation(rng), 4)
+    return g, b
+
+
+def serving_trace(rate: float, seconds: float, ntemplates: int, seed: int = 7):
+    """Poisson arrivals at `rate` per second over `seconds`: (arrival time,
+    template index, time steps 1..10), seeded."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            return out
+        out.append((t, int(rng.integers(ntemplates)), int(rng.integers(1, 11))))
+
+
 def batch_problems(n: int = 64, seed0: int = 0, lo: int = 32, hi: int = 192):
     """Configuration of the batched workload: cubic grids with edge length
     log-uniform in [lo, hi] cells on [0,1]^3 scaled, each with a seeded
