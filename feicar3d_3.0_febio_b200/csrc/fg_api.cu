@@ -298,8 +298,8 @@ struct fg_batch {
     DevLevel *d_levS_next = nullptr;  // level L+1 of S
     DevLevel *d_levC = nullptr;       // level L of C
     int *d_off_cells = nullptr, *d_off_x = nullptr, *d_off_y = nullptr, *d_off_z = nullptr,
-        *d_off_next = nullptr;
-    Launch cells, xl, yl, zl, next;
+        *d_off_next = nullptr, *d_off_quads = nullptr;
+    Launch cells, xl, yl, zl, next, quads;
     int maxnx = 0, maxny = 0, maxnz = 0;
     double ncells = 0.0;  // cells of level L summed over S
     const double **d_G = nullptr;
@@ -309,8 +309,9 @@ struct fg_batch {
   } ls[kMaxLevels];
   // level 0 over all problems
   DevLevel *d_lev0 = nullptr;
-  int *d_off0 = nullptr, *d_offf0 = nullptr;
+  int *d_off0 = nullptr, *d_offf0 = nullptr, *d_offq0 = nullptr;
   Launch all0;   // level-0 cells of all problems
+  Launch all0q;  // level-0 quads of all problems
   Launch flat0;  // level-0 vector elements of all problems (flat passes)
   // rows of all problems (dead rows then ghost rows per problem)
   DevRows rows{};
@@ -373,17 +374,18 @@ static void free_batch_tables(fg_batch *b) {
     auto &s = b->ls[L];
     cudaFree(s.d_levS); cudaFree(s.d_levS_next); cudaFree(s.d_levC);
     cudaFree(s.d_off_cells); cudaFree(s.d_off_x); cudaFree(s.d_off_y); cudaFree(s.d_off_z);
-    cudaFree(s.d_off_next); cudaFree(s.d_G); cudaFree(s.d_gidx); cudaFree(s.d_gn);
+    cudaFree(s.d_off_next); cudaFree(s.d_off_quads); cudaFree(s.d_G); cudaFree(s.d_gidx); cudaFree(s.d_gn);
     s = fg_batch::LevelSet();
   }
-  cudaFree(b->d_lev0); cudaFree(b->d_off0); cudaFree(b->d_offf0);
+  cudaFree(b->d_lev0); cudaFree(b->d_off0); cudaFree(b->d_offf0); cudaFree(b->d_offq0);
   cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
   cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
   cudaFree(b->d_norm); cudaFree(b->d_part);
   b->d_part = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
-  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_rprob = nullptr; b->d_rtgt = nullptr;
+  b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_offq0 = nullptr;
+  b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
   b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
   b->built = false;
@@ -422,7 +424,7 @@ static fg_status build_batch(fg_batch *b) {
   for (int L = 0; L < b->maxdepth; ++L) {
     auto &s = b->ls[L];
     std::vector<DevLevel> vS, vSn, vC;
-    std::vector<int> bc, bx, by, bz, bn;
+    std::vector<int> bc, bx, by, bz, bn, bq;
     std::vector<const double *> gp;
     std::vector<const int *> gi;
     std::vector<int> gn;
@@ -446,6 +448,7 @@ static fg_status build_batch(fg_batch *b) {
         by.push_back(k::blocks_tile(d, 1, s.maxny));
         bz.push_back(k::blocks_tile(d, 2, s.maxnz));
         bn.push_back(k::blocks_cells(c->lev[L + 1].dl));
+        bq.push_back(k::blocks_quads(d));
         s.ncells += (double)d.nx * d.ny * d.nz;
       } else if (L == c->nlev - 1) {
         s.C.push_back(p);
@@ -466,6 +469,7 @@ static fg_status build_batch(fg_batch *b) {
       if ((st = build_offsets(by, &s.d_off_y, s.yl, s.d_levS)) != FG_OK) return st;
       if ((st = build_offsets(bz, &s.d_off_z, s.zl, s.d_levS)) != FG_OK) return st;
       if ((st = build_offsets(bn, &s.d_off_next, s.next, s.d_levS_next)) != FG_OK) return st;
+      if ((st = build_offsets(bq, &s.d_off_quads, s.quads, s.d_levS)) != FG_OK) return st;
     }
     FG_CUDA(run_launch_set_alloc((void **)&s.d_G, gp));
     FG_CUDA(run_launch_set_alloc((void **)&s.d_gidx, gi));
@@ -474,16 +478,19 @@ static fg_status build_batch(fg_batch *b) {
   // level 0 over all problems
   {
     std::vector<DevLevel> v0;
-    std::vector<int> b0, bf;
+    std::vector<int> b0, bf, bq;
     for (auto *c : b->cases) {
       v0.push_back(c->lev[0].dl);
       b0.push_back(k::blocks_cells(c->lev[0].dl));
       bf.push_back(k::blocks_flat(c->lev[0].ntot));
+      bq.push_back(k::blocks_quads(c->lev[0].dl));
     }
     FG_CUDA(run_launch_set_alloc((void **)&b->d_lev0, v0));
     fg_status st = build_offsets(b0, &b->d_off0, b->all0, b->d_lev0);
     if (st != FG_OK) return st;
     st = build_offsets(bf, &b->d_offf0, b->flat0, b->d_lev0);
+    if (st != FG_OK) return st;
+    st = build_offsets(bq, &b->d_offq0, b->all0q, b->d_lev0);
     if (st != FG_OK) return st;
   }
   // rows
@@ -524,7 +531,7 @@ static fg_status build_batch(fg_batch *b) {
     b->rows.rf = mkptr(b->d_rf, n, K_ROWS);
   }
   FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
-  FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, b->all0.blocks) * sizeof(double)));
+  FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
   b->h_norm.assign(3 * np, 0.0);
   b->built = true;
   return FG_OK;
@@ -616,7 +623,7 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
       for (int q = 0; q < b->cfg.nu1; ++q)
         if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
       const size_t e0 = prof_begin(b, s);
-      FG_K(k::residual<T>(ls.cells, nullptr, nullptr, s));
+      FG_K(k::residual_q<T>(ls.quads, s));
       FG_K(k::restrict_to<T>(ls.next, ls.d_levS, s));
       FG_K(k::zero_x<T>(ls.next, s));
       prof_end(b, e0, FG_PROF_TRANSFER, 0.0, s);
@@ -877,7 +884,7 @@ static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
     // ---- true residual V_0 = F - A P, fluid norm, full norm
     FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
     const size_t e_r = prof_begin(b, s);
-    FG_K(k::kr_resid<B>(b->all0, b->rows, b->d_lev0, b->d_kd, 0, b->d_part, b->d_norm, s));
+    FG_K(k::kr_resid<B>(b->all0q, b->rows, b->d_lev0, b->d_kd, 0, b->d_part, b->d_norm, s));
     FG_K(k::kr_dots<B>(b->flat0, b->d_kd, 0, 0, b->d_kpart, b->d_kout, CS, s));
     prof_end(b, e_r, FG_PROF_RESIDUAL, 0.0, s);
     FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -920,7 +927,7 @@ static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
       // ---- Z_j from the V-cycle, W = A Z_j into V_{j+1}; inner products
       // with V_0..V_j and |W|^2
       size_t e0 = prof_begin(b, s);
-      FG_K((k::kr_apply<B, T>(b->all0, b->rows, b->d_lev0, b->d_kd, j, j + 1, s)));
+      FG_K((k::kr_apply<B, T>(b->all0q, b->rows, b->d_lev0, b->d_kd, j, j + 1, s)));
       FG_K(k::kr_dots<B>(b->flat0, b->d_kd, j + 1, j + 1, b->d_kpart, b->d_kout, CS, s));
       prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
       if ((err = read_out()) != FG_OK) break;

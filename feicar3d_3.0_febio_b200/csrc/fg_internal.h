@@ -169,6 +169,8 @@ namespace k {
 int blocks_cells(const DevLevel &L);
 // flat passes over the n elements of a level-0 field (Krylov vectors)
 int blocks_flat(long long n);
+// quad kernels (4 cells of a row per thread)
+int blocks_quads(const DevLevel &L);
 int blocks_xline(const DevLevel &L, int maxn);
 // y/z tiles: blocks depend on the kernel the level set's longest line picks
 int blocks_tile(const DevLevel &L, int axis, int maxn);
@@ -185,6 +187,10 @@ cudaError_t restrict_to(const Launch &fine_cells_of_coarse, const DevLevel *fine
                         cudaStream_t s);
 template <typename T>
 cudaError_t prolong_add(const Launch &fine, const DevLevel *coarse, cudaStream_t s);
+// the residual (no norm) with quads: Launch over the level's quads
+// (blocks_quads)
+template <typename T>
+cudaError_t residual_q(const Launch &quads, cudaStream_t s);
 template <typename T>
 cudaError_t zero_x(const Launch &L, cudaStream_t s);
 template <typename T>
@@ -217,7 +223,7 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
 // the preconditioner's level-0 arrays.
 //  kr_resid:  V_vd = F - A P (rows included), norm2[p] += fluid-row |r|^2
 //  kr_apply:  Z_vz = preconditioner output x_T on rows (0 elsewhere),
-//             V_vw = A Z_vz (rows included)
+//             V_vw = A Z_vz (rows included); launched over the level-0 quads
 //  kr_dots:   out[p*ostride + i] = (V_vw, V_i) for i < nv,
 //             out[p*ostride + nv] = (V_vw, V_vw)
 //  kr_vaxpy:  V_vd = c0 V_vd + sum_{i<ns} c_{1+i} V_{s0+i} (c = coef + p*cs);

@@ -1457,14 +1457,11 @@ __device__ __forceinline__ double block_sum(double v) {
 
 // (A x) at an active cell from its mask: sum over the kept faces of
 // a (x_n - x_c), Dirichlet boundary faces contributing -2 a x_c
+// (A x) at an active cell from its own value xc and its six neighbours xn
+// (faces -x,+x,-y,+y,-z,+z) and the axis coefficients a
 template <typename T>
-__device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, int j, int k,
-                                       uint8_t mk, dptr<const T> FG_RESTRICT x) {
-  const T xc = x[id];
-  const T x0 = x[id - 1], x1 = x[id + 1], x2 = x[id - L.sy], x3 = x[id + L.sy];
-  const T x4 = x[id - L.sz], x5 = x[id + L.sz];
-  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
-  const T xn[6] = {x0, x1, x2, x3, x4, x5};
+__device__ __forceinline__ T apply_vals(const DevLevel &L, int i, int j, int k, uint8_t mk, T xc,
+                                        const T (&xn)[6], const double (&a)[6]) {
   const bool atb[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
   T acc = T(0);
   double diag = 0.0;
@@ -1474,6 +1471,15 @@ __device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, i
     else if (atb[q] && L.bc[q]) diag -= 2.0 * a[q];
   }
   return acc + (T)diag * xc;
+}
+
+template <typename T>
+__device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, int j, int k,
+                                       uint8_t mk, dptr<const T> FG_RESTRICT x) {
+  const T xc = x[id];
+  const T xn[6] = {x[id - 1], x[id + 1], x[id - L.sy], x[id + L.sy], x[id - L.sz], x[id + L.sz]};
+  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+  return apply_vals<T>(L, i, j, k, mk, xc, xn, a);
 }
 
 // per-entry sum of the block partials of a launch (1024 threads, eight
@@ -1614,6 +1620,112 @@ cudaError_t correct_residual(const Launch &Lr, double *norm2, double *part, cuda
   k_residual_mixed<<<Lr.blocks, CELL_BLOCK, 0, s>>>(Lr.off, Lr.n, Lr.lev, part);
   note_launches(1);
   k_reduce_parts<<<Lr.n, 1024, 0, s>>>(Lr.off, part, norm2);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------ quad kernels
+// Cell kernels that take 4 consecutive cells of a row per thread: 16-byte
+// vector loads of the row and of its four transverse neighbour rows (cell 1
+// of every row is 16-byte aligned, so every quad starting at i = 1 + 4q is),
+// the row's two end neighbours as scalars.  A block has QBLOCK threads: QW
+// threads per row (one per quad, at most QBLOCK) and QBLOCK/QW rows at a
+// time, QROWS times.
+constexpr int QBLOCK = 128;
+constexpr int QROWS = 4;
+__host__ __device__ inline int quad_w(int nx) {
+  int q = ((nx + 3) / 4 + 31) / 32 * 32;
+  return q < QBLOCK ? q : QBLOCK;
+}
+int blocks_quads(const DevLevel &L) {
+  const int qw = quad_w(L.nx), rpb = QBLOCK / qw;
+  const int nseg = ((L.nx + 3) / 4 + qw - 1) / qw;
+  const long long rows = (long long)L.ny * L.nz, per = (long long)rpb * QROWS;
+  return (int)(nseg * ((rows + per - 1) / per));
+}
+struct QuadIdx { int i0, j, k; bool ok; };
+__device__ __forceinline__ QuadIdx quad_of(const DevLevel &L, int lb, int r) {
+  const int qw = quad_w(L.nx), rpb = QBLOCK / qw;
+  const int nseg = ((L.nx + 3) / 4 + qw - 1) / qw;
+  const int seg = lb % nseg, rg = lb / nseg;
+  const int t = threadIdx.x;
+  const long long row = ((long long)rg * QROWS + r) * rpb + t / qw;
+  QuadIdx q;
+  q.i0 = 1 + 4 * (seg * qw + t % qw);
+  q.j = 1 + (int)(row % L.ny);
+  q.k = 1 + (int)(row / L.ny);
+  q.ok = q.i0 <= L.nx && q.k <= L.nz;
+  return q;
+}
+
+// A quad's own values, its four transverse neighbour rows and its two end
+// neighbours
+template <typename T>
+struct QuadVals {
+  T c[4], ym[4], yp[4], zm[4], zp[4];
+  T xl, xr;
+  template <typename P>
+  __device__ __forceinline__ void load(const DevLevel &L, const P &x, long long id) {
+    load_run<T, 4>(c, x, id);
+    load_run<T, 4>(ym, x, id - L.sy);
+    load_run<T, 4>(yp, x, id + L.sy);
+    load_run<T, 4>(zm, x, id - L.sz);
+    load_run<T, 4>(zp, x, id + L.sz);
+    xl = x[id - 1];
+    xr = x[id + 4];
+  }
+  // neighbours of cell v (faces -x,+x,-y,+y,-z,+z)
+  __device__ __forceinline__ void nbrs(int v, T (&xn)[6]) const {
+    xn[0] = v == 0 ? xl : c[v - 1];
+    xn[1] = v == 3 ? xr : c[v + 1];
+    xn[2] = ym[v]; xn[3] = yp[v]; xn[4] = zm[v]; xn[5] = zp[v];
+  }
+};
+
+// r = f - A x on active cells, 0 on the other interior cells (the V-cycle's
+// restriction input); the arithmetic of k_residual, per quad
+template <typename T>
+__global__ void __launch_bounds__(QBLOCK)
+k_residual_q(const int *off, int nent, const DevLevel *levs) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const DevLevel &L = levs[p];
+  const int lb = blockIdx.x - off[p];
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  auto res = PrecOf<T>::res(L);
+#pragma unroll
+  for (int r = 0; r < QROWS; ++r) {
+    const QuadIdx q = quad_of(L, lb, r);
+    if (!q.ok) continue;
+    const long long id = q.i0 + L.sy * q.j + L.sz * q.k;
+    QuadVals<T> xv;
+    xv.load(L, x, id);
+    T f[4];
+    uint8_t m4[4];
+    load_run<T, 4>(f, rhs, id);
+    load_run<uint8_t, 4>(m4, L.mask, id);
+    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    T out[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = q.i0 + v;
+      T rv = T(0);
+      if (i <= L.nx && (m4[v] & 64)) {
+        T xn[6];
+        xv.nbrs(v, xn);
+        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        rv = f[v] - apply_vals<T>(L, i, q.j, q.k, m4[v], xv.c[v], xn, a);
+      }
+      out[v] = rv;
+    }
+    store_run<T, 4>(res, id, out, L.nx - q.i0 + 1);
+  }
+}
+
+template <typename T>
+cudaError_t residual_q(const Launch &Lq, cudaStream_t s) {
+  if (Lq.empty()) return cudaSuccess;
+  k_residual_q<T><<<Lq.blocks, QBLOCK, 0, s>>>(Lq.off, Lq.n, Lq.lev);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -1985,9 +2097,10 @@ __device__ __forceinline__ double apply_row_d(const DevLevel &L, long long id, i
 }
 
 // V_vd = F - A P on active rows, 0 on every other interior cell; part[b] =
-// block sum of the squared active-row residuals (fluid-row norm)
+// block sum of the squared active-row residuals (fluid-row norm).  Per quad
+// (4 cells of a row per thread, vector loads), FP64 arithmetic.
 template <typename B>
-__global__ void __launch_bounds__(CELL_BLOCK)
+__global__ void __launch_bounds__(QBLOCK)
 k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
@@ -1997,27 +2110,46 @@ k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
   auto F = mkptr<const double>(d.F, d.n, K_RHS);
   auto D = kvec<B>(d, d.V, vd);
   double r2 = 0.0;
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    const uint8_t mk = L.mask[id];
-    double r = 0.0;
-    if (mk & 64) r = F[id] - apply_row_d<double>(L, id, c.i, c.j, c.k, mk, P);
-    D[id] = (B)r;
-    r2 += r * r;
+#pragma unroll
+  for (int r = 0; r < QROWS; ++r) {
+    const QuadIdx q = quad_of(L, lb, r);
+    if (!q.ok) continue;
+    const long long id = q.i0 + L.sy * q.j + L.sz * q.k;
+    QuadVals<double> pv;
+    pv.load(L, P, id);
+    double f[4];
+    uint8_t m4[4];
+    load_run<double, 4>(f, F, id);
+    load_run<uint8_t, 4>(m4, L.mask, id);
+    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    B out[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = q.i0 + v;
+      double rv = 0.0;
+      if (i <= L.nx && (m4[v] & 64)) {
+        double xn[6];
+        pv.nbrs(v, xn);
+        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        rv = f[v] - apply_vals<double>(L, i, q.j, q.k, m4[v], pv.c[v], xn, a);
+      }
+      out[v] = (B)rv;
+      r2 += rv * rv;
+    }
+    store_run<B, 4>(D, id, out, L.nx - q.i0 + 1);
   }
   const double t = block_sum(r2);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
 // Preconditioner output x_T into Z_vz (rows; 0 elsewhere) and W = A x_T
-// into V_vw on active rows (0 on every other interior cell).  x_T is zero on
-// the pure-solid cells an active row may couple to (they are held at the
-// staged zero), so A x_T equals A Z_vz there.
+// into V_vw on active rows (0 on every other interior cell), per quad (4
+// cells of a row per thread, vector loads), in the FP64 arithmetic of
+// apply_row_d.  x_T is zero on the pure-solid cells an active row may
+// couple to (they are held at the staged zero), so A x_T equals A Z_vz.
 template <typename B, typename T>
-__global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_apply(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw) {
+__global__ void __launch_bounds__(QBLOCK)
+k_kr_apply_q(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2025,13 +2157,42 @@ k_kr_apply(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
   auto x = PrecOf<T>::x(L);
   auto Z = kvec<B>(d, d.Z, vz);
   auto W = kvec<B>(d, d.V, vw);
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(L, lb, rr);
-    if (!c.ok) continue;
-    const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    const uint8_t mk = L.mask[id];
-    Z[id] = is_row(L, id, mk) ? (B)x[id] : B(0);
-    W[id] = (mk & 64) ? (B)apply_row_d<T>(L, id, c.i, c.j, c.k, mk, x) : B(0);
+#pragma unroll
+  for (int r = 0; r < QROWS; ++r) {
+    const QuadIdx q = quad_of(L, lb, r);
+    if (!q.ok) continue;
+    const long long id = q.i0 + L.sy * q.j + L.sz * q.k;
+    QuadVals<T> xv;
+    xv.load(L, x, id);
+    uint8_t m4[4];
+    int8_t t4[4];
+    load_run<uint8_t, 4>(m4, L.mask, id);
+    load_run<int8_t, 4>(t4, L.type, id);
+    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    B z4[4], w4[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = q.i0 + v;
+      const bool row = (m4[v] & 64) || t4[v] == T_GHOST;
+      z4[v] = row ? (B)xv.c[v] : B(0);
+      double wv = 0.0;
+      if (i <= L.nx && (m4[v] & 64)) {
+        T xn[6];
+        xv.nbrs(v, xn);
+        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        const bool atb[6] = {i == 1, i == L.nx, q.j == 1, q.j == L.ny, q.k == 1, q.k == L.nz};
+        double acc = 0.0, diag = 0.0;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+          if ((m4[v] >> f) & 1) { acc += a[f] * (double)xn[f]; diag -= a[f]; }
+          else if (atb[f] && L.bc[f]) diag -= 2.0 * a[f];
+        }
+        wv = acc + diag * (double)xv.c[v];
+      }
+      w4[v] = (B)wv;
+    }
+    store_run<B, 4>(Z, id, z4, L.nx - q.i0 + 1);
+    store_run<B, 4>(W, id, w4, L.nx - q.i0 + 1);
   }
 }
 
@@ -2276,11 +2437,11 @@ k_kr_update(const int *off, int nent, const KDesc *kd, int ns, const double *coe
 static int rows_blocks(const DevRows &R) { return (R.n + CELL_BLOCK - 1) / CELL_BLOCK; }
 
 template <typename B>
-cudaError_t kr_resid(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
+cudaError_t kr_resid(const Launch &quads, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vd,
                      double *part, double *norm2, cudaStream_t s) {
-  if (cells.empty()) return cudaSuccess;
-  k_kr_resid<B><<<cells.blocks, CELL_BLOCK, 0, s>>>(cells.off, cells.n, cells.lev, kd, vd, part);
-  k_reduce_parts<<<cells.n, 1024, 0, s>>>(cells.off, part, norm2);
+  if (quads.empty()) return cudaSuccess;
+  k_kr_resid<B><<<quads.blocks, QBLOCK, 0, s>>>(quads.off, quads.n, quads.lev, kd, vd, part);
+  k_reduce_parts<<<quads.n, 1024, 0, s>>>(quads.off, part, norm2);
   note_launches(2);
   if (R.n > 0) {
     k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, 0, vd);
@@ -2290,10 +2451,10 @@ cudaError_t kr_resid(const Launch &cells, const DevRows &R, const DevLevel *lev0
 }
 
 template <typename B, typename T>
-cudaError_t kr_apply(const Launch &cells, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vz,
+cudaError_t kr_apply(const Launch &quads, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vz,
                      int vw, cudaStream_t s) {
-  if (cells.empty()) return cudaSuccess;
-  k_kr_apply<B, T><<<cells.blocks, CELL_BLOCK, 0, s>>>(cells.off, cells.n, cells.lev, kd, vz, vw);
+  if (quads.empty()) return cudaSuccess;
+  k_kr_apply_q<B, T><<<quads.blocks, QBLOCK, 0, s>>>(quads.off, quads.n, quads.lev, kd, vz, vw);
   note_launches(1);
   if (R.n > 0) {
     k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vz, vw);
@@ -2374,11 +2535,13 @@ extern "C" fg_status fg_debug_check(long long *out) {
 template cudaError_t line_sweep<double>(const Launch &, int, int, double, int, cudaStream_t);
 template cudaError_t line_sweep<float>(const Launch &, int, int, double, int, cudaStream_t);
 template cudaError_t residual<double>(const Launch &, double *, double *, cudaStream_t);
+template cudaError_t residual_q<double>(const Launch &, cudaStream_t);
+template cudaError_t residual_q<float>(const Launch &, cudaStream_t);
+template cudaError_t prolong_add<double>(const Launch &, const DevLevel *, cudaStream_t);
+template cudaError_t prolong_add<float>(const Launch &, const DevLevel *, cudaStream_t);
 template cudaError_t residual<float>(const Launch &, double *, double *, cudaStream_t);
 template cudaError_t restrict_to<double>(const Launch &, const DevLevel *, cudaStream_t);
 template cudaError_t restrict_to<float>(const Launch &, const DevLevel *, cudaStream_t);
-template cudaError_t prolong_add<double>(const Launch &, const DevLevel *, cudaStream_t);
-template cudaError_t prolong_add<float>(const Launch &, const DevLevel *, cudaStream_t);
 template cudaError_t zero_x<double>(const Launch &, cudaStream_t);
 template cudaError_t zero_x<float>(const Launch &, cudaStream_t);
 template cudaError_t rows_relax<double>(const DevRows &, const DevLevel *, int, double *,
