@@ -772,6 +772,8 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
 }
 
 // ------------------------------------------------------------ FGMRES
+constexpr double kReorth = 1e-4;  // second Gram-Schmidt pass below this fraction of |w|^2
+
 static int krylov_restart(const fg_solver_config &cfg) {
   int m = cfg.restart > 0 ? cfg.restart : 10;
   if (m < 2) m = 2;
@@ -936,7 +938,12 @@ static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
         cudaEventElapsedTime(&ms, va, vb);
         vms.push_back(ms);
       }
-      // classical Gram-Schmidt; a second pass where it cancelled badly
+      // classical Gram-Schmidt; a second pass only where the projection
+      // removed all but 1e-4 of |w|^2 (two of the basis's digits lost).  With
+      // a V-cycle preconditioner w = A M^-1 v_j lies mostly in the span of
+      // the basis, so the usual 1/2 test asks for the second pass on almost
+      // every step (a dot and an axpy pass over all vectors each time);
+      // without any second pass the strict convergence cases stall.
       bool reorth = false;
       std::vector<double> hcol((size_t)np * (j + 2), 0.0), ww(np, 0.0);
       for (int p = 0; p < np; ++p) {
@@ -944,7 +951,7 @@ static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
         double sum = 0.0;
         for (int i = 0; i <= j; ++i) { hcol[(size_t)p * (j + 2) + i] = o[i]; sum += o[i] * o[i]; }
         ww[p] = o[j + 1];
-        if (!done[p] && ww[p] - sum < 0.5 * ww[p]) reorth = true;
+        if (!done[p] && ww[p] - sum < kReorth * ww[p]) reorth = true;
       }
       if (reorth) {
         for (int p = 0; p < np; ++p) {
