@@ -353,6 +353,9 @@ __global__ void k_commit(Grid g, const int8_t *ibt, int8_t *ib) {
 // steps; each step is a Jacobi update from cur to nxt.
 // mode 0: 3-D pass (k,j,i order, 6 faces, >= 5); mode 1: x planes (j,k
 // order within an i plane, >= 3); mode 2: y planes (i,k order, >= 3).
+// Only interior cells (1..n-1 on every axis) are updated and written; a
+// backward neighbour on the boundary layer is never updated, so it is read
+// from old, and cur/nxt need no boundary values.
 __global__ void k_smooth_step(Grid g, int mode, const int8_t *old, const int8_t *cur, int8_t *nxt,
                               const int8_t *bold, const int8_t *bcur, int8_t *bnxt, int *changed) {
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -365,28 +368,28 @@ __global__ void k_smooth_step(Grid g, int mode, const int8_t *old, const int8_t 
   if (old[id] == 1) { nxt[id] = 1; bnxt[id] = bcur[id]; return; }
   const long long sx = 1, sy = g.NX, sz = g.NX * g.NY;
   // neighbour offsets in the reference enumeration order, and which are
-  // backward in the loop order
+  // backward in the loop order and updated (backward and not on the boundary)
   long long off[6];
-  bool back[6];
+  bool upd[6];
   int nn, thr;
   if (mode == 0) {
     off[0] = -sz; off[1] = -sy; off[2] = -sx; off[3] = sx; off[4] = sy; off[5] = sz;
-    back[0] = back[1] = back[2] = true; back[3] = back[4] = back[5] = false;
+    upd[0] = k > 1; upd[1] = j > 1; upd[2] = i > 1; upd[3] = upd[4] = upd[5] = false;
     nn = 6; thr = 5;
   } else if (mode == 1) {
     off[0] = -sz; off[1] = -sy; off[2] = sy; off[3] = sz;
-    back[0] = true; back[1] = true; back[2] = false; back[3] = false;
+    upd[0] = k > 1; upd[1] = j > 1; upd[2] = false; upd[3] = false;
     nn = 4; thr = 3;
   } else {
     off[0] = -sz; off[1] = -sx; off[2] = sx; off[3] = sz;
-    back[0] = true; back[1] = true; back[2] = false; back[3] = false;
+    upd[0] = k > 1; upd[1] = i > 1; upd[2] = false; upd[3] = false;
     nn = 4; thr = 3;
   }
   int s = 0, ibody = 0;
   for (int q = 0; q < nn; ++q) {
     const long long nb = id + off[q];
-    const int8_t v = back[q] ? cur[nb] : old[nb];
-    const int8_t bv = back[q] ? bcur[nb] : bold[nb];
+    const int8_t v = upd[q] ? cur[nb] : old[nb];
+    const int8_t bv = upd[q] ? bcur[nb] : bold[nb];
     if (v == 1) {
       s++;
       if (bv > 0) ibody = bv;
@@ -396,7 +399,21 @@ __global__ void k_smooth_step(Grid g, int mode, const int8_t *old, const int8_t 
   if (s >= thr) { nv = 1; nb = (int8_t)(ibody > 0 ? ibody : 1); }
   nxt[id] = nv;
   bnxt[id] = nb;
-  if (nv != cur[id]) atomicOr(changed, 1);
+  if (nv != cur[id] || nb != bcur[id]) atomicOr(changed, 1);
+}
+
+// interior cells of the fixed point back into the case's iblank and body
+__global__ void k_smooth_commit(Grid g, const int8_t *cur, const int8_t *bcur, int8_t *iblank,
+                                int8_t *body) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)(g.nx - 1) * (g.ny - 1) * (g.nz - 1);
+  if (e >= n) return;
+  const int i = 1 + (int)(e % (g.nx - 1));
+  const int j = 1 + (int)((e / (g.nx - 1)) % (g.ny - 1));
+  const int k = 1 + (int)(e / ((long long)(g.nx - 1) * (g.ny - 1)));
+  const long long id = ridx(g, i, j, k);
+  iblank[id] = cur[id];
+  body[id] = bcur[id];
 }
 
 // ---------------------------------------------------------- ghosts
@@ -1027,39 +1044,46 @@ fg_status fg_get_band(const fg_case *c, int8_t *band) {
 // One in-place smoothing pass (mode 0: 3-D, 1: x planes, 2: y planes) as a
 // Jacobi fixed-point iteration.  Every dependency chain of the sequential
 // pass steps backward along x, y or z, so the iteration is exact after at
-// most nx + ny + nz steps.
-static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_changed) {
+// most nx + ny + nz steps.  The first step reads the case's iblank and body
+// as both old and cur; later steps alternate between two scratch pairs.
+// *identity is set when the first step changes nothing: the pass then maps
+// its input to itself and leaves iblank and body untouched.
+static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_changed,
+                             bool *identity) {
   Geom &G = *c->geom;
   cudaStream_t s = c->stream;
   const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
-  int8_t *old = G.d_tmp, *cur = G.d_tmp + n, *nxt = G.d_tmp + 2 * n, *bold = G.d_tmp + 3 * n;
-  int8_t *bcur = G.d_dead, *bnxt = G.d_ghost;  // free until the lists are built
-  FG_CUDA(cudaMemcpyAsync(old, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(cur, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(nxt, G.d_iblank, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(bold, G.d_body, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(bcur, G.d_body, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(bnxt, G.d_body, n, cudaMemcpyDeviceToDevice, s));
+  const int8_t *old = G.d_iblank, *bold = G.d_body;
+  int8_t *buf[2] = {G.d_tmp, G.d_tmp + n}, *bbuf[2] = {G.d_tmp + 2 * n, G.d_tmp + 3 * n};
   const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
+  const unsigned blocks = (unsigned)((ni + 255) / 256);
   const int cap = c->nx + c->ny + c->nz + 2;
-  // SMOOTH_BATCH steps per host check, step q flagging into slot q: the
-  // fixed point is reached at the first step that changes nothing, and the
-  // steps after it change nothing either
+  // batches of 1, 2, 4 then 8 steps per host check, step q flagging into
+  // slot q: most passes reach their fixed point in one or two steps; the
+  // fixed point is the first step that changes nothing, and the steps after
+  // it change nothing either
   constexpr int SMOOTH_BATCH = 8;
   bool done = false;
-  for (int it = 0; it < cap && !done;) {
+  int it = 0, w = 0;  // steps taken; buffer the next step writes
+  *identity = false;
+  for (int nb_want = 1; it < cap && !done; nb_want = std::min(2 * nb_want, SMOOTH_BATCH)) {
     int h[SMOOTH_BATCH];
-    const int nb = std::min(SMOOTH_BATCH, cap - it);
+    const int nb = std::min(nb_want, cap - it);
     FG_CUDA(cudaMemsetAsync(d_changed, 0, nb * sizeof(int), s));
     for (int q = 0; q < nb; ++q) {
-      geo::k_smooth_step<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, mode, old, cur, nxt, bold,
-                                                                       bcur, bnxt, d_changed + q);
-      std::swap(cur, nxt);
-      std::swap(bcur, bnxt);
+      const bool first = (it + q == 0);
+      const int8_t *cur = first ? old : buf[1 - w], *bcur = first ? bold : bbuf[1 - w];
+      geo::k_smooth_step<<<blocks, 256, 0, s>>>(g, mode, old, cur, buf[w], bold, bcur, bbuf[w],
+                                                d_changed + q);
+      w = 1 - w;
     }
     FG_CUDA(cudaGetLastError());
     FG_CUDA(cudaMemcpyAsync(h, d_changed, nb * sizeof(int), cudaMemcpyDeviceToHost, s));
     FG_CUDA(cudaStreamSynchronize(s));
+    if (it == 0 && h[0] == 0) {
+      *identity = true;
+      return FG_OK;
+    }
     it += nb;
     done = (h[nb - 1] == 0);
   }
@@ -1067,9 +1091,8 @@ static fg_status smooth_pass(fg_case *c, const geo::Grid &g, int mode, int *d_ch
     set_last_error("iblank smoothing did not reach its fixed point", __FILE__, __LINE__);
     return FG_TIMEOUT;
   }
-  FG_CUDA(cudaMemcpyAsync(G.d_iblank, cur, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaMemcpyAsync(G.d_body, bcur, n, cudaMemcpyDeviceToDevice, s));
-  FG_CUDA(cudaStreamSynchronize(s));
+  geo::k_smooth_commit<<<blocks, 256, 0, s>>>(g, buf[1 - w], bbuf[1 - w], G.d_iblank, G.d_body);
+  FG_CUDA(cudaGetLastError());
   return FG_OK;
 }
 
@@ -1129,11 +1152,16 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   FG_CUDA(G.flags.ensure(16 * sizeof(int)));
   int *flagp = G.flags.as<int>();
   // smoothing: 5 x 3-D, 5 x x-planes, 5 x y-planes (GCM_SET_BOUNDARY.F90:115-223, :1618-1697)
+  // a pass that maps its input to itself does so again, so the passes of a
+  // mode stop at the first one that changes nothing
   for (int mode = 0; mode < 3; ++mode)
-    for (int it = 0; it < 5; ++it)
-      if ((st = smooth_pass(c, g, mode, flagp + 4)) != FG_OK) return st;
+    for (int it = 0; it < 5; ++it) {
+      bool identity = false;
+      if ((st = smooth_pass(c, g, mode, flagp + 4, &identity)) != FG_OK) return st;
+      if (identity) break;
+    }
   const long long ni = (long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1);
-  FG_CUDA(cudaMemsetAsync(G.d_ghost, 0, n, s));  // held smoothing scratch
+  FG_CUDA(cudaMemsetAsync(G.d_ghost, 0, n, s));
   geo::k_ghost_mark<<<(unsigned)((ni + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_body);
   FG_CUDA(cudaGetLastError());
   geo::k_dead_mark<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(g, G.d_iblank, G.d_ghost, G.d_dead);
