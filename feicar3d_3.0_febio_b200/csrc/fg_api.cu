@@ -1366,6 +1366,18 @@ fg_status fg_case_set_geometry(fg_case *c, const int8_t *iblank, const int8_t *g
   c->iblank.assign(iblank, iblank + nref);
   c->ghost.assign(ghostCellMark, ghostCellMark + nref);
   c->dead.assign(dead_cell, dead_cell + nref);
+  return fg::geometry_rows(c, nGhost, ghost_ijk, ghost_cell, ghost_coefN, nDead, dead_ijk,
+                           dead_cell_idx, dead_coefN, dead_probe, dead_ip);
+}
+
+}  // extern "C"
+
+fg_status fg::geometry_rows(fg_case *c, int nGhost, const int32_t *ghost_ijk,
+                            const int32_t *ghost_cell, const double *ghost_coefN, int nDead,
+                            const int32_t *dead_ijk, const int32_t *dead_cell_idx,
+                            const double *dead_coefN, const double *dead_probe,
+                            const double *dead_ip) {
+  const int8_t *iblank = c->iblank.data(), *dead_cell = c->dead.data();
   c->nGhost = nGhost;
   c->nDead = nDead;
   c->g_ijk.assign(ghost_ijk, ghost_ijk + 3 * (size_t)nGhost);
@@ -1403,6 +1415,8 @@ fg_status fg_case_set_geometry(fg_case *c, const int8_t *iblank, const int8_t *g
   c->prepared = false;
   return FG_OK;
 }
+
+extern "C" {
 
 fg_status fg_mg_prepare(fg_case *c) {
   if (!c) return FG_BAD_INPUT;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <memory>
+#include <new>
 #include <vector>
 
 #include "fg_internal.h"
@@ -35,6 +36,28 @@ struct HLevel {
   DevLevel dl{};
 };
 
+// page-locked host storage for the masks that cross between host and device
+// on every re-tag (copies at full link speed, no staging)
+template <class T>
+struct PinnedAlloc {
+  using value_type = T;
+  PinnedAlloc() = default;
+  template <class U>
+  PinnedAlloc(const PinnedAlloc<U> &) {}
+  T *allocate(size_t n) {
+    void *p = nullptr;
+    if (cudaMallocHost(&p, n * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+    return static_cast<T *>(p);
+  }
+  void deallocate(T *p, size_t) { cudaFreeHost(p); }
+};
+template <class T, class U>
+bool operator==(const PinnedAlloc<T> &, const PinnedAlloc<U> &) { return true; }
+template <class T, class U>
+bool operator!=(const PinnedAlloc<T> &, const PinnedAlloc<U> &) { return false; }
+template <class T>
+using pinned_vector = std::vector<T, PinnedAlloc<T>>;
+
 struct RowsHost {
   std::vector<long long> tgt, cell;
   std::vector<double> w, c0;
@@ -56,7 +79,7 @@ struct fg_case {
   // geometry
   std::unique_ptr<fg::Geom> geom;
   std::vector<double> d_ipv;           // dead-cell image points (3 per row)
-  std::vector<int8_t> iblank, ghost, dead;  // reference layout (host copies)
+  fg::pinned_vector<int8_t> iblank, ghost, dead;  // reference layout (host copies)
   bool has_geometry = false;
   bool prepared = false;
   // interpolation rows (dead rows first, then ghost rows, like the
@@ -78,3 +101,11 @@ struct fg_case {
   struct fg_batch *solo = nullptr;
 };
 
+namespace fg {
+// the interpolation rows of a geometry whose masks are already in
+// c->iblank / c->ghost / c->dead (argument meaning as fg_case_set_geometry)
+fg_status geometry_rows(fg_case *c, int nGhost, const int32_t *ghost_ijk, const int32_t *ghost_cell,
+                        const double *ghost_coefN, int nDead, const int32_t *dead_ijk,
+                        const int32_t *dead_cell_idx, const double *dead_coefN,
+                        const double *dead_probe, const double *dead_ip);
+}  // namespace fg

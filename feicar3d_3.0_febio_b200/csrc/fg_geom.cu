@@ -1200,11 +1200,15 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   FG_CUDA(cudaStreamSynchronize(s));
   G.nWarnSide += flags[0];
   G.nHostFail = flags[1];
-  // host copies of masks and rows
-  std::vector<int8_t> hib, hgh, hde;
-  if ((st = d2h(G.d_iblank, n, hib)) != FG_OK) return st;
-  if ((st = d2h(G.d_ghost, n, hgh)) != FG_OK) return st;
-  if ((st = d2h(G.d_dead, n, hde)) != FG_OK) return st;
+  // host copies of the masks (straight into the case's page-locked copies)
+  // and of the rows
+  c->iblank.resize(n);
+  c->ghost.resize(n);
+  c->dead.resize(n);
+  FG_CUDA(cudaMemcpyAsync(c->iblank.data(), G.d_iblank, n, cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaMemcpyAsync(c->ghost.data(), G.d_ghost, n, cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaMemcpyAsync(c->dead.data(), G.d_dead, n, cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
   std::vector<int> hgl, hdl;
   if ((st = d2h(glp, (size_t)ng, hgl)) != FG_OK) return st;
   if ((st = d2h(dlp, (size_t)nd, hdl)) != FG_OK) return st;
@@ -1227,15 +1231,14 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   if ((st = d2h((const double *)db.cD, 8 * (size_t)nd, G.d_coefD)) != FG_OK) return st;
   if ((st = d2h((const double *)db.o.bi, 3 * (size_t)nd, G.d_bi)) != FG_OK) return st;
   if ((st = d2h((const int32_t *)db.o.closest, (size_t)nd, G.d_closest)) != FG_OK) return st;
-  // hand the masks and rows to the solver (same path as caller-supplied
-  // geometry, which also marks the dead rows using the fallback)
-  st = fg_case_set_geometry(c, hib.data(), hgh.data(), hde.data(), ng, g_ijk.data(), g_cell.data(),
-                            g_coefN.data(), nd, d_ijk.data(), d_cell.data(), d_coefN.data(),
-                            d_probe.data(), d_ip.data());
+  // hand the rows to the solver (same path as caller-supplied geometry,
+  // which also marks the dead rows using the fallback)
+  st = fg::geometry_rows(c, ng, g_ijk.data(), g_cell.data(), g_coefN.data(), nd, d_ijk.data(),
+                         d_cell.data(), d_coefN.data(), d_probe.data(), d_ip.data());
   if (st != FG_OK) return st;
-  if (iblank) memcpy(iblank, hib.data(), n);
-  if (ghostCellMark) memcpy(ghostCellMark, hgh.data(), n);
-  if (dead_cell) memcpy(dead_cell, hde.data(), n);
+  if (iblank) memcpy(iblank, c->iblank.data(), n);
+  if (ghostCellMark) memcpy(ghostCellMark, c->ghost.data(), n);
+  if (dead_cell) memcpy(dead_cell, c->dead.data(), n);
   if (nGhost) *nGhost = ng;
   if (nDead) *nDead = nd;
   if (flags[2]) return FG_GEOMETRY_DEAD_NO_BODY;
