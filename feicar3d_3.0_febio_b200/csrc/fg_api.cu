@@ -341,9 +341,15 @@ struct fg_batch {
   struct VGraph {
     cudaGraphExec_t exec = nullptr;
     int key = -1;
-    long long launches = 0;  // kernels per replay
-    bool off = false;        // capture failed once: launch directly
+    std::vector<char> params;  // geometry-dependent launch arguments captured
+    long long launches = 0;    // kernels per replay
+    bool off = false;          // capture failed once: launch directly
   } vg;
+  // what the tables were built for: the problems and their level
+  // descriptors (fixed by the grids), and each problem's geometry version
+  std::vector<char> sig;
+  std::vector<long long> versions;
+  long long row_cap = 0;  // rows the row buffers hold
   // optional CUDA-event timing of launch classes (fg_profile)
   struct Prof {
     bool on = false;
@@ -388,6 +394,9 @@ static void free_batch_tables(fg_batch *b) {
   b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
   b->d_rf = nullptr; b->d_tmp = nullptr; b->d_norm = nullptr;
+  b->row_cap = 0;
+  b->sig.clear();
+  b->versions.clear();
   b->built = false;
 }
 
@@ -416,7 +425,103 @@ static fg_status build_offsets(const std::vector<int> &blocks, int **d_off, Laun
   return FG_OK;
 }
 
+// The problems of a batch and their level descriptors: device pointers and
+// sizes, which the grids fix.  A new geometry of the same problems changes
+// none of them, only the rows and the coarsest inverses.
+static std::vector<char> batch_signature(const fg_batch *b) {
+  std::vector<char> sig;
+  auto put = [&](const void *p, size_t n) {
+    sig.insert(sig.end(), (const char *)p, (const char *)p + n);
+  };
+  for (const fg_case *c : b->cases) {
+    put(&c, sizeof(c));
+    put(&c->nlev, sizeof(int));
+    for (int l = 0; l < c->nlev; ++l) put(&c->lev[l].dl, sizeof(DevLevel));
+  }
+  return sig;
+}
+
+// The geometry-dependent parts of the tables: the rows of all problems and
+// the coarsest inverses of every level set.  Called by a full build and,
+// alone, when only the problems' geometry changed since the last one.
+static fg_status upload_geometry(fg_batch *b) {
+  const int np = (int)b->cases.size();
+  for (int L = 0; L < b->maxdepth; ++L) {
+    auto &s = b->ls[L];
+    if (s.C.empty()) continue;
+    std::vector<const double *> gp;
+    std::vector<const int *> gi;
+    std::vector<int> gn;
+    s.maxgn = 0;
+    for (int p : s.C) {
+      const fg_case *c = b->cases[p];
+      gp.push_back(c->d_G);
+      gi.push_back(c->d_gidx);
+      gn.push_back((int)c->gidx.size());
+      s.maxgn = std::max(s.maxgn, (int)c->gidx.size());
+    }
+    FG_CUDA(cudaMemcpy(s.d_G, gp.data(), gp.size() * sizeof(double *), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(s.d_gidx, gi.data(), gi.size() * sizeof(int *), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(s.d_gn, gn.data(), gn.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  // rows (dead rows then ghost rows of each problem, problems in order)
+  std::vector<int> prob;
+  std::vector<long long> tgt, cell;
+  std::vector<double> w, c0;
+  for (int p = 0; p < np; ++p) {
+    const RowsHost &R = b->cases[p]->rows;
+    for (size_t r = 0; r < R.tgt.size(); ++r) {
+      prob.push_back(p);
+      tgt.push_back(R.tgt[r]);
+      cell.push_back(R.cell[r]);
+      c0.push_back(R.c0[r]);
+      for (int q = 0; q < 8; ++q) w.push_back(R.w[8 * r + q]);
+    }
+  }
+  const long long n = (long long)tgt.size();
+  if (n > b->row_cap) {
+    // all row buffers share one capacity, with room for the row count to
+    // grow as a body moves
+    const long long cap = n + n / 4 + 64;
+    cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
+    cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
+    b->d_rprob = nullptr; b->d_rtgt = nullptr; b->d_rcell = nullptr; b->d_rw = nullptr;
+    b->d_rc0 = nullptr; b->d_rd = nullptr; b->d_rf = nullptr; b->d_tmp = nullptr;
+    b->row_cap = 0;
+    FG_CUDA(cudaMalloc(&b->d_rprob, cap * sizeof(int)));
+    FG_CUDA(cudaMalloc(&b->d_rtgt, cap * sizeof(long long)));
+    FG_CUDA(cudaMalloc(&b->d_rcell, cap * sizeof(long long)));
+    FG_CUDA(cudaMalloc(&b->d_rw, 8 * cap * sizeof(double)));
+    FG_CUDA(cudaMalloc(&b->d_rc0, cap * sizeof(double)));
+    FG_CUDA(cudaMalloc(&b->d_rd, cap * sizeof(double)));
+    FG_CUDA(cudaMalloc(&b->d_rf, cap * sizeof(float)));
+    FG_CUDA(cudaMalloc(&b->d_tmp, cap * sizeof(double)));
+    b->row_cap = cap;
+  }
+  if (n > 0) {
+    FG_CUDA(cudaMemcpy(b->d_rprob, prob.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(b->d_rtgt, tgt.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(b->d_rcell, cell.data(), n * sizeof(long long), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(b->d_rw, w.data(), 8 * n * sizeof(double), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemcpy(b->d_rc0, c0.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    FG_CUDA(cudaMemset(b->d_rd, 0, n * sizeof(double)));
+    FG_CUDA(cudaMemset(b->d_rf, 0, n * sizeof(float)));
+  }
+  b->rows.n = (int)n;
+  b->rows.prob = mkptr<const int>(b->d_rprob, n, K_ROWS);
+  b->rows.tgt = mkptr<const long long>(b->d_rtgt, n, K_ROWS);
+  b->rows.cell = mkptr<const long long>(b->d_rcell, n, K_ROWS);
+  b->rows.w = mkptr<const double>(b->d_rw, 8LL * n, K_ROWS);
+  b->rows.c0 = mkptr<const double>(b->d_rc0, n, K_ROWS);
+  b->rows.rd = mkptr(b->d_rd, n, K_ROWS);
+  b->rows.rf = mkptr(b->d_rf, n, K_ROWS);
+  b->versions.clear();
+  for (const fg_case *c : b->cases) b->versions.push_back(c->geom_version);
+  return FG_OK;
+}
+
 static fg_status build_batch(fg_batch *b) {
+  if (b->built && b->sig == batch_signature(b)) return upload_geometry(b);
   free_batch_tables(b);
   const int np = (int)b->cases.size();
   b->maxdepth = 0;
@@ -425,9 +530,6 @@ static fg_status build_batch(fg_batch *b) {
     auto &s = b->ls[L];
     std::vector<DevLevel> vS, vSn, vC;
     std::vector<int> bc, bx, by, bz, bn, bq;
-    std::vector<const double *> gp;
-    std::vector<const int *> gi;
-    std::vector<int> gn;
     for (int p = 0; p < np; ++p) {
       const fg_case *c = b->cases[p];
       if (L < c->nlev - 1) {
@@ -453,10 +555,6 @@ static fg_status build_batch(fg_batch *b) {
       } else if (L == c->nlev - 1) {
         s.C.push_back(p);
         vC.push_back(c->lev[L].dl);
-        gp.push_back(c->d_G);
-        gi.push_back(c->d_gidx);
-        gn.push_back((int)c->gidx.size());
-        s.maxgn = std::max(s.maxgn, (int)c->gidx.size());
       }
     }
     FG_CUDA(run_launch_set_alloc((void **)&s.d_levS, vS));
@@ -471,9 +569,11 @@ static fg_status build_batch(fg_batch *b) {
       if ((st = build_offsets(bn, &s.d_off_next, s.next, s.d_levS_next)) != FG_OK) return st;
       if ((st = build_offsets(bq, &s.d_off_quads, s.quads, s.d_levS)) != FG_OK) return st;
     }
-    FG_CUDA(run_launch_set_alloc((void **)&s.d_G, gp));
-    FG_CUDA(run_launch_set_alloc((void **)&s.d_gidx, gi));
-    FG_CUDA(run_launch_set_alloc((void **)&s.d_gn, gn));
+    if (!s.C.empty()) {
+      FG_CUDA(cudaMalloc(&s.d_G, s.C.size() * sizeof(double *)));
+      FG_CUDA(cudaMalloc(&s.d_gidx, s.C.size() * sizeof(int *)));
+      FG_CUDA(cudaMalloc(&s.d_gn, s.C.size() * sizeof(int)));
+    }
   }
   // level 0 over all problems
   {
@@ -493,46 +593,12 @@ static fg_status build_batch(fg_batch *b) {
     st = build_offsets(bq, &b->d_offq0, b->all0q, b->d_lev0);
     if (st != FG_OK) return st;
   }
-  // rows
-  {
-    std::vector<int> prob;
-    std::vector<long long> tgt, cell;
-    std::vector<double> w, c0;
-    for (int p = 0; p < np; ++p) {
-      const RowsHost &R = b->cases[p]->rows;
-      for (size_t r = 0; r < R.tgt.size(); ++r) {
-        prob.push_back(p);
-        tgt.push_back(R.tgt[r]);
-        cell.push_back(R.cell[r]);
-        c0.push_back(R.c0[r]);
-        for (int q = 0; q < 8; ++q) w.push_back(R.w[8 * r + q]);
-      }
-    }
-    const int n = (int)tgt.size();
-    FG_CUDA(run_launch_set_alloc((void **)&b->d_rprob, prob));
-    FG_CUDA(run_launch_set_alloc((void **)&b->d_rtgt, tgt));
-    FG_CUDA(run_launch_set_alloc((void **)&b->d_rcell, cell));
-    FG_CUDA(run_launch_set_alloc((void **)&b->d_rw, w));
-    FG_CUDA(run_launch_set_alloc((void **)&b->d_rc0, c0));
-    if (n > 0) {
-      FG_CUDA(cudaMalloc(&b->d_rd, n * sizeof(double)));
-      FG_CUDA(cudaMalloc(&b->d_rf, n * sizeof(float)));
-      FG_CUDA(cudaMalloc(&b->d_tmp, n * sizeof(double)));
-      FG_CUDA(cudaMemset(b->d_rd, 0, n * sizeof(double)));
-      FG_CUDA(cudaMemset(b->d_rf, 0, n * sizeof(float)));
-    }
-    b->rows.n = n;
-    b->rows.prob = mkptr<const int>(b->d_rprob, n, K_ROWS);
-    b->rows.tgt = mkptr<const long long>(b->d_rtgt, n, K_ROWS);
-    b->rows.cell = mkptr<const long long>(b->d_rcell, n, K_ROWS);
-    b->rows.w = mkptr<const double>(b->d_rw, 8LL * n, K_ROWS);
-    b->rows.c0 = mkptr<const double>(b->d_rc0, n, K_ROWS);
-    b->rows.rd = mkptr(b->d_rd, n, K_ROWS);
-    b->rows.rf = mkptr(b->d_rf, n, K_ROWS);
-  }
+  fg_status st;
+  if ((st = upload_geometry(b)) != FG_OK) return st;
   FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
   FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
   b->h_norm.assign(3 * np, 0.0);
+  b->sig = batch_signature(b);
   b->built = true;
   return FG_OK;
 }
@@ -651,20 +717,35 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
   return FG_OK;
 }
 
+// Launch arguments of a V-cycle that a new geometry of the same problems
+// may change: the rows (count and buffers) and the coarsest sizes.
+static std::vector<char> vcycle_params(const fg_batch *b) {
+  std::vector<char> v;
+  auto put = [&](const void *p, size_t n) { v.insert(v.end(), (const char *)p, (const char *)p + n); };
+  put(&b->rows, sizeof(DevRows));
+  put(&b->d_tmp, sizeof(b->d_tmp));
+  for (int L = 0; L < b->maxdepth; ++L) put(&b->ls[L].maxgn, sizeof(int));
+  return v;
+}
+
 // One V-cycle as a CUDA graph: captured on first use after the batch's
 // tables are built, then replayed (one launch instead of a few hundred on a
-// deep hierarchy).  Direct launches while launch classes are timed, while
-// the stream is already being captured by the caller, or after a capture
-// failed.
+// deep hierarchy).  A new geometry that changes only launch arguments is
+// re-captured and patched into the instantiated graph in place.  Direct
+// launches while launch classes are timed, while the stream is already
+// being captured by the caller, or after a capture failed.
 template <typename T>
 static fg_status run_vcycle(fg_batch *b, cudaStream_t s) {
   if (b->prof.on || b->vg.off) return vcycle<T>(b, s);
   const int key = (sizeof(T) == 4 ? 1 : 0) | (b->krylov ? 2 : 0);
-  if (!b->vg.exec || b->vg.key != key) {
+  const bool same_key = b->vg.exec && b->vg.key == key;
+  std::vector<char> params;
+  if (same_key) params = vcycle_params(b);
+  if (!same_key || params != b->vg.params) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     FG_CUDA(cudaStreamIsCapturing(s, &cs));
     if (cs != cudaStreamCaptureStatusNone) return vcycle<T>(b, s);
-    if (b->vg.exec) { cudaGraphExecDestroy(b->vg.exec); b->vg.exec = nullptr; }
+    if (b->vg.exec && !same_key) { cudaGraphExecDestroy(b->vg.exec); b->vg.exec = nullptr; }
     const long long n0 = thread_launches();
     FG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     const fg_status st = vcycle<T>(b, s);
@@ -673,15 +754,28 @@ static fg_status run_vcycle(fg_batch *b, cudaStream_t s) {
     const long long captured = thread_launches() - n0;
     note_launches(-captured);  // counted when replayed
     cudaError_t ei = cudaErrorUnknown;
-    if (st == FG_OK && e == cudaSuccess && g) ei = cudaGraphInstantiate(&b->vg.exec, g, 0);
+    if (st == FG_OK && e == cudaSuccess && g) {
+      if (b->vg.exec) {
+        cudaGraphExecUpdateResultInfo info;
+        ei = cudaGraphExecUpdate(b->vg.exec, g, &info);
+        if (ei != cudaSuccess) {
+          (void)cudaGetLastError();
+          cudaGraphExecDestroy(b->vg.exec);
+          b->vg.exec = nullptr;
+        }
+      }
+      if (!b->vg.exec) ei = cudaGraphInstantiate(&b->vg.exec, g, 0);
+    }
     if (g) cudaGraphDestroy(g);
     if (ei != cudaSuccess) {
+      if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
       b->vg.exec = nullptr;
       b->vg.off = true;
       (void)cudaGetLastError();
       return vcycle<T>(b, s);
     }
     b->vg.key = key;
+    b->vg.params = same_key ? params : vcycle_params(b);
     b->vg.launches = captured;
   }
   FG_CUDA(cudaGraphLaunch(b->vg.exec, s));
@@ -1204,17 +1298,29 @@ static fg_status prepare(fg_case *c) {
     FG_CUDA(cudaMemcpy(L.d_mask, L.mask.data(), L.ntot, cudaMemcpyHostToDevice));
   }
   coarsest_inverse(c);
-  cudaFree(c->d_G); cudaFree(c->d_gidx);
-  c->d_G = nullptr; c->d_gidx = nullptr;
+  // grow-only: a moving body changes the coarsest size a little per step
   if (!c->G.empty()) {
-    FG_CUDA(cudaMalloc(&c->d_G, c->G.size() * sizeof(double)));
+    if (c->G.size() > c->G_cap) {
+      cudaFree(c->d_G);
+      c->d_G = nullptr;
+      c->G_cap = 0;
+      FG_CUDA(cudaMalloc(&c->d_G, c->G.size() * sizeof(double)));
+      c->G_cap = c->G.size();
+    }
     FG_CUDA(cudaMemcpy(c->d_G, c->G.data(), c->G.size() * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<int> gi(c->gidx.begin(), c->gidx.end());
-    FG_CUDA(cudaMalloc(&c->d_gidx, gi.size() * sizeof(int)));
+    if (gi.size() > c->gidx_cap) {
+      cudaFree(c->d_gidx);
+      c->d_gidx = nullptr;
+      c->gidx_cap = 0;
+      FG_CUDA(cudaMalloc(&c->d_gidx, gi.size() * sizeof(int)));
+      c->gidx_cap = gi.size();
+    }
     FG_CUDA(cudaMemcpy(c->d_gidx, gi.data(), gi.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   c->prepared = true;
   c->batch_dirty = true;
+  c->geom_version++;
   return FG_OK;
 }
 
@@ -1618,7 +1724,10 @@ fg_status fg_batch_solve_device(fg_batch *b, double **d_p, const double **d_div,
       fg_status s = prepare(c);
       if (s != FG_OK) return s;
     }
-  if (!b->built) {
+  bool stale = !b->built || b->versions.size() != b->cases.size();
+  for (size_t p = 0; !stale && p < b->cases.size(); ++p)
+    stale = b->versions[p] != b->cases[p]->geom_version;
+  if (stale) {
     fg_status s = build_batch(b);
     if (s != FG_OK) return s;
   }

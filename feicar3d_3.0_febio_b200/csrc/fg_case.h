@@ -94,6 +94,8 @@ struct fg_case {
   std::vector<int> gidx;
   double *d_G = nullptr;
   int *d_gidx = nullptr;
+  size_t G_cap = 0, gidx_cap = 0;  // elements the two device arrays hold
+  long long geom_version = 0;      // bumped by every prepare
   // reference-layout staging buffers on the device
   double *d_pin = nullptr, *d_fin = nullptr;
   double *d_gauge = nullptr;  // p(1,1,1) of the output gauge
