@@ -98,6 +98,7 @@ static fg_status alloc_level(fg_case *c, HLevel &L, bool lvl0) {
   fg_status st;
   if ((st = alloc_field(L, &L.d_type)) != FG_OK) return st;
   if ((st = alloc_field(L, &L.d_mask)) != FG_OK) return st;
+  if ((st = alloc_field(L, &L.d_ibk)) != FG_OK) return st;
   if (!mixed || lvl0) {
     if ((st = alloc_field(L, &L.d_x64)) != FG_OK) return st;
     if ((st = alloc_field(L, &L.d_rhs64)) != FG_OK) return st;
@@ -169,6 +170,16 @@ static fg_status upload_axes(fg_case *c, int l) {
   }
   FG_CUDA(cudaMalloc(&L.d_coef, dbl.size() * sizeof(double)));
   FG_CUDA(cudaMemcpy(L.d_coef, dbl.data(), dbl.size() * sizeof(double), cudaMemcpyHostToDevice));
+  {
+    std::vector<double> nodes(L.x);
+    nodes.insert(nodes.end(), L.y.begin(), L.y.end());
+    nodes.insert(nodes.end(), L.z.begin(), L.z.end());
+    void *raw = nullptr;
+    FG_CUDA(cudaMalloc(&raw, nodes.size() * sizeof(double)));
+    L.raw.push_back(raw);
+    L.d_nodes = static_cast<double *>(raw);
+    FG_CUDA(cudaMemcpy(L.d_nodes, nodes.data(), nodes.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   FG_CUDA(cudaMalloc(&L.d_int, ints.size() * sizeof(int)));
   FG_CUDA(cudaMemcpy(L.d_int, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
   DevLevel &d = L.dl;
@@ -1177,27 +1188,116 @@ static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
 }
 
 // -------------------------------------------------------- case geometry
-// level-0 types and rows from the reference masks and lists
-static fg_status install_geometry(fg_case *c) {
+namespace prep {
+
+// one level as the mask kernels see it
+struct Lv {
+  int nx, ny, nz;
+  long long sy, sz;
+  int8_t *type, *ibk;
+  uint8_t *mask;
+  const double *x, *y, *z;  // node arrays (x: nx+2 entries, ...)
+};
+
+__device__ __forceinline__ bool cell_of(const Lv &L, long long e, int &i, int &j, int &k) {
+  if (e >= (long long)L.nx * L.ny * L.nz) return false;
+  i = 1 + (int)(e % L.nx);
+  j = 1 + (int)((e / L.nx) % L.ny);
+  k = 1 + (int)(e / ((long long)L.nx * L.ny));
+  return true;
+}
+
+// level-0 interior: fluid (iblank 0, not a ghost) or solid; solid flag =
+// iblank.  Rows then turn their non-fluid targets into ghost cells.
+__global__ void k_install(Lv L, const int8_t *iblank, const int8_t *ghost, long long RX, long long RY) {
+  int i, j, k;
+  if (!cell_of(L, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const long long r = i + RX * (j + RY * (long long)k), d = i + L.sy * j + L.sz * k;
+  const int8_t ib = iblank[r], gh = ghost[r];
+  L.type[d] = (ib == 0 && gh == 0) ? T_ACTIVE : T_SOLID;
+  L.ibk[d] = ib;
+}
+
+__global__ void k_mark_rows(Lv L, const long long *tgt, int n) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const long long t = tgt[r];
+  if (L.type[t] != T_ACTIVE) L.type[t] = T_GHOST;
+}
+
+// CORE_MG.F90:1459-1506: a coarse cell is solid (excluded) when its
+// children's solid volume fraction is >= 0.5.  Products and sums are
+// rounded one by one (no fused multiply-add) in the order of the loops, so
+// the fraction is the same double as a plain sequential evaluation.
+__global__ void k_coarse(Lv F, Lv C, int cx, int cy, int cz) {
+  int I, J, K;
+  if (!cell_of(C, (long long)blockIdx.x * blockDim.x + threadIdx.x, I, J, K)) return;
+  const int i1 = cx ? 2 * I - 1 : I, i2 = cx ? min(2 * I, F.nx) : I;
+  const int j1 = cy ? 2 * J - 1 : J, j2 = cy ? min(2 * J, F.ny) : J;
+  const int k1 = cz ? 2 * K - 1 : K, k2 = cz ? min(2 * K, F.nz) : K;
+  double v0 = 0.0, vb = 0.0;
+  for (int kk = k1; kk <= k2; ++kk)
+    for (int jj = j1; jj <= j2; ++jj)
+      for (int ii = i1; ii <= i2; ++ii) {
+        const double v = __dmul_rn(__dmul_rn(__dsub_rn(F.x[ii + 1], F.x[ii]),
+                                             __dsub_rn(F.y[jj + 1], F.y[jj])),
+                                   __dsub_rn(F.z[kk + 1], F.z[kk]));
+        v0 = __dadd_rn(v0, v);
+        if (F.ibk[ii + F.sy * jj + F.sz * kk]) vb = __dadd_rn(vb, v);
+      }
+  const long long d = I + C.sy * J + C.sz * K;
+  const bool sol = __ddiv_rn(vb, v0) >= 0.5;
+  C.ibk[d] = sol ? 1 : 0;
+  C.type[d] = sol ? T_OFF : T_ACTIVE;
+}
+
+// operator mask of every interior cell (see DevLevel::mask)
+__global__ void k_mask(Lv L) {
+  int i, j, k;
+  if (!cell_of(L, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+  const long long id = i + L.sy * j + L.sz * k;
+  const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
+  const int8_t t = L.type[id];
+  uint8_t m = 0;
+  for (int q = 0; q < 6; ++q) {
+    const int8_t nt = L.type[id + off[q]];
+    if (nt == T_ACTIVE || nt == T_GHOST || nt == T_SOLID) m |= (uint8_t)(1u << q);
+  }
+  if (t == T_ACTIVE) m |= 64;
+  if (t == T_ACTIVE || t == T_GHOST) m |= 128;
+  L.mask[id] = m;
+}
+
+static Lv lv(const HLevel &L) {
+  Lv v;
+  v.nx = L.nx; v.ny = L.ny; v.nz = L.nz;
+  v.sy = L.sy; v.sz = L.sz;
+  v.type = L.d_type; v.ibk = L.d_ibk; v.mask = L.d_mask;
+  v.x = L.d_nodes;
+  v.y = L.d_nodes + L.x.size();
+  v.z = L.d_nodes + L.x.size() + L.y.size();
+  return v;
+}
+
+static unsigned cell_blocks(const HLevel &L) {
+  return (unsigned)(((long long)L.nx * L.ny * L.nz + 255) / 256);
+}
+
+}  // namespace prep
+
+// level-0 rows from the reference lists: target and host-cell elements,
+// weights with the own slot zeroed (all zero for fallback dead rows)
+static void install_rows(fg_case *c) {
   HLevel &L0 = c->lev[0];
-  const int nx = c->nx, ny = c->ny;  // nodes
-  const long long RX = nx + 2, RY = ny + 2;
-  auto ref = [&](int i, int j, int k) { return (long long)i + RX * ((long long)j + RY * k); };
-  L0.type.assign(L0.ntot, T_BOUND);
-  L0.ibk.assign(L0.ntot, 0);
-  // rows first: which dead rows are valid / use the fallback
-  std::vector<int8_t> has_row(L0.ntot, 0);
   c->rows = RowsHost();
   auto add_rows = [&](int n, const std::vector<int32_t> &ijk, const std::vector<int32_t> &cell,
-                      const std::vector<double> &coef, const std::vector<double> *probe,
-                      const std::vector<int8_t> *fallback) {
+                      const std::vector<double> &coef, const std::vector<int8_t> *fallback) {
     for (int r = 0; r < n; ++r) {
       int i = ijk[3 * r], j = ijk[3 * r + 1], k = ijk[3 * r + 2];
       int ci = cell[3 * r], cj = cell[3 * r + 1], ck = cell[3 * r + 2];
       if (i < 1 || i > L0.nx || j < 1 || j > L0.ny || k < 1 || k > L0.nz) continue;
       if (ci < 0 || cj < 0 || ck < 0 || ci > L0.nx || cj > L0.ny || ck > L0.nz) continue;
-      long long t = dev_index(L0, i, j, k);
-      c->rows.tgt.push_back(t);
+      c->rows.tgt.push_back(dev_index(L0, i, j, k));
       c->rows.cell.push_back(dev_index(L0, ci, cj, ck));
       static const int inc[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
                                     {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
@@ -1207,78 +1307,55 @@ static fg_status install_geometry(fg_case *c) {
         c->rows.w.push_back((own || fb) ? 0.0 : coef[8 * r + q]);
       }
       c->rows.c0.push_back(0.0);
-      has_row[t] = 1;
     }
   };
-  add_rows(c->nDead, c->d_ijk, c->d_cell, c->d_coefN, &c->d_probe, &c->d_fallback);
-  add_rows(c->nGhost, c->g_ijk, c->g_cell, c->g_coefN, nullptr, nullptr);
-  // every cell is written once: the planes go to the host threads
-#pragma omp parallel for schedule(static)
-  for (int k = 1; k <= L0.nz; ++k)
-    for (int j = 1; j <= L0.ny; ++j)
-      for (int i = 1; i <= L0.nx; ++i) {
-        long long r = ref(i, j, k), d = dev_index(L0, i, j, k);
-        int8_t ib = c->iblank[r], gh = c->ghost[r], dd = c->dead[r];
-        int8_t t;
-        if (ib == 0 && gh == 0) t = T_ACTIVE;
-        else if (has_row[d]) t = T_GHOST;
-        else t = T_SOLID;
-        L0.type[d] = t;
-        L0.ibk[d] = ib;
-      }
-  return FG_OK;
+  add_rows(c->nDead, c->d_ijk, c->d_cell, c->d_coefN, &c->d_fallback);
+  add_rows(c->nGhost, c->g_ijk, c->g_cell, c->g_coefN, nullptr);
 }
 
-// CORE_MG.F90:1459-1506: coarse cell solid when its children's solid
-// volume fraction is >= 0.5
-static void coarse_masks(fg_case *c) {
-  for (int l = 1; l < c->nlev; ++l) {
-    HLevel &F = c->lev[l - 1], &C = c->lev[l];
-    C.type.assign(C.ntot, T_BOUND);
-    C.ibk.assign(C.ntot, 0);
-    const bool cx = C.nx != F.nx, cy = C.ny != F.ny, cz = C.nz != F.nz;
-#pragma omp parallel for schedule(static)
-    for (int K = 1; K <= C.nz; ++K)
-      for (int J = 1; J <= C.ny; ++J)
-        for (int I = 1; I <= C.nx; ++I) {
-          int i1 = cx ? 2 * I - 1 : I, i2 = cx ? std::min(2 * I, F.nx) : I;
-          int j1 = cy ? 2 * J - 1 : J, j2 = cy ? std::min(2 * J, F.ny) : J;
-          int k1 = cz ? 2 * K - 1 : K, k2 = cz ? std::min(2 * K, F.nz) : K;
-          double v0 = 0.0, vb = 0.0;
-          for (int kk = k1; kk <= k2; ++kk)
-            for (int jj = j1; jj <= j2; ++jj)
-              for (int ii = i1; ii <= i2; ++ii) {
-                double v = (F.x[ii + 1] - F.x[ii]) * (F.y[jj + 1] - F.y[jj]) * (F.z[kk + 1] - F.z[kk]);
-                v0 += v;
-                if (F.ibk[dev_index(F, ii, jj, kk)]) vb += v;
-              }
-          long long d = dev_index(C, I, J, K);
-          int8_t sol = (vb / v0 >= 0.5) ? 1 : 0;
-          C.ibk[d] = sol;
-          C.type[d] = sol ? T_OFF : T_ACTIVE;
-        }
+// Types and operator masks of every level, built on the device from the
+// reference masks and the rows: level 0 from iblank / ghostCellMark and the
+// row targets, coarser levels by solid volume fraction, then the masks.
+// Only the coarsest level's types come back (for its generalised inverse).
+static fg_status build_levels(fg_case *c) {
+  cudaStream_t s = c->stream;
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  if (!c->d_refmask) FG_CUDA(cudaMalloc(&c->d_refmask, 2 * nref));
+  FG_CUDA(cudaMemcpyAsync(c->d_refmask, c->iblank.data(), nref, cudaMemcpyHostToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(c->d_refmask + nref, c->ghost.data(), nref, cudaMemcpyHostToDevice, s));
+  const int nr = (int)c->rows.tgt.size();
+  if ((size_t)nr > c->rowtgt_cap) {
+    cudaFree(c->d_rowtgt);
+    c->d_rowtgt = nullptr;
+    c->rowtgt_cap = 0;
+    const size_t cap = (size_t)nr + nr / 4 + 64;
+    FG_CUDA(cudaMalloc(&c->d_rowtgt, cap * sizeof(long long)));
+    c->rowtgt_cap = cap;
   }
-}
-
-// operator mask of every interior cell (see DevLevel::mask)
-static void build_mask(HLevel &L) {
-  L.mask.assign(L.ntot, 0);
-  const long long off[6] = {-1, 1, -L.sy, L.sy, -L.sz, L.sz};
-#pragma omp parallel for schedule(static)
-  for (int k = 1; k <= L.nz; ++k)
-    for (int j = 1; j <= L.ny; ++j)
-      for (int i = 1; i <= L.nx; ++i) {
-        const long long id = dev_index(L, i, j, k);
-        const int8_t t = L.type[id];
-        uint8_t m = 0;
-        for (int q = 0; q < 6; ++q) {
-          const int8_t nt = L.type[id + off[q]];
-          if (nt == T_ACTIVE || nt == T_GHOST || nt == T_SOLID) m |= (uint8_t)(1u << q);
-        }
-        if (t == T_ACTIVE) m |= 64;
-        if (t == T_ACTIVE || t == T_GHOST) m |= 128;
-        L.mask[id] = m;
-      }
+  if (nr > 0)
+    FG_CUDA(cudaMemcpyAsync(c->d_rowtgt, c->rows.tgt.data(), nr * sizeof(long long),
+                            cudaMemcpyHostToDevice, s));
+  for (int l = 0; l < c->nlev; ++l) {
+    FG_CUDA(cudaMemsetAsync(c->lev[l].d_type, T_BOUND, c->lev[l].ntot, s));
+    FG_CUDA(cudaMemsetAsync(c->lev[l].d_mask, 0, c->lev[l].ntot, s));
+  }
+  const HLevel &L0 = c->lev[0];
+  prep::k_install<<<prep::cell_blocks(L0), 256, 0, s>>>(prep::lv(L0), c->d_refmask,
+                                                        c->d_refmask + nref, c->nx + 2, c->ny + 2);
+  if (nr > 0) prep::k_mark_rows<<<(nr + 255) / 256, 256, 0, s>>>(prep::lv(L0), c->d_rowtgt, nr);
+  for (int l = 1; l < c->nlev; ++l) {
+    const HLevel &F = c->lev[l - 1], &C = c->lev[l];
+    prep::k_coarse<<<prep::cell_blocks(C), 256, 0, s>>>(prep::lv(F), prep::lv(C), C.nx != F.nx,
+                                                         C.ny != F.ny, C.nz != F.nz);
+  }
+  for (int l = 0; l < c->nlev; ++l)
+    prep::k_mask<<<prep::cell_blocks(c->lev[l]), 256, 0, s>>>(prep::lv(c->lev[l]));
+  FG_CUDA(cudaGetLastError());
+  HLevel &Lc = c->lev[c->nlev - 1];
+  Lc.type.resize(Lc.ntot);
+  FG_CUDA(cudaMemcpyAsync(Lc.type.data(), Lc.d_type, Lc.ntot, cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  return FG_OK;
 }
 
 static fg_status prepare(fg_case *c) {
@@ -1289,14 +1366,9 @@ static fg_status prepare(fg_case *c) {
     c->nGhost = c->nDead = 0;
     c->has_geometry = true;
   }
-  install_geometry(c);
-  coarse_masks(c);
-  for (int l = 0; l < c->nlev; ++l) {
-    HLevel &L = c->lev[l];
-    build_mask(L);
-    FG_CUDA(cudaMemcpy(L.d_type, L.type.data(), L.ntot, cudaMemcpyHostToDevice));
-    FG_CUDA(cudaMemcpy(L.d_mask, L.mask.data(), L.ntot, cudaMemcpyHostToDevice));
-  }
+  install_rows(c);
+  fg_status st = build_levels(c);
+  if (st != FG_OK) return st;
   coarsest_inverse(c);
   // grow-only: a moving body changes the coarsest size a little per step
   if (!c->G.empty()) {
@@ -1441,6 +1513,7 @@ fg_status fg_case_destroy(fg_case *c) {
     L.raw.clear();
   }
   cudaFree(c->d_G); cudaFree(c->d_gidx); cudaFree(c->d_pin); cudaFree(c->d_fin);
+  cudaFree(c->d_refmask); cudaFree(c->d_rowtgt);
   cudaFree(c->d_gauge);
   if (c->geom) geom_free(*c->geom);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);

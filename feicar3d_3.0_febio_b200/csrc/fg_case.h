@@ -22,12 +22,12 @@ struct HLevel {
   long long sy = 0, sz = 0, ntot = 0;
   std::vector<double> x, y, z, xc, yc, zc;          // 0..n+1 (reference level arrays)
   std::vector<double> dxinv, dyinv, dzinv, dxcinv, dycinv, dzcinv;
-  std::vector<int8_t> ibk;   // solid flag on the device layout (interior)
-  std::vector<int8_t> type;  // device layout
+  std::vector<int8_t> type;  // device layout, host copy of the coarsest level only
   // device
   int8_t *d_type = nullptr;
   uint8_t *d_mask = nullptr;
-  std::vector<uint8_t> mask;
+  int8_t *d_ibk = nullptr;      // solid flag (interior cells)
+  double *d_nodes = nullptr;    // x, y, z node arrays back to back
   double *d_coef = nullptr;  // packed 1-D double arrays
   int *d_int = nullptr;      // packed 1-D int arrays
   double *d_x64 = nullptr, *d_rhs64 = nullptr, *d_res64 = nullptr;
@@ -98,6 +98,9 @@ struct fg_case {
   long long geom_version = 0;      // bumped by every prepare
   // reference-layout staging buffers on the device
   double *d_pin = nullptr, *d_fin = nullptr;
+  int8_t *d_refmask = nullptr;      // iblank then ghostCellMark (reference layout)
+  long long *d_rowtgt = nullptr;    // level-0 element of every row
+  size_t rowtgt_cap = 0;
   double *d_gauge = nullptr;  // p(1,1,1) of the output gauge
   bool batch_dirty = true;
   struct fg_batch *solo = nullptr;
