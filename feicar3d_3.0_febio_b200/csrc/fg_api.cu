@@ -2,6 +2,7 @@
 // multigrid hierarchy (CORE_GRID.F90:29-205, CORE_MG.F90:22-599), masks
 // (CORE_MG.F90:1365-1555), batched V-cycle driver, C ABI.
 #include <cuda_runtime.h>
+#include <omp.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
@@ -9,8 +10,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "fg_case.h"
@@ -25,6 +29,59 @@ void set_last_error(const char *msg, const char *file, int line) {
   g_err = buf;
 }
 const char *last_error_msg() { return g_err.c_str(); }
+
+// ------------------------------------------------- page-locked host pool
+namespace {
+struct PinnedPool {
+  std::mutex mu;
+  std::multimap<size_t, void *> free_by_size;
+  std::unordered_map<void *, size_t> size_of;
+  size_t cached = 0;
+};
+PinnedPool &pinned_pool() {
+  static PinnedPool *pool = new PinnedPool();  // lives until exit: no CUDA calls at teardown
+  return *pool;
+}
+constexpr size_t kPinnedCacheMax = size_t(2) << 30;
+}  // namespace
+
+void *pinned_get(size_t bytes) {
+  if (bytes == 0) bytes = 1;
+  PinnedPool &P = pinned_pool();
+  {
+    std::lock_guard<std::mutex> lk(P.mu);
+    // smallest cached block that fits, unless it would waste most of itself
+    auto it = P.free_by_size.lower_bound(bytes);
+    if (it != P.free_by_size.end() && it->first / 4 <= bytes) {
+      void *p = it->second;
+      P.cached -= it->first;
+      P.free_by_size.erase(it);
+      return p;
+    }
+  }
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(P.mu);
+  P.size_of[p] = bytes;
+  return p;
+}
+
+void pinned_put(void *p) {
+  if (!p) return;
+  PinnedPool &P = pinned_pool();
+  std::lock_guard<std::mutex> lk(P.mu);
+  const size_t n = P.size_of[p];
+  if (P.cached + n > kPinnedCacheMax) {
+    P.size_of.erase(p);
+    cudaFreeHost(p);
+    return;
+  }
+  P.free_by_size.emplace(n, p);
+  P.cached += n;
+}
 
 static int coarsen_count(int n) { return (n % 2 == 0) ? n / 2 + 1 : (n + 1) / 2; }
 static int auto_levels(int n) {
@@ -258,21 +315,42 @@ static void coarsest_inverse(fg_case *c) {
   for (double v : A) amax = std::max(amax, std::fabs(v));
   std::vector<char> used_r(n, 0), used_c(n, 0);
   std::vector<int> piv_r, piv_c;
+  // Rows are split between the host threads on large coarsest levels (a
+  // few hundred unknowns): each thread owns whole rows, so every element
+  // sees the same operations in the same order as a sequential run, and the
+  // pivot is the first largest element in row-major order either way
+  // (per-thread row ranges ascend and are combined in order).
+  const bool par = n >= 128;
+  const int nth = par ? std::max(1, omp_get_max_threads()) : 1;
+  std::vector<double> tb(nth);
+  std::vector<int> tr(nth), tq(nth);
   for (int step = 0; step < n; ++step) {
     double best = 0.0; int br = -1, bc = -1;
-    for (int r = 0; r < n; ++r) {
-      if (used_r[r]) continue;
-      for (int q = 0; q < n; ++q) {
-        if (used_c[q]) continue;
-        double v = std::fabs(M[(size_t)r * n + q]);
-        if (v > best) { best = v; br = r; bc = q; }
+#pragma omp parallel num_threads(nth) if (par)
+    {
+      const int t = par ? omp_get_thread_num() : 0, m = par ? omp_get_num_threads() : 1;
+      const int r0 = (int)((long long)n * t / m), r1 = (int)((long long)n * (t + 1) / m);
+      double b_ = 0.0; int rr = -1, qq = -1;
+      for (int r = r0; r < r1; ++r) {
+        if (used_r[r]) continue;
+        for (int q = 0; q < n; ++q) {
+          if (used_c[q]) continue;
+          double v = std::fabs(M[(size_t)r * n + q]);
+          if (v > b_) { b_ = v; rr = r; qq = q; }
+        }
       }
+      tb[t] = b_; tr[t] = rr; tq[t] = qq;
+      if (m < nth && t == 0)
+        for (int u = m; u < nth; ++u) { tb[u] = 0.0; tr[u] = -1; tq[u] = -1; }
     }
+    for (int t = 0; t < nth; ++t)
+      if (tb[t] > best) { best = tb[t]; br = tr[t]; bc = tq[t]; }
     if (br < 0 || best <= 1e-12 * amax) break;
     used_r[br] = 1; used_c[bc] = 1;
     piv_r.push_back(br); piv_c.push_back(bc);
     const double pv = M[(size_t)br * n + bc];
     for (int q = 0; q < n; ++q) { M[(size_t)br * n + q] /= pv; Iv[(size_t)br * n + q] /= pv; }
+#pragma omp parallel for schedule(static) num_threads(nth) if (par)
     for (int r = 0; r < n; ++r) {
       if (r == br) continue;
       const double f = M[(size_t)r * n + bc];
@@ -877,7 +955,12 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
 }
 
 // ------------------------------------------------------------ FGMRES
-constexpr double kReorth = 1e-4;  // second Gram-Schmidt pass below this fraction of |w|^2
+// Second Gram-Schmidt pass when the first leaves less than this fraction of
+// |w|^2.  At 1e-4 the FP32 basis of small sphere/ellipsoid problems lost
+// enough orthogonality to cost two extra cycles (9 instead of 7); at 1e-2
+// they keep 7 and the large box case keeps its time (a test at 0.1 or 0.5
+// fires on almost every step and costs 6 % there).
+constexpr double kReorth = 1e-2;
 
 static int krylov_restart(const fg_solver_config &cfg) {
   int m = cfg.restart > 0 ? cfg.restart : 10;

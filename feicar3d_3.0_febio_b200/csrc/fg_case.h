@@ -37,7 +37,12 @@ struct HLevel {
 };
 
 // page-locked host storage for the masks that cross between host and device
-// on every re-tag (copies at full link speed, no staging)
+// on every re-tag (copies at full link speed, no staging).  Blocks come
+// from a process-wide pool and go back to it: pinning and unpinning pages
+// costs milliseconds per call and serialises with the device, too much for
+// a case that lives one request.
+void *pinned_get(size_t bytes);
+void pinned_put(void *p);
 template <class T>
 struct PinnedAlloc {
   using value_type = T;
@@ -45,11 +50,11 @@ struct PinnedAlloc {
   template <class U>
   PinnedAlloc(const PinnedAlloc<U> &) {}
   T *allocate(size_t n) {
-    void *p = nullptr;
-    if (cudaMallocHost(&p, n * sizeof(T)) != cudaSuccess) throw std::bad_alloc();
+    void *p = pinned_get(n * sizeof(T));
+    if (!p) throw std::bad_alloc();
     return static_cast<T *>(p);
   }
-  void deallocate(T *p, size_t) { cudaFreeHost(p); }
+  void deallocate(T *p, size_t) { pinned_put(p); }
 };
 template <class T, class U>
 bool operator==(const PinnedAlloc<T> &, const PinnedAlloc<U> &) { return true; }
