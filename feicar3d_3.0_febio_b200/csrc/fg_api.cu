@@ -45,6 +45,100 @@ PinnedPool &pinned_pool() {
 constexpr size_t kPinnedCacheMax = size_t(2) << 30;
 }  // namespace
 
+// ------------------------------------------------------ device block cache
+namespace {
+struct DevCache {
+  std::mutex mu;
+  std::multimap<std::pair<int, size_t>, void *> free_blocks;  // (device, rounded size)
+  std::unordered_map<void *, std::pair<int, size_t>> owner;
+  std::unordered_map<int, size_t> cached;
+};
+DevCache &dev_cache() {
+  static DevCache *c = new DevCache();  // lives until exit: no CUDA calls at teardown
+  return *c;
+}
+constexpr size_t kDevCacheMax = size_t(8) << 30;  // per device
+size_t dev_round(size_t b) {
+  if (b <= (size_t(1) << 20)) {
+    size_t r = 256;
+    while (r < b) r <<= 1;
+    return r;
+  }
+  const size_t g = size_t(2) << 20;
+  return (b + g - 1) / g * g;
+}
+}  // namespace
+
+cudaError_t dev_alloc_raw(void **p, size_t bytes) {
+  *p = nullptr;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const size_t r = dev_round(bytes > 0 ? bytes : 1);
+  DevCache &C = dev_cache();
+  {
+    std::lock_guard<std::mutex> lk(C.mu);
+    auto it = C.free_blocks.find({dev, r});
+    if (it != C.free_blocks.end()) {
+      *p = it->second;
+      C.free_blocks.erase(it);
+      C.cached[dev] -= r;
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, r);
+  if (e == cudaErrorMemoryAllocation) {
+    // give the cached blocks of this device back and try once more
+    (void)cudaGetLastError();
+    cudaDeviceSynchronize();
+    std::lock_guard<std::mutex> lk(C.mu);
+    for (auto it = C.free_blocks.begin(); it != C.free_blocks.end();) {
+      if (it->first.first == dev) {
+        cudaFree(it->second);
+        C.owner.erase(it->second);
+        it = C.free_blocks.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    C.cached[dev] = 0;
+    e = cudaMalloc(p, r);
+  }
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return e;
+  }
+  std::lock_guard<std::mutex> lk(C.mu);
+  C.owner[*p] = {dev, r};
+  return cudaSuccess;
+}
+
+void dev_free(void *p) {
+  if (!p) return;
+  DevCache &C = dev_cache();
+  std::pair<int, size_t> o;
+  {
+    std::lock_guard<std::mutex> lk(C.mu);
+    auto it = C.owner.find(p);
+    if (it == C.owner.end()) return;  // not from dev_alloc
+    o = it->second;
+  }
+  // the block may still be read by queued work: wait like cudaFree does
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != o.first) cudaSetDevice(o.first);
+  cudaDeviceSynchronize();
+  std::lock_guard<std::mutex> lk(C.mu);
+  if (C.cached[o.first] + o.second > kDevCacheMax) {
+    C.owner.erase(p);
+    cudaFree(p);
+  } else {
+    C.free_blocks.emplace(o, p);
+    C.cached[o.first] += o.second;
+  }
+  if (cur != o.first) cudaSetDevice(cur);
+}
+
 void *pinned_get(size_t bytes) {
   if (bytes == 0) bytes = 1;
   PinnedPool &P = pinned_pool();
@@ -139,7 +233,7 @@ constexpr long long kFieldPad = 15;
 template <typename T>
 static fg_status alloc_field(HLevel &L, T **p) {
   void *raw = nullptr;
-  FG_CUDA(cudaMalloc(&raw, (size_t)(L.ntot + kFieldPad + 1) * sizeof(T)));
+  FG_CUDA(fg::dev_alloc(&raw, (size_t)(L.ntot + kFieldPad + 1) * sizeof(T)));
   L.raw.push_back(raw);
   FG_CUDA(cudaMemset(raw, 0, (size_t)(L.ntot + kFieldPad + 1) * sizeof(T)));
   *p = reinterpret_cast<T *>(raw) + kFieldPad;
@@ -225,19 +319,19 @@ static fg_status upload_axes(fg_case *c, int l) {
     ioff[a][1] = ints.size(); ints.insert(ints.end(), ch.begin(), ch.end());
     ioff[a][2] = ints.size(); ints.insert(ints.end(), pl.begin(), pl.end());
   }
-  FG_CUDA(cudaMalloc(&L.d_coef, dbl.size() * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&L.d_coef, dbl.size() * sizeof(double)));
   FG_CUDA(cudaMemcpy(L.d_coef, dbl.data(), dbl.size() * sizeof(double), cudaMemcpyHostToDevice));
   {
     std::vector<double> nodes(L.x);
     nodes.insert(nodes.end(), L.y.begin(), L.y.end());
     nodes.insert(nodes.end(), L.z.begin(), L.z.end());
     void *raw = nullptr;
-    FG_CUDA(cudaMalloc(&raw, nodes.size() * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&raw, nodes.size() * sizeof(double)));
     L.raw.push_back(raw);
     L.d_nodes = static_cast<double *>(raw);
     FG_CUDA(cudaMemcpy(L.d_nodes, nodes.data(), nodes.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
-  FG_CUDA(cudaMalloc(&L.d_int, ints.size() * sizeof(int)));
+  FG_CUDA(fg::dev_alloc(&L.d_int, ints.size() * sizeof(int)));
   FG_CUDA(cudaMemcpy(L.d_int, ints.data(), ints.size() * sizeof(int), cudaMemcpyHostToDevice));
   DevLevel &d = L.dl;
   d = DevLevel{};
@@ -459,7 +553,7 @@ namespace fg {
 template <typename T>
 static cudaError_t run_launch_set_alloc(void **p, const std::vector<T> &v) {
   if (v.empty()) { *p = nullptr; return cudaSuccess; }
-  cudaError_t e = cudaMalloc(p, v.size() * sizeof(T));
+  cudaError_t e = fg::dev_alloc(p, v.size() * sizeof(T));
   if (e != cudaSuccess) return e;
   return cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
@@ -467,15 +561,15 @@ static cudaError_t run_launch_set_alloc(void **p, const std::vector<T> &v) {
 static void free_batch_tables(fg_batch *b) {
   for (int L = 0; L < kMaxLevels; ++L) {
     auto &s = b->ls[L];
-    cudaFree(s.d_levS); cudaFree(s.d_levS_next); cudaFree(s.d_levC);
-    cudaFree(s.d_off_cells); cudaFree(s.d_off_x); cudaFree(s.d_off_y); cudaFree(s.d_off_z);
-    cudaFree(s.d_off_next); cudaFree(s.d_off_quads); cudaFree(s.d_G); cudaFree(s.d_gidx); cudaFree(s.d_gn);
+    fg::dev_free(s.d_levS); fg::dev_free(s.d_levS_next); fg::dev_free(s.d_levC);
+    fg::dev_free(s.d_off_cells); fg::dev_free(s.d_off_x); fg::dev_free(s.d_off_y); fg::dev_free(s.d_off_z);
+    fg::dev_free(s.d_off_next); fg::dev_free(s.d_off_quads); fg::dev_free(s.d_G); fg::dev_free(s.d_gidx); fg::dev_free(s.d_gn);
     s = fg_batch::LevelSet();
   }
-  cudaFree(b->d_lev0); cudaFree(b->d_off0); cudaFree(b->d_offf0); cudaFree(b->d_offq0);
-  cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
-  cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
-  cudaFree(b->d_norm); cudaFree(b->d_part);
+  fg::dev_free(b->d_lev0); fg::dev_free(b->d_off0); fg::dev_free(b->d_offf0); fg::dev_free(b->d_offq0);
+  fg::dev_free(b->d_rprob); fg::dev_free(b->d_rtgt); fg::dev_free(b->d_rcell); fg::dev_free(b->d_rw);
+  fg::dev_free(b->d_rc0); fg::dev_free(b->d_rd); fg::dev_free(b->d_rf); fg::dev_free(b->d_tmp);
+  fg::dev_free(b->d_norm); fg::dev_free(b->d_part);
   b->d_part = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
@@ -493,9 +587,9 @@ static void free_batch_tables(fg_batch *b) {
 // same problems keeps their sizes): every solve rewrites each vector's
 // interior before reading it, and nothing writes outside it.
 static void free_krylov(fg_batch *b) {
-  for (void *r : b->kraw) cudaFree(r);
+  for (void *r : b->kraw) fg::dev_free(r);
   b->kraw.clear();
-  cudaFree(b->d_kd); cudaFree(b->d_kpart); cudaFree(b->d_kout); cudaFree(b->d_kcoef);
+  fg::dev_free(b->d_kd); fg::dev_free(b->d_kpart); fg::dev_free(b->d_kout); fg::dev_free(b->d_kcoef);
   b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
   b->km = 0;
   b->kbytes = 0;
@@ -572,19 +666,19 @@ static fg_status upload_geometry(fg_batch *b) {
     // all row buffers share one capacity, with room for the row count to
     // grow as a body moves
     const long long cap = n + n / 4 + 64;
-    cudaFree(b->d_rprob); cudaFree(b->d_rtgt); cudaFree(b->d_rcell); cudaFree(b->d_rw);
-    cudaFree(b->d_rc0); cudaFree(b->d_rd); cudaFree(b->d_rf); cudaFree(b->d_tmp);
+    fg::dev_free(b->d_rprob); fg::dev_free(b->d_rtgt); fg::dev_free(b->d_rcell); fg::dev_free(b->d_rw);
+    fg::dev_free(b->d_rc0); fg::dev_free(b->d_rd); fg::dev_free(b->d_rf); fg::dev_free(b->d_tmp);
     b->d_rprob = nullptr; b->d_rtgt = nullptr; b->d_rcell = nullptr; b->d_rw = nullptr;
     b->d_rc0 = nullptr; b->d_rd = nullptr; b->d_rf = nullptr; b->d_tmp = nullptr;
     b->row_cap = 0;
-    FG_CUDA(cudaMalloc(&b->d_rprob, cap * sizeof(int)));
-    FG_CUDA(cudaMalloc(&b->d_rtgt, cap * sizeof(long long)));
-    FG_CUDA(cudaMalloc(&b->d_rcell, cap * sizeof(long long)));
-    FG_CUDA(cudaMalloc(&b->d_rw, 8 * cap * sizeof(double)));
-    FG_CUDA(cudaMalloc(&b->d_rc0, cap * sizeof(double)));
-    FG_CUDA(cudaMalloc(&b->d_rd, cap * sizeof(double)));
-    FG_CUDA(cudaMalloc(&b->d_rf, cap * sizeof(float)));
-    FG_CUDA(cudaMalloc(&b->d_tmp, cap * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&b->d_rprob, cap * sizeof(int)));
+    FG_CUDA(fg::dev_alloc(&b->d_rtgt, cap * sizeof(long long)));
+    FG_CUDA(fg::dev_alloc(&b->d_rcell, cap * sizeof(long long)));
+    FG_CUDA(fg::dev_alloc(&b->d_rw, 8 * cap * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&b->d_rc0, cap * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&b->d_rd, cap * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&b->d_rf, cap * sizeof(float)));
+    FG_CUDA(fg::dev_alloc(&b->d_tmp, cap * sizeof(double)));
     b->row_cap = cap;
   }
   if (n > 0) {
@@ -659,9 +753,9 @@ static fg_status build_batch(fg_batch *b) {
       if ((st = build_offsets(bq, &s.d_off_quads, s.quads, s.d_levS)) != FG_OK) return st;
     }
     if (!s.C.empty()) {
-      FG_CUDA(cudaMalloc(&s.d_G, s.C.size() * sizeof(double *)));
-      FG_CUDA(cudaMalloc(&s.d_gidx, s.C.size() * sizeof(int *)));
-      FG_CUDA(cudaMalloc(&s.d_gn, s.C.size() * sizeof(int)));
+      FG_CUDA(fg::dev_alloc(&s.d_G, s.C.size() * sizeof(double *)));
+      FG_CUDA(fg::dev_alloc(&s.d_gidx, s.C.size() * sizeof(int *)));
+      FG_CUDA(fg::dev_alloc(&s.d_gn, s.C.size() * sizeof(int)));
     }
   }
   // level 0 over all problems
@@ -684,8 +778,8 @@ static fg_status build_batch(fg_batch *b) {
   }
   fg_status st;
   if ((st = upload_geometry(b)) != FG_OK) return st;
-  FG_CUDA(cudaMalloc(&b->d_norm, 3 * np * sizeof(double)));
-  FG_CUDA(cudaMalloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_norm, 3 * np * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
   b->h_norm.assign(3 * np, 0.0);
   b->sig = batch_signature(b);
   b->built = true;
@@ -990,7 +1084,7 @@ static fg_status ensure_krylov(fg_batch *b, int bytes) {
     unsigned char *raw[3];
     for (int q = 0; q < 3; ++q) {
       void *r = nullptr;
-      FG_CUDA(cudaMalloc(&r, nel[q] * esz[q]));
+      FG_CUDA(fg::dev_alloc(&r, nel[q] * esz[q]));
       b->kraw.push_back(r);
       FG_CUDA(cudaMemset(r, 0, nel[q] * esz[q]));
       raw[q] = reinterpret_cast<unsigned char *>(r) + kFieldPad * esz[q];
@@ -1005,9 +1099,9 @@ static fg_status ensure_krylov(fg_batch *b, int bytes) {
   FG_CUDA(run_launch_set_alloc((void **)&b->d_kd, kd));
   b->h_kd = kd;
   const int nblk = std::max(1, std::max(b->all0.blocks, b->flat0.blocks));
-  FG_CUDA(cudaMalloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * nblk * sizeof(double)));
-  FG_CUDA(cudaMalloc(&b->d_kout, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
-  FG_CUDA(cudaMalloc(&b->d_kcoef, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * nblk * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_kout, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_kcoef, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
   b->h_kout.assign((size_t)np * (KR_MAXV + 2), 0.0);
   b->h_kcoef.assign((size_t)np * (KR_MAXV + 2), 0.0);
   b->km = m;
@@ -1403,16 +1497,16 @@ static void install_rows(fg_case *c) {
 static fg_status build_levels(fg_case *c) {
   cudaStream_t s = c->stream;
   const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
-  if (!c->d_refmask) FG_CUDA(cudaMalloc(&c->d_refmask, 2 * nref));
+  if (!c->d_refmask) FG_CUDA(fg::dev_alloc(&c->d_refmask, 2 * nref));
   FG_CUDA(cudaMemcpyAsync(c->d_refmask, c->iblank.data(), nref, cudaMemcpyHostToDevice, s));
   FG_CUDA(cudaMemcpyAsync(c->d_refmask + nref, c->ghost.data(), nref, cudaMemcpyHostToDevice, s));
   const int nr = (int)c->rows.tgt.size();
   if ((size_t)nr > c->rowtgt_cap) {
-    cudaFree(c->d_rowtgt);
+    fg::dev_free(c->d_rowtgt);
     c->d_rowtgt = nullptr;
     c->rowtgt_cap = 0;
     const size_t cap = (size_t)nr + nr / 4 + 64;
-    FG_CUDA(cudaMalloc(&c->d_rowtgt, cap * sizeof(long long)));
+    FG_CUDA(fg::dev_alloc(&c->d_rowtgt, cap * sizeof(long long)));
     c->rowtgt_cap = cap;
   }
   if (nr > 0)
@@ -1456,19 +1550,19 @@ static fg_status prepare(fg_case *c) {
   // grow-only: a moving body changes the coarsest size a little per step
   if (!c->G.empty()) {
     if (c->G.size() > c->G_cap) {
-      cudaFree(c->d_G);
+      fg::dev_free(c->d_G);
       c->d_G = nullptr;
       c->G_cap = 0;
-      FG_CUDA(cudaMalloc(&c->d_G, c->G.size() * sizeof(double)));
+      FG_CUDA(fg::dev_alloc(&c->d_G, c->G.size() * sizeof(double)));
       c->G_cap = c->G.size();
     }
     FG_CUDA(cudaMemcpy(c->d_G, c->G.data(), c->G.size() * sizeof(double), cudaMemcpyHostToDevice));
     std::vector<int> gi(c->gidx.begin(), c->gidx.end());
     if (gi.size() > c->gidx_cap) {
-      cudaFree(c->d_gidx);
+      fg::dev_free(c->d_gidx);
       c->d_gidx = nullptr;
       c->gidx_cap = 0;
-      FG_CUDA(cudaMalloc(&c->d_gidx, gi.size() * sizeof(int)));
+      FG_CUDA(fg::dev_alloc(&c->d_gidx, gi.size() * sizeof(int)));
       c->gidx_cap = gi.size();
     }
     FG_CUDA(cudaMemcpy(c->d_gidx, gi.data(), gi.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1574,9 +1668,9 @@ fg_status fg_case_create(int nx, int ny, int nz, const double *xn, const double 
   if (st != FG_OK) { fg_case_destroy(c); return st; }
   cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   const size_t nref = (size_t)(nx + 2) * (ny + 2) * (nz + 2);
-  if (cudaMalloc(&c->d_pin, nref * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->d_fin, nref * sizeof(double)) != cudaSuccess ||
-      cudaMalloc(&c->d_gauge, sizeof(double)) != cudaSuccess) {
+  if (fg::dev_alloc(&c->d_pin, nref * sizeof(double)) != cudaSuccess ||
+      fg::dev_alloc(&c->d_fin, nref * sizeof(double)) != cudaSuccess ||
+      fg::dev_alloc(&c->d_gauge, sizeof(double)) != cudaSuccess) {
     fg_case_destroy(c);
     return FG_ALLOC_FAIL;
   }
@@ -1591,13 +1685,13 @@ fg_status fg_case_destroy(fg_case *c) {
   if (c->solo) { fg_batch_destroy(c->solo); c->solo = nullptr; }
   for (int l = 0; l < c->nlev; ++l) {
     HLevel &L = c->lev[l];
-    cudaFree(L.d_coef); cudaFree(L.d_int);
-    for (void *r : L.raw) cudaFree(r);
+    fg::dev_free(L.d_coef); fg::dev_free(L.d_int);
+    for (void *r : L.raw) fg::dev_free(r);
     L.raw.clear();
   }
-  cudaFree(c->d_G); cudaFree(c->d_gidx); cudaFree(c->d_pin); cudaFree(c->d_fin);
-  cudaFree(c->d_refmask); cudaFree(c->d_rowtgt);
-  cudaFree(c->d_gauge);
+  fg::dev_free(c->d_G); fg::dev_free(c->d_gidx); fg::dev_free(c->d_pin); fg::dev_free(c->d_fin);
+  fg::dev_free(c->d_refmask); fg::dev_free(c->d_rowtgt);
+  fg::dev_free(c->d_gauge);
   if (c->geom) geom_free(*c->geom);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;

@@ -22,12 +22,12 @@ namespace fg {
 
 void geom_free(Geom &g) {
   for (auto &b : g.bodies) {
-    cudaFree(b.d_xyz); cudaFree(b.d_en); cudaFree(b.d_vn); cudaFree(b.d_tri);
-    cudaFree(b.d_v2t_off); cudaFree(b.d_v2t);
+    fg::dev_free(b.d_xyz); fg::dev_free(b.d_en); fg::dev_free(b.d_vn); fg::dev_free(b.d_tri);
+    fg::dev_free(b.d_v2t_off); fg::dev_free(b.d_v2t);
   }
   g.bodies.clear();
-  cudaFree(g.d_iblank); cudaFree(g.d_ghost); cudaFree(g.d_dead); cudaFree(g.d_body);
-  cudaFree(g.d_band); cudaFree(g.d_tmp); cudaFree(g.d_xc);
+  fg::dev_free(g.d_iblank); fg::dev_free(g.d_ghost); fg::dev_free(g.d_dead); fg::dev_free(g.d_body);
+  fg::dev_free(g.d_band); fg::dev_free(g.d_tmp); fg::dev_free(g.d_xc);
   g.d_iblank = g.d_ghost = g.d_dead = g.d_body = g.d_band = g.d_tmp = nullptr;
   g.d_xc = nullptr;
   for (DevScratch *b : {&g.cub_tmp, &g.sel_out, &g.sel_count, &g.cells, &g.glist, &g.dlist, &g.alpha,
@@ -818,7 +818,7 @@ static fg_status geom_grid(fg_case *c, geo::Grid &g) {
       all.insert(all.end(), dx.begin(), dx.end());
       all.insert(all.end(), dxc.begin(), dxc.end());
     }
-    FG_CUDA(cudaMalloc(&G.d_xc, all.size() * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&G.d_xc, all.size() * sizeof(double)));
     FG_CUDA(cudaMemcpy(G.d_xc, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   const double *p = G.d_xc;
@@ -869,9 +869,9 @@ static fg_status upload_body(DevBody &B) {
     soa[v] = B.xyz[3 * v]; soa[B.nvert + v] = B.xyz[3 * v + 1]; soa[2 * B.nvert + v] = B.xyz[3 * v + 2];
   }
   if (!B.d_xyz) {
-    FG_CUDA(cudaMalloc(&B.d_xyz, soa.size() * sizeof(double)));
-    FG_CUDA(cudaMalloc(&B.d_en, en.size() * sizeof(double)));
-    FG_CUDA(cudaMalloc(&B.d_vn, vn.size() * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&B.d_xyz, soa.size() * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&B.d_en, en.size() * sizeof(double)));
+    FG_CUDA(fg::dev_alloc(&B.d_vn, vn.size() * sizeof(double)));
   }
   FG_CUDA(cudaMemcpy(B.d_xyz, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice));
   FG_CUDA(cudaMemcpy(B.d_en, en.data(), en.size() * sizeof(double), cudaMemcpyHostToDevice));
@@ -893,12 +893,12 @@ static fg_status ensure_fields(fg_case *c) {
   Geom &G = *c->geom;
   const size_t n = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
   if (!G.d_iblank) {
-    FG_CUDA(cudaMalloc(&G.d_iblank, n));
-    FG_CUDA(cudaMalloc(&G.d_ghost, n));
-    FG_CUDA(cudaMalloc(&G.d_dead, n));
-    FG_CUDA(cudaMalloc(&G.d_body, n));
-    FG_CUDA(cudaMalloc(&G.d_band, n));
-    FG_CUDA(cudaMalloc(&G.d_tmp, 4 * n));  // iblankTemp, smoothing buffers
+    FG_CUDA(fg::dev_alloc(&G.d_iblank, n));
+    FG_CUDA(fg::dev_alloc(&G.d_ghost, n));
+    FG_CUDA(fg::dev_alloc(&G.d_dead, n));
+    FG_CUDA(fg::dev_alloc(&G.d_body, n));
+    FG_CUDA(fg::dev_alloc(&G.d_band, n));
+    FG_CUDA(fg::dev_alloc(&G.d_tmp, 4 * n));  // iblankTemp, smoothing buffers
     FG_CUDA(cudaMemset(G.d_iblank, 0, n));
   }
   return FG_OK;
@@ -962,11 +962,11 @@ fg_status fg_case_add_body(fg_case *c, int nvert, int ntri, const double *xyz, c
     if (b != a) v2t[off[b] + cnt[b]++] = m;
     if (d != a && d != b) v2t[off[d] + cnt[d]++] = m;
   }
-  FG_CUDA(cudaMalloc(&B.d_tri, 3 * (size_t)ntri * sizeof(int32_t)));
+  FG_CUDA(fg::dev_alloc(&B.d_tri, 3 * (size_t)ntri * sizeof(int32_t)));
   FG_CUDA(cudaMemcpy(B.d_tri, tri, 3 * (size_t)ntri * sizeof(int32_t), cudaMemcpyHostToDevice));
-  FG_CUDA(cudaMalloc(&B.d_v2t_off, (nvert + 1) * sizeof(int32_t)));
+  FG_CUDA(fg::dev_alloc(&B.d_v2t_off, (nvert + 1) * sizeof(int32_t)));
   FG_CUDA(cudaMemcpy(B.d_v2t_off, off.data(), (nvert + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
-  FG_CUDA(cudaMalloc(&B.d_v2t, std::max<size_t>(1, v2t.size()) * sizeof(int32_t)));
+  FG_CUDA(fg::dev_alloc(&B.d_v2t, std::max<size_t>(1, v2t.size()) * sizeof(int32_t)));
   FG_CUDA(cudaMemcpy(B.d_v2t, v2t.data(), v2t.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   fg_status st = upload_body(B);
   if (st != FG_OK) return st;

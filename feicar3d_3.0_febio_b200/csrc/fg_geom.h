@@ -28,15 +28,15 @@ struct DevScratch {
   size_t cap = 0;
   cudaError_t ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
-    cudaFree(p);
+    fg::dev_free(p);
     p = nullptr;
     cap = 0;
-    const cudaError_t e = cudaMalloc(&p, bytes > 0 ? bytes : 1);
+    const cudaError_t e = fg::dev_alloc(&p, bytes > 0 ? bytes : 1);
     if (e == cudaSuccess) cap = bytes;
     return e;
   }
   template <class T> T *as() const { return static_cast<T *>(p); }
-  void release() { cudaFree(p); p = nullptr; cap = 0; }
+  void release() { fg::dev_free(p); p = nullptr; cap = 0; }
 };
 
 // device outputs of one row list (ghost or dead) of the tagging

@@ -135,6 +135,19 @@ struct Launch {
 void set_last_error(const char *msg, const char *file, int line);
 const char *last_error_msg();
 
+// Device memory of the library, through a per-process cache: a freed block
+// waits (after a device synchronisation, as cudaFree's own) for the next
+// request of its rounded size on its device, so cases that live one
+// request, and buffers that grow, map and unmap no memory in steady state.
+// The cache holds at most a few GB per device and is emptied when an
+// allocation fails.
+cudaError_t dev_alloc_raw(void **p, size_t bytes);
+void dev_free(void *p);
+template <class T>
+inline cudaError_t dev_alloc(T **p, size_t bytes) {
+  return dev_alloc_raw(reinterpret_cast<void **>(p), bytes);
+}
+
 // kernels launched by this process (every launch site adds its count)
 void note_launches(long long n);
 long long launches_so_far();
