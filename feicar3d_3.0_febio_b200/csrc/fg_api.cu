@@ -490,6 +490,13 @@ struct fg_batch {
     int *d_gn = nullptr;
     int maxgn = 0;
   } ls[kMaxLevels];
+  // the small levels (k_small_cycle): from level small_L down, one block per
+  // problem whose hierarchy reaches small_L (small_L == maxdepth: none)
+  int small_L = 0;
+  int n_small = 0, small_maxgn = 0;
+  std::vector<SmallProb> h_small;
+  SmallProb *d_small = nullptr;
+  DevLevel *d_small_levs = nullptr;
   // level 0 over all problems
   DevLevel *d_lev0 = nullptr;
   int *d_off0 = nullptr, *d_offf0 = nullptr, *d_offq0 = nullptr;
@@ -567,6 +574,9 @@ static void free_batch_tables(fg_batch *b) {
     s = fg_batch::LevelSet();
   }
   fg::dev_free(b->d_lev0); fg::dev_free(b->d_off0); fg::dev_free(b->d_offf0); fg::dev_free(b->d_offq0);
+  fg::dev_free(b->d_small); fg::dev_free(b->d_small_levs);
+  b->d_small = nullptr; b->d_small_levs = nullptr; b->n_small = 0; b->small_maxgn = 0;
+  b->h_small.clear();
   fg::dev_free(b->d_rprob); fg::dev_free(b->d_rtgt); fg::dev_free(b->d_rcell); fg::dev_free(b->d_rw);
   fg::dev_free(b->d_rc0); fg::dev_free(b->d_rd); fg::dev_free(b->d_rf); fg::dev_free(b->d_tmp);
   fg::dev_free(b->d_norm); fg::dev_free(b->d_part);
@@ -646,6 +656,20 @@ static fg_status upload_geometry(fg_batch *b) {
     FG_CUDA(cudaMemcpy(s.d_G, gp.data(), gp.size() * sizeof(double *), cudaMemcpyHostToDevice));
     FG_CUDA(cudaMemcpy(s.d_gidx, gi.data(), gi.size() * sizeof(int *), cudaMemcpyHostToDevice));
     FG_CUDA(cudaMemcpy(s.d_gn, gn.data(), gn.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (b->n_small > 0) {
+    b->small_maxgn = 0;
+    int q = 0;
+    for (const fg_case *c : b->cases) {
+      if (c->nlev <= b->small_L) continue;
+      SmallProb &sp = b->h_small[q++];
+      sp.G = c->d_G;
+      sp.gidx = c->d_gidx;
+      sp.gn = (int)c->gidx.size();
+      b->small_maxgn = std::max(b->small_maxgn, sp.gn);
+    }
+    FG_CUDA(cudaMemcpy(b->d_small, b->h_small.data(), b->h_small.size() * sizeof(SmallProb),
+                       cudaMemcpyHostToDevice));
   }
   // rows (dead rows then ghost rows of each problem, problems in order)
   std::vector<int> prob;
@@ -758,6 +782,33 @@ static fg_status build_batch(fg_batch *b) {
       FG_CUDA(fg::dev_alloc(&s.d_gn, s.C.size() * sizeof(int)));
     }
   }
+  // the small levels: the first level below level 0 from which every level
+  // of every problem that reaches it fits one block's sweeps
+  b->small_L = b->maxdepth;
+  for (int L = 1; L < b->maxdepth; ++L) {
+    bool fits = true;
+    for (auto *c : b->cases)
+      for (int l = L; l < c->nlev && fits; ++l) {
+        const HLevel &H = c->lev[l];
+        fits = (long long)H.nx * H.ny * H.nz <= SC_MAXCELLS && H.nx <= SC_MAXN && H.ny <= SC_MAXN &&
+               H.nz <= SC_MAXN;
+      }
+    if (fits) { b->small_L = L; break; }
+  }
+  if (b->small_L < b->maxdepth) {
+    std::vector<DevLevel> lv;
+    for (auto *c : b->cases) {
+      if (c->nlev <= b->small_L) continue;
+      SmallProb q{};
+      q.l0 = (int)lv.size();
+      q.nl = c->nlev - b->small_L;
+      for (int l = b->small_L; l < c->nlev; ++l) lv.push_back(c->lev[l].dl);
+      b->h_small.push_back(q);
+    }
+    FG_CUDA(run_launch_set_alloc((void **)&b->d_small_levs, lv));
+    FG_CUDA(fg::dev_alloc(&b->d_small, b->h_small.size() * sizeof(SmallProb)));
+    b->n_small = (int)b->h_small.size();
+  }
   // level 0 over all problems
   {
     std::vector<DevLevel> v0;
@@ -866,7 +917,8 @@ template <typename T>
 static fg_status vcycle(fg_batch *b, cudaStream_t s) {
   const int corr = (b->krylov || sizeof(T) == 4) ? 1 : 0;
   fg_status st;
-  for (int L = 0; L < b->maxdepth; ++L) {
+  const int Ls = std::min(b->maxdepth, b->small_L);  // levels from Ls down: one block per problem
+  for (int L = 0; L < Ls; ++L) {
     auto &ls = b->ls[L];
     if (!ls.S.empty()) {
       for (int q = 0; q < b->cfg.nu1; ++q)
@@ -883,7 +935,13 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
       prof_end(b, e0, FG_PROF_COARSEST, 0.0, s);
     }
   }
-  for (int L = b->maxdepth - 2; L >= 0; --L) {
+  if (Ls < b->maxdepth) {
+    const size_t e0 = prof_begin(b, s);
+    FG_K(k::small_cycle<T>(b->n_small, b->d_small, b->d_small_levs, b->small_maxgn, b->cfg.nu1,
+                           b->cfg.nu2, b->cfg.omega, s));
+    prof_end(b, e0, FG_PROF_LINE_COARSE, 0.0, s);
+  }
+  for (int L = std::min(b->maxdepth - 2, Ls - 1); L >= 0; --L) {
     auto &ls = b->ls[L];
     if (ls.S.empty()) continue;
     size_t e0 = prof_begin(b, s);
@@ -908,6 +966,7 @@ static std::vector<char> vcycle_params(const fg_batch *b) {
   put(&b->rows, sizeof(DevRows));
   put(&b->d_tmp, sizeof(b->d_tmp));
   for (int L = 0; L < b->maxdepth; ++L) put(&b->ls[L].maxgn, sizeof(int));
+  put(&b->small_maxgn, sizeof(int));
   return v;
 }
 

@@ -176,6 +176,19 @@ struct KDesc {
 };
 constexpr int KR_MAXV = 16;  // most vectors one dot-product pass reads
 
+// A problem's small levels that one block cycles through (k_small_cycle):
+// levels [l0, l0 + nl) of a packed DevLevel table, the last one the
+// coarsest, with its generalised inverse G (gn x gn) over the cells gidx.
+constexpr int SC_THREADS = 256;           // threads of the block
+constexpr int SC_MAXN = 32;               // longest line of such a level
+constexpr long long SC_MAXCELLS = 2048;   // most cells of any such level
+struct SmallProb {
+  int l0, nl;
+  const double *G;
+  const int *gidx;
+  int gn;
+};
+
 // kernel launchers (fg_mg.cu)
 namespace k {
 // blocks needed by one problem's level for each kernel family
@@ -206,6 +219,10 @@ template <typename T>
 cudaError_t residual_q(const Launch &quads, cudaStream_t s);
 template <typename T>
 cudaError_t zero_x(const Launch &L, cudaStream_t s);
+// the V-cycle of each problem's small levels, one block per problem
+template <typename T>
+cudaError_t small_cycle(int nprob, const SmallProb *probs, const DevLevel *levs, int maxgn, int nu1,
+                        int nu2, double omega, cudaStream_t s);
 template <typename T>
 cudaError_t rows_relax(const DevRows &R, const DevLevel *lev0, int correction_form,
                        double *tmp, cudaStream_t s);

@@ -1733,6 +1733,27 @@ cudaError_t residual_q(const Launch &Lq, cudaStream_t s) {
 // ------------------------------------------------------- restriction
 // coarse rhs = volume-weighted mean of the children's residuals on active
 // coarse cells (the sum of the children's finite-volume equations)
+// the restriction into coarse cell (I,J,K)
+template <typename T>
+__device__ __forceinline__ void restrict_cell(const DevLevel &C, const DevLevel &F, int I, int J, int K) {
+  auto rc = PrecOf<T>::rhs(C);
+  auto rf = PrecOf<T>::res(F);
+  const long long id = I + C.sy * J + C.sz * K;
+  if (!(C.mask[id] & 64)) { rc[id] = T(0); return; }
+  double s = 0.0, v = 0.0;
+  for (int k = C.clz[K]; k <= C.chz[K]; ++k)
+    for (int j = C.cly[J]; j <= C.chy[J]; ++j) {
+      const double wyz = F.wy[j] * F.wz[k];
+      const long long rb = F.sy * j + F.sz * k;
+      for (int i = C.clx[I]; i <= C.chx[I]; ++i) {
+        const double w = F.wx[i] * wyz;
+        s += w * (double)rf[rb + i];
+        v += w;
+      }
+    }
+  rc[id] = (T)(s / v);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
 k_restrict(const int *off, int nent, const DevLevel *coarse, const DevLevel *fine) {
@@ -1740,26 +1761,9 @@ k_restrict(const int *off, int nent, const DevLevel *coarse, const DevLevel *fin
   const DevLevel &C = coarse[p];
   const DevLevel &F = fine[p];
   const int lb = blockIdx.x - off[p];
-  auto rc = PrecOf<T>::rhs(C);
-  auto rf = PrecOf<T>::res(F);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(C, lb, rr);
-    if (!c.ok) continue;
-    const int I = c.i, J = c.j, K = c.k;
-    const long long id = I + C.sy * J + C.sz * K;
-    if (!(C.mask[id] & 64)) { rc[id] = T(0); continue; }
-    double s = 0.0, v = 0.0;
-    for (int k = C.clz[K]; k <= C.chz[K]; ++k)
-      for (int j = C.cly[J]; j <= C.chy[J]; ++j) {
-        const double wyz = F.wy[j] * F.wz[k];
-        const long long rb = F.sy * j + F.sz * k;
-        for (int i = C.clx[I]; i <= C.chx[I]; ++i) {
-          const double w = F.wx[i] * wyz;
-          s += w * (double)rf[rb + i];
-          v += w;
-        }
-      }
-    rc[id] = (T)(s / v);
+    if (c.ok) restrict_cell<T>(C, F, c.i, c.j, c.k);
   }
 }
 
@@ -1774,6 +1778,30 @@ cudaError_t restrict_to(const Launch &Lc, const DevLevel *fine, cudaStream_t s) 
 // ------------------------------------------------------ prolongation
 // fine x += trilinear interpolation of the coarse correction at the fine
 // cell centre, over the active coarse corners only (renormalised)
+// the prolongation into fine cell (i,j,k)
+template <typename T>
+__device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &C, int i, int j, int k) {
+  auto xc = PrecOf<T>::x(C);
+  auto x = PrecOf<T>::x(F);
+  const long long id = i + F.sy * j + F.sz * k;
+  if (!(F.mask[id] & 128)) return;
+  const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
+  const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
+  const double wx1 = F.pwx[i], wy1 = F.pwy[j], wz1 = F.pwz[k];
+  double s = 0.0, ws = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
+    const double w = ((q & 1) ? wx1 : 1.0 - wx1) * ((q & 2) ? wy1 : 1.0 - wy1) *
+                     ((q & 4) ? wz1 : 1.0 - wz1);
+    const long long cid = ci + C.sy * cj + C.sz * ck;
+    const double act = (C.mask[cid] & 64) ? w : 0.0;
+    s += act * (double)xc[cid];
+    ws += act;
+  }
+  if (ws > 1e-12) x[id] = x[id] + (T)(s / ws);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
 k_prolong(const int *off, int nent, const DevLevel *fine, const DevLevel *coarse) {
@@ -1781,29 +1809,9 @@ k_prolong(const int *off, int nent, const DevLevel *fine, const DevLevel *coarse
   const DevLevel &F = fine[p];
   const DevLevel &C = coarse[p];
   const int lb = blockIdx.x - off[p];
-  auto xc = PrecOf<T>::x(C);
-  auto x = PrecOf<T>::x(F);
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
     const CellIdx c = cell_of(F, lb, rr);
-    if (!c.ok) continue;
-    const int i = c.i, j = c.j, k = c.k;
-    const long long id = i + F.sy * j + F.sz * k;
-    if (!(F.mask[id] & 128)) continue;
-    const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
-    const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
-    const double wx1 = F.pwx[i], wy1 = F.pwy[j], wz1 = F.pwz[k];
-    double s = 0.0, ws = 0.0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
-      const double w = ((q & 1) ? wx1 : 1.0 - wx1) * ((q & 2) ? wy1 : 1.0 - wy1) *
-                       ((q & 4) ? wz1 : 1.0 - wz1);
-      const long long cid = ci + C.sy * cj + C.sz * ck;
-      const double act = (C.mask[cid] & 64) ? w : 0.0;
-      s += act * (double)xc[cid];
-      ws += act;
-    }
-    if (ws > 1e-12) x[id] = x[id] + (T)(s / ws);
+    if (c.ok) prolong_cell<T>(F, C, c.i, c.j, c.k);
   }
 }
 
@@ -1962,6 +1970,158 @@ cudaError_t coarsest_solve(int nprob, const DevLevel *lev, const double *const *
   note_launches(1);
   return cudaGetLastError();
 }
+
+// ------------------------------------------------ small levels, one block
+// The V-cycle from the first level whose every line has at most SC_MAXN
+// cells and every level at most SC_MAXCELLS cells down to the coarsest, as
+// one block per problem.  On such levels each launch of the level-by-level
+// cycle (six line sweeps per smoothing step, residual, restriction,
+// prolongation, coarsest solve) is a few microseconds of fixed cost for a
+// few hundred cells; here they are phases of one kernel separated by
+// __syncthreads, on data that stays in the SM's L1.  The line sweeps keep
+// the line kernels' colours ((transverse index sum) & 1), rows, held rows,
+// couplings and omega, one line per thread solved by the Thomas algorithm;
+// residual, restriction, prolongation and coarsest solve use the
+// arithmetic of their kernels.
+template <typename T>
+__device__ void sc_sweep(const DevLevel &L, int axis, int color, T omega) {
+  const int n = axis == 0 ? L.nx : axis == 1 ? L.ny : L.nz;
+  const int n1 = axis == 0 ? L.ny : L.nx;  // first transverse extent
+  const int n2 = axis == 2 ? L.ny : L.nz;  // second transverse extent
+  const long long ls = axis == 0 ? 1 : axis == 1 ? L.sy : L.sz;
+  auto x = PrecOf<T>::x(L);
+  auto rhs = PrecOf<T>::rhs(L);
+  auto am_ = axis == 0 ? L.amx : axis == 1 ? L.amy : L.amz;
+  auto ap_ = axis == 0 ? L.apx : axis == 1 ? L.apy : L.apz;
+  for (int line = threadIdx.x; line < n1 * n2; line += blockDim.x) {
+    const int a = 1 + line % n1, b = 1 + line / n1;  // transverse indices
+    if (((a + b) & 1) != color) continue;
+    const int i = axis == 0 ? 1 : a, j = axis == 0 ? a : axis == 1 ? 1 : b, k = axis == 2 ? 1 : b;
+    const LineCoef lc = line_coef(L, axis, i, j, k);
+    const bool iso_line = lc.tdir == 0.0 && !lc.dirm && !lc.dirp;
+    const long long base = (long long)i + L.sy * j + L.sz * k - ls;  // row r at base + ls (r + 1)
+    T cpa[SC_MAXN], dpa[SC_MAXN];
+    T cprev = T(0), dprev = T(0);
+    for (int r = 0; r < n; ++r) {
+      const long long id = base + ls * (r + 1);
+      const uint8_t m8 = L.mask[id];
+      T aa = T(0), bb = T(1), cc = T(0), dd;
+      const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+      if (held) {
+        dd = x[id];
+      } else {
+        T acc = rhs[id];
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if ((m8 >> lc.qt[t]) & 1) acc -= (T)lc.tq[t] * x[id + lc.to[t]];
+        dd = acc;
+        row_coef<T>(m8, r, n, am_[1 + r], ap_[1 + r], lc, aa, bb, cc);
+      }
+      const T den = bb - aa * cprev;
+      cprev = cc / den;
+      dprev = (dd - aa * dprev) / den;
+      cpa[r] = cprev;
+      dpa[r] = dprev;
+    }
+    T xn = T(0);
+    for (int r = n - 1; r >= 0; --r) {
+      xn = dpa[r] - cpa[r] * xn;
+      const long long id = base + ls * (r + 1);
+      T v = xn;
+      if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+      x[id] = v;
+    }
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void sc_smooth(const DevLevel &L, int nu, T omega) {
+  for (int s_ = 0; s_ < nu; ++s_)
+    for (int axis = 0; axis < 3; ++axis)
+      for (int color = 0; color < 2; ++color) sc_sweep<T>(L, axis, color, omega);
+}
+
+// residual of fine level F restricted into coarse level C, coarse x = 0
+template <typename T>
+__device__ void sc_down(const DevLevel &F, const DevLevel &C) {
+  auto x = PrecOf<T>::x(F);
+  auto rhs = PrecOf<T>::rhs(F);
+  auto res = PrecOf<T>::res(F);
+  const int nf = F.nx * F.ny * F.nz;
+  for (int c = threadIdx.x; c < nf; c += blockDim.x) {
+    const int i = 1 + c % F.nx, j = 1 + (c / F.nx) % F.ny, k = 1 + c / (F.nx * F.ny);
+    const long long id = i + F.sy * j + F.sz * k;
+    const uint8_t mk = F.mask[id];
+    T r = T(0);
+    if (mk & 64) r = rhs[id] - apply_row<T>(F, id, i, j, k, mk, x);
+    res[id] = r;
+  }
+  __syncthreads();
+  auto xc = PrecOf<T>::x(C);
+  const int ncc = C.nx * C.ny * C.nz;
+  for (int c = threadIdx.x; c < ncc; c += blockDim.x) {
+    const int I = 1 + c % C.nx, J = 1 + (c / C.nx) % C.ny, K = 1 + c / (C.nx * C.ny);
+    restrict_cell<T>(C, F, I, J, K);
+    xc[I + C.sy * J + C.sz * K] = T(0);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void sc_up(const DevLevel &F, const DevLevel &C) {
+  const int nf = F.nx * F.ny * F.nz;
+  for (int c = threadIdx.x; c < nf; c += blockDim.x) {
+    const int i = 1 + c % F.nx, j = 1 + (c / F.nx) % F.ny, k = 1 + c / (F.nx * F.ny);
+    prolong_cell<T>(F, C, i, j, k);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SC_THREADS)
+k_small_cycle(const SmallProb *probs, const DevLevel *levs, int nu1, int nu2, T omega) {
+  extern __shared__ double sc_sr[];  // coarsest right-hand side (gn values)
+  const SmallProb P = probs[blockIdx.x];
+  for (int l = 0; l < P.nl - 1; ++l) {
+    sc_smooth<T>(levs[P.l0 + l], nu1, omega);
+    sc_down<T>(levs[P.l0 + l], levs[P.l0 + l + 1]);
+  }
+  {
+    const DevLevel &L = levs[P.l0 + P.nl - 1];
+    auto rhs = PrecOf<T>::rhs(L);
+    auto x = PrecOf<T>::x(L);
+    for (int c = threadIdx.x; c < P.gn; c += blockDim.x) sc_sr[c] = (double)rhs[P.gidx[c]];
+    __syncthreads();
+    for (int r = threadIdx.x; r < P.gn; r += blockDim.x) {
+      double acc = 0.0;
+      const double *gr = P.G + (size_t)r * P.gn;
+      for (int c = 0; c < P.gn; ++c) acc += gr[c] * sc_sr[c];
+      x[P.gidx[r]] = (T)acc;
+    }
+    __syncthreads();
+  }
+  for (int l = P.nl - 2; l >= 0; --l) {
+    sc_up<T>(levs[P.l0 + l], levs[P.l0 + l + 1]);
+    sc_smooth<T>(levs[P.l0 + l], nu2, omega);
+  }
+}
+
+template <typename T>
+cudaError_t small_cycle(int nprob, const SmallProb *probs, const DevLevel *levs, int maxgn, int nu1,
+                        int nu2, double omega, cudaStream_t s) {
+  if (nprob <= 0) return cudaSuccess;
+  const size_t sm = (size_t)std::max(1, maxgn) * sizeof(double);
+  if (sm > 48 * 1024)
+    cudaFuncSetAttribute(k_small_cycle<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_small_cycle<T><<<nprob, SC_THREADS, sm, s>>>(probs, levs, nu1, nu2, (T)omega);
+  note_launches(1);
+  return cudaGetLastError();
+}
+template cudaError_t small_cycle<float>(int, const SmallProb *, const DevLevel *, int, int, int, double,
+                                        cudaStream_t);
+template cudaError_t small_cycle<double>(int, const SmallProb *, const DevLevel *, int, int, int, double,
+                                         cudaStream_t);
 
 // ----------------------------------------- layout conversion (boundary)
 // reference field (0:nx+1 nodes) <-> device level-0 layout, nx ny nz cells
