@@ -45,6 +45,20 @@ PinnedPool &pinned_pool() {
 constexpr size_t kPinnedCacheMax = size_t(2) << 30;
 }  // namespace
 
+void host_copy(void *dst, const void *src, size_t bytes) {
+  constexpr size_t kChunk = size_t(1) << 20;
+  if (bytes < 2 * kChunk) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  const long long nch = (long long)((bytes + kChunk - 1) / kChunk);
+#pragma omp parallel for schedule(static)
+  for (long long q = 0; q < nch; ++q) {
+    const size_t o = (size_t)q * kChunk;
+    memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, std::min(kChunk, bytes - o));
+  }
+}
+
 // ------------------------------------------------------ device block cache
 namespace {
 struct DevCache {

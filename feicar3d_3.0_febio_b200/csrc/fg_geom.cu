@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "fg_case.h"
@@ -1029,7 +1030,12 @@ fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank) {
   FG_CUDA(cudaMemcpyAsync(&hw, d_warn, sizeof(int), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaStreamSynchronize(s));
   G.nWarnSide = hw;
-  if (iblank) FG_CUDA(cudaMemcpy(iblank, G.d_iblank, n, cudaMemcpyDeviceToHost));
+  if (iblank) {
+    G.h_stage.resize(std::max(G.h_stage.size(), n));
+    FG_CUDA(cudaMemcpyAsync(G.h_stage.data(), G.d_iblank, n, cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    fg::host_copy(iblank, G.h_stage.data(), n);
+  }
   G.tagged = true;
   return FG_OK;
 }
@@ -1119,13 +1125,6 @@ struct RowBufs {
   }
 };
 
-template <typename T>
-fg_status d2h(const T *d, size_t m, std::vector<T> &h) {
-  h.resize(m);
-  if (m) FG_CUDA(cudaMemcpy(h.data(), d, m * sizeof(T), cudaMemcpyDeviceToHost));
-  return FG_OK;
-}
-
 void list_ijk(const std::vector<int> &l, long long NX, long long NY, std::vector<int32_t> &ijk) {
   ijk.resize(3 * l.size());
   for (size_t r = 0; r < l.size(); ++r) {
@@ -1209,36 +1208,59 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   FG_CUDA(cudaMemcpyAsync(c->ghost.data(), G.d_ghost, n, cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaMemcpyAsync(c->dead.data(), G.d_dead, n, cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaStreamSynchronize(s));
+  // the row lists and row outputs: one landing area, one synchronisation
   std::vector<int> hgl, hdl;
-  if ((st = d2h(glp, (size_t)ng, hgl)) != FG_OK) return st;
-  if ((st = d2h(dlp, (size_t)nd, hdl)) != FG_OK) return st;
   std::vector<int32_t> g_ijk, d_ijk, g_cell, d_cell;
   std::vector<double> g_coefN, d_coefN, d_probe, d_ip;
+  {
+    struct Piece { const void *src; size_t bytes; size_t off; };
+    std::vector<Piece> pieces;
+    size_t tot = 0;
+    auto add = [&](const void *src, size_t bytes) {
+      pieces.push_back({src, bytes, tot});
+      tot += (bytes + 15) & ~size_t(15);
+      return pieces.size() - 1;
+    };
+    const size_t ngs = (size_t)ng, nds = (size_t)nd, I = sizeof(int32_t), D = sizeof(double);
+    const size_t p_gl = add(glp, ngs * I), p_dl = add(dlp, nds * I);
+    const size_t p_gcell = add(gb.o.cell, 3 * ngs * I), p_dcell = add(db.o.cell, 3 * nds * I);
+    const size_t p_gcN = add(gb.cN, 8 * ngs * D), p_dcN = add(db.cN, 8 * nds * D);
+    const size_t p_dprobe = add(db.o.probe, nds * D), p_dip = add(db.o.ip, 3 * nds * D);
+    const size_t p_gcD = add(gb.cD, 8 * ngs * D), p_gbi = add(gb.o.bi, 3 * ngs * D);
+    const size_t p_gip = add(gb.o.ip, 3 * ngs * D), p_gprobe = add(gb.o.probe, ngs * D);
+    const size_t p_alpha = add(alpha, ngs * D), p_gcl = add(gb.o.closest, ngs * I);
+    const size_t p_dcD = add(db.cD, 8 * nds * D), p_dbi = add(db.o.bi, 3 * nds * D);
+    const size_t p_dcl = add(db.o.closest, nds * I);
+    G.h_stage.resize(std::max(G.h_stage.size(), tot));
+    char *h = G.h_stage.data();
+    for (const Piece &q : pieces)
+      if (q.bytes) FG_CUDA(cudaMemcpyAsync(h + q.off, q.src, q.bytes, cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    auto take = [&](size_t pi, auto &v, size_t count) {
+      using E = typename std::remove_reference<decltype(v)>::type::value_type;
+      v.resize(count);
+      if (count) memcpy(v.data(), h + pieces[pi].off, count * sizeof(E));
+    };
+    take(p_gl, hgl, ngs); take(p_dl, hdl, nds);
+    take(p_gcell, g_cell, 3 * ngs); take(p_dcell, d_cell, 3 * nds);
+    take(p_gcN, g_coefN, 8 * ngs); take(p_dcN, d_coefN, 8 * nds);
+    take(p_dprobe, d_probe, nds); take(p_dip, d_ip, 3 * nds);
+    take(p_gcD, G.g_coefD, 8 * ngs); take(p_gbi, G.g_bi, 3 * ngs);
+    take(p_gip, G.g_ip, 3 * ngs); take(p_gprobe, G.g_probe, ngs);
+    take(p_alpha, G.g_alpha, ngs); take(p_gcl, G.g_closest, ngs);
+    take(p_dcD, G.d_coefD, 8 * nds); take(p_dbi, G.d_bi, 3 * nds);
+    take(p_dcl, G.d_closest, nds);
+  }
   list_ijk(hgl, c->nx + 2, c->ny + 2, g_ijk);
   list_ijk(hdl, c->nx + 2, c->ny + 2, d_ijk);
-  if ((st = d2h((const int32_t *)gb.o.cell, 3 * (size_t)ng, g_cell)) != FG_OK) return st;
-  if ((st = d2h((const int32_t *)db.o.cell, 3 * (size_t)nd, d_cell)) != FG_OK) return st;
-  if ((st = d2h((const double *)gb.cN, 8 * (size_t)ng, g_coefN)) != FG_OK) return st;
-  if ((st = d2h((const double *)db.cN, 8 * (size_t)nd, d_coefN)) != FG_OK) return st;
-  if ((st = d2h((const double *)db.o.probe, (size_t)nd, d_probe)) != FG_OK) return st;
-  if ((st = d2h((const double *)db.o.ip, 3 * (size_t)nd, d_ip)) != FG_OK) return st;
-  if ((st = d2h((const double *)gb.cD, 8 * (size_t)ng, G.g_coefD)) != FG_OK) return st;
-  if ((st = d2h((const double *)gb.o.bi, 3 * (size_t)ng, G.g_bi)) != FG_OK) return st;
-  if ((st = d2h((const double *)gb.o.ip, 3 * (size_t)ng, G.g_ip)) != FG_OK) return st;
-  if ((st = d2h((const double *)gb.o.probe, (size_t)ng, G.g_probe)) != FG_OK) return st;
-  if ((st = d2h((const double *)alpha, (size_t)ng, G.g_alpha)) != FG_OK) return st;
-  if ((st = d2h((const int32_t *)gb.o.closest, (size_t)ng, G.g_closest)) != FG_OK) return st;
-  if ((st = d2h((const double *)db.cD, 8 * (size_t)nd, G.d_coefD)) != FG_OK) return st;
-  if ((st = d2h((const double *)db.o.bi, 3 * (size_t)nd, G.d_bi)) != FG_OK) return st;
-  if ((st = d2h((const int32_t *)db.o.closest, (size_t)nd, G.d_closest)) != FG_OK) return st;
   // hand the rows to the solver (same path as caller-supplied geometry,
   // which also marks the dead rows using the fallback)
   st = fg::geometry_rows(c, ng, g_ijk.data(), g_cell.data(), g_coefN.data(), nd, d_ijk.data(),
                          d_cell.data(), d_coefN.data(), d_probe.data(), d_ip.data());
   if (st != FG_OK) return st;
-  if (iblank) memcpy(iblank, c->iblank.data(), n);
-  if (ghostCellMark) memcpy(ghostCellMark, c->ghost.data(), n);
-  if (dead_cell) memcpy(dead_cell, c->dead.data(), n);
+  if (iblank) fg::host_copy(iblank, c->iblank.data(), n);
+  if (ghostCellMark) fg::host_copy(ghostCellMark, c->ghost.data(), n);
+  if (dead_cell) fg::host_copy(dead_cell, c->dead.data(), n);
   if (nGhost) *nGhost = ng;
   if (nDead) *nDead = nd;
   if (flags[2]) return FG_GEOMETRY_DEAD_NO_BODY;

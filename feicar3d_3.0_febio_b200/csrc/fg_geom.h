@@ -62,6 +62,7 @@ struct Geom {
   // lists (host copies after fg_gcm_set_internal_boundary)
   std::vector<double> g_coefD, g_bi, g_ip, g_probe, g_alpha, d_coefD, d_bi, d_probe;
   std::vector<int32_t> g_closest, d_closest;
+  pinned_vector<char> h_stage;  // page-locked landing area of device -> host copies
   bool tagged = false;
 };
 

@@ -141,6 +141,10 @@ const char *last_error_msg();
 // request, and buffers that grow, map and unmap no memory in steady state.
 // The cache holds at most a few GB per device and is emptied when an
 // allocation fails.
+// host memcpy split over the host threads for large copies (the masks
+// handed to the caller: several MB of freshly mapped pages)
+void host_copy(void *dst, const void *src, size_t bytes);
+
 cudaError_t dev_alloc_raw(void **p, size_t bytes);
 void dev_free(void *p);
 template <class T>
