@@ -1778,7 +1778,8 @@ cudaError_t restrict_to(const Launch &Lc, const DevLevel *fine, cudaStream_t s) 
 // ------------------------------------------------------ prolongation
 // fine x += trilinear interpolation of the coarse correction at the fine
 // cell centre, over the active coarse corners only (renormalised)
-// the prolongation into fine cell (i,j,k)
+// the prolongation into fine cell (i,j,k), in the arithmetic of the cycle
+// (FP32 weights and sums in the mixed path: the correction itself is FP32)
 template <typename T>
 __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &C, int i, int j, int k) {
   auto xc = PrecOf<T>::x(C);
@@ -1787,19 +1788,20 @@ __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &
   if (!(F.mask[id] & 128)) return;
   const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
   const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
-  const double wx1 = F.pwx[i], wy1 = F.pwy[j], wz1 = F.pwz[k];
-  double s = 0.0, ws = 0.0;
+  const T wx1 = (T)F.pwx[i], wy1 = (T)F.pwy[j], wz1 = (T)F.pwz[k];
+  const T wx[2] = {T(1) - wx1, wx1};
+  const T wyz[4] = {(T(1) - wy1) * (T(1) - wz1), wy1 * (T(1) - wz1), (T(1) - wy1) * wz1, wy1 * wz1};
+  T s = T(0), ws = T(0);
 #pragma unroll
   for (int q = 0; q < 8; ++q) {
     const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
-    const double w = ((q & 1) ? wx1 : 1.0 - wx1) * ((q & 2) ? wy1 : 1.0 - wy1) *
-                     ((q & 4) ? wz1 : 1.0 - wz1);
+    const T w = wx[q & 1] * wyz[q >> 1];
     const long long cid = ci + C.sy * cj + C.sz * ck;
-    const double act = (C.mask[cid] & 64) ? w : 0.0;
-    s += act * (double)xc[cid];
+    const T act = (C.mask[cid] & 64) ? w : T(0);
+    s += act * xc[cid];
     ws += act;
   }
-  if (ws > 1e-12) x[id] = x[id] + (T)(s / ws);
+  if (ws > T(1e-12)) x[id] = x[id] + s / ws;
 }
 
 template <typename T>
