@@ -181,7 +181,9 @@ void pinned_put(void *p) {
   if (!p) return;
   PinnedPool &P = pinned_pool();
   std::lock_guard<std::mutex> lk(P.mu);
-  const size_t n = P.size_of[p];
+  auto it = P.size_of.find(p);
+  if (it == P.size_of.end()) return;  // not from pinned_get
+  const size_t n = it->second;
   if (P.cached + n > kPinnedCacheMax) {
     P.size_of.erase(p);
     cudaFreeHost(p);
