@@ -742,6 +742,21 @@ PAR_NOTE = ("the line sweeps run as z-slabs, one per thread, as the reference ru
             "faces, z lines in per-slab segments); residual and transfers in parallel loops")
 
 
+def extrapolate_iterations(res0, res):
+    """Residual factor per outer iteration and iterations to RTOL from a zero
+    initial guess (relative residual res0), given the relative residuals
+    after each timed iteration: with two or more, the factor of the
+    iterations after the first (the first one reaches res[0]); with one, that
+    iteration's own factor."""
+    if len(res) > 1:
+        rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if res[0] > 0 else float("nan")
+        n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
+    else:
+        rho = res[0] / res0 if res0 > 0 else float("nan")
+        n_need = max(1.0, math.log(RTOL / res0) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
+    return rho, n_need
+
+
 def cpu_baseline_sample(grid, body, rhs, iters):
     """The CPU restatement of the reference solver on the same grid, body
     and RHS: `iters` outer iterations of solve_poisson (each one MG cycle,
@@ -761,6 +776,7 @@ def cpu_baseline_sample(grid, body, rhs, iters):
     t_setup = time.time() - t0
     p = np.zeros(grid.shape, order="F")
     f = np.asfortranarray(rhs)
+    res0 = oc.relres(p, f)  # untimed: the zero initial guess
     res, secs = [], []
     for _ in range(iters):
         t = time.time()
@@ -769,11 +785,7 @@ def cpu_baseline_sample(grid, body, rhs, iters):
         secs.append(time.time() - t)
         res.append(oc.relres(p, f))
     s_it = float(np.mean(secs))
-    rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if len(res) > 1 and res[0] > 0 else float("nan")
-    if 0.0 < rho < 1.0:
-        n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho))
-    else:
-        n_need = float("nan")
+    rho, n_need = extrapolate_iterations(res0, res)
     val = 1.0 / (s_it * n_need) if n_need == n_need else None
     O.set_threads(1)
     return {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
@@ -809,6 +821,7 @@ def run_reference(args):
     for _ in range(args.warmup):
         oc.solve_poisson(p, f, params=prm)
     p[...] = 0.0
+    res0 = oc.relres(p, f)  # untimed: the zero initial guess
     res, secs = [], []
     for _ in range(args.steps):
         t = time.time()
@@ -816,8 +829,7 @@ def run_reference(args):
         secs.append(time.time() - t)
         res.append(oc.relres(p, f))
     s_it = float(np.mean(secs))
-    rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if len(res) > 1 and res[0] > 0 else float("nan")
-    n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
+    rho, n_need = extrapolate_iterations(res0, res)
     val = 1.0 / (s_it * n_need) if n_need == n_need else 0.0
     sample = (f"each step one outer iteration (one V-cycle, iterInter=0) of the reference solve_poisson "
               f"restatement on {nthr} threads ({PAR_NOTE}) on the full "
