@@ -40,14 +40,22 @@ PKG_DIR = os.path.join(ROOT, "feicar3d_3.0_febio_b200")
 
 METRIC = "Poisson solves/s & HBM GB/s, mixed vs FP64 MG at 1e-8 resid; p50/p99 latency"
 UNIT = "solves/s"
-RTOL = 1e-8
+# Stopping tolerance (relative residual |f - A p| / |f| over fluid rows).
+# BASELINE's metric quotes 1e-8; on the stretched 512x256x256 workload a
+# 1e-8 residual leaves ~1.7e-7 relative L2 error against the exact discrete
+# solution, and 1e-11 is the tolerance at which both the mixed and the FP64
+# path come within 1e-9 (~2e-10), the accuracy the pressure must reach.  The
+# single-grid workloads run at RTOL_ACCURATE by default and also report
+# 1e-8; the batch, moving-body and serving workloads run at 1e-8.
+RTOL_BASELINE = 1e-8
+RTOL_ACCURATE = 1e-11
+RTOL = RTOL_ACCURATE
 
 # DRAM bytes per finest-level cell of one colour launch of the dominant line
 # class, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
 # 256^3 case, whose y and z lines run the same kernels as the 512x256x256
 # case's (256-row lines, k_yzline_pcr<float, 8, 32, axis>); a launch moves
-# the same bytes per cell, so the figure scales by the cell count
-# (profiles/yzline_pcr_cube256_mixed.md).
+# the same bytes per cell, so the figure scales by the cell count.
 DRAM_BYTES_PER_CELL = {("config1", "mixed", "line_y0"): (170.546 + 33.888) / 16.7772,
                        ("config1", "mixed", "line_z0"): (170.532 + 34.614) / 16.7772}
 
@@ -164,8 +172,8 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ our path
-def build_case(fg, synth, grid, body, precision, dev, geometry_from=None):
-    cfg = fg.default_config(precision=precision, rtol=RTOL, max_cycles=200)
+def build_case(fg, synth, grid, body, precision, dev, geometry_from=None, rtol=None):
+    cfg = fg.default_config(precision=precision, rtol=RTOL if rtol is None else rtol, max_cycles=200)
     c = fg.Case(grid, cfg, device=dev)
     if geometry_from is None:
         c.add_body(body)
@@ -626,6 +634,27 @@ def run_ours(args):
     p_o = d_p.cpu().numpy().transpose(2, 1, 0)
     err_o = relerr(p_o, phi, mask)
 
+    # both paths again at BASELINE's 1e-8 (where the error to the exact
+    # discrete solution is larger than 1e-9 on this workload)
+    at8 = None
+    if RTOL != RTOL_BASELINE:
+        at8 = {}
+        for name, prec in (("mixed", fg.FG_PREC_MIXED), ("fp64", fg.FG_PREC_FP64)):
+            c8, _ = build_case(fg, synth, grid, body, prec, dev, geometry_from=geo, rtol=RTOL_BASELINE)
+            c8.set_stream(stream.cuda_stream)
+            for _ in range(max(1, args.warmup // 2)):
+                timed_device_solves(torch, fg, c8, d_p, d_f, 1, stream)
+            barrier()
+            t8, _, st8 = timed_device_solves(torch, fg, c8, d_p, d_f, args.steps, stream)
+            barrier()
+            t8 = max_over_ranks(t8)
+            p8 = d_p.cpu().numpy().transpose(2, 1, 0)
+            at8[name] = {"value": args.steps * world / (t8 / 1e3), "ms_per_step": t8 / args.steps,
+                         "cycles": st8[-1]["cycles"], "relres": max(s_["relres"] for s_ in st8),
+                         "err_vs_exact": relerr(p8, phi, mask)}
+            c8.close()
+        at8["speedup_mixed_over_fp64"] = at8["mixed"]["value"] / at8["fp64"]["value"]
+
     # end to end through the host-buffer entry point (pinned host memory):
     # every step's inputs (a zero initial pressure, as the device-timed
     # solves start from, and the div field) are in pinned buffers before the
@@ -663,7 +692,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(grid, body, rhs, args.cpu_iters)
+        cpu = cpu_measured_solve(grid, body, rhs, args.cpu_budget_s)
 
     if rank == 0:
         nsteps = args.steps * world
@@ -682,6 +711,9 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded smoothed-noise RHS with known discrete solution; body tagged on device)",
+            "accuracy": f"solved to relative residual {RTOL:g}: err_vs_exact is the relative L2 distance (fluid "
+                        "cells, mean removed) to the exact discrete solution, which the FP64 oracle's solve "
+                        "converges to",
             "config": {
                 "workload": args.workload, "desc": desc, "cells": cells,
                 "precision": args.precision, "rtol": RTOL, "cycle": "FGMRES(8) right-preconditioned by one V(2,2) cycle, x/y/z zebra line relaxation",
@@ -699,6 +731,7 @@ def run_ours(args):
                 "err_vs_exact": err_o,
             },
             "speedup_mixed_over_fp64": (tot_o / tot_ms) if args.precision == "mixed" else (tot_ms / tot_o),
+            "at_rtol_1e-8": at8,
             "roofline": {
                 "bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
@@ -742,28 +775,18 @@ PAR_NOTE = ("the line sweeps run as z-slabs, one per thread, as the reference ru
             "faces, z lines in per-slab segments); residual and transfers in parallel loops")
 
 
-def extrapolate_iterations(res0, res):
-    """Residual factor per outer iteration and iterations to RTOL from a zero
-    initial guess (relative residual res0), given the relative residuals
-    after each timed iteration: with two or more, the factor of the
-    iterations after the first (the first one reaches res[0]); with one, that
-    iteration's own factor."""
-    if len(res) > 1:
-        rho = (res[-1] / res[0]) ** (1.0 / (len(res) - 1)) if res[0] > 0 else float("nan")
-        n_need = 1 + max(0.0, math.log(RTOL / res[0]) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
-    else:
-        rho = res[0] / res0 if res0 > 0 else float("nan")
-        n_need = max(1.0, math.log(RTOL / res0) / math.log(rho)) if 0.0 < rho < 1.0 else float("nan")
-    return rho, n_need
-
-
-def cpu_baseline_sample(grid, body, rhs, iters):
+def cpu_measured_solve(grid, body, rhs, budget_s, warm_iters=1):
     """The CPU restatement of the reference solver on the same grid, body
-    and RHS: `iters` outer iterations of solve_poisson (each one MG cycle,
-    ghost-cell update, residual), continued from the previous iterate.
-    solves/s = 1 / (seconds per iteration x iterations to reach 1e-8), the
-    iteration count extrapolated from the measured per-iteration residual
-    reduction."""
+    and RHS, run as one solve: outer iterations of solve_poisson (each one
+    MG V-cycle, iterInter = 0, with the ghost-cell update and the residual
+    tests of CORE_POISSON.F90:83-200) from the zero initial guess until the
+    relative residual (the GPU path's stopping test, evaluated between
+    iterations and not timed) reaches RTOL, or until the iterations have
+    used `budget_s` seconds.  Converged: solves/s = 1 / the measured time.
+    Not converged within the budget: the value is 1 / the time spent, an
+    upper bound on the CPU's solves/s (the solve needs more than that), and
+    the residual it reached is reported.  No extrapolation either way.
+    `warm_iters` untimed iterations on a throwaway iterate come first."""
     O = _oracle()
     nthr = host_threads()
     O.set_threads(nthr)
@@ -774,27 +797,37 @@ def cpu_baseline_sample(grid, body, rhs, iters):
     oc.gcm(2.0, 2.0)
     oc.mg_prepare()
     t_setup = time.time() - t0
-    p = np.zeros(grid.shape, order="F")
     f = np.asfortranarray(rhs)
-    res0 = oc.relres(p, f)  # untimed: the zero initial guess
-    res, secs = [], []
-    for _ in range(iters):
-        t = time.time()
-        rc, st = oc.solve_poisson(p, f, params=O.default_params(itermax_pson=1, iterInter=0,
-                                                                restol_pson=RTOL))
-        secs.append(time.time() - t)
+    prm = O.default_params(itermax_pson=1, iterInter=0, restol_pson=RTOL)
+    pw = np.zeros(grid.shape, order="F")
+    for _ in range(warm_iters):
+        oc.solve_poisson(pw, f, params=prm)
+    del pw
+    p = np.zeros(grid.shape, order="F")
+    res, secs, converged = [], 0.0, False
+    while True:
+        t = time.perf_counter()
+        oc.solve_poisson(p, f, params=prm)
+        secs += time.perf_counter() - t
         res.append(oc.relres(p, f))
-    s_it = float(np.mean(secs))
-    rho, n_need = extrapolate_iterations(res0, res)
-    val = 1.0 / (s_it * n_need) if n_need == n_need else None
+        if res[-1] <= RTOL:
+            converged = True
+            break
+        if secs >= budget_s:
+            break
     O.set_threads(1)
-    return {"value": val, "unit": UNIT, "cores": nthr, "kind": "port",
-            "sample": f"{iters} outer iterations (one V-cycle each, iterInter=0) of the reference "
-                      f"solve_poisson restatement (MG V-cycle, line SOR, ghost-cell update) on the full grid, "
-                      f"{nthr} threads ({PAR_NOTE}); "
-                      f"{s_it:.2f} s/iteration, residual factor {rho:.3f}/iteration, "
-                      f"{n_need:.1f} iterations to 1e-8 (extrapolated); setup {t_setup:.1f} s untimed",
-            "s_per_iteration": s_it, "relres": res}
+    its = len(res)
+    what = (f"solved to relative residual {RTOL:g} in {its} outer iterations, {secs:.1f} s measured"
+            if converged else
+            f"not converged: {its} outer iterations in {secs:.1f} s (the budget) reached relative residual "
+            f"{res[-1]:.3g}; value = 1/{secs:.1f} s is an upper bound on the CPU's solves/s")
+    return {"value": 1.0 / secs, "unit": UNIT, "cores": nthr, "kind": "port",
+            "converged": converged, "value_is_upper_bound": not converged,
+            "sample": f"one solve of the same grid, body and RHS from zero by the reference solve_poisson "
+                      f"restatement (MG V-cycle with line SOR, ghost-cell update; iterInter=0) on {nthr} "
+                      f"threads ({PAR_NOTE}); {what}; setup {t_setup:.1f} s untimed",
+            "iterations": its, "seconds": secs, "s_per_iteration": secs / its,
+            "relres_first": res[0], "relres_last": res[-1]}
 
 
 def run_reference(args):
@@ -805,47 +838,29 @@ def run_reference(args):
     grid, body, desc = workload(args.workload)
     synth = _load_pkg().synth
     O = _oracle()
-    nthr = host_threads()
-    O.set_threads(nthr)
     oc = O.OracleCase(grid)
     oc.add_body(body)
     oc.set_iblank()
     oc.gcm(2.0, 2.0)
-    oc.mg_prepare()
     G, D = oc.ghosts(), oc.deads()
     rows = [synth.Interp(D["ijk"], D["cell"], D["coefN"]), synth.Interp(G["ijk"], G["cell"], G["coefN"])]
     rhs, phi = synth.manufactured_rhs(grid, oc.field(0), oc.field(1), oc.field(2), rows, seed=0)
-    f = np.asfortranarray(rhs)
-    p = np.zeros(grid.shape, order="F")
-    prm = O.default_params(itermax_pson=1, iterInter=0, restol_pson=RTOL)
-    for _ in range(args.warmup):
-        oc.solve_poisson(p, f, params=prm)
-    p[...] = 0.0
-    res0 = oc.relres(p, f)  # untimed: the zero initial guess
-    res, secs = [], []
-    for _ in range(args.steps):
-        t = time.time()
-        oc.solve_poisson(p, f, params=prm)
-        secs.append(time.time() - t)
-        res.append(oc.relres(p, f))
-    s_it = float(np.mean(secs))
-    rho, n_need = extrapolate_iterations(res0, res)
-    val = 1.0 / (s_it * n_need) if n_need == n_need else 0.0
-    sample = (f"each step one outer iteration (one V-cycle, iterInter=0) of the reference solve_poisson "
-              f"restatement on {nthr} threads ({PAR_NOTE}) on the full "
-              f"grid (continued iterate); solves/s = 1/(s per iteration x {n_need:.1f} iterations to 1e-8, "
-              f"extrapolated from residual factor {rho:.3f})")
+    del oc
+    cpu = cpu_measured_solve(grid, body, rhs, args.cpu_budget_s, warm_iters=args.warmup)
+    val = cpu["value"]
     cells = (grid.nx - 1) * (grid.ny - 1) * (grid.nz - 1)
     out = {
-        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * s_it, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": cpu["iterations"],
+        "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cpu["s_per_iteration"],
+        "step": "one outer iteration (one V-cycle) of the reference solve; the timed region is one solve "
+                "from zero to the relative residual, or the time budget",
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "desc": desc, "cells": cells, "precision": "fp64",
-                   "rtol": RTOL},
+                   "rtol": RTOL, "cpu_budget_s": args.cpu_budget_s},
         "impl": "reference",
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthr, "kind": "port", "sample": sample},
+        "cpu_baseline": cpu,
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "relres": res,
     }
     print(json.dumps(out), flush=True)
 
@@ -858,7 +873,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="config1")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
-    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--rtol", type=float, default=None,
+                    help="stopping tolerance (default 1e-11 for single grids, 1e-8 for batch/config2/serve)")
+    ap.add_argument("--cpu-budget-s", type=float, default=30.0,
+                    help="CPU baseline: seconds of solve iterations before it is reported unconverged")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="serve: offered arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serve: length of the offered trace")
@@ -869,6 +887,24 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    global RTOL
+    if args.rtol is not None:
+        RTOL = args.rtol
+    elif args.workload in ("batch64", "config2", "serve"):
+        RTOL = RTOL_BASELINE
+    world = int(os.environ.get("WORLD_SIZE", "0"))
+    if world == 0 and args.gpus > 1:
+        # one process per GPU: start the ranks under torchrun on this node
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+               f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1",
+               "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        os.execv(sys.executable, cmd)
+    if world > 0 and world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <chrono>
 #include <cmath>
 #include <map>
@@ -527,8 +528,13 @@ struct fg_batch {
   float *d_rf = nullptr;
   double *d_part = nullptr;   // per-block partial sums of level-0 reductions
   double *d_norm = nullptr;   // per problem: [0] ||r||^2, [1] ||f||^2, [2] ghost max
-  std::vector<double> h_norm;
+  double *h_norm = nullptr;   // page-locked: read back without blocking the host
+  size_t h_norm_n = 0;
+  bool pending = false;       // a queued solve waits for batch_collect
+  fg_status rich_status = FG_OK;
+  fg_solve_stats rich_stats{};
   std::vector<double> history;  // max relative residual over the batch after each cycle
+  int last_mode = 0;  // how the last solve ran: 0 host-driven launches, 1 one graph launch
   // FGMRES state (outer == FG_OUTER_FGMRES): per problem the FP64 vectors
   // P, F and the basis V_0..V_m, Z_0..Z_{m-1} (FP32 in the mixed path) of
   // the finest level's layout
@@ -540,7 +546,19 @@ struct fg_batch {
   KDesc *d_kd = nullptr;
   std::vector<KDesc> h_kd;
   double *d_kpart = nullptr, *d_kout = nullptr, *d_kcoef = nullptr;
-  std::vector<double> h_kout, h_kcoef;
+  KCtl *d_kctl = nullptr;   // scalar FGMRES state on the device
+  KProb *d_kprob = nullptr;
+  KCtl *h_kctl = nullptr;   // page-locked copy the host reads
+  // the whole FGMRES solve captured as one CUDA graph (conditional nodes
+  // for its loops); key: basis precision
+  struct SGraph {
+    cudaGraphExec_t exec = nullptr;
+    int key = -1;
+    std::vector<char> params;
+    bool off = false;
+    cudaStream_t streams[4] = {nullptr, nullptr, nullptr, nullptr};  // nested body captures
+    long long n_pre = 0, n_restart = 0, n_body = 0, n_inner = 0, n_reorth = 0, n_post = 0;
+  } sg;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // the V-cycle captured as a CUDA graph (replayed while the batch's tables
   // stay as built); key: precision and correction form
@@ -599,6 +617,10 @@ static void free_batch_tables(fg_batch *b) {
   b->d_part = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
+  if (b->sg.exec) cudaGraphExecDestroy(b->sg.exec);
+  b->sg.exec = nullptr;
+  b->sg.key = -1;
+  b->sg.params.clear();
   b->d_lev0 = nullptr; b->d_off0 = nullptr; b->d_offf0 = nullptr; b->d_offq0 = nullptr;
   b->d_rprob = nullptr; b->d_rtgt = nullptr;
   b->d_rcell = nullptr; b->d_rw = nullptr; b->d_rc0 = nullptr; b->d_rd = nullptr;
@@ -616,7 +638,9 @@ static void free_krylov(fg_batch *b) {
   for (void *r : b->kraw) fg::dev_free(r);
   b->kraw.clear();
   fg::dev_free(b->d_kd); fg::dev_free(b->d_kpart); fg::dev_free(b->d_kout); fg::dev_free(b->d_kcoef);
+  fg::dev_free(b->d_kctl); fg::dev_free(b->d_kprob);
   b->d_kd = nullptr; b->d_kpart = nullptr; b->d_kout = nullptr; b->d_kcoef = nullptr;
+  b->d_kctl = nullptr; b->d_kprob = nullptr;
   b->km = 0;
   b->kbytes = 0;
   b->ksig.clear();
@@ -847,7 +871,13 @@ static fg_status build_batch(fg_batch *b) {
   if ((st = upload_geometry(b)) != FG_OK) return st;
   FG_CUDA(fg::dev_alloc(&b->d_norm, 3 * np * sizeof(double)));
   FG_CUDA(fg::dev_alloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
-  b->h_norm.assign(3 * np, 0.0);
+  if (b->h_norm_n < (size_t)(3 * np)) {
+    if (b->h_norm) pinned_put(b->h_norm);
+    b->h_norm = static_cast<double *>(pinned_get(3 * np * sizeof(double)));
+    if (!b->h_norm) return FG_ALLOC_FAIL;
+    b->h_norm_n = 3 * np;
+  }
+  std::fill(b->h_norm, b->h_norm + 3 * np, 0.0);
   b->sig = batch_signature(b);
   b->built = true;
   return FG_OK;
@@ -1041,11 +1071,10 @@ static fg_status run_vcycle(fg_batch *b, cudaStream_t s) {
   return FG_OK;
 }
 
-// Outer iteration over the whole batch until every problem meets rtol.
-static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st);
+// Richardson outer iteration (V-cycles on p, host-driven) over the whole
+// batch until every problem meets rtol.
 
-static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
-  if (b->cfg.outer == FG_OUTER_FGMRES) return batch_solve_fgmres(b, st);
+static fg_status batch_solve_richardson(fg_batch *b, fg_solve_stats *st) {
   const int np = (int)b->cases.size();
   cudaStream_t s = b->stream;
   const bool mixed = b->cfg.precision == FG_PREC_MIXED;
@@ -1084,7 +1113,7 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
     }
     FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
     prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-    FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double),
+    FG_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, 3 * np * sizeof(double),
                             cudaMemcpyDeviceToHost, s));
     FG_CUDA(cudaStreamSynchronize(s));
     float ms = 0.0f;
@@ -1124,13 +1153,6 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
 }
 
 // ------------------------------------------------------------ FGMRES
-// Second Gram-Schmidt pass when the first leaves less than this fraction of
-// |w|^2.  At 1e-4 the FP32 basis of small sphere/ellipsoid problems lost
-// enough orthogonality to cost two extra cycles (9 instead of 7); at 1e-2
-// they keep 7 and the large box case keeps its time (a test at 0.1 or 0.5
-// fires on almost every step and costs 6 % there).
-constexpr double kReorth = 1e-2;
-
 static int krylov_restart(const fg_solver_config &cfg) {
   int m = cfg.restart > 0 ? cfg.restart : 10;
   if (m < 2) m = 2;
@@ -1140,7 +1162,8 @@ static int krylov_restart(const fg_solver_config &cfg) {
 
 // Krylov vectors per problem in three allocations with the field padding:
 // P, F (FP64) and the m+1 basis and m preconditioned vectors (basis type,
-// `bytes` per element); one vector every `stride` elements.
+// `bytes` per element); one vector every `stride` elements.  Also the
+// device-side scalar state (KCtl, one KProb per problem).
 static fg_status ensure_krylov(fg_batch *b, int bytes) {
   const int m = krylov_restart(b->cfg);
   std::vector<long long> sig;
@@ -1175,13 +1198,297 @@ static fg_status ensure_krylov(fg_batch *b, int bytes) {
   b->h_kd = kd;
   const int nblk = std::max(1, std::max(b->all0.blocks, b->flat0.blocks));
   FG_CUDA(fg::dev_alloc(&b->d_kpart, (size_t)(KR_MAXV + 1) * nblk * sizeof(double)));
-  FG_CUDA(fg::dev_alloc(&b->d_kout, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
-  FG_CUDA(fg::dev_alloc(&b->d_kcoef, (size_t)np * (KR_MAXV + 2) * sizeof(double)));
-  b->h_kout.assign((size_t)np * (KR_MAXV + 2), 0.0);
-  b->h_kcoef.assign((size_t)np * (KR_MAXV + 2), 0.0);
+  FG_CUDA(fg::dev_alloc(&b->d_kout, (size_t)np * KR_CS * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_kcoef, (size_t)np * KR_CS * sizeof(double)));
+  FG_CUDA(fg::dev_alloc(&b->d_kctl, sizeof(KCtl)));
+  FG_CUDA(fg::dev_alloc(&b->d_kprob, (size_t)np * sizeof(KProb)));
+  FG_CUDA(cudaMemset(b->d_kprob, 0, (size_t)np * sizeof(KProb)));
+  if (!b->h_kctl) {
+    b->h_kctl = static_cast<KCtl *>(pinned_get(sizeof(KCtl)));
+    if (!b->h_kctl) return FG_ALLOC_FAIL;
+  }
   b->km = m;
   b->kbytes = bytes;
   b->ksig = sig;
+  return FG_OK;
+}
+
+// The pieces of one FGMRES(m) solve over the batch, as launch sequences on
+// a stream.  Direct mode runs them from a host loop that reads the device's
+// decisions (KCtl) after the scalar steps; graph mode captures them once
+// into a CUDA graph whose WHILE / IF conditional nodes take the same
+// decisions on the device, so a whole solve is one graph launch and the
+// host waits only for its end.  Both run the same kernels in the same
+// order, so they give identical results.
+template <typename B, typename T>
+struct FgPieces {
+  fg_batch *b;
+  bool graph;  // V-cycles launched inline (being captured) instead of replayed
+  // residual and norms consistent with the initial field, Krylov P and F,
+  // scalar state reset
+  fg_status pre(cudaStream_t s) {
+    const int np = (int)b->cases.size();
+    FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
+    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
+    FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
+    for (int p = 0; p < np; ++p) {
+      const HLevel &L0 = b->cases[p]->lev[0];
+      FG_CUDA(cudaMemcpyAsync(b->h_kd[p].P, L0.d_x64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      FG_CUDA(cudaMemcpyAsync(b->h_kd[p].F, L0.d_rhs64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    FG_K(k::fg_begin(b->d_kctl, np, b->km, b->cfg.max_cycles, b->cfg.rtol, s));
+    return FG_OK;
+  }
+  // true residual V_0 = F - A P, its norms, the restart decision
+  fg_status restart(cudaStream_t s, int use_cond, unsigned long long ho, unsigned long long hb,
+                    unsigned long long hi) {
+    const int np = (int)b->cases.size();
+    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
+    const size_t e_r = prof_begin(b, s);
+    FG_K(k::kr_resid<B>(b->all0q, b->rows, b->d_lev0, b->d_kd, 0, b->d_part, b->d_norm, s));
+    FG_K(k::krd_dots<B>(b->flat0, b->d_kd, b->d_kctl, KPH_RESTART, b->d_kpart, b->d_kout, s));
+    prof_end(b, e_r, FG_PROF_RESIDUAL, 0.0, s);
+    FG_K(k::fg_restart(b->d_kctl, b->d_kprob, b->d_kout, b->d_norm, b->d_kcoef, use_cond, ho, hb, hi, s));
+    return FG_OK;
+  }
+  // V_0 / beta, staged as the first preconditioner input
+  fg_status stage(cudaStream_t s) {
+    const size_t e0 = prof_begin(b, s);
+    FG_K((k::krd_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, b->d_kctl, KPH_RESTART, b->d_kcoef, s)));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    return FG_OK;
+  }
+  // Z_j = M^-1 V_j (one V-cycle), V_{j+1} = A Z_j, first Gram-Schmidt dots
+  fg_status step_a(cudaStream_t s, int use_cond, unsigned long long hr) {
+    fg_status r = graph ? vcycle<T>(b, s) : run_vcycle<T>(b, s);
+    if (r != FG_OK) return r;
+    const size_t e0 = prof_begin(b, s);
+    FG_K((k::krd_apply<B, T>(b->all0q, b->rows, b->d_lev0, b->d_kd, b->d_kctl, s)));
+    FG_K(k::krd_dots<B>(b->flat0, b->d_kd, b->d_kctl, KPH_APPLY, b->d_kpart, b->d_kout, s));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    FG_K(k::fg_reorth_test(b->d_kctl, b->d_kprob, b->d_kout, b->d_kcoef, use_cond, hr, s));
+    return FG_OK;
+  }
+  // the second Gram-Schmidt pass
+  fg_status reorth(cudaStream_t s) {
+    const size_t e0 = prof_begin(b, s);
+    FG_K((k::krd_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, b->d_kctl, KPH_REORTH, b->d_kcoef, s)));
+    FG_K(k::krd_dots<B>(b->flat0, b->d_kd, b->d_kctl, KPH_APPLY, b->d_kpart, b->d_kout, s));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    return FG_OK;
+  }
+  // rotations and the next basis vector (staged when another step follows)
+  fg_status step_b(cudaStream_t s, int use_cond, unsigned long long hi) {
+    FG_K(k::fg_arnoldi(b->d_kctl, b->d_kprob, b->d_kout, b->d_kcoef, use_cond, hi, s));
+    const size_t e0 = prof_begin(b, s);
+    FG_K((k::krd_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, b->d_kctl, KPH_NORMALIZE, b->d_kcoef,
+                             s)));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    return FG_OK;
+  }
+  // P += sum y_i Z_i
+  fg_status finish_cycle(cudaStream_t s) {
+    FG_K(k::fg_lsq(b->d_kctl, b->d_kprob, b->d_kcoef, s));
+    const size_t e0 = prof_begin(b, s);
+    FG_K(k::krd_update<B>(b->flat0, b->d_kd, b->d_kctl, b->d_kcoef, s));
+    prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
+    return FG_OK;
+  }
+  // solution back into the finest-level field; ghost-row residual
+  fg_status post(cudaStream_t s) {
+    const int np = (int)b->cases.size();
+    for (int p = 0; p < np; ++p) {
+      const HLevel &L0 = b->cases[p]->lev[0];
+      FG_CUDA(cudaMemcpyAsync(L0.d_x64, b->h_kd[p].P, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      FG_CUDA(cudaMemcpyAsync(L0.d_rhs64, b->h_kd[p].F, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
+    FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+    return FG_OK;
+  }
+};
+
+static fg_status read_ctl(fg_batch *b, cudaStream_t s) {
+  FG_CUDA(cudaMemcpyAsync(b->h_kctl, b->d_kctl, offsetof(KCtl, hist), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  return FG_OK;
+}
+
+template <typename B, typename T>
+static fg_status fgmres_direct(fg_batch *b, cudaStream_t s) {
+  FgPieces<B, T> F{b, false};
+  fg_status r;
+  if ((r = F.pre(s)) != FG_OK) return r;
+  for (;;) {
+    if ((r = F.restart(s, 0, 0, 0, 0)) != FG_OK) return r;
+    if ((r = read_ctl(b, s)) != FG_OK) return r;
+    if (!b->h_kctl->outer) break;
+    if ((r = F.stage(s)) != FG_OK) return r;
+    for (;;) {
+      if ((r = F.step_a(s, 0, 0)) != FG_OK) return r;
+      if ((r = read_ctl(b, s)) != FG_OK) return r;
+      if (b->h_kctl->reorth && (r = F.reorth(s)) != FG_OK) return r;
+      if ((r = F.step_b(s, 0, 0)) != FG_OK) return r;
+      if ((r = read_ctl(b, s)) != FG_OK) return r;
+      if (!b->h_kctl->inner) break;
+    }
+    if ((r = F.finish_cycle(s)) != FG_OK) return r;
+  }
+  return F.post(s);
+}
+
+// Appends a conditional node to the graph being captured on `s` (after
+// everything captured so far) and starts capturing its body on `sb`.
+static cudaError_t cond_begin(cudaStream_t s, cudaStream_t sb, cudaGraphConditionalHandle h,
+                              cudaGraphConditionalNodeType type) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = type;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if ((e = cudaGraphAddNode(&node, g, deps, nd, &cp)) != cudaSuccess) return e;
+  if ((e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+    return e;
+  return cudaStreamBeginCaptureToGraph(sb, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal);
+}
+static cudaError_t cond_end(cudaStream_t sb) {
+  cudaGraph_t g = nullptr;
+  return cudaStreamEndCapture(sb, &g);
+}
+
+// Captures the whole solve: pre; WHILE(outer) { restart; IF(body) { stage;
+// WHILE(inner) { step_a; IF(reorth) { reorth } step_b } finish_cycle } };
+// post.  Launch counts of each section are kept for the launch counter.
+template <typename B, typename T>
+static fg_status capture_solve(fg_batch *b, cudaStream_t s, cudaGraph_t *out) {
+  auto &SG = b->sg;
+  if (!SG.streams[0])
+    for (auto &q : SG.streams) FG_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  FG_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle ho, hb, hi, hr;
+  auto fail = [&](fg_status st) {
+    for (auto &q : SG.streams) {
+      cudaStreamCaptureStatus cs;
+      if (cudaStreamIsCapturing(q, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t t = nullptr;
+        cudaStreamEndCapture(q, &t);
+      }
+    }
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t t = nullptr;
+      cudaStreamEndCapture(s, &t);
+    }
+    (void)cudaGetLastError();
+    cudaGraphDestroy(g);
+    return st;
+  };
+  if (cudaGraphConditionalHandleCreate(&ho, g, 1, cudaGraphCondAssignDefault) != cudaSuccess ||
+      cudaGraphConditionalHandleCreate(&hb, g, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
+      cudaGraphConditionalHandleCreate(&hi, g, 0, cudaGraphCondAssignDefault) != cudaSuccess ||
+      cudaGraphConditionalHandleCreate(&hr, g, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+    return fail(FG_CUDA_ERROR);
+  FgPieces<B, T> F{b, true};
+  cudaStream_t s1 = SG.streams[0], s2 = SG.streams[1], s3 = SG.streams[2], s4 = SG.streams[3];
+  const long long n0 = thread_launches();
+  long long m0;
+  fg_status r;
+  if (cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return fail(FG_CUDA_ERROR);
+  if ((r = F.pre(s)) != FG_OK) return fail(r);
+  SG.n_pre = thread_launches() - n0;
+  if (cond_begin(s, s1, ho, cudaGraphCondTypeWhile) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.restart(s1, 1, ho, hb, hi)) != FG_OK) return fail(r);
+  SG.n_restart = thread_launches() - m0;
+  if (cond_begin(s1, s2, hb, cudaGraphCondTypeIf) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.stage(s2)) != FG_OK) return fail(r);
+  SG.n_body = thread_launches() - m0;
+  if (cond_begin(s2, s3, hi, cudaGraphCondTypeWhile) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.step_a(s3, 1, hr)) != FG_OK) return fail(r);
+  SG.n_inner = thread_launches() - m0;
+  if (cond_begin(s3, s4, hr, cudaGraphCondTypeIf) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.reorth(s4)) != FG_OK) return fail(r);
+  SG.n_reorth = thread_launches() - m0;
+  if (cond_end(s4) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.step_b(s3, 1, hi)) != FG_OK) return fail(r);
+  SG.n_inner += thread_launches() - m0;
+  if (cond_end(s3) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.finish_cycle(s2)) != FG_OK) return fail(r);
+  SG.n_body += thread_launches() - m0;
+  if (cond_end(s2) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  if (cond_end(s1) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  m0 = thread_launches();
+  if ((r = F.post(s)) != FG_OK) return fail(r);
+  SG.n_post = thread_launches() - m0;
+  cudaGraph_t gout = nullptr;
+  if (cudaStreamEndCapture(s, &gout) != cudaSuccess) return fail(FG_CUDA_ERROR);
+  note_launches(-(thread_launches() - n0));  // counted per replay
+  *out = g;
+  return FG_OK;
+}
+
+// Launch arguments the captured solve depends on beyond the batch tables:
+// the V-cycle's (rows, coarsest sizes) and the Krylov buffers.
+static std::vector<char> solve_params(const fg_batch *b) {
+  std::vector<char> v = vcycle_params(b);
+  auto put = [&](const void *p, size_t n) { v.insert(v.end(), (const char *)p, (const char *)p + n); };
+  put(&b->d_kd, sizeof(b->d_kd));
+  put(&b->d_kctl, sizeof(b->d_kctl));
+  put(&b->km, sizeof(b->km));
+  put(&b->cfg.max_cycles, sizeof(int));
+  put(&b->cfg.rtol, sizeof(double));
+  return v;
+}
+
+template <typename B, typename T>
+static fg_status fgmres_graph(fg_batch *b, cudaStream_t s) {
+  auto &SG = b->sg;
+  const int key = sizeof(B) == 4 ? 1 : 0;
+  const std::vector<char> params = solve_params(b);
+  if (!SG.exec || SG.key != key || SG.params != params) {
+    cudaGraph_t g = nullptr;
+    fg_status r = capture_solve<B, T>(b, s, &g);
+    if (r != FG_OK) return r;
+    cudaError_t e = cudaErrorUnknown;
+    if (SG.exec && SG.key == key) {
+      cudaGraphExecUpdateResultInfo info;
+      e = cudaGraphExecUpdate(SG.exec, g, &info);
+      if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        cudaGraphExecDestroy(SG.exec);
+        SG.exec = nullptr;
+      }
+    } else if (SG.exec) {
+      cudaGraphExecDestroy(SG.exec);
+      SG.exec = nullptr;
+    }
+    if (!SG.exec) e = cudaGraphInstantiate(&SG.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      SG.exec = nullptr;
+      return FG_CUDA_ERROR;
+    }
+    SG.key = key;
+    SG.params = params;
+  }
+  FG_CUDA(cudaGraphLaunch(SG.exec, s));
   return FG_OK;
 }
 
@@ -1193,250 +1500,98 @@ static fg_status ensure_krylov(fg_batch *b, int bytes) {
 // stay FP64, so the basis precision only limits how far one restart cycle
 // reduces the residual), T the V-cycle's.  All problems of the batch
 // iterate in lockstep; each has its own Arnoldi basis, Hessenberg matrix
-// and Givens rotations (host).  Convergence: true fluid-row relative
-// residual <= rtol at a restart.
+// and Givens rotations (device).  Convergence: true fluid-row relative
+// residual <= rtol at a restart.  The whole solve is one CUDA graph launch
+// (conditional nodes for the loops) unless launch classes are timed, the
+// caller's stream is being captured, or the capture failed once; then the
+// host drives the same kernels.
 template <typename B, typename T>
-static fg_status fgmres_run(fg_batch *b, fg_solve_stats *st) {
+static fg_status fgmres_enqueue(fg_batch *b) {
   const int np = (int)b->cases.size();
   cudaStream_t s = b->stream;
   fg_status r = ensure_krylov(b, (int)sizeof(B));
   if (r != FG_OK) return r;
-  const int m = b->km;
-  const int CS = KR_MAXV + 2;  // coefficient / output stride per problem
   if (!b->ev0) { cudaEventCreate(&b->ev0); cudaEventCreate(&b->ev1); }
   FG_CUDA(cudaEventRecord(b->ev0, s));
-  FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
-  FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
-  FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
-  for (int p = 0; p < np; ++p) {
-    const HLevel &L0 = b->cases[p]->lev[0];
-    FG_CUDA(cudaMemcpyAsync(b->h_kd[p].P, L0.d_x64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    FG_CUDA(cudaMemcpyAsync(b->h_kd[p].F, L0.d_rhs64, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  }
   b->krylov = true;
-  b->history.clear();
-  auto upload_coef = [&]() -> fg_status {
-    FG_CUDA(cudaMemcpyAsync(b->d_kcoef, b->h_kcoef.data(), b->h_kcoef.size() * sizeof(double),
-                            cudaMemcpyHostToDevice, s));
-    return FG_OK;
-  };
-  auto read_out = [&]() -> fg_status {
-    FG_CUDA(cudaMemcpyAsync(b->h_kout.data(), b->d_kout, b->h_kout.size() * sizeof(double),
-                            cudaMemcpyDeviceToHost, s));
-    FG_CUDA(cudaStreamSynchronize(s));
-    return FG_OK;
-  };
-  std::vector<double> f2(np, 0.0), relres(np, 1.0), beta(np, 0.0);
-  std::vector<double> H((size_t)np * (m + 1) * m, 0.0), g((size_t)np * (m + 1), 0.0);
-  std::vector<double> cs_((size_t)np * m, 0.0), sn_((size_t)np * m, 0.0);
-  std::vector<int> ncol(np, 0);
-  std::vector<char> done(np, 0);
-  auto Hx = [&](int p, int i, int j) -> double & { return H[((size_t)p * (m + 1) + i) * m + j]; };
-  int cycles = 0;
-  std::vector<double> vms;
-  cudaEvent_t va, vb;
-  cudaEventCreate(&va); cudaEventCreate(&vb);
-  fg_status status = FG_NOT_CONVERGED;
-  bool first = true;
-  fg_status err = FG_OK;
-  while (err == FG_OK) {
-    // ---- true residual V_0 = F - A P, fluid norm, full norm
-    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
-    const size_t e_r = prof_begin(b, s);
-    FG_K(k::kr_resid<B>(b->all0q, b->rows, b->d_lev0, b->d_kd, 0, b->d_part, b->d_norm, s));
-    FG_K(k::kr_dots<B>(b->flat0, b->d_kd, 0, 0, b->d_kpart, b->d_kout, CS, s));
-    prof_end(b, e_r, FG_PROF_RESIDUAL, 0.0, s);
-    FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if ((err = read_out()) != FG_OK) break;
-    bool all = true;
-    double worst = 0.0;
-    for (int p = 0; p < np; ++p) {
-      if (first) f2[p] = b->h_norm[np + p];
-      relres[p] = f2[p] > 0.0 ? std::sqrt(b->h_norm[p] / f2[p]) : std::sqrt(b->h_norm[p]);
-      beta[p] = std::sqrt(std::max(0.0, b->h_kout[(size_t)p * CS + 0]));
-      worst = std::max(worst, relres[p]);
-      done[p] = (relres[p] <= b->cfg.rtol || beta[p] == 0.0) ? 1 : 0;
-      if (!done[p]) all = false;
-    }
-    first = false;
-    b->history.push_back(worst);
-    if (all) { status = FG_OK; break; }
-    if (cycles >= b->cfg.max_cycles) break;
-    // ---- V_0 /= beta, staged as the first preconditioner input
-    for (int p = 0; p < np; ++p) {
-      b->h_kcoef[(size_t)p * CS] = done[p] ? 0.0 : 1.0 / beta[p];
-      ncol[p] = 0;
-      for (int i = 0; i <= m; ++i) g[(size_t)p * (m + 1) + i] = 0.0;
-      g[(size_t)p * (m + 1)] = beta[p];
-    }
-    if ((err = upload_coef()) != FG_OK) break;
-    {
-      const size_t e0 = prof_begin(b, s);
-      FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, 0, 0, 0, b->d_kcoef, CS, true, s)));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-    }
-    int jlast = 0;
-    for (int j = 0; j < m && cycles < b->cfg.max_cycles; ++j) {
-      // ---- Z_j = M^-1 V_j (one V-cycle from zero, correction form)
-      cudaEventRecord(va, s);
-      r = run_vcycle<T>(b, s);
-      if (r != FG_OK) { err = r; break; }
-      cudaEventRecord(vb, s);
-      ++cycles;
-      // ---- Z_j from the V-cycle, W = A Z_j into V_{j+1}; inner products
-      // with V_0..V_j and |W|^2
-      size_t e0 = prof_begin(b, s);
-      FG_K((k::kr_apply<B, T>(b->all0q, b->rows, b->d_lev0, b->d_kd, j, j + 1, s)));
-      FG_K(k::kr_dots<B>(b->flat0, b->d_kd, j + 1, j + 1, b->d_kpart, b->d_kout, CS, s));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-      if ((err = read_out()) != FG_OK) break;
-      {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, va, vb);
-        vms.push_back(ms);
-      }
-      // classical Gram-Schmidt; a second pass only where the projection
-      // removed all but 1e-4 of |w|^2 (two of the basis's digits lost).  With
-      // a V-cycle preconditioner w = A M^-1 v_j lies mostly in the span of
-      // the basis, so the usual 1/2 test asks for the second pass on almost
-      // every step (a dot and an axpy pass over all vectors each time);
-      // without any second pass the strict convergence cases stall.
-      bool reorth = false;
-      std::vector<double> hcol((size_t)np * (j + 2), 0.0), ww(np, 0.0);
-      for (int p = 0; p < np; ++p) {
-        const double *o = &b->h_kout[(size_t)p * CS];
-        double sum = 0.0;
-        for (int i = 0; i <= j; ++i) { hcol[(size_t)p * (j + 2) + i] = o[i]; sum += o[i] * o[i]; }
-        ww[p] = o[j + 1];
-        if (!done[p] && ww[p] - sum < kReorth * ww[p]) reorth = true;
-      }
-      if (reorth) {
-        for (int p = 0; p < np; ++p) {
-          double *cf = &b->h_kcoef[(size_t)p * CS];
-          cf[0] = 1.0;
-          for (int i = 0; i <= j; ++i) cf[1 + i] = done[p] ? 0.0 : -hcol[(size_t)p * (j + 2) + i];
-        }
-        if ((err = upload_coef()) != FG_OK) break;
-        e0 = prof_begin(b, s);
-        FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, j + 1, 0, j + 1, b->d_kcoef, CS,
-                                false, s)));
-        FG_K(k::kr_dots<B>(b->flat0, b->d_kd, j + 1, j + 1, b->d_kpart, b->d_kout, CS, s));
-        prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-        if ((err = read_out()) != FG_OK) break;
-      }
-      // normalise: V_{j+1} = (W - sum h_i V_i) / h_{j+1}
-      for (int p = 0; p < np; ++p) {
-        double *cf = &b->h_kcoef[(size_t)p * CS];
-        const double *o = &b->h_kout[(size_t)p * CS];
-        double sum = 0.0;
-        for (int i = 0; i <= j; ++i) {
-          const double hi = o[i];  // second-pass corrections when reorthogonalised
-          if (reorth) hcol[(size_t)p * (j + 2) + i] += hi;
-          sum += hi * hi;
-        }
-        const double h2 = o[j + 1] - sum;
-        const double hn = h2 > 0.0 ? std::sqrt(h2) : 0.0;
-        hcol[(size_t)p * (j + 2) + j + 1] = hn;
-        const bool brk = done[p] || !(hn > 1e-14 * beta[p]);
-        cf[0] = brk ? 0.0 : 1.0 / hn;
-        for (int i = 0; i <= j; ++i) cf[1 + i] = brk ? 0.0 : -o[i] / hn;
-        if (done[p]) continue;
-        // Hessenberg column j, previous rotations, new rotation
-        for (int i = 0; i <= j + 1; ++i) Hx(p, i, j) = hcol[(size_t)p * (j + 2) + i];
-        for (int i = 0; i < j; ++i) {
-          const double c = cs_[(size_t)p * m + i], sv = sn_[(size_t)p * m + i];
-          const double h0 = Hx(p, i, j), h1 = Hx(p, i + 1, j);
-          Hx(p, i, j) = c * h0 + sv * h1;
-          Hx(p, i + 1, j) = -sv * h0 + c * h1;
-        }
-        const double a = Hx(p, j, j), bb = Hx(p, j + 1, j);
-        const double rr = std::hypot(a, bb);
-        const double c = rr > 0.0 ? a / rr : 1.0, sv = rr > 0.0 ? bb / rr : 0.0;
-        cs_[(size_t)p * m + j] = c; sn_[(size_t)p * m + j] = sv;
-        Hx(p, j, j) = rr; Hx(p, j + 1, j) = 0.0;
-        double *gp = &g[(size_t)p * (m + 1)];
-        gp[j + 1] = -sv * gp[j];
-        gp[j] = c * gp[j];
-        ncol[p] = j + 1;
-        if (brk) done[p] = 1;
-      }
-      jlast = j + 1;
-      // residual estimate |g_{j+1}| (all rows) over the fluid-row |f|
-      bool inner_done = true;
-      double west = 0.0;
-      for (int p = 0; p < np; ++p) {
-        const double est = std::fabs(g[(size_t)p * (m + 1) + ncol[p]]);
-        const double rel = f2[p] > 0.0 ? est / std::sqrt(f2[p]) : est;
-        west = std::max(west, rel);
-        if (!(done[p] || rel <= 0.5 * b->cfg.rtol)) inner_done = false;
-      }
-      b->history.push_back(west);
-      // the next basis vector, staged as the next preconditioner input
-      // unless the cycle ends here
-      const bool more = !inner_done && j + 1 < m && cycles < b->cfg.max_cycles;
-      if ((err = upload_coef()) != FG_OK) break;
-      e0 = prof_begin(b, s);
-      FG_K((k::kr_vaxpy<B, T>(b->flat0, b->rows, b->d_lev0, b->d_kd, j + 1, 0, j + 1, b->d_kcoef, CS, more,
-                              s)));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-      if (!more) break;
-    }
-    if (err != FG_OK) break;
-    // ---- P += sum_i y_i Z_i, y from the rotated Hessenberg system
-    for (int p = 0; p < np; ++p) {
-      double *cf = &b->h_kcoef[(size_t)p * CS];
-      for (int i = 0; i < CS; ++i) cf[i] = 0.0;
-      cf[0] = 1.0;
-      const int nc = ncol[p];
-      std::vector<double> y(nc, 0.0);
-      for (int i = nc - 1; i >= 0; --i) {
-        double v = g[(size_t)p * (m + 1) + i];
-        for (int q = i + 1; q < nc; ++q) v -= Hx(p, i, q) * y[q];
-        y[i] = Hx(p, i, i) != 0.0 ? v / Hx(p, i, i) : 0.0;
-      }
-      for (int i = 0; i < nc; ++i) cf[1 + i] = y[i];
-    }
-    if ((err = upload_coef()) != FG_OK) break;
-    if (jlast > 0) {
-      const size_t e0 = prof_begin(b, s);
-      FG_K(k::kr_update<B>(b->flat0, b->d_kd, jlast, b->d_kcoef, CS, s));
-      prof_end(b, e0, FG_PROF_RESIDUAL, 0.0, s);
-    }
+  bool use_graph = !b->prof.on && !b->sg.off;
+  if (use_graph) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    FG_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) use_graph = false;
   }
-  cudaEventDestroy(va); cudaEventDestroy(vb);
+  bool graphed = false;
+  if (use_graph) {
+    r = fgmres_graph<B, T>(b, s);
+    if (r == FG_OK) graphed = true;
+    else b->sg.off = true;  // launch directly from now on
+  }
+  if (!graphed) r = fgmres_direct<B, T>(b, s);
+  b->last_mode = graphed ? 1 : 0;
   b->krylov = false;
-  if (err != FG_OK) return err;
-  // solution back into the finest-level field; ghost-row residual for stats
-  for (int p = 0; p < np; ++p) {
-    const HLevel &L0 = b->cases[p]->lev[0];
-    FG_CUDA(cudaMemcpyAsync(L0.d_x64, b->h_kd[p].P, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    FG_CUDA(cudaMemcpyAsync(L0.d_rhs64, b->h_kd[p].F, L0.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  }
-  FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
-  FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
-  FG_CUDA(cudaMemcpyAsync(b->h_norm.data(), b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (r != FG_OK) return r;
+  FG_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaMemcpyAsync(b->h_kctl, b->d_kctl, sizeof(KCtl), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaEventRecord(b->ev1, s));
+  b->pending = true;
+  return FG_OK;
+}
+
+// Waits for the solve fgmres_enqueue queued and reads its outcome.
+static fg_status fgmres_collect(fg_batch *b, fg_solve_stats *st) {
+  if (!b->pending) return FG_BAD_INPUT;
+  b->pending = false;
+  const int np = (int)b->cases.size();
   FG_CUDA(cudaEventSynchronize(b->ev1));
+  const KCtl &C = *b->h_kctl;
+  if (b->last_mode == 1) {
+    const auto &SG = b->sg;
+    note_launches(SG.n_pre + C.n_restart * SG.n_restart + C.n_body * SG.n_body + C.n_inner * SG.n_inner +
+                  C.n_reorth * SG.n_reorth + SG.n_post);
+  }
+  b->history.assign(C.hist, C.hist + std::min(C.nhist, KR_HIST));
   float tot = 0.0f;
   cudaEventElapsedTime(&tot, b->ev0, b->ev1);
   if (b->prof.on) prof_collect(b);
   if (st) {
-    double mr = 0.0, mg = 0.0;
-    for (int p = 0; p < np; ++p) { mr = std::max(mr, relres[p]); mg = std::max(mg, b->h_norm[2 * np + p]); }
-    st->cycles = cycles;
-    st->relres = mr;
+    double mg = 0.0;
+    for (int p = 0; p < np; ++p) mg = std::max(mg, b->h_norm[2 * np + p]);
+    st->cycles = C.cycles;
+    st->relres = C.relres_max;
     st->ghost_res = mg;
     st->seconds = tot * 1e-3;
-    double sm = 0.0;
-    for (double v : vms) sm += v;
-    st->vcycle_ms = vms.empty() ? 0.0 : sm / vms.size();
+    st->vcycle_ms = C.cycles > 0 ? (double)tot / C.cycles : 0.0;  // per cycle, Krylov work included
   }
-  return status;
+  return C.status == FG_OK ? FG_OK : FG_NOT_CONVERGED;
 }
 
-static fg_status batch_solve_fgmres(fg_batch *b, fg_solve_stats *st) {
-  if (b->cfg.precision == FG_PREC_MIXED) return fgmres_run<float, float>(b, st);
-  return fgmres_run<double, double>(b, st);
+// Queues one solve of the batch on its stream (FGMRES: a single graph
+// launch in the usual case); batch_collect waits for it.  The Richardson
+// outer iteration runs to completion here.
+static fg_status batch_enqueue(fg_batch *b) {
+  if (b->cfg.outer != FG_OUTER_FGMRES) {
+    b->rich_status = batch_solve_richardson(b, &b->rich_stats);
+    b->pending = true;
+    return (b->rich_status == FG_OK || b->rich_status == FG_NOT_CONVERGED) ? FG_OK : b->rich_status;
+  }
+  if (b->cfg.precision == FG_PREC_MIXED) return fgmres_enqueue<float, float>(b);
+  return fgmres_enqueue<double, double>(b);
+}
+
+static fg_status batch_collect(fg_batch *b, fg_solve_stats *st) {
+  if (b->cfg.outer != FG_OUTER_FGMRES) {
+    if (!b->pending) return FG_BAD_INPUT;
+    b->pending = false;
+    if (st) *st = b->rich_stats;
+    return b->rich_status;
+  }
+  return fgmres_collect(b, st);
+}
+
+static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
+  fg_status r = batch_enqueue(b);
+  if (r != FG_OK) return r;
+  return batch_collect(b, st);
 }
 
 // -------------------------------------------------------- case geometry
@@ -1938,6 +2093,18 @@ static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
   }
 }
 
+// outer-face data of a case (Dirichlet values; Neumann faces carry no
+// gradient data: homogeneous)
+static k::FaceData face_data(const fg_case *c) {
+  k::FaceData fd{};
+  for (int f = 0; f < 6; ++f) {
+    fd.pbc[f] = c->cfg.pbc[f];
+    fd.ppp[f] = c->cfg.ppp[f];
+    fd.pgrad[f] = nullptr;
+  }
+  return fd;
+}
+
 // gauge and outer boundary layers on the device copy of the output
 static fg_status finish_output(fg_case *c) {
   bool allN = true;
@@ -1947,23 +2114,34 @@ static fg_status finish_output(fg_case *c) {
   return FG_OK;
 }
 
-static fg_status solve_common(fg_case *c, const double *p_old, const double *dpdn_g,
-                              const double *dpdn_d, fg_solve_stats *st) {
+}  // extern "C"
+
+// Queues a solve of the fields staged in the case (d_pin: initial pressure,
+// d_fin: right-hand side, both in the reference layout) and the finishing
+// of the output (gauge, outer boundary layers) back into d_pin, on the
+// case's stream; fg::solve_collect waits for it.  With FGMRES the solve is
+// one graph launch and the call returns as soon as the work is queued.
+fg_status fg::solve_enqueue(fg_case *c, const double *p_old, const double *dpdn_g, const double *dpdn_d) {
   fg_status s = ensure_solo(c);
   if (s != FG_OK) return s;
   std::vector<double> c0;
   row_constants(c, p_old, dpdn_g, dpdn_d, c0);
   if ((int)c0.size() != c->solo->rows.n) return FG_BAD_INPUT;
-  if (!c0.empty())
+  if (!c0.empty())  // pageable source: staged before the call returns
     FG_CUDA(cudaMemcpyAsync(c->solo->d_rc0, c0.data(), c0.size() * sizeof(double),
                             cudaMemcpyHostToDevice, c->stream));
   HLevel &L0 = c->lev[0];
   FG_K(k::copy_in(L0.d_x64, c->d_pin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
   FG_K(k::copy_in(L0.d_rhs64, c->d_fin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
-  s = batch_solve(c->solo, st);
+  FG_K(k::face_rhs(L0.d_rhs64, L0.dl, face_data(c), c->stream));
+  if ((s = batch_enqueue(c->solo)) != FG_OK) return s;
   FG_K(k::copy_out(c->d_pin, L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
-  return s;
+  return finish_output(c);
 }
+
+fg_status fg::solve_collect(fg_case *c, fg_solve_stats *st) { return batch_collect(c->solo, st); }
+
+extern "C" {
 
 fg_status fg_solve_poisson(fg_case *c, double *p, const double *div, const double *p_old,
                            const double *dpdn_ghost, const double *dpdn_dead,
@@ -1973,11 +2151,10 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div, const doubl
   const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
   FG_CUDA(cudaMemcpyAsync(c->d_pin, p, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   FG_CUDA(cudaMemcpyAsync(c->d_fin, div, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  fg_status s = solve_common(c, p_old, dpdn_ghost, dpdn_dead, st);
-  if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
-  fg_status f = finish_output(c);
-  if (f != FG_OK) return f;
+  fg_status s = fg::solve_enqueue(c, p_old, dpdn_ghost, dpdn_dead);
+  if (s != FG_OK) return s;
   FG_CUDA(cudaMemcpyAsync(p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  s = fg::solve_collect(c, st);
   FG_CUDA(cudaStreamSynchronize(c->stream));
   return s;
 }
@@ -1990,11 +2167,10 @@ fg_status fg_solve_poisson_device(fg_case *c, double *d_p, const double *d_div,
   const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
   FG_CUDA(cudaMemcpyAsync(c->d_pin, d_p, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   FG_CUDA(cudaMemcpyAsync(c->d_fin, d_div, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  fg_status s = solve_common(c, nullptr, nullptr, nullptr, st);
-  if (s != FG_OK && s != FG_NOT_CONVERGED) return s;
-  fg_status f = finish_output(c);
-  if (f != FG_OK) return f;
+  fg_status s = fg::solve_enqueue(c, nullptr, nullptr, nullptr);
+  if (s != FG_OK) return s;
   FG_CUDA(cudaMemcpyAsync(d_p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  s = fg::solve_collect(c, st);
   FG_CUDA(cudaStreamSynchronize(c->stream));
   return s;
 }
@@ -2073,6 +2249,7 @@ fg_status fg_batch_solve_device(fg_batch *b, double **d_p, const double **d_div,
     HLevel &L0 = c->lev[0];
     FG_K(k::copy_in(L0.d_x64, d_p[p], L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, b->stream));
     FG_K(k::copy_in(L0.d_rhs64, d_div[p], L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, b->stream));
+    FG_K(k::face_rhs(L0.d_rhs64, L0.dl, face_data(c), b->stream));
   }
   fg_status s = batch_solve(b, st);
   for (size_t p = 0; p < b->cases.size(); ++p) {
@@ -2116,6 +2293,12 @@ fg_status fg_case_history(const fg_case *c, double *relres, int capacity, int *c
   return FG_OK;
 }
 
+fg_status fg_case_solve_mode(const fg_case *c, int *mode) {
+  if (!c || !mode) return FG_BAD_INPUT;
+  *mode = c->solo ? c->solo->last_mode : 0;
+  return FG_OK;
+}
+
 fg_status fg_case_profile(fg_case *c, int enable) {
   if (!c) return FG_BAD_INPUT;
   fg_status st = ensure_solo(c);
@@ -2140,6 +2323,10 @@ fg_status fg_batch_destroy(fg_batch *b) {
   cudaSetDevice(b->device);
   free_batch_tables(b);
   free_krylov(b);
+  for (auto &q : b->sg.streams)
+    if (q) cudaStreamDestroy(q);
+  if (b->h_kctl) pinned_put(b->h_kctl);
+  if (b->h_norm) pinned_put(b->h_norm);
   if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }
   delete b;
   return FG_OK;

@@ -118,4 +118,8 @@ fg_status geometry_rows(fg_case *c, int nGhost, const int32_t *ghost_ijk, const 
                         const double *ghost_coefN, int nDead, const int32_t *dead_ijk,
                         const int32_t *dead_cell_idx, const double *dead_coefN,
                         const double *dead_probe, const double *dead_ip);
+// a solve of the fields staged in c->d_pin / c->d_fin queued on the case's
+// stream (output finished into d_pin), and the wait for its outcome
+fg_status solve_enqueue(fg_case *c, const double *p_old, const double *dpdn_g, const double *dpdn_d);
+fg_status solve_collect(fg_case *c, fg_solve_stats *st);
 }  // namespace fg

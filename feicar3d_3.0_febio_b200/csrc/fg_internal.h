@@ -179,6 +179,48 @@ struct KDesc {
   long long stride;  // elements from one vector to the next
 };
 constexpr int KR_MAXV = 16;  // most vectors one dot-product pass reads
+constexpr int KR_CS = KR_MAXV + 2;  // stride of the per-problem dot results and coefficients
+
+// The scalar side of FGMRES, kept on the device so a whole solve runs
+// without the host: per problem the Hessenberg matrix, the Givens rotations
+// and the rotated right-hand side; per batch the step counters and the
+// decisions the loop takes (which the host reads in direct mode, and CUDA
+// graph conditional nodes read in graph mode).
+struct KProb {
+  double H[KR_MAXV * KR_MAXV];  // H(i, j) at i * KR_MAXV + j, i <= j + 1 < m + 1
+  double g[KR_MAXV + 1];
+  double cs[KR_MAXV], sn[KR_MAXV];
+  double hcol[KR_MAXV + 1];  // column j of the current Arnoldi step
+  double f2, beta, relres;
+  int done, ncol;
+};
+constexpr int KR_HIST = 1024;
+struct KCtl {
+  int np, m;
+  int cycles, max_cycles;  // preconditioner applications so far / allowed
+  int j;                   // inner step in progress (vectors V_j -> V_{j+1})
+  int jlast;               // basis columns of the current restart cycle
+  int first;               // the next restart is the first (records |f|^2)
+  int status;              // FG_OK once every problem meets rtol
+  int outer;               // the restart just taken continues the solve
+  int inner;               // another inner step follows
+  int reorth;              // the current step takes a second Gram-Schmidt pass
+  int more;                // the next basis vector is staged as preconditioner input
+  int n_restart, n_body, n_inner, n_reorth;  // executed sections (launch counting)
+  double rtol;
+  double relres_max;       // worst true relative residual at the last restart
+  int nhist, pad_;
+  double hist[KR_HIST];    // worst residual (estimate) after each restart / step
+};
+// what a Krylov vector kernel reads its vector indices from (the step
+// counters of KCtl): see kidx() in fg_mg.cu
+enum : int {
+  KPH_RESTART = 0,    // resid into V_0, dots of V_0, stage V_0 / beta
+  KPH_APPLY = 1,      // Z_j, V_{j+1} = A Z_j, dots of V_{j+1} with V_0..V_j
+  KPH_REORTH = 2,     // V_{j+1} -= sum h_i V_i (second pass), no staging
+  KPH_NORMALIZE = 3,  // V_jlast = (W - sum h_i V_i) / h, staged when `more`
+  KPH_UPDATE = 4      // P += sum y_i Z_i over jlast columns
+};
 
 // A problem's small levels that one block cycles through (k_small_cycle):
 // levels [l0, l0 + nl) of a packed DevLevel table, the last one the
@@ -248,6 +290,14 @@ cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, lon
 // (Neumann) or reflect about ppp (Dirichlet) the first interior layer.
 // nx, ny, nz are node counts; lev0 is the host copy of the level-0
 // descriptor (its type array marks the pure-solid cells).
+// the known outer-face terms of the finest level's right-hand side
+// (Dirichlet values, Neumann gradient data); see k_face_rhs
+struct FaceData {
+  int pbc[6];
+  double ppp[6];
+  const double *pgrad[6];  // device face arrays or null (zero gradient)
+};
+cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaStream_t s);
 cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz,
                          const int *pbc, const double *ppp, int gauge, double *scratch,
                          cudaStream_t s);
@@ -279,6 +329,31 @@ cudaError_t kr_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0,
 template <typename B>
 cudaError_t kr_update(const Launch &flat, const KDesc *kd, int ns, const double *coef, int cs,
                       cudaStream_t s);
+// The same vector passes with their vector indices taken on the device from
+// ctl (phase KPH_*), so one captured launch serves every step of a loop.
+template <typename B, typename T>
+cudaError_t krd_apply(const Launch &quads, const DevRows &R, const DevLevel *lev0, const KDesc *kd,
+                      const KCtl *ctl, cudaStream_t s);
+template <typename B>
+cudaError_t krd_dots(const Launch &flat, const KDesc *kd, const KCtl *ctl, int phase, double *part,
+                     double *out, cudaStream_t s);
+template <typename B, typename T>
+cudaError_t krd_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0, const KDesc *kd,
+                      const KCtl *ctl, int phase, const double *coef, cudaStream_t s);
+template <typename B>
+cudaError_t krd_update(const Launch &flat, const KDesc *kd, const KCtl *ctl, const double *coef,
+                       cudaStream_t s);
+// scalar FGMRES steps (one block over all problems); with use_cond the
+// decisions are also written to the CUDA graph conditional handles
+cudaError_t fg_begin(KCtl *ctl, int np, int m, int max_cycles, double rtol, cudaStream_t s);
+cudaError_t fg_restart(KCtl *ctl, KProb *kp, const double *kout, const double *norm, double *coef,
+                       int use_cond, unsigned long long h_outer, unsigned long long h_body,
+                       unsigned long long h_inner, cudaStream_t s);
+cudaError_t fg_reorth_test(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+                           unsigned long long h_reorth, cudaStream_t s);
+cudaError_t fg_arnoldi(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+                       unsigned long long h_inner, cudaStream_t s);
+cudaError_t fg_lsq(KCtl *ctl, KProb *kp, double *coef, cudaStream_t s);
 }  // namespace k
 
 }  // namespace fg

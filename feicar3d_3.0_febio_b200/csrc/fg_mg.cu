@@ -2228,6 +2228,54 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
   return cudaGetLastError();
 }
 
+// Known boundary terms of the rows next to the outer faces, moved into the
+// right-hand side of the finest level (solution form).  A Dirichlet face
+// (CORE_SET_OUTER_BC.F90:1093-1170: ghost value 2 ppp - p(1)) couples the
+// row by a (p_ghost - p) = 2 a ppp - 2 a p: the operator holds -2 a p, the
+// right-hand side loses 2 a ppp.  A Neumann face with gradient data
+// (CORE_SET_OUTER_BC.F90:831-1042: ghost value p(1) -+ pgrad dxc) adds
+// +- pgrad / w, w the cell width along the face normal; pgrad arrays are
+// the reference's face arrays, (0:ny+1, 0:nz+1) for x faces, (0:nx+1,
+// 0:nz+1) for y faces, (0:nx+1, 0:ny+1) for z faces (node counts),
+// indexed by the face cell's two transverse reference indices.
+// blockIdx.y = face; threads cover the face's cells.
+__global__ void k_face_rhs(double *rhs, const DevLevel L, FaceData fd) {
+  const int f = blockIdx.y, a = f >> 1, up = f & 1;
+  const int n[3] = {L.nx, L.ny, L.nz};
+  const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;  // transverse axes
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n[u] * n[v]) return;
+  int idx[3];
+  idx[u] = 1 + (int)(e % n[u]);
+  idx[v] = 1 + (int)(e / n[u]);
+  idx[a] = up ? n[a] : 1;
+  const long long id = idx[0] + L.sy * idx[1] + L.sz * idx[2];
+  if (!(L.mask[id] & 64)) return;
+  double add = 0.0;
+  if (fd.pbc[f] == FG_PBC_DIRICHLET) {
+    const double am[3] = {L.amx[idx[0]], L.amy[idx[1]], L.amz[idx[2]]};
+    const double ap[3] = {L.apx[idx[0]], L.apy[idx[1]], L.apz[idx[2]]};
+    add = -2.0 * (up ? ap[a] : am[a]) * fd.ppp[f];
+  } else if (fd.pgrad[f]) {
+    const double w[3] = {L.wx[idx[0]], L.wy[idx[1]], L.wz[idx[2]]};
+    const long long stride = (long long)n[u] + 3;  // reference extent of the first transverse index
+    const double g = fd.pgrad[f][idx[u] + stride * idx[v]];
+    add = up ? -g / w[a] : g / w[a];
+  }
+  rhs[id] += add;
+}
+
+cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaStream_t s) {
+  bool any = false;
+  for (int f = 0; f < 6; ++f)
+    any |= (fd.pbc[f] == FG_PBC_DIRICHLET && fd.ppp[f] != 0.0) || (fd.pbc[f] != FG_PBC_DIRICHLET && fd.pgrad[f]);
+  if (!any) return cudaSuccess;
+  const long long m = std::max((long long)L0.ny * L0.nz, std::max((long long)L0.nx * L0.nz, (long long)L0.nx * L0.ny));
+  k_face_rhs<<<dim3((unsigned)((m + 255) / 256), 6), 256, 0, s>>>(rhs, L0, fd);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------- FGMRES
 // Vector v of a Krylov set (basis V or preconditioned Z) of one problem.
 template <typename B>
@@ -2256,6 +2304,25 @@ __device__ __forceinline__ double apply_row_d(const DevLevel &L, long long id, i
     else if (atb[q] && L.bc[q]) diag -= 2.0 * a[q];
   }
   return acc + diag * xc;
+}
+
+// Vector indices of a Krylov pass: the immediates, or, with ctl, those of
+// phase `ph` at the step counters of ctl (one captured launch then serves
+// every step of a device-side loop).
+struct KSel {
+  int vz, vw, nv, vd, s0, ns, stage;
+};
+__device__ __forceinline__ KSel kidx(const KCtl *ctl, int ph, KSel s) {
+  if (!ctl) return s;
+  const int j = ctl->j, jl = ctl->jlast;
+  switch (ph) {
+    case KPH_RESTART: s.vw = 0; s.nv = 0; s.vd = 0; s.s0 = 0; s.ns = 0; s.stage = 1; break;
+    case KPH_APPLY: s.vz = j; s.vw = j + 1; s.nv = j + 1; break;
+    case KPH_REORTH: s.vd = j + 1; s.s0 = 0; s.ns = j + 1; s.stage = 0; break;
+    case KPH_NORMALIZE: s.vd = jl; s.s0 = 0; s.ns = jl; s.stage = ctl->more; break;
+    default: s.ns = jl; break;  // KPH_UPDATE
+  }
+  return s;
 }
 
 // V_vd = F - A P on active rows, 0 on every other interior cell; part[b] =
@@ -2311,7 +2378,9 @@ k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
 // couple to (they are held at the staged zero), so A x_T equals A Z_vz.
 template <typename B, typename T>
 __global__ void __launch_bounds__(QBLOCK)
-k_kr_apply_q(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw) {
+k_kr_apply_q(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw,
+             const KCtl *ctl) {
+  if (ctl) { vz = ctl->j; vw = ctl->j + 1; }
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2364,7 +2433,15 @@ k_kr_apply_q(const int *off, int nent, const DevLevel *levs, const KDesc *kd, in
 // preconditioner: rd = rf = V_vs[t]
 template <typename B>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_kr_rows(DevRows R, const DevLevel *lev0, const KDesc *kd, int mode, int vs, int vd) {
+k_kr_rows(DevRows R, const DevLevel *lev0, const KDesc *kd, int mode, int vs, int vd, const KCtl *ctl,
+          int ph) {
+  if (ctl) {
+    if (mode == 1) { vs = ctl->j; vd = ctl->j + 1; }
+    if (mode == 2) {
+      if (ph == KPH_NORMALIZE && !ctl->more) return;  // nothing staged
+      vs = vd = ph == KPH_RESTART ? 0 : ctl->jlast;
+    }
+  }
   const int r = blockIdx.x * CELL_BLOCK + threadIdx.x;
   if (r >= R.n) return;
   const int p = R.prob[r];
@@ -2414,7 +2491,13 @@ __device__ __forceinline__ long long flat_end(long long n) { return 1 + 4 * ((n 
 // part[i * nblk + b], part[nv * nblk + b]
 template <typename B>
 __global__ void __launch_bounds__(FLAT_THREADS)
-k_kr_dots(const int *off, int nent, const KDesc *kd, int vw, int nv, int nblk, double *part) {
+k_kr_dots(const int *off, int nent, const KDesc *kd, int vw, int nv, int nblk, double *part,
+          const KCtl *ctl, int ph) {
+  {
+    const KSel ks = kidx(ctl, ph, KSel{0, vw, nv, 0, 0, 0, 0});
+    vw = ks.vw;
+    nv = ks.nv;
+  }
   const int p = find_entry(off, nent, blockIdx.x);
   const int lb = blockIdx.x - off[p];
   const KDesc &d = kd[p];
@@ -2482,8 +2565,10 @@ k_kr_dots(const int *off, int nent, const KDesc *kd, int vw, int nv, int nblk, d
 // out[p * ostride + i] = sum of part[i * nblk + off[p] .. off[p+1]) for
 // i < nsum (grid: problems x nsum)
 __global__ void __launch_bounds__(256)
-k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostride) {
+k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostride, const KCtl *ctl,
+            int ph) {
   const int p = blockIdx.x, i = blockIdx.y;
+  if (ctl && i > kidx(ctl, ph, KSel{0, 0, 0, 0, 0, 0, 0}).nv) return;  // grid sized for the most vectors
   double v = 0.0;
   for (int b = off[p] + threadIdx.x; b < off[p + 1]; b += 256) v += part[(size_t)i * nblk + b];
   __shared__ double red[8];
@@ -2503,7 +2588,11 @@ k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostri
 template <typename B, typename T>
 __global__ void __launch_bounds__(FLAT_THREADS)
 k_kr_vaxpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, int s0, int ns,
-           const double *coef, int cs, int stage) {
+           const double *coef, int cs, int stage, const KCtl *ctl, int ph) {
+  {
+    const KSel ks = kidx(ctl, ph, KSel{0, 0, 0, vd, s0, ns, stage});
+    vd = ks.vd; s0 = ks.s0; ns = ks.ns; stage = ks.stage;
+  }
   const int p = find_entry(off, nent, blockIdx.x);
   const int lb = blockIdx.x - off[p];
   const KDesc &d = kd[p];
@@ -2564,7 +2653,10 @@ k_kr_vaxpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
 // P += sum_{i<ns} c_{1+i} Z_i (c_0 is 1)
 template <typename B>
 __global__ void __launch_bounds__(FLAT_THREADS)
-k_kr_update(const int *off, int nent, const KDesc *kd, int ns, const double *coef, int cs) {
+k_kr_update(const int *off, int nent, const KDesc *kd, int ns, const double *coef, int cs,
+            const KCtl *ctl) {
+  if (ctl) ns = ctl->jlast;
+  if (ns == 0) return;
   const int p = find_entry(off, nent, blockIdx.x);
   const int lb = blockIdx.x - off[p];
   const KDesc &d = kd[p];
@@ -2606,7 +2698,7 @@ cudaError_t kr_resid(const Launch &quads, const DevRows &R, const DevLevel *lev0
   k_reduce_parts<<<quads.n, 1024, 0, s>>>(quads.off, part, norm2);
   note_launches(2);
   if (R.n > 0) {
-    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, 0, vd);
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 0, 0, vd, nullptr, 0);
     note_launches(1);
   }
   return cudaGetLastError();
@@ -2616,10 +2708,10 @@ template <typename B, typename T>
 cudaError_t kr_apply(const Launch &quads, const DevRows &R, const DevLevel *lev0, const KDesc *kd, int vz,
                      int vw, cudaStream_t s) {
   if (quads.empty()) return cudaSuccess;
-  k_kr_apply_q<B, T><<<quads.blocks, QBLOCK, 0, s>>>(quads.off, quads.n, quads.lev, kd, vz, vw);
+  k_kr_apply_q<B, T><<<quads.blocks, QBLOCK, 0, s>>>(quads.off, quads.n, quads.lev, kd, vz, vw, nullptr);
   note_launches(1);
   if (R.n > 0) {
-    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vz, vw);
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, vz, vw, nullptr, 0);
     note_launches(1);
   }
   return cudaGetLastError();
@@ -2630,8 +2722,9 @@ cudaError_t kr_dots(const Launch &flat, const KDesc *kd, int vw, int nv, double 
                     int ostride, cudaStream_t s) {
   if (flat.empty()) return cudaSuccess;
   if (nv > KR_MAXV) return cudaErrorInvalidValue;
-  k_kr_dots<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, vw, nv, flat.blocks, part);
-  k_kr_reduce<<<dim3(flat.n, nv + 1), 256, 0, s>>>(flat.off, part, flat.blocks, out, ostride);
+  k_kr_dots<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, vw, nv, flat.blocks, part,
+                                                    nullptr, 0);
+  k_kr_reduce<<<dim3(flat.n, nv + 1), 256, 0, s>>>(flat.off, part, flat.blocks, out, ostride, nullptr, 0);
   note_launches(2);
   return cudaGetLastError();
 }
@@ -2642,10 +2735,10 @@ cudaError_t kr_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0,
   if (flat.empty()) return cudaSuccess;
   if (ns > KR_MAXV) return cudaErrorInvalidValue;
   k_kr_vaxpy<B, T><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, flat.lev, kd, vd, s0, ns, coef,
-                                                        cs, stage ? 1 : 0);
+                                                        cs, stage ? 1 : 0, nullptr, 0);
   note_launches(1);
   if (stage && R.n > 0) {
-    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, vd, vd);
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, vd, vd, nullptr, 0);
     note_launches(1);
   }
   return cudaGetLastError();
@@ -2656,7 +2749,7 @@ cudaError_t kr_update(const Launch &flat, const KDesc *kd, int ns, const double 
                       cudaStream_t s) {
   if (flat.empty() || ns == 0) return cudaSuccess;
   if (ns > KR_MAXV) return cudaErrorInvalidValue;
-  k_kr_update<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, ns, coef, cs);
+  k_kr_update<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, ns, coef, cs, nullptr);
   note_launches(1);
   return cudaGetLastError();
 }
@@ -2680,6 +2773,304 @@ template cudaError_t kr_vaxpy<double, double>(const Launch &, const DevRows &, c
                                               cudaStream_t);
 template cudaError_t kr_update<float>(const Launch &, const KDesc *, int, const double *, int, cudaStream_t);
 template cudaError_t kr_update<double>(const Launch &, const KDesc *, int, const double *, int, cudaStream_t);
+
+// ---- the same passes with their indices read on the device (phase KPH_*)
+template <typename B, typename T>
+cudaError_t krd_apply(const Launch &quads, const DevRows &R, const DevLevel *lev0, const KDesc *kd,
+                      const KCtl *ctl, cudaStream_t s) {
+  if (quads.empty()) return cudaSuccess;
+  k_kr_apply_q<B, T><<<quads.blocks, QBLOCK, 0, s>>>(quads.off, quads.n, quads.lev, kd, 0, 0, ctl);
+  note_launches(1);
+  if (R.n > 0) {
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 1, 0, 0, ctl, KPH_APPLY);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+template <typename B>
+cudaError_t krd_dots(const Launch &flat, const KDesc *kd, const KCtl *ctl, int phase, double *part,
+                     double *out, cudaStream_t s) {
+  if (flat.empty()) return cudaSuccess;
+  k_kr_dots<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, 0, 0, flat.blocks, part, ctl,
+                                                    phase);
+  k_kr_reduce<<<dim3(flat.n, KR_MAXV + 1), 256, 0, s>>>(flat.off, part, flat.blocks, out, KR_CS, ctl, phase);
+  note_launches(2);
+  return cudaGetLastError();
+}
+
+template <typename B, typename T>
+cudaError_t krd_vaxpy(const Launch &flat, const DevRows &R, const DevLevel *lev0, const KDesc *kd,
+                      const KCtl *ctl, int phase, const double *coef, cudaStream_t s) {
+  if (flat.empty()) return cudaSuccess;
+  k_kr_vaxpy<B, T><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, flat.lev, kd, 0, 0, 0, coef, KR_CS,
+                                                        0, ctl, phase);
+  note_launches(1);
+  if (phase != KPH_REORTH && R.n > 0) {  // staged row constants (skipped on the device when not staged)
+    k_kr_rows<B><<<rows_blocks(R), CELL_BLOCK, 0, s>>>(R, lev0, kd, 2, 0, 0, ctl, phase);
+    note_launches(1);
+  }
+  return cudaGetLastError();
+}
+
+template <typename B>
+cudaError_t krd_update(const Launch &flat, const KDesc *kd, const KCtl *ctl, const double *coef,
+                       cudaStream_t s) {
+  if (flat.empty()) return cudaSuccess;
+  k_kr_update<B><<<flat.blocks, FLAT_THREADS, 0, s>>>(flat.off, flat.n, kd, 0, coef, KR_CS, ctl);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+template cudaError_t krd_apply<float, float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *,
+                                             const KCtl *, cudaStream_t);
+template cudaError_t krd_apply<double, double>(const Launch &, const DevRows &, const DevLevel *,
+                                               const KDesc *, const KCtl *, cudaStream_t);
+template cudaError_t krd_dots<float>(const Launch &, const KDesc *, const KCtl *, int, double *, double *,
+                                     cudaStream_t);
+template cudaError_t krd_dots<double>(const Launch &, const KDesc *, const KCtl *, int, double *, double *,
+                                      cudaStream_t);
+template cudaError_t krd_vaxpy<float, float>(const Launch &, const DevRows &, const DevLevel *, const KDesc *,
+                                             const KCtl *, int, const double *, cudaStream_t);
+template cudaError_t krd_vaxpy<double, double>(const Launch &, const DevRows &, const DevLevel *,
+                                               const KDesc *, const KCtl *, int, const double *, cudaStream_t);
+template cudaError_t krd_update<float>(const Launch &, const KDesc *, const KCtl *, const double *,
+                                       cudaStream_t);
+template cudaError_t krd_update<double>(const Launch &, const KDesc *, const KCtl *, const double *,
+                                        cudaStream_t);
+
+// ---- scalar FGMRES steps: one block, problem p on thread p (mod 256)
+constexpr int FG_SCALAR_THREADS = 256;
+
+// Second Gram-Schmidt pass when the first leaves less than this fraction of
+// |w|^2.  With a V-cycle preconditioner w = A M^-1 v_j lies mostly in the
+// span of the basis, so the usual 1/2 test asks for the second pass on
+// almost every step; at 1e-4 the FP32 basis of small sphere and ellipsoid
+// problems loses enough orthogonality to cost two extra cycles, at 1e-2
+// they keep theirs and the large box case its time; without any second
+// pass the strict convergence cases stall.
+constexpr double kReorth = 1e-2;
+
+__device__ __forceinline__ void hist_push(KCtl *ctl, double v) {
+  if (ctl->nhist < KR_HIST) ctl->hist[ctl->nhist] = v;
+  ctl->nhist++;
+}
+
+// block-wide AND of `flag` and max of `v` (non-negative) over the threads
+__device__ __forceinline__ void block_all_max(int &flag, double &v) {
+  __shared__ int s_flag[FG_SCALAR_THREADS / 32];
+  __shared__ double s_v[FG_SCALAR_THREADS / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  flag = __all_sync(0xffffffffu, flag);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  if (l == 0) { s_flag[w] = flag; s_v[w] = v; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < FG_SCALAR_THREADS / 32; ++q) { flag = flag && s_flag[q]; v = fmax(v, s_v[q]); }
+  }
+}
+
+__global__ void __launch_bounds__(FG_SCALAR_THREADS) k_fg_begin(KCtl *ctl, int np, int m, int max_cycles,
+                                                                 double rtol) {
+  if (threadIdx.x != 0) return;
+  ctl->np = np; ctl->m = m; ctl->max_cycles = max_cycles; ctl->rtol = rtol;
+  ctl->cycles = 0; ctl->j = 0; ctl->jlast = 0; ctl->first = 1; ctl->status = FG_NOT_CONVERGED;
+  ctl->outer = 1; ctl->inner = 0; ctl->reorth = 0; ctl->more = 0;
+  ctl->n_restart = 0; ctl->n_body = 0; ctl->n_inner = 0; ctl->n_reorth = 0;
+  ctl->relres_max = 0.0; ctl->nhist = 0;
+}
+
+// After the true residual V_0 = F - A P: per problem |f|^2 (first restart),
+// the relative residual, beta = |V_0| and whether it is done; the solve
+// continues unless every problem meets rtol or the cycles are used up.
+// Stages the coefficients of V_0 / beta and resets the rotated system.
+__global__ void __launch_bounds__(FG_SCALAR_THREADS)
+k_fg_restart(KCtl *ctl, KProb *kp, const double *kout, const double *norm, double *coef, int use_cond,
+             cudaGraphConditionalHandle h_outer, cudaGraphConditionalHandle h_body,
+             cudaGraphConditionalHandle h_inner) {
+  const int np = ctl->np, m = ctl->m;
+  const int first = ctl->first;
+  const double rtol = ctl->rtol;
+  int all = 1;
+  double worst = 0.0;
+  for (int p = threadIdx.x; p < np; p += FG_SCALAR_THREADS) {
+    KProb &q = kp[p];
+    if (first) q.f2 = norm[np + p];
+    q.relres = q.f2 > 0.0 ? sqrt(norm[p] / q.f2) : sqrt(norm[p]);
+    q.beta = sqrt(fmax(0.0, kout[(size_t)p * KR_CS]));
+    q.done = (q.relres <= rtol || q.beta == 0.0) ? 1 : 0;
+    worst = fmax(worst, q.relres);
+    if (!q.done) all = 0;
+    double *cf = coef + (size_t)p * KR_CS;
+    cf[0] = q.done ? 0.0 : 1.0 / q.beta;
+    q.ncol = 0;
+    for (int i = 0; i <= m; ++i) q.g[i] = 0.0;
+    q.g[0] = q.beta;
+  }
+  block_all_max(all, worst);
+  if (threadIdx.x == 0) {
+    ctl->first = 0;
+    hist_push(ctl, worst);
+    ctl->relres_max = worst;
+    ctl->n_restart++;
+    int outer = 1;
+    if (all) { ctl->status = FG_OK; outer = 0; }
+    else if (ctl->cycles >= ctl->max_cycles) outer = 0;
+    ctl->outer = outer;
+    ctl->inner = outer;
+    ctl->j = 0;
+    ctl->jlast = 0;
+    if (outer) ctl->n_body++;
+    if (use_cond) {
+      cudaGraphSetConditional(h_outer, outer);
+      cudaGraphSetConditional(h_body, outer);
+      cudaGraphSetConditional(h_inner, outer);
+    }
+  }
+}
+
+// After the first Gram-Schmidt dots of step j: the Hessenberg column, and
+// whether any problem needs the second pass (its coefficients staged).
+__global__ void __launch_bounds__(FG_SCALAR_THREADS)
+k_fg_reorth_test(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+                 cudaGraphConditionalHandle h_reorth) {
+  const int np = ctl->np, j = ctl->j;
+  int none = 1;
+  double dummy = 0.0;
+  for (int p = threadIdx.x; p < np; p += FG_SCALAR_THREADS) {
+    KProb &q = kp[p];
+    const double *o = kout + (size_t)p * KR_CS;
+    double sum = 0.0;
+    for (int i = 0; i <= j; ++i) { q.hcol[i] = o[i]; sum += o[i] * o[i]; }
+    const double ww = o[j + 1];
+    if (!q.done && ww - sum < kReorth * ww) none = 0;
+    double *cf = coef + (size_t)p * KR_CS;
+    cf[0] = 1.0;
+    for (int i = 0; i <= j; ++i) cf[1 + i] = q.done ? 0.0 : -q.hcol[i];
+  }
+  block_all_max(none, dummy);
+  if (threadIdx.x == 0) {
+    ctl->cycles++;  // the V-cycle of this step
+    ctl->reorth = none ? 0 : 1;
+    if (!none) ctl->n_reorth++;
+    if (use_cond) cudaGraphSetConditional(h_reorth, none ? 0u : 1u);
+  }
+}
+
+// Normalises step j: h_{j+1,j}, the rotations, the rotated right-hand
+// side, the residual estimate; stages the coefficients of
+// V_{j+1} = (W - sum h_i V_i) / h_{j+1,j}; decides whether another inner
+// step follows.
+__global__ void __launch_bounds__(FG_SCALAR_THREADS)
+k_fg_arnoldi(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+             cudaGraphConditionalHandle h_inner) {
+  const int np = ctl->np, j = ctl->j, m = ctl->m, reorth = ctl->reorth;
+  const double rtol = ctl->rtol;
+  int inner_done = 1;
+  double west = 0.0;
+  for (int p = threadIdx.x; p < np; p += FG_SCALAR_THREADS) {
+    KProb &q = kp[p];
+    double *cf = coef + (size_t)p * KR_CS;
+    const double *o = kout + (size_t)p * KR_CS;
+    double sum = 0.0;
+    for (int i = 0; i <= j; ++i) {
+      const double hi = o[i];  // second-pass corrections when reorthogonalised
+      if (reorth) q.hcol[i] += hi;
+      sum += hi * hi;
+    }
+    const double h2 = o[j + 1] - sum;
+    const double hn = h2 > 0.0 ? sqrt(h2) : 0.0;
+    q.hcol[j + 1] = hn;
+    const bool brk = q.done || !(hn > 1e-14 * q.beta);
+    cf[0] = brk ? 0.0 : 1.0 / hn;
+    for (int i = 0; i <= j; ++i) cf[1 + i] = brk ? 0.0 : -o[i] / hn;
+    if (!q.done) {
+      for (int i = 0; i <= j + 1; ++i) q.H[i * KR_MAXV + j] = q.hcol[i];
+      for (int i = 0; i < j; ++i) {
+        const double c = q.cs[i], sv = q.sn[i];
+        const double h0 = q.H[i * KR_MAXV + j], h1 = q.H[(i + 1) * KR_MAXV + j];
+        q.H[i * KR_MAXV + j] = c * h0 + sv * h1;
+        q.H[(i + 1) * KR_MAXV + j] = -sv * h0 + c * h1;
+      }
+      const double a = q.H[j * KR_MAXV + j], bb = q.H[(j + 1) * KR_MAXV + j];
+      const double rr = hypot(a, bb);
+      const double c = rr > 0.0 ? a / rr : 1.0, sv = rr > 0.0 ? bb / rr : 0.0;
+      q.cs[j] = c; q.sn[j] = sv;
+      q.H[j * KR_MAXV + j] = rr; q.H[(j + 1) * KR_MAXV + j] = 0.0;
+      q.g[j + 1] = -sv * q.g[j];
+      q.g[j] = c * q.g[j];
+      q.ncol = j + 1;
+      if (brk) q.done = 1;
+    }
+    // residual estimate |g_ncol| (all rows) over the fluid-row |f|
+    const double est = fabs(q.g[q.ncol]);
+    const double rel = q.f2 > 0.0 ? est / sqrt(q.f2) : est;
+    west = fmax(west, rel);
+    if (!(q.done || rel <= 0.5 * rtol)) inner_done = 0;
+  }
+  block_all_max(inner_done, west);
+  if (threadIdx.x == 0) {
+    hist_push(ctl, west);
+    ctl->jlast = j + 1;
+    ctl->j = j + 1;
+    const int more = (!inner_done && j + 1 < m && ctl->cycles < ctl->max_cycles) ? 1 : 0;
+    ctl->more = more;
+    ctl->inner = more;
+    ctl->n_inner++;
+    if (use_cond) cudaGraphSetConditional(h_inner, more);
+  }
+}
+
+// End of a restart cycle: y from the rotated Hessenberg system (back
+// substitution), staged as the coefficients of P += sum y_i Z_i.
+__global__ void __launch_bounds__(FG_SCALAR_THREADS) k_fg_lsq(KCtl *ctl, KProb *kp, double *coef) {
+  const int np = ctl->np;
+  for (int p = threadIdx.x; p < np; p += FG_SCALAR_THREADS) {
+    const KProb &q = kp[p];
+    double *cf = coef + (size_t)p * KR_CS;
+    for (int i = 0; i < KR_CS; ++i) cf[i] = 0.0;
+    cf[0] = 1.0;
+    const int nc = q.ncol;
+    double y[KR_MAXV];
+    for (int i = nc - 1; i >= 0; --i) {
+      double v = q.g[i];
+      for (int r = i + 1; r < nc; ++r) v -= q.H[i * KR_MAXV + r] * y[r];
+      y[i] = q.H[i * KR_MAXV + i] != 0.0 ? v / q.H[i * KR_MAXV + i] : 0.0;
+    }
+    for (int i = 0; i < nc; ++i) cf[1 + i] = y[i];
+  }
+}
+
+cudaError_t fg_begin(KCtl *ctl, int np, int m, int max_cycles, double rtol, cudaStream_t s) {
+  k_fg_begin<<<1, FG_SCALAR_THREADS, 0, s>>>(ctl, np, m, max_cycles, rtol);
+  note_launches(1);
+  return cudaGetLastError();
+}
+cudaError_t fg_restart(KCtl *ctl, KProb *kp, const double *kout, const double *norm, double *coef,
+                       int use_cond, unsigned long long h_outer, unsigned long long h_body,
+                       unsigned long long h_inner, cudaStream_t s) {
+  k_fg_restart<<<1, FG_SCALAR_THREADS, 0, s>>>(ctl, kp, kout, norm, coef, use_cond, h_outer, h_body, h_inner);
+  note_launches(1);
+  return cudaGetLastError();
+}
+cudaError_t fg_reorth_test(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+                           unsigned long long h_reorth, cudaStream_t s) {
+  k_fg_reorth_test<<<1, FG_SCALAR_THREADS, 0, s>>>(ctl, kp, kout, coef, use_cond, h_reorth);
+  note_launches(1);
+  return cudaGetLastError();
+}
+cudaError_t fg_arnoldi(KCtl *ctl, KProb *kp, const double *kout, double *coef, int use_cond,
+                       unsigned long long h_inner, cudaStream_t s) {
+  k_fg_arnoldi<<<1, FG_SCALAR_THREADS, 0, s>>>(ctl, kp, kout, coef, use_cond, h_inner);
+  note_launches(1);
+  return cudaGetLastError();
+}
+cudaError_t fg_lsq(KCtl *ctl, KProb *kp, double *coef, cudaStream_t s) {
+  k_fg_lsq<<<1, FG_SCALAR_THREADS, 0, s>>>(ctl, kp, coef);
+  note_launches(1);
+  return cudaGetLastError();
+}
 
 #ifdef FG_CHECKED
 // first recorded out-of-range access of a checked build: {hits, index,

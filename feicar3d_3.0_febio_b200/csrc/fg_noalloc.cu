@@ -101,12 +101,27 @@ extern "C" fg_status fg_rows_relax_noalloc(int nx, int ny, int nz, double *d_p, 
   }
   if (nrows == 0 || iterations == 0) return FG_OK;
   if (!d_p || !d_tgt || !d_cell || !d_w) return FG_BAD_INPUT;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (s) {
+    // the scratch address below is the current device's: a stream of
+    // another device would run the kernels where that address means nothing
+    int cur = 0, sdev = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e == cudaSuccess) e = cudaStreamGetDevice(s, &sdev);
+    if (e != cudaSuccess) {
+      fg::set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+      return FG_CUDA_ERROR;
+    }
+    if (sdev != cur) {
+      fg::set_last_error("stream belongs to another device than the current one", __FILE__, __LINE__);
+      return FG_BAD_INPUT;
+    }
+  }
   double *scratch = nullptr;
   fg_status st = fg::scratch_address(&scratch);
   if (st != FG_OK) return st;
   const long long sy = (long long)nx + 2, sz = sy * ((long long)ny + 2);
   const long long nref = sz * ((long long)nz + 2);
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int threads = 128, blocks = (nrows + threads - 1) / threads;
   for (int it = 0; it < iterations; ++it) {
     fg::k_gather<<<blocks, threads, 0, s>>>(d_p, nref, sy, sz, nrows, d_tgt, d_cell, d_w, d_c0, scratch);

@@ -128,6 +128,7 @@ def lib():
         L.fg_case_set_stream.argtypes = [vp, vp]
         L.fg_launch_count.argtypes = [C.POINTER(C.c_longlong)]
         L.fg_case_profile.argtypes = [vp, ip]
+        L.fg_case_solve_mode.argtypes = [vp, C.POINTER(C.c_int)]
         L.fg_case_history.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         L.fg_case_profile_read.argtypes = [vp, C.POINTER(Profile)]
         for name in ["fg_device_count", "fg_case_create", "fg_case_destroy", "fg_case_levels",
@@ -137,7 +138,7 @@ def lib():
                      "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
                      "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy", "fg_case_set_stream",
                      "fg_launch_count", "fg_case_profile", "fg_case_profile_read",
-                     "fg_case_history"]:
+                     "fg_case_history", "fg_case_solve_mode"]:
             getattr(L, name).restype = ip
         _lib = L
     return _lib
@@ -320,6 +321,13 @@ class Case:
         out = np.zeros(n.value)
         _check(lib().fg_case_history(self.h, _p(out), n.value, C.byref(n)), "fg_case_history")
         return out
+
+    def solve_mode(self) -> int:
+        """1 when the last solve was one CUDA graph launch, 0 when the host
+        drove its kernels step by step."""
+        m = C.c_int(0)
+        _check(lib().fg_case_solve_mode(self.h, C.byref(m)), "fg_case_solve_mode")
+        return m.value
 
     def profile(self, enable=True):
         _check(lib().fg_case_profile(self.h, 1 if enable else 0), "fg_case_profile")

@@ -189,6 +189,12 @@ typedef struct fg_profile {
  * reference prints its per-cycle MG residuals with infoconv = 1,
  * CORE_MG.F90:1811-1813): *count = cycles, relres[0..capacity-1] filled. */
 fg_status fg_case_history(const fg_case *c, double *relres, int capacity, int *count);
+/* How the last solve on c ran: *mode = 1 when the whole FGMRES solve was
+ * one CUDA graph launch (its loops are graph conditional nodes decided on
+ * the device, the host waits once at the end), 0 when the host drove the
+ * same kernels step by step (launch-class timing on, the caller's stream
+ * being captured, Richardson outer iteration, or a failed capture). */
+fg_status fg_case_solve_mode(const fg_case *c, int *mode);
 /* enable != 0: later solves on c bracket each launch group with CUDA
  * events on the handle's stream; resets the totals. */
 fg_status fg_case_profile(fg_case *c, int enable);
@@ -208,14 +214,19 @@ fg_status fg_case_profile_read(const fg_case *c, fg_profile *out);
  * element cell[r], in the order of GCM_MEMORY_ALLOCATE.F90:593-623 (a
  * target's own corner carries weight 0); all rows of a pass read the
  * field before any row writes it.  tgt and cell are element indices of
- * the field; rows whose indices leave the field are skipped.  d_c0 may be
- * NULL (all zero).  Work is queued on `stream` (a cudaStream_t, NULL for
- * the default stream) and the call returns without waiting.
+ * the field; rows whose indices leave the field are skipped, and the call
+ * does not report them (it returns FG_OK): the caller validates its row
+ * lists.  d_c0 may be NULL (all zero).  Work is queued on `stream` (a
+ * cudaStream_t of the current device, NULL for the default stream; a
+ * stream of another device returns FG_BAD_INPUT) and the call returns
+ * without waiting.
  * Scratch: a fixed device array of FG_NOALLOC_MAX_ROWS doubles (2 MiB),
  * present on every GPU that loads the library until the process exits;
  * nrows > FG_NOALLOC_MAX_ROWS returns FG_BAD_INPUT.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress), so
- * make the first call on each device before any stream capture.  Every
+ * device looks up that array's device address (cudaGetSymbolAddress) and
+ * keeps it for the life of the process, so make the first call on each
+ * device before any stream capture, and do not call cudaDeviceReset on a
+ * device after its first call (the kept address would be stale).  Every
  * call on a device shares the one array: calls that overlap on the GPU
  * (other streams, other host threads) race and must be ordered by the
  * caller.  Nothing in it needs to start at zero -- each pass writes every

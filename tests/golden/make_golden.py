@@ -1,6 +1,7 @@
 """Writes the oracle's golden fixtures (run from the repository root):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # everything
+    python tests/golden/make_golden.py more     # benched_digests.json only
 
 For config 0 (128x64x64, sphere) and config 2 (256x128x128, pitching
 membrane plate) at steps 0 and 25: SHA-256 digests of iblank,
@@ -85,6 +86,44 @@ def main():
     with open(os.path.join(OUT, "tagging_digests.json"), "w") as f:
         json.dump(gold, f, indent=1, sort_keys=True)
     print(json.dumps({k: (v["nGhost"], v["nDead"]) for k, v in gold.items()}))
+    more_goldens()
+
+
+# problems of the 64-problem batch whose tagging is pinned (edges 32, 35,
+# 45 and 81 cells)
+BATCH_PICK = (4, 9, 3, 0)
+
+
+def more_goldens():
+    """Digests of the benched geometries: config 1 (512x256x256 stretched,
+    81920-triangle sphere), all 100 steps of the config-2 pitching plate
+    (each tagged from scratch at its position), and four problems of the
+    64-problem batch."""
+    gold = {}
+    oc = oracle_tag(synth.config1_grid(), synth.config1_body())
+    gold["config1"] = tagging_digests(oc.field(0), oc.field(1), oc.field(2), oc.ghosts(), oc.deads())
+    del oc
+    steps = []
+    for step in range(100):
+        oc2 = oracle_tag(synth.config2_grid(), synth.config2_body(step))
+        steps.append(tagging_digests(oc2.field(0), oc2.field(1), oc2.field(2), oc2.ghosts(), oc2.deads()))
+    gold["config2_steps"] = steps
+    probs = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)
+    gold["batch64"] = {}
+    for i in BATCH_PICK:
+        g, b, _ = probs[i]
+        ocb = oracle_tag(g, b)
+        gold["batch64"][str(i)] = tagging_digests(ocb.field(0), ocb.field(1), ocb.field(2), ocb.ghosts(),
+                                                  ocb.deads())
+    with open(os.path.join(OUT, "benched_digests.json"), "w") as f:
+        json.dump(gold, f, indent=1, sort_keys=True)
+    print(json.dumps({"config1": (gold["config1"]["nGhost"], gold["config1"]["nDead"]),
+                      "batch64": {k: (v["nGhost"], v["nDead"]) for k, v in gold["batch64"].items()}}))
+
+
+if __name__ == "__main__" and len(sys.argv) > 1 and sys.argv[1] == "more":
+    more_goldens()
+    sys.exit(0)
 
 
 if __name__ == "__main__":

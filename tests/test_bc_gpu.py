@@ -1,0 +1,105 @@
+"""Boundary data on the device path against the oracle.
+
+* The ghost/dead-cell update alone (fg_ghostcell_pressure against
+  GCM_ghostcell_pressure, GCM_GHOSTCELL_UPDATE.F90:361-739): both iterate
+  the interpolation rows with the fluid values held, so both reach the same
+  ghost and dead values.
+* A Dirichlet outer face (CORE_SET_OUTER_BC.F90:831-1186: the ghost layer
+  reflects about the face value) together with inhomogeneous Neumann data
+  on the body (dp/dn on every ghost and dead row, GCM_GHOSTCELL_UPDATE.F90
+  :522 and :596-597): the converged pressure of the FP64 and mixed paths
+  against the oracle's converged solve_poisson.  The Dirichlet face fixes
+  the constant, so the fields are compared as they are.
+
+Tolerance: 1e-12 relative for the row update, 1e-9 relative L2 on fluid
+cells for the solves (rtol 1e-12 on the device).
+"""
+import numpy as np
+import pytest
+
+from feicar_b200 import fg, synth
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _tagged(grid, bodies):
+    oc = O.OracleCase(grid)
+    for b in bodies:
+        oc.add_body(b)
+    oc.set_iblank()
+    oc.gcm(2.0, 2.0)
+    return oc
+
+
+def _device_case(grid, bodies, **kw):
+    c = fg.Case(grid, fg.default_config(**kw))
+    for b in bodies:
+        c.add_body(b)
+    c.set_iblank_body_fast()
+    c.gcm_set_internal_boundary()
+    c.mg_prepare()
+    return c
+
+
+GEOM = (synth.small_grid(32, 16, 16, (4.0, 2.0, 2.0)), [synth.sphere_body((1.0, 1.0, 1.0), 1.0, 3)])
+
+
+def test_ghostcell_pressure_matches_oracle():
+    grid, bodies = GEOM
+    oc = _tagged(grid, bodies)
+    c = _device_case(grid, bodies)
+    rng = np.random.default_rng(3)
+    p0 = np.asfortranarray(rng.standard_normal(grid.shape))
+    want = p0.copy(order="F")
+    rc, its = oc.ghostcell_pressure(want, np.zeros(grid.shape, order="F"), None,
+                                    O.default_params(restol_gcp=1e-15, itermax_gc=2000))
+    got = p0.copy(order="F")
+    c.ghostcell_pressure(got, iterations=400)
+    rows = np.zeros(grid.shape, bool)
+    for R in (oc.ghosts(), oc.deads()):
+        rows[R["ijk"][:, 0], R["ijk"][:, 1], R["ijk"][:, 2]] = True
+    assert rows.sum() > 0
+    assert np.array_equal(got[~rows], p0[~rows])  # nothing but the rows moves
+    scale = float(np.abs(want[rows]).max())
+    assert np.abs(got[rows] - want[rows]).max() <= 1e-12 * scale
+    c.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+@pytest.mark.parametrize("variant", ["dirichlet", "dpdn", "both"])
+def test_dirichlet_face_and_body_dpdn_match_oracle(variant, prec):
+    """variant: a Dirichlet value on the x = L face alone (homogeneous body
+    data), dp/dn data on the body alone (the face's Dirichlet value 0), or
+    both."""
+    grid, bodies = GEOM
+    oc = _tagged(grid, bodies)
+    ib, gh = oc.field(0), oc.field(1)
+    rng = np.random.default_rng(11)
+    fluid = np.zeros(grid.shape, bool)
+    fluid[1:grid.nx, 1:grid.ny, 1:grid.nz] = (ib[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0) & \
+                                            (gh[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0)
+    div = np.asfortranarray(synth.box_smooth(rng.standard_normal(grid.shape)) * fluid)
+    ng, nd = len(oc.ghosts()["ijk"]), len(oc.deads()["ijk"])
+    dpdn_g = 0.1 * rng.standard_normal(ng) if variant != "dirichlet" else None
+    dpdn_d = 0.1 * rng.standard_normal(nd) if variant != "dirichlet" else None
+    pbc = [fg.FG_PBC_NEUMANN] * 6
+    pbc[1] = fg.FG_PBC_DIRICHLET  # x = L outflow face
+    ppp = [0.0, 0.25 if variant != "dpdn" else 0.0, 0.0, 0.0, 0.0, 0.0]
+    po = np.zeros(grid.shape, order="F")
+    rc, ost = oc.solve_poisson(po, div, params=O.default_params(
+        restol_pson=1e-14, restol_gcp=1e-14, itermax_pson=3000, pbc=pbc, ppp=ppp, is_PBC_homogeneous=0),
+        dpdn_g=dpdn_g, dpdn_d=dpdn_d)
+    assert ost["relres"] <= 1e-10, ost
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    c = _device_case(grid, bodies, precision=p_, rtol=1e-12, max_cycles=200, pbc=pbc, ppp=ppp)
+    p = np.zeros(grid.shape, order="F")
+    st = c.solve_poisson(p, div, dpdn_ghost=dpdn_g, dpdn_dead=dpdn_d)
+    assert st["relres"] <= 1e-12
+    m = ib == 0
+    m[0, :, :] = m[-1, :, :] = False
+    m[:, 0, :] = m[:, -1, :] = False
+    m[:, :, 0] = m[:, :, -1] = False
+    err = np.linalg.norm(p[m] - po[m]) / np.linalg.norm(po[m])
+    assert err <= 1e-9, (variant, err, st, ost)
+    c.close()

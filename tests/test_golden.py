@@ -3,9 +3,10 @@
 CPU: the oracle reproduces its committed digests (regression of the
 restatement).  GPU: the device tagging reproduces the same digests --
 iblank, ghostCellMark, dead_cell and every ghost/dead list array bit for
-bit -- on config 0 and on the config-2 pitching plate at steps 0 and 25
-(the second reached by moving the body of the same handle), and the
-converged config-0 pressure matches the oracle's sample to 1e-9.
+bit -- on config 0, on the headline 512x256x256 stretched sphere, on all
+100 steps of the config-2 pitching plate (moved on one handle) and on
+four problems of the 64-problem batch; and the converged config-0
+pressure matches the oracle's sample to 1e-9.
 """
 import importlib.util
 import json
@@ -91,20 +92,58 @@ def test_device_config0_pressure_sample(prec):
     c.close()
 
 
+# ---- the benched geometries (tests/golden/benched_digests.json)
+BENCHED = json.load(open(os.path.join(HERE, "golden", "benched_digests.json")))
+
+
+@pytest.mark.parametrize("i", ["4", "9"])
+def test_oracle_batch64_digests(i):
+    g, b, _ = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)[int(i)]
+    assert _oracle_digests(g, b) == BENCHED["batch64"][i]
+
+
+@pytest.mark.parametrize("step", [50, 75])
+def test_oracle_config2_step_digests(step):
+    assert _oracle_digests(synth.config2_grid(), synth.config2_body(step)) == BENCHED["config2_steps"][step]
+
+
 @pytest.mark.gpu
-def test_device_config2_plate_steps_match_oracle():
-    """The pitching plate moved step by step through one handle (as the
-    time loop re-tags it): iblank, ghostCellMark, dead_cell and the ghost /
-    dead lists equal the oracle's at further points of the period, on both
-    sides of the neutral position and on the way back."""
+def test_device_config1_digests():
+    """The headline geometry: 512x256x256 cells tanh-stretched in y and z,
+    an 81920-triangle sphere; iblank, ghostCellMark, dead_cell and every
+    ghost/dead list array equal the oracle's bit for bit."""
+    c = fg.Case(synth.config1_grid(), fg.default_config())
+    c.add_body(synth.config1_body())
+    c.set_iblank_body_fast()
+    assert _device_digests(c) == BENCHED["config1"]
+    c.close()
+
+
+@pytest.mark.gpu
+def test_device_config2_all_steps_digests():
+    """All 100 steps of the pitching plate, moved step by step on one
+    handle as the time loop does, against the oracle tagging each position
+    from scratch."""
     base = synth.config2_plate()
-    grid = synth.config2_grid()
-    c = fg.Case(grid, fg.default_config())
+    c = fg.Case(synth.config2_grid(), fg.default_config())
     c.add_body(synth.config2_body(0))
-    for step in range(0, 80):
+    bad = []
+    for step in range(100):
         if step:
             c.update_body(0, synth.config2_verts(base, step))
         c.set_iblank_body_fast()
-        if step in (10, 40, 60, 79):
-            assert _device_digests(c) == _oracle_digests(grid, synth.config2_body(step)), step
+        if _device_digests(c) != BENCHED["config2_steps"][step]:
+            bad.append(step)
+    c.close()
+    assert not bad, bad
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("i", sorted(BENCHED["batch64"]))
+def test_device_batch64_digests(i):
+    g, b, _ = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)[int(i)]
+    c = fg.Case(g, fg.default_config())
+    c.add_body(b)
+    c.set_iblank_body_fast()
+    assert _device_digests(c) == BENCHED["batch64"][i]
     c.close()

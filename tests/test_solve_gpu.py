@@ -186,27 +186,34 @@ def test_warm_start_reaches_same_solution():
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_graph_replay_matches_direct_launches(prec):
-    """The V-cycle is captured once as a CUDA graph and replayed; with
-    launch-class timing on it is launched kernel by kernel instead.  Same
-    kernels in the same order: the two solves give identical fields, and
-    the launch counter counts the replayed kernels too."""
+    """The whole FGMRES solve is captured once as a CUDA graph (its restart
+    and inner loops as conditional nodes decided on the device) and
+    replayed as one launch; with launch-class timing on, the host drives
+    the same kernels step by step.  Same kernels in the same order: the two
+    solves give identical fields and histories, and the launch counter
+    counts the kernels the graph ran."""
     grid, bodies = GRIDS["sphere_stretched"]
     _, ib, rhs, phi = _problem(grid, bodies)
     p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
     c = _case(grid, bodies, precision=p_, rtol=1e-10, max_cycles=60)
     p_graph = np.zeros(grid.shape, order="F")
     c.solve_poisson(p_graph, rhs)  # captures
+    assert c.solve_mode() == 1
     p_graph[...] = 0.0
     n0 = fg.launch_count()
     st_g = c.solve_poisson(p_graph, rhs)  # replays
     n_graph = fg.launch_count() - n0
+    h_graph = c.history()
+    assert c.solve_mode() == 1
     c.profile(True)
     p_direct = np.zeros(grid.shape, order="F")
     n0 = fg.launch_count()
     st_d = c.solve_poisson(p_direct, rhs)
     n_direct = fg.launch_count() - n0
+    assert c.solve_mode() == 0
     c.profile(False)
     assert st_g["cycles"] == st_d["cycles"]
+    assert np.array_equal(h_graph, c.history())
     assert np.array_equal(p_graph, p_direct)
     assert n_graph == n_direct
     assert _relerr(p_graph, phi, _fluid(grid, ib)) <= 1e-8
@@ -264,3 +271,39 @@ def test_reused_device_blocks_give_identical_solves():
         o.close()
     assert runs[0][0] == runs[1][0]
     assert np.array_equal(runs[0][1], runs[1][1])
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_batch64_problems_each_reach_their_solution(prec):
+    """Four problems of the 64-problem batched workload (edges 32, 35, 45
+    and 81 cells, seeded 5120-triangle ellipsoids), solved together by one
+    batch: each pressure within 1e-9 of its own exact discrete solution
+    (manufactured from the oracle's rows), not of another solve."""
+    allp = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    cfg = fg.default_config(precision=p_, rtol=1e-12, max_cycles=120)
+    cases, refs, d_ps, d_fs = [], [], [], []
+    for i in (4, 9, 3, 0):
+        g, b, seed = allp[i]
+        _, ib, rhs, phi = _problem(g, [b], seed=seed)
+        c = fg.Case(g, cfg)
+        c.add_body(b)
+        c.set_iblank_body_fast()
+        c.gcm_set_internal_boundary()
+        c.mg_prepare()
+        cases.append(c)
+        refs.append((g, phi, _fluid(g, ib)))
+        d_ps.append(torch.zeros(g.shape[::-1], dtype=torch.float64, device="cuda"))
+        d_fs.append(torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda())
+    bt = fg.Batch(cfg)
+    for c in cases:
+        bt.add(c)
+    st = bt.solve_device([t.data_ptr() for t in d_ps], [t.data_ptr() for t in d_fs])
+    torch.cuda.synchronize()
+    assert st["relres"] <= 1e-12
+    for (g, phi, m), t in zip(refs, d_ps):
+        p = t.cpu().numpy().transpose(2, 1, 0)
+        assert _relerr(p, phi, m) <= TOL
+    bt.close()
+    for c in cases:
+        c.close()

@@ -83,3 +83,54 @@ def test_noalloc_rejects_more_rows_than_its_scratch():
     rc = L.fg_rows_relax_noalloc(4, 4, 4, d.data_ptr(), 262144 + 1, d.data_ptr(), d.data_ptr(),
                                  d.data_ptr(), None, 1, None)
     assert rc == 5  # FG_BAD_INPUT
+
+
+def _relax_numpy(p_flat, tgt, cell, w, c0, nx, ny, iters):
+    """The row update restated in numpy: every row gathers from the field
+    as it was at the start of the pass, then all targets are written."""
+    sy, sz = nx + 2, (nx + 2) * (ny + 2)
+    off = np.array([0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1])
+    ok = (cell >= 0) & (cell + off[6] < p_flat.size) & (tgt >= 0) & (tgt < p_flat.size)
+    p = p_flat.copy()
+    for _ in range(iters):
+        vals = (w[ok] * p[cell[ok, None] + off[None, :]]).sum(axis=1) + c0[ok]
+        p[tgt[ok]] = vals
+    return p
+
+
+def test_noalloc_constant_term_and_skipped_row():
+    """Rows with a non-zero constant (the previous-step pressure of the
+    dead-cell fallback, or dp/dn data) against the numpy restatement, and
+    a row whose host cell lies outside the field: that row is skipped (its
+    target keeps its value) while every other row is relaxed."""
+    grid = synth.small_grid(32, 16, 16, (4.0, 2.0, 2.0))
+    c = fg.Case(grid, fg.default_config())
+    c.add_body(synth.sphere_body((1.0, 1.0, 1.0), 1.0, 3))
+    c.set_iblank_body_fast()
+    c.gcm_set_internal_boundary()
+    tgt, cell, w = _rows(grid, c)
+    c.close()
+    n = len(tgt)
+    assert len(np.unique(tgt)) == n
+    rng = np.random.default_rng(5)
+    c0 = rng.standard_normal(n)
+    bad = n // 2
+    cell = cell.copy()
+    cell[bad] = int(np.prod(grid.shape))  # past the last element
+    p = np.asfortranarray(rng.standard_normal(grid.shape))
+    p_flat = p.ravel(order="F")
+    want = _relax_numpy(p_flat, tgt, cell, w, c0, grid.nx, grid.ny, 2)
+    d_p = torch.from_numpy(p_flat.copy()).cuda()
+    d_tgt, d_cell = torch.from_numpy(tgt).cuda(), torch.from_numpy(cell).cuda()
+    d_w, d_c0 = torch.from_numpy(w.ravel()).cuda(), torch.from_numpy(c0).cuda()
+    L = _lib()
+    for _ in range(2):  # two calls in a row, each from the same start
+        d_p.copy_(torch.from_numpy(p_flat))
+        rc = L.fg_rows_relax_noalloc(grid.nx, grid.ny, grid.nz, d_p.data_ptr(), n, d_tgt.data_ptr(),
+                                     d_cell.data_ptr(), d_w.data_ptr(), d_c0.data_ptr(), 2, None)
+        assert rc == fg.FG_OK
+        torch.cuda.synchronize()
+        got = d_p.cpu().numpy()
+        assert np.abs(got - want).max() <= 1e-12 * max(1.0, float(np.abs(want).max()))
+        assert got[tgt[bad]] == p_flat[tgt[bad]]  # targets are distinct cells
+        assert np.count_nonzero(got != p_flat) > n // 2
