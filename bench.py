@@ -436,24 +436,23 @@ def run_config2(torch, fg, synth, args, dev, stream, nsteps=100):
         "geometry_reproduced_every_step": same, "setup_s": t_setup}), flush=True)
 
 
-# device bytes per finest cell of one resident case (levels, masks, FGMRES
-# vectors, tagging scratch), the admission estimate of the serving workload
-SERVE_BYTES_PER_CELL = {"mixed": 130.0, "fp64": 190.0}
-
-
 def run_serve(fg, synth, args, dev, stream, ntemplates=16):
-    """The serving workload: requests arrive as a seeded Poisson trace; each
-    brings a problem (one of `ntemplates` seeded shapes: edge 32..256 cells,
-    aspect 1:1:1 or 2:1:1, sphere or ellipsoid) and 1..10 time steps.  The
-    server takes requests first-come first-served within a device-memory
-    admission budget, and runs each through the public entry points: create
-    the case, add the body, tag it, prepare the hierarchy, one host-buffer
-    solve per step (the div field in, the pressure out, warm-started from
-    the previous step), destroy.  Latency is arrival to completion.  The
-    RHS of each template is made beforehand (untimed) from its geometry.
-    Traces: the offered rate (default 200/s, which one GPU cannot keep up
-    with: latencies then measure the queue) and a sustainable rate, both on
-    the mixed path, and the sustainable one again on the FP64 path."""
+    """The serving workload through the library's serving engine
+    (fg_server_*).  Requests arrive as a seeded Poisson trace; each brings a
+    problem (one of `ntemplates` seeded shapes: edge 32..256 cells, aspect
+    1:1:1 or 2:1:1, sphere or ellipsoid) and 1..10 time steps, and is
+    submitted at its arrival time.  The engine admits requests first come,
+    first served while at most --serve-slots cases are resident within the
+    150 GB device-memory budget, builds each case (hierarchy, device
+    tagging, lists) and runs its steps (right-hand side in from page-locked
+    host memory, the FGMRES solve as one graph launch, the pressure back to
+    page-locked host memory, warm-started from the previous step); steps of
+    different requests overlap on the device.  Latency runs from submission
+    (the arrival) to the request's last pressure on the host.  The RHS of
+    each template is made beforehand (untimed) from its geometry; requests
+    of one template share its input and output host fields.  Traces: the
+    offered rate (default 200/s) and a lower rate, on the mixed path, and
+    the offered one again on the FP64 path."""
     import multiprocessing as mp
     import torch
     t0 = time.time()
@@ -469,7 +468,20 @@ def run_serve(fg, synth, args, dev, stream, ntemplates=16):
         c.close()
     with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
         rhs = pool.map_async(_c2_rhs, jobs, chunksize=1).get(timeout=1200)
-    rhs = [(np.asfortranarray(rhs[2 * i]), np.asfortranarray(rhs[2 * i + 1])) for i in range(ntemplates)]
+
+    def pinned_field(a):
+        t = torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).pin_memory()
+        return t, t.numpy().transpose(2, 1, 0)  # Fortran view of the page-locked buffer
+
+    keep, divs, outs = [], [], []
+    for i in range(ntemplates):
+        pair = [pinned_field(rhs[2 * i]), pinned_field(rhs[2 * i + 1])]
+        keep += [t for t, _ in pair]
+        divs.append([v for _, v in pair])
+        o, ov = pinned_field(np.zeros(temps[i][0].shape))
+        keep.append(o)
+        outs.append(ov)
+    del rhs
     t_setup = time.time() - t0
     budget = 150e9
 
@@ -477,54 +489,42 @@ def run_serve(fg, synth, args, dev, stream, ntemplates=16):
         cfg = fg.default_config(precision=fg.FG_PREC_MIXED if prec_name == "mixed" else fg.FG_PREC_FP64,
                                 rtol=RTOL, max_cycles=200)
         trace = synth.serving_trace(rate, seconds, ntemplates)
-        lat, nsolves, rejected, worst = [], 0, 0, 0.0
+        srv = fg.Server(cfg, budget_bytes=int(budget), max_active=args.serve_slots, device=dev)
+        n0 = fg.launch_count()
         t_start = time.perf_counter()
-        for (ta, ti, k) in trace:
-            g, b = temps[ti]
-            cells = (g.nx - 1) * (g.ny - 1) * (g.nz - 1)
-            if cells * SERVE_BYTES_PER_CELL[prec_name] > budget:
-                rejected += 1
-                continue
+        for rid, (ta, ti, k) in enumerate(trace):
             now = time.perf_counter() - t_start
             if now < ta:  # idle until the request arrives
                 time.sleep(ta - now)
-            c = fg.Case(g, cfg, device=dev)
-            c.set_stream(stream.cuda_stream)
-            c.add_body(b)
-            c.set_iblank_body_fast()
-            c.gcm_set_internal_boundary()
-            c.mg_prepare()
-            p = np.zeros(g.shape, order="F")
-            for s_ in range(k):
-                st = c.solve_poisson(p, rhs[ti][s_ % 2])
-                worst = max(worst, st["relres"])
-                nsolves += 1
-            c.close()
-            lat.append(time.perf_counter() - t_start - ta)
+            g, b = temps[ti]
+            srv.submit(rid, g, b, [divs[ti][s_ % 2] for s_ in range(k)], [outs[ti]] * k)
+        srv.wait_idle(3600.0)
         span = time.perf_counter() - t_start
-        lat = np.array(lat) * 1e3
+        res = srv.poll(capacity=len(trace) + 16)
+        info = srv.info()
+        srv.close()
+        n1 = fg.launch_count()
+        lat = np.array([r["t_done"] - r["t_submit"] for r in res]) * 1e3
+        wait = np.array([r["t_admit"] - r["t_submit"] for r in res]) * 1e3
+        nsolves = sum(r["steps_done"] for r in res)
         offered = sum(k * (temps[ti][0].nx - 1) * (temps[ti][0].ny - 1) * (temps[ti][0].nz - 1)
                       for (_, ti, k) in trace) / seconds
-        return {"rate_per_s": rate, "seconds": seconds, "requests": len(trace), "rejected": rejected,
-                "solves": nsolves, "span_s": span, "solves_per_s": nsolves / span,
+        return {"rate_per_s": rate, "seconds": seconds, "requests": len(trace),
+                "completed": sum(1 for r in res if r["status"] == fg.FG_OK), "solves": nsolves,
+                "span_s": span, "solves_per_s": nsolves / span,
                 "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                                "max": float(lat.max())},
-                "offered_cell_solves_per_s": offered, "relres_max": worst}
+                "admission_wait_ms": {"p50": float(np.percentile(wait, 50)), "p99": float(np.percentile(wait, 99))},
+                "active_peak": info["active_peak"], "gpu_launches": n1 - n0,
+                "offered_cell_solves_per_s": offered,
+                "relres_max": max(r["relres_max"] for r in res), "cycles_max": max(r["cycles_max"] for r in res)}
 
-    # one untimed request per precision first (module loading, first captures)
+    # a short untimed trace per precision first (module loading)
     for prec_name in ("mixed", "fp64"):
-        cfgw = fg.default_config(precision=fg.FG_PREC_MIXED if prec_name == "mixed" else fg.FG_PREC_FP64)
-        tw = min(range(ntemplates), key=lambda i: temps[i][0].nx * temps[i][0].ny * temps[i][0].nz)
-        cw = fg.Case(temps[tw][0], cfgw, device=dev)
-        cw.add_body(temps[tw][1])
-        cw.set_iblank_body_fast()
-        cw.gcm_set_internal_boundary()
-        cw.mg_prepare()
-        cw.solve_poisson(np.zeros(temps[tw][0].shape, order="F"), rhs[tw][0])
-        cw.close()
+        serve(20.0, 0.2, prec_name)
     offered = serve(args.serve_rate, args.serve_seconds, "mixed")
-    sustain = serve(args.serve_low_rate, args.serve_low_seconds, "mixed")
-    sustain64 = serve(args.serve_low_rate, args.serve_low_seconds, "fp64")
+    low = serve(args.serve_low_rate, args.serve_low_seconds, "mixed")
+    offered64 = serve(args.serve_rate, args.serve_seconds, "fp64")
     print(json.dumps({
         "metric": "serving: solves/s and p50/p99 latency (arrival to completion)",
         "value": offered["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
@@ -533,13 +533,13 @@ def run_serve(fg, synth, args, dev, stream, ntemplates=16):
         "data": "synthetic (seeded Poisson trace; 16 seeded problem shapes with manufactured RHS)",
         "config": {"workload": "serve", "templates": ntemplates,
                    "template_cells": [(g.nx - 1) * (g.ny - 1) * (g.nz - 1) for g, _ in temps],
-                   "admission_budget_gb": budget / 1e9,
-                   "admission_bytes_per_cell": SERVE_BYTES_PER_CELL, "rtol": RTOL,
-                   "server": "first come first served, one request resident at a time, each through "
-                             "fg_case_create / add_body / set_iblank_body_fast / "
-                             "gcm_set_internal_boundary / mg_prepare / solve_poisson (host buffers) "
-                             "/ destroy"},
-        "offered_rate": offered, "sustainable_rate": sustain, "sustainable_rate_fp64": sustain64,
+                   "admission_budget_gb": budget / 1e9, "slots": args.serve_slots, "rtol": RTOL,
+                   "server": "fg_server: continuous admission (first come first served within the slots "
+                             "and the device-memory budget), one case per request resident across its "
+                             "steps, every step one graph launch on the case's stream, steps of "
+                             "different requests overlapping on the device"},
+        "offered_rate": offered, "lower_rate": low, "offered_rate_fp64": offered64,
+        "speedup_mixed_over_fp64": offered["solves_per_s"] / offered64["solves_per_s"],
         "setup_s": t_setup}), flush=True)
 
 
@@ -880,8 +880,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="serve: offered arrivals per second")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="serve: length of the offered trace")
-    ap.add_argument("--serve-low-rate", type=float, default=4.0, help="serve: a sustainable rate")
-    ap.add_argument("--serve-low-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-low-rate", type=float, default=20.0, help="serve: a lower rate")
+    ap.add_argument("--serve-low-seconds", type=float, default=5.0)
+    ap.add_argument("--serve-slots", type=int, default=16, help="serve: most requests resident at once")
     ap.add_argument("--kernels-only", action="store_true",
                     help="one case, timed solves only (for kernel profiling)")
     args = ap.parse_args()

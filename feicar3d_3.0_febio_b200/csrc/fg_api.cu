@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <map>
@@ -128,6 +129,13 @@ cudaError_t dev_alloc_raw(void **p, size_t bytes) {
   return cudaSuccess;
 }
 
+// Set while a case whose stream has drained frees its blocks: nothing
+// queued can still use them, so no device-wide wait (which would stall the
+// other cases' work in flight on other streams).
+static thread_local bool t_idle_free = false;
+IdleFree::IdleFree() : prev(t_idle_free) { t_idle_free = true; }
+IdleFree::~IdleFree() { t_idle_free = prev; }
+
 void dev_free(void *p) {
   if (!p) return;
   DevCache &C = dev_cache();
@@ -142,7 +150,7 @@ void dev_free(void *p) {
   int cur = 0;
   cudaGetDevice(&cur);
   if (cur != o.first) cudaSetDevice(o.first);
-  cudaDeviceSynchronize();
+  if (!t_idle_free) cudaDeviceSynchronize();
   std::lock_guard<std::mutex> lk(C.mu);
   if (C.cached[o.first] + o.second > kDevCacheMax) {
     C.owner.erase(p);
@@ -535,6 +543,10 @@ struct fg_batch {
   fg_solve_stats rich_stats{};
   std::vector<double> history;  // max relative residual over the batch after each cycle
   int last_mode = 0;  // how the last solve ran: 0 host-driven launches, 1 one graph launch
+  // counters of the two-colour y/z sweeps (k::line_sweep_zz); null: one
+  // launch per colour (FEICAR_B200_ZEBRA_TWO_LAUNCH=1 at batch build)
+  void *zz_ctl = nullptr;
+  int *h_zzerr = nullptr;  // page-locked copy of its error flag
   // FGMRES state (outer == FG_OUTER_FGMRES): per problem the FP64 vectors
   // P, F and the basis V_0..V_m, Z_0..Z_{m-1} (FP32 in the mixed path) of
   // the finest level's layout
@@ -613,8 +625,9 @@ static void free_batch_tables(fg_batch *b) {
   b->h_small.clear();
   fg::dev_free(b->d_rprob); fg::dev_free(b->d_rtgt); fg::dev_free(b->d_rcell); fg::dev_free(b->d_rw);
   fg::dev_free(b->d_rc0); fg::dev_free(b->d_rd); fg::dev_free(b->d_rf); fg::dev_free(b->d_tmp);
-  fg::dev_free(b->d_norm); fg::dev_free(b->d_part);
+  fg::dev_free(b->d_norm); fg::dev_free(b->d_part); fg::dev_free(b->zz_ctl);
   b->d_part = nullptr;
+  b->zz_ctl = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
   if (b->sg.exec) cudaGraphExecDestroy(b->sg.exec);
@@ -878,6 +891,13 @@ static fg_status build_batch(fg_batch *b) {
     b->h_norm_n = 3 * np;
   }
   std::fill(b->h_norm, b->h_norm + 3 * np, 0.0);
+  {
+    const char *two = getenv("FEICAR_B200_ZEBRA_TWO_LAUNCH");
+    if (!(two && two[0] == '1')) {
+      FG_CUDA(fg::dev_alloc(&b->zz_ctl, k::zz_ctl_bytes()));
+      FG_CUDA(cudaMemset(b->zz_ctl, 0, k::zz_ctl_bytes()));
+    }
+  }
   b->sig = batch_signature(b);
   b->built = true;
   return FG_OK;
@@ -945,7 +965,22 @@ static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
     const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
     const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
     const int cls = L == 0 ? FG_PROF_LINE_X0 + axis : FG_PROF_LINE_COARSE;
-    for (int color = 0; color < 2; ++color) {
+    bool fused = false;
+    if (axis > 0 && b->zz_ctl && ls.S.size() == 1) {
+      // one problem at this level: both colours in one launch
+      const size_t e0 = prof_begin(b, s);
+      const cudaError_t e = k::line_sweep_zz<T>(ls.d_levS, b->cases[ls.S[0]]->lev[L].dl, axis, om, b->zz_ctl, s);
+      if (e == cudaSuccess) {
+        fused = true;
+        prof_end(b, e0, cls, 2.0 * sweep_bytes<T>(ls.ncells, om), s);
+      } else if (e != cudaErrorNotSupported) {
+        set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+        return FG_CUDA_ERROR;
+      } else if (e0 != (size_t)-1) {
+        b->prof.used -= 2;  // nothing was launched between the events
+      }
+    }
+    for (int color = 0; color < 2 && !fused; ++color) {
       const size_t e0 = prof_begin(b, s);
       FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, s));
       prof_end(b, e0, cls, sweep_bytes<T>(ls.ncells, om), s);
@@ -1532,6 +1567,13 @@ static fg_status fgmres_enqueue(fg_batch *b) {
   if (r != FG_OK) return r;
   FG_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaMemcpyAsync(b->h_kctl, b->d_kctl, sizeof(KCtl), cudaMemcpyDeviceToHost, s));
+  if (b->zz_ctl) {
+    if (!b->h_zzerr) {
+      b->h_zzerr = static_cast<int *>(pinned_get(4 * sizeof(int)));
+      if (!b->h_zzerr) return FG_ALLOC_FAIL;
+    }
+    FG_CUDA(cudaMemcpyAsync(b->h_zzerr, b->zz_ctl, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  }
   FG_CUDA(cudaEventRecord(b->ev1, s));
   b->pending = true;
   return FG_OK;
@@ -1544,6 +1586,10 @@ static fg_status fgmres_collect(fg_batch *b, fg_solve_stats *st) {
   const int np = (int)b->cases.size();
   FG_CUDA(cudaEventSynchronize(b->ev1));
   const KCtl &C = *b->h_kctl;
+  if (b->zz_ctl && b->h_zzerr && k::zz_error(b->h_zzerr)) {
+    set_last_error("a two-colour line sweep gave up waiting for its neighbour planes", __FILE__, __LINE__);
+    return FG_TIMEOUT;
+  }
   if (b->last_mode == 1) {
     const auto &SG = b->sg;
     note_launches(SG.n_pre + C.n_restart * SG.n_restart + C.n_body * SG.n_body + C.n_inner * SG.n_inner +
@@ -1912,6 +1958,10 @@ fg_status fg_case_create(int nx, int ny, int nz, const double *xn, const double 
 fg_status fg_case_destroy(fg_case *c) {
   if (!c) return FG_OK;
   cudaSetDevice(c->device);
+  // every buffer of the case is used on its stream only: once that has
+  // drained, its blocks go back to the cache without a device-wide wait
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  fg::IdleFree idle;
   if (c->solo) { fg_batch_destroy(c->solo); c->solo = nullptr; }
   for (int l = 0; l < c->nlev; ++l) {
     HLevel &L = c->lev[l];
@@ -1925,6 +1975,39 @@ fg_status fg_case_destroy(fg_case *c) {
   if (c->geom) geom_free(*c->geom);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
+  return FG_OK;
+}
+
+fg_status fg_case_estimate_bytes(int nx, int ny, int nz, const fg_solver_config *cfg, size_t *bytes) {
+  if (!bytes || nx < 3 || ny < 3 || nz < 3) return FG_BAD_INPUT;
+  fg_solver_config c{};
+  if (cfg) c = *cfg; else fg_default_config(&c);
+  const bool mixed = c.precision == FG_PREC_MIXED;
+  const int mg[3] = {(c.mgrids[0] <= 0 || c.mgrids[0] > 10) ? auto_levels(nx) : c.mgrids[0],
+                     (c.mgrids[1] <= 0 || c.mgrids[1] > 10) ? auto_levels(ny) : c.mgrids[1],
+                     (c.mgrids[2] <= 0 || c.mgrids[2] > 10) ? auto_levels(nz) : c.mgrids[2]};
+  const int nlev = std::min(kMaxLevels, std::max(mg[0], std::max(mg[1], mg[2])));
+  int I = nx, J = ny, K = nz;
+  double total = 0.0, ntot0 = 0.0;
+  for (int l = 0; l < nlev; ++l) {
+    if (l > 0) {
+      if (l + 1 <= mg[0]) I = coarsen_count(I);
+      if (l + 1 <= mg[1]) J = coarsen_count(J);
+      if (l + 1 <= mg[2]) K = coarsen_count(K);
+    }
+    const double sy = (double)pitch_up(I + 1), ntot = sy * (J + 1) * (K + 1) + kFieldPad + 1;
+    if (l == 0) ntot0 = ntot;
+    // type, mask, solid flag; values of the level's precision
+    double per = 3.0 + (mixed ? (l == 0 ? 2 * 8 + 3 * 4 : 3 * 4) : 3 * 8);
+    total += ntot * per + 2.0 * 8 * (I + J + K + 6) * 4;
+  }
+  const double nref = (double)(nx + 2) * (ny + 2) * (nz + 2);
+  const int m = krylov_restart(c);
+  const double kb = mixed ? 4.0 : 8.0;
+  total += ntot0 * (2 * 8 + (2 * m + 1) * kb);  // FGMRES P, F and the basis
+  total += nref * (2 * 8 + 2);                  // reference-layout staging and masks
+  total += nref * 9;                            // tagging masks and scratch
+  *bytes = (size_t)(total * 1.02) + ((size_t)16 << 20);  // block rounding, lists, tables
   return FG_OK;
 }
 
@@ -2175,6 +2258,46 @@ fg_status fg_solve_poisson_device(fg_case *c, double *d_p, const double *d_div,
   return s;
 }
 
+// reduction of ref_blocks partials on the host (a few thousand values)
+static fg_status ref_measure(fg_case *c, const double *a, const double *b, bool change, double *out) {
+  if (!c || !a || !b || !out) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  if (!c->prepared) {
+    fg_status st = prepare(c);
+    if (st != FG_OK) return st;
+  }
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  const int nb = k::ref_blocks(c->nx, c->ny, c->nz);
+  double *part = nullptr;
+  FG_CUDA(fg::dev_alloc(&part, (size_t)nb * sizeof(double)));
+  std::vector<double> h(nb);
+  cudaError_t e = cudaMemcpyAsync(c->d_pin, a, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_fin, b, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess)
+    e = change ? k::ref_change(c->d_pin, c->d_fin, c->d_refmask, c->nx, c->ny, c->nz, part, c->stream)
+               : k::ref_residual(c->d_pin, c->d_fin, c->d_refmask, c->d_refmask + nref, c->lev[0].dl, c->nx,
+                                 c->ny, c->nz, part, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), part, (size_t)nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  fg::dev_free(part);
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    return FG_CUDA_ERROR;
+  }
+  double v = 0.0;
+  for (double q : h) v = change ? std::max(v, q) : v + q;
+  *out = change ? v : std::sqrt(v / ((double)c->nx * c->ny * c->nz));
+  return FG_OK;
+}
+
+fg_status fg_calc_residual(fg_case *c, const double *p, const double *div, double *maxres) {
+  return ref_measure(c, p, div, false, maxres);
+}
+
+fg_status fg_calc_residual2(fg_case *c, const double *p, const double *p_temp, double *maxres2) {
+  return ref_measure(c, p, p_temp, true, maxres2);
+}
+
 fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old, int iterations) {
   if (!c || !p || iterations < 1) return FG_BAD_INPUT;
   cudaSetDevice(c->device);
@@ -2327,6 +2450,7 @@ fg_status fg_batch_destroy(fg_batch *b) {
     if (q) cudaStreamDestroy(q);
   if (b->h_kctl) pinned_put(b->h_kctl);
   if (b->h_norm) pinned_put(b->h_norm);
+  if (b->h_zzerr) pinned_put(b->h_zzerr);
   if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }
   delete b;
   return FG_OK;

@@ -147,6 +147,16 @@ void host_copy(void *dst, const void *src, size_t bytes);
 
 cudaError_t dev_alloc_raw(void **p, size_t bytes);
 void dev_free(void *p);
+// while one lives on a thread, dev_free on that thread skips the
+// device-wide wait (the caller has drained every stream that used the
+// blocks it frees)
+struct IdleFree {
+  bool prev;
+  IdleFree();
+  ~IdleFree();
+  IdleFree(const IdleFree &) = delete;
+  IdleFree &operator=(const IdleFree &) = delete;
+};
 template <class T>
 inline cudaError_t dev_alloc(T **p, size_t bytes) {
   return dev_alloc_raw(reinterpret_cast<void **>(p), bytes);
@@ -251,6 +261,16 @@ size_t smem_line(int n, int tsize, int axis);
 template <typename T>
 cudaError_t line_sweep(const Launch &L, int axis, int color, double omega, int maxn,
                        cudaStream_t s);
+// both colours of a y/z sweep of a single problem's level in one launch
+// (work items by ticket; colour-1 items wait for their neighbour planes'
+// colour 0); cudaErrorNotSupported when the level's lines do not take that
+// kernel.  ctl: zz_ctl_bytes() of zeroed device memory, reset by every
+// launch at its end.
+template <typename T>
+cudaError_t line_sweep_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, void *ctl,
+                          cudaStream_t s);
+size_t zz_ctl_bytes();
+int zz_error(const void *ctl_host);  // a wait ran out in some launch
 // norm2[p] += ||r||^2 of entry p when norm2 != null (part: one double per block)
 template <typename T>
 cudaError_t residual(const Launch &L, double *norm2, double *part, cudaStream_t s);
@@ -298,6 +318,14 @@ struct FaceData {
   const double *pgrad[6];  // device face arrays or null (zero gradient)
 };
 cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaStream_t s);
+// the reference's own residual measures on reference-layout fields
+// (block partials into part, ref_blocks of them): squared residuals of
+// calc_residual, maxima of |p - p_temp| of calc_residual2
+int ref_blocks(int nx, int ny, int nz);
+cudaError_t ref_residual(const double *p, const double *div, const int8_t *ib, const int8_t *gh,
+                         const DevLevel &L0, int nx, int ny, int nz, double *part, cudaStream_t s);
+cudaError_t ref_change(const double *p, const double *pt, const int8_t *ib, int nx, int ny, int nz, double *part,
+                       cudaStream_t s);
 cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int nz,
                          const int *pbc, const double *ppp, int gauge, double *scratch,
                          cudaStream_t s);

@@ -11,7 +11,9 @@
 // colour are solved in parallel, one warp per line).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
+#include <stdlib.h>
 #include <string.h>
 #include <stdint.h>
 
@@ -780,13 +782,15 @@ struct XsLayout {
 };
 
 // Line (j,k) of warp `warp` in block `lb` of a level's x sweep; false when
-// the warp has no line.
+// the warp has no line.  Colour 1 walks the k planes backward, so its first
+// blocks meet the planes the colour-0 launch left in L2.
 __device__ __forceinline__ bool xs_line(const DevLevel &L, int lb, int warp, int color, int &j, int &k) {
   const int nyh = (L.ny + 1) >> 1;
   const int q = lb * XS_WARPS + warp;
   k = 1 + q / nyh;
   const int jj = q % nyh;
   if (k > L.nz) return false;
+  if (color == 1) k = L.nz + 1 - k;
   j = ((((1 + k) & 1) == color) ? 1 : 2) + 2 * jj;
   return j <= L.ny;
 }
@@ -1243,10 +1247,113 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
 // chunk equations of each line are solved by parallel cyclic reduction
 // across the block (log2 CH steps through shared memory), and every thread
 // back-substitutes its rows.
-template <typename T, int M, int CH, int AXIS>
+// ---- both colours of a zebra sweep in one launch (single problem)
+// Work items (one i-tile of one plane of fixed o, one colour) are taken by
+// ticket in the order c0 slab 0, c0 slab 1, c1 slab 0, c0 slab 2, c1 slab
+// 1, ..., c1 slab S-1 (a slab: `slab` consecutive planes).  A colour-1 item
+// of slab s starts once every colour-0 item of slabs s-1, s and s+1 is
+// done, so it reads the new colour-0 values of its neighbour planes, and
+// no colour-0 item reads a colour-1 value after it changed (those of slab
+// s change only after slab s+1's colour 0 is done): the same arithmetic
+// as two launches, one colour each.  The colour-0 sectors an item pulls
+// in (the other colour's rhs, mask and unknowns share them) are still in
+// L2 when the colour-1 items of the same planes run a few groups later.
+// Items wait only on items with smaller tickets, which running blocks
+// hold and finish without waiting, so the launch cannot deadlock; a wait
+// is still bounded, and when it runs out the item records an error and
+// skips its work.  The last block to finish resets the counters.
+constexpr int ZZ_MAXSLAB = 512;
+struct ZzCtl {
+  int ticket, finished, err, pad_;
+  int done0[ZZ_MAXSLAB];  // finished colour-0 items per slab
+};
+struct ZzPlan {
+  ZzCtl *ctl;
+  int nplanes;  // planes (values of o)
+  int slab;     // planes per slab
+  int nslab;
+  int ntx;      // i-tiles per plane
+  int lag;      // colour-1 groups trail the colour-0 groups by this many slabs (>= 1)
+};
+__host__ __device__ __forceinline__ int zz_tiles(const ZzPlan &z, int s) {
+  const int np = z.nplanes - s * z.slab;
+  return z.ntx * (np < z.slab ? np : z.slab);
+}
+// colour and slab of group g of the ticket order: c0 slabs 0..lag-1, then
+// pairs (c0 slab s, c1 slab s-lag), then the last lag colour-1 slabs
+__host__ __device__ __forceinline__ void zz_group(const ZzPlan &z, int g, int &color, int &slab) {
+  const int L = z.lag < z.nslab ? z.lag : z.nslab;
+  const int mid = 2 * (z.nslab - L);
+  if (g < L) { color = 0; slab = g; return; }
+  if (g < L + mid) {
+    const int h = g - L, s = L + (h >> 1);
+    if (h & 1) { color = 1; slab = s - L; } else { color = 0; slab = s; }
+    return;
+  }
+  color = 1;
+  slab = z.nslab - L + (g - L - mid);
+}
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// block-wide: takes a ticket, decodes it (color, slab, item within the
+// slab), waits for the colour-0 items a colour-1 item depends on; returns
+// false when a wait ran out (the item then skips its work)
+__device__ bool zz_begin(const ZzPlan &z, int &color, int &slab, int &li) {
+  __shared__ int s_v[4];
+  if (threadIdx.x == 0) {
+    int t = atomicAdd(&z.ctl->ticket, 1);
+    int g = 0, cc = 0, ss = 0;
+    for (;; ++g) {
+      zz_group(z, g, cc, ss);
+      const int n = zz_tiles(z, ss);
+      if (t < n) break;
+      t -= n;
+    }
+    int ok = 1;
+    if (cc == 1) {
+      for (int q = ss - 1; q <= ss + 1 && ok; ++q) {
+        if (q < 0 || q >= z.nslab) continue;
+        const int need = zz_tiles(z, q);
+        long long spins = 0;
+        while (ld_acquire(&z.ctl->done0[q]) < need) {
+          if (++spins > (1ll << 24)) {  // ~ seconds: never reached unless something is broken
+            atomicExch(&z.ctl->err, 1);
+            ok = 0;
+            break;
+          }
+          __nanosleep(128);
+        }
+      }
+    }
+    s_v[0] = cc; s_v[1] = ss; s_v[2] = t; s_v[3] = ok;
+  }
+  __syncthreads();
+  color = s_v[0]; slab = s_v[1]; li = s_v[2];
+  return s_v[3] != 0;
+}
+// block-wide, after every thread's stores: publishes a finished colour-0
+// item; the last block of the launch resets the counters
+__device__ void zz_end(const ZzPlan &z, int color, int slab, int total) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (color == 0) atomicAdd(&z.ctl->done0[slab], 1);
+    if (atomicAdd(&z.ctl->finished, 1) == total - 1) {
+      for (int q = 0; q < z.nslab; ++q) z.ctl->done0[q] = 0;
+      z.ctl->ticket = 0;
+      __threadfence();
+      atomicExch(&z.ctl->finished, 0);
+    }
+  }
+}
+
+template <typename T, int M, int CH, int AXIS, bool FUSED = false>
 __global__ void __launch_bounds__(CH * YP_LINES, ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
                                                    ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1)
-k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega, ZzPlan zz) {
   using LC = LineCoefT<T, AXIS>;
   constexpr int NT = CH * YP_LINES;
   __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
@@ -1257,13 +1364,23 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
   auto s_last = reinterpret_cast<T(*)[CH][YP_LINES]>(&s_eq[1][0][0]);
   const int tid = threadIdx.x;
   const int l = tid % YP_LINES, c = tid / YP_LINES;
-  const int p = find_entry(off, nent, blockIdx.x);
+  int p = 0, lb = 0, zslab = 0;
+  bool work = true;
+  if constexpr (FUSED) {
+    int li = 0;
+    work = zz_begin(zz, color, zslab, li);
+    lb = zslab * zz.slab * zz.ntx + li;
+  } else {
+    p = find_entry(off, nent, blockIdx.x);
+    lb = blockIdx.x - off[p];
+  }
   const DevLevel &L = levs[p];
-  const int lb = blockIdx.x - off[p];
   constexpr int TW = 2 * YP_LINES;  // cells of an i-tile
   const int ntx = (L.nx + TW - 1) / TW;
   const int ti = lb % ntx;
-  const int o = 1 + lb / ntx;  // k for AXIS 1, j for AXIS 2
+  // k for AXIS 1, j for AXIS 2; a colour-1 launch walks the planes backward,
+  // so its first blocks meet the planes the colour-0 launch left in L2
+  const int o = (!FUSED && color == 1) ? (AXIS == 1 ? L.nz : L.ny) - lb / ntx : 1 + lb / ntx;
   const int i0 = 1 + TW * ti;
   const int par = (color + i0 + o) & 1;
   const int i = i0 + par + 2 * l;
@@ -1290,12 +1407,19 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
     const int r = r0 + u;
     d[u] = T(0);
     mk[u] = 0;
-    if (any && r < n) {
+    if (work && any && r < n) {
       const long long id = base + ls * (r + 1);
       uint8_t m8 = L.mask[id];
       const T rv = rhs[id];
-      const T xv = x[id];
-      const T nb[4] = {x[id - 1], x[id + 1], x[id - os], x[id + os]};
+      T xv, nb[4];
+      if (FUSED && color == 1) {  // other SMs' new colour-0 values: read at L2, not from this SM's L1
+        xv = x[id];
+        nb[0] = __ldcg(&x[id - 1]); nb[1] = __ldcg(&x[id + 1]);
+        nb[2] = __ldcg(&x[id - os]); nb[3] = __ldcg(&x[id + os]);
+      } else {
+        xv = x[id];
+        nb[0] = x[id - 1]; nb[1] = x[id + 1]; nb[2] = x[id - os]; nb[3] = x[id + os];
+      }
       T acc = rv;
 #pragma unroll
       for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
@@ -1344,17 +1468,19 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
   }
   const T xF = s_eq[buf][c][l].d;
   const T xFn = c + 1 < CH ? s_eq[buf][c + 1][l].d : T(0);
-  if (!any) return;
-  const T xL = dL - aL * xF - cL * xFn;
+  if (work && any) {
+    const T xL = dL - aL * xF - cL * xFn;
 #pragma unroll
-  for (int u = 0; u < M; ++u) {
-    const int r = r0 + u;
-    if (r >= n) break;
-    T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
-    const long long id = base + ls * (r + 1);
-    if (omega != T(1)) v = x[id] + omega * (v - x[id]);
-    x[id] = v;
+    for (int u = 0; u < M; ++u) {
+      const int r = r0 + u;
+      if (r >= n) break;
+      T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+      const long long id = base + ls * (r + 1);
+      if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+      x[id] = v;
+    }
   }
+  if constexpr (FUSED) zz_end(zz, color, zslab, 2 * zz.nplanes * zz.ntx);
 }
 
 template <typename T, int M>
@@ -1370,18 +1496,74 @@ static cudaError_t launch_xsmem(const Launch &Lr, int color, double omega, cudaS
 template <typename T, int M, int CH>
 static cudaError_t launch_yzpcr(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
   const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
+  const ZzPlan none{};
   if (axis == 1) {
     auto kern = k_yzline_pcr<T, M, CH, 1>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega, none);
   } else {
     auto kern = k_yzline_pcr<T, M, CH, 2>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega, none);
   }
   note_launches(1);
   return cudaGetLastError();
 }
+
+// both colours in one launch (see ZzCtl); lev: the one problem's level
+// (device), L its host copy
+int zz_lag();
+template <typename T, int M, int CH>
+static cudaError_t launch_yzpcr_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, ZzCtl *ctl,
+                                   cudaStream_t s) {
+  const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
+  ZzPlan z;
+  z.ctl = ctl;
+  z.ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+  z.nplanes = axis == 1 ? L.nz : L.ny;
+  z.slab = std::max(1, (192 + z.ntx - 1) / z.ntx);
+  z.nslab = (z.nplanes + z.slab - 1) / z.slab;
+  z.lag = zz_lag();
+  if (z.nslab > ZZ_MAXSLAB) return cudaErrorNotSupported;
+  const int total = 2 * z.nplanes * z.ntx;
+  if (axis == 1) {
+    auto kern = k_yzline_pcr<T, M, CH, 1, true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<total, CH * YP_LINES, sm, s>>>(nullptr, 1, lev, 0, (T)omega, z);
+  } else {
+    auto kern = k_yzline_pcr<T, M, CH, 2, true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    kern<<<total, CH * YP_LINES, sm, s>>>(nullptr, 1, lev, 0, (T)omega, z);
+  }
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+size_t zz_ctl_bytes() { return sizeof(ZzCtl); }
+// slabs by which colour 1 trails colour 0 (FEICAR_B200_ZEBRA_LAG, default 2)
+int zz_lag() {
+  static int lag = [] {
+    const char *e = getenv("FEICAR_B200_ZEBRA_LAG");
+    const int v = e ? atoi(e) : 2;
+    return v < 1 ? 1 : v;
+  }();
+  return lag;
+}
+
+// Both colours of a y or z sweep of one problem's level in one launch when
+// its lines take k_yzline_pcr; cudaErrorNotSupported otherwise (the caller
+// then launches the colours one by one).
+template <typename T>
+cudaError_t line_sweep_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, void *ctl,
+                          cudaStream_t s) {
+  const int maxn = axis == 1 ? L.ny : L.nz;
+  if (axis == 0 || !ctl || maxn < YP_MINROWS || maxn > YZ_MAXROWS) return cudaErrorNotSupported;
+  if (maxn <= 128) return launch_yzpcr_zz<T, 8, 16>(lev, L, axis, omega, static_cast<ZzCtl *>(ctl), s);
+  return launch_yzpcr_zz<T, 8, 32>(lev, L, axis, omega, static_cast<ZzCtl *>(ctl), s);
+}
+template cudaError_t line_sweep_zz<float>(const DevLevel *, const DevLevel &, int, double, void *, cudaStream_t);
+template cudaError_t line_sweep_zz<double>(const DevLevel *, const DevLevel &, int, double, void *, cudaStream_t);
+int zz_error(const void *ctl_host) { return static_cast<const ZzCtl *>(ctl_host)->err; }
 
 template <typename T, int M, int CH>
 static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
@@ -2272,6 +2454,79 @@ cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaSt
   if (!any) return cudaSuccess;
   const long long m = std::max((long long)L0.ny * L0.nz, std::max((long long)L0.nx * L0.nz, (long long)L0.nx * L0.ny));
   k_face_rhs<<<dim3((unsigned)((m + 255) / 256), 6), 256, 0, s>>>(rhs, L0, fd);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------ reference residual norms
+// CORE_POISSON.F90:460-551 (calc_residual): r = div - A p on the fluid,
+// non-ghost interior cells of a reference-layout field (its own outer ghost
+// layers as stored), block sums of r^2 into part[b].  CORE_POISSON.F90
+// :679-724 (calc_residual2): block maxima of |p - p_temp| over the
+// non-iblank interior cells into part[b].  mask: iblank then ghostCellMark
+// (reference layout); lev0 supplies the axis coefficients.
+__global__ void __launch_bounds__(256)
+k_ref_residual(const double *p, const double *div, const int8_t *ib, const int8_t *gh, const DevLevel L,
+               int nx, int ny, int nz, double *part) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ni = nx - 1, nj = ny - 1, n = ni * nj * (nz - 1);
+  double r2 = 0.0;
+  if (e < n) {
+    const int i = 1 + (int)(e % ni), j = 1 + (int)((e / ni) % nj), k = 1 + (int)(e / (ni * nj));
+    const long long NX = nx + 2, NXY = NX * (ny + 2), id = i + NX * j + NXY * k;
+    const double bmx = L.amx[i], bpx = L.apx[i], bmy = L.amy[j], bpy = L.apy[j], bmz = L.amz[k], bpz = L.apz[k];
+    const double bc = -(bmx + bpx) + -(bmy + bpy) + -(bmz + bpz);
+    const double res = div[id] - p[id] * bc - p[id - 1] * bmx - p[id + 1] * bpx - p[id - NX] * bmy -
+                       p[id + NX] * bpy - p[id - NXY] * bmz - p[id + NXY] * bpz;
+    const double flag = (1.0 - (double)ib[id]) * (1.0 - (double)gh[id]);
+    r2 = res * flag * (res * flag);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = r2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_ref_change(const double *p, const double *pt, const int8_t *ib, int nx, int ny, int nz, double *part) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ni = nx - 1, nj = ny - 1, n = ni * nj * (nz - 1);
+  double v = 0.0;
+  if (e < n) {
+    const int i = 1 + (int)(e % ni), j = 1 + (int)((e / ni) % nj), k = 1 + (int)(e / (ni * nj));
+    const long long id = i + (long long)(nx + 2) * (j + (long long)(ny + 2) * k);
+    v = fabs(p[id] - pt[id]) * (1.0 - (double)ib[id]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t = fmax(t, red[w]);
+    part[blockIdx.x] = t;
+  }
+}
+
+int ref_blocks(int nx, int ny, int nz) {
+  return (int)(((long long)(nx - 1) * (ny - 1) * (nz - 1) + 255) / 256);
+}
+cudaError_t ref_residual(const double *p, const double *div, const int8_t *ib, const int8_t *gh,
+                         const DevLevel &L0, int nx, int ny, int nz, double *part, cudaStream_t s) {
+  k_ref_residual<<<ref_blocks(nx, ny, nz), 256, 0, s>>>(p, div, ib, gh, L0, nx, ny, nz, part);
+  note_launches(1);
+  return cudaGetLastError();
+}
+cudaError_t ref_change(const double *p, const double *pt, const int8_t *ib, int nx, int ny, int nz, double *part,
+                       cudaStream_t s) {
+  k_ref_change<<<ref_blocks(nx, ny, nz), 256, 0, s>>>(p, pt, ib, nx, ny, nz, part);
   note_launches(1);
   return cudaGetLastError();
 }

@@ -129,6 +129,8 @@ def lib():
         L.fg_launch_count.argtypes = [C.POINTER(C.c_longlong)]
         L.fg_case_profile.argtypes = [vp, ip]
         L.fg_case_solve_mode.argtypes = [vp, C.POINTER(C.c_int)]
+        L.fg_calc_residual.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
+        L.fg_calc_residual2.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
         L.fg_case_history.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         L.fg_case_profile_read.argtypes = [vp, C.POINTER(Profile)]
         for name in ["fg_device_count", "fg_case_create", "fg_case_destroy", "fg_case_levels",
@@ -138,7 +140,7 @@ def lib():
                      "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
                      "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy", "fg_case_set_stream",
                      "fg_launch_count", "fg_case_profile", "fg_case_profile_read",
-                     "fg_case_history", "fg_case_solve_mode"]:
+                     "fg_case_history", "fg_case_solve_mode", "fg_calc_residual", "fg_calc_residual2"]:
             getattr(L, name).restype = ip
         _lib = L
     return _lib
@@ -337,6 +339,20 @@ class Case:
         _check(lib().fg_case_profile_read(self.h, C.byref(pr)), "fg_case_profile_read")
         return pr.as_dict()
 
+    def calc_residual(self, p, div) -> float:
+        """The reference's residual measure (CORE_POISSON.F90:460-551)."""
+        v = C.c_double(0.0)
+        _check(lib().fg_calc_residual(self.h, _p(np.asfortranarray(p)), _p(np.asfortranarray(div)), C.byref(v)),
+               "fg_calc_residual")
+        return v.value
+
+    def calc_residual2(self, p, p_temp) -> float:
+        """The reference's iterate change (CORE_POISSON.F90:679-724)."""
+        v = C.c_double(0.0)
+        _check(lib().fg_calc_residual2(self.h, _p(np.asfortranarray(p)), _p(np.asfortranarray(p_temp)),
+                                       C.byref(v)), "fg_calc_residual2")
+        return v.value
+
     def ghostcell_pressure(self, p, p_old=None, iterations=1):
         _check(lib().fg_ghostcell_pressure(self.h, _p(p), _p(p_old), iterations), "fg_ghostcell_pressure")
 
@@ -368,6 +384,154 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib().fg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving
+class ServeRequest(C.Structure):
+    _fields_ = [
+        ("id", C.c_longlong),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("xn", C.c_void_p), ("yn", C.c_void_p), ("zn", C.c_void_p),
+        ("nvert", C.c_int), ("ntri", C.c_int),
+        ("xyz", C.c_void_p), ("tri", C.c_void_p),
+        ("surface_type", C.c_int),
+        ("membrane_tkns", C.c_double),
+        ("nsteps", C.c_int),
+        ("div", C.c_void_p),
+        ("p", C.c_void_p),
+        ("p0", C.c_void_p),
+    ]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [
+        ("id", C.c_longlong),
+        ("status", C.c_int),
+        ("steps_done", C.c_int),
+        ("cycles_max", C.c_int),
+        ("relres_max", C.c_double),
+        ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("finished", C.c_longlong), ("pending", C.c_longlong),
+        ("active", C.c_int), ("active_peak", C.c_int),
+        ("bytes_in_use", C.c_size_t),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _serve_lib():
+    L = lib()
+    if not getattr(L, "_serve_ready", False):
+        vp, ip = C.c_void_p, C.c_int
+        L.fg_case_estimate_bytes.argtypes = [ip, ip, ip, C.POINTER(SolverConfig), C.POINTER(C.c_size_t)]
+        L.fg_server_create.argtypes = [ip, C.POINTER(SolverConfig), C.c_size_t, ip, C.POINTER(vp)]
+        L.fg_server_submit.argtypes = [vp, C.POINTER(ServeRequest)]
+        L.fg_server_poll.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
+        L.fg_server_wait_idle.argtypes = [vp, C.c_double]
+        L.fg_server_info.argtypes = [vp, C.POINTER(ServerStats)]
+        L.fg_server_clock.argtypes = [vp]
+        L.fg_server_clock.restype = C.c_double
+        L.fg_server_destroy.argtypes = [vp]
+        for name in ["fg_case_estimate_bytes", "fg_server_create", "fg_server_submit", "fg_server_poll",
+                     "fg_server_wait_idle", "fg_server_info", "fg_server_destroy"]:
+            getattr(L, name).restype = ip
+        L._serve_ready = True
+    return L
+
+
+def estimate_bytes(grid, config: SolverConfig | None = None) -> int:
+    n = C.c_size_t(0)
+    cfg = config or default_config()
+    _check(_serve_lib().fg_case_estimate_bytes(grid.nx, grid.ny, grid.nz, C.byref(cfg), C.byref(n)),
+           "fg_case_estimate_bytes")
+    return n.value
+
+
+class Server:
+    """A request stream over many cases (fg_server_*): requests are admitted
+    as slots and device memory free up and their steps overlap on the
+    device.  The host arrays handed to :meth:`submit` are kept alive here
+    until the request's result has been polled."""
+
+    def __init__(self, config: SolverConfig | None = None, budget_bytes: int = 150 * 10**9,
+                 max_active: int = 8, device: int = 0):
+        self.cfg = config or default_config()
+        h = C.c_void_p()
+        _check(_serve_lib().fg_server_create(device, C.byref(self.cfg), int(budget_bytes), max_active,
+                                             C.byref(h)), "fg_server_create")
+        self.h = h
+        self._keep = {}
+
+    def clock(self) -> float:
+        return _serve_lib().fg_server_clock(self.h)
+
+    def submit(self, rid, grid, body, divs, outs=None, p0=None):
+        """divs / outs: lists of Fortran-ordered float64 fields (outs may be
+        None: nothing is copied back)."""
+        xs = [np.ascontiguousarray(a, dtype=np.float64) for a in (grid.xn, grid.yn, grid.zn)]
+        xyz = np.ascontiguousarray(body.verts, dtype=np.float64).ravel()
+        tri = np.ascontiguousarray(body.tri, dtype=np.int32).ravel()
+        n = len(divs)
+        for d in divs:
+            assert d.dtype == np.float64 and d.flags.f_contiguous and d.shape == grid.shape
+        dptrs = (C.c_void_p * n)(*[d.ctypes.data for d in divs])
+        pptrs = None
+        if outs is not None:
+            assert len(outs) == n
+            for o in outs:
+                assert o.dtype == np.float64 and o.flags.f_contiguous and o.shape == grid.shape
+            pptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        r = ServeRequest()
+        r.id = rid
+        r.nx, r.ny, r.nz = grid.nx, grid.ny, grid.nz
+        r.xn, r.yn, r.zn = (a.ctypes.data for a in xs)
+        r.nvert, r.ntri = body.nvert, body.ntri
+        r.xyz, r.tri = xyz.ctypes.data, tri.ctypes.data
+        r.surface_type, r.membrane_tkns = body.surface, body.membrane_tkns
+        r.nsteps = n
+        r.div = C.cast(dptrs, C.c_void_p)
+        r.p = C.cast(pptrs, C.c_void_p) if pptrs is not None else None
+        r.p0 = p0.ctypes.data if p0 is not None else None
+        rc = _serve_lib().fg_server_submit(self.h, C.byref(r))
+        _check(rc, "fg_server_submit")
+        self._keep[rid] = (xs, xyz, tri, divs, outs, dptrs, pptrs, p0)
+
+    def poll(self, capacity=1024):
+        out = (ServeResult * capacity)()
+        n = C.c_int(0)
+        _check(_serve_lib().fg_server_poll(self.h, out, capacity, C.byref(n)), "fg_server_poll")
+        res = [out[i].as_dict() for i in range(n.value)]
+        for r in res:
+            self._keep.pop(r["id"], None)
+        return res
+
+    def wait_idle(self, timeout_s=600.0):
+        _check(_serve_lib().fg_server_wait_idle(self.h, timeout_s), "fg_server_wait_idle")
+
+    def info(self) -> dict:
+        st = ServerStats()
+        _check(_serve_lib().fg_server_info(self.h, C.byref(st)), "fg_server_info")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            _serve_lib().fg_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -153,6 +153,14 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div,
 fg_status fg_solve_poisson_device(fg_case *c, double *d_p,
                                   const double *d_div, const double *d_p_old,
                                   fg_solve_stats *st);
+/* Replaces calc_residual (CORE_POISSON.F90:460-551) on the device:
+ * *maxres = sqrt(sum r^2 / (nx ny nz)), r = div - A p over the fluid,
+ * non-ghost interior cells, p read with its own outer ghost layers; the
+ * normalisation by node counts is the reference's.  Host fields. */
+fg_status fg_calc_residual(fg_case *c, const double *p, const double *div, double *maxres);
+/* Replaces calc_residual2 (CORE_POISSON.F90:679-724) on the device:
+ * *maxres2 = max |p - p_temp| over the non-iblank interior cells. */
+fg_status fg_calc_residual2(fg_case *c, const double *p, const double *p_temp, double *maxres2);
 /* One ghost/dead-cell update pass on a host field (GCM_ghostcell_pressure
  * with itermax_gc iterations). */
 fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old,
@@ -247,6 +255,68 @@ fg_status fg_batch_add(fg_batch *b, fg_case *c);
 fg_status fg_batch_solve_device(fg_batch *b, double **d_p,
                                 const double **d_div, fg_solve_stats *st);
 fg_status fg_batch_destroy(fg_batch *b);
+
+/* ----- serving: a stream of solve requests over many cases (no reference
+ * counterpart: the reference runs one case per process and calls
+ * rhs_poisson -> solve_poisson once per time step, CORE_TIME_STEP.F90
+ * :171-178) -----
+ * An engine thread admits requests first come, first served while at most
+ * max_active cases are resident and their estimated device memory
+ * (fg_case_estimate_bytes) stays within budget_bytes; a request that
+ * arrives while others run is admitted as soon as a slot and memory free
+ * up.  Each admitted request gets its own case (hierarchy, device
+ * tagging, lists) on its own stream, resident across its steps; every
+ * step is the right-hand side's copy in, the FGMRES solve as one CUDA
+ * graph launch and the pressure's copy out, and the steps of different
+ * requests overlap on the device.  Step s starts from step s-1's pressure
+ * (step 0 from p0, NULL = zero).  The host fields div[s] (and p[s], if
+ * given) belong to the caller until the request's result is polled;
+ * page-locked buffers keep the copies asynchronous. */
+typedef struct fg_server fg_server;
+typedef struct fg_serve_request {
+  long long id;                   /* the caller's tag, echoed in the result */
+  int nx, ny, nz;                 /* node counts                            */
+  const double *xn, *yn, *zn;     /* node coordinates (copied at submit)    */
+  int nvert, ntri;                /* one body surface (copied at submit)    */
+  const double *xyz;
+  const int32_t *tri;
+  int surface_type;               /* FG_SOLID or FG_MEMBRANE                */
+  double membrane_tkns;
+  int nsteps;                     /* time steps of the request              */
+  const double *const *div;       /* nsteps right-hand sides (reference layout) */
+  double *const *p;               /* nsteps outputs, or NULL (no copy out)  */
+  const double *p0;               /* initial pressure of step 0, or NULL    */
+} fg_serve_request;
+typedef struct fg_serve_result {
+  long long id;
+  fg_status status;               /* FG_OK, FG_NOT_CONVERGED or an error    */
+  int steps_done;
+  int cycles_max;                 /* most cycles of a step                  */
+  double relres_max;              /* worst final relative residual          */
+  double t_submit, t_admit, t_done;  /* server clock (s): latency = t_done - t_submit */
+} fg_serve_result;
+typedef struct fg_server_stats {
+  long long submitted, finished, pending;
+  int active, active_peak;
+  size_t bytes_in_use;            /* estimated device bytes of active cases */
+} fg_server_stats;
+/* Device memory a case of this grid and configuration holds (levels,
+ * Krylov vectors, staging, tagging), the admission estimate. */
+fg_status fg_case_estimate_bytes(int nx, int ny, int nz, const fg_solver_config *cfg, size_t *bytes);
+fg_status fg_server_create(int device, const fg_solver_config *cfg, size_t budget_bytes, int max_active,
+                           fg_server **out);
+/* Queues a request (FG_REJECTED if it alone exceeds the budget). */
+fg_status fg_server_submit(fg_server *s, const fg_serve_request *req);
+/* Results of finished requests, oldest first (up to capacity). */
+fg_status fg_server_poll(fg_server *s, fg_serve_result *out, int capacity, int *count);
+/* Waits until every submitted request has finished (FG_TIMEOUT after
+ * timeout_s seconds). */
+fg_status fg_server_wait_idle(fg_server *s, double timeout_s);
+fg_status fg_server_info(const fg_server *s, fg_server_stats *out);
+/* Seconds since the server was created (the clock of the results). */
+double fg_server_clock(const fg_server *s);
+/* Finishes every submitted request, then stops the engine. */
+fg_status fg_server_destroy(fg_server *s);
 
 #ifdef __cplusplus
 }

@@ -307,3 +307,28 @@ def test_batch64_problems_each_reach_their_solution(prec):
     bt.close()
     for c in cases:
         c.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_two_colour_sweep_matches_one_launch_per_colour(prec, monkeypatch):
+    """y and z lines of 65..256 cells of a single problem take both zebra
+    colours in one launch (work items by ticket, colour-1 items waiting for
+    their neighbour planes' colour 0); the arithmetic is that of one launch
+    per colour, so both give identical fields."""
+    grid = synth.Grid(synth.uniform_nodes(48, 0, 3), synth.tanh_nodes(96, 0, 2, 2.0),
+                      synth.tanh_nodes(80, 0, 2, 2.0))
+    bodies = [synth.sphere_body((1.0, 1.0, 1.0), 0.8, 4)]
+    _, ib, rhs, phi = _problem(grid, bodies)
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    out = []
+    for two in ("0", "1"):
+        monkeypatch.setenv("FEICAR_B200_ZEBRA_TWO_LAUNCH", two)
+        c = _case(grid, bodies, precision=p_, rtol=1e-11, max_cycles=60)
+        p = np.zeros(grid.shape, order="F")
+        st = c.solve_poisson(p, rhs)
+        out.append((st, p, c.history()))
+        c.close()
+    assert out[0][0]["cycles"] == out[1][0]["cycles"]
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert _relerr(out[0][1], phi, _fluid(grid, ib)) <= 1e-8
