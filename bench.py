@@ -276,6 +276,11 @@ def run_batch(torch, fg, synth, args, dev, stream, R):
             bt.add(c)
         P = [t.data_ptr() for t in d_p]
         F = [t.data_ptr() for t in d_f]
+        # line-kernel families and smoothing steps measured on this batch (untimed)
+        t_tune = time.time()
+        with torch.cuda.stream(stream):
+            tuning = fg.batch_autotune(bt, P, F) if not args.no_autotune else None
+        t_tune = time.time() - t_tune
 
         def batch_once():
             for t in d_p:
@@ -314,7 +319,7 @@ def run_batch(torch, fg, synth, args, dev, stream, R):
                           "cycles": st["cycles"], "relres": st["relres"],
                           "launches_per_batch": (n1 - n0) / args.steps,
                           "one_by_one_solves_per_s": len(allp) / (ms_solo / 1e3),
-                          "setup_s": t_setup}
+                          "setup_s": t_setup, "autotune_s": t_tune, "tuning": tuning}
         bt.close()
         for c in cases:
             c.close()
@@ -332,7 +337,9 @@ def run_batch(torch, fg, synth, args, dev, stream, R):
         "config": {"workload": "batch64", "problems": len(allp), "cells": cells,
                    "edges": [g.nx - 1 for g, _, _ in allp], "rtol": RTOL,
                    "parallelism": f"replicas x{R.world} (problems split by cost)",
-                   "cycle": "FGMRES(8) right-preconditioned by one V(2,2) cycle (CUDA graph), one launch per stage for all problems",
+                   "cycle": "FGMRES(8) right-preconditioned by one V(nu1,nu2) cycle, the whole solve one CUDA graph "
+                            "launch, one launch per stage for all problems; line-kernel families and (nu1,nu2) "
+                            "chosen by the autotuner on the batch (see each precision's tuning)",
                    "l2": "inputs larger than L2"},
         "step": "one batched solve of all 64 problems from zero to 1e-8",
         "mixed": out["mixed"], "fp64": out["fp64"]}), flush=True)
@@ -883,6 +890,7 @@ def main():
     ap.add_argument("--serve-low-rate", type=float, default=20.0, help="serve: a lower rate")
     ap.add_argument("--serve-low-seconds", type=float, default=5.0)
     ap.add_argument("--serve-slots", type=int, default=16, help="serve: most requests resident at once")
+    ap.add_argument("--no-autotune", action="store_true", help="batch64: default kernel families and V(2,2)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="one case, timed solves only (for kernel profiling)")
     args = ap.parse_args()

@@ -515,6 +515,16 @@ struct fg_batch {
     int *d_gn = nullptr;
     int maxgn = 0;
   } ls[kMaxLevels];
+  // line kernel family per level set and axis (k::LV_*), chosen by the
+  // autotuner; kept across table rebuilds while the level sets' line
+  // lengths stay those it was measured on
+  struct Tune {
+    int var[kMaxLevels][3] = {};
+    double us[kMaxLevels][3] = {};
+    std::vector<int> key;
+    bool nu_tuned = false;
+    double solve_ms[4] = {0, 0, 0, 0};
+  } tune;
   // the small levels (k_small_cycle): from level small_L down, one block per
   // problem whose hierarchy reaches small_L (small_L == maxdepth: none)
   int small_L = 0;
@@ -543,10 +553,6 @@ struct fg_batch {
   fg_solve_stats rich_stats{};
   std::vector<double> history;  // max relative residual over the batch after each cycle
   int last_mode = 0;  // how the last solve ran: 0 host-driven launches, 1 one graph launch
-  // counters of the two-colour y/z sweeps (k::line_sweep_zz); null: one
-  // launch per colour (FEICAR_B200_ZEBRA_TWO_LAUNCH=1 at batch build)
-  void *zz_ctl = nullptr;
-  int *h_zzerr = nullptr;  // page-locked copy of its error flag
   // FGMRES state (outer == FG_OUTER_FGMRES): per problem the FP64 vectors
   // P, F and the basis V_0..V_m, Z_0..Z_{m-1} (FP32 in the mixed path) of
   // the finest level's layout
@@ -625,9 +631,8 @@ static void free_batch_tables(fg_batch *b) {
   b->h_small.clear();
   fg::dev_free(b->d_rprob); fg::dev_free(b->d_rtgt); fg::dev_free(b->d_rcell); fg::dev_free(b->d_rw);
   fg::dev_free(b->d_rc0); fg::dev_free(b->d_rd); fg::dev_free(b->d_rf); fg::dev_free(b->d_tmp);
-  fg::dev_free(b->d_norm); fg::dev_free(b->d_part); fg::dev_free(b->zz_ctl);
+  fg::dev_free(b->d_norm); fg::dev_free(b->d_part);
   b->d_part = nullptr;
-  b->zz_ctl = nullptr;
   if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
   b->vg = fg_batch::VGraph();
   if (b->sg.exec) cudaGraphExecDestroy(b->sg.exec);
@@ -780,6 +785,9 @@ static fg_status upload_geometry(fg_batch *b) {
   return FG_OK;
 }
 
+static std::vector<int> tune_key(const fg_batch *b);
+static fg_status rebuild_line_offsets(fg_batch *b, int L, int axis);
+
 static fg_status build_batch(fg_batch *b) {
   if (b->built && b->sig == batch_signature(b)) return upload_geometry(b);
   free_batch_tables(b);
@@ -806,9 +814,9 @@ static fg_status build_batch(fg_batch *b) {
         vS.push_back(d);
         vSn.push_back(c->lev[L + 1].dl);
         bc.push_back(k::blocks_cells(d));
-        bx.push_back(k::blocks_xline(d, s.maxnx));
-        by.push_back(k::blocks_tile(d, 1, s.maxny));
-        bz.push_back(k::blocks_tile(d, 2, s.maxnz));
+        bx.push_back(k::blocks_xline(d, s.maxnx, b->tune.var[L][0]));
+        by.push_back(k::blocks_tile(d, 1, s.maxny, b->tune.var[L][1]));
+        bz.push_back(k::blocks_tile(d, 2, s.maxnz, b->tune.var[L][2]));
         bn.push_back(k::blocks_cells(c->lev[L + 1].dl));
         bq.push_back(k::blocks_quads(d));
         s.ncells += (double)d.nx * d.ny * d.nz;
@@ -882,6 +890,17 @@ static fg_status build_batch(fg_batch *b) {
   }
   fg_status st;
   if ((st = upload_geometry(b)) != FG_OK) return st;
+  if (b->tune.key != tune_key(b)) {
+    // tuned for other line lengths: back to the default families
+    const bool had = !b->tune.key.empty();
+    b->tune = fg_batch::Tune();
+    if (had) {
+      for (int L = 0; L < b->maxdepth; ++L)
+        if (!b->ls[L].S.empty())
+          for (int a = 0; a < 3; ++a)
+            if ((st = rebuild_line_offsets(b, L, a)) != FG_OK) return st;
+    }
+  }
   FG_CUDA(fg::dev_alloc(&b->d_norm, 3 * np * sizeof(double)));
   FG_CUDA(fg::dev_alloc(&b->d_part, (size_t)std::max(1, std::max(b->all0.blocks, b->all0q.blocks)) * sizeof(double)));
   if (b->h_norm_n < (size_t)(3 * np)) {
@@ -891,13 +910,6 @@ static fg_status build_batch(fg_batch *b) {
     b->h_norm_n = 3 * np;
   }
   std::fill(b->h_norm, b->h_norm + 3 * np, 0.0);
-  {
-    const char *two = getenv("FEICAR_B200_ZEBRA_TWO_LAUNCH");
-    if (!(two && two[0] == '1')) {
-      FG_CUDA(fg::dev_alloc(&b->zz_ctl, k::zz_ctl_bytes()));
-      FG_CUDA(cudaMemset(b->zz_ctl, 0, k::zz_ctl_bytes()));
-    }
-  }
   b->sig = batch_signature(b);
   b->built = true;
   return FG_OK;
@@ -965,24 +977,9 @@ static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
     const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
     const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
     const int cls = L == 0 ? FG_PROF_LINE_X0 + axis : FG_PROF_LINE_COARSE;
-    bool fused = false;
-    if (axis > 0 && b->zz_ctl && ls.S.size() == 1) {
-      // one problem at this level: both colours in one launch
+    for (int color = 0; color < 2; ++color) {
       const size_t e0 = prof_begin(b, s);
-      const cudaError_t e = k::line_sweep_zz<T>(ls.d_levS, b->cases[ls.S[0]]->lev[L].dl, axis, om, b->zz_ctl, s);
-      if (e == cudaSuccess) {
-        fused = true;
-        prof_end(b, e0, cls, 2.0 * sweep_bytes<T>(ls.ncells, om), s);
-      } else if (e != cudaErrorNotSupported) {
-        set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
-        return FG_CUDA_ERROR;
-      } else if (e0 != (size_t)-1) {
-        b->prof.used -= 2;  // nothing was launched between the events
-      }
-    }
-    for (int color = 0; color < 2 && !fused; ++color) {
-      const size_t e0 = prof_begin(b, s);
-      FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, s));
+      FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, b->tune.var[L][axis], s));
       prof_end(b, e0, cls, sweep_bytes<T>(ls.ncells, om), s);
     }
     if (L == 0) {
@@ -1567,13 +1564,6 @@ static fg_status fgmres_enqueue(fg_batch *b) {
   if (r != FG_OK) return r;
   FG_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
   FG_CUDA(cudaMemcpyAsync(b->h_kctl, b->d_kctl, sizeof(KCtl), cudaMemcpyDeviceToHost, s));
-  if (b->zz_ctl) {
-    if (!b->h_zzerr) {
-      b->h_zzerr = static_cast<int *>(pinned_get(4 * sizeof(int)));
-      if (!b->h_zzerr) return FG_ALLOC_FAIL;
-    }
-    FG_CUDA(cudaMemcpyAsync(b->h_zzerr, b->zz_ctl, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
-  }
   FG_CUDA(cudaEventRecord(b->ev1, s));
   b->pending = true;
   return FG_OK;
@@ -1586,10 +1576,6 @@ static fg_status fgmres_collect(fg_batch *b, fg_solve_stats *st) {
   const int np = (int)b->cases.size();
   FG_CUDA(cudaEventSynchronize(b->ev1));
   const KCtl &C = *b->h_kctl;
-  if (b->zz_ctl && b->h_zzerr && k::zz_error(b->h_zzerr)) {
-    set_last_error("a two-colour line sweep gave up waiting for its neighbour planes", __FILE__, __LINE__);
-    return FG_TIMEOUT;
-  }
   if (b->last_mode == 1) {
     const auto &SG = b->sg;
     note_launches(SG.n_pre + C.n_restart * SG.n_restart + C.n_body * SG.n_body + C.n_inner * SG.n_inner +
@@ -1611,12 +1597,74 @@ static fg_status fgmres_collect(fg_batch *b, fg_solve_stats *st) {
   return C.status == FG_OK ? FG_OK : FG_NOT_CONVERGED;
 }
 
+// Single-grid line SOR (CORE_POISSON.F90:205-456, it_solver_type = 1):
+// sweeps of x, y and z line relaxation (zebra here, lexicographic x and z
+// lines in the reference) with omega and the ghost/dead rows relaxed after
+// each direction, on the finest level in FP64 and in solution form, until
+// the fluid-row relative residual meets rtol (checked every kLsorCheck
+// sweeps) or max_cycles sweeps have run.  Converges to the same fixed point
+// as the multigrid solve, many times more slowly; kept for callers that
+// select the reference's solver type 1.
+constexpr int kLsorCheck = 16;
+static fg_status batch_solve_lsor(fg_batch *b, fg_solve_stats *st) {
+  const int np = (int)b->cases.size();
+  cudaStream_t s = b->stream;
+  if (b->ls[0].S.empty()) return FG_BAD_INPUT;  // a single-level grid has no line launches
+  if (!b->ev0) { cudaEventCreate(&b->ev0); cudaEventCreate(&b->ev1); }
+  FG_CUDA(cudaEventRecord(b->ev0, s));
+  FG_K(k::rows_relax<double>(b->rows, b->d_lev0, 0, b->d_tmp, s));
+  FG_CUDA(cudaMemsetAsync(b->d_norm, 0, 3 * np * sizeof(double), s));
+  FG_K(k::fluid_norm(b->all0, b->d_norm + np, b->d_part, s));
+  b->history.clear();
+  fg_status status = FG_NOT_CONVERGED;
+  int sweeps = 0;
+  double worst = 1.0, gmax = 0.0;
+  while (sweeps < b->cfg.max_cycles) {
+    const int n = std::min(kLsorCheck, b->cfg.max_cycles - sweeps);
+    for (int q = 0; q < n; ++q) {
+      fg_status r = smooth<double>(b, 0, s);
+      if (r != FG_OK) return r;
+    }
+    sweeps += n;
+    FG_CUDA(cudaMemsetAsync(b->d_norm, 0, np * sizeof(double), s));
+    FG_CUDA(cudaMemsetAsync(b->d_norm + 2 * np, 0, np * sizeof(double), s));
+    FG_K(k::residual<double>(b->all0, b->d_norm, b->d_part, s));
+    FG_K(k::rows_residual(b->rows, b->d_lev0, b->d_norm + 2 * np, s));
+    FG_CUDA(cudaMemcpyAsync(b->h_norm, b->d_norm, 3 * np * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    worst = 0.0;
+    gmax = 0.0;
+    for (int p = 0; p < np; ++p) {
+      const double f2 = b->h_norm[np + p];
+      const double rr = f2 > 0.0 ? std::sqrt(b->h_norm[p] / f2) : std::sqrt(b->h_norm[p]);
+      worst = std::max(worst, rr);
+      gmax = std::max(gmax, b->h_norm[2 * np + p]);
+    }
+    b->history.push_back(worst);
+    if (worst <= b->cfg.rtol) { status = FG_OK; break; }
+  }
+  FG_CUDA(cudaEventRecord(b->ev1, s));
+  FG_CUDA(cudaEventSynchronize(b->ev1));
+  float tot = 0.0f;
+  cudaEventElapsedTime(&tot, b->ev0, b->ev1);
+  if (b->prof.on) prof_collect(b);
+  if (st) {
+    st->cycles = sweeps;
+    st->relres = worst;
+    st->ghost_res = gmax;
+    st->seconds = tot * 1e-3;
+    st->vcycle_ms = sweeps > 0 ? (double)tot / sweeps : 0.0;
+  }
+  return status;
+}
+
 // Queues one solve of the batch on its stream (FGMRES: a single graph
 // launch in the usual case); batch_collect waits for it.  The Richardson
 // outer iteration runs to completion here.
 static fg_status batch_enqueue(fg_batch *b) {
   if (b->cfg.outer != FG_OUTER_FGMRES) {
-    b->rich_status = batch_solve_richardson(b, &b->rich_stats);
+    b->rich_status = b->cfg.outer == FG_OUTER_LSOR ? batch_solve_lsor(b, &b->rich_stats)
+                                                    : batch_solve_richardson(b, &b->rich_stats);
     b->pending = true;
     return (b->rich_status == FG_OK || b->rich_status == FG_NOT_CONVERGED) ? FG_OK : b->rich_status;
   }
@@ -1638,6 +1686,105 @@ static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
   fg_status r = batch_enqueue(b);
   if (r != FG_OK) return r;
   return batch_collect(b, st);
+}
+
+// ------------------------------------------------------------ autotuner
+// line lengths of the level sets, the key the tuned choices belong to
+static std::vector<int> tune_key(const fg_batch *b) {
+  std::vector<int> k;
+  for (int L = 0; L < b->maxdepth; ++L) {
+    k.push_back(b->ls[L].maxnx); k.push_back(b->ls[L].maxny); k.push_back(b->ls[L].maxnz);
+    k.push_back((int)b->ls[L].S.size());
+  }
+  return k;
+}
+
+// launch offsets of one level set's sweeps along `axis` for its current
+// kernel family
+static fg_status rebuild_line_offsets(fg_batch *b, int L, int axis) {
+  auto &s = b->ls[L];
+  std::vector<int> blocks;
+  for (int p : s.S) {
+    const DevLevel &d = b->cases[p]->lev[L].dl;
+    blocks.push_back(axis == 0 ? k::blocks_xline(d, s.maxnx, b->tune.var[L][0])
+                               : k::blocks_tile(d, axis, axis == 1 ? s.maxny : s.maxnz, b->tune.var[L][axis]));
+  }
+  int **off = axis == 0 ? &s.d_off_x : axis == 1 ? &s.d_off_y : &s.d_off_z;
+  Launch &Lr = axis == 0 ? s.xl : axis == 1 ? s.yl : s.zl;
+  fg::dev_free(*off);
+  *off = nullptr;
+  return build_offsets(blocks, off, Lr, s.d_levS);
+}
+
+// the captured V-cycle and solve graphs hold the old launch shapes
+static void drop_graphs(fg_batch *b) {
+  if (b->vg.exec) cudaGraphExecDestroy(b->vg.exec);
+  b->vg.exec = nullptr;
+  b->vg.key = -1;
+  if (b->sg.exec) cudaGraphExecDestroy(b->sg.exec);
+  b->sg.exec = nullptr;
+  b->sg.key = -1;
+  b->sg.params.clear();
+}
+
+// Times every kernel family that can take each level set's lines (two
+// colours, three repetitions after a warm-up, CUDA events) and keeps the
+// fastest.  The sweeps run on the levels' current arrays, which every
+// solve overwrites before reading.  Levels the one-block small cycle
+// takes have no line launches and are skipped.
+template <typename T>
+static fg_status tune_lines(fg_batch *b) {
+  cudaStream_t s = b->stream;
+  const double om = b->cfg.omega;
+  cudaEvent_t e0, e1;
+  FG_CUDA(cudaEventCreate(&e0));
+  FG_CUDA(cudaEventCreate(&e1));
+  fg_status st = FG_OK;
+  const int Ls = std::min(b->maxdepth, b->small_L);
+  for (int L = 0; L < Ls && st == FG_OK; ++L) {
+    auto &ls = b->ls[L];
+    if (ls.S.empty()) continue;
+    for (int axis = 0; axis < 3 && st == FG_OK; ++axis) {
+      const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
+      std::vector<int> cand;
+      for (int v = 1; v <= 3; ++v) {
+        const int r = k::line_variant(axis, maxn, v);
+        if (std::find(cand.begin(), cand.end(), r) == cand.end()) cand.push_back(r);
+      }
+      double best = 1e300;
+      int bestv = cand[0];
+      for (int v : cand) {
+        b->tune.var[L][axis] = v;
+        if ((st = rebuild_line_offsets(b, L, axis)) != FG_OK) break;
+        const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
+        cudaError_t e = cudaSuccess;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+          if (rep == 1) e = cudaEventRecord(e0, s);
+          for (int color = 0; color < 2 && e == cudaSuccess; ++color)
+            e = k::line_sweep<T>(Lr, axis, color, om, maxn, v, s);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+          set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+          st = FG_CUDA_ERROR;
+          break;
+        }
+        const double us = 1e3 * ms / 3.0;
+        if (us < best) { best = us; bestv = v; }
+      }
+      if (st != FG_OK) break;
+      b->tune.var[L][axis] = bestv;
+      b->tune.us[L][axis] = best;
+      st = rebuild_line_offsets(b, L, axis);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  drop_graphs(b);
+  return st;
 }
 
 // -------------------------------------------------------- case geometry
@@ -1972,6 +2119,7 @@ fg_status fg_case_destroy(fg_case *c) {
   fg::dev_free(c->d_G); fg::dev_free(c->d_gidx); fg::dev_free(c->d_pin); fg::dev_free(c->d_fin);
   fg::dev_free(c->d_refmask); fg::dev_free(c->d_rowtgt);
   fg::dev_free(c->d_gauge);
+  fg::dev_free(c->d_pgrad); fg::dev_free(c->d_met); fg::dev_free(c->d_cpart); fg::dev_free(c->d_pmet);
   if (c->geom) geom_free(*c->geom);
   if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -2178,14 +2326,60 @@ static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
 
 // outer-face data of a case (Dirichlet values; Neumann faces carry no
 // gradient data: homogeneous)
+static long long pgrad_size(const fg_case *c, int face) {
+  const long long NX = c->nx + 2, NY = c->ny + 2, NZ = c->nz + 2;
+  return face < 2 ? NY * NZ : face < 4 ? NX * NZ : NX * NY;
+}
+static long long pgrad_offset(const fg_case *c, int face) {
+  long long o = 0;
+  for (int q = 0; q < face; ++q) o += pgrad_size(c, q);
+  return o;
+}
+
 static k::FaceData face_data(const fg_case *c) {
   k::FaceData fd{};
   for (int f = 0; f < 6; ++f) {
     fd.pbc[f] = c->cfg.pbc[f];
     fd.ppp[f] = c->cfg.ppp[f];
-    fd.pgrad[f] = nullptr;
+    fd.pgrad[f] = c->d_pgrad ? c->d_pgrad + pgrad_offset(c, f) : nullptr;
   }
   return fd;
+}
+
+// the face gradients (zero) and the compatibility step's metrics and
+// scratch, made on first use
+static fg_status ensure_pgrad(fg_case *c) {
+  if (c->d_pgrad) return FG_OK;
+  const long long n = pgrad_offset(c, 6);
+  FG_CUDA(fg::dev_alloc(&c->d_pgrad, (size_t)n * sizeof(double)));
+  FG_CUDA(cudaMemsetAsync(c->d_pgrad, 0, (size_t)n * sizeof(double), c->stream));
+  const HLevel &L = c->lev[0];
+  std::vector<double> met;
+  for (const std::vector<double> *x : {&L.x, &L.y, &L.z}) {
+    const size_t m = x->size();  // n + 2
+    for (size_t i = 0; i < m; ++i) met.push_back(i + 1 < m ? (*x)[i + 1] - (*x)[i] : 0.0);
+  }
+  for (const std::vector<double> *v : {&L.dxcinv, &L.dycinv, &L.dzcinv}) met.insert(met.end(), v->begin(), v->end());
+  FG_CUDA(fg::dev_alloc(&c->d_met, met.size() * sizeof(double)));
+  FG_CUDA(cudaMemcpy(c->d_met, met.data(), met.size() * sizeof(double), cudaMemcpyHostToDevice));
+  FG_CUDA(fg::dev_alloc(&c->d_cpart, (size_t)(k::ref_blocks(c->nx, c->ny, c->nz) + 1) * sizeof(double)));
+  return FG_OK;
+}
+
+// GCM_enforce_p_compatibility on a device field in the reference layout:
+// skipped when a face is Dirichlet or no face is zero-gradient
+// (GCM_GHOSTCELL_UPDATE.F90:878-890)
+static fg_status compat_device(fg_case *c, const double *d_p, int vzg) {
+  for (int f = 0; f < 6; ++f)
+    if (c->cfg.pbc[f] == FG_PBC_DIRICHLET) return FG_OK;
+  if (!(vzg & 63)) return FG_OK;
+  fg_status st = ensure_pgrad(c);
+  if (st != FG_OK) return st;
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  const int nb = k::ref_blocks(c->nx, c->ny, c->nz);
+  FG_K(k::compat(d_p, c->d_refmask, c->d_refmask + nref, c->d_met, c->nx, c->ny, c->nz, vzg & 63, c->d_cpart,
+                 c->d_cpart + nb, c->d_pgrad, c->stream));
+  return FG_OK;
 }
 
 // gauge and outer boundary layers on the device copy of the output
@@ -2216,6 +2410,9 @@ fg_status fg::solve_enqueue(fg_case *c, const double *p_old, const double *dpdn_
   HLevel &L0 = c->lev[0];
   FG_K(k::copy_in(L0.d_x64, c->d_pin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
   FG_K(k::copy_in(L0.d_rhs64, c->d_fin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  // GCM_enforce_p_compatibility (CORE_POISSON.F90:160) once, from the
+  // initial pressure, when some face's velocity is zero-gradient
+  if (c->vzg && (s = compat_device(c, c->d_pin, c->vzg)) != FG_OK) return s;
   FG_K(k::face_rhs(L0.d_rhs64, L0.dl, face_data(c), c->stream));
   if ((s = batch_enqueue(c->solo)) != FG_OK) return s;
   FG_K(k::copy_out(c->d_pin, L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
@@ -2296,6 +2493,57 @@ fg_status fg_calc_residual(fg_case *c, const double *p, const double *div, doubl
 
 fg_status fg_calc_residual2(fg_case *c, const double *p, const double *p_temp, double *maxres2) {
   return ref_measure(c, p, p_temp, true, maxres2);
+}
+
+fg_status fg_set_pressure_gradient(fg_case *c, int face, const double *values) {
+  if (!c || face < 0 || face > 5 || !values) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  fg_status st = ensure_pgrad(c);
+  if (st != FG_OK) return st;
+  FG_CUDA(cudaMemcpyAsync(c->d_pgrad + pgrad_offset(c, face), values, pgrad_size(c, face) * sizeof(double),
+                          cudaMemcpyHostToDevice, c->stream));
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+fg_status fg_get_pressure_gradient(fg_case *c, int face, double *values) {
+  if (!c || face < 0 || face > 5 || !values) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  if (!c->d_pgrad) {
+    std::fill(values, values + pgrad_size(c, face), 0.0);
+    return FG_OK;
+  }
+  FG_CUDA(cudaMemcpyAsync(values, c->d_pgrad + pgrad_offset(c, face), pgrad_size(c, face) * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->stream));
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+fg_status fg_case_set_zero_gradient_faces(fg_case *c, const int *vel_zero_gradient) {
+  if (!c) return FG_BAD_INPUT;
+  c->vzg = 0;
+  if (vel_zero_gradient)
+    for (int f = 0; f < 6; ++f)
+      if (vel_zero_gradient[f]) c->vzg |= 1 << f;
+  return FG_OK;
+}
+
+fg_status fg_enforce_p_compatibility(fg_case *c, const double *p, const int *vel_zero_gradient) {
+  if (!c || !p || !vel_zero_gradient) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  if (!c->prepared) {
+    fg_status st = prepare(c);
+    if (st != FG_OK) return st;
+  }
+  int vzg = 0;
+  for (int f = 0; f < 6; ++f)
+    if (vel_zero_gradient[f]) vzg |= 1 << f;
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  FG_CUDA(cudaMemcpyAsync(c->d_pin, p, nref * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  fg_status st = compat_device(c, c->d_pin, vzg);
+  if (st != FG_OK) return st;
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
 }
 
 fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old, int iterations) {
@@ -2384,6 +2632,82 @@ fg_status fg_batch_solve_device(fg_batch *b, double **d_p, const double **d_div,
   return s;
 }
 
+fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_tuning *out) {
+  if (!b || b->cases.empty() || !d_p || !d_div) return FG_BAD_INPUT;
+  cudaSetDevice(b->device);
+  // a first solve builds the tables (and is the warm-up)
+  fg_solve_stats st{};
+  fg_status r = fg_batch_solve_device(b, d_p, d_div, &st);
+  if (r != FG_OK && r != FG_NOT_CONVERGED) return r;
+  b->tune = fg_batch::Tune();
+  for (int L = 0; L < b->maxdepth; ++L)
+    if (!b->ls[L].S.empty())
+      for (int a = 0; a < 3; ++a)
+        if ((r = rebuild_line_offsets(b, L, a)) != FG_OK) return r;
+  r = b->cfg.precision == FG_PREC_MIXED ? tune_lines<float>(b) : tune_lines<double>(b);
+  if (r != FG_OK) return r;
+  // smoothing steps: each candidate solves the problems from zero (the
+  // second of two solves is timed: the first captures its graph)
+  static const int cand[4][2] = {{1, 1}, {2, 1}, {2, 2}, {3, 3}};
+  double best = 1e300;
+  int bi = 2;
+  for (int q = 0; q < 4; ++q) {
+    b->cfg.nu1 = cand[q][0];
+    b->cfg.nu2 = cand[q][1];
+    drop_graphs(b);
+    for (int rep = 0; rep < 2; ++rep) {
+      for (size_t p = 0; p < b->cases.size(); ++p) {
+        const fg_case *c = b->cases[p];
+        FG_CUDA(cudaMemsetAsync(d_p[p], 0, (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2) * sizeof(double),
+                                b->stream));
+      }
+      r = fg_batch_solve_device(b, d_p, d_div, &st);
+      if (r != FG_OK && r != FG_NOT_CONVERGED) return r;
+    }
+    b->tune.solve_ms[q] = r == FG_OK ? 1e3 * st.seconds : -1.0;
+    if (r == FG_OK && 1e3 * st.seconds < best) { best = 1e3 * st.seconds; bi = q; }
+  }
+  b->cfg.nu1 = cand[bi][0];
+  b->cfg.nu2 = cand[bi][1];
+  drop_graphs(b);
+  b->tune.nu_tuned = true;
+  b->tune.key = tune_key(b);
+  return fg_batch_get_tuning(b, out);
+}
+
+fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out) {
+  if (!b || !out) return FG_BAD_INPUT;
+  memset(out, 0, sizeof(*out));
+  out->nlevels = b->maxdepth;
+  for (int L = 0; L < b->maxdepth && L < FG_TUNE_MAXLEVELS; ++L)
+    for (int a = 0; a < 3; ++a) {
+      const auto &ls = b->ls[L];
+      const int maxn = a == 0 ? ls.maxnx : a == 1 ? ls.maxny : ls.maxnz;
+      const bool lines = !ls.S.empty() && L < std::min(b->maxdepth, b->small_L);
+      out->line_variant[L][a] = lines ? k::line_variant(a, maxn, b->tune.var[L][a]) : 0;
+      out->line_us[L][a] = b->tune.us[L][a];
+    }
+  out->nu1 = b->cfg.nu1;
+  out->nu2 = b->cfg.nu2;
+  for (int q = 0; q < 4; ++q) out->solve_ms[q] = b->tune.solve_ms[q];
+  out->tuned = b->tune.nu_tuned ? 1 : 0;
+  return FG_OK;
+}
+
+fg_status fg_case_autotune(fg_case *c, double *d_p, const double *d_div, fg_tuning *out) {
+  if (!c || !d_p || !d_div) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  fg_status st = ensure_solo(c);
+  if (st != FG_OK) return st;
+  // the solve entry points stage the case's own layout; the batch tuner
+  // reads the reference-layout fields directly
+  double *P[1] = {d_p};
+  const double *D[1] = {d_div};
+  st = fg_batch_autotune(c->solo, P, D, out);
+  c->batch_dirty = false;
+  return st;
+}
+
 fg_status fg_case_set_stream(fg_case *c, void *stream) {
   if (!c) return FG_BAD_INPUT;
   cudaSetDevice(c->device);
@@ -2450,7 +2774,6 @@ fg_status fg_batch_destroy(fg_batch *b) {
     if (q) cudaStreamDestroy(q);
   if (b->h_kctl) pinned_put(b->h_kctl);
   if (b->h_norm) pinned_put(b->h_norm);
-  if (b->h_zzerr) pinned_put(b->h_zzerr);
   if (b->ev0) { cudaEventDestroy(b->ev0); cudaEventDestroy(b->ev1); }
   delete b;
   return FG_OK;

@@ -109,6 +109,15 @@ struct fg_case {
   double *d_gauge = nullptr;  // p(1,1,1) of the output gauge
   bool batch_dirty = true;
   struct fg_batch *solo = nullptr;
+  // outer-face pressure gradients (the reference's pgradx1..pgradz2, six
+  // face arrays back to back), the faces whose velocity is zero-gradient
+  // (bit mask: solves first apply GCM_enforce_p_compatibility), and the
+  // reference 1-D metrics and scratch the compatibility step reads
+  double *d_pgrad = nullptr;
+  int vzg = 0;
+  double *d_met = nullptr;
+  double *d_cpart = nullptr;  // flux partials, then the correction
+  double *d_pmet = nullptr;   // grid arrays of the projection steps (fg_proj.cu)
 };
 
 namespace fg {

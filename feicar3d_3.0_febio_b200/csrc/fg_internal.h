@@ -253,24 +253,25 @@ int blocks_cells(const DevLevel &L);
 int blocks_flat(long long n);
 // quad kernels (4 cells of a row per thread)
 int blocks_quads(const DevLevel &L);
-int blocks_xline(const DevLevel &L, int maxn);
+// line kernel families of a sweep (chosen per level set and axis, by
+// default or by the autotuner): x lines in registers (lanes by line
+// length, or always 32), x lines staged in shared memory (one warp per
+// line); y/z tiles in registers with a per-line Thomas over the chunks,
+// with a block-wide PCR over the chunks, or one warp per line
+enum : int {
+  LV_DEFAULT = 0,
+  LV_XREG = 1, LV_XREG32 = 2, LV_XSMEM = 3,
+  LV_YREG = 1, LV_YPCR = 2, LV_YWARP = 3
+};
+int line_variant(int axis, int maxn, int v);  // the family that runs
+int blocks_xline(const DevLevel &L, int maxn, int variant);
 // y/z tiles: blocks depend on the kernel the level set's longest line picks
-int blocks_tile(const DevLevel &L, int axis, int maxn);
+int blocks_tile(const DevLevel &L, int axis, int maxn, int variant);
 size_t smem_line(int n, int tsize, int axis);
 
 template <typename T>
-cudaError_t line_sweep(const Launch &L, int axis, int color, double omega, int maxn,
+cudaError_t line_sweep(const Launch &L, int axis, int color, double omega, int maxn, int variant,
                        cudaStream_t s);
-// both colours of a y/z sweep of a single problem's level in one launch
-// (work items by ticket; colour-1 items wait for their neighbour planes'
-// colour 0); cudaErrorNotSupported when the level's lines do not take that
-// kernel.  ctl: zz_ctl_bytes() of zeroed device memory, reset by every
-// launch at its end.
-template <typename T>
-cudaError_t line_sweep_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, void *ctl,
-                          cudaStream_t s);
-size_t zz_ctl_bytes();
-int zz_error(const void *ctl_host);  // a wait ran out in some launch
 // norm2[p] += ||r||^2 of entry p when norm2 != null (part: one double per block)
 template <typename T>
 cudaError_t residual(const Launch &L, double *norm2, double *part, cudaStream_t s);
@@ -322,6 +323,12 @@ cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaSt
 // (block partials into part, ref_blocks of them): squared residuals of
 // calc_residual, maxima of |p - p_temp| of calc_residual2
 int ref_blocks(int nx, int ny, int nz);
+// GCM_enforce_p_compatibility on the device: pgrad (the six face arrays
+// back to back, x1 x2 y1 y2 z1 z2) shifted by the flux correction of p on
+// the faces flagged in the bit mask vzg; met: dx, dy, dz, dxcinv, dycinv,
+// dzcinv (n+2 each, reference indexing); part: ref_blocks doubles
+cudaError_t compat(const double *p, const int8_t *ib, const int8_t *gh, const double *met, int nx, int ny,
+                   int nz, int vzg, double *part, double *corr, double *pgrad, cudaStream_t s);
 cudaError_t ref_residual(const double *p, const double *div, const int8_t *ib, const int8_t *gh,
                          const DevLevel &L0, int nx, int ny, int nz, double *part, cudaStream_t s);
 cudaError_t ref_change(const double *p, const double *pt, const int8_t *ib, int nx, int ny, int nz, double *part,

@@ -1179,16 +1179,36 @@ int blocks_cells(const DevLevel &L) {
 }
 // lanes per x line of k_xline_reg for a level set whose longest x line is maxn
 int xline_lanes(int maxn) { return maxn <= 16 ? 4 : maxn <= 32 ? 8 : maxn <= 64 ? 16 : 32; }
-int blocks_xline(const DevLevel &L, int maxn) {
+// The line kernel family a level set's sweep along `axis` takes (LV_*):
+// the requested one when it can take lines of maxn cells, else the
+// default (the family measured fastest for that line length on the
+// 512x256x256 case).
+int line_variant(int axis, int maxn, int v) {
+  if (axis == 0) {
+    if (v == LV_XREG && maxn > 128) v = LV_DEFAULT;
+    if (v == LV_XREG32 && maxn > 128) v = LV_DEFAULT;
+    if (v == LV_XSMEM && maxn > 1024) v = LV_DEFAULT;
+    if (v != LV_XREG && v != LV_XREG32 && v != LV_XSMEM) v = maxn <= 128 ? LV_XREG : LV_XSMEM;
+    return v;
+  }
+  if ((v == LV_YREG || v == LV_YPCR) && maxn > YZ_MAXROWS) v = LV_DEFAULT;
+  if (v != LV_YREG && v != LV_YPCR && v != LV_YWARP)
+    v = (maxn >= YP_MINROWS && maxn <= YZ_MAXROWS) ? LV_YPCR : maxn <= YZ_MAXROWS ? LV_YREG : LV_YWARP;
+  return v;
+}
+int blocks_xline(const DevLevel &L, int maxn, int variant) {
   const long long lines = (long long)((L.ny + 1) / 2) * L.nz;
-  // lines of more than 128 cells: k_xline_smem, one line per warp
-  const long long per_block = maxn > 128 ? (long long)XS_WARPS
-                                         : (long long)XL_WARPS * (32 / xline_lanes(maxn));
+  const int v = line_variant(0, maxn, variant);
+  // k_xline_smem: one line per warp; k_xline_reg: 32 / lanes lines per warp
+  const long long per_block = v == LV_XSMEM ? (long long)XS_WARPS
+                              : v == LV_XREG32 ? (long long)XL_WARPS
+                                               : (long long)XL_WARPS * (32 / xline_lanes(maxn));
   return (int)((lines + per_block - 1) / per_block);
 }
-int blocks_tile(const DevLevel &L, int axis, int maxn) {
-  // k_yzline_reg, k_yzline_pcr or k_yzline
-  const int w = maxn < YP_MINROWS ? 64 : maxn <= YZ_MAXROWS ? 2 * YP_LINES : TILE_I;
+int blocks_tile(const DevLevel &L, int axis, int maxn, int variant) {
+  // i-tile of k_yzline_reg (64 cells), k_yzline_pcr (16) or k_yzline (16)
+  const int v = line_variant(axis, maxn, variant);
+  const int w = v == LV_YREG ? 64 : v == LV_YPCR ? 2 * YP_LINES : TILE_I;
   const int ntx = (L.nx + w - 1) / w;
   return ntx * (axis == 1 ? L.nz : L.ny);
 }
@@ -1247,113 +1267,10 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
 // chunk equations of each line are solved by parallel cyclic reduction
 // across the block (log2 CH steps through shared memory), and every thread
 // back-substitutes its rows.
-// ---- both colours of a zebra sweep in one launch (single problem)
-// Work items (one i-tile of one plane of fixed o, one colour) are taken by
-// ticket in the order c0 slab 0, c0 slab 1, c1 slab 0, c0 slab 2, c1 slab
-// 1, ..., c1 slab S-1 (a slab: `slab` consecutive planes).  A colour-1 item
-// of slab s starts once every colour-0 item of slabs s-1, s and s+1 is
-// done, so it reads the new colour-0 values of its neighbour planes, and
-// no colour-0 item reads a colour-1 value after it changed (those of slab
-// s change only after slab s+1's colour 0 is done): the same arithmetic
-// as two launches, one colour each.  The colour-0 sectors an item pulls
-// in (the other colour's rhs, mask and unknowns share them) are still in
-// L2 when the colour-1 items of the same planes run a few groups later.
-// Items wait only on items with smaller tickets, which running blocks
-// hold and finish without waiting, so the launch cannot deadlock; a wait
-// is still bounded, and when it runs out the item records an error and
-// skips its work.  The last block to finish resets the counters.
-constexpr int ZZ_MAXSLAB = 512;
-struct ZzCtl {
-  int ticket, finished, err, pad_;
-  int done0[ZZ_MAXSLAB];  // finished colour-0 items per slab
-};
-struct ZzPlan {
-  ZzCtl *ctl;
-  int nplanes;  // planes (values of o)
-  int slab;     // planes per slab
-  int nslab;
-  int ntx;      // i-tiles per plane
-  int lag;      // colour-1 groups trail the colour-0 groups by this many slabs (>= 1)
-};
-__host__ __device__ __forceinline__ int zz_tiles(const ZzPlan &z, int s) {
-  const int np = z.nplanes - s * z.slab;
-  return z.ntx * (np < z.slab ? np : z.slab);
-}
-// colour and slab of group g of the ticket order: c0 slabs 0..lag-1, then
-// pairs (c0 slab s, c1 slab s-lag), then the last lag colour-1 slabs
-__host__ __device__ __forceinline__ void zz_group(const ZzPlan &z, int g, int &color, int &slab) {
-  const int L = z.lag < z.nslab ? z.lag : z.nslab;
-  const int mid = 2 * (z.nslab - L);
-  if (g < L) { color = 0; slab = g; return; }
-  if (g < L + mid) {
-    const int h = g - L, s = L + (h >> 1);
-    if (h & 1) { color = 1; slab = s - L; } else { color = 0; slab = s; }
-    return;
-  }
-  color = 1;
-  slab = z.nslab - L + (g - L - mid);
-}
-__device__ __forceinline__ int ld_acquire(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-// block-wide: takes a ticket, decodes it (color, slab, item within the
-// slab), waits for the colour-0 items a colour-1 item depends on; returns
-// false when a wait ran out (the item then skips its work)
-__device__ bool zz_begin(const ZzPlan &z, int &color, int &slab, int &li) {
-  __shared__ int s_v[4];
-  if (threadIdx.x == 0) {
-    int t = atomicAdd(&z.ctl->ticket, 1);
-    int g = 0, cc = 0, ss = 0;
-    for (;; ++g) {
-      zz_group(z, g, cc, ss);
-      const int n = zz_tiles(z, ss);
-      if (t < n) break;
-      t -= n;
-    }
-    int ok = 1;
-    if (cc == 1) {
-      for (int q = ss - 1; q <= ss + 1 && ok; ++q) {
-        if (q < 0 || q >= z.nslab) continue;
-        const int need = zz_tiles(z, q);
-        long long spins = 0;
-        while (ld_acquire(&z.ctl->done0[q]) < need) {
-          if (++spins > (1ll << 24)) {  // ~ seconds: never reached unless something is broken
-            atomicExch(&z.ctl->err, 1);
-            ok = 0;
-            break;
-          }
-          __nanosleep(128);
-        }
-      }
-    }
-    s_v[0] = cc; s_v[1] = ss; s_v[2] = t; s_v[3] = ok;
-  }
-  __syncthreads();
-  color = s_v[0]; slab = s_v[1]; li = s_v[2];
-  return s_v[3] != 0;
-}
-// block-wide, after every thread's stores: publishes a finished colour-0
-// item; the last block of the launch resets the counters
-__device__ void zz_end(const ZzPlan &z, int color, int slab, int total) {
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (color == 0) atomicAdd(&z.ctl->done0[slab], 1);
-    if (atomicAdd(&z.ctl->finished, 1) == total - 1) {
-      for (int q = 0; q < z.nslab; ++q) z.ctl->done0[q] = 0;
-      z.ctl->ticket = 0;
-      __threadfence();
-      atomicExch(&z.ctl->finished, 0);
-    }
-  }
-}
-
-template <typename T, int M, int CH, int AXIS, bool FUSED = false>
+template <typename T, int M, int CH, int AXIS>
 __global__ void __launch_bounds__(CH * YP_LINES, ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
                                                    ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1)
-k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega, ZzPlan zz) {
+k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
   using LC = LineCoefT<T, AXIS>;
   constexpr int NT = CH * YP_LINES;
   __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
@@ -1364,23 +1281,15 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega,
   auto s_last = reinterpret_cast<T(*)[CH][YP_LINES]>(&s_eq[1][0][0]);
   const int tid = threadIdx.x;
   const int l = tid % YP_LINES, c = tid / YP_LINES;
-  int p = 0, lb = 0, zslab = 0;
-  bool work = true;
-  if constexpr (FUSED) {
-    int li = 0;
-    work = zz_begin(zz, color, zslab, li);
-    lb = zslab * zz.slab * zz.ntx + li;
-  } else {
-    p = find_entry(off, nent, blockIdx.x);
-    lb = blockIdx.x - off[p];
-  }
+  const int p = find_entry(off, nent, blockIdx.x);
+  const int lb = blockIdx.x - off[p];
   const DevLevel &L = levs[p];
   constexpr int TW = 2 * YP_LINES;  // cells of an i-tile
   const int ntx = (L.nx + TW - 1) / TW;
   const int ti = lb % ntx;
   // k for AXIS 1, j for AXIS 2; a colour-1 launch walks the planes backward,
   // so its first blocks meet the planes the colour-0 launch left in L2
-  const int o = (!FUSED && color == 1) ? (AXIS == 1 ? L.nz : L.ny) - lb / ntx : 1 + lb / ntx;
+  const int o = color == 1 ? (AXIS == 1 ? L.nz : L.ny) - lb / ntx : 1 + lb / ntx;
   const int i0 = 1 + TW * ti;
   const int par = (color + i0 + o) & 1;
   const int i = i0 + par + 2 * l;
@@ -1407,19 +1316,12 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega,
     const int r = r0 + u;
     d[u] = T(0);
     mk[u] = 0;
-    if (work && any && r < n) {
+    if (any && r < n) {
       const long long id = base + ls * (r + 1);
       uint8_t m8 = L.mask[id];
       const T rv = rhs[id];
-      T xv, nb[4];
-      if (FUSED && color == 1) {  // other SMs' new colour-0 values: read at L2, not from this SM's L1
-        xv = x[id];
-        nb[0] = __ldcg(&x[id - 1]); nb[1] = __ldcg(&x[id + 1]);
-        nb[2] = __ldcg(&x[id - os]); nb[3] = __ldcg(&x[id + os]);
-      } else {
-        xv = x[id];
-        nb[0] = x[id - 1]; nb[1] = x[id + 1]; nb[2] = x[id - os]; nb[3] = x[id + os];
-      }
+      const T xv = x[id];
+      const T nb[4] = {x[id - 1], x[id + 1], x[id - os], x[id + os]};
       T acc = rv;
 #pragma unroll
       for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
@@ -1468,19 +1370,17 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega,
   }
   const T xF = s_eq[buf][c][l].d;
   const T xFn = c + 1 < CH ? s_eq[buf][c + 1][l].d : T(0);
-  if (work && any) {
-    const T xL = dL - aL * xF - cL * xFn;
+  if (!any) return;
+  const T xL = dL - aL * xF - cL * xFn;
 #pragma unroll
-    for (int u = 0; u < M; ++u) {
-      const int r = r0 + u;
-      if (r >= n) break;
-      T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
-      const long long id = base + ls * (r + 1);
-      if (omega != T(1)) v = x[id] + omega * (v - x[id]);
-      x[id] = v;
-    }
+  for (int u = 0; u < M; ++u) {
+    const int r = r0 + u;
+    if (r >= n) break;
+    T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
+    const long long id = base + ls * (r + 1);
+    if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+    x[id] = v;
   }
-  if constexpr (FUSED) zz_end(zz, color, zslab, 2 * zz.nplanes * zz.ntx);
 }
 
 template <typename T, int M>
@@ -1496,74 +1396,20 @@ static cudaError_t launch_xsmem(const Launch &Lr, int color, double omega, cudaS
 template <typename T, int M, int CH>
 static cudaError_t launch_yzpcr(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
   const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
-  const ZzPlan none{};
   if (axis == 1) {
     auto kern = k_yzline_pcr<T, M, CH, 1>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega, none);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
   } else {
     auto kern = k_yzline_pcr<T, M, CH, 2>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega, none);
+    kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
   }
   note_launches(1);
   return cudaGetLastError();
 }
 
-// both colours in one launch (see ZzCtl); lev: the one problem's level
-// (device), L its host copy
-int zz_lag();
-template <typename T, int M, int CH>
-static cudaError_t launch_yzpcr_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, ZzCtl *ctl,
-                                   cudaStream_t s) {
-  const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
-  ZzPlan z;
-  z.ctl = ctl;
-  z.ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
-  z.nplanes = axis == 1 ? L.nz : L.ny;
-  z.slab = std::max(1, (192 + z.ntx - 1) / z.ntx);
-  z.nslab = (z.nplanes + z.slab - 1) / z.slab;
-  z.lag = zz_lag();
-  if (z.nslab > ZZ_MAXSLAB) return cudaErrorNotSupported;
-  const int total = 2 * z.nplanes * z.ntx;
-  if (axis == 1) {
-    auto kern = k_yzline_pcr<T, M, CH, 1, true>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<total, CH * YP_LINES, sm, s>>>(nullptr, 1, lev, 0, (T)omega, z);
-  } else {
-    auto kern = k_yzline_pcr<T, M, CH, 2, true>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    kern<<<total, CH * YP_LINES, sm, s>>>(nullptr, 1, lev, 0, (T)omega, z);
-  }
-  note_launches(1);
-  return cudaGetLastError();
-}
 
-size_t zz_ctl_bytes() { return sizeof(ZzCtl); }
-// slabs by which colour 1 trails colour 0 (FEICAR_B200_ZEBRA_LAG, default 2)
-int zz_lag() {
-  static int lag = [] {
-    const char *e = getenv("FEICAR_B200_ZEBRA_LAG");
-    const int v = e ? atoi(e) : 2;
-    return v < 1 ? 1 : v;
-  }();
-  return lag;
-}
-
-// Both colours of a y or z sweep of one problem's level in one launch when
-// its lines take k_yzline_pcr; cudaErrorNotSupported otherwise (the caller
-// then launches the colours one by one).
-template <typename T>
-cudaError_t line_sweep_zz(const DevLevel *lev, const DevLevel &L, int axis, double omega, void *ctl,
-                          cudaStream_t s) {
-  const int maxn = axis == 1 ? L.ny : L.nz;
-  if (axis == 0 || !ctl || maxn < YP_MINROWS || maxn > YZ_MAXROWS) return cudaErrorNotSupported;
-  if (maxn <= 128) return launch_yzpcr_zz<T, 8, 16>(lev, L, axis, omega, static_cast<ZzCtl *>(ctl), s);
-  return launch_yzpcr_zz<T, 8, 32>(lev, L, axis, omega, static_cast<ZzCtl *>(ctl), s);
-}
-template cudaError_t line_sweep_zz<float>(const DevLevel *, const DevLevel &, int, double, void *, cudaStream_t);
-template cudaError_t line_sweep_zz<double>(const DevLevel *, const DevLevel &, int, double, void *, cudaStream_t);
-int zz_error(const void *ctl_host) { return static_cast<const ZzCtl *>(ctl_host)->err; }
 
 template <typename T, int M, int CH>
 static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
@@ -1586,24 +1432,28 @@ static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double om
 // k_yzline_reg, longer ones the shared-memory tile kernel (blocks_tile and
 // blocks_xline count blocks the same way)
 template <typename T>
-cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int maxn,
+cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int maxn, int variant,
                        cudaStream_t s) {
   if (Lr.empty()) return cudaSuccess;
+  const int v = line_variant(axis, maxn, variant);
   if (axis == 0) {
-    if (maxn <= 16) return launch_xreg<T, 4, 4>(Lr, color, omega, s);
-    if (maxn <= 32) return launch_xreg<T, 4, 8>(Lr, color, omega, s);
-    if (maxn <= 64) return launch_xreg<T, 4, 16>(Lr, color, omega, s);
-    if (maxn <= 128) return launch_xreg<T, 4, 32>(Lr, color, omega, s);
+    if (v == LV_XREG) {
+      if (maxn <= 16) return launch_xreg<T, 4, 4>(Lr, color, omega, s);
+      if (maxn <= 32) return launch_xreg<T, 4, 8>(Lr, color, omega, s);
+      if (maxn <= 64) return launch_xreg<T, 4, 16>(Lr, color, omega, s);
+      return launch_xreg<T, 4, 32>(Lr, color, omega, s);
+    }
+    if (v == LV_XREG32) return launch_xreg<T, 4, 32>(Lr, color, omega, s);
     if (maxn <= 256) return launch_xsmem<T, 8>(Lr, color, omega, s);
     if (maxn <= 512) return launch_xsmem<T, 16>(Lr, color, omega, s);
     if (maxn <= 1024) return launch_xsmem<T, 32>(Lr, color, omega, s);
     return cudaErrorInvalidValue;  // lines longer than 1024 cells
   }
-  if (maxn >= YP_MINROWS && maxn <= YZ_MAXROWS) {
+  if (v == LV_YPCR) {
     if (maxn <= 128) return launch_yzpcr<T, 8, 16>(Lr, axis, color, omega, s);
     return launch_yzpcr<T, 8, 32>(Lr, axis, color, omega, s);
   }
-  if (maxn <= YZ_MAXROWS) {
+  if (v == LV_YREG) {
     if (maxn <= 16) return launch_yzreg<T, 4, 4>(Lr, axis, color, omega, s);
     if (maxn <= 32) return launch_yzreg<T, 4, 8>(Lr, axis, color, omega, s);
     if (maxn <= 64) return launch_yzreg<T, 4, 16>(Lr, axis, color, omega, s);
@@ -1709,7 +1559,7 @@ k_residual(const int *off, int nent, const DevLevel *levs, double *part) {
     const uint8_t mk = L.mask[id];
     T r = T(0);
     if (mk & 64) r = rhs[id] - apply_row<T>(L, id, c.i, c.j, c.k, mk, x);
-    res[id] = r;
+    if (res) res[id] = r;  // norm only where the level keeps no residual array
     r2 += (double)r * (double)r;
   }
   if (part) {
@@ -2420,7 +2270,30 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
 // the reference's face arrays, (0:ny+1, 0:nz+1) for x faces, (0:nx+1,
 // 0:nz+1) for y faces, (0:nx+1, 0:ny+1) for z faces (node counts),
 // indexed by the face cell's two transverse reference indices.
-// blockIdx.y = face; threads cover the face's cells.
+//
+// The known term of face f at the face cell idx:
+__device__ __forceinline__ double face_term(const DevLevel &L, const FaceData &fd, int f, const int (&idx)[3]) {
+  const int a = f >> 1, up = f & 1;
+  if (fd.pbc[f] == FG_PBC_DIRICHLET) {
+    const double am[3] = {L.amx[idx[0]], L.amy[idx[1]], L.amz[idx[2]]};
+    const double ap[3] = {L.apx[idx[0]], L.apy[idx[1]], L.apz[idx[2]]};
+    return -2.0 * (up ? ap[a] : am[a]) * fd.ppp[f];
+  }
+  if (fd.pgrad[f]) {
+    const int n[3] = {L.nx, L.ny, L.nz};
+    const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;  // transverse axes
+    const double w[3] = {L.wx[idx[0]], L.wy[idx[1]], L.wz[idx[2]]};
+    const long long stride = (long long)n[u] + 3;  // reference extent of the first transverse index
+    const double g = fd.pgrad[f][idx[u] + stride * idx[v]];
+    return up ? -g / w[a] : g / w[a];
+  }
+  return 0.0;
+}
+
+// blockIdx.y = face; threads cover the face's cells.  A cell on an edge or
+// corner of the box lies on two or three faces: the thread of the lowest
+// of them adds all their terms, in face order (one writer, the same sum
+// on every run).
 __global__ void k_face_rhs(double *rhs, const DevLevel L, FaceData fd) {
   const int f = blockIdx.y, a = f >> 1, up = f & 1;
   const int n[3] = {L.nx, L.ny, L.nz};
@@ -2433,18 +2306,16 @@ __global__ void k_face_rhs(double *rhs, const DevLevel L, FaceData fd) {
   idx[a] = up ? n[a] : 1;
   const long long id = idx[0] + L.sy * idx[1] + L.sz * idx[2];
   if (!(L.mask[id] & 64)) return;
-  double add = 0.0;
-  if (fd.pbc[f] == FG_PBC_DIRICHLET) {
-    const double am[3] = {L.amx[idx[0]], L.amy[idx[1]], L.amz[idx[2]]};
-    const double ap[3] = {L.apx[idx[0]], L.apy[idx[1]], L.apz[idx[2]]};
-    add = -2.0 * (up ? ap[a] : am[a]) * fd.ppp[f];
-  } else if (fd.pgrad[f]) {
-    const double w[3] = {L.wx[idx[0]], L.wy[idx[1]], L.wz[idx[2]]};
-    const long long stride = (long long)n[u] + 3;  // reference extent of the first transverse index
-    const double g = fd.pgrad[f][idx[u] + stride * idx[v]];
-    add = up ? -g / w[a] : g / w[a];
+  int on = 0;  // faces the cell lies on
+  for (int q = 0; q < 3; ++q) {
+    if (idx[q] == 1) on |= 1 << (2 * q);
+    if (idx[q] == n[q]) on |= 1 << (2 * q + 1);
   }
-  rhs[id] += add;
+  if ((on & -on) != (1 << f)) return;  // a lower face owns the cell
+  double add = 0.0;
+  for (int q = 0; q < 6; ++q)
+    if ((on >> q) & 1) add += face_term(L, fd, q, idx);
+  if (add != 0.0) rhs[id] += add;
 }
 
 cudaError_t face_rhs(double *rhs, const DevLevel &L0, const FaceData &fd, cudaStream_t s) {
@@ -2513,6 +2384,117 @@ k_ref_change(const double *p, const double *pt, const int8_t *ib, int nx, int ny
     for (int w = 0; w < 8; ++w) t = fmax(t, red[w]);
     part[blockIdx.x] = t;
   }
+}
+
+// GCM_GHOSTCELL_UPDATE.F90:865-1003 (GCM_enforce_p_compatibility), on a
+// reference-layout field: the net pressure-gradient flux out of the fluid,
+// non-ghost cells, block partials into part.  met: the reference's 1-D
+// arrays dx, dy, dz, dxcinv, dycinv, dzcinv back to back (n+2 each).
+struct RefMet {
+  const double *dx, *dy, *dz, *dxci, *dyci, *dzci;
+};
+__global__ void __launch_bounds__(256)
+k_compat_flux(const double *p, const int8_t *ib, const int8_t *gh, RefMet m, int nx, int ny, int nz,
+              double *part) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ni = nx - 1, nj = ny - 1, n = ni * nj * (nz - 1);
+  double f = 0.0;
+  if (e < n) {
+    const int i = 1 + (int)(e % ni), j = 1 + (int)((e / ni) % nj), k = 1 + (int)(e / (ni * nj));
+    const long long NX = nx + 2, NXY = NX * (ny + 2), id = i + NX * j + NXY * k;
+    const double pc = p[id];
+    const double pxw = (pc - p[id - 1]) * m.dxci[i], pxe = (p[id + 1] - pc) * m.dxci[i + 1];
+    const double pys = (pc - p[id - NX]) * m.dyci[j], pyn = (p[id + NX] - pc) * m.dyci[j + 1];
+    const double pzb = (pc - p[id - NXY]) * m.dzci[k], pzf = (p[id + NXY] - pc) * m.dzci[k + 1];
+    const double flag = (1.0 - (double)ib[id]) * (1.0 - (double)gh[id]);
+    f = flag * ((-pxw + pxe) * m.dy[j] * m.dz[k] + (-pys + pyn) * m.dx[i] * m.dz[k] +
+                (-pzb + pzf) * m.dx[i] * m.dy[j]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
+  __shared__ double red[8];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+// one block: the flux partials summed, the fluid area of the faces whose
+// velocity is zero-gradient (CORE_SET_OUTER_BC.F90:585-643: the first
+// interior layer's non-iblank cells), corr = -flux / area into *corr
+__global__ void __launch_bounds__(1024)
+k_compat_corr(const double *part, int nb, const int8_t *ib, RefMet m, int nx, int ny, int nz, int vzg,
+              double *corr) {
+  const long long NX = nx + 2, NXY = NX * (ny + 2);
+  double flux = 0.0, area = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) flux += part[b];
+  // x faces over (j,k), y faces over (i,k), z faces over (i,j): interior cells
+  for (int f = 0; f < 6; ++f) {
+    if (!((vzg >> f) & 1)) continue;
+    const int a = f >> 1, up = f & 1;
+    const int nu = a == 0 ? ny - 1 : nx - 1, nv = a == 2 ? ny - 1 : nz - 1;
+    const int layer = a == 0 ? (up ? nx - 1 : 1) : a == 1 ? (up ? ny - 1 : 1) : (up ? nz - 1 : 1);
+    for (long long e = threadIdx.x; e < (long long)nu * nv; e += blockDim.x) {
+      const int u = 1 + (int)(e % nu), v = 1 + (int)(e / nu);
+      long long id;
+      double w;
+      if (a == 0) { id = layer + NX * u + NXY * v; w = m.dy[u] * m.dz[v]; }
+      else if (a == 1) { id = u + NX * layer + NXY * v; w = m.dx[u] * m.dz[v]; }
+      else { id = u + NX * v + NXY * layer; w = m.dx[u] * m.dy[v]; }
+      area += w * (1.0 - (double)ib[id]);
+    }
+  }
+  __shared__ double rf[32], ra[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    flux += __shfl_down_sync(0xffffffffu, flux, o);
+    area += __shfl_down_sync(0xffffffffu, area, o);
+  }
+  if ((threadIdx.x & 31) == 0) { rf[threadIdx.x >> 5] = flux; ra[threadIdx.x >> 5] = area; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double F = 0.0, A = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { F += rf[w]; A += ra[w]; }
+    *corr = -F / A;
+  }
+}
+
+// pgrad -= corr on the lower faces, += corr on the upper faces whose
+// velocity is zero-gradient, over every entry (0..n) of the face arrays;
+// blockIdx.y = face
+__global__ void k_compat_apply(double *pg, int nx, int ny, int nz, int vzg, const double *corr) {
+  const int f = blockIdx.y;
+  if (!((vzg >> f) & 1)) return;
+  const long long NX = nx + 2, NY = ny + 2, NZ = nz + 2;
+  const long long ext[3] = {NY * NZ, NX * NZ, NX * NY};
+  long long off = 0;
+  for (int q = 0; q < f; ++q) off += ext[q >> 1];
+  const int a = f >> 1;
+  const long long n0 = a == 0 ? NY : NX;  // first index extent
+  const long long u1 = a == 0 ? ny : nx, v1 = a == 2 ? ny : nz;  // indices 0..u1, 0..v1
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (u1 + 1) * (v1 + 1)) return;
+  const long long u = e % (u1 + 1), v = e / (u1 + 1);
+  const double c = *corr;
+  double &g = pg[off + u + n0 * v];
+  g = (f & 1) ? g + c : g - c;
+}
+
+cudaError_t compat(const double *p, const int8_t *ib, const int8_t *gh, const double *met, int nx, int ny,
+                   int nz, int vzg, double *part, double *corr, double *pgrad, cudaStream_t s) {
+  RefMet m;
+  m.dx = met; m.dy = met + (nx + 2); m.dz = m.dy + (ny + 2);
+  m.dxci = m.dz + (nz + 2); m.dyci = m.dxci + (nx + 2); m.dzci = m.dyci + (ny + 2);
+  const int nb = ref_blocks(nx, ny, nz);
+  k_compat_flux<<<nb, 256, 0, s>>>(p, ib, gh, m, nx, ny, nz, part);
+  k_compat_corr<<<1, 1024, 0, s>>>(part, nb, ib, m, nx, ny, nz, vzg, corr);
+  const long long big = (long long)(std::max(nx, ny) + 1) * (std::max(ny, nz) + 1);
+  k_compat_apply<<<dim3((unsigned)((big + 255) / 256), 6), 256, 0, s>>>(pgrad, nx, ny, nz, vzg, corr);
+  note_launches(3);
+  return cudaGetLastError();
 }
 
 int ref_blocks(int nx, int ny, int nz) {
@@ -3340,8 +3322,8 @@ extern "C" fg_status fg_debug_check(long long *out) {
 }
 #endif
 
-template cudaError_t line_sweep<double>(const Launch &, int, int, double, int, cudaStream_t);
-template cudaError_t line_sweep<float>(const Launch &, int, int, double, int, cudaStream_t);
+template cudaError_t line_sweep<double>(const Launch &, int, int, double, int, int, cudaStream_t);
+template cudaError_t line_sweep<float>(const Launch &, int, int, double, int, int, cudaStream_t);
 template cudaError_t residual<double>(const Launch &, double *, double *, cudaStream_t);
 template cudaError_t residual_q<double>(const Launch &, cudaStream_t);
 template cudaError_t residual_q<float>(const Launch &, cudaStream_t);

@@ -28,7 +28,7 @@ LIB_PATH = os.environ.get("FEICAR_B200_LIB") or os.path.join(_HERE, "libfeicar_b
 FG_OK, FG_NOT_CONVERGED = 0, 1
 FG_PBC_DIRICHLET, FG_PBC_NEUMANN = 1, 2
 FG_PREC_FP64, FG_PREC_MIXED = 0, 1
-FG_OUTER_RICHARDSON, FG_OUTER_FGMRES = 0, 1
+FG_OUTER_RICHARDSON, FG_OUTER_FGMRES, FG_OUTER_LSOR = 0, 1, 2
 STATUS = {0: "ok", 1: "not converged", 2: "image point has no host cell", 3: "allocation failed",
           4: "timeout", 5: "bad input", 6: "dead cell without body", 7: "CUDA error",
           8: "no CUDA device", 9: "rejected by admission"}
@@ -130,6 +130,10 @@ def lib():
         L.fg_case_profile.argtypes = [vp, ip]
         L.fg_case_solve_mode.argtypes = [vp, C.POINTER(C.c_int)]
         L.fg_calc_residual.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
+        L.fg_set_pressure_gradient.argtypes = [vp, ip, vp]
+        L.fg_get_pressure_gradient.argtypes = [vp, ip, vp]
+        L.fg_enforce_p_compatibility.argtypes = [vp, vp, vp]
+        L.fg_case_set_zero_gradient_faces.argtypes = [vp, vp]
         L.fg_calc_residual2.argtypes = [vp, vp, vp, C.POINTER(C.c_double)]
         L.fg_case_history.argtypes = [vp, vp, ip, C.POINTER(C.c_int)]
         L.fg_case_profile_read.argtypes = [vp, C.POINTER(Profile)]
@@ -140,7 +144,9 @@ def lib():
                      "fg_solve_poisson_device", "fg_ghostcell_pressure", "fg_batch_create",
                      "fg_batch_add", "fg_batch_solve_device", "fg_batch_destroy", "fg_case_set_stream",
                      "fg_launch_count", "fg_case_profile", "fg_case_profile_read",
-                     "fg_case_history", "fg_case_solve_mode", "fg_calc_residual", "fg_calc_residual2"]:
+                     "fg_case_history", "fg_case_solve_mode", "fg_calc_residual", "fg_calc_residual2",
+                     "fg_set_pressure_gradient", "fg_get_pressure_gradient", "fg_enforce_p_compatibility",
+                     "fg_case_set_zero_gradient_faces"]:
             getattr(L, name).restype = ip
         _lib = L
     return _lib
@@ -353,6 +359,30 @@ class Case:
                                        C.byref(v)), "fg_calc_residual2")
         return v.value
 
+    def pgrad_shape(self, face):
+        NX, NY, NZ = self.grid.nx + 2, self.grid.ny + 2, self.grid.nz + 2
+        return [(NY, NZ), (NY, NZ), (NX, NZ), (NX, NZ), (NX, NY), (NX, NY)][face]
+
+    def set_pressure_gradient(self, face, values):
+        a = np.asfortranarray(values, dtype=np.float64)
+        assert a.shape == self.pgrad_shape(face)
+        _check(lib().fg_set_pressure_gradient(self.h, face, _p(a)), "fg_set_pressure_gradient")
+
+    def get_pressure_gradient(self, face):
+        out = np.zeros(self.pgrad_shape(face), order="F")
+        _check(lib().fg_get_pressure_gradient(self.h, face, _p(out)), "fg_get_pressure_gradient")
+        return out
+
+    def enforce_p_compatibility(self, p, vel_zero_gradient):
+        v = np.ascontiguousarray(vel_zero_gradient, dtype=np.int32)
+        _check(lib().fg_enforce_p_compatibility(self.h, _p(np.asfortranarray(p)), _p(v)),
+               "fg_enforce_p_compatibility")
+
+    def set_zero_gradient_faces(self, vel_zero_gradient=None):
+        v = None if vel_zero_gradient is None else np.ascontiguousarray(vel_zero_gradient, dtype=np.int32)
+        self._vzg = v
+        _check(lib().fg_case_set_zero_gradient_faces(self.h, _p(v)), "fg_case_set_zero_gradient_faces")
+
     def ghostcell_pressure(self, p, p_old=None, iterations=1):
         _check(lib().fg_ghostcell_pressure(self.h, _p(p), _p(p_old), iterations), "fg_ghostcell_pressure")
 
@@ -539,3 +569,100 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- autotuner
+LINE_FAMILIES = {0: {1: "x_registers", 2: "x_registers_32_lanes", 3: "x_shared_memory"},
+                 1: {1: "yz_registers_thomas", 2: "yz_block_pcr", 3: "yz_warp_per_line"}}
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("nlevels", C.c_int),
+        ("line_variant", (C.c_int * 3) * 12),
+        ("line_us", (C.c_double * 3) * 12),
+        ("nu1", C.c_int), ("nu2", C.c_int),
+        ("solve_ms", C.c_double * 4),
+        ("tuned", C.c_int),
+    ]
+
+    def as_dict(self):
+        levels = []
+        for L in range(self.nlevels):
+            row = {}
+            for a, name in enumerate("xyz"):
+                v = self.line_variant[L][a]
+                if v:
+                    row[name] = {"family": LINE_FAMILIES[0 if a == 0 else 1][v],
+                                 "us": round(self.line_us[L][a], 2)}
+            levels.append(row)
+        return {"levels": levels, "nu1": self.nu1, "nu2": self.nu2,
+                "solve_ms_nu11_21_22_33": [round(x, 3) for x in self.solve_ms], "tuned": bool(self.tuned)}
+
+
+def _tune_lib():
+    L = lib()
+    if not getattr(L, "_tune_ready", False):
+        vp = C.c_void_p
+        L.fg_batch_autotune.argtypes = [vp, vp, vp, C.POINTER(Tuning)]
+        L.fg_batch_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.fg_case_autotune.argtypes = [vp, vp, vp, C.POINTER(Tuning)]
+        for n in ("fg_batch_autotune", "fg_batch_get_tuning", "fg_case_autotune"):
+            getattr(L, n).restype = C.c_int
+        L._tune_ready = True
+    return L
+
+
+def batch_autotune(batch, d_ps, d_divs) -> dict:
+    n = len(batch.cases)
+    P = (C.c_void_p * n)(*[C.c_void_p(x) for x in d_ps])
+    D = (C.c_void_p * n)(*[C.c_void_p(x) for x in d_divs])
+    t = Tuning()
+    _check(_tune_lib().fg_batch_autotune(batch.h, P, D, C.byref(t)), "fg_batch_autotune")
+    return t.as_dict()
+
+
+def case_autotune(case, d_p: int, d_div: int) -> dict:
+    t = Tuning()
+    _check(_tune_lib().fg_case_autotune(case.h, C.c_void_p(d_p), C.c_void_p(d_div), C.byref(t)),
+           "fg_case_autotune")
+    return t.as_dict()
+
+
+# ------------------------------------------------------------ projection steps
+def _proj_lib():
+    L = lib()
+    if not getattr(L, "_proj_ready", False):
+        vp = C.c_void_p
+        L.fg_face_vel_device.argtypes = [vp] + [vp] * 9
+        L.fg_rhs_poisson_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.fg_correct_vel_device.argtypes = [vp, vp, C.c_double, vp, vp, vp, vp, vp, vp]
+        for n in ("fg_face_vel_device", "fg_rhs_poisson_device", "fg_correct_vel_device"):
+            getattr(L, n).restype = C.c_int
+        L._proj_ready = True
+    return L
+
+
+def _dp(x):
+    return None if x is None else C.c_void_p(x)
+
+
+def face_vel_device(case, u, v, w, bcxu, bcyv, bczw, fu, fv, fw):
+    """Device pointers (ints) of reference-layout fields and boundary arrays."""
+    _check(_proj_lib().fg_face_vel_device(case.h, *[_dp(x) for x in (u, v, w, bcxu, bcyv, bczw, fu, fv, fw)]),
+           "fg_face_vel_device")
+
+
+def rhs_poisson_device(case, fu, fv, fw, bcxu, bcyv, bczw, vel_zero_gradient, dt, div):
+    vz = None if vel_zero_gradient is None else np.ascontiguousarray(vel_zero_gradient, dtype=np.int32)
+    sd, rd = C.c_double(0.0), C.c_double(0.0)
+    _check(_proj_lib().fg_rhs_poisson_device(case.h, _dp(fu), _dp(fv), _dp(fw), _dp(bcxu), _dp(bcyv), _dp(bczw),
+                                             _p(vz), dt, _dp(div), C.byref(sd), C.byref(rd)),
+           "fg_rhs_poisson_device")
+    return sd.value, rd.value
+
+
+def correct_vel_device(case, pp, dt, u=None, v=None, w=None, dpdx=None, dpdy=None, dpdz=None):
+    _check(_proj_lib().fg_correct_vel_device(case.h, _dp(pp), dt, *[_dp(x) for x in (u, v, w, dpdx, dpdy, dpdz)]),
+           "fg_correct_vel_device")

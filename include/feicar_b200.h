@@ -41,7 +41,10 @@ typedef enum fg_status {
 enum { FG_PBC_DIRICHLET = 1, FG_PBC_NEUMANN = 2 };
 enum { FG_SOLID = 1, FG_MEMBRANE = 2 };
 enum { FG_PREC_FP64 = 0, FG_PREC_MIXED = 1 };
-enum { FG_OUTER_RICHARDSON = 0, FG_OUTER_FGMRES = 1 };
+/* outer iteration: V-cycles on p, FGMRES preconditioned by a V-cycle, or
+ * the reference's single-grid line SOR (solver type 1, CORE_POISSON.F90
+ * :205-456; FP64 on the finest level, max_cycles counts sweeps) */
+enum { FG_OUTER_RICHARDSON = 0, FG_OUTER_FGMRES = 1, FG_OUTER_LSOR = 2 };
 
 /* Solver settings: the input.dat keys of MAIN.F90:214-254 that the pressure
  * path reads, plus the knobs of the multigrid run on the GPU. */
@@ -153,6 +156,26 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div,
 fg_status fg_solve_poisson_device(fg_case *c, double *d_p,
                                   const double *d_div, const double *d_p_old,
                                   fg_solve_stats *st);
+/* Outer-face pressure gradients, the reference's module arrays pgradx1,
+ * pgradx2, pgrady1, pgrady2, pgradz1, pgradz2 (face 0..5) read by
+ * set_outer_pressure_bc (CORE_SET_OUTER_BC.F90:831-1042): x faces
+ * (0:ny+1, 0:nz+1), y faces (0:nx+1, 0:nz+1), z faces (0:nx+1, 0:ny+1),
+ * node counts, column-major.  Kept on the device (zero until set); a
+ * Neumann face's gradient enters the finest-level right-hand side. */
+fg_status fg_set_pressure_gradient(fg_case *c, int face, const double *values);
+fg_status fg_get_pressure_gradient(fg_case *c, int face, double *values);
+/* Replaces GCM_enforce_p_compatibility (GCM_GHOSTCELL_UPDATE.F90:865-1003)
+ * on the device: with no Dirichlet face and some face whose velocity is
+ * ZERO_GRADIENT (vel_zero_gradient[6] != 0), the net pressure-gradient
+ * flux of p out of the fluid non-ghost cells, divided by the fluid area of
+ * those faces, shifts their gradients (lower faces -, upper faces +).
+ * p: host field. */
+fg_status fg_enforce_p_compatibility(fg_case *c, const double *p, const int *vel_zero_gradient);
+/* The faces whose velocity is ZERO_GRADIENT: every later solve on c first
+ * applies the compatibility step to its initial pressure (the reference
+ * applies it at the top of each outer iteration, CORE_POISSON.F90:160).
+ * NULL clears. */
+fg_status fg_case_set_zero_gradient_faces(fg_case *c, const int *vel_zero_gradient);
 /* Replaces calc_residual (CORE_POISSON.F90:460-551) on the device:
  * *maxres = sqrt(sum r^2 / (nx ny nz)), r = div - A p over the fluid,
  * non-ghost interior cells, p read with its own outer ghost layers; the
@@ -165,6 +188,33 @@ fg_status fg_calc_residual2(fg_case *c, const double *p, const double *p_temp, d
  * with itermax_gc iterations). */
 fg_status fg_ghostcell_pressure(fg_case *c, double *p, const double *p_old,
                                 int iterations);
+
+/* ----- the projection steps either side of the solve, on device fields
+ * (reference layout, on the case's device; each call waits for its
+ * kernels).  Face-velocity boundary arrays as the reference keeps them:
+ * bcxu(0:1, 0:ny+1, 0:nz+1), bcyv(0:nx+1, 0:1, 0:nz+1),
+ * bczw(0:nx+1, 0:ny+1, 0:1). ----- */
+/* Replaces face_vel (CORE_FRAC_STEP_ROUTINES.F90:1-130): face velocities
+ * interpolated from the cell velocities with the factors of
+ * CORE_GRID.F90:194-202, the outer faces from the boundary arrays. */
+fg_status fg_face_vel_device(fg_case *c, const double *u, const double *v, const double *w, const double *bcxu,
+                             const double *bcyv, const double *bczw, double *face_u, double *face_v,
+                             double *face_w);
+/* Replaces rhs_poisson (CORE_POISSON.F90:9-79) with the
+ * enforce_global_mass_consv it calls first (CORE_SET_OUTER_BC.F90:515-735,
+ * mix_GC_form = 0): with zero-gradient faces (vel_zero_gradient[6], may be
+ * NULL) the net mass flux is spread over their fluid area (boundary arrays
+ * and boundary face velocities corrected); then div = (du/dx + dv/dy +
+ * dw/dz)/dt on the fluid non-ghost cells, 0 elsewhere.  *sumd: the mass
+ * flux; *resdiv: max |div| dt (either may be NULL). */
+fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, double *face_w, double *bcxu,
+                                double *bcyv, double *bczw, const int *vel_zero_gradient, double dt, double *div,
+                                double *sumd, double *resdiv);
+/* Replaces correct_vel (CORE_FRAC_STEP_ROUTINES.F90:132-190: u -= dt grad
+ * p' on the non-iblank cells) and calc_pres_grad (:270-320: the gradient
+ * itself); either triple may be NULL. */
+fg_status fg_correct_vel_device(fg_case *c, const double *pPrime, double dt, double *u, double *v, double *w,
+                                double *dpdx, double *dpdy, double *dpdz);
 
 /* ----- stream, launch count and timing (no reference counterpart: the
  * reference prints wall time per solve_poisson call only,
@@ -255,6 +305,36 @@ fg_status fg_batch_add(fg_batch *b, fg_case *c);
 fg_status fg_batch_solve_device(fg_batch *b, double **d_p,
                                 const double **d_div, fg_solve_stats *st);
 fg_status fg_batch_destroy(fg_batch *b);
+
+/* ----- autotuner (no reference counterpart: the reference's smoother and
+ * sweep counts are fixed in CORE_MG.F90) -----
+ * Measures, on the batch's own levels, every line-kernel family that can
+ * take each level set's lines along each axis (x: lines in registers with
+ * lanes by line length, in registers with 32 lanes, or staged in shared
+ * memory; y/z: tiles in registers with a Thomas over the chunks, tiles with
+ * a block-wide cyclic reduction over the chunks, or one warp per line) and
+ * keeps the fastest; then times whole solves of the batch's problems with
+ * (nu1, nu2) = (1,1), (2,1), (2,2), (3,3) and keeps the fastest one that
+ * converges.  The choices hold for later solves of the batch (and across
+ * new geometries of the same grids).  d_p / d_div as for
+ * fg_batch_solve_device; the tuning solves start from zero and leave the
+ * last solution in d_p. */
+#define FG_TUNE_MAXLEVELS 12
+enum { FG_LV_XREG = 1, FG_LV_XREG32 = 2, FG_LV_XSMEM = 3 };   /* x sweeps   */
+enum { FG_LV_YREG = 1, FG_LV_YPCR = 2, FG_LV_YWARP = 3 };     /* y/z sweeps */
+typedef struct fg_tuning {
+  int nlevels;
+  int line_variant[FG_TUNE_MAXLEVELS][3];  /* family that runs, per level and axis (0: no line launches) */
+  double line_us[FG_TUNE_MAXLEVELS][3];    /* its measured time per sweep (both colours), us */
+  int nu1, nu2;                            /* smoothing steps in use */
+  double solve_ms[4];                      /* solve time of each (nu1,nu2) candidate, -1 = not converged */
+  int tuned;                               /* 1 once fg_*_autotune ran */
+} fg_tuning;
+fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_tuning *out);
+fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out);
+/* The same for a single case's solves (d_p, d_div: device fields in the
+ * reference layout, as for fg_solve_poisson_device). */
+fg_status fg_case_autotune(fg_case *c, double *d_p, const double *d_div, fg_tuning *out);
 
 /* ----- serving: a stream of solve requests over many cases (no reference
  * counterpart: the reference runs one case per process and calls

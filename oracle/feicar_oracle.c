@@ -1916,6 +1916,223 @@ static void enforce_p_compatibility(or_case *c, const double *pres, const or_par
     }
 }
 
+/* exported for the tests: one GCM_enforce_p_compatibility step on p, and
+ * access to the outer-face pressure gradients it updates (face 0..5 =
+ * x1, x2, y1, y2, z1, z2; x faces (0:ny+1, 0:nz+1), y faces (0:nx+1,
+ * 0:nz+1), z faces (0:nx+1, 0:ny+1)) */
+int or_enforce_p_compatibility(or_case *c, const double *p, const or_params *prm) {
+  enforce_p_compatibility(c, p, prm);
+  return OR_OK;
+}
+static double *pgrad_face(or_case *c, int face, long *n) {
+  double *a[6] = {c->pgradx1, c->pgradx2, c->pgrady1, c->pgrady2, c->pgradz1, c->pgradz2};
+  const long ext[3] = {(long)c->NY * c->NZ, (long)c->NX * c->NZ, (long)c->NX * c->NY};
+  if (face < 0 || face > 5) return NULL;
+  *n = ext[face / 2];
+  return a[face];
+}
+int or_get_pgrad(or_case *c, int face, double *out) {
+  long n = 0;
+  double *a = pgrad_face(c, face, &n);
+  if (!a) return OR_BAD_INPUT;
+  memcpy(out, a, sizeof(double) * (size_t)n);
+  return OR_OK;
+}
+int or_set_pgrad(or_case *c, int face, const double *in) {
+  long n = 0;
+  double *a = pgrad_face(c, face, &n);
+  if (!a) return OR_BAD_INPUT;
+  memcpy(a, in, sizeof(double) * (size_t)n);
+  return OR_OK;
+}
+
+/* ------------------------------------------------------------------
+ * The steps either side of the pressure solve (fractional-step
+ * projection), restated for nProcs = 1.  Face-velocity boundary arrays as
+ * the reference keeps them: bcxu(0:1, 0:ny+1, 0:nz+1), bcyv(0:nx+1, 0:1,
+ * 0:nz+1), bczw(0:nx+1, 0:ny+1, 0:1), column-major.  vzg: the faces whose
+ * velocity is ZERO_GRADIENT (x1 x2 y1 y2 z1 z2).
+ * ------------------------------------------------------------------ */
+#define BCXU(s, j, k) bcxu[(long)(s) + 2 * ((long)(j) + c->NY * (long)(k))]
+#define BCYV(i, s, k) bcyv[(long)(i) + c->NX * ((long)(s) + 2 * (long)(k))]
+#define BCZW(i, j, s) bczw[(long)(i) + c->NX * ((long)(j) + c->NY * (long)(s))]
+/* CORE_GRID.F90:194-202: face interpolation factor of node i */
+static double fint(const double *x, const double *xc, int i) { return (x[i] - xc[i - 1]) / (xc[i] - xc[i - 1]); }
+
+/* CORE_FRAC_STEP_ROUTINES.F90:1-130 face_vel */
+int or_face_vel(or_case *c, const double *u, const double *v, const double *w, const double *bcxu,
+                const double *bcyv, const double *bczw, double *fu, double *fv, double *fw) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 2; i <= nx - 1; ++i) {
+        const double f = fint(c->x, c->xc, i);
+        fu[IDX(c, i, j, k)] = f * u[IDX(c, i, j, k)] + (1.0 - f) * u[IDX(c, i - 1, j, k)];
+      }
+  for (int j = 2; j <= ny - 1; ++j)
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int i = 1; i <= nx - 1; ++i) {
+        const double f = fint(c->y, c->yc, j);
+        fv[IDX(c, i, j, k)] = f * v[IDX(c, i, j, k)] + (1.0 - f) * v[IDX(c, i, j - 1, k)];
+      }
+  for (int k = 2; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        const double f = fint(c->z, c->zc, k);
+        fw[IDX(c, i, j, k)] = f * w[IDX(c, i, j, k)] + (1.0 - f) * w[IDX(c, i, j, k - 1)];
+      }
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j) {
+      fu[IDX(c, 1, j, k)] = BCXU(0, j, k);
+      fu[IDX(c, nx, j, k)] = BCXU(1, j, k);
+    }
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int i = 1; i <= nx - 1; ++i) {
+      fv[IDX(c, i, 1, k)] = BCYV(i, 0, k);
+      fv[IDX(c, i, ny, k)] = BCYV(i, 1, k);
+    }
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      fw[IDX(c, i, j, 1)] = BCZW(i, j, 0);
+      fw[IDX(c, i, j, nz)] = BCZW(i, j, 1);
+    }
+  return OR_OK;
+}
+
+/* CORE_SET_OUTER_BC.F90:515-735 enforce_global_mass_consv (mix_GC_form =
+ * 0) then CORE_POISSON.F90:9-79 rhs_poisson: div = (du/dx + dv/dy +
+ * dw/dz) / dt on fluid non-ghost cells; *sumd = the mass flux (dt removed),
+ * *resdiv = max |div| dt */
+int or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv, double *bczw,
+                   const int *vzg, double dt, double *div, double *sumd, double *resdiv) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  int any = 0;
+  for (int f = 0; f < 6; ++f) any |= vzg[f];
+  if (any) {
+    double massflux = 0.0;
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int j = 1; j <= ny - 1; ++j)
+        for (int i = 1; i <= nx - 1; ++i) {
+          const long id = IDX(c, i, j, k);
+          const double flag = (1.0 - (double)c->iblank[id]) * (1.0 - (double)c->ghost[id]);
+          massflux = massflux + flag * ((-fu[id] + fu[IDX(c, i + 1, j, k)]) * c->dy[j] * c->dz[k] +
+                                        (-fv[id] + fv[IDX(c, i, j + 1, k)]) * c->dx[i] * c->dz[k] +
+                                        (-fw[id] + fw[IDX(c, i, j, k + 1)]) * c->dx[i] * c->dy[j]);
+        }
+    double aL = 0, aR = 0, aB = 0, aT = 0, aK = 0, aF = 0, area = 0.0;
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int j = 1; j <= ny - 1; ++j) {
+        aL = aL + c->dy[j] * c->dz[k] * (1.0 - c->iblank[IDX(c, 1, j, k)]);
+        aR = aR + c->dy[j] * c->dz[k] * (1.0 - c->iblank[IDX(c, nx - 1, j, k)]);
+      }
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int i = 1; i <= nx - 1; ++i) {
+        aB = aB + c->dx[i] * c->dz[k] * (1.0 - c->iblank[IDX(c, i, 1, k)]);
+        aT = aT + c->dx[i] * c->dz[k] * (1.0 - c->iblank[IDX(c, i, ny - 1, k)]);
+      }
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        aK = aK + c->dx[i] * c->dy[j] * (1.0 - c->iblank[IDX(c, i, j, 1)]);
+        aF = aF + c->dx[i] * c->dy[j] * (1.0 - c->iblank[IDX(c, i, j, nz - 1)]);
+      }
+    if (vzg[0]) area += aL;
+    if (vzg[1]) area += aR;
+    if (vzg[2]) area += aB;
+    if (vzg[3]) area += aT;
+    if (vzg[4]) area += aK;
+    if (vzg[5]) area += aF;
+    const double cv = -massflux / area;
+    for (int k = 0; k <= nz; ++k)
+      for (int j = 0; j <= ny; ++j) {
+        if (vzg[0]) BCXU(0, j, k) = BCXU(0, j, k) - cv;
+        if (vzg[1]) BCXU(1, j, k) = BCXU(1, j, k) + cv;
+      }
+    for (int k = 0; k <= nz; ++k)
+      for (int i = 0; i <= nx; ++i) {
+        if (vzg[2]) BCYV(i, 0, k) = BCYV(i, 0, k) - cv;
+        if (vzg[3]) BCYV(i, 1, k) = BCYV(i, 1, k) + cv;
+      }
+    for (int j = 0; j <= ny; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        if (vzg[4]) BCZW(i, j, 0) = BCZW(i, j, 0) - cv;
+        if (vzg[5]) BCZW(i, j, 1) = BCZW(i, j, 1) + cv;
+      }
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int j = 1; j <= ny - 1; ++j) {
+        if (vzg[0]) fu[IDX(c, 1, j, k)] = fu[IDX(c, 1, j, k)] - cv;
+        if (vzg[1]) fu[IDX(c, nx, j, k)] = fu[IDX(c, nx, j, k)] + cv;
+      }
+    for (int k = 1; k <= nz - 1; ++k)
+      for (int i = 1; i <= nx - 1; ++i) {
+        if (vzg[2]) fv[IDX(c, i, 1, k)] = fv[IDX(c, i, 1, k)] - cv;
+        if (vzg[3]) fv[IDX(c, i, ny, k)] = fv[IDX(c, i, ny, k)] + cv;
+      }
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        if (vzg[4]) fw[IDX(c, i, j, 1)] = fw[IDX(c, i, j, 1)] - cv;
+        if (vzg[5]) fw[IDX(c, i, j, nz)] = fw[IDX(c, i, j, nz)] + cv;
+      }
+  }
+  const double dtinv = 1.0 / dt;
+  double sd = 0.0, rd = 0.0;
+  memset(div, 0, sizeof(double) * (size_t)c->ntot);
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        const long id = IDX(c, i, j, k);
+        const double flag = (1.0 - (double)c->iblank[id]) * (1.0 - (double)c->ghost[id]);
+        double d = dtinv * ((fu[IDX(c, i + 1, j, k)] - fu[id]) * c->dxinv[i] +
+                            (fv[IDX(c, i, j + 1, k)] - fv[id]) * c->dyinv[j] +
+                            (fw[IDX(c, i, j, k + 1)] - fw[id]) * c->dzinv[k]);
+        d = d * flag;
+        div[id] = d;
+        sd = sd + d * c->dx[i] * c->dy[j] * c->dz[k];
+        const double a = fabs(d / dtinv);
+        if (a > rd) rd = a;
+      }
+  *sumd = sd / dtinv;
+  *resdiv = rd;
+  return OR_OK;
+}
+
+/* CORE_FRAC_STEP_ROUTINES.F90:132-190 correct_vel (u -= dt grad p' on
+ * non-iblank cells) and :270-320 calc_pres_grad (grad p' on non-iblank
+ * cells); either output set may be NULL */
+int or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v, double *w, double *dpdx,
+                   double *dpdy, double *dpdz) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        const long id = IDX(c, i, j, k);
+        const double fx1 = fint(c->x, c->xc, i + 1), fx0 = fint(c->x, c->xc, i);
+        const double fy1 = fint(c->y, c->yc, j + 1), fy0 = fint(c->y, c->yc, j);
+        const double fz1 = fint(c->z, c->zc, k + 1), fz0 = fint(c->z, c->zc, k);
+        const double pe = fx1 * pp[IDX(c, i + 1, j, k)] + (1.0 - fx1) * pp[id];
+        const double pw = fx0 * pp[id] + (1.0 - fx0) * pp[IDX(c, i - 1, j, k)];
+        const double pn = fy1 * pp[IDX(c, i, j + 1, k)] + (1.0 - fy1) * pp[id];
+        const double ps = fy0 * pp[id] + (1.0 - fy0) * pp[IDX(c, i, j - 1, k)];
+        const double pf = fz1 * pp[IDX(c, i, j, k + 1)] + (1.0 - fz1) * pp[id];
+        const double pb = fz0 * pp[id] + (1.0 - fz0) * pp[IDX(c, i, j, k - 1)];
+        const double pgx = (pe - pw) * c->dxinv[i], pgy = (pn - ps) * c->dyinv[j], pgz = (pf - pb) * c->dzinv[k];
+        const double flag = 1.0 - (double)c->iblank[id];
+        if (u) {
+          u[id] = u[id] - dt * pgx * flag;
+          v[id] = v[id] - dt * pgy * flag;
+          w[id] = w[id] - dt * pgz * flag;
+        }
+        if (dpdx) {
+          dpdx[id] = pgx * flag;
+          dpdy[id] = pgy * flag;
+          dpdz[id] = pgz * flag;
+        }
+      }
+  return OR_OK;
+}
+#undef BCXU
+#undef BCYV
+#undef BCZW
+
 /* CORE_POISSON.F90:205-456 itsolv (LSOR: x lexicographic, y zebra, z) on
  * the fine grid with the iblank/ghost flag */
 static void itsolv_lsor(or_case *c, double *var, const double *r, const or_params *prm) {

@@ -104,6 +104,21 @@ int  or_mg_prepare(or_case *c);
 int  or_get_field_i8(const or_case *c, int which, int8_t *out);
 /* counts: nGhost, nDead, nWarnSide, nHostFail, nStencilSolid, nFallbackDead */
 int  or_get_counts(const or_case *c, int *out);
+/* GCM_GHOSTCELL_UPDATE.F90:865-1003 on p (updates the face gradients) and
+ * the face gradient arrays it reads and writes (face 0..5: x1..z2) */
+int  or_enforce_p_compatibility(or_case *c, const double *p, const or_params *prm);
+int  or_get_pgrad(or_case *c, int face, double *out);
+int  or_set_pgrad(or_case *c, int face, const double *in);
+/* the fractional-step projection either side of the solve:
+ * CORE_FRAC_STEP_ROUTINES.F90 face_vel, correct_vel / calc_pres_grad,
+ * CORE_SET_OUTER_BC.F90 enforce_global_mass_consv + CORE_POISSON.F90
+ * rhs_poisson */
+int  or_face_vel(or_case *c, const double *u, const double *v, const double *w, const double *bcxu,
+                 const double *bcyv, const double *bczw, double *fu, double *fv, double *fw);
+int  or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv,
+                    double *bczw, const int *vzg, double dt, double *div, double *sumd, double *resdiv);
+int  or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v, double *w,
+                    double *dpdx, double *dpdy, double *dpdz);
 int  or_get_ghosts(const or_case *c, int32_t *ijk, int32_t *cell,
                    double *coeffN, double *coeffD, double *bi, double *ip,
                    double *probeLength, int32_t *closestElem, double *alpha);

@@ -95,6 +95,13 @@ def lib():
         L.or_tdma.argtypes = [C.c_void_p] * 5 + [C.c_int, C.c_int]
         L.or_invert8.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
         L.or_set_threads.argtypes = [C.c_int]
+        L.or_enforce_p_compatibility.argtypes = [P, C.c_void_p, C.POINTER(Params)]
+        L.or_get_pgrad.argtypes = [P, C.c_int, C.c_void_p]
+        L.or_set_pgrad.argtypes = [P, C.c_int, C.c_void_p]
+        L.or_face_vel.argtypes = [P] + [C.c_void_p] * 9
+        L.or_rhs_poisson.argtypes = [P] + [C.c_void_p] * 7 + [C.c_double, C.c_void_p, C.POINTER(C.c_double),
+                                                             C.POINTER(C.c_double)]
+        L.or_correct_vel.argtypes = [P, C.c_void_p, C.c_double] + [C.c_void_p] * 6
         _lib = L
     return _lib
 
@@ -230,6 +237,47 @@ class OracleCase:
         rc = lib().or_ghostcell_pressure(self.h, _ptr(p), _ptr(div), _ptr(p_old), None, None,
                                          C.byref(prm), C.byref(it))
         return rc, it.value
+
+    def pgrad_shape(self, face):
+        NX, NY, NZ = self.grid.nx + 2, self.grid.ny + 2, self.grid.nz + 2
+        return [(NY, NZ), (NY, NZ), (NX, NZ), (NX, NZ), (NX, NY), (NX, NY)][face]
+
+    def get_pgrad(self, face):
+        out = np.zeros(self.pgrad_shape(face), order="F")
+        lib().or_get_pgrad(self.h, face, _ptr(out))
+        return out
+
+    def set_pgrad(self, face, values):
+        a = np.asfortranarray(values, dtype=np.float64)
+        assert a.shape == self.pgrad_shape(face)
+        lib().or_set_pgrad(self.h, face, _ptr(a))
+
+    def enforce_p_compatibility(self, p, params=None):
+        """GCM_GHOSTCELL_UPDATE.F90:865-1003 on p: updates the face gradients."""
+        prm = params or default_params()
+        lib().or_enforce_p_compatibility(self.h, _ptr(np.asfortranarray(p)), C.byref(prm))
+
+    # the projection steps either side of the solve (Fortran-ordered arrays)
+    def face_vel(self, u, v, w, bcxu, bcyv, bczw):
+        out = [np.zeros(self.shape, order="F") for _ in range(3)]
+        lib().or_face_vel(self.h, *[_ptr(np.asfortranarray(a)) for a in (u, v, w, bcxu, bcyv, bczw)],
+                          *[_ptr(a) for a in out])
+        return out
+
+    def rhs_poisson(self, fu, fv, fw, bcxu, bcyv, bczw, vzg, dt):
+        """Arrays are updated in place (mass conservation); returns (div, sumd, resdiv)."""
+        div = np.zeros(self.shape, order="F")
+        sd, rd = C.c_double(0.0), C.c_double(0.0)
+        vz = np.ascontiguousarray(vzg, dtype=np.int32)
+        lib().or_rhs_poisson(self.h, *[_ptr(a) for a in (fu, fv, fw, bcxu, bcyv, bczw, vz)], dt, _ptr(div),
+                             C.byref(sd), C.byref(rd))
+        return div, sd.value, rd.value
+
+    def correct_vel(self, pp, dt, u, v, w):
+        """u, v, w updated in place; returns (dpdx, dpdy, dpdz)."""
+        g = [np.zeros(self.shape, order="F") for _ in range(3)]
+        lib().or_correct_vel(self.h, _ptr(np.asfortranarray(pp)), dt, _ptr(u), _ptr(v), _ptr(w), *[_ptr(a) for a in g])
+        return g
 
     def relres(self, p, div):
         return lib().or_relres(self.h, _ptr(p), _ptr(div))

@@ -123,3 +123,59 @@ def test_reference_residual_measures_match_oracle():
     ref2 = float(np.abs(p - pt)[m].max())  # CORE_POISSON.F90:679-724 restated
     assert c.calc_residual2(p, pt) == ref2
     c.close()
+
+
+def test_enforce_p_compatibility_matches_oracle():
+    """GCM_enforce_p_compatibility: the flux of a pressure field out of the
+    fluid cells, spread over the zero-gradient outflow faces, shifts their
+    gradient arrays; device against oracle, applied twice in a row (the
+    shifts accumulate), for one and for two outflow faces."""
+    grid, bodies = GEOM
+    for vzg in ([0, 1, 0, 0, 0, 0], [0, 1, 0, 0, 0, 1]):
+        oc = _tagged(grid, bodies)
+        c = _device_case(grid, bodies)
+        rng = np.random.default_rng(5)
+        for rep in range(2):
+            p = np.asfortranarray(synth.box_smooth(rng.standard_normal(grid.shape)))
+            oc.enforce_p_compatibility(p, O.default_params(vzg=vzg))
+            c.enforce_p_compatibility(p, vzg)
+        for f in range(6):
+            want, got = oc.get_pgrad(f), c.get_pressure_gradient(f)
+            scale = max(1e-300, float(np.abs(want).max()))
+            assert np.abs(got - want).max() <= 1e-12 * scale, (vzg, f)
+            assert (np.abs(want).max() > 0) == bool(vzg[f])
+        c.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_neumann_face_gradient_data_matches_oracle(prec):
+    """Inhomogeneous Neumann data on the x = 0 face (a seeded smooth
+    gradient field) with a Dirichlet x = L face: the converged pressure
+    against the oracle's solve with the same face arrays."""
+    grid, bodies = GEOM
+    oc = _tagged(grid, bodies)
+    ib, gh = oc.field(0), oc.field(1)
+    rng = np.random.default_rng(17)
+    fluid = np.zeros(grid.shape, bool)
+    fluid[1:grid.nx, 1:grid.ny, 1:grid.nz] = (ib[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0) & \
+                                            (gh[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0)
+    div = np.asfortranarray(synth.box_smooth(rng.standard_normal(grid.shape)) * fluid)
+    g0 = np.asfortranarray(0.3 * synth.box_smooth(rng.standard_normal(oc.pgrad_shape(0))))
+    oc.set_pgrad(0, g0)
+    pbc = [fg.FG_PBC_NEUMANN] * 6
+    pbc[1] = fg.FG_PBC_DIRICHLET
+    ppp = [0.0, 0.1, 0.0, 0.0, 0.0, 0.0]
+    po = np.zeros(grid.shape, order="F")
+    rc, ost = oc.solve_poisson(po, div, params=O.default_params(
+        restol_pson=1e-14, restol_gcp=1e-14, itermax_pson=3000, pbc=pbc, ppp=ppp))
+    assert ost["relres"] <= 1e-10, ost
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    c = _device_case(grid, bodies, precision=p_, rtol=1e-12, max_cycles=200, pbc=pbc, ppp=ppp)
+    c.set_pressure_gradient(0, g0)
+    p = np.zeros(grid.shape, order="F")
+    c.solve_poisson(p, div)
+    m = np.zeros(grid.shape, bool)
+    m[1:grid.nx, 1:grid.ny, 1:grid.nz] = ib[1:grid.nx, 1:grid.ny, 1:grid.nz] == 0
+    err = np.linalg.norm(p[m] - po[m]) / np.linalg.norm(po[m])
+    assert err <= 1e-9, err
+    c.close()

@@ -309,26 +309,61 @@ def test_batch64_problems_each_reach_their_solution(prec):
         c.close()
 
 
-@pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_two_colour_sweep_matches_one_launch_per_colour(prec, monkeypatch):
-    """y and z lines of 65..256 cells of a single problem take both zebra
-    colours in one launch (work items by ticket, colour-1 items waiting for
-    their neighbour planes' colour 0); the arithmetic is that of one launch
-    per colour, so both give identical fields."""
-    grid = synth.Grid(synth.uniform_nodes(48, 0, 3), synth.tanh_nodes(96, 0, 2, 2.0),
-                      synth.tanh_nodes(80, 0, 2, 2.0))
-    bodies = [synth.sphere_body((1.0, 1.0, 1.0), 0.8, 4)]
-    _, ib, rhs, phi = _problem(grid, bodies)
+def test_line_sor_solver_reaches_the_same_solution():
+    """The reference's single-grid solver type 1 (line SOR on the fine
+    grid, CORE_POISSON.F90:205-456): on the device it converges to the
+    same discrete solution as the multigrid path and as the oracle's own
+    line-SOR solve."""
+    grid, bodies = GRIDS["sphere_small"]
+    oc, ib, rhs, phi = _problem(grid, bodies)
+    m = _fluid(grid, ib)
+    c = _case(grid, bodies, outer=fg.FG_OUTER_LSOR, omega=1.6, rtol=1e-11, max_cycles=40000)
+    p = np.zeros(grid.shape, order="F")
+    st = c.solve_poisson(p, rhs)
+    assert st["relres"] <= 1e-11
+    assert _relerr(p, phi, m) <= 1e-8
+    po = np.zeros(grid.shape, order="F")
+    oc.solve_poisson(po, rhs.copy(order="F"), params=O.default_params(
+        lsor=True, omega_pson=1.6, restol_pson=1e-13, restol_gcp=1e-13, itermax_pson=40000))
+    assert _relerr(p, po, m) <= 1e-8
+    c.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_autotuned_batch_reaches_each_solution(prec):
+    """The autotuner measures the line-kernel families of every level set
+    and the (nu1, nu2) candidates on the batch itself and keeps the
+    fastest; the tuned batch still solves each problem to its own exact
+    discrete solution."""
+    allp = synth.batch_problems(n=64, seed0=0, lo=32, hi=192)
     p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
-    out = []
-    for two in ("0", "1"):
-        monkeypatch.setenv("FEICAR_B200_ZEBRA_TWO_LAUNCH", two)
-        c = _case(grid, bodies, precision=p_, rtol=1e-11, max_cycles=60)
-        p = np.zeros(grid.shape, order="F")
-        st = c.solve_poisson(p, rhs)
-        out.append((st, p, c.history()))
+    cfg = fg.default_config(precision=p_, rtol=1e-12, max_cycles=120)
+    cases, refs, d_ps, d_fs = [], [], [], []
+    for i in (4, 9, 0):
+        g, b, seed = allp[i]
+        _, ib, rhs, phi = _problem(g, [b], seed=seed)
+        c = fg.Case(g, cfg)
+        c.add_body(b)
+        c.set_iblank_body_fast()
+        c.gcm_set_internal_boundary()
+        c.mg_prepare()
+        cases.append(c)
+        refs.append((phi, _fluid(g, ib)))
+        d_ps.append(torch.zeros(g.shape[::-1], dtype=torch.float64, device="cuda"))
+        d_fs.append(torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda())
+    bt = fg.Batch(cfg)
+    for c in cases:
+        bt.add(c)
+    tun = fg.batch_autotune(bt, [t.data_ptr() for t in d_ps], [t.data_ptr() for t in d_fs])
+    assert tun["tuned"] and (tun["nu1"], tun["nu2"]) in [(1, 1), (2, 1), (2, 2), (3, 3)]
+    assert tun["levels"][0]["x"]["us"] > 0
+    for t in d_ps:
+        t.zero_()
+    st = bt.solve_device([t.data_ptr() for t in d_ps], [t.data_ptr() for t in d_fs])
+    torch.cuda.synchronize()
+    assert st["relres"] <= 1e-12
+    for (phi, m), t in zip(refs, d_ps):
+        assert _relerr(t.cpu().numpy().transpose(2, 1, 0), phi, m) <= TOL
+    bt.close()
+    for c in cases:
         c.close()
-    assert out[0][0]["cycles"] == out[1][0]["cycles"]
-    assert np.array_equal(out[0][2], out[1][2])
-    assert np.array_equal(out[0][1], out[1][1])
-    assert _relerr(out[0][1], phi, _fluid(grid, ib)) <= 1e-8
