@@ -24,6 +24,7 @@ namespace fg {
 void geom_free(Geom &g) {
   for (auto &b : g.bodies) {
     fg::dev_free(b.d_xyz); fg::dev_free(b.d_en); fg::dev_free(b.d_vn); fg::dev_free(b.d_tri);
+    fg::dev_free(b.d_uvw); fg::dev_free(b.d_uvw_old); fg::dev_free(b.d_snap); fg::dev_free(b.d_dpdn);
     fg::dev_free(b.d_v2t_off); fg::dev_free(b.d_v2t);
   }
   g.bodies.clear();
@@ -980,6 +981,7 @@ fg_status fg_case_update_body(fg_case *c, int ibody, const double *xyz) {
   cudaSetDevice(c->device);
   DevBody &B = c->geom->bodies[ibody];
   B.xyz.assign(xyz, xyz + 3 * (size_t)B.nvert);
+  B.host_stale = false;
   return upload_body(B);
 }
 
@@ -1300,6 +1302,236 @@ fg_status fg_get_dead_rows(const fg_case *c, int32_t *ijk, int32_t *cell, double
   if (ip && c->d_ipv.size() >= 3 * n) memcpy(ip, c->d_ipv.data(), 3 * n * sizeof(double));
   if (probe && c->d_probe.size() >= n) memcpy(probe, c->d_probe.data(), n * sizeof(double));
   if (closest && G.d_closest.size() >= n) memcpy(closest, G.d_closest.data(), n * sizeof(int32_t));
+  return FG_OK;
+}
+
+}  // extern "C"
+
+
+// ===================================================== prescribed body motion
+// BOUNDARY_MOVE.F90:3-186 (move_boundary for PRESCRIBED_RIGID bodies) with
+// BOUNDARY_MARKER_VEL.F90:5-125 (forced_motion, compute_marker_vel) and
+// BOUNDARY_MOVE.F90:151-186 (compute_marker_poisition), on the device.  The
+// body's scalars of the step (centroid velocity, angular velocity, the
+// length-preserving rotation coefficients) are formed on the host in the
+// reference's order; every marker's velocity, position, displacement since
+// the last re-tag and dp/dn, and the surface normals
+// (BOUNDARY_SET_ARCLENGTH_NORM.F90:2-189), are computed here without fused
+// multiply-adds, so the markers are the same doubles as a sequential run.
+namespace fg {
+namespace mv {
+
+struct Step {
+  double vc[3];     // vxcent, vycent, vzcent
+  double ta[3];     // the half-sum of the old and new angular velocities
+  double cent[3];   // xcent, ycent, zcent before the step
+  double co[3][3];  // coefficient of temp_(u,v,w)B in (u,v,w)B, times total_omega applied after
+  double tot;       // total_omega
+  double dt;
+  int with_dpdn;    // ntime > 1
+};
+
+// marker velocities (the old ones kept), positions, displacement from the
+// re-tag snapshot (max into *dsmax as the bits of a non-negative double)
+__global__ void k_markers(int nv, double *x, double *uvw, double *uvw_old, const double *snap, Step st,
+                          unsigned long long *dsmax) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  double *y = x + nv, *z = y + nv;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  const double tu = (st.ta[1] * (zi - st.cent[2]) - st.ta[2] * (yi - st.cent[1]));
+  const double tv = -(st.ta[0] * (zi - st.cent[2]) - st.ta[2] * (xi - st.cent[0]));
+  const double tw = (st.ta[0] * (yi - st.cent[1]) - st.ta[1] * (xi - st.cent[0]));
+  double b[3];
+  for (int r = 0; r < 3; ++r)
+    b[r] = st.vc[r] + st.tot * (tu * st.co[r][0] + tv * st.co[r][1] + tw * st.co[r][2]);
+  for (int r = 0; r < 3; ++r) {
+    uvw_old[r * nv + i] = uvw[r * nv + i];
+    uvw[r * nv + i] = b[r];
+  }
+  const double nx = xi + st.dt * b[0], ny = yi + st.dt * b[1], nz = zi + st.dt * b[2];
+  x[i] = nx; y[i] = ny; z[i] = nz;
+  const double dx = nx - snap[i], dy = ny - snap[nv + i], dz = nz - snap[2 * nv + i];
+  const double ds = sqrt(dx * dx + dy * dy + dz * dz);
+  atomicMax(dsmax, (unsigned long long)__double_as_longlong(ds));
+}
+
+// element unit normals (v2-v1) x (v3-v2) / |.| (host_normals' arithmetic)
+__global__ void k_elem_normals(int nt, int nv, const double *x, const int32_t *tri, double *en) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nt) return;
+  const double *y = x + nv, *z = y + nv;
+  const int n1 = tri[3 * m], n2 = tri[3 * m + 1], n3 = tri[3 * m + 2];
+  const double ax = x[n2] - x[n1], ay = y[n2] - y[n1], az = z[n2] - z[n1];
+  const double bx = x[n3] - x[n2], by = y[n3] - y[n2], bz = z[n3] - z[n2];
+  const double nxv = (ay * bz - az * by);
+  const double nyv = (az * bx - ax * bz);
+  const double nzv = (ax * by - ay * bx);
+  const double mag = sqrt(nxv * nxv + nyv * nyv + nzv * nzv);
+  en[m] = nxv / mag; en[nt + m] = nyv / mag; en[2 * nt + m] = nzv / mag;
+}
+
+// vertex unit normals: the incident element normals summed in ascending
+// element order (once per occurrence of the vertex in the element, as the
+// sequential loop does), normalised; then dp/dn at the marker
+// (BOUNDARY_MOVE.F90:96-110: -D u_n / Dt, 0 on the first step)
+__global__ void k_vert_normals(int nt, int nv, const int32_t *tri, const int32_t *off, const int32_t *v2t,
+                               const double *en, double *vn, const double *uvw, const double *uvw_old, double dt,
+                               int with_dpdn, double *dpdn) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  double sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int q = off[v]; q < off[v + 1]; ++q) {
+    const int m = v2t[q];
+    const int mult = (tri[3 * m] == v) + (tri[3 * m + 1] == v) + (tri[3 * m + 2] == v);
+    for (int r = 0; r < mult; ++r) { sx = sx + en[m]; sy = sy + en[nt + m]; sz = sz + en[2 * nt + m]; }
+  }
+  const double mag = sqrt(sx * sx + sy * sy + sz * sz);
+  const double nx = sx / mag, ny = sy / mag, nz = sz / mag;
+  vn[v] = nx; vn[nv + v] = ny; vn[2 * nv + v] = nz;
+  if (dpdn) {
+    double d = 0.0;
+    if (with_dpdn)
+      d = -((uvw[v] - uvw_old[v]) / dt * nx + (uvw[nv + v] - uvw_old[nv + v]) / dt * ny +
+            (uvw[2 * nv + v] - uvw_old[2 * nv + v]) / dt * nz);
+    dpdn[v] = d;
+  }
+}
+
+}  // namespace mv
+}  // namespace fg
+
+namespace {
+
+fg_status ensure_motion(DevBody &B, cudaStream_t s) {
+  if (B.d_uvw) return FG_OK;
+  const size_t n3 = 3 * (size_t)B.nvert * sizeof(double);
+  FG_CUDA(fg::dev_alloc(&B.d_uvw, n3));
+  FG_CUDA(fg::dev_alloc(&B.d_uvw_old, n3));
+  FG_CUDA(fg::dev_alloc(&B.d_snap, n3));
+  FG_CUDA(fg::dev_alloc(&B.d_dpdn, (size_t)B.nvert * sizeof(double)));
+  FG_CUDA(cudaMemsetAsync(B.d_uvw, 0, n3, s));
+  FG_CUDA(cudaMemsetAsync(B.d_uvw_old, 0, n3, s));
+  FG_CUDA(cudaMemcpyAsync(B.d_snap, B.d_xyz, n3, cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaMemsetAsync(B.d_dpdn, 0, (size_t)B.nvert * sizeof(double), s));
+  return FG_OK;
+}
+
+// the host copy of the vertices from the device (after device moves)
+fg_status sync_host_body(DevBody &B, cudaStream_t s) {
+  if (!B.host_stale) return FG_OK;
+  std::vector<double> soa(3 * (size_t)B.nvert);
+  FG_CUDA(cudaMemcpyAsync(soa.data(), B.d_xyz, soa.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FG_CUDA(cudaStreamSynchronize(s));
+  for (int v = 0; v < B.nvert; ++v) {
+    B.xyz[3 * v] = soa[v]; B.xyz[3 * v + 1] = soa[B.nvert + v]; B.xyz[3 * v + 2] = soa[2 * B.nvert + v];
+  }
+  B.host_stale = false;
+  return FG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fg_status fg_move_body(fg_case *c, int ibody, fg_rigid_motion *m, int ntime, double time, double dt,
+                       double *ds_max, int *iblank_reset) {
+  if (!c || !m || ibody < 0 || ibody >= (int)c->geom->bodies.size() || !(dt > 0.0)) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  DevBody &B = c->geom->bodies[ibody];
+  fg_status st = ensure_motion(B, s);
+  if (st != FG_OK) return st;
+  // forced_motion (BOUNDARY_MARKER_VEL.F90:5-33)
+  const double PI = 3.14159265358979323846;
+  double vc[3], av[3];
+  for (int a = 0; a < 3; ++a) {
+    vc[a] = m->vcent_trans[a] + m->amp[a] * sin(2.0 * PI * m->freq[a] * time);
+    av[a] = m->angv_init[a] + m->ampang[a] * sin(2.0 * PI * m->freqang[a] * time + m->angphase[a]);
+  }
+  // compute_marker_vel's scalars (BOUNDARY_MARKER_VEL.F90:60-125)
+  mv::Step S{};
+  for (int a = 0; a < 3; ++a) {
+    S.vc[a] = vc[a];
+    S.ta[a] = 0.5 * (m->angv_old[a] + av[a]);
+    S.cent[a] = m->cent[a];
+  }
+  const double ax = av[0], ay = av[1], az = av[2];
+  S.tot = 1.0 / (1.0 + 0.25 * (dt * dt) * (ax * ax + ay * ay + az * az));
+  const double q = 0.25 * (dt * dt), h = 0.5 * dt;
+  S.co[0][0] = 1.0 + q * (ax * ax);  S.co[0][1] = -h * az - q * ax * ay;  S.co[0][2] = -h * ay + q * ax * az;
+  S.co[1][0] = h * az - q * ax * ay; S.co[1][1] = 1.0 + q * (ay * ay);   S.co[1][2] = -h * ax - q * ay * az;
+  S.co[2][0] = h * ay + q * ax * az; S.co[2][1] = h * ax - q * ay * az;  S.co[2][2] = 1.0 + q * (az * az);
+  S.dt = dt;
+  S.with_dpdn = ntime > 1 ? 1 : 0;
+  unsigned long long *d_ds = nullptr;
+  FG_CUDA(fg::dev_alloc(&d_ds, sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(d_ds, 0, sizeof(unsigned long long), s);
+  const int nv = B.nvert, nt = B.ntri;
+  if (e == cudaSuccess) {
+    mv::k_markers<<<(nv + 255) / 256, 256, 0, s>>>(nv, B.d_xyz, B.d_uvw, B.d_uvw_old, B.d_snap, S, d_ds);
+    mv::k_elem_normals<<<(nt + 255) / 256, 256, 0, s>>>(nt, nv, B.d_xyz, B.d_tri, B.d_en);
+    mv::k_vert_normals<<<(nv + 255) / 256, 256, 0, s>>>(nt, nv, B.d_tri, B.d_v2t_off, B.d_v2t, B.d_en, B.d_vn,
+                                                        B.d_uvw, B.d_uvw_old, dt, S.with_dpdn, B.d_dpdn);
+    note_launches(3);
+    e = cudaGetLastError();
+  }
+  unsigned long long bits = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, d_ds, sizeof(bits), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  fg::dev_free(d_ds);
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    return FG_CUDA_ERROR;
+  }
+  B.host_stale = true;
+  // compute_marker_poisition's centroid, and the state the next step reads
+  for (int a = 0; a < 3; ++a) {
+    m->cent[a] = m->cent[a] + dt * vc[a];
+    m->angv_old[a] = av[a];
+  }
+  // the re-tag policy (BOUNDARY_MOVE.F90:122-145): a marker moved more than
+  // 0.05 of the smallest cell width since the last snapshot
+  double ds;
+  memcpy(&ds, &bits, sizeof(ds));
+  double hmin = 1e300;
+  const HLevel &L = c->lev[0];
+  for (const std::vector<double> *xv : {&L.x, &L.y, &L.z})
+    for (size_t i = 1; i + 2 < xv->size(); ++i) hmin = std::min(hmin, (*xv)[i + 1] - (*xv)[i]);
+  const int reset = ds > 0.05 * hmin ? 1 : 0;
+  if (reset) FG_CUDA(cudaMemcpyAsync(B.d_snap, B.d_xyz, 3 * (size_t)nv * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (ds_max) *ds_max = ds;
+  if (iblank_reset) *iblank_reset = reset;
+  return FG_OK;
+}
+
+fg_status fg_get_body_markers(fg_case *c, int ibody, double *xyz, double *uvw, double *dpdn) {
+  if (!c || ibody < 0 || ibody >= (int)c->geom->bodies.size()) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  DevBody &B = c->geom->bodies[ibody];
+  const int nv = B.nvert;
+  if (xyz) {
+    fg_status st = sync_host_body(B, c->stream);
+    if (st != FG_OK) return st;
+    memcpy(xyz, B.xyz.data(), 3 * (size_t)nv * sizeof(double));
+  }
+  if ((uvw || dpdn) && !B.d_uvw) {
+    if (uvw) memset(uvw, 0, 3 * (size_t)nv * sizeof(double));
+    if (dpdn) memset(dpdn, 0, (size_t)nv * sizeof(double));
+    return FG_OK;
+  }
+  std::vector<double> soa(3 * (size_t)nv);
+  if (uvw) {
+    FG_CUDA(cudaMemcpyAsync(soa.data(), B.d_uvw, soa.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < nv; ++v) {
+      uvw[3 * v] = soa[v]; uvw[3 * v + 1] = soa[nv + v]; uvw[3 * v + 2] = soa[2 * nv + v];
+    }
+  }
+  if (dpdn) {
+    FG_CUDA(cudaMemcpyAsync(dpdn, B.d_dpdn, (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    FG_CUDA(cudaStreamSynchronize(c->stream));
+  }
   return FG_OK;
 }
 

@@ -18,6 +18,12 @@ struct DevBody {
   double *d_vn = nullptr;      // vertex normals (3*nvert, SoA)
   int32_t *d_tri = nullptr;    // 3*ntri
   int32_t *d_v2t_off = nullptr, *d_v2t = nullptr;  // vertex -> triangles
+  // prescribed motion on the device (fg_move_body): marker velocities of
+  // this and the previous step, positions at the last re-tag, dp/dn at
+  // the markers (all SoA, nvert each); the host copy xyz is brought up to
+  // date only when asked for
+  double *d_uvw = nullptr, *d_uvw_old = nullptr, *d_snap = nullptr, *d_dpdn = nullptr;
+  bool host_stale = false;
 };
 
 // Device buffer that only grows: kept across calls, so re-tagging a moving

@@ -576,6 +576,36 @@ LINE_FAMILIES = {0: {1: "x_registers", 2: "x_registers_32_lanes", 3: "x_shared_m
                  1: {1: "yz_registers_thomas", 2: "yz_block_pcr", 3: "yz_warp_per_line"}}
 
 
+class RigidMotion(C.Structure):
+    """fg_rigid_motion: PRESCRIBED_RIGID parameters and state."""
+    _fields_ = [(n, C.c_double * 3) for n in ("vcent_trans", "amp", "freq", "angv_init", "ampang", "freqang",
+                                              "angphase", "cent", "angv_old")]
+
+
+def move_body(case, ibody, motion, ntime, time, dt):
+    """One prescribed-motion step on the device; returns (ds_max, iblank_reset)."""
+    L = lib()
+    if not getattr(L, "_move_ready", False):
+        L.fg_move_body.argtypes = [C.c_void_p, C.c_int, C.POINTER(RigidMotion), C.c_int, C.c_double, C.c_double,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.fg_get_body_markers.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.fg_move_body.restype = C.c_int
+        L.fg_get_body_markers.restype = C.c_int
+        L._move_ready = True
+    ds, rs = C.c_double(0.0), C.c_int(0)
+    _check(L.fg_move_body(case.h, ibody, C.byref(motion), ntime, time, dt, C.byref(ds), C.byref(rs)), "fg_move_body")
+    return ds.value, rs.value
+
+
+def body_markers(case, ibody, nvert):
+    L = lib()
+    xyz, uvw, dpdn = np.zeros((nvert, 3)), np.zeros((nvert, 3)), np.zeros(nvert)
+    L.fg_get_body_markers.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fg_get_body_markers.restype = C.c_int
+    _check(L.fg_get_body_markers(case.h, ibody, _p(xyz), _p(uvw), _p(dpdn)), "fg_get_body_markers")
+    return xyz, uvw, dpdn
+
+
 class Tuning(C.Structure):
     _fields_ = [
         ("nlevels", C.c_int),

@@ -102,6 +102,33 @@ fg_status fg_case_add_body(fg_case *c, int nvert, int ntri, const double *xyz,
 /* Moves body `ibody` (BOUNDARY_MOVE.F90:151-186 output). */
 fg_status fg_case_update_body(fg_case *c, int ibody, const double *xyz);
 
+/* Prescribed rigid motion of a body (boundary_motion_type
+ * PRESCRIBED_RIGID): the input.dat parameters forced_motion reads
+ * (BOUNDARY_MARKER_VEL.F90:5-33) and the state the next step needs
+ * (centroid, the previous step's angular velocity), updated by each move. */
+typedef struct fg_rigid_motion {
+  double vcent_trans[3];  /* vxcentTrans, vycentTrans, vzcentTrans   */
+  double amp[3], freq[3]; /* ampx.., freqx.. (translation)           */
+  double angv_init[3];    /* angvxinit..                             */
+  double ampang[3], freqang[3], angphase[3];
+  double cent[3];         /* xcent, ycent, zcent                     */
+  double angv_old[3];     /* angvx_old..                             */
+} fg_rigid_motion;
+/* Replaces move_boundary for a PRESCRIBED_RIGID body (BOUNDARY_MOVE.F90
+ * :3-186 with forced_motion / compute_marker_vel, BOUNDARY_MARKER_VEL.F90
+ * :5-125, and compute_marker_poisition, BOUNDARY_MOVE.F90:151-186) on the
+ * device: the marker velocities of time `time`, the markers moved by dt,
+ * the surface normals (calculate_arclength_norm_ds) and the marker dp/dn
+ * (-Du_n/Dt, 0 when ntime <= 1) recomputed on the device, where the next
+ * tagging reads them.  *ds_max: the largest marker displacement since the
+ * last re-tag snapshot; *iblank_reset = 1 when it exceeds 0.05 of the
+ * smallest cell width (the snapshot then moves to the new positions). */
+fg_status fg_move_body(fg_case *c, int ibody, fg_rigid_motion *m, int ntime, double time, double dt,
+                       double *ds_max, int *iblank_reset);
+/* The markers of body ibody: positions xyz[3n], velocities uvw[3n] and
+ * dp/dn[n] (any may be NULL). */
+fg_status fg_get_body_markers(fg_case *c, int ibody, double *xyz, double *uvw, double *dpdn);
+
 /* Replaces set_iblank_body_fast (BOUNDARY_IBLANK_FAST.F90:2-854) on the
  * device.  iblank (host, int8, the field above) may be NULL. */
 fg_status fg_set_iblank_body_fast(fg_case *c, int8_t *iblank);

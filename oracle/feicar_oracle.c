@@ -52,6 +52,9 @@ typedef struct or_body {
   /* vertex -> incident triangles in ascending triangle order: the same
    * sequence the full scan of BOUNDARY_IBLANK_FAST.F90:992-999 produces */
   int32_t *v2t_off, *v2t;
+  /* prescribed motion: marker velocities (this and the previous step),
+   * positions at the last re-tag, marker dp/dn (made on the first move) */
+  double *mu, *mv, *mw, *muo, *mvo, *mwo, *sx, *sy, *sz, *dpdn;
 } or_body;
 
 typedef struct or_level {
@@ -281,6 +284,8 @@ void or_case_destroy(or_case *c) {
     free(B->enx); free(B->eny); free(B->enz); free(B->ecx); free(B->ecy); free(B->ecz);
     free(B->earea); free(B->vnx); free(B->vny); free(B->vnz);
     free(B->v2t_off); free(B->v2t);
+    free(B->mu); free(B->mv); free(B->mw); free(B->muo); free(B->mvo); free(B->mwo);
+    free(B->sx); free(B->sy); free(B->sz); free(B->dpdn);
   }
   free_ghosts(c); free_deads(c);
   free(c);
@@ -396,6 +401,86 @@ int or_case_update_body(or_case *c, int ibody, const double *xyz) {
     B->xv[v] = xyz[3 * v]; B->yv[v] = xyz[3 * v + 1]; B->zv[v] = xyz[3 * v + 2];
   }
   body_normals(B);
+  return OR_OK;
+}
+
+/* ------------------------------------------------ prescribed rigid motion
+ * BOUNDARY_MOVE.F90:3-186 (move_boundary, PRESCRIBED_RIGID) with
+ * BOUNDARY_MARKER_VEL.F90:5-33 forced_motion, :60-125 compute_marker_vel
+ * and BOUNDARY_MOVE.F90:151-186 compute_marker_poisition; the normals of
+ * calculate_arclength_norm_ds; dp/dn at the markers (:96-110); the re-tag
+ * test (:122-145). */
+int or_move_body(or_case *c, int ibody, or_rigid_motion *m, int ntime, double time, double dt,
+                 double *ds_max, int *iblank_reset) {
+  if (ibody < 0 || ibody >= c->nbody || !(dt > 0.0)) return OR_BAD_INPUT;
+  or_body *B = &c->body[ibody];
+  const int nv = B->nvert;
+  if (!B->mu) {
+    B->mu = dzalloc(nv); B->mv = dzalloc(nv); B->mw = dzalloc(nv);
+    B->muo = dzalloc(nv); B->mvo = dzalloc(nv); B->mwo = dzalloc(nv);
+    B->sx = dzalloc(nv); B->sy = dzalloc(nv); B->sz = dzalloc(nv); B->dpdn = dzalloc(nv);
+    for (int v = 0; v < nv; ++v) { B->sx[v] = B->xv[v]; B->sy[v] = B->yv[v]; B->sz[v] = B->zv[v]; }
+  }
+  const double PI = 3.14159265358979323846;
+  double vc[3], av[3], ta[3];
+  for (int a = 0; a < 3; ++a) {
+    vc[a] = m->vcent_trans[a] + m->amp[a] * sin(2.0 * PI * m->freq[a] * time);
+    av[a] = m->angv_init[a] + m->ampang[a] * sin(2.0 * PI * m->freqang[a] * time + m->angphase[a]);
+  }
+  for (int a = 0; a < 3; ++a) ta[a] = 0.5 * (m->angv_old[a] + av[a]);
+  const double ax = av[0], ay = av[1], az = av[2];
+  const double tot = 1.0 / (1.0 + 0.25 * (dt * dt) * (ax * ax + ay * ay + az * az));
+  const double q = 0.25 * (dt * dt), h = 0.5 * dt;
+  double ds = 0.0;
+  for (int i = 0; i < nv; ++i) {
+    const double tu = (ta[1] * (B->zv[i] - m->cent[2]) - ta[2] * (B->yv[i] - m->cent[1]));
+    const double tv = -(ta[0] * (B->zv[i] - m->cent[2]) - ta[2] * (B->xv[i] - m->cent[0]));
+    const double tw = (ta[0] * (B->yv[i] - m->cent[1]) - ta[1] * (B->xv[i] - m->cent[0]));
+    const double uB = vc[0] + tot * (tu * (1.0 + q * (ax * ax)) + tv * (-h * az - q * ax * ay) + tw * (-h * ay + q * ax * az));
+    const double vB = vc[1] + tot * (tu * (h * az - q * ax * ay) + tv * (1.0 + q * (ay * ay)) + tw * (-h * ax - q * ay * az));
+    const double wB = vc[2] + tot * (tu * (h * ay + q * ax * az) + tv * (h * ax - q * ay * az) + tw * (1.0 + q * (az * az)));
+    B->muo[i] = B->mu[i]; B->mvo[i] = B->mv[i]; B->mwo[i] = B->mw[i];
+    B->mu[i] = uB; B->mv[i] = vB; B->mw[i] = wB;
+    B->xv[i] = B->xv[i] + dt * uB;
+    B->yv[i] = B->yv[i] + dt * vB;
+    B->zv[i] = B->zv[i] + dt * wB;
+    const double dx = B->xv[i] - B->sx[i], dy = B->yv[i] - B->sy[i], dz = B->zv[i] - B->sz[i];
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (d > ds) ds = d;
+  }
+  for (int a = 0; a < 3; ++a) {
+    m->cent[a] = m->cent[a] + dt * vc[a];
+    m->angv_old[a] = av[a];
+  }
+  body_normals(B);
+  for (int i = 0; i < nv; ++i)
+    B->dpdn[i] = ntime > 1 ? -((B->mu[i] - B->muo[i]) / dt * B->vnx[i] + (B->mv[i] - B->mvo[i]) / dt * B->vny[i] +
+                               (B->mw[i] - B->mwo[i]) / dt * B->vnz[i])
+                           : 0.0;
+  double hmin = 1e300;
+  for (int i = 1; i <= c->nx - 1; ++i) if (c->dx[i] < hmin) hmin = c->dx[i];
+  for (int j = 1; j <= c->ny - 1; ++j) if (c->dy[j] < hmin) hmin = c->dy[j];
+  for (int k = 1; k <= c->nz - 1; ++k) if (c->dz[k] < hmin) hmin = c->dz[k];
+  const int reset = ds > 0.05 * hmin;
+  if (reset)
+    for (int v = 0; v < nv; ++v) { B->sx[v] = B->xv[v]; B->sy[v] = B->yv[v]; B->sz[v] = B->zv[v]; }
+  if (ds_max) *ds_max = ds;
+  if (iblank_reset) *iblank_reset = reset;
+  return OR_OK;
+}
+
+int or_get_body_markers(or_case *c, int ibody, double *xyz, double *uvw, double *dpdn) {
+  if (ibody < 0 || ibody >= c->nbody) return OR_BAD_INPUT;
+  or_body *B = &c->body[ibody];
+  for (int v = 0; v < B->nvert; ++v) {
+    if (xyz) { xyz[3 * v] = B->xv[v]; xyz[3 * v + 1] = B->yv[v]; xyz[3 * v + 2] = B->zv[v]; }
+    if (uvw) {
+      uvw[3 * v] = B->mu ? B->mu[v] : 0.0;
+      uvw[3 * v + 1] = B->mv ? B->mv[v] : 0.0;
+      uvw[3 * v + 2] = B->mw ? B->mw[v] : 0.0;
+    }
+    if (dpdn) dpdn[v] = B->dpdn ? B->dpdn[v] : 0.0;
+  }
   return OR_OK;
 }
 

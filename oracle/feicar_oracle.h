@@ -107,6 +107,16 @@ int  or_get_counts(const or_case *c, int *out);
 /* GCM_GHOSTCELL_UPDATE.F90:865-1003 on p (updates the face gradients) and
  * the face gradient arrays it reads and writes (face 0..5: x1..z2) */
 int  or_enforce_p_compatibility(or_case *c, const double *p, const or_params *prm);
+/* prescribed rigid motion of a body (BOUNDARY_MOVE.F90 move_boundary,
+ * BOUNDARY_MARKER_VEL.F90 forced_motion / compute_marker_vel) */
+typedef struct or_rigid_motion {
+  double vcent_trans[3], amp[3], freq[3];
+  double angv_init[3], ampang[3], freqang[3], angphase[3];
+  double cent[3], angv_old[3];
+} or_rigid_motion;
+int  or_move_body(or_case *c, int ibody, or_rigid_motion *m, int ntime, double time, double dt,
+                  double *ds_max, int *iblank_reset);
+int  or_get_body_markers(or_case *c, int ibody, double *xyz, double *uvw, double *dpdn);
 int  or_get_pgrad(or_case *c, int face, double *out);
 int  or_set_pgrad(or_case *c, int face, const double *in);
 /* the fractional-step projection either side of the solve:

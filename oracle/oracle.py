@@ -39,6 +39,12 @@ class Params(C.Structure):
     ]
 
 
+class RigidMotion(C.Structure):
+    """PRESCRIBED_RIGID parameters and state (or_rigid_motion / fg_rigid_motion)."""
+    _fields_ = [(n, C.c_double * 3) for n in ("vcent_trans", "amp", "freq", "angv_init", "ampang", "freqang",
+                                              "angphase", "cent", "angv_old")]
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("outer_iterations", C.c_int),
@@ -99,6 +105,9 @@ def lib():
         L.or_get_pgrad.argtypes = [P, C.c_int, C.c_void_p]
         L.or_set_pgrad.argtypes = [P, C.c_int, C.c_void_p]
         L.or_face_vel.argtypes = [P] + [C.c_void_p] * 9
+        L.or_move_body.argtypes = [P, C.c_int, C.POINTER(RigidMotion), C.c_int, C.c_double, C.c_double,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.or_get_body_markers.argtypes = [P, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.or_rhs_poisson.argtypes = [P] + [C.c_void_p] * 7 + [C.c_double, C.c_void_p, C.POINTER(C.c_double),
                                                              C.POINTER(C.c_double)]
         L.or_correct_vel.argtypes = [P, C.c_void_p, C.c_double] + [C.c_void_p] * 6
@@ -278,6 +287,18 @@ class OracleCase:
         g = [np.zeros(self.shape, order="F") for _ in range(3)]
         lib().or_correct_vel(self.h, _ptr(np.asfortranarray(pp)), dt, _ptr(u), _ptr(v), _ptr(w), *[_ptr(a) for a in g])
         return g
+
+    def move_body(self, ibody, motion, ntime, time, dt):
+        """One prescribed-motion step; motion (RigidMotion) is updated.
+        Returns (ds_max, iblank_reset)."""
+        ds, rs = C.c_double(0.0), C.c_int(0)
+        lib().or_move_body(self.h, ibody, C.byref(motion), ntime, time, dt, C.byref(ds), C.byref(rs))
+        return ds.value, rs.value
+
+    def body_markers(self, ibody, nvert):
+        xyz, uvw, dpdn = np.zeros((nvert, 3)), np.zeros((nvert, 3)), np.zeros(nvert)
+        lib().or_get_body_markers(self.h, ibody, _ptr(xyz), _ptr(uvw), _ptr(dpdn))
+        return xyz, uvw, dpdn
 
     def relres(self, p, div):
         return lib().or_relres(self.h, _ptr(p), _ptr(div))
