@@ -2027,6 +2027,7 @@ const char *fg_status_string(fg_status s) {
     }
     case FG_NO_DEVICE: return "no CUDA device";
     case FG_REJECTED: return "rejected by admission";
+    case FG_IO_ERROR: return "file could not be read or written";
   }
   return "unknown";
 }

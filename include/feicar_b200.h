@@ -35,7 +35,10 @@ typedef enum fg_status {
   FG_GEOMETRY_DEAD_NO_BODY = 6,  /* GCM_SET_BOUNDARY.F90:1061-1066       */
   FG_CUDA_ERROR = 7,
   FG_NO_DEVICE = 8,
-  FG_REJECTED = 9                /* serving admission refused            */
+  FG_REJECTED = 9,               /* serving admission refused            */
+  FG_IO_ERROR = 10               /* a file could not be opened, read or
+                                    written, or its layout is not the one
+                                    expected                             */
 } fg_status;
 
 enum { FG_PBC_DIRICHLET = 1, FG_PBC_NEUMANN = 2 };
@@ -424,6 +427,76 @@ fg_status fg_server_info(const fg_server *s, fg_server_stats *out);
 double fg_server_clock(const fg_server *s);
 /* Finishes every submitted request, then stops the engine. */
 fg_status fg_server_destroy(fg_server *s);
+
+/* ----- formats around the path (host code; no device is touched) ----- */
+
+/* Gmsh MSH 2.2 ASCII body surface, the unstructured surface input of the
+ * marker initialisation (BOUNDARY_MARKER_INIT.F90:247-296).  The reference
+ * skips a fixed number of lines and reads every element line as
+ * `elm type ntags tag tag n1 n2 n3`; here the sections are found by name,
+ * the tags are counted, elements other than 3-node triangles (type 2) are
+ * skipped and counted in *nskipped, and node tags are mapped to 0-based
+ * vertex indices (the reference's marker index is the tag itself; files
+ * whose tags run 1..n in order give the same triangles).  Call with
+ * xyz = tri = NULL for the counts, then with xyz[3*cap_vert] and
+ * tri[3*cap_tri].  FG_IO_ERROR: no file, not ASCII 2.x, a short section;
+ * FG_BAD_INPUT: buffers too small, a triangle naming a node not listed. */
+fg_status fg_read_msh22(const char *path, int *nvert, int *ntri, double *xyz, int cap_vert, int *tri,
+                        int cap_tri, int *nskipped);
+
+/* The restart file of write_restart / read_restart (MAIN.F90:1049-1122,
+ * 983-1040) for one rank (nProcs = 1): an unformatted sequential file of
+ * records with 4-byte length markers (time, ntime), (every flow array), then
+ * one record per body.  A record longer than the maximum subrecord length
+ * is split: every subrecord but the last carries a negative leading marker,
+ * every one but the first a negative trailing marker (the layout of
+ * gfortran and of Intel Fortran's variable-length records).  NULL arrays
+ * are written as zeros and skipped on reading.  Arrays are the reference's
+ * Fortran arrays (column-major, lower bounds 0). */
+typedef struct fg_restart_flow {
+  int nx, ny, nz;                 /* node counts                            */
+  double time;
+  int ntime;
+  /* (0:nx+1, 0:ny+1, 0:nz+1) */
+  double *u, *v, *w, *p, *face_u, *face_v, *face_w, *pPrime;
+  double *bcxu, *bcxv, *bcxw, *bcxp;  /* (0:1, 0:ny+1, 0:nz+1)              */
+  double *bcyu, *bcyv, *bcyw, *bcyp;  /* (0:nx+1, 0:1, 0:nz+1)              */
+  double *bczu, *bczv, *bczw, *bczp;  /* (0:nx+1, 0:ny+1, 0:1)              */
+  /* pgradx1, pgradx2 (0:ny+1,0:nz+1); pgrady1, pgrady2 (0:nx+1,0:nz+1);
+   * pgradz1, pgradz2 (0:nx+1,0:ny+1) -- the order of fg_get_pressure_gradient */
+  double *pgrad[6];
+  int8_t *iblank, *ghostcellmark;     /* (0:nx+1, 0:ny+1, 0:nz+1)           */
+} fg_restart_flow;
+typedef struct fg_restart_body {
+  int npts, nelm;
+  double *x, *y, *z, *u, *v, *w;  /* marker positions and velocities [npts] */
+  double *fx, *fy, *fz;           /* marker forces [npts]                   */
+  int *tri;                       /* [3*nelm] 0-based; stored 1-based       */
+  double cent[3], ang[3], vcent[3], angv[3];
+} fg_restart_body;
+fg_status fg_write_restart(const char *path, const fg_restart_flow *f, int nbody, const fg_restart_body *b);
+/* Reads into the arrays of f and b, whose sizes (nx, ny, nz, npts, nelm)
+ * must be those of the file (FG_IO_ERROR otherwise); sets time and ntime. */
+fg_status fg_read_restart(const char *path, fg_restart_flow *f, int nbody, fg_restart_body *b);
+/* The longest subrecord written (bytes, 16 .. 2**31-9; other values give
+ * the default 2**31-9), the counterpart of gfortran's
+ * -fmax-subrecord-length.  Process-wide. */
+void fg_set_max_subrecord(long long bytes);
+
+/* The Tecplot POINT dump of write_flowfield for nDim = 3
+ * (UTIL_GENERAL.F90:167-247): a VARIABLES line, a ZONE line of
+ * I = nx+1, J = ny+1, K = nz+1 points, then for k = 0..nz, j = 0..ny,
+ * i = 0..nx one line in format 11(2x,1PE12.5),5(2x,I2) of
+ * xc, yc, zc, u, v, w, p, ox, oy, oz, lmd, iblank, ghost, dead, body, goa.
+ * xc[0..nx], yc[0..ny], zc[0..nz] are the cell centres with the ghost
+ * layers; fields are (0:nx+1, 0:ny+1, 0:nz+1); a NULL field is written as
+ * zeros.  The reference gzips the file afterwards; this does not. */
+typedef struct fg_tecplot_fields {
+  const double *u, *v, *w, *p, *ox, *oy, *oz, *lmd;
+  const int8_t *iblank, *ghost, *dead, *bodynum, *goa;
+} fg_tecplot_fields;
+fg_status fg_write_tecplot(const char *path, int nx, int ny, int nz, const double *xc, const double *yc,
+                           const double *zc, const fg_tecplot_fields *f);
 
 #ifdef __cplusplus
 }

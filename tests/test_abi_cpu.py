@@ -32,7 +32,7 @@ def test_library_exports_header_symbols():
 def test_version_and_status_strings():
     L = fg.lib()
     assert L.fg_version().decode().startswith("feicar-b200")
-    for s in range(10):
+    for s in range(11):
         assert len(L.fg_status_string(s).decode()) > 0
 
 
