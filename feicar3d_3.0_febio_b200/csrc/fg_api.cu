@@ -664,15 +664,20 @@ static void free_krylov(fg_batch *b) {
   b->ksig.clear();
 }
 
+// wave: room behind the offsets for the ticket and plane counters of a
+// both-colour y/z sweep (zeroed by each such launch)
 static fg_status build_offsets(const std::vector<int> &blocks, int **d_off, Launch &Lr,
-                               const DevLevel *d_lev) {
+                               const DevLevel *d_lev, bool wave = false) {
   std::vector<int> off(blocks.size() + 1, 0);
   for (size_t p = 0; p < blocks.size(); ++p) off[p + 1] = off[p] + blocks[p];
+  const int total = off.back();
+  if (wave) off.resize(off.size() + (size_t)total + 2, 0);
   FG_CUDA(run_launch_set_alloc((void **)d_off, off));
   Lr.n = (int)blocks.size();
-  Lr.blocks = off.back();
+  Lr.blocks = total;
   Lr.off = *d_off;
   Lr.lev = d_lev;
+  Lr.wave = wave ? *d_off + blocks.size() + 1 : nullptr;
   return FG_OK;
 }
 
@@ -832,8 +837,8 @@ static fg_status build_batch(fg_batch *b) {
       fg_status st;
       if ((st = build_offsets(bc, &s.d_off_cells, s.cells, s.d_levS)) != FG_OK) return st;
       if ((st = build_offsets(bx, &s.d_off_x, s.xl, s.d_levS)) != FG_OK) return st;
-      if ((st = build_offsets(by, &s.d_off_y, s.yl, s.d_levS)) != FG_OK) return st;
-      if ((st = build_offsets(bz, &s.d_off_z, s.zl, s.d_levS)) != FG_OK) return st;
+      if ((st = build_offsets(by, &s.d_off_y, s.yl, s.d_levS, true)) != FG_OK) return st;
+      if ((st = build_offsets(bz, &s.d_off_z, s.zl, s.d_levS, true)) != FG_OK) return st;
       if ((st = build_offsets(bn, &s.d_off_next, s.next, s.d_levS_next)) != FG_OK) return st;
       if ((st = build_offsets(bq, &s.d_off_quads, s.quads, s.d_levS)) != FG_OK) return st;
     }
@@ -977,10 +982,11 @@ static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
     const Launch &Lr = axis == 0 ? ls.xl : axis == 1 ? ls.yl : ls.zl;
     const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
     const int cls = L == 0 ? FG_PROF_LINE_X0 + axis : FG_PROF_LINE_COARSE;
-    for (int color = 0; color < 2; ++color) {
+    const bool both = k::line_both_colours(axis, maxn, b->tune.var[L][axis]);
+    for (int color = 0; color < (both ? 1 : 2); ++color) {
       const size_t e0 = prof_begin(b, s);
       FG_K(k::line_sweep<T>(Lr, axis, color, om, maxn, b->tune.var[L][axis], s));
-      prof_end(b, e0, cls, sweep_bytes<T>(ls.ncells, om), s);
+      prof_end(b, e0, cls, (both ? 2.0 : 1.0) * sweep_bytes<T>(ls.ncells, om), s);
     }
     if (L == 0) {
       const size_t e0 = prof_begin(b, s);
@@ -1672,14 +1678,31 @@ static fg_status batch_enqueue(fg_batch *b) {
   return fgmres_enqueue<double, double>(b);
 }
 
+static bool uses_wave(const fg_batch *b) {
+  for (int L = 0; L < b->maxdepth; ++L) {
+    const auto &ls = b->ls[L];
+    if (ls.S.empty()) continue;
+    if (k::line_both_colours(1, ls.maxny, b->tune.var[L][1]) || k::line_both_colours(2, ls.maxnz, b->tune.var[L][2]))
+      return true;
+  }
+  return false;
+}
+
 static fg_status batch_collect(fg_batch *b, fg_solve_stats *st) {
+  fg_status r;
   if (b->cfg.outer != FG_OUTER_FGMRES) {
     if (!b->pending) return FG_BAD_INPUT;
     b->pending = false;
     if (st) *st = b->rich_stats;
-    return b->rich_status;
+    r = b->rich_status;
+  } else {
+    r = fgmres_collect(b, st);
   }
-  return fgmres_collect(b, st);
+  if (uses_wave(b)) {
+    const fg_status w = k::wave_error_take();
+    if (w != FG_OK) return w;
+  }
+  return r;
 }
 
 static fg_status batch_solve(fg_batch *b, fg_solve_stats *st) {
@@ -1713,7 +1736,7 @@ static fg_status rebuild_line_offsets(fg_batch *b, int L, int axis) {
   Launch &Lr = axis == 0 ? s.xl : axis == 1 ? s.yl : s.zl;
   fg::dev_free(*off);
   *off = nullptr;
-  return build_offsets(blocks, off, Lr, s.d_levS);
+  return build_offsets(blocks, off, Lr, s.d_levS, axis != 0);
 }
 
 // the captured V-cycle and solve graphs hold the old launch shapes
@@ -1747,7 +1770,7 @@ static fg_status tune_lines(fg_batch *b) {
     for (int axis = 0; axis < 3 && st == FG_OK; ++axis) {
       const int maxn = axis == 0 ? ls.maxnx : axis == 1 ? ls.maxny : ls.maxnz;
       std::vector<int> cand;
-      for (int v = 1; v <= 3; ++v) {
+      for (int v = 1; v <= (axis == 0 ? k::LV_NX : k::LV_NYZ); ++v) {
         const int r = k::line_variant(axis, maxn, v);
         if (std::find(cand.begin(), cand.end(), r) == cand.end()) cand.push_back(r);
       }
@@ -1920,9 +1943,10 @@ static void install_rows(fg_case *c) {
 static fg_status build_levels(fg_case *c) {
   cudaStream_t s = c->stream;
   const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
-  if (!c->d_refmask) FG_CUDA(fg::dev_alloc(&c->d_refmask, 2 * nref));
+  if (!c->d_refmask) FG_CUDA(fg::dev_alloc(&c->d_refmask, 3 * nref));
   FG_CUDA(cudaMemcpyAsync(c->d_refmask, c->iblank.data(), nref, cudaMemcpyHostToDevice, s));
   FG_CUDA(cudaMemcpyAsync(c->d_refmask + nref, c->ghost.data(), nref, cudaMemcpyHostToDevice, s));
+  FG_CUDA(cudaMemcpyAsync(c->d_refmask + 2 * nref, c->dead.data(), nref, cudaMemcpyHostToDevice, s));
   const int nr = (int)c->rows.tgt.size();
   if ((size_t)nr > c->rowtgt_cap) {
     fg::dev_free(c->d_rowtgt);
@@ -2118,7 +2142,7 @@ fg_status fg_case_destroy(fg_case *c) {
     L.raw.clear();
   }
   fg::dev_free(c->d_G); fg::dev_free(c->d_gidx); fg::dev_free(c->d_pin); fg::dev_free(c->d_fin);
-  fg::dev_free(c->d_refmask); fg::dev_free(c->d_rowtgt);
+  fg::dev_free(c->d_refmask); fg::dev_free(c->d_rowtgt); fg::dev_free(c->d_rcg);
   fg::dev_free(c->d_gauge);
   fg::dev_free(c->d_pgrad); fg::dev_free(c->d_met); fg::dev_free(c->d_cpart); fg::dev_free(c->d_pmet);
   if (c->geom) geom_free(*c->geom);
@@ -2325,6 +2349,102 @@ static void row_constants(fg_case *c, const double *p_old, const double *dpdn_g,
   }
 }
 
+// The per-row data row_constants reads, for the device kernel: built on
+// the host once per geometry, in the order row_constants emits the rows.
+static fg_status ensure_rowconst_geo(fg_case *c, k::RowConstGeo &g) {
+  if (c->rcg_version != c->geom_version || !c->d_rcg) {
+    const long long RX = c->nx + 2, RY = c->ny + 2;
+    static const int inc[8][3] = {{0, 0, 0}, {0, 1, 0}, {1, 1, 0}, {1, 0, 0},
+                                  {0, 0, 1}, {0, 1, 1}, {1, 1, 1}, {1, 0, 1}};
+    auto xcv = [&](int ax, int i) {
+      return ax == 0 ? c->lev[0].xc[i] : ax == 1 ? c->lev[0].yc[i] : c->lev[0].zc[i];
+    };
+    std::vector<int> src;
+    std::vector<int8_t> fb;
+    std::vector<double> a, b, fw;
+    std::vector<long long> fid;
+    for (int r = 0; r < c->nDead; ++r) {
+      const int i = c->d_ijk[3 * r], j = c->d_ijk[3 * r + 1], k = c->d_ijk[3 * r + 2];
+      const int ci = c->d_cell[3 * r], cj = c->d_cell[3 * r + 1], ck = c->d_cell[3 * r + 2];
+      if (i < 1 || i > c->lev[0].nx || j < 1 || j > c->lev[0].ny || k < 1 || k > c->lev[0].nz) continue;
+      if (ci < 0 || cj < 0 || ck < 0) continue;
+      src.push_back(r);
+      double own = 0.0;
+      long long ids[8];
+      double ws[8];
+      const bool fall = c->d_fallback[r] != 0;
+      const double *ipp = c->d_ipv.size() >= 3 * (size_t)(r + 1) ? &c->d_ipv[3 * r] : nullptr;
+      const double X = ipp ? ipp[0] : 0.5 * (xcv(0, ci) + xcv(0, ci + 1));
+      const double Y = ipp ? ipp[1] : 0.5 * (xcv(1, cj) + xcv(1, cj + 1));
+      const double Z = ipp ? ipp[2] : 0.5 * (xcv(2, ck) + xcv(2, ck + 1));
+      for (int q = 0; q < 8; ++q) {
+        const int ii = ci + inc[q][0], jj = cj + inc[q][1], kk = ck + inc[q][2];
+        ids[q] = -1;
+        ws[q] = 0.0;
+        if (ii == i && jj == j && kk == k) {
+          if (!fall) own += c->d_coefN[8 * r + q];
+          continue;
+        }
+        const long long id = ii + RX * (jj + RY * (long long)kk);
+        if (fall && (c->iblank[id] == 0 || c->dead[id] == -1)) {
+          const double d = (xcv(0, ii) - X) * (xcv(0, ii) - X) + (xcv(1, jj) - Y) * (xcv(1, jj) - Y) +
+                           (xcv(2, kk) - Z) * (xcv(2, kk) - Z);
+          ids[q] = id;
+          ws[q] = 1.0 / d;
+        }
+      }
+      fb.push_back(fall ? 1 : 0);
+      a.push_back(own);
+      b.push_back(c->d_probe[r]);
+      fid.insert(fid.end(), ids, ids + 8);
+      fw.insert(fw.end(), ws, ws + 8);
+    }
+    for (int r = 0; r < c->nGhost; ++r) {
+      const int i = c->g_ijk[3 * r], j = c->g_ijk[3 * r + 1], k = c->g_ijk[3 * r + 2];
+      const int ci = c->g_cell[3 * r], cj = c->g_cell[3 * r + 1], ck = c->g_cell[3 * r + 2];
+      if (ci < 0 || cj < 0 || ck < 0) continue;
+      src.push_back(c->nDead + r);
+      double own = 0.0;
+      for (int q = 0; q < 8; ++q)
+        if (ci + inc[q][0] == i && cj + inc[q][1] == j && ck + inc[q][2] == k) own += c->g_coefN[8 * r + q];
+      fb.push_back(0);
+      a.push_back(own);
+      b.push_back(0.0);
+      for (int q = 0; q < 8; ++q) { fid.push_back(-1); fw.push_back(0.0); }
+    }
+    const size_t n = src.size();
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t o_src = 0, o_fb = al(n * 4), o_a = o_fb + al(n), o_b = o_a + al(n * 8), o_fid = o_b + al(n * 8),
+                 o_fw = o_fid + al(n * 64), total = o_fw + al(n * 64) + 256;
+    std::vector<unsigned char> blob(total, 0);
+    if (n) {
+      memcpy(blob.data() + o_src, src.data(), n * 4);
+      memcpy(blob.data() + o_fb, fb.data(), n);
+      memcpy(blob.data() + o_a, a.data(), n * 8);
+      memcpy(blob.data() + o_b, b.data(), n * 8);
+      memcpy(blob.data() + o_fid, fid.data(), n * 64);
+      memcpy(blob.data() + o_fw, fw.data(), n * 64);
+    }
+    fg::dev_free(c->d_rcg);
+    c->d_rcg = nullptr;
+    FG_CUDA(fg::dev_alloc(&c->d_rcg, total));
+    FG_CUDA(cudaMemcpy(c->d_rcg, blob.data(), total, cudaMemcpyHostToDevice));
+    c->rcg_version = c->geom_version;
+    c->rcg_n = (int)n;
+    unsigned char *base = static_cast<unsigned char *>(c->d_rcg);
+    g.src = reinterpret_cast<const int *>(base + o_src);
+    g.fb = reinterpret_cast<const int8_t *>(base + o_fb);
+    g.a = reinterpret_cast<const double *>(base + o_a);
+    g.b = reinterpret_cast<const double *>(base + o_b);
+    g.fid = reinterpret_cast<const long long *>(base + o_fid);
+    g.fw = reinterpret_cast<const double *>(base + o_fw);
+    c->rcg_ptrs = g;
+    return FG_OK;
+  }
+  g = c->rcg_ptrs;
+  return FG_OK;
+}
+
 // outer-face data of a case (Dirichlet values; Neumann faces carry no
 // gradient data: homogeneous)
 static long long pgrad_size(const fg_case *c, int face) {
@@ -2420,6 +2540,23 @@ fg_status fg::solve_enqueue(fg_case *c, const double *p_old, const double *dpdn_
   return finish_output(c);
 }
 
+fg_status fg::solve_enqueue_dev(fg_case *c, const double *d_p_old, const double *d_dpdn_g, const double *d_dpdn_d) {
+  fg_status s = ensure_solo(c);
+  if (s != FG_OK) return s;
+  k::RowConstGeo g;
+  if ((s = ensure_rowconst_geo(c, g)) != FG_OK) return s;
+  if (c->rcg_n != c->solo->rows.n) return FG_BAD_INPUT;
+  FG_K(k::row_constants_device(c->rcg_n, g, d_p_old, d_dpdn_g, d_dpdn_d, c->nDead, c->solo->d_rc0, c->stream));
+  HLevel &L0 = c->lev[0];
+  FG_K(k::copy_in(L0.d_x64, c->d_pin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  FG_K(k::copy_in(L0.d_rhs64, c->d_fin, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  if (c->vzg && (s = compat_device(c, c->d_pin, c->vzg)) != FG_OK) return s;
+  FG_K(k::face_rhs(L0.d_rhs64, L0.dl, face_data(c), c->stream));
+  if ((s = batch_enqueue(c->solo)) != FG_OK) return s;
+  FG_K(k::copy_out(c->d_pin, L0.d_x64, L0.nx, L0.ny, L0.nz, L0.sy, L0.sz, c->stream));
+  return finish_output(c);
+}
+
 fg_status fg::solve_collect(fg_case *c, fg_solve_stats *st) { return batch_collect(c->solo, st); }
 
 extern "C" {
@@ -2442,13 +2579,18 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div, const doubl
 
 fg_status fg_solve_poisson_device(fg_case *c, double *d_p, const double *d_div,
                                   const double *d_p_old, fg_solve_stats *st) {
+  return fg_solve_poisson_device_bc(c, d_p, d_div, d_p_old, nullptr, nullptr, st);
+}
+
+fg_status fg_solve_poisson_device_bc(fg_case *c, double *d_p, const double *d_div, const double *d_p_old,
+                                     const double *d_dpdn_ghost, const double *d_dpdn_dead, fg_solve_stats *st) {
   if (!c || !d_p || !d_div) return FG_BAD_INPUT;
-  if (d_p_old) return FG_BAD_INPUT;  // the fallback constants need host p_old
   cudaSetDevice(c->device);
   const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
   FG_CUDA(cudaMemcpyAsync(c->d_pin, d_p, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   FG_CUDA(cudaMemcpyAsync(c->d_fin, d_div, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  fg_status s = fg::solve_enqueue(c, nullptr, nullptr, nullptr);
+  fg_status s = (d_p_old || d_dpdn_ghost || d_dpdn_dead) ? fg::solve_enqueue_dev(c, d_p_old, d_dpdn_ghost, d_dpdn_dead)
+                                                          : fg::solve_enqueue(c, nullptr, nullptr, nullptr);
   if (s != FG_OK) return s;
   FG_CUDA(cudaMemcpyAsync(d_p, c->d_pin, nref * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   s = fg::solve_collect(c, st);
@@ -2693,6 +2835,51 @@ fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out) {
   for (int q = 0; q < 4; ++q) out->solve_ms[q] = b->tune.solve_ms[q];
   out->tuned = b->tune.nu_tuned ? 1 : 0;
   return FG_OK;
+}
+
+fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t) {
+  if (!b || b->cases.empty() || !t) return FG_BAD_INPUT;
+  if (t->nu1 < 0 || t->nu2 < 0 || t->nu1 + t->nu2 > 16) return FG_BAD_INPUT;
+  cudaSetDevice(b->device);
+  if (!b->stream) cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (auto *c : b->cases)
+    if (!c->prepared) {
+      fg_status s = prepare(c);
+      if (s != FG_OK) return s;
+    }
+  bool stale = !b->built || b->versions.size() != b->cases.size();
+  for (size_t p = 0; !stale && p < b->cases.size(); ++p) stale = b->versions[p] != b->cases[p]->geom_version;
+  if (stale) {
+    fg_status s = build_batch(b);
+    if (s != FG_OK) return s;
+  }
+  for (int L = 0; L < b->maxdepth && L < FG_TUNE_MAXLEVELS; ++L) {
+    if (b->ls[L].S.empty()) continue;
+    for (int a = 0; a < 3; ++a) {
+      const int v = t->line_variant[L][a];
+      if (v < 0 || v > (a == 0 ? k::LV_NX : k::LV_NYZ)) return FG_BAD_INPUT;
+      b->tune.var[L][a] = v;  // 0 or a family that cannot take the lines: the default
+      b->tune.us[L][a] = 0.0;
+      fg_status s = rebuild_line_offsets(b, L, a);
+      if (s != FG_OK) return s;
+    }
+  }
+  if (t->nu1 + t->nu2 > 0) {
+    b->cfg.nu1 = t->nu1;
+    b->cfg.nu2 = t->nu2;
+  }
+  drop_graphs(b);
+  b->tune.nu_tuned = false;
+  b->tune.key = tune_key(b);
+  return FG_OK;
+}
+
+fg_status fg_case_set_tuning(fg_case *c, const fg_tuning *t) {
+  if (!c || !t) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  fg_status st = ensure_solo(c);
+  if (st != FG_OK) return st;
+  return fg_batch_set_tuning(c->solo, t);
 }
 
 fg_status fg_case_autotune(fg_case *c, double *d_p, const double *d_div, fg_tuning *out) {

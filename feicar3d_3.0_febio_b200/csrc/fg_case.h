@@ -101,9 +101,15 @@ struct fg_case {
   int *d_gidx = nullptr;
   size_t G_cap = 0, gidx_cap = 0;  // elements the two device arrays hold
   long long geom_version = 0;      // bumped by every prepare
+  // per interpolation row, for row constants formed on the device: the
+  // dp/dn index, its two factors, the fallback corners and weights
+  void *d_rcg = nullptr;
+  long long rcg_version = -1;
+  int rcg_n = 0;
+  fg::k::RowConstGeo rcg_ptrs{};
   // reference-layout staging buffers on the device
   double *d_pin = nullptr, *d_fin = nullptr;
-  int8_t *d_refmask = nullptr;      // iblank then ghostCellMark (reference layout)
+  int8_t *d_refmask = nullptr;      // iblank, ghostCellMark, dead_cell (reference layout)
   long long *d_rowtgt = nullptr;    // level-0 element of every row
   size_t rowtgt_cap = 0;
   double *d_gauge = nullptr;  // p(1,1,1) of the output gauge
@@ -130,5 +136,8 @@ fg_status geometry_rows(fg_case *c, int nGhost, const int32_t *ghost_ijk, const 
 // a solve of the fields staged in c->d_pin / c->d_fin queued on the case's
 // stream (output finished into d_pin), and the wait for its outcome
 fg_status solve_enqueue(fg_case *c, const double *p_old, const double *dpdn_g, const double *dpdn_d);
+// the same with the row constants formed on the device from device p_old
+// and dp/dn arrays (each may be NULL)
+fg_status solve_enqueue_dev(fg_case *c, const double *d_p_old, const double *d_dpdn_g, const double *d_dpdn_d);
 fg_status solve_collect(fg_case *c, fg_solve_stats *st);
 }  // namespace fg

@@ -129,6 +129,7 @@ struct Launch {
   int blocks = 0;
   const int *off = nullptr;
   const DevLevel *lev = nullptr;
+  int *wave = nullptr;  // y/z sweeps: ticket and plane counters (blocks + 2 ints)
   bool empty() const { return n == 0 || blocks == 0; }
 };
 
@@ -257,12 +258,22 @@ int blocks_quads(const DevLevel &L);
 // default or by the autotuner): x lines in registers (lanes by line
 // length, or always 32), x lines staged in shared memory (one warp per
 // line); y/z tiles in registers with a per-line Thomas over the chunks,
-// with a block-wide PCR over the chunks, or one warp per line
+// with a block-wide PCR over the chunks, or one warp per line; the PCR
+// tile with every row's loads issued first at fewer blocks per SM (8 rows
+// per thread), with 4 rows per thread and twice the chunks, or both
+// colours of a sweep in one launch (plane-ordered tickets)
 enum : int {
   LV_DEFAULT = 0,
   LV_XREG = 1, LV_XREG32 = 2, LV_XSMEM = 3,
-  LV_YREG = 1, LV_YPCR = 2, LV_YWARP = 3
+  LV_YREG = 1, LV_YPCR = 2, LV_YWARP = 3, LV_YPCRH = 4, LV_YPCR4 = 5, LV_YWAVE = 6
 };
+constexpr int LV_NX = 3, LV_NYZ = 6;  // families per axis kind
+// the family does both colours in the colour-0 call of line_sweep (the
+// colour-1 call launches nothing)
+bool line_both_colours(int axis, int maxn, int variant);
+// FG_TIMEOUT (once) if a both-colour y/z sweep gave up a wait since the
+// last call
+fg_status wave_error_take();
 int line_variant(int axis, int maxn, int v);  // the family that runs
 int blocks_xline(const DevLevel &L, int maxn, int variant);
 // y/z tiles: blocks depend on the kernel the level set's longest line picks
@@ -300,6 +311,18 @@ cudaError_t coarsest_solve(int nprob, const DevLevel *lev, const double *const *
                            const int *const *gidx, const int *gn, int maxn, cudaStream_t s);
 cudaError_t correct_residual(const Launch &L0, double *norm2, double *part, cudaStream_t s);
 cudaError_t fluid_norm(const Launch &L, double *norm2, double *part, cudaStream_t s);
+// row constants on the device (one thread per interpolation row):
+// c0[r] = (fallback ? sum w p_old / sum w : 0) + a dpdn + dpdn b, with dpdn =
+// dpdn[src[r]] (ghost rows after the nd dead ones) or 0 without dp/dn data
+struct RowConstGeo {
+  const int *src;
+  const int8_t *fb;
+  const double *a, *b;
+  const long long *fid;  // 8 per row, -1 = not a fallback corner
+  const double *fw;      // 8 per row
+};
+cudaError_t row_constants_device(int n, RowConstGeo g, const double *p_old, const double *dpdn_g,
+                                 const double *dpdn_d, int nd, double *c0, cudaStream_t s);
 cudaError_t copy_in(double *dst, const double *src, int nx, int ny, int nz, long long sy,
                     long long sz, cudaStream_t s);
 cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, long long sy,

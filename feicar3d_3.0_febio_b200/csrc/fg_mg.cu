@@ -1191,8 +1191,10 @@ int line_variant(int axis, int maxn, int v) {
     if (v != LV_XREG && v != LV_XREG32 && v != LV_XSMEM) v = maxn <= 128 ? LV_XREG : LV_XSMEM;
     return v;
   }
-  if ((v == LV_YREG || v == LV_YPCR) && maxn > YZ_MAXROWS) v = LV_DEFAULT;
-  if (v != LV_YREG && v != LV_YPCR && v != LV_YWARP)
+  const bool pcr = v == LV_YPCR || v == LV_YPCRH || v == LV_YPCR4 || v == LV_YWAVE;
+  if ((v == LV_YREG || pcr) && maxn > YZ_MAXROWS) v = LV_DEFAULT;
+  if (pcr && v != LV_YPCR && maxn < YP_MINROWS) v = LV_DEFAULT;
+  if (v != LV_YREG && v != LV_YWARP && !pcr)
     v = (maxn >= YP_MINROWS && maxn <= YZ_MAXROWS) ? LV_YPCR : maxn <= YZ_MAXROWS ? LV_YREG : LV_YWARP;
   return v;
 }
@@ -1208,7 +1210,7 @@ int blocks_xline(const DevLevel &L, int maxn, int variant) {
 int blocks_tile(const DevLevel &L, int axis, int maxn, int variant) {
   // i-tile of k_yzline_reg (64 cells), k_yzline_pcr (16) or k_yzline (16)
   const int v = line_variant(axis, maxn, variant);
-  const int w = v == LV_YREG ? 64 : v == LV_YPCR ? 2 * YP_LINES : TILE_I;
+  const int w = v == LV_YREG ? 64 : (v == LV_YPCR || v == LV_YPCRH || v == LV_YPCR4 || v == LV_YWAVE) ? 2 * YP_LINES : TILE_I;
   const int ntx = (L.nx + w - 1) / w;
   return ntx * (axis == 1 ? L.nz : L.ny);
 }
@@ -1259,18 +1261,27 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
   return cudaGetLastError();
 }
 
-// Zebra y/z line relaxation in short chunks, for lines of YP_MINROWS..
-// YZ_MAXROWS cells.  A block takes YP_LINES lines of one colour in an i-tile
-// of 2 YP_LINES cells (thread t: line t % YP_LINES at i = i0 + par + 2 (t % YP_LINES),
-// chunk t / YP_LINES of CH chunks of M rows).  Every thread issues the
-// loads of all its rows at once, eliminates its chunk in registers, the CH
-// chunk equations of each line are solved by parallel cyclic reduction
-// across the block (log2 CH steps through shared memory), and every thread
+// x loads of a tile: through L1, or (COH) from L2 only, for values other
+// blocks of the same launch may have written since this launch began
+template <bool COH, typename T>
+__device__ __forceinline__ T ldx(const T *p) {
+  if constexpr (COH) return __ldcg(p);
+  else return *p;
+}
+
+// One tile of zebra y/z line relaxation in short chunks, for lines of
+// YP_MINROWS..YZ_MAXROWS cells: YP_LINES lines of one colour in the i-tile
+// ti (2 YP_LINES cells) of plane o (k for AXIS 1, j for AXIS 2); thread t
+// takes line t % YP_LINES at i = i0 + par + 2 (t % YP_LINES) and chunk
+// t / YP_LINES of CH chunks of M rows.  Every thread issues the loads of
+// all its rows at once, eliminates its chunk in registers, the CH chunk
+// equations of each line are solved by parallel cyclic reduction across
+// the block (log2 CH steps through shared memory), and every thread
 // back-substitutes its rows.
-template <typename T, int M, int CH, int AXIS>
-__global__ void __launch_bounds__(CH * YP_LINES, ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
-                                                   ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1)
-k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+// NB > 0: the loads of all of a thread's rows are issued before the first
+// row's arithmetic (the kernels give NB blocks per SM, more registers).
+template <typename T, int M, int CH, int AXIS, int NB, bool COH>
+__device__ __forceinline__ void yz_pcr_tile(const DevLevel &L, int ti, int o, int color, T omega) {
   using LC = LineCoefT<T, AXIS>;
   constexpr int NT = CH * YP_LINES;
   __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
@@ -1281,15 +1292,7 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
   auto s_last = reinterpret_cast<T(*)[CH][YP_LINES]>(&s_eq[1][0][0]);
   const int tid = threadIdx.x;
   const int l = tid % YP_LINES, c = tid / YP_LINES;
-  const int p = find_entry(off, nent, blockIdx.x);
-  const int lb = blockIdx.x - off[p];
-  const DevLevel &L = levs[p];
   constexpr int TW = 2 * YP_LINES;  // cells of an i-tile
-  const int ntx = (L.nx + TW - 1) / TW;
-  const int ti = lb % ntx;
-  // k for AXIS 1, j for AXIS 2; a colour-1 launch walks the planes backward,
-  // so its first blocks meet the planes the colour-0 launch left in L2
-  const int o = color == 1 ? (AXIS == 1 ? L.nz : L.ny) - lb / ntx : 1 + lb / ntx;
   const int i0 = 1 + TW * ti;
   const int par = (color + i0 + o) & 1;
   const int i = i0 + par + 2 * l;
@@ -1311,24 +1314,57 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
   const bool any = valid && r0 < n;
   T d[M], al[M], ga[M];
   uint8_t mk[M];
+  if constexpr (NB > 0) {
+    // every load of the thread's rows first, then the arithmetic
+    T rv[M], xv[M], nb[M][4];
 #pragma unroll
-  for (int u = 0; u < M; ++u) {
-    const int r = r0 + u;
-    d[u] = T(0);
-    mk[u] = 0;
-    if (any && r < n) {
-      const long long id = base + ls * (r + 1);
-      uint8_t m8 = L.mask[id];
-      const T rv = rhs[id];
-      const T xv = x[id];
-      const T nb[4] = {x[id - 1], x[id + 1], x[id - os], x[id + os]};
-      T acc = rv;
+    for (int u = 0; u < M; ++u) {
+      const int r = r0 + u;
+      mk[u] = 0;
+      rv[u] = xv[u] = T(0);
+      nb[u][0] = nb[u][1] = nb[u][2] = nb[u][3] = T(0);
+      if (any && r < n) {
+        const long long id = base + ls * (r + 1);
+        mk[u] = L.mask[id];
+        rv[u] = rhs[id];
+        xv[u] = ldx<COH>(x + id);
+        nb[u][0] = ldx<COH>(x + id - 1);
+        nb[u][1] = ldx<COH>(x + id + 1);
+        nb[u][2] = ldx<COH>(x + id - os);
+        nb[u][3] = ldx<COH>(x + id + os);
+      }
+    }
 #pragma unroll
-      for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
+    for (int u = 0; u < M; ++u) {
+      uint8_t m8 = mk[u];
+      T acc = rv[u];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[u][t] : T(0);
       const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
-      if (held) { acc = xv; m8 = 0; }
-      d[u] = acc;
-      mk[u] = m8;
+      if (held) { acc = xv[u]; m8 = 0; }
+      d[u] = (any && r0 + u < n) ? acc : T(0);
+      mk[u] = (any && r0 + u < n) ? m8 : (uint8_t)0;
+    }
+  } else {
+#pragma unroll
+    for (int u = 0; u < M; ++u) {
+      const int r = r0 + u;
+      d[u] = T(0);
+      mk[u] = 0;
+      if (any && r < n) {
+        const long long id = base + ls * (r + 1);
+        uint8_t m8 = L.mask[id];
+        const T rv = rhs[id];
+        const T xv = ldx<COH>(x + id);
+        const T nb[4] = {ldx<COH>(x + id - 1), ldx<COH>(x + id + 1), ldx<COH>(x + id - os), ldx<COH>(x + id + os)};
+        T acc = rv;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
+        const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+        if (held) { acc = xv; m8 = 0; }
+        d[u] = acc;
+        mk[u] = m8;
+      }
     }
   }
   __syncthreads();  // s_am, s_ap
@@ -1378,8 +1414,103 @@ k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega)
     if (r >= n) break;
     T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
     const long long id = base + ls * (r + 1);
-    if (omega != T(1)) v = x[id] + omega * (v - x[id]);
+    if (omega != T(1)) {
+      const T xo = ldx<COH>(x + id);
+      v = xo + omega * (v - xo);
+    }
     x[id] = v;
+  }
+}
+
+
+// occupancy bound of the y/z PCR kernels
+template <typename T, int CH, int NB>
+struct YpBound {
+  static constexpr int def = ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
+                                 ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1;
+  static constexpr int v = NB > 0 ? NB : def;
+};
+
+// one colour of a sweep: block -> (problem, tile, plane); a colour-1
+// launch walks the planes backward, so its first blocks meet the planes
+// the colour-0 launch left in L2
+template <typename T, int M, int CH, int AXIS, int NB>
+__global__ void __launch_bounds__(CH * YP_LINES, YpBound<T, CH, NB>::v)
+k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+  const int p = find_entry(off, nent, blockIdx.x);
+  const int lb = blockIdx.x - off[p];
+  const DevLevel &L = levs[p];
+  const int ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+  const int ti = lb % ntx;
+  const int o = color == 1 ? (AXIS == 1 ? L.nz : L.ny) - lb / ntx : 1 + lb / ntx;
+  yz_pcr_tile<T, M, CH, AXIS, NB, false>(L, ti, o, color, omega);
+}
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Both colours of a y/z sweep in one launch.  Each block draws a ticket
+// (in the order blocks start) that names one tile of one plane and colour;
+// per problem the tickets run through the plane groups C0(0) .. C0(D),
+// then C0(D+1), C1(0), C0(D+2), C1(1), ..., then C1(N-D-1) .. C1(N-1): a
+// colour-1 plane comes D planes after the colour-0 plane it needs last,
+// with D (at most N-1) such that D planes of tiles fill the GPU's resident
+// blocks (`resident`), so a colour-1 tile rarely finds them unfinished.  A colour-0 tile
+// reads only values no block of the launch writes before it; a colour-1
+// tile of plane q waits until every colour-0 tile of planes q-1, q, q+1
+// has stored its lines (a per-plane count), so it reads their new values
+// (from L2, where the colour-0 tiles left them) and none of its writes
+// reaches a colour-0 tile that still reads the old ones.  Every wait is on
+// tiles with earlier tickets, whose blocks have started, so all waits end;
+// each is also bounded, and one that gives up sets *err and goes on.
+// wave: [0] the ticket counter, [2 + off[p] + q ntx] the colour-0 count of
+// plane q of problem p; zeroed before each launch.
+template <typename T, int M, int CH, int AXIS>
+__global__ void __launch_bounds__(CH * YP_LINES, YpBound<T, CH, 0>::v)
+k_yzline_wave(const int *off, int nent, const DevLevel *levs, T omega, int *wave, int *err, int resident) {
+  __shared__ int s_ticket;
+  if (threadIdx.x == 0) s_ticket = atomicAdd(wave, 1);
+  __syncthreads();
+  const int t = s_ticket;
+  const int p = find_entry(off, nent, t >> 1);
+  const DevLevel &L = levs[p];
+  const int ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+  const int N = AXIS == 1 ? L.nz : L.ny;
+  const int u = t - 2 * off[p];
+  const int g = u / ntx, ti = u % ntx;
+  const int D = min(N - 1, (resident + ntx - 1) / ntx);
+  const int npair = 2 * (N - 1 - D);  // groups of the interleaved middle
+  int color, q;
+  if (g <= D) { color = 0; q = g; }
+  else if (g - (D + 1) < npair) {
+    const int h = g - (D + 1);
+    if (h & 1) { color = 1; q = h >> 1; }
+    else { color = 0; q = D + 1 + (h >> 1); }
+  } else { color = 1; q = N - 1 - D + (g - (D + 1) - npair); }
+  int *cnt = wave + 2 + off[p];
+  if (color == 1) {
+    if (threadIdx.x == 0) {
+      for (int dq = -1; dq <= 1; ++dq) {
+        const int qq = q + dq;
+        if (qq < 0 || qq >= N) continue;
+        unsigned spins = 0;
+        while (ld_acquire_gpu(cnt + qq * ntx) < ntx) {
+          if (++spins > (1u << 22)) { atomicOr(err, 1); break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    yz_pcr_tile<T, M, CH, AXIS, 0, true>(L, ti, 1 + q, 1, omega);
+  } else {
+    yz_pcr_tile<T, M, CH, AXIS, 0, false>(L, ti, 1 + q, 0, omega);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(cnt + q * ntx, 1);
   }
 }
 
@@ -1393,15 +1524,15 @@ static cudaError_t launch_xsmem(const Launch &Lr, int color, double omega, cudaS
   return cudaGetLastError();
 }
 
-template <typename T, int M, int CH>
+template <typename T, int M, int CH, int NB = 0>
 static cudaError_t launch_yzpcr(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
   const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
   if (axis == 1) {
-    auto kern = k_yzline_pcr<T, M, CH, 1>;
+    auto kern = k_yzline_pcr<T, M, CH, 1, NB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
   } else {
-    auto kern = k_yzline_pcr<T, M, CH, 2>;
+    auto kern = k_yzline_pcr<T, M, CH, 2, NB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     kern<<<Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, color, (T)omega);
   }
@@ -1410,6 +1541,75 @@ static cudaError_t launch_yzpcr(const Launch &Lr, int axis, int color, double om
 }
 
 
+
+__global__ void k_row_consts(int n, RowConstGeo g, const double *p_old, const double *dpdn_g, const double *dpdn_d,
+                             int nd, double *c0) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int q = g.src[r];
+  const double *dp = q < nd ? dpdn_d : dpdn_g;
+  const double dpdn = dp ? dp[q < nd ? q : q - nd] : 0.0;
+  double v = 0.0;
+  if (g.fb[r]) {
+    double num = 0.0, den = 0.0;
+    for (int t = 0; t < 8; ++t) {
+      const long long id = g.fid[8 * (long long)r + t];
+      if (id < 0) continue;
+      const double w = g.fw[8 * (long long)r + t];
+      den += w;
+      num += w * (p_old ? p_old[id] : 0.0);
+    }
+    v = num / den;
+  }
+  v += g.a[r] * dpdn;
+  v += dpdn * g.b[r];
+  c0[r] = v;
+}
+
+cudaError_t row_constants_device(int n, RowConstGeo g, const double *p_old, const double *dpdn_g,
+                                 const double *dpdn_d, int nd, double *c0, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_row_consts<<<(n + 127) / 128, 128, 0, s>>>(n, g, p_old, dpdn_g, dpdn_d, nd, c0);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+__device__ int g_wave_err;  // set by a k_yzline_wave wait that gave up
+
+template <typename T, int M, int CH>
+static cudaError_t launch_yzwave(const Launch &Lr, int axis, double omega, cudaStream_t s) {
+  if (!Lr.wave) return cudaErrorInvalidValue;
+  int *err = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void **)&err, g_wave_err);
+  if (e == cudaSuccess) e = cudaMemsetAsync(Lr.wave, 0, (size_t)(Lr.blocks + 2) * sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  const size_t sm = (size_t)2 * CH * YP_LINES * sizeof(Eq3<T>);
+  auto kern = axis == 1 ? k_yzline_wave<T, M, CH, 1> : k_yzline_wave<T, M, CH, 2>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  // blocks resident on the whole GPU at once (the lag of the colour-1 planes)
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CH * YP_LINES, sm);
+  const int resident = std::max(1, sms * per_sm);
+  kern<<<2 * Lr.blocks, CH * YP_LINES, sm, s>>>(Lr.off, Lr.n, Lr.lev, (T)omega, Lr.wave, err, resident);
+  note_launches(1);
+  return cudaGetLastError();
+}
+
+fg_status wave_error_take() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_wave_err, sizeof(int)) != cudaSuccess) return FG_CUDA_ERROR;
+  if (!v) return FG_OK;
+  const int zero = 0;
+  cudaMemcpyToSymbol(g_wave_err, &zero, sizeof(int));
+  set_last_error("a y/z line sweep gave up waiting for its neighbour planes", __FILE__, __LINE__);
+  return FG_TIMEOUT;
+}
+
+bool line_both_colours(int axis, int maxn, int variant) {
+  return axis != 0 && line_variant(axis, maxn, variant) == LV_YWAVE;
+}
 
 template <typename T, int M, int CH>
 static cudaError_t launch_yzreg(const Launch &Lr, int axis, int color, double omega, cudaStream_t s) {
@@ -1452,6 +1652,19 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
   if (v == LV_YPCR) {
     if (maxn <= 128) return launch_yzpcr<T, 8, 16>(Lr, axis, color, omega, s);
     return launch_yzpcr<T, 8, 32>(Lr, axis, color, omega, s);
+  }
+  if (v == LV_YPCRH) {
+    if (maxn <= 128) return launch_yzpcr<T, 8, 16, 4>(Lr, axis, color, omega, s);
+    return launch_yzpcr<T, 8, 32, 2>(Lr, axis, color, omega, s);
+  }
+  if (v == LV_YWAVE) {  // both colours in the colour-0 call
+    if (color == 1) return cudaSuccess;
+    if (maxn <= 128) return launch_yzwave<T, 8, 16>(Lr, axis, omega, s);
+    return launch_yzwave<T, 8, 32>(Lr, axis, omega, s);
+  }
+  if (v == LV_YPCR4) {
+    if (maxn <= 128) return launch_yzpcr<T, 4, 32, 4>(Lr, axis, color, omega, s);
+    return launch_yzpcr<T, 4, 64, 2>(Lr, axis, color, omega, s);
   }
   if (v == LV_YREG) {
     if (maxn <= 16) return launch_yzreg<T, 4, 4>(Lr, axis, color, omega, s);

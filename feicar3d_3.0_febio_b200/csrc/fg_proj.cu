@@ -227,6 +227,37 @@ __global__ void k_correct(Dims d, Met m, const int8_t *ib, const double *pp, dou
   }
 }
 
+// update_pressure: p' = 0 on the solid cells not dead-marked -1, i = 0..nx,
+// j = 0..ny+1, k = 0..nz+1
+__global__ void k_zero_solid(Dims d, const int8_t *ib, const int8_t *dead, double *pp) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ni = d.nx + 1, nj = d.NY;
+  if (e >= ni * nj * (d.nz + 2)) return;
+  const int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / (ni * nj));
+  const long long id = d.id(i, j, k);
+  if (ib[id] == 0 || dead[id] == -1) return;
+  pp[id] = 0.0;
+}
+
+// update_pressure's domain edge lines for one rank: i = 0..nx on j in
+// {0, ny} and j = 0..ny+1 on i in {0, nx}, each in the planes 0, nz, nz+1;
+// the four k lines at (i, j) in {0, nx} x {0, ny}
+__global__ void k_zero_edges(Dims d, double *pp) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int na = 6 * (d.nx + 1), nb = 6 * (d.ny + 2), nc = 4 * (d.nz + 2);
+  const int pl[3] = {0, d.nz, d.nz + 1};
+  if (t < na) {
+    const int i = t % (d.nx + 1), q = t / (d.nx + 1);
+    pp[d.id(i, (q & 1) ? d.ny : 0, pl[q >> 1])] = 0.0;
+  } else if (t < na + nb) {
+    const int u = t - na, j = u % (d.ny + 2), q = u / (d.ny + 2);
+    pp[d.id((q & 1) ? d.nx : 0, j, pl[q >> 1])] = 0.0;
+  } else if (t < na + nb + nc) {
+    const int u = t - na - nb, k = u % (d.nz + 2), q = u / (d.nz + 2);
+    pp[d.id((q & 1) ? d.nx : 0, (q & 2) ? d.ny : 0, k)] = 0.0;
+  }
+}
+
 }  // namespace proj
 }  // namespace fg
 
@@ -353,6 +384,27 @@ fg_status fg_correct_vel_device(fg_case *c, const double *pPrime, double dt, dou
   note_launches(1);
   FG_CUDA(cudaGetLastError());
   FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+fg_status fg_update_pressure_device(fg_case *c, double *pPrime, double *p) {
+  if (!c || !pPrime) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  proj::Met m;
+  proj::Dims d;
+  fg_status st = proj_setup(c, m, d);
+  if (st != FG_OK) return st;
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  const int8_t *ib = c->d_refmask, *dead = c->d_refmask + 2 * nref;
+  cudaStream_t s = c->stream;
+  const long long ncell = (long long)(c->nx + 1) * (c->ny + 2) * (c->nz + 2);
+  proj::k_zero_solid<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(d, ib, dead, pPrime);
+  const int nedge = 6 * (c->nx + 1) + 6 * (c->ny + 2) + 4 * (c->nz + 2);
+  proj::k_zero_edges<<<(nedge + 255) / 256, 256, 0, s>>>(d, pPrime);
+  note_launches(2);
+  FG_CUDA(cudaGetLastError());
+  if (p && p != pPrime) FG_CUDA(cudaMemcpyAsync(p, pPrime, nref * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  FG_CUDA(cudaStreamSynchronize(s));
   return FG_OK;
 }
 

@@ -308,10 +308,22 @@ class Case:
         _check(rc, "fg_solve_poisson", ok)
         return st.as_dict()
 
-    def solve_poisson_device(self, d_p: int, d_div: int, allow_not_converged=False):
-        """Device pointers (ints) of Fortran-layout float64 fields."""
+    def solve_poisson_device(self, d_p: int, d_div: int, allow_not_converged=False, d_p_old=None,
+                             d_dpdn_ghost=None, d_dpdn_dead=None):
+        """Device pointers (ints) of Fortran-layout float64 fields (and of
+        the previous pressure and dp/dn data, when given)."""
         st = SolveStats()
-        rc = lib().fg_solve_poisson_device(self.h, C.c_void_p(d_p), C.c_void_p(d_div), None, C.byref(st))
+        L = lib()
+        if d_p_old is None and d_dpdn_ghost is None and d_dpdn_dead is None:
+            rc = L.fg_solve_poisson_device(self.h, C.c_void_p(d_p), C.c_void_p(d_div), None, C.byref(st))
+        else:
+            if not getattr(L, "_bc_ready", False):
+                L.fg_solve_poisson_device_bc.argtypes = [C.c_void_p] * 6 + [C.POINTER(SolveStats)]
+                L.fg_solve_poisson_device_bc.restype = C.c_int
+                L._bc_ready = True
+            vp = lambda x: C.c_void_p(x) if x else None
+            rc = L.fg_solve_poisson_device_bc(self.h, C.c_void_p(d_p), C.c_void_p(d_div), vp(d_p_old),
+                                              vp(d_dpdn_ghost), vp(d_dpdn_dead), C.byref(st))
         ok = (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,)
         _check(rc, "fg_solve_poisson_device", ok)
         return st.as_dict()
@@ -573,7 +585,9 @@ class Server:
 
 # ---------------------------------------------------------------- autotuner
 LINE_FAMILIES = {0: {1: "x_registers", 2: "x_registers_32_lanes", 3: "x_shared_memory"},
-                 1: {1: "yz_registers_thomas", 2: "yz_block_pcr", 3: "yz_warp_per_line"}}
+                 1: {1: "yz_registers_thomas", 2: "yz_block_pcr", 3: "yz_warp_per_line",
+                     4: "yz_block_pcr_loads_first", 5: "yz_block_pcr_4_rows",
+                     6: "yz_block_pcr_both_colours_one_launch"}}
 
 
 class RigidMotion(C.Structure):
@@ -637,7 +651,10 @@ def _tune_lib():
         L.fg_batch_autotune.argtypes = [vp, vp, vp, C.POINTER(Tuning)]
         L.fg_batch_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.fg_case_autotune.argtypes = [vp, vp, vp, C.POINTER(Tuning)]
-        for n in ("fg_batch_autotune", "fg_batch_get_tuning", "fg_case_autotune"):
+        L.fg_batch_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.fg_case_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        for n in ("fg_batch_autotune", "fg_batch_get_tuning", "fg_case_autotune", "fg_batch_set_tuning",
+                  "fg_case_set_tuning"):
             getattr(L, n).restype = C.c_int
         L._tune_ready = True
     return L
@@ -649,6 +666,35 @@ def batch_autotune(batch, d_ps, d_divs) -> dict:
     D = (C.c_void_p * n)(*[C.c_void_p(x) for x in d_divs])
     t = Tuning()
     _check(_tune_lib().fg_batch_autotune(batch.h, P, D, C.byref(t)), "fg_batch_autotune")
+    return t.as_dict()
+
+
+def _tuning_struct(families, nu=(0, 0)):
+    """families: {level: {"x": v, "y": v, "z": v}} or one family per axis
+    {"x": v, ...} for every level (LINE_FAMILIES numbers)."""
+    t = Tuning()
+    t.nlevels = 12
+    for L in range(12):
+        row = families.get(L, {}) if any(isinstance(k, int) for k in families) else families
+        for a, name in enumerate("xyz"):
+            t.line_variant[L][a] = int(row.get(name, 0))
+    t.nu1, t.nu2 = int(nu[0]), int(nu[1])
+    return t
+
+
+def case_set_tuning(case, families, nu=(0, 0)):
+    t = _tuning_struct(families, nu)
+    _check(_tune_lib().fg_case_set_tuning(case.h, C.byref(t)), "fg_case_set_tuning")
+
+
+def batch_set_tuning(batch, families, nu=(0, 0)):
+    t = _tuning_struct(families, nu)
+    _check(_tune_lib().fg_batch_set_tuning(batch.h, C.byref(t)), "fg_batch_set_tuning")
+
+
+def batch_get_tuning(batch) -> dict:
+    t = Tuning()
+    _check(_tune_lib().fg_batch_get_tuning(batch.h, C.byref(t)), "fg_batch_get_tuning")
     return t.as_dict()
 
 
@@ -668,7 +714,9 @@ def _proj_lib():
         L.fg_rhs_poisson_device.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, C.c_double, vp,
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.fg_correct_vel_device.argtypes = [vp, vp, C.c_double, vp, vp, vp, vp, vp, vp]
-        for n in ("fg_face_vel_device", "fg_rhs_poisson_device", "fg_correct_vel_device"):
+        L.fg_update_pressure_device.argtypes = [vp, vp, vp]
+        for n in ("fg_face_vel_device", "fg_rhs_poisson_device", "fg_correct_vel_device",
+                  "fg_update_pressure_device"):
             getattr(L, n).restype = C.c_int
         L._proj_ready = True
     return L
@@ -691,6 +739,13 @@ def rhs_poisson_device(case, fu, fv, fw, bcxu, bcyv, bczw, vel_zero_gradient, dt
                                              _p(vz), dt, _dp(div), C.byref(sd), C.byref(rd)),
            "fg_rhs_poisson_device")
     return sd.value, rd.value
+
+
+def update_pressure_device(case, d_pprime: int, d_p: int | None = None):
+    """update_pressure on device fields: p' zeroed on non-dead solid cells
+    and the domain edge lines, then copied to p."""
+    _check(_proj_lib().fg_update_pressure_device(case.h, C.c_void_p(d_pprime), C.c_void_p(d_p) if d_p else None),
+           "fg_update_pressure_device")
 
 
 def correct_vel_device(case, pp, dt, u=None, v=None, w=None, dpdx=None, dpdy=None, dpdz=None):

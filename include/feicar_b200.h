@@ -182,10 +182,18 @@ fg_status fg_solve_poisson(fg_case *c, double *p, const double *div,
                            const double *p_old, const double *dpdn_ghost,
                            const double *dpdn_dead, fg_solve_stats *st);
 /* Same with device pointers on the handle's layout-compatible arrays
- * (Fortran field layout, double, on the handle's device). */
+ * (Fortran field layout, double, on the handle's device); d_p_old (NULL =
+ * 0) feeds the dead-cell fallback. */
 fg_status fg_solve_poisson_device(fg_case *c, double *d_p,
                                   const double *d_div, const double *d_p_old,
                                   fg_solve_stats *st);
+/* The same with device dp/dn data, d_dpdn_ghost[nGhost] and
+ * d_dpdn_dead[nDead] (NULL: homogeneous): the rows' constants (dp/dn
+ * terms, the p_old fallback) are formed by a kernel, so a time step's
+ * pressure data stay on the device. */
+fg_status fg_solve_poisson_device_bc(fg_case *c, double *d_p, const double *d_div, const double *d_p_old,
+                                     const double *d_dpdn_ghost, const double *d_dpdn_dead,
+                                     fg_solve_stats *st);
 /* Outer-face pressure gradients, the reference's module arrays pgradx1,
  * pgradx2, pgrady1, pgrady2, pgradz1, pgradz2 (face 0..5) read by
  * set_outer_pressure_bc (CORE_SET_OUTER_BC.F90:831-1042): x faces
@@ -245,6 +253,12 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
  * itself); either triple may be NULL. */
 fg_status fg_correct_vel_device(fg_case *c, const double *pPrime, double dt, double *u, double *v, double *w,
                                 double *dpdx, double *dpdy, double *dpdz);
+/* update_pressure (CORE_FRAC_STEP_ROUTINES.F90:212-299) for one rank:
+ * pPrime = 0 on the solid cells (iblank) not dead-marked -1, for
+ * i = 0..nx, j = 0..ny+1, k = 0..nz+1, and on the domain edge lines the
+ * reference's twelve edge assignments name (its plane k = -1, outside
+ * the array, is left out); then p = pPrime when p is not NULL. */
+fg_status fg_update_pressure_device(fg_case *c, double *pPrime, double *p);
 
 /* ----- stream, launch count and timing (no reference counterpart: the
  * reference prints wall time per solve_poisson call only,
@@ -351,7 +365,8 @@ fg_status fg_batch_destroy(fg_batch *b);
  * last solution in d_p. */
 #define FG_TUNE_MAXLEVELS 12
 enum { FG_LV_XREG = 1, FG_LV_XREG32 = 2, FG_LV_XSMEM = 3 };   /* x sweeps   */
-enum { FG_LV_YREG = 1, FG_LV_YPCR = 2, FG_LV_YWARP = 3 };     /* y/z sweeps */
+enum { FG_LV_YREG = 1, FG_LV_YPCR = 2, FG_LV_YWARP = 3,       /* y/z sweeps */
+       FG_LV_YPCR_HOISTED = 4, FG_LV_YPCR_4ROWS = 5, FG_LV_YWAVE = 6 };
 typedef struct fg_tuning {
   int nlevels;
   int line_variant[FG_TUNE_MAXLEVELS][3];  /* family that runs, per level and axis (0: no line launches) */
@@ -365,6 +380,13 @@ fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out);
 /* The same for a single case's solves (d_p, d_div: device fields in the
  * reference layout, as for fg_solve_poisson_device). */
 fg_status fg_case_autotune(fg_case *c, double *d_p, const double *d_div, fg_tuning *out);
+/* Sets the families and smoothing steps of an earlier tuning (a tuning
+ * kept from another process or run on the same problems): line_variant
+ * per level and axis (0 or a family that cannot take that level's lines:
+ * the default), nu1/nu2 when their sum is positive.  The tables are built
+ * first if needed; the captured graphs are dropped. */
+fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t);
+fg_status fg_case_set_tuning(fg_case *c, const fg_tuning *t);
 
 /* ----- serving: a stream of solve requests over many cases (no reference
  * counterpart: the reference runs one case per process and calls

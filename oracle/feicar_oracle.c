@@ -2218,6 +2218,50 @@ int or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v
 #undef BCYV
 #undef BCZW
 
+/* CORE_FRAC_STEP_ROUTINES.F90:212-299 update_pressure for one rank
+ * (jProc = kProc = 0 = nProcY-1 = nProcZ-1): p' = 0 on the solid cells
+ * that are not dead-marked -1 (k, j from 0 to n+1, i from 0 to nx), p' = 0
+ * on the domain edge lines of its twelve assignments, then p = p'.  The
+ * assignment !07 names plane k = zc_start-2 = -1, outside the array
+ * (lower bound 0); its plane 0 part is kept, the rest is not restated. */
+int or_update_pressure(or_case *c, double *pp, double *p) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  for (int k = 0; k <= nz + 1; ++k)
+    for (int j = 0; j <= ny + 1; ++j)
+      for (int i = 0; i <= nx; ++i) {
+        const long id = IDX(c, i, j, k);
+        if (c->iblank[id] == 0 || c->dead[id] == -1) continue;
+        pp[id] = 0.0;
+      }
+  /* !01-!04: i = 0..nx on the lines j = 0 and j = ny, planes 0 and nz..nz+1 */
+  for (int jj = 0; jj < 2; ++jj) {
+    const int j = jj ? ny : 0;
+    for (int i = 0; i <= nx; ++i) {
+      pp[IDX(c, i, j, 0)] = 0.0;
+      pp[IDX(c, i, j, nz)] = 0.0;
+      pp[IDX(c, i, j, nz + 1)] = 0.0;
+    }
+  }
+  /* !05-!08: i = 0 and nx, j = 0..ny+1, planes 0 and nz..nz+1 */
+  for (int ii = 0; ii < 2; ++ii) {
+    const int i = ii ? nx : 0;
+    for (int j = 0; j <= ny + 1; ++j) {
+      pp[IDX(c, i, j, 0)] = 0.0;
+      pp[IDX(c, i, j, nz)] = 0.0;
+      pp[IDX(c, i, j, nz + 1)] = 0.0;
+    }
+  }
+  /* !09-!12: the four lines along k at (i, j) in {0, nx} x {0, ny} */
+  for (int k = 0; k <= nz + 1; ++k) {
+    pp[IDX(c, 0, 0, k)] = 0.0;
+    pp[IDX(c, nx, 0, k)] = 0.0;
+    pp[IDX(c, 0, ny, k)] = 0.0;
+    pp[IDX(c, nx, ny, k)] = 0.0;
+  }
+  if (p) memcpy(p, pp, sizeof(double) * (size_t)c->NX * c->NY * c->NZ);
+  return OR_OK;
+}
+
 /* CORE_POISSON.F90:205-456 itsolv (LSOR: x lexicographic, y zebra, z) on
  * the fine grid with the iblank/ghost flag */
 static void itsolv_lsor(or_case *c, double *var, const double *r, const or_params *prm) {

@@ -129,6 +129,7 @@ int  or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu
                     double *bczw, const int *vzg, double dt, double *div, double *sumd, double *resdiv);
 int  or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v, double *w,
                     double *dpdx, double *dpdy, double *dpdz);
+int  or_update_pressure(or_case *c, double *pp, double *p);
 int  or_get_ghosts(const or_case *c, int32_t *ijk, int32_t *cell,
                    double *coeffN, double *coeffD, double *bi, double *ip,
                    double *probeLength, int32_t *closestElem, double *alpha);

@@ -111,6 +111,7 @@ def lib():
         L.or_rhs_poisson.argtypes = [P] + [C.c_void_p] * 7 + [C.c_double, C.c_void_p, C.POINTER(C.c_double),
                                                              C.POINTER(C.c_double)]
         L.or_correct_vel.argtypes = [P, C.c_void_p, C.c_double] + [C.c_void_p] * 6
+        L.or_update_pressure.argtypes = [P, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -287,6 +288,12 @@ class OracleCase:
         g = [np.zeros(self.shape, order="F") for _ in range(3)]
         lib().or_correct_vel(self.h, _ptr(np.asfortranarray(pp)), dt, _ptr(u), _ptr(v), _ptr(w), *[_ptr(a) for a in g])
         return g
+
+    def update_pressure(self, pp):
+        """pp updated in place; returns p (= pp after the update)."""
+        p = np.zeros(self.shape, order="F")
+        lib().or_update_pressure(self.h, _ptr(pp), _ptr(p))
+        return p
 
     def move_body(self, ibody, motion, ntime, time, dt):
         """One prescribed-motion step; motion (RigidMotion) is updated.

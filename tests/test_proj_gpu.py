@@ -156,3 +156,20 @@ def test_time_step_stays_on_device():
         h = _host(d[k])
         assert np.abs(h[m] - a[m]).max() <= 1e-8 * np.abs(a[m]).max()
     c.close()
+
+
+def test_update_pressure_matches_oracle():
+    """update_pressure zeroes p' on the solid cells that are not dead-marked
+    -1 and on the domain edge lines, then copies it to p: bit for bit."""
+    oc, c = _setup()
+    rng = np.random.default_rng(6)
+    pp = np.asfortranarray(rng.standard_normal(GRID.shape))
+    assert (oc.field(2) == -1).any() and (oc.field(0) == 1).any()
+    po = pp.copy(order="F")
+    p_o = oc.update_pressure(po)
+    d_pp = _dev(pp)
+    d_p = torch.full_like(d_pp, 7.0)
+    fg.update_pressure_device(c, d_pp.data_ptr(), d_p.data_ptr())
+    assert np.array_equal(_host(d_pp), po)
+    assert np.array_equal(_host(d_p), p_o)
+    c.close()

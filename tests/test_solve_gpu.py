@@ -367,3 +367,61 @@ def test_autotuned_batch_reaches_each_solution(prec):
     bt.close()
     for c in cases:
         c.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+@pytest.mark.parametrize("fam", [(1, 1), (2, 2), (3, 3), (3, 4), (3, 5), (1, 4), (2, 5), (3, 6), (1, 6)])
+def test_every_line_family_reaches_the_solution(prec, fam):
+    """Each line-kernel family the autotuner may pick, forced on every
+    level (a family that cannot take a level's lines falls back to the
+    default there), solves to the exact discrete solution: the families
+    differ only in how a line's tridiagonal system is split over threads."""
+    grid = synth.small_grid(128, 96, 80, (4.0, 3.0, 2.5), stretch=1.5)
+    body = synth.sphere_body((1.7, 1.4, 1.2), 0.9, 3)
+    _, ib, rhs, phi = _problem(grid, [body], seed=11)
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    c = fg.Case(grid, fg.default_config(precision=p_, rtol=1e-12, max_cycles=150))
+    c.add_body(body)
+    c.set_iblank_body_fast()
+    c.gcm_set_internal_boundary()
+    c.mg_prepare()
+    fg.case_set_tuning(c, {"x": fam[0], "y": fam[1], "z": fam[1]}, nu=(2, 1))
+    d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device="cuda")
+    d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda()
+    st = c.solve_poisson_device(d_p.data_ptr(), d_f.data_ptr())
+    assert st["relres"] <= 1e-12
+    assert _relerr(d_p.cpu().numpy().transpose(2, 1, 0), phi, _fluid(grid, ib)) <= TOL
+    c.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_both_colour_sweep_equals_two_launches(prec):
+    """The both-colour y/z sweep (one launch, plane-ordered tickets) runs
+    the tile of the two colour launches of the block-PCR family on the same
+    values (its colour-1 tiles read x from L2, where the colour-0 tiles of
+    the launch left it), so whole solves take the same cycles and agree to
+    rounding: the two kernels are compiled separately, and the compiler may
+    contract a multiply-add in one and not in the other."""
+    grid = synth.small_grid(96, 80, 72, (4.0, 3.0, 2.5), stretch=1.5)
+    body = synth.sphere_body((1.7, 1.4, 1.2), 0.9, 3)
+    _, ib, rhs, phi = _problem(grid, [body], seed=12)
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    c = fg.Case(grid, fg.default_config(precision=p_, rtol=1e-12, max_cycles=150))
+    c.add_body(body)
+    c.set_iblank_body_fast()
+    c.gcm_set_internal_boundary()
+    c.mg_prepare()
+    d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda()
+    out = []
+    for fam in (2, 6, 2):
+        fg.case_set_tuning(c, {"x": 3, "y": fam, "z": fam}, nu=(2, 1))
+        d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device="cuda")
+        st = c.solve_poisson_device(d_p.data_ptr(), d_f.data_ptr())
+        out.append((d_p.cpu().numpy(), st["cycles"]))
+    assert out[0][1] == out[1][1] == out[2][1]
+    assert np.array_equal(out[0][0], out[2][0])  # the solve itself is deterministic
+    # the all-Neumann solution is fixed up to a constant: compare without it
+    a, b = out[0][0] - out[0][0].mean(), out[1][0] - out[1][0].mean()
+    assert np.abs(a - b).max() <= 1e-11 * np.abs(a).max()
+    assert _relerr(out[1][0].transpose(2, 1, 0), phi, _fluid(grid, ib)) <= TOL
+    c.close()
