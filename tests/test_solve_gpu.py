@@ -401,7 +401,10 @@ def test_both_colour_sweep_equals_two_launches(prec):
     values (its colour-1 tiles read x from L2, where the colour-0 tiles of
     the launch left it), so whole solves take the same cycles and agree to
     rounding: the two kernels are compiled separately, and the compiler may
-    contract a multiply-add in one and not in the other."""
+    contract a multiply-add in one and not in the other.  In FP64 the two
+    solutions agree to 1e-11; the FP32 V-cycles of the mixed path carry
+    that rounding into the Krylov iterates, so there the two converged
+    solutions agree to the solve's own accuracy (1e-9)."""
     grid = synth.small_grid(96, 80, 72, (4.0, 3.0, 2.5), stretch=1.5)
     body = synth.sphere_body((1.7, 1.4, 1.2), 0.9, 3)
     _, ib, rhs, phi = _problem(grid, [body], seed=12)
@@ -422,6 +425,6 @@ def test_both_colour_sweep_equals_two_launches(prec):
     assert np.array_equal(out[0][0], out[2][0])  # the solve itself is deterministic
     # the all-Neumann solution is fixed up to a constant: compare without it
     a, b = out[0][0] - out[0][0].mean(), out[1][0] - out[1][0].mean()
-    assert np.abs(a - b).max() <= 1e-11 * np.abs(a).max()
+    assert np.abs(a - b).max() <= (1e-9 if prec == "mixed" else 1e-11) * np.abs(a).max()
     assert _relerr(out[1][0].transpose(2, 1, 0), phi, _fluid(grid, ib)) <= TOL
     c.close()
