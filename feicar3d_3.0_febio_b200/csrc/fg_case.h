@@ -103,6 +103,7 @@ struct fg_case {
   long long geom_version = 0;      // bumped by every prepare
   // per interpolation row, for row constants formed on the device: the
   // dp/dn index, its two factors, the fallback corners and weights
+  double *d_admet = nullptr;          // momentum sweeps: metrics and set_solve_ad coefficients
   void *d_rcg = nullptr;
   long long rcg_version = -1;
   int rcg_n = 0;

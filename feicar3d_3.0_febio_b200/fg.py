@@ -748,6 +748,38 @@ def update_pressure_device(case, d_pprime: int, d_p: int | None = None):
            "fg_update_pressure_device")
 
 
+class AdParams(C.Structure):
+    """fg_ad_params: the momentum sweeps' time step, viscosity (1/Re),
+    relaxation and whether convection is implicit (Crank-Nicolson)."""
+    _fields_ = [("dt", C.c_double), ("reinv", C.c_double), ("omega_ad", C.c_double), ("crank_nicolson", C.c_int)]
+
+
+def _ad_lib():
+    L = lib()
+    if not getattr(L, "_ad_ready", False):
+        vp = C.c_void_p
+        L.fg_itsolv_ad_device.argtypes = [vp] * 6 + [C.POINTER(AdParams)]
+        L.fg_calc_residual_ad_device.argtypes = [vp] * 6 + [C.POINTER(AdParams), C.POINTER(C.c_double), vp]
+        L.fg_itsolv_ad_device.restype = C.c_int
+        L.fg_calc_residual_ad_device.restype = C.c_int
+        L._ad_ready = True
+    return L
+
+
+def itsolv_ad_device(case, var, r, fu, fv, fw, prm: AdParams):
+    """One pass of the momentum line SOR on device fields (pointers)."""
+    _check(_ad_lib().fg_itsolv_ad_device(case.h, *[C.c_void_p(x) for x in (var, r, fu, fv, fw)], C.byref(prm)),
+           "fg_itsolv_ad_device")
+
+
+def calc_residual_ad_device(case, var, r, fu, fv, fw, prm: AdParams):
+    m = C.c_double(0.0)
+    loc = np.zeros(3, np.int32)
+    _check(_ad_lib().fg_calc_residual_ad_device(case.h, *[C.c_void_p(x) for x in (var, r, fu, fv, fw)],
+                                                C.byref(prm), C.byref(m), _p(loc)), "fg_calc_residual_ad_device")
+    return m.value, tuple(int(x) for x in loc)
+
+
 def correct_vel_device(case, pp, dt, u=None, v=None, w=None, dpdx=None, dpdy=None, dpdz=None):
     _check(_proj_lib().fg_correct_vel_device(case.h, _dp(pp), dt, *[_dp(x) for x in (u, v, w, dpdx, dpdy, dpdz)]),
            "fg_correct_vel_device")

@@ -253,6 +253,30 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
  * itself); either triple may be NULL. */
 fg_status fg_correct_vel_device(fg_case *c, const double *pPrime, double dt, double *u, double *v, double *w,
                                 double *dpdx, double *dpdy, double *dpdz);
+/* The momentum equation's line SOR on device fields (one rank):
+ * set_solve_ad's diffusion coefficients with viscosity reinv
+ * (CORE_SET_SOLVERS.F90:591-677), then one pass of itsolv_ad
+ * (CORE_SOLVE_AD.F90:131-776): x, y and z line sweeps of one velocity
+ * component var with right-hand side r, the implicit convection terms
+ * from face_u/v/w when crank_nicolson (advec_scheme == CRANK_NICOLSON2;
+ * central for 25 <= i <= 375, first-order upwind elsewhere, as the
+ * reference), relaxation omega_ad.  The lines of each direction are
+ * solved one anti-diagonal at a time, which gives the reference's
+ * lexicographic Gauss-Seidel sweep bit for bit.  The ghost-cell
+ * coefficients the z sweep stores (ghostNScoeff) are not kept: the
+ * velocity ghost-cell update stays with the caller. */
+typedef struct fg_ad_params {
+  double dt, reinv, omega_ad;
+  int crank_nicolson;
+} fg_ad_params;
+fg_status fg_itsolv_ad_device(fg_case *c, double *var, const double *r, const double *face_u,
+                              const double *face_v, const double *face_w, const fg_ad_params *prm);
+/* calc_residual_ad (CORE_SOLVE_AD.F90:780-964): max |res| over the fluid
+ * non-ghost cells and its first location (i, j, k) in the reference's
+ * loop order ((1,1,1) when every residual is 0). */
+fg_status fg_calc_residual_ad_device(fg_case *c, const double *var, const double *r, const double *face_u,
+                                     const double *face_v, const double *face_w, const fg_ad_params *prm,
+                                     double *resm, int *loc);
 /* update_pressure (CORE_FRAC_STEP_ROUTINES.F90:212-299) for one rank:
  * pPrime = 0 on the solid cells (iblank) not dead-marked -1, for
  * i = 0..nx, j = 0..ny+1, k = 0..nz+1, and on the domain edge lines the

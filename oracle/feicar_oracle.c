@@ -2262,6 +2262,215 @@ int or_update_pressure(or_case *c, double *pp, double *p) {
   return OR_OK;
 }
 
+/* ---------------------------------------------- momentum line SOR
+ * CORE_SET_SOLVERS.F90:591-677 set_solve_ad (diffusion coefficients with
+ * nu = reinv), CORE_SOLVE_AD.F90:162-776 itsolv_ad_x/y/z (one Gauss-Seidel
+ * line sweep per direction, lexicographic, with the implicit convection
+ * terms: central for 25 <= i <= 375, first-order upwind elsewhere) and
+ * :780-964 calc_residual_ad, for one rank. */
+typedef struct {
+  double amx, apx, acx, amy, apy, acy, amz, apz, acz;
+} ad_coef;
+
+static double fsign1(double x) { return copysign(1.0, x); }
+
+/* the coefficients of cell (i,j,k) as each sweep forms them (:215-330) */
+static void ad_cell(const or_case *c, const double *ad, const double *fu, const double *fv, const double *fw,
+                    double half_dt, int i, int j, int k, ad_coef *q) {
+  const int nx = c->nx, ny = c->ny;
+  const double *amx_ad = ad, *apx_ad = ad + (nx + 2), *amy_ad = ad + 2 * (nx + 2),
+               *apy_ad = ad + 2 * (nx + 2) + (ny + 2), *amz_ad = ad + 2 * (nx + 2) + 2 * (ny + 2),
+               *apz_ad = amz_ad + (c->nz + 2);
+  const long id = IDX(c, i, j, k);
+  const long ip = IDX(c, i + 1, j, k), jp = IDX(c, i, j + 1, k), kp = IDX(c, i, j, k + 1);
+  const int central = (i >= 25) && (i <= 375);
+  double hyb1, hyb2, tmp1, tmp2;
+  q->amx = amx_ad[i]; q->apx = apx_ad[i]; q->acx = -(q->amx + q->apx);
+  q->amy = amy_ad[j]; q->apy = apy_ad[j]; q->acy = -(q->amy + q->apy);
+  q->amz = amz_ad[k]; q->apz = apz_ad[k]; q->acz = -(q->amz + q->apz);
+  /* x */
+  hyb1 = 0.5 * (1.0 + fsign1(fu[id])); hyb2 = 0.5 * (1.0 - fsign1(fu[ip]));
+  tmp1 = 1.0 - fint(c->x, c->xc, i); tmp2 = fint(c->x, c->xc, i + 1);
+  if (central) {
+    q->amx = q->amx - half_dt * fu[id] * tmp1 * c->dxinv[i];
+    q->apx = q->apx + half_dt * fu[ip] * tmp2 * c->dxinv[i];
+  } else {
+    q->amx = q->amx - half_dt * hyb1 * fu[id] * c->dxinv[i];
+    q->apx = q->apx + half_dt * hyb2 * fu[ip] * c->dxinv[i];
+  }
+  hyb1 = 0.5 * (1.0 - fsign1(fu[id])); hyb2 = 0.5 * (1.0 + fsign1(fu[ip]));
+  tmp1 = fint(c->x, c->xc, i); tmp2 = 1.0 - fint(c->x, c->xc, i + 1);
+  if (central) q->acx = q->acx + half_dt * (fu[ip] * tmp2 - fu[id] * tmp1) * c->dxinv[i];
+  else q->acx = q->acx + half_dt * (fu[ip] * hyb2 - fu[id] * hyb1) * c->dxinv[i];
+  /* y */
+  hyb1 = 0.5 * (1.0 + fsign1(fv[id])); hyb2 = 0.5 * (1.0 - fsign1(fv[jp]));
+  tmp1 = 1.0 - fint(c->y, c->yc, j); tmp2 = fint(c->y, c->yc, j + 1);
+  if (central) {
+    q->amy = q->amy - half_dt * fv[id] * tmp1 * c->dyinv[j];
+    q->apy = q->apy + half_dt * fv[jp] * tmp2 * c->dyinv[j];
+  } else {
+    q->amy = q->amy - half_dt * hyb1 * fv[id] * c->dyinv[j];
+    q->apy = q->apy + half_dt * hyb2 * fv[jp] * c->dyinv[j];
+  }
+  hyb1 = 0.5 * (1.0 - fsign1(fv[id])); hyb2 = 0.5 * (1.0 + fsign1(fv[jp]));
+  tmp1 = fint(c->y, c->yc, j); tmp2 = 1.0 - fint(c->y, c->yc, j + 1);
+  if (central) q->acy = q->acy + half_dt * (fv[jp] * tmp2 - fv[id] * tmp1) * c->dyinv[j];
+  else q->acy = q->acy + half_dt * (fv[jp] * hyb2 - fv[id] * hyb1) * c->dyinv[j];
+  /* z */
+  hyb1 = 0.5 * (1.0 + fsign1(fw[id])); hyb2 = 0.5 * (1.0 - fsign1(fw[kp]));
+  tmp1 = 1.0 - fint(c->z, c->zc, k); tmp2 = fint(c->z, c->zc, k + 1);
+  if (central) {
+    q->amz = q->amz - half_dt * fw[id] * tmp1 * c->dzinv[k];
+    q->apz = q->apz + half_dt * fw[kp] * tmp2 * c->dzinv[k];
+  } else {
+    q->amz = q->amz - half_dt * hyb1 * fw[id] * c->dzinv[k];
+    q->apz = q->apz + half_dt * hyb2 * fw[kp] * c->dzinv[k];
+  }
+  hyb1 = 0.5 * (1.0 - fsign1(fw[id])); hyb2 = 0.5 * (1.0 + fsign1(fw[kp]));
+  tmp1 = fint(c->z, c->zc, k); tmp2 = 1.0 - fint(c->z, c->zc, k + 1);
+  if (central) q->acz = q->acz + half_dt * (fw[kp] * tmp2 - fw[id] * tmp1) * c->dzinv[k];
+  else q->acz = q->acz + half_dt * (fw[kp] * hyb2 - fw[id] * hyb1) * c->dzinv[k];
+}
+
+/* CORE_TDMA.F90:11-34 on a[n1..n2] (gam in g, result in u) */
+static void tdma_ad(const double *a, const double *b, const double *cc, const double *r, double *u, double *g, int n1,
+                    int n2) {
+  double binv = 1.0 / b[n1];
+  u[n1] = r[n1] * binv;
+  for (int j = n1 + 1; j <= n2; ++j) {
+    g[j] = cc[j - 1] * binv;
+    binv = 1.0 / (b[j] - a[j] * g[j]);
+    u[j] = (r[j] - a[j] * u[j - 1]) * binv;
+  }
+  for (int j = n2 - 1; j >= n1; --j) u[j] = u[j] - g[j + 1] * u[j + 1];
+}
+
+int or_set_solve_ad(or_case *c, double dt, double reinv, double *ad) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  double *amx = ad, *apx = ad + (nx + 2), *amy = ad + 2 * (nx + 2), *apy = amy + (ny + 2),
+         *amz = apy + (ny + 2), *apz = amz + (nz + 2);
+  memset(ad, 0, sizeof(double) * (size_t)(2 * (nx + 2) + 2 * (ny + 2) + 2 * (nz + 2)));
+  for (int i = 1; i <= nx - 1; ++i) {
+    amx[i] = (c->dxcinv[i]) * c->dxinv[i];
+    apx[i] = (c->dxcinv[i + 1]) * c->dxinv[i];
+    amx[i] = -(0.50 * dt * reinv) * amx[i];
+    apx[i] = -(0.50 * dt * reinv) * apx[i];
+  }
+  for (int j = 1; j <= ny - 1; ++j) {
+    amy[j] = c->dycinv[j] * c->dyinv[j];
+    apy[j] = c->dycinv[j + 1] * c->dyinv[j];
+    amy[j] = -(0.50 * dt * reinv) * amy[j];
+    apy[j] = -(0.50 * dt * reinv) * apy[j];
+  }
+  for (int k = 1; k <= nz - 1; ++k) {
+    amz[k] = c->dzcinv[k] * c->dzinv[k];
+    apz[k] = c->dzcinv[k + 1] * c->dzinv[k];
+    amz[k] = -(0.50 * dt * reinv) * amz[k];
+    apz[k] = -(0.50 * dt * reinv) * apz[k];
+  }
+  return OR_OK;
+}
+
+int or_itsolv_ad(or_case *c, const double *ad, double *var, const double *r, const double *fu, const double *fv,
+                 const double *fw, double half_dt, double omega_ad) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  const int nmax = (nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz)) + 2;
+  double *am = dzalloc(nmax), *ac = dzalloc(nmax), *ap = dzalloc(nmax), *rh = dzalloc(nmax), *u = dzalloc(nmax),
+         *g = dzalloc(nmax);
+  ad_coef q;
+  /* x lines (CORE_SOLVE_AD.F90:162-349): k, then j */
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j) {
+      for (int i = 1; i <= nx - 1; ++i) {
+        const long id = IDX(c, i, j, k);
+        ad_cell(c, ad, fu, fv, fw, half_dt, i, j, k, &q);
+        rh[i] = r[id] - (var[IDX(c, i, j - 1, k)] * q.amy + var[IDX(c, i, j + 1, k)] * q.apy +
+                         var[IDX(c, i, j, k - 1)] * q.amz + var[IDX(c, i, j, k + 1)] * q.apz);
+        const double rib = (1.0 - (double)c->iblank[id]) * (1.0 - (double)abs(c->ghost[id]));
+        am[i] = q.amx * rib;
+        ap[i] = q.apx * rib;
+        ac[i] = 1.0 + (q.acx + q.acy + q.acz) * rib;
+        rh[i] = rh[i] * rib + var[id] * (1.0 - rib);
+      }
+      am[0] = 0.0; ap[0] = 0.0; ac[0] = 1.0; rh[0] = var[IDX(c, 0, j, k)];
+      am[nx] = 0.0; ap[nx] = 0.0; ac[nx] = 1.0; rh[nx] = var[IDX(c, nx, j, k)];
+      tdma_ad(am, ac, ap, rh, u, g, 0, nx);
+      for (int i = 1; i <= nx - 1; ++i) {
+        const long id = IDX(c, i, j, k);
+        var[id] = var[id] + omega_ad * (u[i] - var[id]);
+      }
+    }
+  /* y lines (:353-549): k, then i */
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int i = 1; i <= nx - 1; ++i) {
+      for (int j = 1; j <= ny - 1; ++j) {
+        const long id = IDX(c, i, j, k);
+        ad_cell(c, ad, fu, fv, fw, half_dt, i, j, k, &q);
+        rh[j] = r[id] - (var[IDX(c, i - 1, j, k)] * q.amx + var[IDX(c, i + 1, j, k)] * q.apx +
+                         var[IDX(c, i, j, k - 1)] * q.amz + var[IDX(c, i, j, k + 1)] * q.apz);
+        const double rib = (1.0 - (double)c->iblank[id]) * (1.0 - (double)abs(c->ghost[id]));
+        am[j] = q.amy * rib;
+        ap[j] = q.apy * rib;
+        ac[j] = 1.0 + (q.acx + q.acy + q.acz) * rib;
+        rh[j] = rh[j] * rib + var[id] * (1.0 - rib);
+      }
+      am[0] = 0.0; ap[0] = 0.0; ac[0] = 1.0; rh[0] = var[IDX(c, i, 0, k)];
+      am[ny] = 0.0; ap[ny] = 0.0; ac[ny] = 1.0; rh[ny] = var[IDX(c, i, ny, k)];
+      tdma_ad(am, ac, ap, rh, u, g, 0, ny);
+      for (int j = 1; j <= ny - 1; ++j) {
+        const long id = IDX(c, i, j, k);
+        var[id] = var[id] + omega_ad * (u[j] - var[id]);
+      }
+    }
+  /* z lines (:553-776): j, then i */
+  for (int j = 1; j <= ny - 1; ++j)
+    for (int i = 1; i <= nx - 1; ++i) {
+      for (int k = 1; k <= nz - 1; ++k) {
+        const long id = IDX(c, i, j, k);
+        ad_cell(c, ad, fu, fv, fw, half_dt, i, j, k, &q);
+        rh[k] = r[id] - (var[IDX(c, i - 1, j, k)] * q.amx + var[IDX(c, i + 1, j, k)] * q.apx +
+                         var[IDX(c, i, j - 1, k)] * q.amy + var[IDX(c, i, j + 1, k)] * q.apy);
+        const double rib = (1.0 - (double)c->iblank[id]) * (1.0 - (double)abs(c->ghost[id]));
+        am[k] = q.amz * rib;
+        ap[k] = q.apz * rib;
+        ac[k] = 1.0 + (q.acx + q.acy + q.acz) * rib;
+        rh[k] = rh[k] * rib + var[id] * (1.0 - rib);
+      }
+      am[0] = 0.0; ap[0] = 0.0; ac[0] = 1.0; rh[0] = var[IDX(c, i, j, 0)];
+      am[nz] = 0.0; ap[nz] = 0.0; ac[nz] = 1.0; rh[nz] = var[IDX(c, i, j, nz)];
+      tdma_ad(am, ac, ap, rh, u, g, 0, nz);
+      for (int k = 1; k <= nz - 1; ++k) {
+        const long id = IDX(c, i, j, k);
+        var[id] = var[id] + omega_ad * (u[k] - var[id]);
+      }
+    }
+  free(am); free(ac); free(ap); free(rh); free(u); free(g);
+  return OR_OK;
+}
+
+int or_calc_residual_ad(or_case *c, const double *ad, const double *var, const double *r, const double *fu,
+                        const double *fv, const double *fw, double half_dt, double *resm, int *loc) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  ad_coef q;
+  double m = 0.0;
+  int li = 1, lj = 1, lk = 1;
+  for (int k = 1; k <= nz - 1; ++k)
+    for (int j = 1; j <= ny - 1; ++j)
+      for (int i = 1; i <= nx - 1; ++i) {
+        const long id = IDX(c, i, j, k);
+        ad_cell(c, ad, fu, fv, fw, half_dt, i, j, k, &q);
+        double res = r[id] - var[id] * (1.0 + q.acx + q.acy + q.acz) - var[IDX(c, i - 1, j, k)] * q.amx -
+                     var[IDX(c, i + 1, j, k)] * q.apx - var[IDX(c, i, j - 1, k)] * q.amy -
+                     var[IDX(c, i, j + 1, k)] * q.apy - var[IDX(c, i, j, k - 1)] * q.amz -
+                     var[IDX(c, i, j, k + 1)] * q.apz;
+        res = res * (1.0 - (double)c->iblank[id]) * (1.0 - (double)c->ghost[id]);
+        if (fabs(res) > m) { m = fabs(res); li = i; lj = j; lk = k; }
+      }
+  if (resm) *resm = m;
+  if (loc) { loc[0] = li; loc[1] = lj; loc[2] = lk; }
+  return OR_OK;
+}
+
 /* CORE_POISSON.F90:205-456 itsolv (LSOR: x lexicographic, y zebra, z) on
  * the fine grid with the iblank/ghost flag */
 static void itsolv_lsor(or_case *c, double *var, const double *r, const or_params *prm) {

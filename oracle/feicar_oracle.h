@@ -130,6 +130,14 @@ int  or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu
 int  or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v, double *w,
                     double *dpdx, double *dpdy, double *dpdz);
 int  or_update_pressure(or_case *c, double *pp, double *p);
+/* momentum line SOR (CORE_SET_SOLVERS.F90:591-677, CORE_SOLVE_AD.F90):
+ * ad holds amx_ad, apx_ad (nx+2 each), amy_ad, apy_ad (ny+2), amz_ad,
+ * apz_ad (nz+2) */
+int  or_set_solve_ad(or_case *c, double dt, double reinv, double *ad);
+int  or_itsolv_ad(or_case *c, const double *ad, double *var, const double *r, const double *fu,
+                  const double *fv, const double *fw, double half_dt, double omega_ad);
+int  or_calc_residual_ad(or_case *c, const double *ad, const double *var, const double *r, const double *fu,
+                         const double *fv, const double *fw, double half_dt, double *resm, int *loc);
 int  or_get_ghosts(const or_case *c, int32_t *ijk, int32_t *cell,
                    double *coeffN, double *coeffD, double *bi, double *ip,
                    double *probeLength, int32_t *closestElem, double *alpha);

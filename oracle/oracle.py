@@ -112,6 +112,9 @@ def lib():
                                                              C.POINTER(C.c_double)]
         L.or_correct_vel.argtypes = [P, C.c_void_p, C.c_double] + [C.c_void_p] * 6
         L.or_update_pressure.argtypes = [P, C.c_void_p, C.c_void_p]
+        L.or_set_solve_ad.argtypes = [P, C.c_double, C.c_double, C.c_void_p]
+        L.or_itsolv_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_double]
+        L.or_calc_residual_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -294,6 +297,26 @@ class OracleCase:
         p = np.zeros(self.shape, order="F")
         lib().or_update_pressure(self.h, _ptr(pp), _ptr(p))
         return p
+
+    # momentum line SOR (CORE_SET_SOLVERS.F90 set_solve_ad, CORE_SOLVE_AD.F90)
+    def set_solve_ad(self, dt, reinv):
+        g = self.grid
+        ad = np.zeros(2 * (g.nx + 2) + 2 * (g.ny + 2) + 2 * (g.nz + 2))
+        lib().or_set_solve_ad(self.h, dt, reinv, _ptr(ad))
+        return ad
+
+    def itsolv_ad(self, ad, var, r, fu, fv, fw, half_dt, omega_ad):
+        """One x/y/z line-sweep pass; var (Fortran-ordered) updated in place."""
+        assert var.flags.f_contiguous
+        lib().or_itsolv_ad(self.h, _ptr(ad), _ptr(var), *[_ptr(np.asfortranarray(a)) for a in (r, fu, fv, fw)],
+                           half_dt, omega_ad)
+
+    def calc_residual_ad(self, ad, var, r, fu, fv, fw, half_dt):
+        m = C.c_double(0.0)
+        loc = np.zeros(3, np.int32)
+        lib().or_calc_residual_ad(self.h, _ptr(ad), *[_ptr(np.asfortranarray(a)) for a in (var, r, fu, fv, fw)],
+                                  half_dt, C.byref(m), _ptr(loc))
+        return m.value, tuple(int(x) for x in loc)
 
     def move_body(self, ibody, motion, ntime, time, dt):
         """One prescribed-motion step; motion (RigidMotion) is updated.

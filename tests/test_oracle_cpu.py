@@ -187,3 +187,46 @@ def test_slab_parallel_sweeps_reach_same_solution():
     finally:
         O.set_threads(1)
     assert np.linalg.norm(sols[0] - sols[1]) / np.linalg.norm(e) < 1e-9
+
+
+def test_oracle_momentum_sweep_reaches_a_manufactured_solution():
+    """With no convection (crank_nicolson off) the momentum system is
+    (I - dt/2 nu L) v = r on the fluid cells (set_solve_ad's coefficients,
+    CORE_SET_SOLVERS.F90:650-675) with v held on solid and ghost cells and
+    on the boundary layers.  r is formed from a known v by that operator,
+    so the line sweeps must return v."""
+    grid = synth.small_grid(24, 16, 12, (3.0, 2.0, 1.5), stretch=1.5)
+    oc = O.OracleCase(grid)
+    oc.add_body(synth.sphere_body((1.5, 1.0, 0.75), 0.6, 2))
+    oc.set_iblank()
+    oc.gcm(2.0, 2.0)
+    dt, reinv = 0.2, 1.0 / 10.0
+    ad = oc.set_solve_ad(dt, reinv)
+    rng = np.random.default_rng(3)
+    vex = np.asfortranarray(rng.standard_normal(grid.shape))
+    zero = np.zeros(grid.shape, order="F")
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    I, J, K = nx + 2, ny + 2, nz + 2
+    amx, apx = ad[0:I], ad[I:2 * I]
+    amy, apy = ad[2 * I:2 * I + J], ad[2 * I + J:2 * I + 2 * J]
+    amz, apz = ad[2 * I + 2 * J:2 * I + 2 * J + K], ad[2 * I + 2 * J + K:]
+    # r = A vex on the fluid cells, cell by cell from the coefficients
+    r = np.zeros(grid.shape, order="F")
+    ib, gh = oc.field(0), oc.field(1)
+    for k in range(1, nz):
+        for j in range(1, ny):
+            for i in range(1, nx):
+                ac = 1.0 - (amx[i] + apx[i]) - (amy[j] + apy[j]) - (amz[k] + apz[k])
+                r[i, j, k] = (ac * vex[i, j, k] + amx[i] * vex[i - 1, j, k] + apx[i] * vex[i + 1, j, k]
+                              + amy[j] * vex[i, j - 1, k] + apy[j] * vex[i, j + 1, k]
+                              + amz[k] * vex[i, j, k - 1] + apz[k] * vex[i, j, k + 1])
+    fluid = (ib == 0) & (gh == 0)
+    interior = np.zeros(grid.shape, bool)
+    interior[1:nx, 1:ny, 1:nz] = True
+    var = np.where(fluid & interior, 0.0, vex).copy(order="F")  # held cells start at their values
+    for _ in range(60):
+        oc.itsolv_ad(ad, var, r, zero, zero, zero, 0.0, 1.0)
+    m = fluid & interior
+    assert np.abs(var[m] - vex[m]).max() <= 1e-11
+    res, _ = oc.calc_residual_ad(ad, var, r, zero, zero, zero, 0.0)
+    assert res <= 1e-11
