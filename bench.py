@@ -228,6 +228,19 @@ def run_kernels_only(torch, fg, synth, grid, c, geo, args, dev):
     c.set_stream(stream.cuda_stream)
     d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).to(f"cuda:{dev}")
     d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device=f"cuda:{dev}")
+    tuning = None
+    if args.tuning_json:  # choices measured in an earlier run (a profiler distorts the tuner's timings)
+        with open(args.tuning_json) as f:
+            tuning = json.load(f)
+        names = {nm: v for kind in fg.LINE_FAMILIES.values() for v, nm in kind.items()}
+        fams = {L: {a: names[row[a]["family"]] for a in row} for L, row in enumerate(tuning["levels"])}
+        fg.case_set_tuning(c, fams, nu=(tuning["nu1"], tuning["nu2"]))
+    elif not args.no_autotune:  # the same choices as the headline run
+        with torch.cuda.stream(stream):
+            tuning = fg.case_autotune(c, d_p.data_ptr(), d_f.data_ptr())
+        if args.save_tuning:
+            with open(args.save_tuning, "w") as f:
+                json.dump(tuning, f)
     for _ in range(args.warmup):
         timed_device_solves(torch, fg, c, d_p, d_f, 1, stream)
     tot, per, stats = timed_device_solves(torch, fg, c, d_p, d_f, args.steps, stream)
@@ -239,7 +252,8 @@ def run_kernels_only(torch, fg, synth, grid, c, geo, args, dev):
                       "cycles": stats[-1]["cycles"], "relres": stats[-1]["relres"],
                       "classes_ms": {k: round(v["ms"], 3) for k, v in prof.items()},
                       "classes_gbs": {k: round(v["bytes"] / 1e6 / v["ms"], 1)
-                                      for k, v in prof.items() if v["ms"] > 0 and v["bytes"] > 0}}),
+                                      for k, v in prof.items() if v["ms"] > 0 and v["bytes"] > 0},
+                      "tuning": tuning}),
           flush=True)
     c.close()
 
@@ -913,7 +927,11 @@ def main():
     ap.add_argument("--serve-low-rate", type=float, default=20.0, help="serve: a lower rate")
     ap.add_argument("--serve-low-seconds", type=float, default=5.0)
     ap.add_argument("--serve-slots", type=int, default=16, help="serve: most requests resident at once")
-    ap.add_argument("--no-autotune", action="store_true", help="batch64: default kernel families and V(2,2)")
+    ap.add_argument("--no-autotune", action="store_true", help="default kernel families and V(2,2)")
+    ap.add_argument("--save-tuning", default=None, help="--kernels-only: write the measured tuning to this file")
+    ap.add_argument("--tuning-json", default=None,
+                    help="--kernels-only: apply this tuning (the 'tuning' object of an earlier line) instead of "
+                         "measuring one")
     ap.add_argument("--kernels-only", action="store_true",
                     help="one case, timed solves only (for kernel profiling)")
     args = ap.parse_args()

@@ -365,6 +365,16 @@ static fg_status upload_axes(fg_case *c, int l) {
   const long long nt = L.ntot, ax[3] = {L.nx + 2, L.ny + 2, L.nz + 2};
   d.type = mkptr<const int8_t>(L.d_type, nt, K_TYPE);
   d.mask = mkptr<const uint8_t>(L.d_mask, nt, K_MASK);
+  {
+    const long long ntx = (L.nx + 15) / 16, ny_ = ntx * L.nz, nz_ = ntx * L.ny;
+    void *raw = nullptr;
+    FG_CUDA(fg::dev_alloc(&raw, (size_t)(ny_ + nz_ + 1)));
+    L.raw.push_back(raw);
+    FG_CUDA(cudaMemset(raw, 0, (size_t)(ny_ + nz_ + 1)));  // no tile regular until the masks are built
+    L.d_reg = static_cast<uint8_t *>(raw);
+    d.regy = mkptr<const uint8_t>(L.d_reg, ny_, K_MASK);
+    d.regz = mkptr<const uint8_t>(L.d_reg + ny_, nz_, K_MASK);
+  }
   const double *cf = L.d_coef;
   const int *ci = L.d_int;
   d.amx = mkptr(cf + doff[0][0], ax[0], K_AXIS); d.apx = mkptr(cf + doff[0][1], ax[0], K_AXIS);
@@ -1975,6 +1985,11 @@ static fg_status build_levels(fg_case *c) {
   for (int l = 0; l < c->nlev; ++l)
     prep::k_mask<<<prep::cell_blocks(c->lev[l]), 256, 0, s>>>(prep::lv(c->lev[l]));
   FG_CUDA(cudaGetLastError());
+  for (int l = 0; l < c->nlev; ++l) {
+    HLevel &L = c->lev[l];
+    const long long ntx = (L.nx + 15) / 16;
+    FG_K(k::reg_tiles(L.dl, L.d_reg, L.d_reg + ntx * L.nz, s));
+  }
   HLevel &Lc = c->lev[c->nlev - 1];
   Lc.type.resize(Lc.ntot);
   FG_CUDA(cudaMemcpyAsync(Lc.type.data(), Lc.d_type, Lc.ntot, cudaMemcpyDeviceToHost, s));
@@ -2717,6 +2732,11 @@ fg_status fg_batch_create(int device, const fg_solver_config *cfg, fg_batch **ou
   auto *b = new fg_batch();
   b->device = device;
   if (cfg) b->cfg = *cfg; else fg_default_config(&b->cfg);
+  // FEICAR_B200_SOLVE_GRAPH=0: the solve's kernels go out one by one from
+  // the host (same kernels, same results), for kernel profilers that follow
+  // individual launches rather than graphs with conditional nodes
+  const char *g = getenv("FEICAR_B200_SOLVE_GRAPH");
+  if (g && g[0] == '0') b->sg.off = true;
   *out = b;
   return FG_OK;
 }

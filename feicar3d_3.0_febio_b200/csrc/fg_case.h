@@ -26,6 +26,7 @@ struct HLevel {
   // device
   int8_t *d_type = nullptr;
   uint8_t *d_mask = nullptr;
+  uint8_t *d_reg = nullptr;     // regular-tile flags of the y then the z line tiles
   int8_t *d_ibk = nullptr;      // solid flag (interior cells)
   double *d_nodes = nullptr;    // x, y, z node arrays back to back
   double *d_coef = nullptr;  // packed 1-D double arrays

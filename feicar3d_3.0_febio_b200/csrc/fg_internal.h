@@ -104,6 +104,10 @@ struct DevLevel {
   // cell and the weight of the upper one, per fine cell (1..n)
   dptr<const int> plx, ply, plz;
   dptr<const double> pwx, pwy, pwz;
+  // y/z line tiles (16 cells of i, one plane) whose inner rows are all
+  // active with every face coupled: flag[ti + ntx (plane - 1)], ntx =
+  // ceil(nx / 16); such tiles skip the mask decode
+  dptr<const uint8_t> regy, regz;
   int bc[6];             // 0 Neumann (face dropped), 1 Dirichlet
   // value arrays (only those of the level's precision are set)
   dptr<double> x64, rhs64, res64;
@@ -323,6 +327,8 @@ struct RowConstGeo {
 };
 cudaError_t row_constants_device(int n, RowConstGeo g, const double *p_old, const double *dpdn_g,
                                  const double *dpdn_d, int nd, double *c0, cudaStream_t s);
+// the regular-tile flags of a level (DevLevel::regy, regz) from its masks
+cudaError_t reg_tiles(const DevLevel &L, uint8_t *flags_y, uint8_t *flags_z, cudaStream_t s);
 cudaError_t copy_in(double *dst, const double *src, int nx, int ny, int nz, long long sy,
                     long long sz, cudaStream_t s);
 cudaError_t copy_out(double *dst, const double *src, int nx, int ny, int nz, long long sy,

@@ -538,7 +538,9 @@ __device__ __forceinline__ void chunk_eliminate(int r0, int n, const uint8_t (&m
 
 // chunk_eliminate with coefficients in T (LineCoefT) and the couplings
 // along the line staged as am_[r], ap_[r] for line row r (0-based).
-template <typename T, int M, typename LC>
+// REG: every row but the line's first and last has all six faces coupled
+// and is active (a regular tile), so those rows skip the mask decode
+template <typename T, int M, typename LC, bool REG = false>
 __device__ __forceinline__ void chunk_eliminate_t(int r0, int n, const uint8_t (&mk)[M], T (&d)[M],
                                                   T (&al)[M], T (&ga)[M], const T *am_, const T *ap_,
                                                   const LC &lc, T &aF, T &bF, T &cF, T &dF, T &aL,
@@ -551,7 +553,17 @@ __device__ __forceinline__ void chunk_eliminate_t(int r0, int n, const uint8_t (
     if (r < n) {
       const uint8_t m8 = mk[u];
       dd = d[u];
-      if (m8 & 64) {
+      if (REG && r != 0 && r != n - 1) {
+        const T am = am_[r], ap = ap_[r];
+        T diag = -lc.tdir;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) diag -= lc.tq[t];
+        diag -= am;
+        diag -= ap;
+        a = am;
+        c = ap;
+        b = diag;
+      } else if (m8 & 64) {
         const T am = am_[r], ap = ap_[r];
         T diag = -lc.tdir;
 #pragma unroll
@@ -1280,8 +1292,8 @@ __device__ __forceinline__ T ldx(const T *p) {
 // back-substitutes its rows.
 // NB > 0: the loads of all of a thread's rows are issued before the first
 // row's arithmetic (the kernels give NB blocks per SM, more registers).
-template <typename T, int M, int CH, int AXIS, int NB, bool COH>
-__device__ __forceinline__ void yz_pcr_tile(const DevLevel &L, int ti, int o, int color, T omega) {
+template <typename T, int M, int CH, int AXIS, int NB, bool COH, bool REG>
+__device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int o, int color, T omega) {
   using LC = LineCoefT<T, AXIS>;
   constexpr int NT = CH * YP_LINES;
   __shared__ T s_am[M * CH], s_ap[M * CH];  // couplings along the line
@@ -1353,23 +1365,32 @@ __device__ __forceinline__ void yz_pcr_tile(const DevLevel &L, int ti, int o, in
       mk[u] = 0;
       if (any && r < n) {
         const long long id = base + ls * (r + 1);
-        uint8_t m8 = L.mask[id];
         const T rv = rhs[id];
-        const T xv = ldx<COH>(x + id);
         const T nb[4] = {ldx<COH>(x + id - 1), ldx<COH>(x + id + 1), ldx<COH>(x + id - os), ldx<COH>(x + id + os)};
-        T acc = rv;
+        if (REG && r != 0 && r != n - 1) {
+          // a regular tile's inner row: active, all faces coupled (no mask read)
+          T acc = rv;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
-        const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
-        if (held) { acc = xv; m8 = 0; }
-        d[u] = acc;
-        mk[u] = m8;
+          for (int t = 0; t < 4; ++t) acc -= lc.tq[t] * nb[t];
+          d[u] = acc;
+          mk[u] = 0x7F;
+        } else {
+          uint8_t m8 = L.mask[id];
+          const T xv = ldx<COH>(x + id);
+          T acc = rv;
+#pragma unroll
+          for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
+          const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
+          if (held) { acc = xv; m8 = 0; }
+          d[u] = acc;
+          mk[u] = m8;
+        }
       }
     }
   }
   __syncthreads();  // s_am, s_ap
   T aF, bF, cF, dF, aL, cL, dL;
-  chunk_eliminate_t<T, M>(r0, any ? n : r0, mk, d, al, ga, s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
+  chunk_eliminate_t<T, M, LC, REG>(r0, any ? n : r0, mk, d, al, ga, s_am, s_ap, lc, aF, bF, cF, dF, aL, cL, dL);
   s_last[0][c][l] = aL;
   s_last[1][c][l] = cL;
   s_last[2][c][l] = dL;
@@ -1422,6 +1443,54 @@ __device__ __forceinline__ void yz_pcr_tile(const DevLevel &L, int ti, int o, in
   }
 }
 
+
+// A tile runs the regular form when its flag says so (every inner row of
+// its 16 lines active with all faces coupled, set when the level's masks
+// are built); otherwise the general one.  The loads-first variants always
+// take the general form.
+template <typename T, int M, int CH, int AXIS, int NB, bool COH>
+__device__ __forceinline__ void yz_pcr_tile(const DevLevel &L, int ti, int o, int color, T omega) {
+  if constexpr (NB > 0) {
+    yz_pcr_tile_impl<T, M, CH, AXIS, NB, COH, false>(L, ti, o, color, omega);
+  } else {
+    const int ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+    const auto reg = AXIS == 1 ? L.regy : L.regz;
+    if (reg && reg[ti + (long long)ntx * (o - 1)])
+      yz_pcr_tile_impl<T, M, CH, AXIS, NB, COH, true>(L, ti, o, color, omega);
+    else
+      yz_pcr_tile_impl<T, M, CH, AXIS, NB, COH, false>(L, ti, o, color, omega);
+  }
+}
+
+// Regular-tile flags of a level's y (AXIS 1) or z (AXIS 2) PCR tiles, one
+// block per (tile, plane): 1 when all 16 cells of the tile lie inside the
+// level and every row but the first and last of each of its lines is active
+// with all six faces coupled.
+template <int AXIS>
+__global__ void k_reg_tiles(DevLevel L, uint8_t *flags) {
+  const int ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+  const int ti = blockIdx.x % ntx, o = 1 + blockIdx.x / ntx;
+  const int i0 = 1 + 2 * YP_LINES * ti;
+  const int n = AXIS == 1 ? L.ny : L.nz;
+  const long long ls = AXIS == 1 ? L.sy : L.sz, os = AXIS == 1 ? L.sz : L.sy;
+  bool ok = i0 + 2 * YP_LINES - 1 <= L.nx;
+  const int inner = n > 2 ? n - 2 : 0;
+  for (int e = threadIdx.x; ok && e < 2 * YP_LINES * inner; e += blockDim.x) {
+    const int i = i0 + e % (2 * YP_LINES), r = 1 + e / (2 * YP_LINES);
+    const long long id = (long long)i + os * o + ls * (r + 1);
+    if ((L.mask[id] & 0x7F) != 0x7F) ok = false;
+  }
+  ok = __syncthreads_and(ok);
+  if (threadIdx.x == 0) flags[blockIdx.x] = ok ? 1 : 0;
+}
+
+cudaError_t reg_tiles(const DevLevel &L, uint8_t *flags_y, uint8_t *flags_z, cudaStream_t s) {
+  const int ntx = (L.nx + 2 * YP_LINES - 1) / (2 * YP_LINES);
+  if (ntx * L.nz > 0) k_reg_tiles<1><<<ntx * L.nz, 256, 0, s>>>(L, flags_y);
+  if (ntx * L.ny > 0) k_reg_tiles<2><<<ntx * L.ny, 256, 0, s>>>(L, flags_z);
+  note_launches(2);
+  return cudaGetLastError();
+}
 
 // occupancy bound of the y/z PCR kernels
 template <typename T, int CH, int NB>
@@ -1649,7 +1718,9 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
     if (maxn <= 1024) return launch_xsmem<T, 32>(Lr, color, omega, s);
     return cudaErrorInvalidValue;  // lines longer than 1024 cells
   }
-  if (v == LV_YPCR) {
+  if (v == LV_YPCR) {  // lines shorter than YP_MINROWS only when chosen (autotuner)
+    if (maxn <= 32) return launch_yzpcr<T, 4, 8>(Lr, axis, color, omega, s);
+    if (maxn <= 64) return launch_yzpcr<T, 4, 16>(Lr, axis, color, omega, s);
     if (maxn <= 128) return launch_yzpcr<T, 8, 16>(Lr, axis, color, omega, s);
     return launch_yzpcr<T, 8, 32>(Lr, axis, color, omega, s);
   }
