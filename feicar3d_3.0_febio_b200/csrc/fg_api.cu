@@ -2215,6 +2215,7 @@ fg_status fg_case_set_geometry(fg_case *c, const int8_t *iblank, const int8_t *g
                                const int32_t *dead_ijk, const int32_t *dead_cell_idx,
                                const double *dead_coefN, const double *dead_probe,
                                const double *dead_ip) {
+  if (c) c->geom->rows_ng = c->geom->rows_nd = -1;  // rows without a device copy
   if (!c || !iblank || !ghostCellMark || !dead_cell || nGhost < 0 || nDead < 0) return FG_BAD_INPUT;
   if ((nGhost > 0 && (!ghost_ijk || !ghost_cell || !ghost_coefN)) ||
       (nDead > 0 && (!dead_ijk || !dead_cell_idx || !dead_coefN)))

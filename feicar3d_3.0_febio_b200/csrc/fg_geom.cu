@@ -1265,6 +1265,8 @@ fg_status fg_gcm_set_internal_boundary(fg_case *c, int8_t *iblank, int8_t *ghost
   if (dead_cell) fg::host_copy(dead_cell, c->dead.data(), n);
   if (nGhost) *nGhost = ng;
   if (nDead) *nDead = nd;
+  G.rows_ng = ng;
+  G.rows_nd = nd;
   if (flags[2]) return FG_GEOMETRY_DEAD_NO_BODY;
   if (G.nHostFail) return FG_GEOMETRY_NO_HOST_CELL;
   return FG_OK;
@@ -1533,6 +1535,311 @@ fg_status fg_get_body_markers(fg_case *c, int ibody, double *xyz, double *uvw, d
     FG_CUDA(cudaStreamSynchronize(c->stream));
   }
   return FG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ body-intercept values
+// and the velocity ghost cells (GCM_BODYINTERCEPT_VALUES.F90,
+// GCM_GHOSTCELL_UPDATE.F90:1-359), on the rows of the last device tagging
+namespace fg {
+namespace bi {
+
+struct BodyVel {
+  int n;
+  const double *u[8], *uo[8];  // marker velocities (SoA, nvert each), this and the previous step; may be null
+};
+
+// LAPACK getrf/getri semantics on a 4x4 column-major matrix (partial
+// pivoting on the largest |a|, first index on ties; inverse of U, then
+// inv(A) L = inv(U), column interchanges)
+__device__ void invert4(double *a) {
+  int ipiv[4];
+#define A(i, j) a[(i) + 4 * (j)]
+  for (int j = 0; j < 4; ++j) {
+    int p = j;
+    double mx = fabs(A(j, j));
+    for (int i = j + 1; i < 4; ++i)
+      if (fabs(A(i, j)) > mx) { mx = fabs(A(i, j)); p = i; }
+    ipiv[j] = p;
+    if (A(p, j) == 0.0) continue;
+    if (p != j)
+      for (int q = 0; q < 4; ++q) { const double t = A(j, q); A(j, q) = A(p, q); A(p, q) = t; }
+    const double r = 1.0 / A(j, j);
+    for (int i = j + 1; i < 4; ++i) A(i, j) = A(i, j) * r;
+    for (int q = j + 1; q < 4; ++q)
+      for (int i = j + 1; i < 4; ++i) A(i, q) = A(i, q) - A(i, j) * A(j, q);
+  }
+  double t4[4];
+  for (int j = 0; j < 4; ++j) {
+    A(j, j) = 1.0 / A(j, j);
+    const double ajj = -A(j, j);
+    for (int i = 0; i < j; ++i) {
+      double s = 0.0;
+      for (int q = i; q < j; ++q) s = s + A(i, q) * A(q, j);
+      t4[i] = s;
+    }
+    for (int i = 0; i < j; ++i) A(i, j) = t4[i] * ajj;
+  }
+  double work[4];
+  for (int j = 3; j >= 0; --j) {
+    for (int i = j + 1; i < 4; ++i) { work[i] = A(i, j); A(i, j) = 0.0; }
+    for (int q = j + 1; q < 4; ++q)
+      for (int i = 0; i < 4; ++i) A(i, j) = A(i, j) - A(i, q) * work[q];
+  }
+  for (int j = 2; j >= 0; --j) {
+    const int jp = ipiv[j];
+    if (jp != j)
+      for (int i = 0; i < 4; ++i) { const double t = A(i, j); A(i, j) = A(i, jp); A(i, jp) = t; }
+  }
+#undef A
+}
+
+// one thread per row: the intercept velocity of this and the previous
+// step (GCM_calc_BIVelocity_Unstruc, :198-388) and dp/dn (:80-95, :141-156)
+__global__ void k_bi_values(int n, const int *list, const double *bi, const double *nrm, const int *closest,
+                            const int8_t *body, geo::Bodies BB, BodyVel V, int ntime, double dt, double *ubi,
+                            double *dpdn) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int ib = body[list[r]] - 1, e = closest[r];
+  double u[3] = {0.0, 0.0, 0.0}, uo[3] = {0.0, 0.0, 0.0};
+  if (ib >= 0 && ib < BB.n && e >= 0) {
+    const geo::Body &B = BB.b[ib];
+    const int n1 = B.tri[3 * e], n2 = B.tri[3 * e + 1], n3 = B.tri[3 * e + 2];
+    const int nd[3] = {n1, n2, n3};
+    double a[16];
+    for (int q = 0; q < 3; ++q) {
+      a[q] = B.vx[nd[q]]; a[q + 4] = B.vy[nd[q]]; a[q + 8] = B.vz[nd[q]]; a[q + 12] = 1.0;
+    }
+    a[3] = B.enx[e]; a[7] = B.eny[e]; a[11] = B.enz[e]; a[15] = 0.0;
+    invert4(a);
+    const double xB = bi[3 * r], yB = bi[3 * r + 1], zB = bi[3 * r + 2];
+    for (int q = 0; q < 6; ++q) {
+      const double *src = q < 3 ? V.u[ib] : V.uo[ib];
+      const int comp = q % 3;
+      double rhs[4] = {0.0, 0.0, 0.0, 0.0};
+      if (src) {
+        const double *sc = src + (size_t)comp * B.nvert;
+        rhs[0] = sc[n1]; rhs[1] = sc[n2]; rhs[2] = sc[n3];
+      }
+      double cX = 0.0, cY = 0.0, cZ = 0.0, cC = 0.0;
+      for (int i = 0; i < 4; ++i) {
+        cX = cX + a[0 + 4 * i] * rhs[i];
+        cY = cY + a[1 + 4 * i] * rhs[i];
+        cZ = cZ + a[2 + 4 * i] * rhs[i];
+        cC = cC + a[3 + 4 * i] * rhs[i];
+      }
+      const double v = cX * xB + cY * yB + cZ * zB + cC;
+      if (q < 3) u[comp] = v; else uo[comp] = v;
+    }
+  }
+  if (ubi) { ubi[3 * r] = u[0]; ubi[3 * r + 1] = u[1]; ubi[3 * r + 2] = u[2]; }
+  if (dpdn) {
+    double d = 0.0;
+    if (ntime > 1) {
+      d = (u[0] - uo[0]) / dt * nrm[3 * r] + (u[1] - uo[1]) / dt * nrm[3 * r + 1] + (u[2] - uo[2]) / dt * nrm[3 * r + 2];
+      d = -d;
+    }
+    dpdn[r] = d;
+  }
+}
+
+__constant__ int c_incI[8] = {0, 0, 1, 1, 0, 0, 1, 1};  // GCM_MEMORY_ALLOCATE.F90:593-623
+__constant__ int c_incJ[8] = {0, 1, 1, 0, 0, 1, 1, 0};
+__constant__ int c_incK[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+
+struct VelRows {
+  int nd, ng;
+  const int *dlist, *glist;     // cell ids
+  const int *dcell, *gcell;     // host cells (3 per row)
+  const double *dip;            // dead image points (3 per row)
+  const double *dcD, *gcD;      // Dirichlet weights (8 per row)
+  const double *alpha;          // ghost blending factors
+  const double *ubi_d, *ubi_g;  // intercept velocities (3 per row)
+};
+
+// one Jacobi step of the velocity ghost and dead cells: new values of
+// every row from the current fields into nv (3 per row; dead rows first)
+__global__ void k_vel_rows(geo::Grid g, VelRows R, const int8_t *iblank, const int8_t *dead, double bw, double iw,
+                           const double *u, const double *v, const double *w, double *nv, int *skip) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R.nd + R.ng) return;
+  const double *fld[3] = {u, v, w};
+  const bool isdead = r < R.nd;
+  const int q = isdead ? r : r - R.nd;
+  const long long id = isdead ? R.dlist[q] : R.glist[q];
+  const int i = (int)(id % g.NX), j = (int)((id / g.NX) % g.NY), k = (int)(id / (g.NX * g.NY));
+  const int *cell = isdead ? R.dcell + 3 * q : R.gcell + 3 * q;
+  double out[3];
+  if (cell[0] < 0 || (isdead && (j < 1 || j > g.ny - 1 || k < 1 || k > g.nz - 1))) {
+    skip[r] = 1;  // rows the reference leaves out keep their value
+    for (int c = 0; c < 3; ++c) nv[3 * r + c] = fld[c][id];
+    return;
+  }
+  skip[r] = 0;
+  if (isdead) {
+    const double xIP = R.dip[3 * q], yIP = R.dip[3 * q + 1], zIP = R.dip[3 * q + 2];
+    double ip[3] = {0.0, 0.0, 0.0}, inv[3] = {0.0, 0.0, 0.0}, dint = 0.0;
+    int sumk = 0;
+    bool solid = false;
+    for (int t = 0; t < 8; ++t) {
+      const int ii = cell[0] + c_incI[t], jj = cell[1] + c_incJ[t], kk = cell[2] + c_incK[t];
+      const long long q2 = ii + g.NX * (jj + g.NY * (long long)kk);
+      if (iblank[q2] == 1 && dead[q2] == 0) solid = true;
+      if (ii == i && jj == j && kk == k) continue;
+      const double dist = (g.xc[ii] - xIP) * (g.xc[ii] - xIP) + (g.yc[jj] - yIP) * (g.yc[jj] - yIP) +
+                          (g.zc[kk] - zIP) * (g.zc[kk] - zIP);
+      if (iblank[q2] == 0 || dead[q2] == -1) {
+        sumk++;
+        dint = dint + (1.0 / dist);
+        for (int c = 0; c < 3; ++c) inv[c] = inv[c] + (1.0 / dist) * fld[c][q2];
+      }
+    }
+    const bool fallback = solid && !(dint < 0.000001 || sumk == 1);
+    if (fallback) {
+      for (int c = 0; c < 3; ++c) ip[c] = inv[c] / dint;
+    } else {
+      for (int t = 0; t < 8; ++t) {
+        const int ii = cell[0] + c_incI[t], jj = cell[1] + c_incJ[t], kk = cell[2] + c_incK[t];
+        const long long q2 = ii + g.NX * (jj + g.NY * (long long)kk);
+        const bool own = ii == i && jj == j && kk == k;
+        for (int c = 0; c < 3; ++c)
+          ip[c] = ip[c] + R.dcD[8 * q + t] * (own ? R.ubi_d[3 * q + c] : fld[c][q2]);
+      }
+    }
+    for (int c = 0; c < 3; ++c) out[c] = R.ubi_d[3 * q + c] * bw - ip[c] * iw;
+  } else {
+    double gg[3] = {0.0, 0.0, 0.0};
+    for (int t = 0; t < 8; ++t) {
+      const int ii = cell[0] + c_incI[t], jj = cell[1] + c_incJ[t], kk = cell[2] + c_incK[t];
+      const long long q2 = ii + g.NX * (jj + g.NY * (long long)kk);
+      const bool own = ii == i && jj == j && kk == k;
+      for (int c = 0; c < 3; ++c) gg[c] = gg[c] + R.gcD[8 * q + t] * (own ? R.ubi_g[3 * q + c] : fld[c][q2]);
+    }
+    const double flag = R.alpha[q];
+    for (int c = 0; c < 3; ++c) out[c] = (1.0 - flag) * gg[c] + flag * gg[c];
+  }
+  for (int c = 0; c < 3; ++c) nv[3 * r + c] = out[c];
+}
+
+// the new values into the fields and the largest |du|+|dv|+|dw| (as the
+// bits of a non-negative double, which order like the values)
+__global__ void k_vel_scatter(VelRows R, long long NX, long long NY, const double *nv, const int *skip, double *u,
+                              double *v, double *w, unsigned long long *res) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R.nd + R.ng || skip[r]) return;
+  const long long id = r < R.nd ? R.dlist[r] : R.glist[r - R.nd];
+  const double d = fabs(nv[3 * r] - u[id]) + fabs(nv[3 * r + 1] - v[id]) + fabs(nv[3 * r + 2] - w[id]);
+  u[id] = nv[3 * r];
+  v[id] = nv[3 * r + 1];
+  w[id] = nv[3 * r + 2];
+  atomicMax(res, (unsigned long long)__double_as_longlong(d));
+  (void)NX; (void)NY;
+}
+
+}  // namespace bi
+}  // namespace fg
+
+namespace {
+
+fg_status bi_rows_ready(fg_case *c) {
+  const Geom &G = *c->geom;
+  if (G.rows_ng < 0 || G.rows_nd < 0 || G.rows_ng != c->nGhost || G.rows_nd != c->nDead) return FG_BAD_INPUT;
+  return FG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fg_status fg_body_intercept_values_device(fg_case *c, int ntime, double dt, double *ubi_ghost, double *ubi_dead,
+                                          double *dpdn_ghost, double *dpdn_dead) {
+  if (!c || !(dt > 0.0)) return FG_BAD_INPUT;
+  fg_status st = bi_rows_ready(c);
+  if (st != FG_OK) return st;
+  cudaSetDevice(c->device);
+  Geom &G = *c->geom;
+  cudaStream_t s = c->stream;
+  geo::Bodies BB = make_bodies(c);
+  bi::BodyVel V{};
+  V.n = BB.n;
+  for (int b = 0; b < BB.n && b < 8; ++b) {
+    V.u[b] = G.bodies[b].d_uvw;
+    V.uo[b] = G.bodies[b].d_uvw_old;
+  }
+  const int ng = G.rows_ng, nd = G.rows_nd;
+  if (ng > 0)
+    bi::k_bi_values<<<(ng + 127) / 128, 128, 0, s>>>(ng, G.glist.as<int>(), G.rg.bi.as<double>(), G.rg.nrm.as<double>(),
+                                                     G.rg.closest.as<int>(), G.d_body, BB, V, ntime, dt, ubi_ghost,
+                                                     dpdn_ghost);
+  if (nd > 0)
+    bi::k_bi_values<<<(nd + 127) / 128, 128, 0, s>>>(nd, G.dlist.as<int>(), G.rd.bi.as<double>(), G.rd.nrm.as<double>(),
+                                                     G.rd.closest.as<int>(), G.d_body, BB, V, ntime, dt, ubi_dead,
+                                                     dpdn_dead);
+  note_launches((ng > 0) + (nd > 0));
+  FG_CUDA(cudaGetLastError());
+  FG_CUDA(cudaStreamSynchronize(s));
+  return FG_OK;
+}
+
+fg_status fg_ghostcell_velocity_device(fg_case *c, double *u, double *v, double *w, const double *ubi_ghost,
+                                       const double *ubi_dead, int itermax_gc, double restol_gcv, int *iterations) {
+  if (!c || !u || !v || !w || itermax_gc < 0) return FG_BAD_INPUT;
+  fg_status st = bi_rows_ready(c);
+  if (st != FG_OK) return st;
+  Geom &G = *c->geom;
+  const int ng = G.rows_ng, nd = G.rows_nd;
+  if ((ng > 0 && !ubi_ghost) || (nd > 0 && !ubi_dead)) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  cudaStream_t s = c->stream;
+  geo::Grid g;
+  if ((st = geom_grid(c, g)) != FG_OK) return st;
+  bi::VelRows R{};
+  R.nd = nd; R.ng = ng;
+  R.dlist = G.dlist.as<int>(); R.glist = G.glist.as<int>();
+  R.dcell = G.rd.cell.as<int>(); R.gcell = G.rg.cell.as<int>();
+  R.dip = G.rd.ip.as<double>();
+  R.dcD = G.rd.cD.as<double>(); R.gcD = G.rg.cD.as<double>();
+  R.alpha = G.alpha.as<double>();
+  R.ubi_d = ubi_dead; R.ubi_g = ubi_ghost;
+  const double pld = c->cfg.probe_length_dead;
+  const double bw = pld / (pld - 1.0), iw = 1.0 / (pld - 1.0);
+  const int nr = nd + ng;
+  int it = 0;
+  double res = 1.0e10;
+  if (nr > 0) {
+    double *nv = nullptr;
+    int *skip = nullptr;
+    unsigned long long *d_res = nullptr;
+    FG_CUDA(fg::dev_alloc(&nv, 3 * (size_t)nr * sizeof(double)));
+    cudaError_t e = fg::dev_alloc(&skip, (size_t)nr * sizeof(int));
+    if (e == cudaSuccess) e = fg::dev_alloc(&d_res, sizeof(unsigned long long));
+    // GCM_GHOSTCELL_UPDATE.F90:73: iterate while iterGC < itermax_gc and
+    // the last sweep changed some row by more than restol_gcv
+    while (e == cudaSuccess && it < itermax_gc && res > restol_gcv) {
+      e = cudaMemsetAsync(d_res, 0, sizeof(unsigned long long), s);
+      if (e != cudaSuccess) break;
+      bi::k_vel_rows<<<(nr + 127) / 128, 128, 0, s>>>(g, R, G.d_iblank, G.d_dead, bw, iw, u, v, w, nv, skip);
+      bi::k_vel_scatter<<<(nr + 127) / 128, 128, 0, s>>>(R, g.NX, g.NY, nv, skip, u, v, w, d_res);
+      note_launches(2);
+      unsigned long long bits = 0;
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, d_res, sizeof(bits), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      memcpy(&res, &bits, sizeof(res));
+      ++it;
+    }
+    fg::dev_free(nv);
+    fg::dev_free(skip);
+    fg::dev_free(d_res);
+    if (e != cudaSuccess) {
+      set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+      return FG_CUDA_ERROR;
+    }
+  }
+  if (iterations) *iterations = it;
+  return (nr > 0 && it == itermax_gc && res > restol_gcv) ? FG_NOT_CONVERGED : FG_OK;
 }
 
 }  // extern "C"

@@ -65,6 +65,9 @@ struct Geom {
   int8_t *d_band = nullptr, *d_tmp = nullptr;
   double *d_xc = nullptr;      // xc[0..nx+1], yc, zc concatenated
   int nWarnSide = 0, nHostFail = 0;
+  // ghost and dead rows of the last device tagging (-1: the case's rows
+  // came from the caller, fg_case_set_geometry, and have no device copy)
+  int rows_ng = -1, rows_nd = -1;
   // lists (host copies after fg_gcm_set_internal_boundary)
   std::vector<double> g_coefD, g_bi, g_ip, g_probe, g_alpha, d_coefD, d_bi, d_probe;
   std::vector<int32_t> g_closest, d_closest;

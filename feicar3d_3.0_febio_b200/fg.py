@@ -748,6 +748,40 @@ def update_pressure_device(case, d_pprime: int, d_p: int | None = None):
            "fg_update_pressure_device")
 
 
+def _bi_lib():
+    L = lib()
+    if not getattr(L, "_bi_ready", False):
+        vp = C.c_void_p
+        L.fg_body_intercept_values_device.argtypes = [vp, C.c_int, C.c_double] + [vp] * 4
+        L.fg_ghostcell_velocity_device.argtypes = [vp] * 6 + [C.c_int, C.c_double, C.POINTER(C.c_int)]
+        L.fg_body_intercept_values_device.restype = C.c_int
+        L.fg_ghostcell_velocity_device.restype = C.c_int
+        L._bi_ready = True
+    return L
+
+
+def body_intercept_values_device(case, ntime, dt, d_ubi_ghost=None, d_ubi_dead=None, d_dpdn_ghost=None,
+                                 d_dpdn_dead=None):
+    """Intercept velocities and dp/dn of the ghost and dead rows into device
+    arrays (pointers; None skips an output)."""
+    vp = lambda x: C.c_void_p(x) if x else None
+    _check(_bi_lib().fg_body_intercept_values_device(case.h, ntime, dt, vp(d_ubi_ghost), vp(d_ubi_dead),
+                                                     vp(d_dpdn_ghost), vp(d_dpdn_dead)),
+           "fg_body_intercept_values_device")
+
+
+def ghostcell_velocity_device(case, d_u, d_v, d_w, d_ubi_ghost, d_ubi_dead, itermax_gc=200, restol_gcv=1e-10,
+                              allow_not_converged=False):
+    """The velocity ghost and dead cells on device fields; returns the sweeps run."""
+    vp = lambda x: C.c_void_p(x) if x else None
+    it = C.c_int(0)
+    rc = _bi_lib().fg_ghostcell_velocity_device(case.h, C.c_void_p(d_u), C.c_void_p(d_v), C.c_void_p(d_w),
+                                                 vp(d_ubi_ghost), vp(d_ubi_dead), itermax_gc, restol_gcv,
+                                                 C.byref(it))
+    _check(rc, "fg_ghostcell_velocity_device", (FG_OK, FG_NOT_CONVERGED) if allow_not_converged else (FG_OK,))
+    return it.value
+
+
 class AdParams(C.Structure):
     """fg_ad_params: the momentum sweeps' time step, viscosity (1/Re),
     relaxation and whether convection is implicit (Crank-Nicolson)."""

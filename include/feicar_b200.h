@@ -253,6 +253,28 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
  * itself); either triple may be NULL. */
 fg_status fg_correct_vel_device(fg_case *c, const double *pPrime, double dt, double *u, double *v, double *w,
                                 double *dpdx, double *dpdy, double *dpdz);
+/* GCM_SetBodyInterceptValues (GCM_BODYINTERCEPT_VALUES.F90:22-388) on the
+ * rows of the last fg_gcm_set_internal_boundary: per ghost and dead row the
+ * velocity at its body intercept, interpolated linearly over the closest
+ * element's markers (the element's three vertices and its normal), from
+ * the marker velocities fg_move_body keeps (zero before the first move),
+ * this and the previous step's, and dp/dn = -(du/dt . n) at the intercept
+ * (0 when ntime <= 1) -- the dp/dn data of fg_solve_poisson_device_bc.
+ * Device outputs: ubi_*[3 * rows], dpdn_*[rows]; any may be NULL.
+ * FG_BAD_INPUT when the rows came from fg_case_set_geometry. */
+fg_status fg_body_intercept_values_device(fg_case *c, int ntime, double dt, double *ubi_ghost, double *ubi_dead,
+                                          double *dpdn_ghost, double *dpdn_dead);
+/* GCM_ghostcell_velocity (GCM_GHOSTCELL_UPDATE.F90:1-359) for iOpt = 2 and
+ * mix_GC_form = 0 on device fields u, v, w (the reference updates the dead
+ * cells of its arguments and the ghost cells of the module arrays, the
+ * same arrays in solve_ad): dead cells u_BI w_BI - u_IP w_IP, ghost cells
+ * the Dirichlet interpolation with the intercept velocity in their own
+ * slot, iterated (Jacobi sweeps; the reference's in-place sweeps reach the
+ * same values) while a sweep changes some row by more than restol_gcv and
+ * fewer than itermax_gc sweeps ran.  FG_NOT_CONVERGED when the limit ran
+ * out. */
+fg_status fg_ghostcell_velocity_device(fg_case *c, double *u, double *v, double *w, const double *ubi_ghost,
+                                       const double *ubi_dead, int itermax_gc, double restol_gcv, int *iterations);
 /* The momentum equation's line SOR on device fields (one rank):
  * set_solve_ad's diffusion coefficients with viscosity reinv
  * (CORE_SET_SOLVERS.F90:591-677), then one pass of itsolv_ad

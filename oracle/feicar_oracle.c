@@ -82,11 +82,11 @@ struct or_case {
   /* ghost cells */
   int nGhost;
   int32_t *gijk, *gcell, *gclosest;
-  double *gcoefN, *gcoefD, *gbi, *gip, *gprobe, *galpha;
+  double *gcoefN, *gcoefD, *gbi, *gip, *gprobe, *galpha, *gnrm;
   /* dead cells */
   int nDead;
   int32_t *dijk, *dcell, *dclosest;
-  double *dcoefN, *dcoefD, *dbi, *dip, *dprobe;
+  double *dcoefN, *dcoefD, *dbi, *dip, *dprobe, *dnrm;
   /* outer BC state (CORE_SET_OUTER_BC.F90): persistent like the module
    * arrays bcxp/bcyp/bczp and pgrad* */
   double *bcxp, *bcyp, *bczp;
@@ -248,15 +248,15 @@ or_case *or_case_create(int nx, int ny, int nz, const double *xn,
 
 static void free_ghosts(or_case *c) {
   free(c->gijk); free(c->gcell); free(c->gclosest); free(c->gcoefN); free(c->gcoefD);
-  free(c->gbi); free(c->gip); free(c->gprobe); free(c->galpha);
+  free(c->gbi); free(c->gip); free(c->gprobe); free(c->galpha); free(c->gnrm);
   c->gijk = c->gcell = c->gclosest = NULL;
-  c->gcoefN = c->gcoefD = c->gbi = c->gip = c->gprobe = c->galpha = NULL;
+  c->gcoefN = c->gcoefD = c->gbi = c->gip = c->gprobe = c->galpha = c->gnrm = NULL;
 }
 static void free_deads(or_case *c) {
   free(c->dijk); free(c->dcell); free(c->dclosest); free(c->dcoefN); free(c->dcoefD);
-  free(c->dbi); free(c->dip); free(c->dprobe);
+  free(c->dbi); free(c->dip); free(c->dprobe); free(c->dnrm);
   c->dijk = c->dcell = c->dclosest = NULL;
-  c->dcoefN = c->dcoefD = c->dbi = c->dip = c->dprobe = NULL;
+  c->dcoefN = c->dcoefD = c->dbi = c->dip = c->dprobe = c->dnrm = NULL;
 }
 
 void or_case_destroy(or_case *c) {
@@ -747,29 +747,29 @@ int or_set_iblank_body_fast(or_case *c, int ntime, int ntime_start) {
  * ties, inverse of U then solve inv(A) L = inv(U), column interchanges).
  * MKL's exact operation order is not published; weights built from this
  * inverse are compared to the CUDA path to a relative tolerance. */
-int or_invert8(const double *a_in, double *inv, int *info) {
+static int invert_n(int N, const double *a_in, double *inv, int *info) {
   double a[64];
   int ipiv[8];
-  memcpy(a, a_in, sizeof(a));
-#define A(i, j) a[(i) + 8 * (j)]
+  memcpy(a, a_in, sizeof(double) * (size_t)(N * N));
+#define A(i, j) a[(i) + N * (j)]
   *info = 0;
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < N; ++j) {
     int p = j;
     double mx = fabs(A(j, j));
-    for (int i = j + 1; i < 8; ++i)
+    for (int i = j + 1; i < N; ++i)
       if (fabs(A(i, j)) > mx) { mx = fabs(A(i, j)); p = i; }
     ipiv[j] = p;
     if (A(p, j) == 0.0) { if (*info == 0) *info = j + 1; continue; }
     if (p != j)
-      for (int q = 0; q < 8; ++q) { double t = A(j, q); A(j, q) = A(p, q); A(p, q) = t; }
+      for (int q = 0; q < N; ++q) { double t = A(j, q); A(j, q) = A(p, q); A(p, q) = t; }
     double r = 1.0 / A(j, j);
-    for (int i = j + 1; i < 8; ++i) A(i, j) = A(i, j) * r;
-    for (int q = j + 1; q < 8; ++q)
-      for (int i = j + 1; i < 8; ++i) A(i, q) = A(i, q) - A(i, j) * A(j, q);
+    for (int i = j + 1; i < N; ++i) A(i, j) = A(i, j) * r;
+    for (int q = j + 1; q < N; ++q)
+      for (int i = j + 1; i < N; ++i) A(i, q) = A(i, q) - A(i, j) * A(j, q);
   }
-  if (*info != 0) { memcpy(inv, a, sizeof(a)); return OR_BAD_INPUT; }
+  if (*info != 0) { memcpy(inv, a, sizeof(double) * (size_t)(N * N)); return OR_BAD_INPUT; }
   /* DTRTRI: inverse of upper-triangular U in place */
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < N; ++j) {
     A(j, j) = 1.0 / A(j, j);
     double ajj = -A(j, j);
     /* x = triu(A(0:j-1,0:j-1)) * A(0:j-1, j) */
@@ -782,20 +782,22 @@ int or_invert8(const double *a_in, double *inv, int *info) {
   }
   /* DGETRI: solve inv(A)*L = inv(U) column by column from the right */
   double work[8];
-  for (int j = 7; j >= 0; --j) {
-    for (int i = j + 1; i < 8; ++i) { work[i] = A(i, j); A(i, j) = 0.0; }
-    for (int q = j + 1; q < 8; ++q)
-      for (int i = 0; i < 8; ++i) A(i, j) = A(i, j) - A(i, q) * work[q];
+  for (int j = N - 1; j >= 0; --j) {
+    for (int i = j + 1; i < N; ++i) { work[i] = A(i, j); A(i, j) = 0.0; }
+    for (int q = j + 1; q < N; ++q)
+      for (int i = 0; i < N; ++i) A(i, j) = A(i, j) - A(i, q) * work[q];
   }
-  for (int j = 6; j >= 0; --j) {
+  for (int j = N - 2; j >= 0; --j) {
     int jp = ipiv[j];
     if (jp != j)
-      for (int i = 0; i < 8; ++i) { double t = A(i, j); A(i, j) = A(i, jp); A(i, jp) = t; }
+      for (int i = 0; i < N; ++i) { double t = A(i, j); A(i, j) = A(i, jp); A(i, jp) = t; }
   }
 #undef A
-  memcpy(inv, a, sizeof(a));
+  memcpy(inv, a, sizeof(double) * (size_t)(N * N));
   return OR_OK;
 }
+
+int or_invert8(const double *a_in, double *inv, int *info) { return invert_n(8, a_in, inv, info); }
 
 static const int incI[8] = {0, 0, 1, 1, 0, 0, 1, 1}; /* GCM_MEMORY_ALLOCATE.F90:593-623 */
 static const int incJ[8] = {0, 1, 1, 0, 0, 1, 1, 0};
@@ -942,7 +944,7 @@ static int ghost_dead_setup(or_case *c, double pln, double plnD) {
   c->nGhost = ng;
   c->gijk = izalloc(3L * ng); c->gcell = izalloc(3L * ng); c->gclosest = izalloc(ng);
   c->gcoefN = dzalloc(8L * ng); c->gcoefD = dzalloc(8L * ng);
-  c->gbi = dzalloc(3L * ng); c->gip = dzalloc(3L * ng); c->gprobe = dzalloc(ng);
+  c->gbi = dzalloc(3L * ng); c->gip = dzalloc(3L * ng); c->gprobe = dzalloc(ng); c->gnrm = dzalloc(3L * ng);
   c->galpha = dzalloc(ng);
   ng = 0;
   for (int k = 1; k <= nz - 1; ++k)
@@ -973,6 +975,7 @@ static int ghost_dead_setup(or_case *c, double pln, double plnD) {
       ds = sqrt((xGC - xBI) * (xGC - xBI) + (yGC - yBI) * (yGC - yBI) + (zGC - zBI) * (zGC - zBI));
     }
     double bnx = -sx, bny = -sy, bnz = -sz;
+    c->gnrm[3 * n] = bnx; c->gnrm[3 * n + 1] = bny; c->gnrm[3 * n + 2] = bnz;  /* xBodyInterceptNorm (:386-388) */
     c->gprobe[n] = ds * pln;
     double xIP = xBI - (xBI - xGC) * pln;
     double yIP = yBI - (yBI - yGC) * pln;
@@ -1036,7 +1039,7 @@ static int ghost_dead_setup(or_case *c, double pln, double plnD) {
   c->nDead = nd;
   c->dijk = izalloc(3L * nd); c->dcell = izalloc(3L * nd); c->dclosest = izalloc(nd);
   c->dcoefN = dzalloc(8L * nd); c->dcoefD = dzalloc(8L * nd);
-  c->dbi = dzalloc(3L * nd); c->dip = dzalloc(3L * nd); c->dprobe = dzalloc(nd);
+  c->dbi = dzalloc(3L * nd); c->dip = dzalloc(3L * nd); c->dprobe = dzalloc(nd); c->dnrm = dzalloc(3L * nd);
   nd = 0;
   for (int k = 0; k <= nz; ++k)
     for (int j = 0; j <= ny; ++j)
@@ -1060,6 +1063,7 @@ static int ghost_dead_setup(or_case *c, double pln, double plnD) {
     double ds = sqrt((xDC - xBI) * (xDC - xBI) + (yDC - yBI) * (yDC - yBI) + (zDC - zBI) * (zDC - zBI));
     double sx = (xBI - xDC) / ds, sy = (yBI - yDC) / ds, sz = (zBI - zDC) / ds;
     double bnx = -sx, bny = -sy, bnz = -sz;
+    c->dnrm[3 * n] = bnx; c->dnrm[3 * n + 1] = bny; c->dnrm[3 * n + 2] = bnz;  /* xNormInterceptDead (:1109-1111) */
     double xIP, yIP, zIP;
     if (c->body[ib].type == OR_MEMBRANE) {
       /* :1115-1216.  The reference tests yIP before assigning it in this
@@ -2260,6 +2264,159 @@ int or_update_pressure(or_case *c, double *pp, double *p) {
   }
   if (p) memcpy(p, pp, sizeof(double) * (size_t)c->NX * c->NY * c->NZ);
   return OR_OK;
+}
+
+/* ------------------------------------------ body-intercept values
+ * GCM_BODYINTERCEPT_VALUES.F90:22-178 GCM_SetBodyInterceptValues with
+ * :198-388 GCM_calc_BIVelocity_Unstruc: per ghost and dead row the marker
+ * velocities of the closest element interpolated linearly to the body
+ * intercept (the 4x4 system of the element's three vertices and its normal,
+ * inverted with LAPACK DGETRF/DGETRI semantics), this step's and the
+ * previous step's, and dp/dn = -(du/dt . n) at the intercept (0 on the
+ * first step). */
+static void bi_velocity(const or_case *c, int ib, int elem, double xB, double yB, double zB, double *uvw,
+                        double *uvw_old) {
+  const or_body *B = &c->body[ib];
+  const int n1 = B->tri[3 * elem], n2 = B->tri[3 * elem + 1], n3 = B->tri[3 * elem + 2];
+  double van[16], inv[16];
+  const int nd[3] = {n1, n2, n3};
+  for (int r = 0; r < 3; ++r) {
+    van[r + 4 * 0] = B->xv[nd[r]]; van[r + 4 * 1] = B->yv[nd[r]]; van[r + 4 * 2] = B->zv[nd[r]];
+    van[r + 4 * 3] = 1.0;
+  }
+  van[3 + 4 * 0] = B->enx[elem]; van[3 + 4 * 1] = B->eny[elem]; van[3 + 4 * 2] = B->enz[elem];
+  van[3 + 4 * 3] = 0.0;
+  int info;
+  invert_n(4, van, inv, &info);
+  const double *src[6] = {B->mu, B->mv, B->mw, B->muo, B->mvo, B->mwo};
+  for (int q = 0; q < 6; ++q) {
+    double rhs[4] = {0.0, 0.0, 0.0, 0.0};
+    if (src[q]) { rhs[0] = src[q][n1]; rhs[1] = src[q][n2]; rhs[2] = src[q][n3]; }
+    double cX = 0.0, cY = 0.0, cZ = 0.0, cC = 0.0;
+    for (int i = 0; i < 4; ++i) {
+      cX = cX + inv[0 + 4 * i] * rhs[i];
+      cY = cY + inv[1 + 4 * i] * rhs[i];
+      cZ = cZ + inv[2 + 4 * i] * rhs[i];
+      cC = cC + inv[3 + 4 * i] * rhs[i];
+    }
+    const double v = cX * xB + cY * yB + cZ * zB + cC;
+    if (q < 3) uvw[q] = v; else uvw_old[q - 3] = v;
+  }
+}
+
+int or_body_intercept_values(or_case *c, int ntime, double dt, double *ubi_g, double *ubi_d, double *dpdn_g,
+                             double *dpdn_d) {
+  for (int pass = 0; pass < 2; ++pass) {
+    const int nr = pass == 0 ? c->nGhost : c->nDead;
+    const int32_t *ijk = pass == 0 ? c->gijk : c->dijk, *ce = pass == 0 ? c->gclosest : c->dclosest;
+    const double *bi = pass == 0 ? c->gbi : c->dbi, *nrm = pass == 0 ? c->gnrm : c->dnrm;
+    double *ub = pass == 0 ? ubi_g : ubi_d, *dp = pass == 0 ? dpdn_g : dpdn_d;
+    for (int n = 0; n < nr; ++n) {
+      int ib = c->bodyNum[IDX(c, ijk[3 * n], ijk[3 * n + 1], ijk[3 * n + 2])] - 1;
+      double u[3] = {0.0, 0.0, 0.0}, uo[3] = {0.0, 0.0, 0.0};
+      if (ib >= 0 && ib < c->nbody && ce[n] >= 0)
+        bi_velocity(c, ib, ce[n], bi[3 * n], bi[3 * n + 1], bi[3 * n + 2], u, uo);
+      if (ub) { ub[3 * n] = u[0]; ub[3 * n + 1] = u[1]; ub[3 * n + 2] = u[2]; }
+      if (dp) {
+        double d = 0.0;
+        if (ntime > 1) {
+          d = (u[0] - uo[0]) / dt * nrm[3 * n] + (u[1] - uo[1]) / dt * nrm[3 * n + 1] +
+              (u[2] - uo[2]) / dt * nrm[3 * n + 2];
+          d = -d;
+        }
+        dp[n] = d;
+      }
+    }
+  }
+  return OR_OK;
+}
+
+/* GCM_GHOSTCELL_UPDATE.F90:1-359 GCM_ghostcell_velocity for iOpt = 2 and
+ * mix_GC_form = 0, one rank: Gauss-Seidel over the dead rows, then the
+ * ghost rows, until the largest |du|+|dv|+|dw| of a sweep is at most
+ * restol_gcv or itermax_gc sweeps ran.  A dead row takes the intercept
+ * velocity through the Dirichlet weights (or the inverse-distance average
+ * of its fluid corners when a corner is pure solid) and is set to
+ * u_BI w_BI - u_IP w_IP with w_BI = pLD/(pLD-1), w_IP = 1/(pLD-1), pLD =
+ * probeLengthNormalizedD; a ghost row is the Dirichlet interpolation with
+ * the intercept velocity in its own slot. */
+int or_ghostcell_velocity(or_case *c, double *u, double *v, double *w, const double *ubi_g, const double *ubi_d,
+                          double pld, int itermax_gc, double restol_gcv, int *iterations) {
+  const double bw = pld / (pld - 1.0), iw = 1.0 / (pld - 1.0);
+  double *fld[3] = {u, v, w};
+  int it = 0;
+  double resMax = 1.0e10;
+  while (it < itermax_gc && resMax > restol_gcv) {
+    resMax = 0.0;
+    for (int n = 0; n < c->nDead; ++n) {
+      const int i = c->dijk[3 * n], j = c->dijk[3 * n + 1], k = c->dijk[3 * n + 2];
+      if (j < 1 || j > c->ny - 1 || k < 1 || k > c->nz - 1) continue;
+      if (c->dcell[3 * n] < 0) continue;
+      const long id = IDX(c, i, j, k);
+      const double xIP = c->dip[3 * n], yIP = c->dip[3 * n + 1], zIP = c->dip[3 * n + 2];
+      double prev[3], ip[3] = {0.0, 0.0, 0.0}, inv[3] = {0.0, 0.0, 0.0};
+      for (int q = 0; q < 3; ++q) prev[q] = fld[q][id];
+      double dint = 0.0;
+      int sumk = 0;
+      for (int r = 0; r < 8; ++r) {
+        const int ii = c->dcell[3 * n] + incI[r], jj = c->dcell[3 * n + 1] + incJ[r], kk = c->dcell[3 * n + 2] + incK[r];
+        if (ii == i && jj == j && kk == k) continue;
+        const double dist = (c->xc[ii] - xIP) * (c->xc[ii] - xIP) + (c->yc[jj] - yIP) * (c->yc[jj] - yIP) +
+                            (c->zc[kk] - zIP) * (c->zc[kk] - zIP);
+        const long q2 = IDX(c, ii, jj, kk);
+        if (c->iblank[q2] == 0 || c->dead[q2] == -1) {
+          sumk++;
+          dint = dint + (1.0 / dist);
+          for (int q = 0; q < 3; ++q) inv[q] = inv[q] + (1.0 / dist) * fld[q][q2];
+        }
+      }
+      int fallback = 0;
+      for (int r = 0; r < 8 && !fallback; ++r) {
+        const int ii = c->dcell[3 * n] + incI[r], jj = c->dcell[3 * n + 1] + incJ[r], kk = c->dcell[3 * n + 2] + incK[r];
+        const long q2 = IDX(c, ii, jj, kk);
+        if (c->iblank[q2] == 1 && c->dead[q2] == 0) {
+          if (dint < 0.000001 || sumk == 1) {
+            ip[0] = ip[1] = ip[2] = 0.0;
+          } else {
+            for (int q = 0; q < 3; ++q) ip[q] = inv[q] / dint;
+            fallback = 1;
+          }
+        }
+      }
+      if (!fallback)
+        for (int r = 0; r < 8; ++r) {
+          const int ii = c->dcell[3 * n] + incI[r], jj = c->dcell[3 * n + 1] + incJ[r], kk = c->dcell[3 * n + 2] + incK[r];
+          for (int q = 0; q < 3; ++q) {
+            if (ii != i || jj != j || kk != k) ip[q] = ip[q] + c->dcoefD[8 * n + r] * fld[q][IDX(c, ii, jj, kk)];
+            else ip[q] = ip[q] + c->dcoefD[8 * n + r] * ubi_d[3 * n + q];
+          }
+        }
+      for (int q = 0; q < 3; ++q) fld[q][id] = ubi_d[3 * n + q] * bw - ip[q] * iw;
+      const double rv = fabs(u[id] - prev[0]) + fabs(v[id] - prev[1]) + fabs(w[id] - prev[2]);
+      if (rv > resMax) resMax = rv;
+    }
+    for (int n = 0; n < c->nGhost; ++n) {
+      const int i = c->gijk[3 * n], j = c->gijk[3 * n + 1], k = c->gijk[3 * n + 2];
+      if (c->gcell[3 * n] < 0) continue;
+      const long id = IDX(c, i, j, k);
+      double prev[3], g[3] = {0.0, 0.0, 0.0};
+      for (int q = 0; q < 3; ++q) prev[q] = fld[q][id];
+      for (int r = 0; r < 8; ++r) {
+        const int ii = c->gcell[3 * n] + incI[r], jj = c->gcell[3 * n + 1] + incJ[r], kk = c->gcell[3 * n + 2] + incK[r];
+        for (int q = 0; q < 3; ++q) {
+          if (ii != i || jj != j || kk != k) g[q] = g[q] + c->gcoefD[8 * n + r] * fld[q][IDX(c, ii, jj, kk)];
+          else g[q] = g[q] + c->gcoefD[8 * n + r] * ubi_g[3 * n + q];
+        }
+      }
+      const double flag = c->galpha[n];
+      for (int q = 0; q < 3; ++q) fld[q][id] = (1.0 - flag) * g[q] + flag * g[q];
+      const double rv = fabs(u[id] - prev[0]) + fabs(v[id] - prev[1]) + fabs(w[id] - prev[2]);
+      if (rv > resMax) resMax = rv;
+    }
+    it++;
+  }
+  if (iterations) *iterations = it;
+  return (it == itermax_gc && resMax > restol_gcv) ? OR_NOT_CONVERGED : OR_OK;
 }
 
 /* ---------------------------------------------- momentum line SOR

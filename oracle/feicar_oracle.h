@@ -133,6 +133,13 @@ int  or_update_pressure(or_case *c, double *pp, double *p);
 /* momentum line SOR (CORE_SET_SOLVERS.F90:591-677, CORE_SOLVE_AD.F90):
  * ad holds amx_ad, apx_ad (nx+2 each), amy_ad, apy_ad (ny+2), amz_ad,
  * apz_ad (nz+2) */
+/* body-intercept velocities (3 per row) and dp/dn of the ghost and dead
+ * rows (GCM_BODYINTERCEPT_VALUES.F90:22-388); any output may be NULL */
+int  or_body_intercept_values(or_case *c, int ntime, double dt, double *ubi_g, double *ubi_d, double *dpdn_g,
+                              double *dpdn_d);
+/* velocity ghost and dead cells (GCM_GHOSTCELL_UPDATE.F90:1-359, mix_GC_form 0) */
+int  or_ghostcell_velocity(or_case *c, double *u, double *v, double *w, const double *ubi_g, const double *ubi_d,
+                           double pld, int itermax_gc, double restol_gcv, int *iterations);
 int  or_set_solve_ad(or_case *c, double dt, double reinv, double *ad);
 int  or_itsolv_ad(or_case *c, const double *ad, double *var, const double *r, const double *fu,
                   const double *fv, const double *fw, double half_dt, double omega_ad);

@@ -113,6 +113,9 @@ def lib():
         L.or_correct_vel.argtypes = [P, C.c_void_p, C.c_double] + [C.c_void_p] * 6
         L.or_update_pressure.argtypes = [P, C.c_void_p, C.c_void_p]
         L.or_set_solve_ad.argtypes = [P, C.c_double, C.c_double, C.c_void_p]
+        L.or_body_intercept_values.argtypes = [P, C.c_int, C.c_double] + [C.c_void_p] * 4
+        L.or_ghostcell_velocity.argtypes = [P] + [C.c_void_p] * 5 + [C.c_double, C.c_int, C.c_double,
+                                                                     C.POINTER(C.c_int)]
         L.or_itsolv_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_double]
         L.or_calc_residual_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_void_p, C.c_void_p]
         _lib = L
@@ -297,6 +300,23 @@ class OracleCase:
         p = np.zeros(self.shape, order="F")
         lib().or_update_pressure(self.h, _ptr(pp), _ptr(p))
         return p
+
+    def body_intercept_values(self, ntime, dt):
+        """(ubi_ghost (ng,3), ubi_dead (nd,3), dpdn_ghost, dpdn_dead):
+        GCM_SetBodyInterceptValues on the current rows."""
+        cnt = self.counts()
+        ng, nd = cnt["nGhost"], cnt["nDead"]
+        ug, ud, pg, pd = np.zeros((ng, 3)), np.zeros((nd, 3)), np.zeros(ng), np.zeros(nd)
+        lib().or_body_intercept_values(self.h, ntime, dt, _ptr(ug), _ptr(ud), _ptr(pg), _ptr(pd))
+        return ug, ud, pg, pd
+
+    def ghostcell_velocity(self, u, v, w, ubi_g, ubi_d, pld, itermax_gc, restol_gcv):
+        """u, v, w (Fortran-ordered) updated in place; returns (status, sweeps)."""
+        it = C.c_int(0)
+        rc = lib().or_ghostcell_velocity(self.h, _ptr(u), _ptr(v), _ptr(w), _ptr(np.ascontiguousarray(ubi_g)),
+                                         _ptr(np.ascontiguousarray(ubi_d)), pld, itermax_gc, restol_gcv,
+                                         C.byref(it))
+        return rc, it.value
 
     # momentum line SOR (CORE_SET_SOLVERS.F90 set_solve_ad, CORE_SOLVE_AD.F90)
     def set_solve_ad(self, dt, reinv):
