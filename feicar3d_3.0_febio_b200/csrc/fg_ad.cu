@@ -2,8 +2,10 @@
 // set_solve_ad's diffusion coefficients (CORE_SET_SOLVERS.F90:591-677),
 // one pass of itsolv_ad (CORE_SOLVE_AD.F90:131-776: x, then y, then z line
 // sweeps with the implicit convection terms) and calc_residual_ad
-// (:780-964).  Fields are device arrays in the reference layout
-// (0:nx+1, 0:ny+1, 0:nz+1), node counts.
+// (:780-964), the outer velocity boundaries (CORE_SET_OUTER_BC.F90
+// set_outer_velocity_bc, set_outer_ghost_velocity) and the solve_ad
+// iteration around them (CORE_SOLVE_AD.F90:11-127).  Fields are device
+// arrays in the reference layout (0:nx+1, 0:ny+1, 0:nz+1), node counts.
 //
 // The reference sweeps the lines of each direction in lexicographic order,
 // Gauss-Seidel style: an x line (j,k) reads the new values of lines (j-1,k)
@@ -210,6 +212,129 @@ k_ad_resid(Dims d, Met m, const int8_t *ib, const int8_t *gh, const double *var,
   }
 }
 
+// ---- outer velocity boundaries (CORE_SET_OUTER_BC.F90:18-509, :739-823)
+// Face order f: x1, x2, y1, y2, z1, z2.  puls holds the pulsatile values
+// val * sin(2 pi freq t) (x1's u: val t / 30), formed on the host with the
+// host's libm as the reference.
+struct VelBC {
+  int type[6];
+  double val[6][3], puls[6][3];
+  double yOrigin, yout, zOrigin, zout;
+};
+struct BCArr {
+  double *a[9];  // bcxu, bcxv, bcxw, bcyu, bcyv, bcyw, bczu, bczv, bczw
+};
+struct Vel {
+  const double *f[3];
+};
+
+// the user-specified channel profile val 6 (s - lo)(hi - s) / (hi - lo)^2
+__device__ __forceinline__ double channel(double val, double s, double lo, double hi) {
+  const double e = hi - lo;
+  return val * 6.0 * (s - lo) * (hi - s) / (e * e);
+}
+
+// x faces: one thread per (side, j, k), j = 0..ny+1, k = 0..nz+1
+__global__ void k_outer_bc_x(Dims d, VelBC p, const double *y, Vel U, BCArr B) {
+  const long long n = d.NY * (long long)(d.nz + 2), e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * n) return;
+  const int side = (int)(e / n), j = (int)((e % n) % d.NY), k = (int)((e % n) / d.NY);
+  const int i = side ? d.nx - 1 : 1, io = side ? 1 : d.nx - 1;
+  const long long b = side + 2 * (j + d.NY * (long long)k), id = d.id(i, j, k), ido = d.id(io, j, k);
+  const double *val = p.val[side];
+  switch (p.type[side]) {
+    case 1: for (int a = 0; a < 3; ++a) B.a[a][b] = val[a]; break;
+    case 2: for (int a = 0; a < 3; ++a) B.a[a][b] = U.f[a][id]; break;
+    case 3: for (int a = 0; a < 3; ++a) B.a[a][b] = p.puls[side][a]; break;
+    case 4: B.a[0][b] = 0.0; B.a[1][b] = U.f[1][id]; B.a[2][b] = U.f[2][id]; break;
+    case 5: for (int a = 0; a < 3; ++a) B.a[a][b] = 0.5 * (U.f[a][id] + U.f[a][ido]); break;
+    case 6:
+      B.a[0][b] = channel(val[0], y[j], p.yOrigin, p.yout);
+      if (side) { B.a[1][b] = val[1]; B.a[2][b] = val[2]; }
+      break;
+  }
+}
+
+// y faces: one thread per (side, i, k), i = 0..nx, k = 0..nz+1; the
+// user-specified profile goes into the x2 arrays at (1, j, k), written by
+// the i = 0 thread alone (the reference writes the same value for each i)
+__global__ void k_outer_bc_y(Dims d, VelBC p, const double *z, Vel U, BCArr B) {
+  const long long ni = d.nx + 1, n = ni * (d.nz + 2), e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * n) return;
+  const int side = (int)(e / n), i = (int)((e % n) % ni), k = (int)((e % n) / ni), f = 2 + side;
+  const int j = side ? d.ny - 1 : 1, jo = side ? 1 : d.ny - 1;
+  const long long b = i + d.NX * (side + 2 * (long long)k), id = d.id(i, j, k), ido = d.id(i, jo, k);
+  const double *val = p.val[f];
+  switch (p.type[f]) {
+    case 1: for (int a = 0; a < 3; ++a) B.a[3 + a][b] = val[a]; break;
+    case 2: for (int a = 0; a < 3; ++a) B.a[3 + a][b] = U.f[a][id]; break;
+    case 3: for (int a = 0; a < 3; ++a) B.a[3 + a][b] = p.puls[f][a]; break;
+    case 4: B.a[3][b] = U.f[0][id]; B.a[4][b] = 0.0; B.a[5][b] = U.f[2][id]; break;
+    case 5: for (int a = 0; a < 3; ++a) B.a[3 + a][b] = 0.5 * (U.f[a][id] + U.f[a][ido]); break;
+    case 6:
+      if (i == 0) {
+        const long long bx = 1 + 2 * (j + d.NY * (long long)k);
+        B.a[0][bx] = val[0];
+        B.a[1][bx] = channel(val[1], z[k], p.zOrigin, p.zout);
+        B.a[2][bx] = val[2];
+      }
+      break;
+  }
+}
+
+// z faces: one thread per (side, i, j), i = 0..nx, j = 0..ny+1
+__global__ void k_outer_bc_z(Dims d, VelBC p, const double *y, Vel U, BCArr B) {
+  const long long ni = d.nx + 1, n = ni * d.NY, e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= 2 * n) return;
+  const int side = (int)(e / n), i = (int)((e % n) % ni), j = (int)((e % n) / ni), f = 4 + side;
+  const int k = side ? d.nz - 1 : 1, ko = side ? 1 : d.nz - 1;
+  const long long b = i + d.NX * (j + d.NY * (long long)side), id = d.id(i, j, k), ido = d.id(i, j, ko);
+  const double *val = p.val[f];
+  switch (p.type[f]) {
+    case 1: for (int a = 0; a < 3; ++a) B.a[6 + a][b] = val[a]; break;
+    case 2: for (int a = 0; a < 3; ++a) B.a[6 + a][b] = U.f[a][id]; break;
+    case 3: for (int a = 0; a < 3; ++a) B.a[6 + a][b] = p.puls[f][a]; break;
+    case 4: B.a[6][b] = U.f[0][id]; B.a[7][b] = U.f[1][id]; B.a[8][b] = 0.0; break;
+    case 5: for (int a = 0; a < 3; ++a) B.a[6 + a][b] = 0.5 * (U.f[a][id] + U.f[a][ido]); break;
+    case 6:
+      if (i == 0) {
+        const long long bx = 1 + 2 * (j + d.NY * (long long)k);
+        B.a[0][bx] = val[0];
+        B.a[1][bx] = val[1];
+        B.a[2][bx] = channel(val[2], y[j], p.yOrigin, p.yout);
+      }
+      break;
+  }
+}
+
+// the outer ghost layer of one axis: u(ghost) = 2 bc - u(first interior);
+// x over (j, k) of 0..ny+1 x 0..nz+1, y over (i, k) of 0..nx x 0..nz+1,
+// z over (i, j) of 0..nx x 0..ny+1
+template <int AXIS>
+__global__ void k_outer_ghost(Dims d, double *u, double *v, double *w, BCArr B) {
+  const long long n1 = AXIS == 0 ? d.NY : d.nx + 1, n2 = AXIS == 2 ? d.NY : d.nz + 2;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n1 * n2) return;
+  const int p = (int)(e % n1), q = (int)(e / n1);
+  double *F[3] = {u, v, w};
+  long long g0, g1, i0, i1, b0, b1;
+  if (AXIS == 0) {
+    g0 = d.id(0, p, q); i0 = d.id(1, p, q); g1 = d.id(d.nx, p, q); i1 = d.id(d.nx - 1, p, q);
+    b0 = 2 * (p + d.NY * (long long)q); b1 = b0 + 1;
+  } else if (AXIS == 1) {
+    g0 = d.id(p, 0, q); i0 = d.id(p, 1, q); g1 = d.id(p, d.ny, q); i1 = d.id(p, d.ny - 1, q);
+    b0 = p + d.NX * (2 * (long long)q); b1 = b0 + d.NX;
+  } else {
+    g0 = d.id(p, q, 0); i0 = d.id(p, q, 1); g1 = d.id(p, q, d.nz); i1 = d.id(p, q, d.nz - 1);
+    b0 = p + d.NX * (long long)q; b1 = b0 + d.NX * d.NY;
+  }
+  for (int a = 0; a < 3; ++a) {
+    const double *bc = B.a[3 * AXIS + a];
+    F[a][g0] = 2.0 * bc[b0] - F[a][i0];
+    F[a][g1] = 2.0 * bc[b1] - F[a][i1];
+  }
+}
+
 }  // namespace ad
 }  // namespace fg
 
@@ -268,6 +393,83 @@ fg_status ad_setup(fg_case *c, const fg_ad_params *prm, ad::Met &m, ad::Dims &d)
 
 bool ad_params_ok(const fg_ad_params *p) {
   return p && p->dt > 0.0 && std::isfinite(p->reinv) && std::isfinite(p->omega_ad);
+}
+
+bool bc_arrays_ok(const fg_velocity_bc_arrays *b) {
+  return b && b->bcxu && b->bcxv && b->bcxw && b->bcyu && b->bcyv && b->bcyw && b->bczu && b->bczv && b->bczw;
+}
+
+ad::BCArr bc_arr(const fg_velocity_bc_arrays *b) {
+  ad::BCArr B;
+  double *const src[9] = {b->bcxu, b->bcxv, b->bcxw, b->bcyu, b->bcyv, b->bcyw, b->bczu, b->bczv, b->bczw};
+  for (int q = 0; q < 9; ++q) B.a[q] = src[q];
+  return B;
+}
+
+// the grid dimensions alone (the boundary kernels need no coefficients)
+fg_status dims_setup(fg_case *c, ad::Dims &d) {
+  if (!c->prepared) {
+    fg_status st = fg_mg_prepare(c);
+    if (st != FG_OK) return st;
+  }
+  d.nx = c->nx; d.ny = c->ny; d.nz = c->nz;
+  d.NX = (long long)c->nx + 2; d.NY = (long long)c->ny + 2;
+  return FG_OK;
+}
+
+unsigned blocks_of(long long n) { return (unsigned)((n + 255) / 256); }
+
+// set_outer_velocity_bc's face data; the pulsatile values with the host's
+// sin, pi = 4 atan(1) (CORE_SET_OUTER_BC.F90:40-42)
+bool vel_bc(const fg_velocity_bc *vb, ad::VelBC &p) {
+  const double pi = 4.0 * std::atan(1.0), t = vb->time;
+  for (int f = 0; f < 6; ++f) {
+    if (vb->type[f] < 1 || vb->type[f] > 6) return false;
+    p.type[f] = vb->type[f];
+    for (int a = 0; a < 3; ++a) {
+      p.val[f][a] = vb->val[f][a];
+      p.puls[f][a] = vb->val[f][a] * std::sin(2.0 * pi * vb->freq[f][a] * t);
+    }
+  }
+  p.puls[0][0] = vb->val[0][0] * t / 30.0;
+  p.yOrigin = vb->yOrigin; p.yout = vb->yout; p.zOrigin = vb->zOrigin; p.zout = vb->zout;
+  return true;
+}
+
+// the three face kernels of set_outer_velocity_bc, in the reference's order
+fg_status enqueue_outer_bc(fg_case *c, const ad::Dims &d, const double *u, const double *v, const double *w,
+                           const fg_velocity_bc_arrays *bc, const fg_velocity_bc *vb) {
+  ad::VelBC p;
+  if (!vel_bc(vb, p)) return FG_BAD_INPUT;
+  const HLevel &L = c->lev[0];
+  if (!c->d_vbcmet) {
+    std::vector<double> yz(L.y);
+    yz.insert(yz.end(), L.z.begin(), L.z.end());
+    FG_CUDA(fg::dev_alloc(&c->d_vbcmet, yz.size() * sizeof(double)));
+    FG_CUDA(cudaMemcpy(c->d_vbcmet, yz.data(), yz.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const double *y = c->d_vbcmet, *z = c->d_vbcmet + d.NY;
+  const ad::Vel U = {{u, v, w}};
+  const ad::BCArr B = bc_arr(bc);
+  cudaStream_t s = c->stream;
+  ad::k_outer_bc_x<<<blocks_of(2 * d.NY * (d.nz + 2)), 256, 0, s>>>(d, p, y, U, B);
+  ad::k_outer_bc_y<<<blocks_of(2 * (long long)(d.nx + 1) * (d.nz + 2)), 256, 0, s>>>(d, p, z, U, B);
+  ad::k_outer_bc_z<<<blocks_of(2 * (long long)(d.nx + 1) * d.NY), 256, 0, s>>>(d, p, y, U, B);
+  note_launches(3);
+  FG_CUDA(cudaGetLastError());
+  return FG_OK;
+}
+
+fg_status enqueue_outer_ghost(fg_case *c, const ad::Dims &d, double *u, double *v, double *w,
+                              const fg_velocity_bc_arrays *bc) {
+  const ad::BCArr B = bc_arr(bc);
+  cudaStream_t s = c->stream;
+  ad::k_outer_ghost<0><<<blocks_of(d.NY * (d.nz + 2)), 256, 0, s>>>(d, u, v, w, B);
+  ad::k_outer_ghost<1><<<blocks_of((long long)(d.nx + 1) * (d.nz + 2)), 256, 0, s>>>(d, u, v, w, B);
+  ad::k_outer_ghost<2><<<blocks_of((long long)(d.nx + 1) * d.NY), 256, 0, s>>>(d, u, v, w, B);
+  note_launches(3);
+  FG_CUDA(cudaGetLastError());
+  return FG_OK;
 }
 
 }  // namespace
@@ -371,6 +573,76 @@ fg_status fg_calc_residual_ad_device(fg_case *c, const double *var, const double
     loc[2] = v > 0.0 ? 1 + (int)(at / (ni * nj)) : 1;
   }
   return FG_OK;
+}
+
+fg_status fg_set_outer_velocity_bc_device(fg_case *c, const double *u, const double *v, const double *w,
+                                          const fg_velocity_bc_arrays *bc, const fg_velocity_bc *vb) {
+  if (!c || !u || !v || !w || !bc_arrays_ok(bc) || !vb) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  ad::Dims d;
+  fg_status st = dims_setup(c, d);
+  if (st == FG_OK) st = enqueue_outer_bc(c, d, u, v, w, bc, vb);
+  if (st != FG_OK) return st;
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+fg_status fg_set_outer_ghost_velocity_device(fg_case *c, double *u, double *v, double *w,
+                                             const fg_velocity_bc_arrays *bc) {
+  if (!c || !u || !v || !w || !bc_arrays_ok(bc)) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  ad::Dims d;
+  fg_status st = dims_setup(c, d);
+  if (st == FG_OK) st = enqueue_outer_ghost(c, d, u, v, w, bc);
+  if (st != FG_OK) return st;
+  FG_CUDA(cudaStreamSynchronize(c->stream));
+  return FG_OK;
+}
+
+fg_status fg_solve_ad_device(fg_case *c, double *u, double *v, double *w, const double *nlu, const double *nlv,
+                             const double *nlw, double *face_u, double *face_v, double *face_w,
+                             const fg_velocity_bc_arrays *bc, const double *ubi_ghost, const double *ubi_dead,
+                             const fg_ad_params *prm, const fg_velocity_bc *vb, int itermax_gc, double restol_gcv,
+                             int itermax_ad, double restol_ad, fg_solve_ad_stats *stats) {
+  if (!c || !u || !v || !w || !nlu || !nlv || !nlw || !face_u || !face_v || !face_w || !bc_arrays_ok(bc) ||
+      !ad_params_ok(prm) || !vb || itermax_ad < 0)
+    return FG_BAD_INPUT;
+  ad::VelBC chk;
+  if (!vel_bc(vb, chk)) return FG_BAD_INPUT;
+  int vzg[6];
+  for (int f = 0; f < 6; ++f) vzg[f] = vb->type[f] == 2;
+  int iter = 0, loc[3] = {1, 1, 1};
+  double res2 = 1.0e10;
+  fg_status st = FG_OK;
+  while (st == FG_OK && iter < itermax_ad && res2 > restol_ad) {
+    st = fg_itsolv_ad_device(c, u, nlu, face_u, face_v, face_w, prm);
+    if (st == FG_OK) st = fg_itsolv_ad_device(c, v, nlv, face_u, face_v, face_w, prm);
+    if (st == FG_OK) st = fg_itsolv_ad_device(c, w, nlw, face_u, face_v, face_w, prm);
+    if (st == FG_OK) st = fg_ghostcell_velocity_device(c, u, v, w, ubi_ghost, ubi_dead, itermax_gc, restol_gcv, nullptr);
+    if (st == FG_OK) st = fg_face_vel_device(c, u, v, w, bc->bcxu, bc->bcyv, bc->bczw, face_u, face_v, face_w);
+    if (st == FG_OK)
+      st = fg_enforce_global_mass_consv_device(c, face_u, face_v, face_w, bc->bcxu, bc->bcyv, bc->bczw, vzg);
+    if (st == FG_OK) st = fg_set_outer_velocity_bc_device(c, u, v, w, bc, vb);
+    if (st == FG_OK) st = fg_set_outer_ghost_velocity_device(c, u, v, w, bc);
+    double r[3] = {0.0, 0.0, 0.0};
+    int l[3][3];
+    const double *var[3] = {u, v, w}, *rhs[3] = {nlu, nlv, nlw};
+    for (int a = 0; a < 3 && st == FG_OK; ++a)
+      st = fg_calc_residual_ad_device(c, var[a], rhs[a], face_u, face_v, face_w, prm, &r[a], l[a]);
+    if (st != FG_OK) break;
+    int best = 0;
+    res2 = std::fabs(r[0]);
+    for (int a = 1; a < 3; ++a)
+      if (std::fabs(r[a]) > res2) { res2 = std::fabs(r[a]); best = a; }
+    std::memcpy(loc, l[best], sizeof(loc));
+    ++iter;
+  }
+  if (stats) {
+    stats->iterations = iter;
+    stats->residual = res2;
+    std::memcpy(stats->loc, loc, sizeof(loc));
+  }
+  return st;
 }
 
 }  // extern "C"

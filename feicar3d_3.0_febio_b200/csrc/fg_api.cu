@@ -2158,6 +2158,7 @@ fg_status fg_case_destroy(fg_case *c) {
   }
   fg::dev_free(c->d_G); fg::dev_free(c->d_gidx); fg::dev_free(c->d_pin); fg::dev_free(c->d_fin);
   fg::dev_free(c->d_refmask); fg::dev_free(c->d_rowtgt); fg::dev_free(c->d_rcg); fg::dev_free(c->d_admet);
+  fg::dev_free(c->d_vbcmet);
   fg::dev_free(c->d_gauge);
   fg::dev_free(c->d_pgrad); fg::dev_free(c->d_met); fg::dev_free(c->d_cpart); fg::dev_free(c->d_pmet);
   if (c->geom) geom_free(*c->geom);

@@ -105,6 +105,7 @@ struct fg_case {
   // per interpolation row, for row constants formed on the device: the
   // dp/dn index, its two factors, the fallback corners and weights
   double *d_admet = nullptr;          // momentum sweeps: metrics and set_solve_ad coefficients
+  double *d_vbcmet = nullptr;         // outer velocity boundaries: node coordinates y, z
   void *d_rcg = nullptr;
   long long rcg_version = -1;
   int rcg_n = 0;

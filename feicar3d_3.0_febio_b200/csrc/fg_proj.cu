@@ -298,6 +298,30 @@ unsigned cells_blocks(const fg_case *c) {
   return (unsigned)(((long long)(c->nx - 1) * (c->ny - 1) * (c->nz - 1) + 255) / 256);
 }
 
+int zero_gradient_faces(const int *vel_zero_gradient) {
+  int vzg = 0;
+  if (vel_zero_gradient)
+    for (int f = 0; f < 6; ++f)
+      if (vel_zero_gradient[f]) vzg |= 1 << f;
+  return vzg;
+}
+
+// enforce_global_mass_consv on the stream: the flux partials into part
+// (nb entries), the correction into part[2 nb], then applied
+void enqueue_mass_consv(fg_case *c, const proj::Met &m, const proj::Dims &d, int vzg, double *fu, double *fv,
+                        double *fw, double *bcxu, double *bcyv, double *bczw, double *part, unsigned nb,
+                        long long &launches) {
+  const size_t nref = (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2);
+  const int8_t *ib = c->d_refmask, *gh = c->d_refmask + nref;
+  cudaStream_t s = c->stream;
+  proj::k_massflux<<<nb, 256, 0, s>>>(d, m, ib, gh, fu, fv, fw, part);
+  proj::k_massflux_corr<<<1, 1024, 0, s>>>(d, m, ib, part, (int)nb, vzg, part + 2 * nb);
+  const long long big = (long long)(std::max(c->nx, c->ny) + 1) * (std::max(c->ny, c->nz) + 1);
+  proj::k_massflux_apply<<<dim3((unsigned)((big + 255) / 256), 6), 256, 0, s>>>(d, vzg, part + 2 * nb, bcxu, bcyv,
+                                                                              bczw, fu, fv, fw);
+  launches += 3;
+}
+
 }  // namespace
 
 extern "C" {
@@ -322,10 +346,7 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
                                 double *bcyv, double *bczw, const int *vel_zero_gradient, double dt, double *div,
                                 double *sumd, double *resdiv) {
   if (!c || !face_u || !face_v || !face_w || !div || !(dt > 0.0)) return FG_BAD_INPUT;
-  int vzg = 0;
-  if (vel_zero_gradient)
-    for (int f = 0; f < 6; ++f)
-      if (vel_zero_gradient[f]) vzg |= 1 << f;
+  const int vzg = zero_gradient_faces(vel_zero_gradient);
   if (vzg && (!bcxu || !bcyv || !bczw)) return FG_BAD_INPUT;
   cudaSetDevice(c->device);
   proj::Met m;
@@ -340,14 +361,7 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
   cudaStream_t s = c->stream;
   cudaError_t e = cudaSuccess;
   long long launches = 0;
-  if (vzg) {
-    proj::k_massflux<<<nb, 256, 0, s>>>(d, m, ib, gh, face_u, face_v, face_w, part);
-    proj::k_massflux_corr<<<1, 1024, 0, s>>>(d, m, ib, part, (int)nb, vzg, part + 2 * nb);
-    const long long big = (long long)(std::max(c->nx, c->ny) + 1) * (std::max(c->ny, c->nz) + 1);
-    proj::k_massflux_apply<<<dim3((unsigned)((big + 255) / 256), 6), 256, 0, s>>>(d, vzg, part + 2 * nb, bcxu, bcyv,
-                                                                                bczw, face_u, face_v, face_w);
-    launches += 3;
-  }
+  if (vzg) enqueue_mass_consv(c, m, d, vzg, face_u, face_v, face_w, bcxu, bcyv, bczw, part, nb, launches);
   e = cudaMemsetAsync(div, 0, nref * sizeof(double), s);
   if (e == cudaSuccess) {
     proj::k_div<<<nb, 256, 0, s>>>(d, m, ib, gh, face_u, face_v, face_w, 1.0 / dt, div, part, part + nb);
@@ -367,6 +381,34 @@ fg_status fg_rhs_poisson_device(fg_case *c, double *face_u, double *face_v, doub
   for (unsigned b = 0; b < nb; ++b) { sd += h[b]; rd = std::max(rd, h[nb + b]); }
   if (sumd) *sumd = sd / (1.0 / dt);  // the mass flux, dt removed
   if (resdiv) *resdiv = rd;
+  return FG_OK;
+}
+
+fg_status fg_enforce_global_mass_consv_device(fg_case *c, double *face_u, double *face_v, double *face_w,
+                                              double *bcxu, double *bcyv, double *bczw,
+                                              const int *vel_zero_gradient) {
+  if (!c || !face_u || !face_v || !face_w) return FG_BAD_INPUT;
+  const int vzg = zero_gradient_faces(vel_zero_gradient);
+  if (!vzg) return FG_OK;
+  if (!bcxu || !bcyv || !bczw) return FG_BAD_INPUT;
+  cudaSetDevice(c->device);
+  proj::Met m;
+  proj::Dims d;
+  fg_status st = proj_setup(c, m, d);
+  if (st != FG_OK) return st;
+  const unsigned nb = cells_blocks(c);
+  double *part = nullptr;
+  FG_CUDA(fg::dev_alloc(&part, (2 * (size_t)nb + 1) * sizeof(double)));
+  long long launches = 0;
+  enqueue_mass_consv(c, m, d, vzg, face_u, face_v, face_w, bcxu, bcyv, bczw, part, nb, launches);
+  note_launches(launches);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  fg::dev_free(part);
+  if (e != cudaSuccess) {
+    set_last_error(cudaGetErrorString(e), __FILE__, __LINE__);
+    return FG_CUDA_ERROR;
+  }
   return FG_OK;
 }
 

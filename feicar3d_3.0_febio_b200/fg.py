@@ -814,6 +814,86 @@ def calc_residual_ad_device(case, var, r, fu, fv, fw, prm: AdParams):
     return m.value, tuple(int(x) for x in loc)
 
 
+class VelocityBC(C.Structure):
+    """fg_velocity_bc: outer velocity boundary type per face x1, x2, y1, y2,
+    z1, z2 (1 Dirichlet, 2 zero gradient, 3 pulsatile inflow, 4 symmetry, 5
+    periodic, 6 user specified), (u, v, w) values and frequencies per face,
+    the flow time and the bounds of the user-specified channel profiles."""
+    _fields_ = [("type", C.c_int * 6), ("val", (C.c_double * 3) * 6), ("freq", (C.c_double * 3) * 6),
+                ("time", C.c_double), ("yOrigin", C.c_double), ("yout", C.c_double), ("zOrigin", C.c_double),
+                ("zout", C.c_double)]
+
+
+BC_ARRAY_NAMES = ("bcxu", "bcxv", "bcxw", "bcyu", "bcyv", "bcyw", "bczu", "bczv", "bczw")
+
+
+class VelocityBCArrays(C.Structure):
+    """fg_velocity_bc_arrays: device pointers of the nine outer boundary
+    arrays in the reference layout."""
+    _fields_ = [(n, C.c_void_p) for n in BC_ARRAY_NAMES]
+
+    @classmethod
+    def of(cls, ptrs):
+        assert len(ptrs) == 9
+        return cls(*[C.c_void_p(int(x)) for x in ptrs])
+
+
+class SolveAdStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("residual", C.c_double), ("loc", C.c_int * 3)]
+
+
+def _vbc_lib():
+    L = lib()
+    if not getattr(L, "_vbc_ready", False):
+        vp = C.c_void_p
+        A, V = C.POINTER(VelocityBCArrays), C.POINTER(VelocityBC)
+        L.fg_set_outer_velocity_bc_device.argtypes = [vp] * 4 + [A, V]
+        L.fg_set_outer_ghost_velocity_device.argtypes = [vp] * 4 + [A]
+        L.fg_enforce_global_mass_consv_device.argtypes = [vp] * 8
+        L.fg_solve_ad_device.argtypes = ([vp] * 10 + [A, vp, vp, C.POINTER(AdParams), V, C.c_int, C.c_double,
+                                                      C.c_int, C.c_double, C.POINTER(SolveAdStats)])
+        for n in ("fg_set_outer_velocity_bc_device", "fg_set_outer_ghost_velocity_device",
+                  "fg_enforce_global_mass_consv_device", "fg_solve_ad_device"):
+            getattr(L, n).restype = C.c_int
+        L._vbc_ready = True
+    return L
+
+
+def set_outer_velocity_bc_device(case, d_u, d_v, d_w, bc_ptrs, vb: VelocityBC):
+    """set_outer_velocity_bc into the nine device boundary arrays (pointers)."""
+    a = VelocityBCArrays.of(bc_ptrs)
+    _check(_vbc_lib().fg_set_outer_velocity_bc_device(case.h, *[C.c_void_p(x) for x in (d_u, d_v, d_w)],
+                                                      C.byref(a), C.byref(vb)), "fg_set_outer_velocity_bc_device")
+
+
+def set_outer_ghost_velocity_device(case, d_u, d_v, d_w, bc_ptrs):
+    a = VelocityBCArrays.of(bc_ptrs)
+    _check(_vbc_lib().fg_set_outer_ghost_velocity_device(case.h, *[C.c_void_p(x) for x in (d_u, d_v, d_w)],
+                                                         C.byref(a)), "fg_set_outer_ghost_velocity_device")
+
+
+def enforce_global_mass_consv_device(case, fu, fv, fw, bcxu, bcyv, bczw, vel_zero_gradient):
+    vz = np.ascontiguousarray(vel_zero_gradient, dtype=np.int32)
+    _check(_vbc_lib().fg_enforce_global_mass_consv_device(case.h, *[_dp(x) for x in (fu, fv, fw, bcxu, bcyv, bczw)],
+                                                          _p(vz)), "fg_enforce_global_mass_consv_device")
+
+
+def solve_ad_device(case, d_u, d_v, d_w, d_nlu, d_nlv, d_nlw, d_fu, d_fv, d_fw, bc_ptrs, d_ubi_ghost, d_ubi_dead,
+                    prm: AdParams, vb: VelocityBC, itermax_gc=200, restol_gcv=1e-10, itermax_ad=100,
+                    restol_ad=1e-8):
+    """solve_ad on device fields (pointers); returns (iterations, residual,
+    location)."""
+    a = VelocityBCArrays.of(bc_ptrs)
+    st = SolveAdStats()
+    vp = lambda x: C.c_void_p(x) if x else None
+    _check(_vbc_lib().fg_solve_ad_device(case.h, *[C.c_void_p(x) for x in (d_u, d_v, d_w, d_nlu, d_nlv, d_nlw,
+                                                                            d_fu, d_fv, d_fw)],
+                                         C.byref(a), vp(d_ubi_ghost), vp(d_ubi_dead), C.byref(prm), C.byref(vb),
+                                         itermax_gc, restol_gcv, itermax_ad, restol_ad, C.byref(st)),
+           "fg_solve_ad_device")
+    return st.iterations, st.residual, tuple(st.loc)
+
+
 def correct_vel_device(case, pp, dt, u=None, v=None, w=None, dpdx=None, dpdy=None, dpdz=None):
     _check(_proj_lib().fg_correct_vel_device(case.h, _dp(pp), dt, *[_dp(x) for x in (u, v, w, dpdx, dpdy, dpdz)]),
            "fg_correct_vel_device")

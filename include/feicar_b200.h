@@ -299,6 +299,66 @@ fg_status fg_itsolv_ad_device(fg_case *c, double *var, const double *r, const do
 fg_status fg_calc_residual_ad_device(fg_case *c, const double *var, const double *r, const double *face_u,
                                      const double *face_v, const double *face_w, const fg_ad_params *prm,
                                      double *resm, int *loc);
+/* Outer velocity boundary data: the input.dat keys of MAIN.F90:196-207.
+ * type per face x1, x2, y1, y2, z1, z2 (bcx1 ... bcz2): 1 Dirichlet, 2
+ * zero gradient, 3 pulsatile inflow, 4 symmetry, 5 periodic, 6 user
+ * specified; val the face's (u, v, w) (ux1, vx1, wx1, ...), freq their
+ * frequencies (freq_ux1, ...), time the flow time, and the bounds of the
+ * user-specified channel profiles. */
+typedef struct fg_velocity_bc {
+  int type[6];
+  double val[6][3];
+  double freq[6][3];
+  double time, yOrigin, yout, zOrigin, zout;
+} fg_velocity_bc;
+/* The nine outer boundary arrays in the reference layout: bcxu, bcxv,
+ * bcxw (0:1, 0:ny+1, 0:nz+1), bcyu, bcyv, bcyw (0:nx+1, 0:1, 0:nz+1),
+ * bczu, bczv, bczw (0:nx+1, 0:ny+1, 0:1), device memory. */
+typedef struct fg_velocity_bc_arrays {
+  double *bcxu, *bcxv, *bcxw, *bcyu, *bcyv, *bcyw, *bczu, *bczv, *bczw;
+} fg_velocity_bc_arrays;
+/* Replaces set_outer_velocity_bc (CORE_SET_OUTER_BC.F90:18-509) for one
+ * rank: x faces over j = 0..ny+1, k = 0..nz+1, then y faces over
+ * i = 0..nx, k = 0..nz+1, then z faces over i = 0..nx, j = 0..ny+1, each
+ * face by its type as the reference (the user-specified y and z faces
+ * write the x2 arrays at (1, j, k), as it does).  A shear face (7) or an
+ * unknown type returns FG_BAD_INPUT: the reference stops there. */
+fg_status fg_set_outer_velocity_bc_device(fg_case *c, const double *u, const double *v, const double *w,
+                                          const fg_velocity_bc_arrays *bc, const fg_velocity_bc *vb);
+/* Replaces set_outer_ghost_velocity (CORE_SET_OUTER_BC.F90:739-823): the
+ * outer ghost layer u = 2 bc - u(first interior), x faces, then y, then z
+ * (the corners take the later face's value, as the reference). */
+fg_status fg_set_outer_ghost_velocity_device(fg_case *c, double *u, double *v, double *w,
+                                             const fg_velocity_bc_arrays *bc);
+/* Replaces enforce_global_mass_consv (CORE_SET_OUTER_BC.F90:515-735) for
+ * one rank: when a face of vel_zero_gradient[6] is set, the net mass flux
+ * out of the fluid non-ghost cells is removed by a uniform outflow
+ * correction on those faces (bcxu/bcyv/bczw and the boundary face
+ * velocities). */
+fg_status fg_enforce_global_mass_consv_device(fg_case *c, double *face_u, double *face_v, double *face_w,
+                                              double *bcxu, double *bcyv, double *bczw,
+                                              const int *vel_zero_gradient);
+/* Replaces solve_ad (CORE_SOLVE_AD.F90:11-127) for one rank: while
+ * iterations < itermax_ad and the residual > restol_ad, one itsolv_ad pass
+ * of u, v, w (right-hand sides nlu, nlv, nlw), the velocity ghost and dead
+ * cells (fg_ghostcell_velocity_device with the intercept velocities
+ * ubi_ghost, ubi_dead), face_vel, enforce_global_mass_consv on vb's
+ * zero-gradient faces, the outer velocity boundaries and their ghost
+ * layer, and the largest of the three components' calc_residual_ad with
+ * its location.  An iteration count that reaches itermax_ad is reported
+ * in the outputs, not as an error (the reference prints it and goes on);
+ * ghost velocities that do not converge return FG_NOT_CONVERGED (the
+ * reference stops the run there). */
+typedef struct fg_solve_ad_stats {
+  int iterations;
+  double residual;
+  int loc[3];
+} fg_solve_ad_stats;
+fg_status fg_solve_ad_device(fg_case *c, double *u, double *v, double *w, const double *nlu, const double *nlv,
+                             const double *nlw, double *face_u, double *face_v, double *face_w,
+                             const fg_velocity_bc_arrays *bc, const double *ubi_ghost, const double *ubi_dead,
+                             const fg_ad_params *prm, const fg_velocity_bc *vb, int itermax_gc, double restol_gcv,
+                             int itermax_ad, double restol_ad, fg_solve_ad_stats *stats);
 /* update_pressure (CORE_FRAC_STEP_ROUTINES.F90:212-299) for one rank:
  * pPrime = 0 on the solid cells (iblank) not dead-marked -1, for
  * i = 0..nx, j = 0..ny+1, k = 0..nz+1, and on the domain edge lines the

@@ -2092,8 +2092,8 @@ int or_face_vel(or_case *c, const double *u, const double *v, const double *w, c
  * 0) then CORE_POISSON.F90:9-79 rhs_poisson: div = (du/dx + dv/dy +
  * dw/dz) / dt on fluid non-ghost cells; *sumd = the mass flux (dt removed),
  * *resdiv = max |div| dt */
-int or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv, double *bczw,
-                   const int *vzg, double dt, double *div, double *sumd, double *resdiv) {
+int or_enforce_global_mass_consv(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv,
+                                 double *bczw, const int *vzg) {
   const int nx = c->nx, ny = c->ny, nz = c->nz;
   int any = 0;
   for (int f = 0; f < 6; ++f) any |= vzg[f];
@@ -2162,6 +2162,13 @@ int or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu,
         if (vzg[5]) fw[IDX(c, i, j, nz)] = fw[IDX(c, i, j, nz)] + cv;
       }
   }
+  return OR_OK;
+}
+
+int or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv, double *bczw,
+                   const int *vzg, double dt, double *div, double *sumd, double *resdiv) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  or_enforce_global_mass_consv(c, fu, fv, fw, bcxu, bcyv, bczw, vzg);
   const double dtinv = 1.0 / dt;
   double sd = 0.0, rd = 0.0;
   memset(div, 0, sizeof(double) * (size_t)c->ntot);
@@ -2419,6 +2426,136 @@ int or_ghostcell_velocity(or_case *c, double *u, double *v, double *w, const dou
   return (it == itermax_gc && resMax > restol_gcv) ? OR_NOT_CONVERGED : OR_OK;
 }
 
+/* ------------------------------------------ outer velocity boundaries
+ * CORE_SET_OUTER_BC.F90:18-509 set_outer_velocity_bc and :739-823
+ * set_outer_ghost_velocity, one rank.  bc holds bcxu, bcxv, bcxw
+ * (0:1,0:ny+1,0:nz+1), bcyu, bcyv, bcyw (0:nx+1,0:1,0:nz+1), bczu, bczv, bczw
+ * (0:nx+1,0:ny+1,0:1).  The user-specified case of the y and z faces writes
+ * the x-face arrays at (1, j, k), as the reference does. */
+#define BX(a, s, j, k) bc[a][(long)(s) + 2 * ((long)(j) + c->NY * (long)(k))]
+#define BY(a, i, s, k) bc[3 + (a)][(long)(i) + c->NX * ((long)(s) + 2 * (long)(k))]
+#define BZ(a, i, j, s) bc[6 + (a)][(long)(i) + c->NX * ((long)(j) + c->NY * (long)(s))]
+int or_set_outer_velocity_bc(or_case *c, const double *u, const double *v, const double *w, double *const *bc,
+                             const or_velocity_bc *p) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  const double pi = 4.0 * atan(1.0), t = p->time;
+  const double *f3[3] = {u, v, w};
+  for (int f = 0; f < 6; ++f)
+    if (p->type[f] < 1 || p->type[f] > 6) return OR_BAD_INPUT;  /* shear: not implemented (:102-105) */
+  /* x faces */
+  for (int side = 0; side < 2; ++side) {
+    const int i = side == 0 ? 1 : nx - 1, io = side == 0 ? nx - 1 : 1, f = side;
+    const double *val = p->val[f], *fr = p->freq[f];
+    for (int k = 0; k <= nz + 1; ++k)
+      for (int j = 0; j <= ny + 1; ++j)
+        switch (p->type[f]) {
+          case 1: for (int a = 0; a < 3; ++a) BX(a, side, j, k) = val[a]; break;
+          case 2: for (int a = 0; a < 3; ++a) BX(a, side, j, k) = f3[a][IDX(c, i, j, k)]; break;
+          case 3:
+            BX(0, side, j, k) = side == 0 ? val[0] * t / 30.0 : val[0] * sin(2.0 * pi * fr[0] * t);
+            BX(1, side, j, k) = val[1] * sin(2.0 * pi * fr[1] * t);
+            BX(2, side, j, k) = val[2] * sin(2.0 * pi * fr[2] * t);
+            break;
+          case 4:
+            BX(0, side, j, k) = 0.0;
+            BX(1, side, j, k) = v[IDX(c, i, j, k)];
+            BX(2, side, j, k) = w[IDX(c, i, j, k)];
+            break;
+          case 5:
+            for (int a = 0; a < 3; ++a) BX(a, side, j, k) = 0.5 * (f3[a][IDX(c, i, j, k)] + f3[a][IDX(c, io, j, k)]);
+            break;
+          case 6: {
+            const double e = p->yout - p->yOrigin;
+            BX(0, side, j, k) = val[0] * 6.0 * (c->y[j] - p->yOrigin) * (p->yout - c->y[j]) / (e * e);
+            if (side == 1) { BX(1, side, j, k) = val[1]; BX(2, side, j, k) = val[2]; }
+            break;
+          }
+        }
+  }
+  /* y faces */
+  for (int side = 0; side < 2; ++side) {
+    const int j = side == 0 ? 1 : ny - 1, jo = side == 0 ? ny - 1 : 1, f = 2 + side;
+    const double *val = p->val[f], *fr = p->freq[f];
+    for (int k = 0; k <= nz + 1; ++k)
+      for (int i = 0; i <= nx; ++i)
+        switch (p->type[f]) {
+          case 1: for (int a = 0; a < 3; ++a) BY(a, i, side, k) = val[a]; break;
+          case 2: for (int a = 0; a < 3; ++a) BY(a, i, side, k) = f3[a][IDX(c, i, j, k)]; break;
+          case 3: for (int a = 0; a < 3; ++a) BY(a, i, side, k) = val[a] * sin(2.0 * pi * fr[a] * t); break;
+          case 4:
+            BY(0, i, side, k) = u[IDX(c, i, j, k)];
+            BY(1, i, side, k) = 0.0;
+            BY(2, i, side, k) = w[IDX(c, i, j, k)];
+            break;
+          case 5:
+            for (int a = 0; a < 3; ++a) BY(a, i, side, k) = 0.5 * (f3[a][IDX(c, i, j, k)] + f3[a][IDX(c, i, jo, k)]);
+            break;
+          case 6: {
+            const double e = p->zout - p->zOrigin;
+            BX(0, 1, j, k) = val[0];
+            BX(1, 1, j, k) = val[1] * 6.0 * (c->z[k] - p->zOrigin) * (p->zout - c->z[k]) / (e * e);
+            BX(2, 1, j, k) = val[2];
+            break;
+          }
+        }
+  }
+  /* z faces */
+  for (int side = 0; side < 2; ++side) {
+    const int k = side == 0 ? 1 : nz - 1, ko = side == 0 ? nz - 1 : 1, f = 4 + side;
+    const double *val = p->val[f], *fr = p->freq[f];
+    for (int i = 0; i <= nx; ++i)
+      for (int j = 0; j <= ny + 1; ++j)
+        switch (p->type[f]) {
+          case 1: for (int a = 0; a < 3; ++a) BZ(a, i, j, side) = val[a]; break;
+          case 2: for (int a = 0; a < 3; ++a) BZ(a, i, j, side) = f3[a][IDX(c, i, j, k)]; break;
+          case 3: for (int a = 0; a < 3; ++a) BZ(a, i, j, side) = val[a] * sin(2.0 * pi * fr[a] * t); break;
+          case 4:
+            BZ(0, i, j, side) = u[IDX(c, i, j, k)];
+            BZ(2, i, j, side) = 0.0;
+            BZ(1, i, j, side) = v[IDX(c, i, j, k)];
+            break;
+          case 5:
+            for (int a = 0; a < 3; ++a) BZ(a, i, j, side) = 0.5 * (f3[a][IDX(c, i, j, k)] + f3[a][IDX(c, i, j, ko)]);
+            break;
+          case 6: {
+            const double e = p->yout - p->yOrigin;
+            BX(0, 1, j, k) = val[0];
+            BX(1, 1, j, k) = val[1];
+            BX(2, 1, j, k) = val[2] * 6.0 * (c->y[j] - p->yOrigin) * (p->yout - c->y[j]) / (e * e);
+            break;
+          }
+        }
+  }
+  return OR_OK;
+}
+
+int or_set_outer_ghost_velocity(or_case *c, double *u, double *v, double *w, double *const *bc) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  double *f3[3] = {u, v, w};
+  for (int k = 0; k <= nz + 1; ++k)
+    for (int j = 0; j <= ny + 1; ++j)
+      for (int a = 0; a < 3; ++a) {
+        f3[a][IDX(c, 0, j, k)] = 2.0 * BX(a, 0, j, k) - f3[a][IDX(c, 1, j, k)];
+        f3[a][IDX(c, nx, j, k)] = 2.0 * BX(a, 1, j, k) - f3[a][IDX(c, nx - 1, j, k)];
+      }
+  for (int k = 0; k <= nz + 1; ++k)
+    for (int i = 0; i <= nx; ++i)
+      for (int a = 0; a < 3; ++a) {
+        f3[a][IDX(c, i, 0, k)] = 2.0 * BY(a, i, 0, k) - f3[a][IDX(c, i, 1, k)];
+        f3[a][IDX(c, i, ny, k)] = 2.0 * BY(a, i, 1, k) - f3[a][IDX(c, i, ny - 1, k)];
+      }
+  for (int i = 0; i <= nx; ++i)
+    for (int j = 0; j <= ny + 1; ++j)
+      for (int a = 0; a < 3; ++a) {
+        f3[a][IDX(c, i, j, 0)] = 2.0 * BZ(a, i, j, 0) - f3[a][IDX(c, i, j, 1)];
+        f3[a][IDX(c, i, j, nz)] = 2.0 * BZ(a, i, j, 1) - f3[a][IDX(c, i, j, nz - 1)];
+      }
+  return OR_OK;
+}
+#undef BX
+#undef BY
+#undef BZ
+
 /* ---------------------------------------------- momentum line SOR
  * CORE_SET_SOLVERS.F90:591-677 set_solve_ad (diffusion coefficients with
  * nu = reinv), CORE_SOLVE_AD.F90:162-776 itsolv_ad_x/y/z (one Gauss-Seidel
@@ -2626,6 +2763,52 @@ int or_calc_residual_ad(or_case *c, const double *ad, const double *var, const d
   if (resm) *resm = m;
   if (loc) { loc[0] = li; loc[1] = lj; loc[2] = lk; }
   return OR_OK;
+}
+
+/* CORE_SOLVE_AD.F90:11-127 solve_ad, one rank: while iter < itermax_ad and
+ * the largest of the three components' max residual exceeds restol_ad:
+ * itsolv_ad of u, v, w; the velocity ghost cells; face_vel;
+ * enforce_global_mass_consv; the outer velocity BCs and their ghost layer;
+ * calc_residual_ad of the three components.  The zero-gradient faces of vb
+ * are the ones whose outflow enforce_global_mass_consv corrects. */
+int or_solve_ad(or_case *c, const double *ad, double *u, double *v, double *w, const double *nlu, const double *nlv,
+                const double *nlw, double *fu, double *fv, double *fw, double *const *bc, const double *ubi_g,
+                const double *ubi_d, double half_dt, double omega_ad, const or_velocity_bc *vb, double pld,
+                int itermax_gc, double restol_gcv, int itermax_ad, double restol_ad, int *iterations, double *resm,
+                int *loc) {
+  int vzg[6];
+  for (int f = 0; f < 6; ++f) vzg[f] = vb->type[f] == 2;
+  int iter = 0;
+  double res2 = 1.0e10;
+  int l[3] = {1, 1, 1};
+  while (iter < itermax_ad && res2 > restol_ad) {
+    or_itsolv_ad(c, ad, u, nlu, fu, fv, fw, half_dt, omega_ad);
+    or_itsolv_ad(c, ad, v, nlv, fu, fv, fw, half_dt, omega_ad);
+    or_itsolv_ad(c, ad, w, nlw, fu, fv, fw, half_dt, omega_ad);
+    /* the reference stops the run when the ghost velocities do not converge
+       (GCM_GHOSTCELL_UPDATE.F90:344-356) */
+    if (or_ghostcell_velocity(c, u, v, w, ubi_g, ubi_d, pld, itermax_gc, restol_gcv, NULL) != OR_OK)
+      return OR_NOT_CONVERGED;
+    or_face_vel(c, u, v, w, bc[0], bc[4], bc[8], fu, fv, fw);
+    or_enforce_global_mass_consv(c, fu, fv, fw, bc[0], bc[4], bc[8], vzg);
+    int st = or_set_outer_velocity_bc(c, u, v, w, bc, vb);
+    if (st != OR_OK) return st;
+    or_set_outer_ghost_velocity(c, u, v, w, bc);
+    double ru, rv, rw;
+    int lu[3], lv[3], lw[3];
+    or_calc_residual_ad(c, ad, u, nlu, fu, fv, fw, half_dt, &ru, lu);
+    or_calc_residual_ad(c, ad, v, nlv, fu, fv, fw, half_dt, &rv, lv);
+    or_calc_residual_ad(c, ad, w, nlw, fu, fv, fw, half_dt, &rw, lw);
+    res2 = fabs(ru);
+    memcpy(l, lu, sizeof(l));
+    if (fabs(rv) > res2) { res2 = fabs(rv); memcpy(l, lv, sizeof(l)); }
+    if (fabs(rw) > res2) { res2 = fabs(rw); memcpy(l, lw, sizeof(l)); }
+    iter++;
+  }
+  if (iterations) *iterations = iter;
+  if (resm) *resm = res2;
+  if (loc) memcpy(loc, l, sizeof(l));
+  return OR_OK;  /* an unconverged sweep count is reported, not an error (CORE_SOLVE_AD.F90:110-114) */
 }
 
 /* CORE_POISSON.F90:205-456 itsolv (LSOR: x lexicographic, y zebra, z) on

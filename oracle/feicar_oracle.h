@@ -130,9 +130,6 @@ int  or_rhs_poisson(or_case *c, double *fu, double *fv, double *fw, double *bcxu
 int  or_correct_vel(or_case *c, const double *pp, double dt, double *u, double *v, double *w,
                     double *dpdx, double *dpdy, double *dpdz);
 int  or_update_pressure(or_case *c, double *pp, double *p);
-/* momentum line SOR (CORE_SET_SOLVERS.F90:591-677, CORE_SOLVE_AD.F90):
- * ad holds amx_ad, apx_ad (nx+2 each), amy_ad, apy_ad (ny+2), amz_ad,
- * apz_ad (nz+2) */
 /* body-intercept velocities (3 per row) and dp/dn of the ghost and dead
  * rows (GCM_BODYINTERCEPT_VALUES.F90:22-388); any output may be NULL */
 int  or_body_intercept_values(or_case *c, int ntime, double dt, double *ubi_g, double *ubi_d, double *dpdn_g,
@@ -140,6 +137,29 @@ int  or_body_intercept_values(or_case *c, int ntime, double dt, double *ubi_g, d
 /* velocity ghost and dead cells (GCM_GHOSTCELL_UPDATE.F90:1-359, mix_GC_form 0) */
 int  or_ghostcell_velocity(or_case *c, double *u, double *v, double *w, const double *ubi_g, const double *ubi_d,
                            double pld, int itermax_gc, double restol_gcv, int *iterations);
+/* outer velocity boundary data (CORE_SET_OUTER_BC.F90:18-509): type per
+ * face x1,x2,y1,y2,z1,z2 (1 Dirichlet, 2 zero gradient, 3 pulsatile
+ * inflow, 4 symmetry, 5 periodic, 6 user specified), (u,v,w) values and
+ * frequencies per face, the time, the channel-profile bounds */
+typedef struct or_velocity_bc {
+  int type[6];
+  double val[6][3], freq[6][3];
+  double time, yOrigin, yout, zOrigin, zout;
+} or_velocity_bc;
+int  or_enforce_global_mass_consv(or_case *c, double *fu, double *fv, double *fw, double *bcxu, double *bcyv,
+                                  double *bczw, const int *vzg);
+/* bc: bcxu, bcxv, bcxw, bcyu, bcyv, bcyw, bczu, bczv, bczw */
+int  or_set_outer_velocity_bc(or_case *c, const double *u, const double *v, const double *w, double *const *bc,
+                              const or_velocity_bc *p);
+int  or_set_outer_ghost_velocity(or_case *c, double *u, double *v, double *w, double *const *bc);
+int  or_solve_ad(or_case *c, const double *ad, double *u, double *v, double *w, const double *nlu,
+                 const double *nlv, const double *nlw, double *fu, double *fv, double *fw, double *const *bc,
+                 const double *ubi_g, const double *ubi_d, double half_dt, double omega_ad,
+                 const or_velocity_bc *vb, double pld, int itermax_gc, double restol_gcv, int itermax_ad,
+                 double restol_ad, int *iterations, double *resm, int *loc);
+/* momentum line SOR (CORE_SET_SOLVERS.F90:591-677, CORE_SOLVE_AD.F90):
+ * ad holds amx_ad, apx_ad (nx+2 each), amy_ad, apy_ad (ny+2), amz_ad,
+ * apz_ad (nz+2) */
 int  or_set_solve_ad(or_case *c, double dt, double reinv, double *ad);
 int  or_itsolv_ad(or_case *c, const double *ad, double *var, const double *r, const double *fu,
                   const double *fv, const double *fw, double half_dt, double omega_ad);

@@ -45,6 +45,17 @@ class RigidMotion(C.Structure):
                                               "angphase", "cent", "angv_old")]
 
 
+class VelocityBC(C.Structure):
+    """Outer velocity boundary data (or_velocity_bc / fg_velocity_bc): type
+    per face x1, x2, y1, y2, z1, z2 (1 Dirichlet, 2 zero gradient, 3
+    pulsatile inflow, 4 symmetry, 5 periodic, 6 user specified), (u, v, w)
+    values and frequencies per face, the time and the channel-profile
+    bounds (input.dat keys of MAIN.F90:196-207)."""
+    _fields_ = [("type", C.c_int * 6), ("val", (C.c_double * 3) * 6), ("freq", (C.c_double * 3) * 6),
+                ("time", C.c_double), ("yOrigin", C.c_double), ("yout", C.c_double), ("zOrigin", C.c_double),
+                ("zout", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("outer_iterations", C.c_int),
@@ -117,6 +128,12 @@ def lib():
         L.or_ghostcell_velocity.argtypes = [P] + [C.c_void_p] * 5 + [C.c_double, C.c_int, C.c_double,
                                                                      C.POINTER(C.c_int)]
         L.or_itsolv_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_double]
+        L.or_enforce_global_mass_consv.argtypes = [P] + [C.c_void_p] * 7
+        L.or_set_outer_velocity_bc.argtypes = [P] + [C.c_void_p] * 4 + [C.POINTER(VelocityBC)]
+        L.or_set_outer_ghost_velocity.argtypes = [P] + [C.c_void_p] * 4
+        L.or_solve_ad.argtypes = ([P] + [C.c_void_p] * 13 + [C.c_double, C.c_double, C.POINTER(VelocityBC),
+                                                            C.c_double, C.c_int, C.c_double, C.c_int, C.c_double,
+                                                            C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_void_p])
         L.or_calc_residual_ad.argtypes = [P] + [C.c_void_p] * 6 + [C.c_double, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
@@ -337,6 +354,52 @@ class OracleCase:
         lib().or_calc_residual_ad(self.h, _ptr(ad), *[_ptr(np.asfortranarray(a)) for a in (var, r, fu, fv, fw)],
                                   half_dt, C.byref(m), _ptr(loc))
         return m.value, tuple(int(x) for x in loc)
+
+    # the outer velocity boundaries and the momentum iteration around them
+    # (CORE_SET_OUTER_BC.F90, CORE_SOLVE_AD.F90:11-127); bc is the list of
+    # the nine Fortran-ordered arrays bcxu, bcxv, bcxw (2, ny+2, nz+2),
+    # bcyu, bcyv, bcyw (nx+2, 2, nz+2), bczu, bczv, bczw (nx+2, ny+2, 2)
+    def bc_arrays(self):
+        NX, NY, NZ = self.shape
+        return ([np.zeros((2, NY, NZ), order="F") for _ in range(3)] +
+                [np.zeros((NX, 2, NZ), order="F") for _ in range(3)] +
+                [np.zeros((NX, NY, 2), order="F") for _ in range(3)])
+
+    @staticmethod
+    def _bcp(bc):
+        assert len(bc) == 9 and all(a.flags.f_contiguous and a.dtype == np.float64 for a in bc)
+        return (C.c_void_p * 9)(*[a.ctypes.data for a in bc])
+
+    def enforce_global_mass_consv(self, fu, fv, fw, bcxu, bcyv, bczw, vzg):
+        vz = np.ascontiguousarray(vzg, dtype=np.int32)
+        lib().or_enforce_global_mass_consv(self.h, *[_ptr(a) for a in (fu, fv, fw, bcxu, bcyv, bczw, vz)])
+
+    def set_outer_velocity_bc(self, u, v, w, bc, vb):
+        """Fills the nine arrays of bc in place; returns the status."""
+        bp = self._bcp(bc)
+        return lib().or_set_outer_velocity_bc(self.h, *[_ptr(np.asfortranarray(a)) for a in (u, v, w)],
+                                              C.cast(bp, C.c_void_p), C.byref(vb))
+
+    def set_outer_ghost_velocity(self, u, v, w, bc):
+        assert u.flags.f_contiguous and v.flags.f_contiguous and w.flags.f_contiguous
+        bp = self._bcp(bc)
+        lib().or_set_outer_ghost_velocity(self.h, _ptr(u), _ptr(v), _ptr(w), C.cast(bp, C.c_void_p))
+
+    def solve_ad(self, ad, u, v, w, nlu, nlv, nlw, fu, fv, fw, bc, ubi_g, ubi_d, half_dt, omega_ad, vb, pld,
+                 itermax_gc, restol_gcv, itermax_ad, restol_ad):
+        """u, v, w, fu, fv, fw and bc updated in place; returns (status,
+        iterations, residual, location)."""
+        for a in (u, v, w, fu, fv, fw):
+            assert a.flags.f_contiguous
+        bp = self._bcp(bc)
+        it, rm = C.c_int(0), C.c_double(0.0)
+        loc = np.zeros(3, np.int32)
+        rc = lib().or_solve_ad(self.h, _ptr(ad), _ptr(u), _ptr(v), _ptr(w),
+                               *[_ptr(np.asfortranarray(a)) for a in (nlu, nlv, nlw)], _ptr(fu), _ptr(fv), _ptr(fw),
+                               C.cast(bp, C.c_void_p), _ptr(np.ascontiguousarray(ubi_g)),
+                               _ptr(np.ascontiguousarray(ubi_d)), half_dt, omega_ad, C.byref(vb), pld, itermax_gc,
+                               restol_gcv, itermax_ad, restol_ad, C.byref(it), C.byref(rm), _ptr(loc))
+        return rc, it.value, rm.value, tuple(int(x) for x in loc)
 
     def move_body(self, ibody, motion, ntime, time, dt):
         """One prescribed-motion step; motion (RigidMotion) is updated.
