@@ -668,7 +668,7 @@ __device__ __forceinline__ void chunk_eliminate_smem(int r0, int n, const uint8_
 // lines; no shared memory.
 template <typename T, int M, int W>
 __global__ void __launch_bounds__(XL_WARPS * 32, 1)
-k_xline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_xline_reg(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -809,7 +809,7 @@ __device__ __forceinline__ bool xs_line(const DevLevel &L, int lb, int warp, int
 
 template <typename T, int M>
 __global__ void __launch_bounds__(XS_WARPS * 32)
-k_xline_smem(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_xline_smem(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   using LY = XsLayout<T, M>;
   using LC = LineCoefT<T, 0>;
   constexpr int P = XS_PIECE;
@@ -924,7 +924,7 @@ struct Eq3 { T a, c, d; };  // a x_prev + x + c x_next = d
 
 template <typename T, int M, int CH, int AXIS>
 __global__ void __launch_bounds__(CH * 32, (sizeof(T) == 4 && CH == 16) ? (M <= 8 ? 3 : 2) : 1)
-k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_yzline_reg(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   using LC = LineCoefT<T, AXIS>;
   __shared__ ChunkEq<T> s_eq[CH][32];
   __shared__ T s_f[CH + 1][32];   // chunk-first unknowns
@@ -1046,7 +1046,7 @@ k_yzline_reg(const int *off, int nent, const DevLevel *levs, int color, T omega)
 // Lines (j,k) with (j+k)%2 == color; one warp per line.
 template <typename T, int MAXM>
 __global__ void __launch_bounds__(XL_WARPS * 32, 2)
-k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_xline(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
@@ -1106,7 +1106,7 @@ k_xline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
 // tile: line slot e%8, row e/8), then one warp solves each line.
 template <typename T, int MAXM, int AXIS>
 __global__ void __launch_bounds__(YZ_WARPS * 32, 2)
-k_yzline(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_yzline(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
@@ -1505,7 +1505,7 @@ struct YpBound {
 // the colour-0 launch left in L2
 template <typename T, int M, int CH, int AXIS, int NB>
 __global__ void __launch_bounds__(CH * YP_LINES, YpBound<T, CH, NB>::v)
-k_yzline_pcr(const int *off, int nent, const DevLevel *levs, int color, T omega) {
+k_yzline_pcr(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, int color, T omega) {
   const int p = find_entry(off, nent, blockIdx.x);
   const int lb = blockIdx.x - off[p];
   const DevLevel &L = levs[p];
@@ -1539,7 +1539,7 @@ __device__ __forceinline__ int ld_acquire_gpu(const int *p) {
 // plane q of problem p; zeroed before each launch.
 template <typename T, int M, int CH, int AXIS>
 __global__ void __launch_bounds__(CH * YP_LINES, YpBound<T, CH, 0>::v)
-k_yzline_wave(const int *off, int nent, const DevLevel *levs, T omega, int *wave, int *err, int resident) {
+k_yzline_wave(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, T omega, int *wave, int *err, int resident) {
   __shared__ int s_ticket;
   if (threadIdx.x == 0) s_ticket = atomicAdd(wave, 1);
   __syncthreads();
@@ -1827,7 +1827,7 @@ __global__ void __launch_bounds__(1024) k_reduce_parts(const int *off, const dou
 
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_residual(const int *off, int nent, const DevLevel *levs, double *part) {
+k_residual(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -1866,7 +1866,7 @@ cudaError_t residual(const Launch &Lr, double *norm2, double *part, cudaStream_t
 
 // ||f||^2 over active cells of level 0 (FP64 rhs)
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_fluid_norm(const int *off, int nent, const DevLevel *levs, double *part) {
+k_fluid_norm(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -1892,7 +1892,7 @@ cudaError_t fluid_norm(const Launch &Lr, double *norm2, double *part, cudaStream
 
 // Mixed precision outer step, part 1: p += e (FP64 += FP32) and e = 0.
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_correct(const int *off, int nent, const DevLevel *levs) {
+k_correct(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -1909,7 +1909,7 @@ k_correct(const int *off, int nent, const DevLevel *levs) {
 // part 2: FP64 residual of the corrected field, stored as the FP32 rhs of
 // the next correction V-cycle
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_residual_mixed(const int *off, int nent, const DevLevel *levs, double *part) {
+k_residual_mixed(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2002,7 +2002,7 @@ struct QuadVals {
 // restriction input); the arithmetic of k_residual, per quad
 template <typename T>
 __global__ void __launch_bounds__(QBLOCK)
-k_residual_q(const int *off, int nent, const DevLevel *levs) {
+k_residual_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2072,14 +2072,57 @@ __device__ __forceinline__ void restrict_cell(const DevLevel &C, const DevLevel 
 
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_restrict(const int *off, int nent, const DevLevel *coarse, const DevLevel *fine) {
+k_restrict(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT coarse, const DevLevel *FG_RESTRICT fine) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &C = coarse[p];
   const DevLevel &F = fine[p];
   const int lb = blockIdx.x - off[p];
+  // the arithmetic of restrict_cell with the thread's i-children and their
+  // widths kept over the block's CELL_ROWS rows (at most two children per
+  // axis: cl = 2I-1, ch = min(2I, n))
+  const int tpr = (C.nx + CELL_BLOCK - 1) / CELL_BLOCK;
+  const int rb = lb / tpr;
+  const int I = 1 + (lb - rb * tpr) * CELL_BLOCK + (int)threadIdx.x;
+  if (I > C.nx) return;
+  dptr<T> FG_RESTRICT rc = PrecOf<T>::rhs(C);
+  dptr<const T> FG_RESTRICT rf = PrecOf<T>::res(F);
+  dptr<const uint8_t> FG_RESTRICT cm = C.mask;
+  const long long csy = C.sy, csz = C.sz, fsy = F.sy, fsz = F.sz;
+  const int cny = C.ny, cnz = C.nz;
+  const int il = C.clx[I], ih = C.chx[I];
+  const double wx0 = F.wx[il], wx1 = F.wx[ih];
+#pragma unroll
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(C, lb, rr);
-    if (c.ok) restrict_cell<T>(C, F, c.i, c.j, c.k);
+    const int row = rb * CELL_ROWS + rr;
+    const int J = 1 + row % cny, K = 1 + row / cny;
+    if (K > cnz) break;  // rows only grow with rr
+    const long long id = I + csy * J + csz * K;
+    if (!(cm[id] & 64)) { rc[id] = T(0); continue; }
+    const int kl = C.clz[K], kh = C.chz[K], jl = C.cly[J], jh = C.chy[J];
+    double s = 0.0, v = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 2; ++kk) {
+      const int k = kl + kk;
+      if (k > kh) break;
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int j = jl + jj;
+        if (j > jh) break;
+        const double wyz = F.wy[j] * F.wz[k];
+        const long long rb2 = fsy * j + fsz * k;
+        {
+          const double w = wx0 * wyz;
+          s += w * (double)rf[rb2 + il];
+          v += w;
+        }
+        if (ih > il) {
+          const double w = wx1 * wyz;
+          s += w * (double)rf[rb2 + ih];
+          v += w;
+        }
+      }
+    }
+    rc[id] = (T)(s / v);
   }
 }
 
@@ -2122,14 +2165,48 @@ __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &
 
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_prolong(const int *off, int nent, const DevLevel *fine, const DevLevel *coarse) {
+k_prolong(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT fine, const DevLevel *FG_RESTRICT coarse) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &F = fine[p];
   const DevLevel &C = coarse[p];
   const int lb = blockIdx.x - off[p];
+  // a block covers CELL_ROWS rows of one i-range: the thread's i, its lower
+  // coarse cell and weight stay the same over the rows
+  const int tpr = (F.nx + CELL_BLOCK - 1) / CELL_BLOCK;
+  const int rb = lb / tpr;
+  const int i = 1 + (lb - rb * tpr) * CELL_BLOCK + (int)threadIdx.x;
+  if (i > F.nx) return;
+  dptr<T> FG_RESTRICT x = PrecOf<T>::x(F);
+  dptr<const T> FG_RESTRICT xc = PrecOf<T>::x(C);
+  dptr<const uint8_t> FG_RESTRICT fm = F.mask;
+  dptr<const uint8_t> FG_RESTRICT cm = C.mask;
+  const long long fsy = F.sy, fsz = F.sz, csy = C.sy, csz = C.sz;
+  const int fny = F.ny, fnz = F.nz, cny = C.ny, cnz = C.nz;
+  const int i0 = F.plx[i], i1 = i0 < C.nx ? i0 + 1 : i0;
+  const T wx1 = (T)F.pwx[i];
+  const T wx[2] = {T(1) - wx1, wx1};
+#pragma unroll
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const CellIdx c = cell_of(F, lb, rr);
-    if (c.ok) prolong_cell<T>(F, C, c.i, c.j, c.k);
+    const int row = rb * CELL_ROWS + rr;
+    const int j = 1 + row % fny, k = 1 + row / fny;
+    if (k > fnz) break;  // rows only grow with rr
+    const long long id = i + fsy * j + fsz * k;
+    if (!(fm[id] & 128)) continue;
+    const int j0 = F.ply[j], k0 = F.plz[k];
+    const int j1 = j0 < cny ? j0 + 1 : j0, k1 = k0 < cnz ? k0 + 1 : k0;
+    const T wy1 = (T)F.pwy[j], wz1 = (T)F.pwz[k];
+    const T wyz[4] = {(T(1) - wy1) * (T(1) - wz1), wy1 * (T(1) - wz1), (T(1) - wy1) * wz1, wy1 * wz1};
+    T s = T(0), ws = T(0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
+      const T w = wx[q & 1] * wyz[q >> 1];
+      const long long cid = ci + csy * cj + csz * ck;
+      const T act = (cm[cid] & 64) ? w : T(0);
+      s += act * xc[cid];
+      ws += act;
+    }
+    if (ws > T(1e-12)) x[id] = x[id] + s / ws;
   }
 }
 
@@ -2143,7 +2220,7 @@ cudaError_t prolong_add(const Launch &Lf, const DevLevel *coarse, cudaStream_t s
 
 template <typename T>
 __global__ void __launch_bounds__(CELL_BLOCK)
-k_zero(const int *off, int nent, const DevLevel *levs) {
+k_zero(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2258,7 +2335,7 @@ cudaError_t rows_residual(const DevRows &R, const DevLevel *lev0, double *maxabs
 // generalised inverse of the coarsest operator (FP64)
 template <typename T>
 __global__ void __launch_bounds__(256)
-k_coarsest(const DevLevel *levs, const double *const *G, const int *const *gidx, const int *gn) {
+k_coarsest(const DevLevel *FG_RESTRICT levs, const double *const *G, const int *const *gidx, const int *gn) {
   extern __shared__ double sr[];
   const int p = blockIdx.x;
   const DevLevel &L = levs[p];
@@ -2398,7 +2475,7 @@ __device__ void sc_up(const DevLevel &F, const DevLevel &C) {
 
 template <typename T>
 __global__ void __launch_bounds__(SC_THREADS)
-k_small_cycle(const SmallProb *probs, const DevLevel *levs, int nu1, int nu2, T omega) {
+k_small_cycle(const SmallProb *probs, const DevLevel *FG_RESTRICT levs, int nu1, int nu2, T omega) {
   extern __shared__ double sc_sr[];  // coarsest right-hand side (gn values)
   const SmallProb P = probs[blockIdx.x];
   for (int l = 0; l < P.nl - 1; ++l) {
@@ -2851,7 +2928,7 @@ __device__ __forceinline__ KSel kidx(const KCtl *ctl, int ph, KSel s) {
 // (4 cells of a row per thread, vector loads), FP64 arithmetic.
 template <typename B>
 __global__ void __launch_bounds__(QBLOCK)
-k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, double *part) {
+k_kr_resid(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, const KDesc *kd, int vd, double *part) {
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
@@ -2899,7 +2976,7 @@ k_kr_resid(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int 
 // couple to (they are held at the staged zero), so A x_T equals A Z_vz.
 template <typename B, typename T>
 __global__ void __launch_bounds__(QBLOCK)
-k_kr_apply_q(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vz, int vw,
+k_kr_apply_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, const KDesc *kd, int vz, int vw,
              const KCtl *ctl) {
   if (ctl) { vz = ctl->j; vw = ctl->j + 1; }
   const int p = find_entry(off, nent, blockIdx.x);
@@ -3108,7 +3185,7 @@ k_kr_reduce(const int *off, const double *part, int nblk, double *out, int ostri
 // stage, rhs_T = V_vd on active rows (0 elsewhere) and x_T = 0
 template <typename B, typename T>
 __global__ void __launch_bounds__(FLAT_THREADS)
-k_kr_vaxpy(const int *off, int nent, const DevLevel *levs, const KDesc *kd, int vd, int s0, int ns,
+k_kr_vaxpy(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT levs, const KDesc *kd, int vd, int s0, int ns,
            const double *coef, int cs, int stage, const KCtl *ctl, int ph) {
   {
     const KSel ks = kidx(ctl, ph, KSel{0, 0, 0, vd, s0, ns, stage});
