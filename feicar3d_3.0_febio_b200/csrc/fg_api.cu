@@ -828,7 +828,7 @@ static fg_status build_batch(fg_batch *b) {
         const DevLevel &d = c->lev[L].dl;
         vS.push_back(d);
         vSn.push_back(c->lev[L + 1].dl);
-        bc.push_back(k::blocks_cells(d));
+        bc.push_back(k::blocks_ptile(d));  // the prolongation into level L
         bx.push_back(k::blocks_xline(d, s.maxnx, b->tune.var[L][0]));
         by.push_back(k::blocks_tile(d, 1, s.maxny, b->tune.var[L][1]));
         bz.push_back(k::blocks_tile(d, 2, s.maxnz, b->tune.var[L][2]));

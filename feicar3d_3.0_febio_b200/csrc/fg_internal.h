@@ -258,6 +258,9 @@ int blocks_cells(const DevLevel &L);
 int blocks_flat(long long n);
 // quad kernels (4 cells of a row per thread)
 int blocks_quads(const DevLevel &L);
+// the prolongation into a level (shared-memory tiles of PT_I x PT_J cells
+// of one plane)
+int blocks_ptile(const DevLevel &L);
 // line kernel families of a sweep (chosen per level set and axis, by
 // default or by the autotuner): x lines in registers (lanes by line
 // length, or always 32), x lines staged in shared memory (one warp per

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <type_traits>
 #include <stdlib.h>
 #include <string.h>
 #include <stdint.h>
@@ -1275,10 +1276,11 @@ static cudaError_t launch_xreg(const Launch &Lr, int color, double omega, cudaSt
 
 // x loads of a tile: through L1, or (COH) from L2 only, for values other
 // blocks of the same launch may have written since this launch began
-template <bool COH, typename T>
-__device__ __forceinline__ T ldx(const T *p) {
-  if constexpr (COH) return __ldcg(p);
-  else return *p;
+template <bool COH, typename P>
+__device__ __forceinline__ auto ldx(const P &x, long long i)
+    -> std::remove_cv_t<std::remove_reference_t<decltype(x[i])>> {
+  if constexpr (COH) return __ldcg(&x[i]);
+  else return x[i];
 }
 
 // One tile of zebra y/z line relaxation in short chunks, for lines of
@@ -1339,11 +1341,11 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
         const long long id = base + ls * (r + 1);
         mk[u] = L.mask[id];
         rv[u] = rhs[id];
-        xv[u] = ldx<COH>(x + id);
-        nb[u][0] = ldx<COH>(x + id - 1);
-        nb[u][1] = ldx<COH>(x + id + 1);
-        nb[u][2] = ldx<COH>(x + id - os);
-        nb[u][3] = ldx<COH>(x + id + os);
+        xv[u] = ldx<COH>(x, id);
+        nb[u][0] = ldx<COH>(x, id - 1);
+        nb[u][1] = ldx<COH>(x, id + 1);
+        nb[u][2] = ldx<COH>(x, id - os);
+        nb[u][3] = ldx<COH>(x, id + os);
       }
     }
 #pragma unroll
@@ -1366,7 +1368,7 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
       if (any && r < n) {
         const long long id = base + ls * (r + 1);
         const T rv = rhs[id];
-        const T nb[4] = {ldx<COH>(x + id - 1), ldx<COH>(x + id + 1), ldx<COH>(x + id - os), ldx<COH>(x + id + os)};
+        const T nb[4] = {ldx<COH>(x, id - 1), ldx<COH>(x, id + 1), ldx<COH>(x, id - os), ldx<COH>(x, id + os)};
         if (REG && r != 0 && r != n - 1) {
           // a regular tile's inner row: active, all faces coupled (no mask read)
           T acc = rv;
@@ -1376,7 +1378,7 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
           mk[u] = 0x7F;
         } else {
           uint8_t m8 = L.mask[id];
-          const T xv = ldx<COH>(x + id);
+          const T xv = ldx<COH>(x, id);
           T acc = rv;
 #pragma unroll
           for (int t = 0; t < 4; ++t) acc -= ((m8 >> LC::qt(t)) & 1) ? lc.tq[t] * nb[t] : T(0);
@@ -1436,7 +1438,7 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
     T v = u == 0 ? xF : (u == M - 1 ? xL : d[u] - al[u] * xF - ga[u] * xL);
     const long long id = base + ls * (r + 1);
     if (omega != T(1)) {
-      const T xo = ldx<COH>(x + id);
+      const T xo = ldx<COH>(x, id);
       v = xo + omega * (v - xo);
     }
     x[id] = v;
@@ -2091,33 +2093,41 @@ k_restrict(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT coa
   const int cny = C.ny, cnz = C.nz;
   const int il = C.clx[I], ih = C.chx[I];
   const double wx0 = F.wx[il], wx1 = F.wx[ih];
+  // every child's value is loaded before the coarse mask decides (the
+  // children exist for every coarse cell), so the rows' loads are in
+  // flight together; the sums take the valid children in the order of
+  // restrict_cell
+  const int row0 = rb * CELL_ROWS;
+  int J = 1 + row0 % cny, K = 1 + row0 / cny;
 #pragma unroll
   for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const int row = rb * CELL_ROWS + rr;
-    const int J = 1 + row % cny, K = 1 + row / cny;
+    if (rr > 0 && ++J > cny) { J = 1; ++K; }
     if (K > cnz) break;  // rows only grow with rr
     const long long id = I + csy * J + csz * K;
-    if (!(cm[id] & 64)) { rc[id] = T(0); continue; }
     const int kl = C.clz[K], kh = C.chz[K], jl = C.cly[J], jh = C.chy[J];
+    const double wy0 = F.wy[jl], wy1 = F.wy[jh], wz0 = F.wz[kl], wz1 = F.wz[kh];
+    const long long b00 = fsy * jl + fsz * kl, b10 = fsy * jh + fsz * kl, b01 = fsy * jl + fsz * kh,
+                    b11 = fsy * jh + fsz * kh;
+    const T f[8] = {rf[b00 + il], rf[b00 + ih], rf[b10 + il], rf[b10 + ih],
+                    rf[b01 + il], rf[b01 + ih], rf[b11 + il], rf[b11 + ih]};
+    if (!(cm[id] & 64)) { rc[id] = T(0); continue; }
     double s = 0.0, v = 0.0;
 #pragma unroll
     for (int kk = 0; kk < 2; ++kk) {
-      const int k = kl + kk;
-      if (k > kh) break;
+      if (kk == 1 && kh == kl) break;
+      const double wz = kk ? wz1 : wz0;
 #pragma unroll
       for (int jj = 0; jj < 2; ++jj) {
-        const int j = jl + jj;
-        if (j > jh) break;
-        const double wyz = F.wy[j] * F.wz[k];
-        const long long rb2 = fsy * j + fsz * k;
+        if (jj == 1 && jh == jl) break;
+        const double wyz = (jj ? wy1 : wy0) * wz;
         {
           const double w = wx0 * wyz;
-          s += w * (double)rf[rb2 + il];
+          s += w * (double)f[4 * kk + 2 * jj];
           v += w;
         }
         if (ih > il) {
           const double w = wx1 * wyz;
-          s += w * (double)rf[rb2 + ih];
+          s += w * (double)f[4 * kk + 2 * jj + 1];
           v += w;
         }
       }
@@ -2163,50 +2173,120 @@ __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &
   if (ws > T(1e-12)) x[id] = x[id] + s / ws;
 }
 
+// A block prolongs PT_I consecutive fine cells of i in PT_J consecutive
+// rows of j of one fine plane k.  The coarse corners those cells read (the
+// lower coarse cell never decreases with the fine index, so they form a box
+// of at most PT_I + 2 by PT_J + 2 by 2 coarse cells) and their mask bytes
+// are copied into shared memory by asynchronous copies (no registers
+// held), while the thread's own fine column is loaded into registers; then
+// each fine cell reads its eight corners from shared memory, with the
+// arithmetic of prolong_cell.
+constexpr int PT_I = 128, PT_J = 8;
+constexpr int PT_CI = PT_I + 2, PT_CJ = PT_J + 2;
+constexpr int PT_MW = (PT_CI + 3 + 3) / 4;  // mask words of a tile row (from a word boundary)
+int blocks_ptile(const DevLevel &L) {
+  return ((L.nx + PT_I - 1) / PT_I) * ((L.ny + PT_J - 1) / PT_J) * L.nz;
+}
+
+// global -> shared copy of B bytes (4, 8 or 16, both addresses aligned to B)
+template <int B>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(B) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 template <typename T>
-__global__ void __launch_bounds__(CELL_BLOCK)
+__global__ void __launch_bounds__(PT_I)
 k_prolong(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT fine, const DevLevel *FG_RESTRICT coarse) {
+  __shared__ T sv[2 * PT_CJ * PT_CI];
+  __shared__ uint32_t smw[2 * PT_CJ * PT_MW];
+  __shared__ T swy[PT_J];
+  __shared__ int sr0[PT_J], sr1[PT_J];
   const int p = find_entry(off, nent, blockIdx.x);
   const DevLevel &F = fine[p];
   const DevLevel &C = coarse[p];
   const int lb = blockIdx.x - off[p];
-  // a block covers CELL_ROWS rows of one i-range: the thread's i, its lower
-  // coarse cell and weight stay the same over the rows
-  const int tpr = (F.nx + CELL_BLOCK - 1) / CELL_BLOCK;
-  const int rb = lb / tpr;
-  const int i = 1 + (lb - rb * tpr) * CELL_BLOCK + (int)threadIdx.x;
-  if (i > F.nx) return;
+  const int nti = (F.nx + PT_I - 1) / PT_I, ntj = (F.ny + PT_J - 1) / PT_J;
+  const int ti = lb % nti, rest = lb / nti, tj = rest % ntj, k = 1 + rest / ntj;
+  const int ia = 1 + ti * PT_I, ib = min(F.nx, ia + PT_I - 1);
+  const int ja = 1 + tj * PT_J, jb = min(F.ny, ja + PT_J - 1);
+  const int ca = F.plx[ia], cb = min(F.plx[ib] + 1, C.nx);
+  const int da = F.ply[ja], db = min(F.ply[jb] + 1, C.ny);
+  const int k0 = F.plz[k], k1 = k0 < C.nz ? k0 + 1 : k0;
+  const int ni = cb - ca + 1, nj = db - da + 1;
+  const int i = ia + (int)threadIdx.x;
+  if (ni > PT_CI || nj > PT_CJ) {  // a box larger than the tile (no level builds one): per cell
+    if (i <= ib)
+      for (int j = ja; j <= jb; ++j) prolong_cell<T>(F, C, i, j, k);
+    return;
+  }
+  // the coarse box: tile row r = (plane kk, row jj) at r = kk PT_CJ + jj;
+  // the mask words from the word holding cell ca (cell 1 of a row starts a
+  // word), so byte sh of a row is cell ca
+  const int ca4 = ca - ((ca - 1) & 3), sh = ca - ca4, nw = (sh + ni + 3) >> 2;
+  {
+    dptr<const T> xc = PrecOf<T>::x(C);
+    dptr<const uint8_t> cm = C.mask;
+    const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+    for (int r = warp; r < 2 * nj; r += PT_I / 32) {
+      const int kk = r >= nj ? 1 : 0, jj = r - kk * nj;
+      const long long rb = C.sy * (da + jj) + C.sz * (kk ? k1 : k0);
+      const int srow = kk * PT_CJ + jj;
+      for (int c = lane; c < ni; c += 32) cp_async<sizeof(T)>(&sv[srow * PT_CI + c], &xc[rb + ca + c]);
+      for (int w = lane; w < nw; w += 32) cp_async<4>(&smw[srow * PT_MW + w], &cm[rb + ca4 + 4 * w]);
+    }
+  }
+  // the thread's fine column: masks packed four to a word, values
   dptr<T> FG_RESTRICT x = PrecOf<T>::x(F);
-  dptr<const T> FG_RESTRICT xc = PrecOf<T>::x(C);
-  dptr<const uint8_t> FG_RESTRICT fm = F.mask;
-  dptr<const uint8_t> FG_RESTRICT cm = C.mask;
-  const long long fsy = F.sy, fsz = F.sz, csy = C.sy, csz = C.sz;
-  const int fny = F.ny, fnz = F.nz, cny = C.ny, cnz = C.nz;
-  const int i0 = F.plx[i], i1 = i0 < C.nx ? i0 + 1 : i0;
-  const T wx1 = (T)F.pwx[i];
+  const long long fsy = F.sy, id0 = i + fsy * ja + F.sz * k;
+  uint32_t mp[2] = {0u, 0u};
+  T xf[PT_J];
+  if (i <= ib) {
+    dptr<const uint8_t> FG_RESTRICT fm = F.mask;
+#pragma unroll
+    for (int jj = 0; jj < PT_J; ++jj) {
+      xf[jj] = T(0);
+      if (ja + jj <= jb) {
+        mp[jj >> 2] |= (uint32_t)fm[id0 + fsy * jj] << (8 * (jj & 3));
+        xf[jj] = x[id0 + fsy * jj];
+      }
+    }
+  }
+  if (threadIdx.x < PT_J && ja + (int)threadIdx.x <= jb) {
+    const int j = ja + (int)threadIdx.x, cj0 = F.ply[j];
+    sr0[threadIdx.x] = cj0 - da;
+    sr1[threadIdx.x] = (cj0 < C.ny ? cj0 + 1 : cj0) - da;
+    swy[threadIdx.x] = (T)F.pwy[j];
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  if (i > ib) return;
+  const uint8_t *smb = reinterpret_cast<const uint8_t *>(smw);
+  const int ci0 = F.plx[i];
+  const int i0 = ci0 - ca, i1 = (ci0 < C.nx ? ci0 + 1 : ci0) - ca;
+  const T wx1 = (T)F.pwx[i], wz1 = (T)F.pwz[k];
   const T wx[2] = {T(1) - wx1, wx1};
 #pragma unroll
-  for (int rr = 0; rr < CELL_ROWS; ++rr) {
-    const int row = rb * CELL_ROWS + rr;
-    const int j = 1 + row % fny, k = 1 + row / fny;
-    if (k > fnz) break;  // rows only grow with rr
-    const long long id = i + fsy * j + fsz * k;
-    if (!(fm[id] & 128)) continue;
-    const int j0 = F.ply[j], k0 = F.plz[k];
-    const int j1 = j0 < cny ? j0 + 1 : j0, k1 = k0 < cnz ? k0 + 1 : k0;
-    const T wy1 = (T)F.pwy[j], wz1 = (T)F.pwz[k];
+  for (int jj = 0; jj < PT_J; ++jj) {
+    if (ja + jj > jb) break;
+    if (!((mp[jj >> 2] >> (8 * (jj & 3))) & 128)) continue;
+    const int r0 = sr0[jj], r1 = sr1[jj];
+    const T wy1 = swy[jj];
     const T wyz[4] = {(T(1) - wy1) * (T(1) - wz1), wy1 * (T(1) - wz1), (T(1) - wy1) * wz1, wy1 * wz1};
     T s = T(0), ws = T(0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
+      const int row = ((q & 4) ? PT_CJ : 0) + ((q & 2) ? r1 : r0), col = (q & 1) ? i1 : i0;
       const T w = wx[q & 1] * wyz[q >> 1];
-      const long long cid = ci + csy * cj + csz * ck;
-      const T act = (cm[cid] & 64) ? w : T(0);
-      s += act * xc[cid];
+      const T act = (smb[row * (4 * PT_MW) + sh + col] & 64) ? w : T(0);
+      s += act * sv[row * PT_CI + col];
       ws += act;
     }
-    if (ws > T(1e-12)) x[id] = x[id] + s / ws;
+    if (ws > T(1e-12)) x[id0 + fsy * jj] = xf[jj] + s / ws;
   }
 }
 
