@@ -77,6 +77,19 @@ __host__ __device__ inline T *mkptr(T *p, long long, int) { return p; }
 #define FG_RESTRICT __restrict__
 #endif
 
+// A level array's pointer marked as global memory (the pointers are read
+// from the level descriptors, so the compiler cannot tell their address
+// space): loads and stores through it take the global forms, not the
+// generic ones.  Checked builds keep their bounds-checked pointers.
+#ifdef FG_CHECKED
+template <class P> __device__ __forceinline__ P glob(P p) { return p; }
+#else
+template <class T> __device__ __forceinline__ T *glob(T *p) {
+  __builtin_assume(__isGlobal(p));
+  return p;
+}
+#endif
+
 // array kinds reported by a checked build
 enum : int {
   K_TYPE = 1, K_MASK = 2, K_AXIS = 3, K_WIDTH = 4, K_CHILD = 5, K_PROL = 6, K_X = 7, K_RHS = 8,

@@ -139,8 +139,8 @@ struct LineCoef {
 
 __device__ __forceinline__ LineCoef line_coef(const DevLevel &L, int axis, int i, int j, int k) {
   LineCoef c;
-  const double am[3] = {L.amx[i], L.amy[j], L.amz[k]};
-  const double ap[3] = {L.apx[i], L.apy[j], L.apz[k]};
+  const double am[3] = {glob(L.amx)[i], glob(L.amy)[j], glob(L.amz)[k]};
+  const double ap[3] = {glob(L.apx)[i], glob(L.apy)[j], glob(L.apz)[k]};
   const long long st[3] = {1, L.sy, L.sz};
   const int idx[3] = {i, j, k};
   const int nn[3] = {L.nx, L.ny, L.nz};
@@ -206,7 +206,7 @@ template <typename T>
 __device__ __forceinline__ void stage(const DevLevel &L, long long id, const LineCoef &lc,
                                       dptr<const T> FG_RESTRICT x,
                                       dptr<const T> FG_RESTRICT rhs, T &d, uint8_t &mk) {
-  mk = L.mask[id];
+  mk = glob(L.mask)[id];
   const T r = rhs[id], xo = x[id];
   const T x0 = x[id + lc.to[0]], x1 = x[id + lc.to[1]], x2 = x[id + lc.to[2]], x3 = x[id + lc.to[3]];
   T acc = r;
@@ -374,14 +374,14 @@ __device__ __forceinline__ void warp_solve(int n, dptr<const double> FG_RESTRICT
 
 template <typename T> struct PrecOf;
 template <> struct PrecOf<double> {
-  static __device__ __forceinline__ dptr<double> x(const DevLevel &L) { return L.x64; }
-  static __device__ __forceinline__ dptr<double> rhs(const DevLevel &L) { return L.rhs64; }
-  static __device__ __forceinline__ dptr<double> res(const DevLevel &L) { return L.res64; }
+  static __device__ __forceinline__ dptr<double> x(const DevLevel &L) { return glob(L.x64); }
+  static __device__ __forceinline__ dptr<double> rhs(const DevLevel &L) { return glob(L.rhs64); }
+  static __device__ __forceinline__ dptr<double> res(const DevLevel &L) { return glob(L.res64); }
 };
 template <> struct PrecOf<float> {
-  static __device__ __forceinline__ dptr<float> x(const DevLevel &L) { return L.x32; }
-  static __device__ __forceinline__ dptr<float> rhs(const DevLevel &L) { return L.rhs32; }
-  static __device__ __forceinline__ dptr<float> res(const DevLevel &L) { return L.res32; }
+  static __device__ __forceinline__ dptr<float> x(const DevLevel &L) { return glob(L.x32); }
+  static __device__ __forceinline__ dptr<float> rhs(const DevLevel &L) { return glob(L.rhs32); }
+  static __device__ __forceinline__ dptr<float> res(const DevLevel &L) { return glob(L.res32); }
 };
 
 // bytes of dynamic shared memory of the launch (checked builds bound the
@@ -698,7 +698,7 @@ k_xline_reg(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT le
     // every load of the chunk is issued before the first use
     T nb[4][M], xv[M];
     load_run<T, M>(d, rhs, row + r0);
-    load_run<uint8_t, M>(mk, L.mask, row + r0);
+    load_run<uint8_t, M>(mk, glob(L.mask), row + r0);
 #pragma unroll
     for (int t = 0; t < 4; ++t) load_run<T, M>(nb[t], x, row + r0 + lc.to[t]);
     load_run<T, M>(xv, x, row + r0);
@@ -824,8 +824,8 @@ k_xline_smem(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
   const int lb = blockIdx.x - off[p];
   const int n = L.nx;
   for (int r = threadIdx.x; r < n; r += XS_WARPS * 32) {
-    s_am[r + r / M] = (T)L.amx[1 + r];
-    s_ap[r + r / M] = (T)L.apx[1 + r];
+    s_am[r + r / M] = (T)glob(L.amx)[1 + r];
+    s_ap[r + r / M] = (T)glob(L.apx)[1 + r];
   }
   __syncthreads();
   int j, k;
@@ -848,7 +848,7 @@ k_xline_smem(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
       uint8_t m4[P];
       load_run<T, P>(rv, rhs, row + e);
       load_run<T, P>(xo, x, row + e);
-      load_run<uint8_t, P>(m4, L.mask, row + e);
+      load_run<uint8_t, P>(m4, glob(L.mask), row + e);
       T nb[4][P];
 #pragma unroll
       for (int t = 0; t < 4; ++t) load_run<T, P>(nb[t], x, row + e + to[t]);
@@ -972,7 +972,7 @@ k_yzline_reg(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
     mk[u] = 0;
     if (any && r < n) {
       const long long id = base + ls * (r + 1);
-      uint8_t m8 = L.mask[id];
+      uint8_t m8 = glob(L.mask)[id];
       const T rv = rhs[id];
       const T xv = x[id];
       T nb[4];
@@ -1314,13 +1314,14 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
   const int n = AXIS == 1 ? L.ny : L.nz;
   const long long ls = AXIS == 1 ? L.sy : L.sz;  // row stride along the line
   const long long os = AXIS == 1 ? L.sz : L.sy;  // stride of the fixed index
-  auto x = PrecOf<T>::x(L);
-  auto rhs = PrecOf<T>::rhs(L);
+  auto x = glob(PrecOf<T>::x(L));
+  auto rhs = glob(PrecOf<T>::rhs(L));
   {
-    auto am = AXIS == 1 ? L.amy : L.amz;
-    auto ap = AXIS == 1 ? L.apy : L.apz;
+    auto am = glob(AXIS == 1 ? L.amy : L.amz);
+    auto ap = glob(AXIS == 1 ? L.apy : L.apz);
     for (int r = tid; r < n; r += NT) { s_am[r] = (T)am[1 + r]; s_ap[r] = (T)ap[1 + r]; }
   }
+  auto mask = glob(L.mask);
   const LC lc(line_coef(L, AXIS, valid ? i : L.nx, AXIS == 1 ? 1 : o, AXIS == 1 ? o : 1));
   const bool iso_line = lc.iso();
   const long long base = (long long)(valid ? i : L.nx) + os * o;  // row index 0 of the line
@@ -1339,7 +1340,7 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
       nb[u][0] = nb[u][1] = nb[u][2] = nb[u][3] = T(0);
       if (any && r < n) {
         const long long id = base + ls * (r + 1);
-        mk[u] = L.mask[id];
+        mk[u] = mask[id];
         rv[u] = rhs[id];
         xv[u] = ldx<COH>(x, id);
         nb[u][0] = ldx<COH>(x, id - 1);
@@ -1377,7 +1378,7 @@ __device__ __forceinline__ void yz_pcr_tile_impl(const DevLevel &L, int ti, int 
           d[u] = acc;
           mk[u] = 0x7F;
         } else {
-          uint8_t m8 = L.mask[id];
+          uint8_t m8 = mask[id];
           const T xv = ldx<COH>(x, id);
           T acc = rv;
 #pragma unroll
@@ -1480,7 +1481,7 @@ __global__ void k_reg_tiles(DevLevel L, uint8_t *flags) {
   for (int e = threadIdx.x; ok && e < 2 * YP_LINES * inner; e += blockDim.x) {
     const int i = i0 + e % (2 * YP_LINES), r = 1 + e / (2 * YP_LINES);
     const long long id = (long long)i + os * o + ls * (r + 1);
-    if ((L.mask[id] & 0x7F) != 0x7F) ok = false;
+    if ((glob(L.mask)[id] & 0x7F) != 0x7F) ok = false;
   }
   ok = __syncthreads_and(ok);
   if (threadIdx.x == 0) flags[blockIdx.x] = ok ? 1 : 0;
@@ -1796,7 +1797,7 @@ __device__ __forceinline__ T apply_row(const DevLevel &L, long long id, int i, i
                                        uint8_t mk, dptr<const T> FG_RESTRICT x) {
   const T xc = x[id];
   const T xn[6] = {x[id - 1], x[id + 1], x[id - L.sy], x[id + L.sy], x[id - L.sz], x[id + L.sz]};
-  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+  const double a[6] = {glob(L.amx)[i], glob(L.apx)[i], glob(L.amy)[j], glob(L.apy)[j], glob(L.amz)[k], glob(L.apz)[k]};
   return apply_vals<T>(L, i, j, k, mk, xc, xn, a);
 }
 
@@ -1842,7 +1843,7 @@ k_residual(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT lev
     const CellIdx c = cell_of(L, lb, rr);
     if (!c.ok) continue;
     const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    const uint8_t mk = L.mask[id];
+    const uint8_t mk = glob(L.mask)[id];
     T r = T(0);
     if (mk & 64) r = rhs[id] - apply_row<T>(L, id, c.i, c.j, c.k, mk, x);
     if (res) res[id] = r;  // norm only where the level keeps no residual array
@@ -1877,7 +1878,7 @@ k_fluid_norm(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
     const CellIdx c = cell_of(L, lb, rr);
     if (!c.ok) continue;
     const long long id = c.i + L.sy * c.j + L.sz * c.k;
-    if (L.mask[id] & 64) r2 += L.rhs64[id] * L.rhs64[id];
+    if (glob(L.mask)[id] & 64) r2 += L.rhs64[id] * L.rhs64[id];
   }
   const double t = block_sum(r2);
   if (threadIdx.x == 0) part[blockIdx.x] = t;
@@ -1922,7 +1923,7 @@ k_residual_mixed(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRI
     if (!c.ok) continue;
     const long long id = c.i + L.sy * c.j + L.sz * c.k;
     double r = 0.0;
-    const uint8_t mk = L.mask[id];
+    const uint8_t mk = glob(L.mask)[id];
     if (mk & 64) r = L.rhs64[id] - apply_row<double>(L, id, c.i, c.j, c.k, mk, L.x64);
     L.rhs32[id] = (float)r;
     r2 += r * r;
@@ -2021,8 +2022,8 @@ k_residual_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
     T f[4];
     uint8_t m4[4];
     load_run<T, 4>(f, rhs, id);
-    load_run<uint8_t, 4>(m4, L.mask, id);
-    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    load_run<uint8_t, 4>(m4, glob(L.mask), id);
+    const double ay0 = glob(L.amy)[q.j], ay1 = glob(L.apy)[q.j], az0 = glob(L.amz)[q.k], az1 = glob(L.apz)[q.k];
     T out[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -2031,7 +2032,7 @@ k_residual_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
       if (i <= L.nx && (m4[v] & 64)) {
         T xn[6];
         xv.nbrs(v, xn);
-        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        const double a[6] = {glob(L.amx)[i], glob(L.apx)[i], ay0, ay1, az0, az1};
         rv = f[v] - apply_vals<T>(L, i, q.j, q.k, m4[v], xv.c[v], xn, a);
       }
       out[v] = rv;
@@ -2057,14 +2058,14 @@ __device__ __forceinline__ void restrict_cell(const DevLevel &C, const DevLevel 
   auto rc = PrecOf<T>::rhs(C);
   auto rf = PrecOf<T>::res(F);
   const long long id = I + C.sy * J + C.sz * K;
-  if (!(C.mask[id] & 64)) { rc[id] = T(0); return; }
+  if (!(glob(C.mask)[id] & 64)) { rc[id] = T(0); return; }
   double s = 0.0, v = 0.0;
-  for (int k = C.clz[K]; k <= C.chz[K]; ++k)
-    for (int j = C.cly[J]; j <= C.chy[J]; ++j) {
-      const double wyz = F.wy[j] * F.wz[k];
+  for (int k = glob(C.clz)[K]; k <= glob(C.chz)[K]; ++k)
+    for (int j = glob(C.cly)[J]; j <= glob(C.chy)[J]; ++j) {
+      const double wyz = glob(F.wy)[j] * glob(F.wz)[k];
       const long long rb = F.sy * j + F.sz * k;
-      for (int i = C.clx[I]; i <= C.chx[I]; ++i) {
-        const double w = F.wx[i] * wyz;
+      for (int i = glob(C.clx)[I]; i <= glob(C.chx)[I]; ++i) {
+        const double w = glob(F.wx)[i] * wyz;
         s += w * (double)rf[rb + i];
         v += w;
       }
@@ -2091,8 +2092,8 @@ k_restrict(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT coa
   dptr<const uint8_t> FG_RESTRICT cm = C.mask;
   const long long csy = C.sy, csz = C.sz, fsy = F.sy, fsz = F.sz;
   const int cny = C.ny, cnz = C.nz;
-  const int il = C.clx[I], ih = C.chx[I];
-  const double wx0 = F.wx[il], wx1 = F.wx[ih];
+  const int il = glob(C.clx)[I], ih = glob(C.chx)[I];
+  const double wx0 = glob(F.wx)[il], wx1 = glob(F.wx)[ih];
   // every child's value is loaded before the coarse mask decides (the
   // children exist for every coarse cell), so the rows' loads are in
   // flight together; the sums take the valid children in the order of
@@ -2104,8 +2105,8 @@ k_restrict(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT coa
     if (rr > 0 && ++J > cny) { J = 1; ++K; }
     if (K > cnz) break;  // rows only grow with rr
     const long long id = I + csy * J + csz * K;
-    const int kl = C.clz[K], kh = C.chz[K], jl = C.cly[J], jh = C.chy[J];
-    const double wy0 = F.wy[jl], wy1 = F.wy[jh], wz0 = F.wz[kl], wz1 = F.wz[kh];
+    const int kl = glob(C.clz)[K], kh = glob(C.chz)[K], jl = glob(C.cly)[J], jh = glob(C.chy)[J];
+    const double wy0 = glob(F.wy)[jl], wy1 = glob(F.wy)[jh], wz0 = glob(F.wz)[kl], wz1 = glob(F.wz)[kh];
     const long long b00 = fsy * jl + fsz * kl, b10 = fsy * jh + fsz * kl, b01 = fsy * jl + fsz * kh,
                     b11 = fsy * jh + fsz * kh;
     const T f[8] = {rf[b00 + il], rf[b00 + ih], rf[b10 + il], rf[b10 + ih],
@@ -2154,10 +2155,10 @@ __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &
   auto xc = PrecOf<T>::x(C);
   auto x = PrecOf<T>::x(F);
   const long long id = i + F.sy * j + F.sz * k;
-  if (!(F.mask[id] & 128)) return;
-  const int i0 = F.plx[i], j0 = F.ply[j], k0 = F.plz[k];
+  if (!(glob(F.mask)[id] & 128)) return;
+  const int i0 = glob(F.plx)[i], j0 = glob(F.ply)[j], k0 = glob(F.plz)[k];
   const int i1 = i0 < C.nx ? i0 + 1 : i0, j1 = j0 < C.ny ? j0 + 1 : j0, k1 = k0 < C.nz ? k0 + 1 : k0;
-  const T wx1 = (T)F.pwx[i], wy1 = (T)F.pwy[j], wz1 = (T)F.pwz[k];
+  const T wx1 = (T)glob(F.pwx)[i], wy1 = (T)glob(F.pwy)[j], wz1 = (T)glob(F.pwz)[k];
   const T wx[2] = {T(1) - wx1, wx1};
   const T wyz[4] = {(T(1) - wy1) * (T(1) - wz1), wy1 * (T(1) - wz1), (T(1) - wy1) * wz1, wy1 * wz1};
   T s = T(0), ws = T(0);
@@ -2166,7 +2167,7 @@ __device__ __forceinline__ void prolong_cell(const DevLevel &F, const DevLevel &
     const int ci = (q & 1) ? i1 : i0, cj = (q & 2) ? j1 : j0, ck = (q & 4) ? k1 : k0;
     const T w = wx[q & 1] * wyz[q >> 1];
     const long long cid = ci + C.sy * cj + C.sz * ck;
-    const T act = (C.mask[cid] & 64) ? w : T(0);
+    const T act = (glob(C.mask)[cid] & 64) ? w : T(0);
     s += act * xc[cid];
     ws += act;
   }
@@ -2214,9 +2215,9 @@ k_prolong(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT fine
   const int ti = lb % nti, rest = lb / nti, tj = rest % ntj, k = 1 + rest / ntj;
   const int ia = 1 + ti * PT_I, ib = min(F.nx, ia + PT_I - 1);
   const int ja = 1 + tj * PT_J, jb = min(F.ny, ja + PT_J - 1);
-  const int ca = F.plx[ia], cb = min(F.plx[ib] + 1, C.nx);
-  const int da = F.ply[ja], db = min(F.ply[jb] + 1, C.ny);
-  const int k0 = F.plz[k], k1 = k0 < C.nz ? k0 + 1 : k0;
+  const int ca = glob(F.plx)[ia], cb = min(glob(F.plx)[ib] + 1, C.nx);
+  const int da = glob(F.ply)[ja], db = min(glob(F.ply)[jb] + 1, C.ny);
+  const int k0 = glob(F.plz)[k], k1 = k0 < C.nz ? k0 + 1 : k0;
   const int ni = cb - ca + 1, nj = db - da + 1;
   const int i = ia + (int)threadIdx.x;
   if (ni > PT_CI || nj > PT_CJ) {  // a box larger than the tile (no level builds one): per cell
@@ -2257,18 +2258,18 @@ k_prolong(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT fine
     }
   }
   if (threadIdx.x < PT_J && ja + (int)threadIdx.x <= jb) {
-    const int j = ja + (int)threadIdx.x, cj0 = F.ply[j];
+    const int j = ja + (int)threadIdx.x, cj0 = glob(F.ply)[j];
     sr0[threadIdx.x] = cj0 - da;
     sr1[threadIdx.x] = (cj0 < C.ny ? cj0 + 1 : cj0) - da;
-    swy[threadIdx.x] = (T)F.pwy[j];
+    swy[threadIdx.x] = (T)glob(F.pwy)[j];
   }
   cp_async_wait_all();
   __syncthreads();
   if (i > ib) return;
   const uint8_t *smb = reinterpret_cast<const uint8_t *>(smw);
-  const int ci0 = F.plx[i];
+  const int ci0 = glob(F.plx)[i];
   const int i0 = ci0 - ca, i1 = (ci0 < C.nx ? ci0 + 1 : ci0) - ca;
-  const T wx1 = (T)F.pwx[i], wz1 = (T)F.pwz[k];
+  const T wx1 = (T)glob(F.pwx)[i], wz1 = (T)glob(F.pwz)[k];
   const T wx[2] = {T(1) - wx1, wx1};
 #pragma unroll
   for (int jj = 0; jj < PT_J; ++jj) {
@@ -2479,7 +2480,7 @@ __device__ void sc_sweep(const DevLevel &L, int axis, int color, T omega) {
     T cprev = T(0), dprev = T(0);
     for (int r = 0; r < n; ++r) {
       const long long id = base + ls * (r + 1);
-      const uint8_t m8 = L.mask[id];
+      const uint8_t m8 = glob(L.mask)[id];
       T aa = T(0), bb = T(1), cc = T(0), dd;
       const bool held = !(m8 & 64) || (((m8 & 63) == 0) && iso_line);
       if (held) {
@@ -2527,7 +2528,7 @@ __device__ void sc_down(const DevLevel &F, const DevLevel &C) {
   for (int c = threadIdx.x; c < nf; c += blockDim.x) {
     const int i = 1 + c % F.nx, j = 1 + (c / F.nx) % F.ny, k = 1 + c / (F.nx * F.ny);
     const long long id = i + F.sy * j + F.sz * k;
-    const uint8_t mk = F.mask[id];
+    const uint8_t mk = glob(F.mask)[id];
     T r = T(0);
     if (mk & 64) r = rhs[id] - apply_row<T>(F, id, i, j, k, mk, x);
     res[id] = r;
@@ -2640,7 +2641,7 @@ __global__ void k_gauge(double *ref, const DevLevel L, int nx, int ny, int nz, c
   if (e >= X * Y * Z) return;
   const int i = (int)(e % X), j = (int)((e / X) % Y), k = (int)(e / (X * Y));
   if (i >= 1 && i <= nx - 1 && j >= 1 && j <= ny - 1 && k >= 1 && k <= nz - 1 &&
-      L.type[i + L.sy * j + L.sz * k] == T_SOLID)
+      glob(L.type)[i + L.sy * j + L.sz * k] == T_SOLID)
     return;  // pure-solid values are held
   ref[i + (long long)(nx + 2) * (j + (long long)(ny + 2) * k)] -= *pa;
 }
@@ -2716,14 +2717,14 @@ cudaError_t finish_field(double *ref, const DevLevel *lev0, int nx, int ny, int 
 __device__ __forceinline__ double face_term(const DevLevel &L, const FaceData &fd, int f, const int (&idx)[3]) {
   const int a = f >> 1, up = f & 1;
   if (fd.pbc[f] == FG_PBC_DIRICHLET) {
-    const double am[3] = {L.amx[idx[0]], L.amy[idx[1]], L.amz[idx[2]]};
-    const double ap[3] = {L.apx[idx[0]], L.apy[idx[1]], L.apz[idx[2]]};
+    const double am[3] = {glob(L.amx)[idx[0]], glob(L.amy)[idx[1]], glob(L.amz)[idx[2]]};
+    const double ap[3] = {glob(L.apx)[idx[0]], glob(L.apy)[idx[1]], glob(L.apz)[idx[2]]};
     return -2.0 * (up ? ap[a] : am[a]) * fd.ppp[f];
   }
   if (fd.pgrad[f]) {
     const int n[3] = {L.nx, L.ny, L.nz};
     const int u = a == 0 ? 1 : 0, v = a == 2 ? 1 : 2;  // transverse axes
-    const double w[3] = {L.wx[idx[0]], L.wy[idx[1]], L.wz[idx[2]]};
+    const double w[3] = {glob(L.wx)[idx[0]], glob(L.wy)[idx[1]], glob(L.wz)[idx[2]]};
     const long long stride = (long long)n[u] + 3;  // reference extent of the first transverse index
     const double g = fd.pgrad[f][idx[u] + stride * idx[v]];
     return up ? -g / w[a] : g / w[a];
@@ -2746,7 +2747,7 @@ __global__ void k_face_rhs(double *rhs, const DevLevel L, FaceData fd) {
   idx[v] = 1 + (int)(e / n[u]);
   idx[a] = up ? n[a] : 1;
   const long long id = idx[0] + L.sy * idx[1] + L.sz * idx[2];
-  if (!(L.mask[id] & 64)) return;
+  if (!(glob(L.mask)[id] & 64)) return;
   int on = 0;  // faces the cell lies on
   for (int q = 0; q < 3; ++q) {
     if (idx[q] == 1) on |= 1 << (2 * q);
@@ -2786,7 +2787,7 @@ k_ref_residual(const double *p, const double *div, const int8_t *ib, const int8_
   if (e < n) {
     const int i = 1 + (int)(e % ni), j = 1 + (int)((e / ni) % nj), k = 1 + (int)(e / (ni * nj));
     const long long NX = nx + 2, NXY = NX * (ny + 2), id = i + NX * j + NXY * k;
-    const double bmx = L.amx[i], bpx = L.apx[i], bmy = L.amy[j], bpy = L.apy[j], bmz = L.amz[k], bpz = L.apz[k];
+    const double bmx = glob(L.amx)[i], bpx = glob(L.apx)[i], bmy = glob(L.amy)[j], bpy = glob(L.apy)[j], bmz = glob(L.amz)[k], bpz = glob(L.apz)[k];
     const double bc = -(bmx + bpx) + -(bmy + bpy) + -(bmz + bpz);
     const double res = div[id] - p[id] * bc - p[id - 1] * bmx - p[id + 1] * bpx - p[id - NX] * bmy -
                        p[id + NX] * bpy - p[id - NXY] * bmz - p[id + NXY] * bpz;
@@ -2962,7 +2963,7 @@ __device__ __forceinline__ dptr<B> kvec(const KDesc &d, void *base, int v) {
 }
 
 __device__ __forceinline__ bool is_row(const DevLevel &L, long long id, uint8_t mk) {
-  return (mk & 64) || L.type[id] == T_GHOST;
+  return (mk & 64) || glob(L.type)[id] == T_GHOST;
 }
 
 // (A x) at an active cell in FP64 from values of type T: the sum of
@@ -2973,7 +2974,7 @@ __device__ __forceinline__ double apply_row_d(const DevLevel &L, long long id, i
   const double xc = (double)x[id];
   const double xn[6] = {(double)x[id - 1],    (double)x[id + 1],    (double)x[id - L.sy],
                         (double)x[id + L.sy], (double)x[id - L.sz], (double)x[id + L.sz]};
-  const double a[6] = {L.amx[i], L.apx[i], L.amy[j], L.apy[j], L.amz[k], L.apz[k]};
+  const double a[6] = {glob(L.amx)[i], glob(L.apx)[i], glob(L.amy)[j], glob(L.apy)[j], glob(L.amz)[k], glob(L.apz)[k]};
   const bool atb[6] = {i == 1, i == L.nx, j == 1, j == L.ny, k == 1, k == L.nz};
   double acc = 0.0, diag = 0.0;
 #pragma unroll
@@ -3027,8 +3028,8 @@ k_kr_resid(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT lev
     double f[4];
     uint8_t m4[4];
     load_run<double, 4>(f, F, id);
-    load_run<uint8_t, 4>(m4, L.mask, id);
-    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    load_run<uint8_t, 4>(m4, glob(L.mask), id);
+    const double ay0 = glob(L.amy)[q.j], ay1 = glob(L.apy)[q.j], az0 = glob(L.amz)[q.k], az1 = glob(L.apz)[q.k];
     B out[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -3037,7 +3038,7 @@ k_kr_resid(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT lev
       if (i <= L.nx && (m4[v] & 64)) {
         double xn[6];
         pv.nbrs(v, xn);
-        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        const double a[6] = {glob(L.amx)[i], glob(L.apx)[i], ay0, ay1, az0, az1};
         rv = f[v] - apply_vals<double>(L, i, q.j, q.k, m4[v], pv.c[v], xn, a);
       }
       out[v] = (B)rv;
@@ -3075,9 +3076,9 @@ k_kr_apply_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
     xv.load(L, x, id);
     uint8_t m4[4];
     int8_t t4[4];
-    load_run<uint8_t, 4>(m4, L.mask, id);
-    load_run<int8_t, 4>(t4, L.type, id);
-    const double ay0 = L.amy[q.j], ay1 = L.apy[q.j], az0 = L.amz[q.k], az1 = L.apz[q.k];
+    load_run<uint8_t, 4>(m4, glob(L.mask), id);
+    load_run<int8_t, 4>(t4, glob(L.type), id);
+    const double ay0 = glob(L.amy)[q.j], ay1 = glob(L.apy)[q.j], az0 = glob(L.amz)[q.k], az1 = glob(L.apz)[q.k];
     B z4[4], w4[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -3088,7 +3089,7 @@ k_kr_apply_q(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT l
       if (i <= L.nx && (m4[v] & 64)) {
         T xn[6];
         xv.nbrs(v, xn);
-        const double a[6] = {L.amx[i], L.apx[i], ay0, ay1, az0, az1};
+        const double a[6] = {glob(L.amx)[i], glob(L.apx)[i], ay0, ay1, az0, az1};
         const bool atb[6] = {i == 1, i == L.nx, q.j == 1, q.j == L.ny, q.k == 1, q.k == L.nz};
         double acc = 0.0, diag = 0.0;
 #pragma unroll
@@ -3318,7 +3319,7 @@ k_kr_vaxpy(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT lev
     store_run<B, 4>(D, e, o, 4);
     if (stage) {
       uint8_t m4[4];
-      load_run<uint8_t, 4>(m4, L.mask, e);
+      load_run<uint8_t, 4>(m4, glob(L.mask), e);
       T r4[4], z4[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) { r4[q] = (m4[q] & 64) ? (T)o[q] : T(0); z4[q] = T(0); }
