@@ -2959,7 +2959,7 @@ cudaError_t ref_change(const double *p, const double *pt, const int8_t *ib, int 
 // Vector v of a Krylov set (basis V or preconditioned Z) of one problem.
 template <typename B>
 __device__ __forceinline__ dptr<B> kvec(const KDesc &d, void *base, int v) {
-  return mkptr(reinterpret_cast<B *>(base) + (long long)v * d.stride, d.n, K_X);
+  return glob(mkptr(reinterpret_cast<B *>(base) + (long long)v * d.stride, d.n, K_X));
 }
 
 __device__ __forceinline__ bool is_row(const DevLevel &L, long long id, uint8_t mk) {
@@ -3014,8 +3014,8 @@ k_kr_resid(const int *FG_RESTRICT off, int nent, const DevLevel *FG_RESTRICT lev
   const DevLevel &L = levs[p];
   const int lb = blockIdx.x - off[p];
   const KDesc &d = kd[p];
-  auto P = mkptr<const double>(d.P, d.n, K_X);
-  auto F = mkptr<const double>(d.F, d.n, K_RHS);
+  auto P = glob(mkptr<const double>(d.P, d.n, K_X));
+  auto F = glob(mkptr<const double>(d.F, d.n, K_RHS));
   auto D = kvec<B>(d, d.V, vd);
   double r2 = 0.0;
 #pragma unroll
@@ -3138,7 +3138,7 @@ k_kr_rows(DevRows R, const DevLevel *lev0, const KDesc *kd, int mode, int vs, in
   const long long o[8] = {0, sy, sy + 1, 1, sz, sz + sy, sz + sy + 1, sz + 1};
   double acc = 0.0;
   if (mode == 0) {
-    auto S = mkptr<const double>(d.P, d.n, K_X);
+    auto S = glob(mkptr<const double>(d.P, d.n, K_X));
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc += R.w[8 * r + q] * S[b + o[q]];
     D[t] = (B)(R.c0[r] + acc - S[t]);
@@ -3341,7 +3341,7 @@ k_kr_update(const int *off, int nent, const KDesc *kd, int ns, const double *coe
   const KDesc &d = kd[p];
   const long long lim = flat_end(d.n);
   const double *cf = coef + (size_t)p * cs;
-  auto P = mkptr<double>(d.P, d.n, K_X);
+  auto P = glob(mkptr<double>(d.P, d.n, K_X));
   double acc[FLAT_PPT][4];
   bool ok[FLAT_PPT];
 #pragma unroll
