@@ -534,6 +534,9 @@ struct fg_batch {
     std::vector<int> key;
     bool nu_tuned = false;
     double solve_ms[4] = {0, 0, 0, 0};
+    // smoothing steps from level 2 down (0, 0: the cfg's nu1, nu2)
+    int cnu1 = 0, cnu2 = 0;
+    double solve_ms_coarse = 0.0;
   } tune;
   // the small levels (k_small_cycle): from level small_L down, one block per
   // problem whose hierarchy reaches small_L (small_L == maxdepth: none)
@@ -983,6 +986,14 @@ static double sweep_bytes(double cells, double omega) {
   return 0.5 * cells * (3.0 * s + 1.0 + (omega != 1.0 ? s : 0.0));
 }
 
+// the smoothing steps before and after the coarse correction at level L
+static int nu_pre(const fg_batch *b, int L) {
+  return (L >= 2 && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu1 : b->cfg.nu1;
+}
+static int nu_post(const fg_batch *b, int L) {
+  return (L >= 2 && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu2 : b->cfg.nu2;
+}
+
 template <typename T>
 static fg_status smooth(fg_batch *b, int L, cudaStream_t s) {
   auto &ls = b->ls[L];
@@ -1015,7 +1026,7 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
   for (int L = 0; L < Ls; ++L) {
     auto &ls = b->ls[L];
     if (!ls.S.empty()) {
-      for (int q = 0; q < b->cfg.nu1; ++q)
+      for (int q = 0; q < nu_pre(b, L); ++q)
         if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
       const size_t e0 = prof_begin(b, s);
       FG_K(k::residual_q<T>(ls.quads, s));
@@ -1031,8 +1042,8 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
   }
   if (Ls < b->maxdepth) {
     const size_t e0 = prof_begin(b, s);
-    FG_K(k::small_cycle<T>(b->n_small, b->d_small, b->d_small_levs, b->small_maxgn, b->cfg.nu1,
-                           b->cfg.nu2, b->cfg.omega, s));
+    FG_K(k::small_cycle<T>(b->n_small, b->d_small, b->d_small_levs, b->small_maxgn, nu_pre(b, Ls),
+                           nu_post(b, Ls), b->cfg.omega, s));
     prof_end(b, e0, FG_PROF_LINE_COARSE, 0.0, s);
   }
   for (int L = std::min(b->maxdepth - 2, Ls - 1); L >= 0; --L) {
@@ -1046,7 +1057,7 @@ static fg_status vcycle(fg_batch *b, cudaStream_t s) {
       FG_K(k::rows_relax<T>(b->rows, b->d_lev0, corr, b->d_tmp, s));
       prof_end(b, e0, FG_PROF_ROWS, 0.0, s);
     }
-    for (int q = 0; q < b->cfg.nu2; ++q)
+    for (int q = 0; q < nu_post(b, L); ++q)
       if ((st = smooth<T>(b, L, s)) != FG_OK) return st;
   }
   return FG_OK;
@@ -2834,6 +2845,22 @@ fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_
   }
   b->cfg.nu1 = cand[bi][0];
   b->cfg.nu2 = cand[bi][1];
+  // then (1, 1) from level 2 down, kept when it is faster still
+  if (cand[bi][0] + cand[bi][1] > 2 && b->maxdepth > 2) {
+    b->tune.cnu1 = b->tune.cnu2 = 1;
+    drop_graphs(b);
+    for (int rep = 0; rep < 2; ++rep) {
+      for (size_t p = 0; p < b->cases.size(); ++p) {
+        const fg_case *c = b->cases[p];
+        FG_CUDA(cudaMemsetAsync(d_p[p], 0, (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2) * sizeof(double),
+                                b->stream));
+      }
+      r = fg_batch_solve_device(b, d_p, d_div, &st);
+      if (r != FG_OK && r != FG_NOT_CONVERGED) return r;
+    }
+    b->tune.solve_ms_coarse = r == FG_OK ? 1e3 * st.seconds : -1.0;
+    if (!(r == FG_OK && 1e3 * st.seconds < best)) b->tune.cnu1 = b->tune.cnu2 = 0;
+  }
   drop_graphs(b);
   b->tune.nu_tuned = true;
   b->tune.key = tune_key(b);
@@ -2856,12 +2883,16 @@ fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out) {
   out->nu2 = b->cfg.nu2;
   for (int q = 0; q < 4; ++q) out->solve_ms[q] = b->tune.solve_ms[q];
   out->tuned = b->tune.nu_tuned ? 1 : 0;
+  out->nu1_coarse = b->tune.cnu1;
+  out->nu2_coarse = b->tune.cnu2;
+  out->solve_ms_coarse = b->tune.solve_ms_coarse;
   return FG_OK;
 }
 
 fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t) {
   if (!b || b->cases.empty() || !t) return FG_BAD_INPUT;
   if (t->nu1 < 0 || t->nu2 < 0 || t->nu1 + t->nu2 > 16) return FG_BAD_INPUT;
+  if (t->nu1_coarse < 0 || t->nu2_coarse < 0 || t->nu1_coarse + t->nu2_coarse > 16) return FG_BAD_INPUT;
   cudaSetDevice(b->device);
   if (!b->stream) cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   for (auto *c : b->cases)
@@ -2890,6 +2921,8 @@ fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t) {
     b->cfg.nu1 = t->nu1;
     b->cfg.nu2 = t->nu2;
   }
+  b->tune.cnu1 = t->nu1_coarse;
+  b->tune.cnu2 = t->nu2_coarse;
   drop_graphs(b);
   b->tune.nu_tuned = false;
   b->tune.key = tune_key(b);

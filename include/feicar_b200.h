@@ -480,6 +480,11 @@ typedef struct fg_tuning {
   int nu1, nu2;                            /* smoothing steps in use */
   double solve_ms[4];                      /* solve time of each (nu1,nu2) candidate, -1 = not converged */
   int tuned;                               /* 1 once fg_*_autotune ran */
+  /* smoothing steps of the levels from level 2 down (0, 0: nu1, nu2 as
+   * the finer levels); the autotuner tries (1, 1) there after choosing
+   * (nu1, nu2) and keeps it when the solve is faster */
+  int nu1_coarse, nu2_coarse;
+  double solve_ms_coarse;                  /* the solve time with them, -1 = not converged, 0 = not tried */
 } fg_tuning;
 fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_tuning *out);
 fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out);

@@ -395,6 +395,28 @@ def test_every_line_family_reaches_the_solution(prec, fam):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_coarse_level_smoothing_steps_reach_the_solution(prec):
+    """V(2,1) on the two finest levels and V(1,1) from level 2 down (the
+    autotuner's coarse candidate) solves to the exact discrete solution."""
+    grid = synth.small_grid(128, 96, 80, (4.0, 3.0, 2.5), stretch=1.5)
+    body = synth.sphere_body((1.7, 1.4, 1.2), 0.9, 3)
+    _, ib, rhs, phi = _problem(grid, [body], seed=12)
+    p_ = fg.FG_PREC_MIXED if prec == "mixed" else fg.FG_PREC_FP64
+    c = fg.Case(grid, fg.default_config(precision=p_, rtol=1e-12, max_cycles=150))
+    c.add_body(body)
+    c.set_iblank_body_fast()
+    c.gcm_set_internal_boundary()
+    c.mg_prepare()
+    fg.case_set_tuning(c, {}, nu=(2, 1), nu_coarse=(1, 1))
+    d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device="cuda")
+    d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda()
+    st = c.solve_poisson_device(d_p.data_ptr(), d_f.data_ptr())
+    assert st["relres"] <= 1e-12
+    assert _relerr(d_p.cpu().numpy().transpose(2, 1, 0), phi, _fluid(grid, ib)) <= TOL
+    c.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_both_colour_sweep_equals_two_launches(prec):
     """The both-colour y/z sweep (one launch, plane-ordered tickets) runs
     the tile of the two colour launches of the block-PCR family on the same
