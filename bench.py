@@ -237,7 +237,7 @@ def run_kernels_only(torch, fg, synth, grid, c, geo, args, dev):
         names = {nm: v for kind in fg.LINE_FAMILIES.values() for v, nm in kind.items()}
         fams = {L: {a: names[row[a]["family"]] for a in row} for L, row in enumerate(tuning["levels"])}
         fg.case_set_tuning(c, fams, nu=(tuning["nu1"], tuning["nu2"]),
-                           nu_coarse=tuple(tuning.get("nu_coarse", (0, 0))))
+                           nu_coarse=tuple(tuning.get("nu_coarse", (0, 0))), coarse_from=tuning.get("coarse_from", 2))
     elif not args.no_autotune:  # the same choices as the headline run
         with torch.cuda.stream(stream):
             tuning = fg.case_autotune(c, d_p.data_ptr(), d_f.data_ptr())

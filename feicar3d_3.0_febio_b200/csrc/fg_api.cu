@@ -534,9 +534,9 @@ struct fg_batch {
     std::vector<int> key;
     bool nu_tuned = false;
     double solve_ms[4] = {0, 0, 0, 0};
-    // smoothing steps from level 2 down (0, 0: the cfg's nu1, nu2)
-    int cnu1 = 0, cnu2 = 0;
-    double solve_ms_coarse = 0.0;
+    // smoothing steps from level cfrom down (0, 0: the cfg's nu1, nu2)
+    int cnu1 = 0, cnu2 = 0, cfrom = 2;
+    double solve_ms_coarse[2] = {0.0, 0.0};
   } tune;
   // the small levels (k_small_cycle): from level small_L down, one block per
   // problem whose hierarchy reaches small_L (small_L == maxdepth: none)
@@ -988,10 +988,10 @@ static double sweep_bytes(double cells, double omega) {
 
 // the smoothing steps before and after the coarse correction at level L
 static int nu_pre(const fg_batch *b, int L) {
-  return (L >= 2 && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu1 : b->cfg.nu1;
+  return (L >= b->tune.cfrom && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu1 : b->cfg.nu1;
 }
 static int nu_post(const fg_batch *b, int L) {
-  return (L >= 2 && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu2 : b->cfg.nu2;
+  return (L >= b->tune.cfrom && b->tune.cnu1 + b->tune.cnu2 > 0) ? b->tune.cnu2 : b->cfg.nu2;
 }
 
 template <typename T>
@@ -2845,21 +2845,28 @@ fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_
   }
   b->cfg.nu1 = cand[bi][0];
   b->cfg.nu2 = cand[bi][1];
-  // then (1, 1) from level 2 down, kept when it is faster still
+  // then (1, 1) from level 2 down, then from level 1 down, the fastest kept
   if (cand[bi][0] + cand[bi][1] > 2 && b->maxdepth > 2) {
-    b->tune.cnu1 = b->tune.cnu2 = 1;
-    drop_graphs(b);
-    for (int rep = 0; rep < 2; ++rep) {
-      for (size_t p = 0; p < b->cases.size(); ++p) {
-        const fg_case *c = b->cases[p];
-        FG_CUDA(cudaMemsetAsync(d_p[p], 0, (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2) * sizeof(double),
-                                b->stream));
+    int keep = 0;  // 0: none, else the level the coarse steps start at
+    for (int from = 2; from >= 1; --from) {
+      b->tune.cnu1 = b->tune.cnu2 = 1;
+      b->tune.cfrom = from;
+      drop_graphs(b);
+      for (int rep = 0; rep < 2; ++rep) {
+        for (size_t p = 0; p < b->cases.size(); ++p) {
+          const fg_case *c = b->cases[p];
+          FG_CUDA(cudaMemsetAsync(d_p[p], 0, (size_t)(c->nx + 2) * (c->ny + 2) * (c->nz + 2) * sizeof(double),
+                                  b->stream));
+        }
+        r = fg_batch_solve_device(b, d_p, d_div, &st);
+        if (r != FG_OK && r != FG_NOT_CONVERGED) return r;
       }
-      r = fg_batch_solve_device(b, d_p, d_div, &st);
-      if (r != FG_OK && r != FG_NOT_CONVERGED) return r;
+      b->tune.solve_ms_coarse[2 - from] = r == FG_OK ? 1e3 * st.seconds : -1.0;
+      if (r == FG_OK && 1e3 * st.seconds < best) { best = 1e3 * st.seconds; keep = from; }
+      else break;  // no gain from level 2: none from level 1 either
     }
-    b->tune.solve_ms_coarse = r == FG_OK ? 1e3 * st.seconds : -1.0;
-    if (!(r == FG_OK && 1e3 * st.seconds < best)) b->tune.cnu1 = b->tune.cnu2 = 0;
+    if (keep) { b->tune.cnu1 = b->tune.cnu2 = 1; b->tune.cfrom = keep; }
+    else { b->tune.cnu1 = b->tune.cnu2 = 0; b->tune.cfrom = 2; }
   }
   drop_graphs(b);
   b->tune.nu_tuned = true;
@@ -2885,7 +2892,9 @@ fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out) {
   out->tuned = b->tune.nu_tuned ? 1 : 0;
   out->nu1_coarse = b->tune.cnu1;
   out->nu2_coarse = b->tune.cnu2;
-  out->solve_ms_coarse = b->tune.solve_ms_coarse;
+  out->solve_ms_coarse[0] = b->tune.solve_ms_coarse[0];
+  out->solve_ms_coarse[1] = b->tune.solve_ms_coarse[1];
+  out->coarse_from = b->tune.cfrom;
   return FG_OK;
 }
 
@@ -2893,6 +2902,7 @@ fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t) {
   if (!b || b->cases.empty() || !t) return FG_BAD_INPUT;
   if (t->nu1 < 0 || t->nu2 < 0 || t->nu1 + t->nu2 > 16) return FG_BAD_INPUT;
   if (t->nu1_coarse < 0 || t->nu2_coarse < 0 || t->nu1_coarse + t->nu2_coarse > 16) return FG_BAD_INPUT;
+  if (t->coarse_from < 0 || t->coarse_from > 2) return FG_BAD_INPUT;
   cudaSetDevice(b->device);
   if (!b->stream) cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   for (auto *c : b->cases)
@@ -2923,6 +2933,7 @@ fg_status fg_batch_set_tuning(fg_batch *b, const fg_tuning *t) {
   }
   b->tune.cnu1 = t->nu1_coarse;
   b->tune.cnu2 = t->nu2_coarse;
+  b->tune.cfrom = t->coarse_from > 0 ? t->coarse_from : 2;
   drop_graphs(b);
   b->tune.nu_tuned = false;
   b->tune.key = tune_key(b);

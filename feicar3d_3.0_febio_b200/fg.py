@@ -629,7 +629,8 @@ class Tuning(C.Structure):
         ("solve_ms", C.c_double * 4),
         ("tuned", C.c_int),
         ("nu1_coarse", C.c_int), ("nu2_coarse", C.c_int),
-        ("solve_ms_coarse", C.c_double),
+        ("solve_ms_coarse", C.c_double * 2),
+        ("coarse_from", C.c_int),
     ]
 
     def as_dict(self):
@@ -644,8 +645,8 @@ class Tuning(C.Structure):
             levels.append(row)
         return {"levels": levels, "nu1": self.nu1, "nu2": self.nu2,
                 "solve_ms_nu11_21_22_33": [round(x, 3) for x in self.solve_ms], "tuned": bool(self.tuned),
-                "nu_coarse": [self.nu1_coarse, self.nu2_coarse],
-                "solve_ms_nu_coarse_11": round(self.solve_ms_coarse, 3)}
+                "nu_coarse": [self.nu1_coarse, self.nu2_coarse], "coarse_from": self.coarse_from,
+                "solve_ms_nu_coarse_11_from_2_1": [round(x, 3) for x in self.solve_ms_coarse]}
 
 
 def _tune_lib():
@@ -673,12 +674,13 @@ def batch_autotune(batch, d_ps, d_divs) -> dict:
     return t.as_dict()
 
 
-def _tuning_struct(families, nu=(0, 0), nu_coarse=(0, 0)):
+def _tuning_struct(families, nu=(0, 0), nu_coarse=(0, 0), coarse_from=2):
     """families: {level: {"x": v, "y": v, "z": v}} or one family per axis
     {"x": v, ...} for every level (LINE_FAMILIES numbers); nu_coarse: the
-    smoothing steps from level 2 down ((0, 0): nu)."""
+    smoothing steps from level coarse_from down ((0, 0): nu)."""
     t = Tuning()
     t.nu1_coarse, t.nu2_coarse = int(nu_coarse[0]), int(nu_coarse[1])
+    t.coarse_from = int(coarse_from)
     t.nlevels = 12
     for L in range(12):
         row = families.get(L, {}) if any(isinstance(k, int) for k in families) else families
@@ -688,13 +690,13 @@ def _tuning_struct(families, nu=(0, 0), nu_coarse=(0, 0)):
     return t
 
 
-def case_set_tuning(case, families, nu=(0, 0), nu_coarse=(0, 0)):
-    t = _tuning_struct(families, nu, nu_coarse)
+def case_set_tuning(case, families, nu=(0, 0), nu_coarse=(0, 0), coarse_from=2):
+    t = _tuning_struct(families, nu, nu_coarse, coarse_from)
     _check(_tune_lib().fg_case_set_tuning(case.h, C.byref(t)), "fg_case_set_tuning")
 
 
-def batch_set_tuning(batch, families, nu=(0, 0), nu_coarse=(0, 0)):
-    t = _tuning_struct(families, nu, nu_coarse)
+def batch_set_tuning(batch, families, nu=(0, 0), nu_coarse=(0, 0), coarse_from=2):
+    t = _tuning_struct(families, nu, nu_coarse, coarse_from)
     _check(_tune_lib().fg_batch_set_tuning(batch.h, C.byref(t)), "fg_batch_set_tuning")
 
 

@@ -480,11 +480,13 @@ typedef struct fg_tuning {
   int nu1, nu2;                            /* smoothing steps in use */
   double solve_ms[4];                      /* solve time of each (nu1,nu2) candidate, -1 = not converged */
   int tuned;                               /* 1 once fg_*_autotune ran */
-  /* smoothing steps of the levels from level 2 down (0, 0: nu1, nu2 as
-   * the finer levels); the autotuner tries (1, 1) there after choosing
-   * (nu1, nu2) and keeps it when the solve is faster */
+  /* smoothing steps of the levels from level coarse_from (1 or 2; 0: 2)
+   * down (0, 0: nu1, nu2 as the finer levels); the autotuner tries (1, 1)
+   * from level 2, then from level 1, after choosing (nu1, nu2) and keeps
+   * the fastest solve */
   int nu1_coarse, nu2_coarse;
-  double solve_ms_coarse;                  /* the solve time with them, -1 = not converged, 0 = not tried */
+  double solve_ms_coarse[2];               /* those solve times, -1 = not converged, 0 = not tried */
+  int coarse_from;
 } fg_tuning;
 fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_tuning *out);
 fg_status fg_batch_get_tuning(const fg_batch *b, fg_tuning *out);

@@ -395,9 +395,10 @@ def test_every_line_family_reaches_the_solution(prec, fam):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
-def test_coarse_level_smoothing_steps_reach_the_solution(prec):
-    """V(2,1) on the two finest levels and V(1,1) from level 2 down (the
-    autotuner's coarse candidate) solves to the exact discrete solution."""
+@pytest.mark.parametrize("cfrom", [2, 1])
+def test_coarse_level_smoothing_steps_reach_the_solution(prec, cfrom):
+    """V(2,1) on the finest levels and V(1,1) from level cfrom down (the
+    autotuner's coarse candidates) solves to the exact discrete solution."""
     grid = synth.small_grid(128, 96, 80, (4.0, 3.0, 2.5), stretch=1.5)
     body = synth.sphere_body((1.7, 1.4, 1.2), 0.9, 3)
     _, ib, rhs, phi = _problem(grid, [body], seed=12)
@@ -407,7 +408,7 @@ def test_coarse_level_smoothing_steps_reach_the_solution(prec):
     c.set_iblank_body_fast()
     c.gcm_set_internal_boundary()
     c.mg_prepare()
-    fg.case_set_tuning(c, {}, nu=(2, 1), nu_coarse=(1, 1))
+    fg.case_set_tuning(c, {}, nu=(2, 1), nu_coarse=(1, 1), coarse_from=cfrom)
     d_p = torch.zeros(grid.shape[::-1], dtype=torch.float64, device="cuda")
     d_f = torch.from_numpy(np.ascontiguousarray(rhs.transpose(2, 1, 0))).cuda()
     st = c.solve_poisson_device(d_p.data_ptr(), d_f.data_ptr())
