@@ -645,8 +645,7 @@ class Tuning(C.Structure):
             levels.append(row)
         return {"levels": levels, "nu1": self.nu1, "nu2": self.nu2,
                 "solve_ms_nu11_21_22_33": [round(x, 3) for x in self.solve_ms], "tuned": bool(self.tuned),
-                "nu_coarse": [self.nu1_coarse, self.nu2_coarse], "coarse_from": self.coarse_from,
-                "solve_ms_nu_coarse_11_from_2_1": [round(x, 3) for x in self.solve_ms_coarse]}
+                "nu_coarse": [self.nu1_coarse, self.nu2_coarse], "coarse_from": self.coarse_from}
 
 
 def _tune_lib():

@@ -481,11 +481,12 @@ typedef struct fg_tuning {
   double solve_ms[4];                      /* solve time of each (nu1,nu2) candidate, -1 = not converged */
   int tuned;                               /* 1 once fg_*_autotune ran */
   /* smoothing steps of the levels from level coarse_from (1 or 2; 0: 2)
-   * down (0, 0: nu1, nu2 as the finer levels); the autotuner tries (1, 1)
-   * from level 2, then from level 1, after choosing (nu1, nu2) and keeps
-   * the fastest solve */
+   * down (0, 0: nu1, nu2 as the finer levels), set by fg_*_set_tuning
+   * only: fewer coarse steps shorten a solve to a given rtol but leave a
+   * residual with a larger error to the exact discrete solution, so the
+   * autotuner (which sees only the time to rtol) leaves them at (0, 0) */
   int nu1_coarse, nu2_coarse;
-  double solve_ms_coarse[2];               /* those solve times, -1 = not converged, 0 = not tried */
+  double solve_ms_coarse[2];               /* reserved (0) */
   int coarse_from;
 } fg_tuning;
 fg_status fg_batch_autotune(fg_batch *b, double **d_p, const double **d_div, fg_tuning *out);
