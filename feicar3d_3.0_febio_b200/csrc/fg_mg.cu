@@ -1495,11 +1495,17 @@ cudaError_t reg_tiles(const DevLevel &L, uint8_t *flags_y, uint8_t *flags_z, cud
   return cudaGetLastError();
 }
 
-// occupancy bound of the y/z PCR kernels
+// occupancy bound of the y/z PCR kernels: the resident threads per SM the
+// register budget is sized for.  The kernels wait on their row loads, so
+// more resident blocks at fewer registers pay until the spills grow:
+// measured on the 512x256x256 case, FP32 256-thread tiles run fastest at
+// 1536 threads (40 registers; 288 -> 242 us per level-0 y sweep against
+// 1024), 128-thread tiles at 1280 (1536 spills more and is slower), FP64
+// at 1024 (450 -> 387 us against 768)
 template <typename T, int CH, int NB>
 struct YpBound {
-  static constexpr int def = ((sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES)) > 0
-                                 ? (sizeof(T) == 4 ? 1024 : 768) / (CH * YP_LINES) : 1;
+  static constexpr int budget = sizeof(T) == 4 ? (CH * YP_LINES >= 256 ? 1536 : 1280) : 1024;
+  static constexpr int def = (budget / (CH * YP_LINES)) > 0 ? budget / (CH * YP_LINES) : 1;
   static constexpr int v = NB > 0 ? NB : def;
 };
 
