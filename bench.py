@@ -59,11 +59,10 @@ RTOL = RTOL_ACCURATE
 # class, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
 # 256^3 case, whose y and z lines run the same kernels as the 512x256x256
 # case's (256-row lines, k_yzline_pcr<float, 8, 32, axis>); a launch moves
-# the same bytes per cell, so the figure scales by the cell count.  z: the
-# mean of the two colours of the regular-tile form; y: a capture of the
-# form that still read every row's mask (0.4 B per cell more).
-DRAM_BYTES_PER_CELL = {("config1", "mixed", "line_y0"): (170.546 + 33.888) / 16.7772,
-                       ("config1", "mixed", "line_z0"): (164.447 + 33.037) / 16.7772}
+# the same bytes per cell, so the figure scales by the cell count.  The
+# mean of the two colour launches of each axis.
+DRAM_BYTES_PER_CELL = {("config1", "mixed", "line_y0"): 197.440 / 16.7772,
+                       ("config1", "mixed", "line_z0"): 197.962 / 16.7772}
 
 
 def _load_pkg():
