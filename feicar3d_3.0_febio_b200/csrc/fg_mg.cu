@@ -1206,7 +1206,7 @@ int line_variant(int axis, int maxn, int v) {
   }
   const bool pcr = v == LV_YPCR || v == LV_YPCRH || v == LV_YPCR4 || v == LV_YWAVE;
   if ((v == LV_YREG || pcr) && maxn > YZ_MAXROWS) v = LV_DEFAULT;
-  if (pcr && v != LV_YPCR && maxn < YP_MINROWS) v = LV_DEFAULT;
+  if (pcr && v != LV_YPCR && v != LV_YWAVE && maxn < YP_MINROWS) v = LV_DEFAULT;
   if (v != LV_YREG && v != LV_YWARP && !pcr)
     v = (maxn >= YP_MINROWS && maxn <= YZ_MAXROWS) ? LV_YPCR : maxn <= YZ_MAXROWS ? LV_YREG : LV_YWARP;
   return v;
@@ -1739,6 +1739,8 @@ cudaError_t line_sweep(const Launch &Lr, int axis, int color, double omega, int 
   }
   if (v == LV_YWAVE) {  // both colours in the colour-0 call
     if (color == 1) return cudaSuccess;
+    if (maxn <= 32) return launch_yzwave<T, 4, 8>(Lr, axis, omega, s);
+    if (maxn <= 64) return launch_yzwave<T, 4, 16>(Lr, axis, omega, s);
     if (maxn <= 128) return launch_yzwave<T, 8, 16>(Lr, axis, omega, s);
     return launch_yzwave<T, 8, 32>(Lr, axis, omega, s);
   }
