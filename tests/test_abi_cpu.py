@@ -70,3 +70,30 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(fg.FGError) as e:
         fg.Case(synth.small_grid(8, 8, 8))
     assert e.value.status == 8  # FG_NO_DEVICE
+
+
+def test_momentum_and_boundary_entry_points_reject_missing_arguments():
+    """The momentum iteration and outer-boundary entry points refuse a
+    missing handle, array or parameter block before any device call."""
+    L = C.CDLL(fg.lib()._name)  # its own function objects: the bindings' argtypes stay untouched
+    vp = C.c_void_p
+    f = L.fg_body_intercept_values_device
+    f.restype = C.c_int
+    f.argtypes = [vp, C.c_int, C.c_double] + [vp] * 4
+    assert f(None, 1, 0.1, None, None, None, None) == 5
+    for n, k in (("fg_itsolv_ad_device", 7), ("fg_calc_residual_ad_device", 9),
+                 ("fg_set_outer_velocity_bc_device", 6), ("fg_set_outer_ghost_velocity_device", 5),
+                 ("fg_enforce_global_mass_consv_device", 8),
+                 ("fg_face_vel_device", 10), ("fg_update_pressure_device", 3)):
+        f = getattr(L, n)
+        f.restype = C.c_int
+        f.argtypes = [vp] * k
+        assert f(*([None] * k)) == 5, n  # FG_BAD_INPUT
+    f = L.fg_solve_ad_device
+    f.restype = C.c_int
+    f.argtypes = [vp] * 15 + [C.c_int, C.c_double, C.c_int, C.c_double, vp]
+    assert f(*([None] * 15), 10, 1e-10, 10, 1e-8, None) == 5
+    f = L.fg_ghostcell_velocity_device
+    f.restype = C.c_int
+    f.argtypes = [vp] * 6 + [C.c_int, C.c_double, vp]
+    assert f(*([None] * 6), 10, 1e-10, None) == 5
